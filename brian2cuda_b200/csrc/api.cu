@@ -1,0 +1,1186 @@
+// Host runtime of libb2b: the C ABI of include/b2b.h.
+//
+// Plays the role of brian2cuda's generated project scaffold (templates/objects.cu array
+// management, templates/network.cu step loop, templates/rand.cu buffers) for the hot path,
+// but as a library: the network is described once, laid out on the GPU by b2b_finalize,
+// and advanced by replaying a CUDA graph of `steps_per_graph` steps per launch with no host
+// synchronisation inside a run.
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+#include <numeric>
+
+#include "b2b_build.h"
+#include "b2b_internal.h"
+
+using namespace b2b;
+
+namespace {
+
+b2b_status fail(b2b_net* net, b2b_status code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (net) net->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t _e = (call);                                                              \
+    if (_e != cudaSuccess)                                                                \
+      return fail(net, B2B_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e));     \
+  } while (0)
+
+#define CHECK(cond, code, ...)                       \
+  do {                                               \
+    if (!(cond)) return fail(net, code, __VA_ARGS__); \
+  } while (0)
+
+#define GUARD_BEGIN try {
+#define GUARD_END                                                     \
+  }                                                                   \
+  catch (const std::bad_alloc&) {                                     \
+    return fail(net, B2B_ERR_OOM, "host allocation failed");          \
+  }
+
+size_t var_size(int dtype, int var) {
+  if (var == B2B_VAR_NOT_REFRACTORY) return 1;
+  return dtype == B2B_F32 ? 4 : 8;
+}
+size_t real_size(int dtype) { return dtype == B2B_F32 ? 4 : 8; }
+
+bool kind_has_var(int kind, int var) {
+  switch (kind) {
+    case KIND_LIF:
+      return var == B2B_VAR_V || var == B2B_VAR_GE || var == B2B_VAR_GI ||
+             var == B2B_VAR_LASTSPIKE || var == B2B_VAR_NOT_REFRACTORY;
+    case KIND_HH:
+      return var >= 0 && var < kMaxVars;
+    default:
+      return false;
+  }
+}
+
+int64_t pad_to(int64_t n, int64_t q) { return (n + q - 1) / q * q; }
+
+// Brian2's timestep(t, dt) on the host.
+int64_t timestep_host(double t, double dt) { return (int64_t)((t + 1e-3 * dt) / dt); }
+
+template <typename T>
+cudaError_t dalloc(Pop& pop, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+  if (e == cudaSuccess) pop.allocs.push_back(*p);
+  return e;
+}
+template <typename T>
+cudaError_t dalloc(Proj& pr, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+  if (e == cudaSuccess) pr.allocs.push_back(*p);
+  return e;
+}
+
+void put_real(std::vector<uint8_t>& buf, int dtype, int64_t i, double v) {
+  if (dtype == B2B_F32) reinterpret_cast<float*>(buf.data())[i] = (float)v;
+  else reinterpret_cast<double*>(buf.data())[i] = v;
+}
+
+LifDev lif_dev(const Group& g, double dt) {
+  const b2b_lif_params& p = g.lif;
+  LifDev d{};
+  const bool leak = std::isfinite(p.taum) && p.taum > 0;
+  d.A = leak ? std::exp(-dt / p.taum) : 1.0;
+  d.De = p.taue > 0 ? std::exp(-dt / p.taue) : 0.0;
+  d.Di = p.taui > 0 ? std::exp(-dt / p.taui) : 0.0;
+  auto coupling = [&](double k, double tau, double D) {
+    if (k == 0.0 || !leak) return 0.0;
+    if (tau == p.taum) return k * (dt / p.taum) * d.A;
+    return k * tau / (tau - p.taum) * (D - d.A);
+  };
+  d.Be = coupling(p.ke, p.taue, d.De);
+  d.Bi = coupling(p.ki, p.taui, d.Di);
+  d.El = p.El;
+  d.Vt = p.Vt;
+  d.Vr = p.Vr;
+  d.ref_steps = p.refractory > 0 ? timestep_host(p.refractory, dt) : -1;
+  d.offset = g.offset;
+  d.n = g.n;
+  d.has_threshold = p.has_threshold;
+  d.has_reset = p.has_reset;
+  d.unless_refractory = p.unless_refractory;
+  return d;
+}
+
+HhDev hh_dev(const Group& g, double dt) {
+  const b2b_hh_params& p = g.hh;
+  HhDev d{};
+  d.Cm = p.Cm; d.gl = p.gl; d.El = p.El; d.EK = p.EK; d.ENa = p.ENa; d.gNa = p.gNa;
+  d.gK = p.gK; d.VT = p.VT; d.Ee = p.Ee; d.Ei = p.Ei;
+  d.De = p.taue > 0 ? std::exp(-dt / p.taue) : 0.0;
+  d.Di = p.taui > 0 ? std::exp(-dt / p.taui) : 0.0;
+  d.Vthr = p.Vthr;
+  d.ref_steps = p.refractory > 0 ? timestep_host(p.refractory, dt) : -1;
+  d.offset = g.offset;
+  d.n = g.n;
+  return d;
+}
+
+bool has_refractory(const Group& g) {
+  if (g.kind == KIND_LIF) return g.lif.refractory > 0;
+  if (g.kind == KIND_HH) return g.hh.refractory > 0;
+  return false;
+}
+
+b2b_status check_net(b2b_net* net) {
+  if (!net) return B2B_ERR_INVALID_ARG;
+  cudaError_t e = cudaSetDevice(net->cfg.device);
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return B2B_OK;
+}
+
+b2b_status add_group(b2b_net* net, Group&& g, int32_t* gid) {
+  CHECK(!net->finalized, B2B_ERR_STATE, "groups must be added before b2b_finalize");
+  CHECK(gid != nullptr, B2B_ERR_INVALID_ARG, "gid is NULL");
+  CHECK(g.n > 0 && g.n < ((int64_t)1 << 31) - 4096, B2B_ERR_INVALID_ARG, "bad group size %lld",
+        (long long)g.n);
+  CHECK(g.dtype == B2B_F32 || g.dtype == B2B_F64, B2B_ERR_INVALID_ARG, "bad dtype %d", g.dtype);
+  g.staged.resize(kMaxVars);
+  net->groups.push_back(std::move(g));
+  *gid = (int32_t)net->groups.size() - 1;
+  return B2B_OK;
+}
+
+b2b_status add_syn(b2b_net* net, Syn&& s, int32_t* sid) {
+  CHECK(!net->finalized, B2B_ERR_STATE, "synapses must be added before b2b_finalize");
+  CHECK(sid != nullptr, B2B_ERR_INVALID_ARG, "sid is NULL");
+  CHECK(s.pre_gid >= 0 && s.pre_gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG,
+        "bad pre group %d", s.pre_gid);
+  CHECK(s.post_gid >= 0 && s.post_gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG,
+        "bad post group %d", s.post_gid);
+  const Group& post = net->groups[s.post_gid];
+  CHECK(post.kind == KIND_LIF || post.kind == KIND_HH, B2B_ERR_INVALID_ARG,
+        "synapse targets must be LIF or HH groups");
+  CHECK(s.target_var == B2B_VAR_V || s.target_var == B2B_VAR_GE || s.target_var == B2B_VAR_GI,
+        B2B_ERR_INVALID_ARG, "target variable must be v, ge or gi");
+  CHECK(s.effect == B2B_EFFECT_ADD || s.effect == B2B_EFFECT_STDP, B2B_ERR_INVALID_ARG,
+        "bad effect %d", s.effect);
+  net->syns.push_back(std::move(s));
+  *sid = (int32_t)net->syns.size() - 1;
+  return B2B_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+b2b_status finalize_pops(b2b_net* net) {
+  const double dt = net->cfg.dt;
+  // populations: one per (kind, dtype), in order of first appearance
+  for (size_t gi = 0; gi < net->groups.size(); ++gi) {
+    Group& g = net->groups[gi];
+    int pi = -1;
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      if (net->pops[p].kind == g.kind && net->pops[p].dtype == g.dtype) pi = (int)p;
+    if (pi < 0) {
+      net->pops.emplace_back();
+      net->pops.back().kind = g.kind;
+      net->pops.back().dtype = g.dtype;
+      pi = (int)net->pops.size() - 1;
+    }
+    Pop& pop = net->pops[pi];
+    g.pop = pi;
+    g.offset = pop.n;
+    pop.n = pad_to(pop.n + g.n, kPad);
+    pop.groups.push_back((int)gi);
+  }
+  // delay range and reset placement, from the synapses
+  for (const Syn& s : net->syns) {
+    Pop& src = net->pops[net->groups[s.pre_gid].pop];
+    src.max_delay = std::max(src.max_delay, s.dmax);
+    const Group& post = net->groups[s.post_gid];
+    if (post.kind == KIND_LIF && post.lif.has_reset && s.target_var == B2B_VAR_V &&
+        !(net->cfg.flags & B2B_NET_RESET_BEFORE_SYNAPSES))
+      net->pops[post.pop].late_reset = true;
+  }
+  for (size_t pi = 0; pi < net->pops.size(); ++pi) {
+    Pop& pop = net->pops[pi];
+    PopDev& D = pop.dev;
+    D.n = pop.n;
+    D.n_groups = (int32_t)pop.groups.size();
+    D.ring_len = pop.max_delay + 2;
+    D.late_reset = pop.late_reset ? 1 : 0;
+    const size_t rs = real_size(pop.dtype);
+    // state
+    if (pop.kind == KIND_LIF || pop.kind == KIND_HH) {
+      for (int v = 0; v < kMaxVars; ++v) {
+        if (!kind_has_var(pop.kind, v)) continue;
+        const size_t es = var_size(pop.dtype, v);
+        std::vector<uint8_t> host(es * pop.n, 0);
+        for (int gi : pop.groups) {
+          const Group& g = net->groups[gi];
+          if (v == B2B_VAR_LASTSPIKE && has_refractory(g))
+            for (int64_t i = 0; i < g.n; ++i) put_real(host, pop.dtype, g.offset + i, -1e4);
+          if (v == B2B_VAR_NOT_REFRACTORY)
+            std::memset(host.data() + g.offset, 1, g.n);
+          if (!g.staged[v].empty())
+            std::memcpy(host.data() + es * g.offset, g.staged[v].data(), g.staged[v].size());
+        }
+        void* d = nullptr;
+        CU(dalloc(pop, (uint8_t**)&d, es * pop.n));
+        CU(cudaMemcpyAsync(d, host.data(), es * pop.n, cudaMemcpyHostToDevice, net->stream));
+        CU(cudaStreamSynchronize(net->stream));
+        D.var[v] = d;
+      }
+    }
+    // parameters
+    std::vector<uint8_t> prm;
+    for (int gi : pop.groups) {
+      const Group& g = net->groups[gi];
+      if (pop.kind == KIND_LIF) {
+        LifDev d = lif_dev(g, dt);
+        prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
+      } else if (pop.kind == KIND_HH) {
+        HhDev d = hh_dev(g, dt);
+        prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
+      } else if (pop.kind == KIND_POISSON) {
+        PoissonDev d{g.rate * dt, g.offset, g.n};
+        prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
+      }
+    }
+    if (!prm.empty()) {
+      CU(dalloc(pop, (uint8_t**)&pop.params_dev, prm.size()));
+      CU(cudaMemcpy(pop.params_dev, prm.data(), prm.size(), cudaMemcpyHostToDevice));
+      D.params = pop.params_dev;
+    }
+    if (pop.groups.size() > 1) {
+      std::vector<int32_t> vg(pop.n / 4, (int32_t)pop.groups.size() - 1);
+      for (size_t k = 0; k < pop.groups.size(); ++k) {
+        const Group& g = net->groups[pop.groups[k]];
+        const int64_t end = k + 1 < pop.groups.size()
+                                ? net->groups[pop.groups[k + 1]].offset
+                                : pop.n;
+        for (int64_t q = g.offset / 4; q < end / 4; ++q) vg[q] = (int32_t)k;
+      }
+      CU(dalloc(pop, &pop.vec_group_dev, vg.size()));
+      CU(cudaMemcpy(pop.vec_group_dev, vg.data(), vg.size() * 4, cudaMemcpyHostToDevice));
+      D.vec_group = pop.vec_group_dev;
+    }
+    // spike-history ring
+    CU(dalloc(pop, &D.ring_idx, (size_t)D.ring_len * pop.n));
+    CU(dalloc(pop, &D.ring_cnt, (size_t)D.ring_len));
+    CU(cudaMemset(D.ring_cnt, 0, sizeof(int32_t) * D.ring_len));
+    // spike monitor
+    int64_t cap = 0;
+    for (int gi : pop.groups) cap += net->groups[gi].mon_cap;
+    if (cap > 0) {
+      CU(dalloc(pop, &D.mon_idx, (size_t)cap));
+      CU(dalloc(pop, &D.mon_step, (size_t)cap));
+      CU(dalloc(pop, &D.mon_cnt, 1));
+      CU(cudaMemset(D.mon_cnt, 0, sizeof(unsigned long long)));
+      D.mon_cap = cap;
+    }
+    // Poisson uniform buffer
+    if (pop.kind == KIND_POISSON) {
+      pop.rng_steps = net->cfg.steps_per_graph;
+      CU(dalloc(pop, (uint8_t**)&pop.rng_buf, rs * pop.rng_steps * pop.n));
+      D.rng = pop.rng_buf;
+      if (!net->gen) {
+        if (curandCreateGenerator(&net->gen, CURAND_RNG_PSEUDO_PHILOX4_32_10) !=
+                CURAND_STATUS_SUCCESS ||
+            curandSetPseudoRandomGeneratorSeed(net->gen, net->cfg.seed) !=
+                CURAND_STATUS_SUCCESS ||
+            curandSetStream(net->gen, net->stream) != CURAND_STATUS_SUCCESS)
+          return fail(net, B2B_ERR_CUDA, "cuRAND generator setup failed");
+      }
+    }
+    // spike generator entries
+    if (pop.kind == KIND_SPIKEGEN) {
+      std::vector<std::pair<int64_t, int32_t>> ent;
+      for (int gi : pop.groups) {
+        const Group& g = net->groups[gi];
+        for (size_t k = 0; k < g.sg_idx.size(); ++k)
+          ent.emplace_back(g.sg_step[k], (int32_t)(g.sg_idx[k] + g.offset));
+      }
+      std::stable_sort(ent.begin(), ent.end(),
+                       [](const auto& a, const auto& b) { return a.first < b.first; });
+      std::vector<int64_t> st(ent.size());
+      std::vector<int32_t> ix(ent.size());
+      for (size_t k = 0; k < ent.size(); ++k) { st[k] = ent[k].first; ix[k] = ent[k].second; }
+      int64_t* dst = nullptr;
+      int32_t* dix = nullptr;
+      CU(dalloc(pop, &dst, st.size()));
+      CU(dalloc(pop, &dix, ix.size()));
+      if (!st.empty()) {
+        CU(cudaMemcpy(dst, st.data(), st.size() * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dix, ix.data(), ix.size() * 4, cudaMemcpyHostToDevice));
+      }
+      D.sg_step = dst;
+      D.sg_idx = dix;
+      D.sg_n = (int64_t)st.size();
+    }
+  }
+  return B2B_OK;
+}
+
+bool same_stdp(const b2b_stdp_params& a, const b2b_stdp_params& b) {
+  return a.taupre == b.taupre && a.taupost == b.taupost && a.dApre == b.dApre &&
+         a.dApost == b.dApost && a.wmin == b.wmin && a.wmax == b.wmax &&
+         a.pre_adds_weight == b.pre_adds_weight;
+}
+
+struct MemberTmp {
+  int32_t *i = nullptr, *j = nullptr, *d = nullptr;
+  void* w = nullptr;
+  uint32_t *keys = nullptr, *vals = nullptr;
+  int64_t* inv = nullptr;
+  void release() {
+    cudaFree(i); cudaFree(j); cudaFree(d); cudaFree(w); cudaFree(keys); cudaFree(vals);
+    i = j = d = nullptr; w = nullptr; keys = vals = nullptr;
+  }
+};
+
+b2b_status build_proj(b2b_net* net, int pj) {
+  Proj& pr = net->projs[pj];
+  const Pop& src = net->pops[pr.src_pop];
+  const Pop& dst = net->pops[pr.dst_pop];
+  const int32_t nd = pr.dmax - pr.dmin + 1;
+  const int64_t nkeys = src.n * (int64_t)nd;
+  cudaStream_t s = net->stream;
+  CU(dalloc(pr, &pr.off, (size_t)nkeys + 1));
+  CU(cudaMemsetAsync(pr.off, 0, sizeof(int64_t) * (nkeys + 1), s));
+  std::vector<MemberTmp> tmp(pr.members.size());
+  struct Cleanup {
+    std::vector<MemberTmp>* t;
+    ~Cleanup() { for (auto& m : *t) m.release(); }
+  } cleanup{&tmp};
+  const size_t rs = real_size(pr.dtype);
+  bool need_w = pr.effect == B2B_EFFECT_STDP;
+  for (int sid : pr.members) {
+    const Syn& sy = net->syns[sid];
+    if (!sy.w.empty()) need_w = true;
+    if (net->syns[pr.members[0]].w_scalar != sy.w_scalar) need_w = true;
+  }
+  // 1) upload or generate, keys, histogram
+  for (size_t m = 0; m < pr.members.size(); ++m) {
+    Syn& sy = net->syns[pr.members[m]];
+    const Group& gpre = net->groups[sy.pre_gid];
+    const Group& gpost = net->groups[sy.post_gid];
+    MemberTmp& t = tmp[m];
+    if (sy.generated) {
+      int64_t n = 0;
+      CU(generate_random_ijd(sy.pre_lo, sy.pre_hi, gpost.n, sy.p, sy.gdmin, sy.gdmax, sy.gseed,
+                             &t.i, &t.j, &t.d, &n, s));
+      sy.n = n;
+    } else {
+      CU(cudaMalloc(&t.i, 4 * std::max<int64_t>(sy.n, 1)));
+      CU(cudaMalloc(&t.j, 4 * std::max<int64_t>(sy.n, 1)));
+      CU(cudaMalloc(&t.d, 4 * std::max<int64_t>(sy.n, 1)));
+      if (sy.n) {
+        CU(cudaMemcpyAsync(t.i, sy.i.data(), 4 * sy.n, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(t.j, sy.j.data(), 4 * sy.n, cudaMemcpyHostToDevice, s));
+        if (!sy.delay.empty()) {
+          CU(cudaMemcpyAsync(t.d, sy.delay.data(), 4 * sy.n, cudaMemcpyHostToDevice, s));
+        } else {
+          std::vector<int32_t> dd(sy.n, sy.delay_scalar);
+          CU(cudaMemcpyAsync(t.d, dd.data(), 4 * sy.n, cudaMemcpyHostToDevice, s));
+          CU(cudaStreamSynchronize(s));
+        }
+      }
+      if (!sy.w.empty()) {
+        CU(cudaMalloc(&t.w, sy.w.size()));
+        CU(cudaMemcpyAsync(t.w, sy.w.data(), sy.w.size(), cudaMemcpyHostToDevice, s));
+      }
+      CU(cudaMalloc(&t.inv, 8 * std::max<int64_t>(sy.n, 1)));
+      pr.allocs.push_back(t.inv);
+      sy.inv = t.inv;
+    }
+    CHECK((uint64_t)(sy.pre_hi - sy.pre_lo) * (uint64_t)nd < (1ull << 32), B2B_ERR_UNSUPPORTED,
+          "pre group size x delay range exceeds 2^32");
+    CHECK(sy.n < (1ll << 31), B2B_ERR_UNSUPPORTED, "more than 2^31 synapses in one Synapses");
+    CU(cudaMalloc(&t.keys, 4 * std::max<int64_t>(sy.n, 1)));
+    CU(cudaMalloc(&t.vals, 4 * std::max<int64_t>(sy.n, 1)));
+    CU(member_keys(t.i, t.d, sy.n, sy.pre_lo, nd, pr.dmin, (gpre.offset + sy.pre_lo) * (int64_t)nd,
+                   t.keys, t.vals, pr.off, s));
+    pr.n_syn += sy.n;
+  }
+  CU(cudaStreamSynchronize(s));
+  // 2) offsets
+  int64_t maxb = 0;
+  CU(counts_to_offsets(pr.off, nkeys, &maxb, s));
+  pr.max_bundle = maxb;
+  CU(dalloc(pr, &pr.post, (size_t)pr.n_syn));
+  if (need_w) CU(dalloc(pr, (uint8_t**)&pr.w, rs * (size_t)pr.n_syn));
+  // 3) sort + scatter
+  for (size_t m = 0; m < pr.members.size(); ++m) {
+    Syn& sy = net->syns[pr.members[m]];
+    const Group& gpre = net->groups[sy.pre_gid];
+    const Group& gpost = net->groups[sy.post_gid];
+    MemberTmp& t = tmp[m];
+    const int64_t key_base = (gpre.offset + sy.pre_lo) * (int64_t)nd;
+    CU(cudaMemcpy(&sy.base, pr.off + key_base, 8, cudaMemcpyDeviceToHost));
+    CU(member_sort_scatter(t.keys, t.vals, sy.n, (uint64_t)(sy.pre_hi - sy.pre_lo) * nd, pr.off,
+                           key_base, t.j,
+                           gpost.offset, t.w, pr.dtype, pr.post, need_w ? pr.w : nullptr,
+                           t.inv, s));
+    if (need_w && !t.w) CU(fill_value((uint8_t*)pr.w + rs * sy.base, pr.dtype, sy.n, sy.w_scalar, s));
+    t.release();
+  }
+  CU(cudaStreamSynchronize(s));
+  // device view
+  ProjDev& D = pr.dev;
+  D.src_ring_idx = src.dev.ring_idx;
+  D.src_ring_cnt = src.dev.ring_cnt;
+  D.src_n = src.n;
+  D.src_ring_len = src.dev.ring_len;
+  D.dmin = pr.dmin;
+  D.nd = nd;
+  D.chunks = (int32_t)std::max<int64_t>(1, (pr.max_bundle + kChunk - 1) / kChunk);
+  D.off = pr.off;
+  D.post = pr.post;
+  D.w = pr.w;
+  D.w_scalar = net->syns[pr.members[0]].w_scalar;
+  D.target = dst.dev.var[pr.target_var];
+  int64_t n_dst_valid = 0;
+  for (int gi : dst.groups) n_dst_valid += net->groups[gi].n;
+  D.aggregate = n_dst_valid < 64 ? 1 : 0;
+  if (pr.effect == B2B_EFFECT_STDP) {
+    const b2b_stdp_params& sp = net->syns[pr.members[0]].stdp;
+    CHECK(pr.n_syn < (1ll << 31), B2B_ERR_UNSUPPORTED, "STDP projection above 2^31 synapses");
+    CU(dalloc(pr, (uint8_t**)&D.apre, rs * (size_t)pr.n_syn));
+    CU(dalloc(pr, (uint8_t**)&D.apost, rs * (size_t)pr.n_syn));
+    CU(dalloc(pr, (uint8_t**)&D.lastupdate, rs * (size_t)pr.n_syn));
+    CU(cudaMemsetAsync(D.apre, 0, rs * pr.n_syn, s));
+    CU(cudaMemsetAsync(D.apost, 0, rs * pr.n_syn, s));
+    CU(cudaMemsetAsync(D.lastupdate, 0, rs * pr.n_syn, s));
+    D.taupre = sp.taupre; D.taupost = sp.taupost; D.dApre = sp.dApre; D.dApost = sp.dApost;
+    D.wmin = sp.wmin; D.wmax = sp.wmax; D.pre_adds_weight = sp.pre_adds_weight;
+    int64_t* poff = nullptr;
+    int32_t* psyn = nullptr;
+    CU(dalloc(pr, &poff, (size_t)dst.n + 1));
+    CU(dalloc(pr, &psyn, (size_t)pr.n_syn));
+    int64_t maxp = 0;
+    CU(build_post_index(pr.post, pr.n_syn, 0, dst.n, poff, psyn, &maxp, s));
+    pr.max_post_bundle = maxp;
+    D.post_ring_idx = dst.dev.ring_idx;
+    D.post_ring_cnt = dst.dev.ring_cnt;
+    D.post_src_n = dst.n;
+    D.post_ring_len = dst.dev.ring_len;
+    D.post_chunks = (int32_t)std::max<int64_t>(1, (maxp + kChunk - 1) / kChunk);
+    D.post_off = poff;
+    D.post_syn = psyn;
+  }
+  return B2B_OK;
+}
+
+b2b_status finalize_projs(b2b_net* net) {
+  // merge Synapses objects into projections
+  for (size_t si = 0; si < net->syns.size(); ++si) {
+    Syn& sy = net->syns[si];
+    const Group& gpre = net->groups[sy.pre_gid];
+    const Group& gpost = net->groups[sy.post_gid];
+    int pj = -1;
+    for (size_t p = 0; p < net->projs.size() && pj < 0; ++p) {
+      Proj& pr = net->projs[p];
+      if (pr.src_pop != gpre.pop || pr.dst_pop != gpost.pop || pr.target_var != sy.target_var ||
+          pr.effect != sy.effect)
+        continue;
+      if (sy.effect == B2B_EFFECT_STDP && !same_stdp(net->syns[pr.members[0]].stdp, sy.stdp))
+        continue;
+      bool clash = false;
+      for (int m : pr.members) {
+        const Syn& o = net->syns[m];
+        clash |= o.pre_gid == sy.pre_gid && o.pre_lo < sy.pre_hi && sy.pre_lo < o.pre_hi;
+      }
+      if (!clash) pj = (int)p;
+    }
+    if (pj < 0) {
+      net->projs.emplace_back();
+      Proj& pr = net->projs.back();
+      pr.src_pop = gpre.pop;
+      pr.dst_pop = gpost.pop;
+      pr.target_var = sy.target_var;
+      pr.effect = sy.effect;
+      pr.dtype = gpost.dtype;
+      pr.dmin = sy.dmin;
+      pr.dmax = sy.dmax;
+      pj = (int)net->projs.size() - 1;
+    }
+    Proj& pr = net->projs[pj];
+    pr.members.push_back((int)si);
+    pr.dmin = std::min(pr.dmin, sy.dmin);
+    pr.dmax = std::max(pr.dmax, sy.dmax);
+    sy.proj = pj;
+  }
+  for (Proj& pr : net->projs)
+    std::sort(pr.members.begin(), pr.members.end(), [&](int a, int b) {
+      return net->groups[net->syns[a].pre_gid].offset + net->syns[a].pre_lo <
+             net->groups[net->syns[b].pre_gid].offset + net->syns[b].pre_lo;
+    });
+  for (size_t p = 0; p < net->projs.size(); ++p) {
+    b2b_status st = build_proj(net, (int)p);
+    if (st != B2B_OK) return st;
+  }
+  return B2B_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+b2b_status enqueue_steps(b2b_net* net, int kk) {
+  for (int k = 0; k < kk; ++k) {
+    for (const Pop& pop : net->pops) {
+      CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      ++net->launches;
+    }
+    for (const Proj& pr : net->projs) {
+      CU(launch_proj_pre(pr, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      ++net->launches;
+    }
+    for (const Proj& pr : net->projs) {
+      if (pr.effect != B2B_EFFECT_STDP) continue;
+      CU(launch_proj_post(pr, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      ++net->launches;
+    }
+    for (const Pop& pop : net->pops) {
+      if (!pop.late_reset) continue;
+      CU(launch_pop_late_reset(pop, net->d_clock, k, net->stream));
+      ++net->launches;
+    }
+  }
+  CU(launch_tick(net->d_clock, kk, net->stream));
+  ++net->launches;
+  return B2B_OK;
+}
+
+b2b_status refill_rng(b2b_net* net, int kk) {
+  for (Pop& pop : net->pops) {
+    if (pop.kind != KIND_POISSON) continue;
+    const size_t n = (size_t)kk * pop.n;
+    curandStatus_t st = pop.dtype == B2B_F32
+                            ? curandGenerateUniform(net->gen, (float*)pop.rng_buf, n)
+                            : curandGenerateUniformDouble(net->gen, (double*)pop.rng_buf, n);
+    if (st != CURAND_STATUS_SUCCESS)
+      return fail(net, B2B_ERR_CUDA, "curandGenerateUniform failed (%d)", (int)st);
+  }
+  return B2B_OK;
+}
+
+b2b_status capture_graph(b2b_net* net) {
+  const int64_t before = net->launches;
+  CU(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+  b2b_status st = enqueue_steps(net, net->cfg.steps_per_graph);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(net->stream, &g);
+  net->launches = before;
+  if (st != B2B_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  e = cudaGraphInstantiate(&net->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  net->graph_nodes = (int64_t)nodes;
+  net->graph_steps = net->cfg.steps_per_graph;
+  return B2B_OK;
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+int32_t b2b_abi_version(void) { return B2B_ABI_VERSION; }
+
+const char* b2b_status_string(b2b_status s) {
+  switch (s) {
+    case B2B_OK: return "ok";
+    case B2B_ERR_INVALID_ARG: return "invalid argument";
+    case B2B_ERR_OOM: return "out of memory";
+    case B2B_ERR_QUEUE_OVERFLOW: return "device buffer overflow";
+    case B2B_ERR_TIMEOUT: return "device wait timed out";
+    case B2B_ERR_CUDA: return "CUDA error";
+    case B2B_ERR_STATE: return "invalid state";
+    case B2B_ERR_UNSUPPORTED: return "unsupported";
+    case B2B_ERR_INDEX: return "index out of range";
+    default: return "unknown status";
+  }
+}
+
+b2b_status b2b_last_error(const b2b_net* net, char* buf, size_t len) {
+  if (!net || !buf || len == 0) return B2B_ERR_INVALID_ARG;
+  std::snprintf(buf, len, "%s", net->err.c_str());
+  return B2B_OK;
+}
+
+b2b_status b2b_create(const b2b_config* cfg, b2b_net** out) {
+  if (!cfg || !out) return B2B_ERR_INVALID_ARG;
+  if (!(cfg->dt > 0) || !std::isfinite(cfg->dt)) return B2B_ERR_INVALID_ARG;
+  *out = nullptr;
+  b2b_net* net = new (std::nothrow) b2b_net();
+  if (!net) return B2B_ERR_OOM;
+  net->cfg = *cfg;
+  if (net->cfg.steps_per_graph <= 0) net->cfg.steps_per_graph = 50;
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) {
+    if (cfg->stream) {
+      net->stream = (cudaStream_t)cfg->stream;
+    } else {
+      e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
+      net->own_stream = e == cudaSuccess;
+    }
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&net->d_clock, sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&net->d_status, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemset(net->d_clock, 0, sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMemset(net->d_status, 0, sizeof(int32_t));
+  if (e != cudaSuccess) {
+    b2b_destroy(net);
+    return e == cudaErrorMemoryAllocation ? B2B_ERR_OOM : B2B_ERR_CUDA;
+  }
+  *out = net;
+  return B2B_OK;
+}
+
+b2b_status b2b_destroy(b2b_net* net) {
+  if (!net) return B2B_ERR_INVALID_ARG;
+  cudaSetDevice(net->cfg.device);
+  if (net->stream) cudaStreamSynchronize(net->stream);
+  const std::vector<b2b_hines*> hines = net->hines;
+  for (b2b_hines* h : hines) b2b_hines_destroy(h);
+  if (net->graph) cudaGraphExecDestroy(net->graph);
+  if (net->gen) curandDestroyGenerator(net->gen);
+  for (Pop& p : net->pops)
+    for (void* a : p.allocs) cudaFree(a);
+  for (Proj& p : net->projs)
+    for (void* a : p.allocs) cudaFree(a);
+  cudaFree(net->d_clock);
+  cudaFree(net->d_status);
+  if (net->own_stream) cudaStreamDestroy(net->stream);
+  delete net;
+  return B2B_OK;
+}
+
+b2b_status b2b_group_lif(b2b_net* net, int64_t n, int32_t dtype, const b2b_lif_params* p,
+                         int32_t* gid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(p != nullptr, B2B_ERR_INVALID_ARG, "params is NULL");
+  CHECK(!(p->taum <= 0) && !(p->taue < 0) && !(p->taui < 0) && !(p->refractory < 0),
+        B2B_ERR_INVALID_ARG, "time constants must be positive");
+  GUARD_BEGIN
+  Group g;
+  g.kind = KIND_LIF; g.n = n; g.dtype = dtype; g.lif = *p;
+  return add_group(net, std::move(g), gid);
+  GUARD_END
+}
+
+b2b_status b2b_group_hh(b2b_net* net, int64_t n, int32_t dtype, const b2b_hh_params* p,
+                        int32_t* gid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(p != nullptr, B2B_ERR_INVALID_ARG, "params is NULL");
+  CHECK(p->Cm > 0 && p->taue > 0 && p->taui > 0 && !(p->refractory < 0), B2B_ERR_INVALID_ARG,
+        "Cm and time constants must be positive");
+  GUARD_BEGIN
+  Group g;
+  g.kind = KIND_HH; g.n = n; g.dtype = dtype; g.hh = *p;
+  return add_group(net, std::move(g), gid);
+  GUARD_END
+}
+
+b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate_hz,
+                             int32_t* gid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(rate_hz >= 0 && std::isfinite(rate_hz), B2B_ERR_INVALID_ARG, "bad rate");
+  GUARD_BEGIN
+  Group g;
+  g.kind = KIND_POISSON; g.n = n; g.dtype = dtype; g.rate = rate_hz;
+  return add_group(net, std::move(g), gid);
+  GUARD_END
+}
+
+b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const int32_t* idx,
+                              const int64_t* step, int32_t* gid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(n_spikes >= 0 && (n_spikes == 0 || (idx && step)), B2B_ERR_INVALID_ARG,
+        "bad spike list");
+  GUARD_BEGIN
+  Group g;
+  g.kind = KIND_SPIKEGEN; g.n = n; g.dtype = B2B_F32;
+  std::vector<std::pair<int64_t, int32_t>> ent;
+  for (int64_t k = 0; k < n_spikes; ++k) {
+    CHECK(idx[k] >= 0 && idx[k] < n && step[k] >= 0, B2B_ERR_INDEX,
+          "spike %lld: index %d / step %lld out of range", (long long)k, idx[k],
+          (long long)step[k]);
+    ent.emplace_back(step[k], idx[k]);
+  }
+  std::sort(ent.begin(), ent.end());
+  for (size_t k = 1; k < ent.size(); ++k)
+    CHECK(ent[k] != ent[k - 1], B2B_ERR_INVALID_ARG, "neuron %d spikes twice in step %lld",
+          ent[k].second, (long long)ent[k].first);
+  for (auto& e : ent) { g.sg_step.push_back(e.first); g.sg_idx.push_back(e.second); }
+  return add_group(net, std::move(g), gid);
+  GUARD_END
+}
+
+b2b_status b2b_state_set(b2b_net* net, int32_t gid, int32_t var, const void* host, int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  Group& g = net->groups[gid];
+  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(host && n == g.n, B2B_ERR_INVALID_ARG, "expected %lld values", (long long)g.n);
+  const size_t es = var_size(g.dtype, var);
+  GUARD_BEGIN
+  if (!net->finalized) {
+    g.staged[var].assign((const uint8_t*)host, (const uint8_t*)host + es * n);
+    return B2B_OK;
+  }
+  uint8_t* d = (uint8_t*)net->pops[g.pop].dev.var[var] + es * g.offset;
+  CU(cudaMemcpyAsync(d, host, es * n, cudaMemcpyHostToDevice, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_state_get(b2b_net* net, int32_t gid, int32_t var, void* host, int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  Group& g = net->groups[gid];
+  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(host && n == g.n, B2B_ERR_INVALID_ARG, "expected %lld values", (long long)g.n);
+  CHECK(net->finalized, B2B_ERR_STATE, "state is on the device only after b2b_finalize");
+  const size_t es = var_size(g.dtype, var);
+  const uint8_t* d = (const uint8_t*)net->pops[g.pop].dev.var[var] + es * g.offset;
+  CU(cudaMemcpyAsync(host, d, es * n, cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  return B2B_OK;
+}
+
+b2b_status b2b_state_ptr(b2b_net* net, int32_t gid, int32_t var, void** dev, int64_t* n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  Group& g = net->groups[gid];
+  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(dev && n, B2B_ERR_INVALID_ARG, "NULL output");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  *dev = (uint8_t*)net->pops[g.pop].dev.var[var] + var_size(g.dtype, var) * g.offset;
+  *n = g.n;
+  return B2B_OK;
+}
+
+b2b_status b2b_synapses(b2b_net* net, int32_t pre_gid, int32_t post_gid, int32_t target_var,
+                        int32_t effect, int64_t n_syn, const int32_t* i, const int32_t* j,
+                        const void* w, double w_scalar, const int32_t* delay_steps,
+                        int32_t delay_scalar, const b2b_stdp_params* stdp, int32_t* sid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(pre_gid >= 0 && pre_gid < (int)net->groups.size() && post_gid >= 0 &&
+            post_gid < (int)net->groups.size(),
+        B2B_ERR_INVALID_ARG, "bad group id");
+  CHECK(n_syn >= 0 && (n_syn == 0 || (i && j)), B2B_ERR_INVALID_ARG, "bad synapse arrays");
+  CHECK(effect != B2B_EFFECT_STDP || stdp, B2B_ERR_INVALID_ARG, "STDP needs parameters");
+  CHECK(delay_steps || delay_scalar >= 0, B2B_ERR_INVALID_ARG, "negative delay");
+  GUARD_BEGIN
+  const Group& gpre = net->groups[pre_gid];
+  const Group& gpost = net->groups[post_gid];
+  Syn s;
+  s.pre_gid = pre_gid; s.post_gid = post_gid; s.target_var = target_var; s.effect = effect;
+  s.n = n_syn;
+  s.i.assign(i, i + n_syn);
+  s.j.assign(j, j + n_syn);
+  int32_t dmin = delay_scalar, dmax = delay_scalar;
+  for (int64_t k = 0; k < n_syn; ++k) {
+    CHECK(i[k] >= 0 && i[k] < gpre.n && j[k] >= 0 && j[k] < gpost.n, B2B_ERR_INDEX,
+          "synapse %lld: (%d, %d) outside (%lld, %lld)", (long long)k, i[k], j[k],
+          (long long)gpre.n, (long long)gpost.n);
+  }
+  if (delay_steps) {
+    s.delay.assign(delay_steps, delay_steps + n_syn);
+    dmin = n_syn ? INT32_MAX : 0;
+    dmax = 0;
+    for (int64_t k = 0; k < n_syn; ++k) {
+      CHECK(delay_steps[k] >= 0, B2B_ERR_INVALID_ARG, "negative delay at synapse %lld",
+            (long long)k);
+      dmin = std::min(dmin, delay_steps[k]);
+      dmax = std::max(dmax, delay_steps[k]);
+    }
+  }
+  s.delay_scalar = delay_scalar;
+  s.dmin = dmin; s.dmax = dmax;
+  s.pre_lo = 0;
+  s.pre_hi = (int32_t)gpre.n;
+  if (w) {
+    const size_t rs = real_size(gpost.dtype);
+    s.w.assign((const uint8_t*)w, (const uint8_t*)w + rs * n_syn);
+  }
+  s.w_scalar = w_scalar;
+  if (stdp) s.stdp = *stdp;
+  return add_syn(net, std::move(s), sid);
+  GUARD_END
+}
+
+b2b_status b2b_synapses_random(b2b_net* net, int32_t pre_gid, int32_t pre_lo, int32_t pre_hi,
+                               int32_t post_gid, int32_t target_var, double p, int32_t dmin,
+                               int32_t dmax, double w, uint64_t seed, int32_t* sid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(p >= 0 && p <= 1, B2B_ERR_INVALID_ARG, "p must be in [0, 1]");
+  CHECK(dmin >= 0 && dmax >= dmin, B2B_ERR_INVALID_ARG, "bad delay range");
+  CHECK(pre_gid >= 0 && pre_gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG,
+        "bad pre group %d", pre_gid);
+  CHECK(pre_lo >= 0 && pre_lo < pre_hi && pre_hi <= net->groups[pre_gid].n, B2B_ERR_INVALID_ARG,
+        "bad presynaptic range [%d, %d)", pre_lo, pre_hi);
+  GUARD_BEGIN
+  Syn s;
+  s.pre_gid = pre_gid; s.post_gid = post_gid; s.target_var = target_var;
+  s.effect = B2B_EFFECT_ADD;
+  s.generated = true;
+  s.p = p; s.gdmin = dmin; s.gdmax = dmax; s.gseed = seed;
+  s.dmin = dmin; s.dmax = dmax;
+  s.pre_lo = pre_lo;
+  s.pre_hi = pre_hi;
+  s.w_scalar = w;
+  return add_syn(net, std::move(s), sid);
+  GUARD_END
+}
+
+b2b_status b2b_spikemon(b2b_net* net, int32_t gid, int64_t capacity) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "monitors must be added before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  CHECK(capacity > 0, B2B_ERR_INVALID_ARG, "capacity must be positive");
+  net->groups[gid].mon_cap = capacity;
+  return B2B_OK;
+}
+
+b2b_status b2b_finalize(b2b_net* net) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "already finalized");
+  GUARD_BEGIN
+  b2b_status st = finalize_pops(net);
+  if (st == B2B_OK) st = finalize_projs(net);
+  if (st != B2B_OK) return st;
+  CU(cudaMemcpy(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice));
+  CU(cudaDeviceSynchronize());
+  net->finalized = true;
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_run(b2b_net* net, int64_t n_steps) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(n_steps >= 0, B2B_ERR_INVALID_ARG, "negative step count");
+  const int K = net->cfg.steps_per_graph;
+  const bool use_graph = !(net->cfg.flags & B2B_NET_NO_GRAPH);
+  while (n_steps > 0) {
+    const int kk = (int)std::min<int64_t>(n_steps, K);
+    if (b2b_status st = refill_rng(net, kk)) return st;
+    if (use_graph && kk == K) {
+      if (!net->graph) {
+        if (b2b_status st = capture_graph(net)) return st;
+      }
+      CU(cudaGraphLaunch(net->graph, net->stream));
+      net->launches += net->graph_nodes;
+    } else {
+      if (b2b_status st = enqueue_steps(net, kk)) return st;
+    }
+    net->last_chunk_steps = kk;
+    net->ts += kk;
+    n_steps -= kk;
+  }
+  return B2B_OK;
+}
+
+b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
+                       int32_t cap, int32_t* n_sites) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(n_steps > 0 && n_sites, B2B_ERR_INVALID_ARG, "bad arguments");
+  GUARD_BEGIN
+  struct Site { int kind; int idx; };
+  std::vector<Site> sites;
+  for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
+  for (size_t p = 0; p < net->projs.size(); ++p) sites.push_back({2, (int)p});
+  for (size_t p = 0; p < net->projs.size(); ++p)
+    if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    if (net->pops[p].late_reset) sites.push_back({4, (int)p});
+  const size_t ns = sites.size();
+  std::vector<cudaEvent_t> ev(2 * ns);
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  std::vector<double> acc(ns, 0.0);
+  b2b_status result = B2B_OK;
+  for (int64_t step = 0; step < n_steps && result == B2B_OK; ++step) {
+    if ((result = refill_rng(net, 1)) != B2B_OK) break;
+    for (size_t k = 0; k < ns && result == B2B_OK; ++k) {
+      const Site& s = sites[k];
+      cudaEventRecord(ev[2 * k], net->stream);
+      cudaError_t e = cudaSuccess;
+      const int64_t* clk = net->d_clock;
+      if (s.kind == 1) e = launch_pop_step(net->pops[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
+      cudaEventRecord(ev[2 * k + 1], net->stream);
+      if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
+      ++net->launches;
+    }
+    if (result != B2B_OK) break;
+    cudaError_t e = launch_tick(net->d_clock, 1, net->stream);
+    ++net->launches;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+    if (e != cudaSuccess) { result = fail(net, B2B_ERR_CUDA, "profile: %s", cudaGetErrorString(e)); break; }
+    for (size_t k = 0; k < ns; ++k) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+      acc[k] += ms;
+    }
+    net->ts += 1;
+    net->last_chunk_steps = 1;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (result != B2B_OK) return result;
+  *n_sites = (int32_t)ns;
+  for (size_t k = 0; k < ns && (int32_t)k < cap; ++k) {
+    if (mean_ms) mean_ms[k] = acc[k] / (double)n_steps;
+    if (site_kind) site_kind[k] = sites[k].kind;
+  }
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_sync(b2b_net* net, int32_t* device_status) {
+  if (b2b_status st = check_net(net)) return st;
+  CU(cudaStreamSynchronize(net->stream));
+  int32_t s = 0;
+  CU(cudaMemcpy(&s, net->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (device_status) *device_status = s;
+  return B2B_OK;
+}
+
+b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t) {
+  if (!net) return B2B_ERR_INVALID_ARG;
+  if (timestep) *timestep = net->ts;
+  if (t) *t = (double)net->ts * net->cfg.dt;
+  return B2B_OK;
+}
+
+b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n) {
+  if (!net || !n) return B2B_ERR_INVALID_ARG;
+  *n = net->launches;
+  return B2B_OK;
+}
+
+b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
+                            int64_t* step, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  CHECK(n != nullptr, B2B_ERR_INVALID_ARG, "n is NULL");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  const Group& g = net->groups[gid];
+  CHECK(g.mon_cap > 0, B2B_ERR_STATE, "group %d has no spike monitor", gid);
+  GUARD_BEGIN
+  const PopDev& D = net->pops[g.pop].dev;
+  CU(cudaStreamSynchronize(net->stream));
+  unsigned long long total = 0;
+  CU(cudaMemcpy(&total, D.mon_cnt, sizeof(total), cudaMemcpyDeviceToHost));
+  const int64_t m = std::min<int64_t>((int64_t)total, D.mon_cap);
+  std::vector<int32_t> hi(m);
+  std::vector<int64_t> hs(m);
+  if (m) {
+    CU(cudaMemcpy(hi.data(), D.mon_idx, 4 * m, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(hs.data(), D.mon_step, 8 * m, cudaMemcpyDeviceToHost));
+  }
+  std::vector<std::pair<int64_t, int32_t>> ent;
+  for (int64_t k = 0; k < m; ++k)
+    if (hi[k] >= g.offset && hi[k] < g.offset + g.n)
+      ent.emplace_back(hs[k], (int32_t)(hi[k] - g.offset));
+  std::sort(ent.begin(), ent.end());
+  *n = (int64_t)ent.size();
+  for (int64_t k = 0; k < (int64_t)ent.size() && k < cap; ++k) {
+    if (idx) idx[k] = ent[k].second;
+    if (step) step[k] = ent[k].first;
+  }
+  if ((int64_t)total > D.mon_cap)
+    return fail(net, B2B_ERR_QUEUE_OVERFLOW, "spike monitor overflowed (%llu > %lld)",
+                total, (long long)D.mon_cap);
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total,
+                              int64_t* n, int32_t* idx, int64_t* step, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  CHECK(total && n && start >= 0 && cap >= 0, B2B_ERR_INVALID_ARG, "bad arguments");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  const Group& g = net->groups[gid];
+  CHECK(g.mon_cap > 0, B2B_ERR_STATE, "group %d has no spike monitor", gid);
+  const PopDev& D = net->pops[g.pop].dev;
+  unsigned long long rec = 0;
+  CU(cudaMemcpyAsync(&rec, D.mon_cnt, sizeof(rec), cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  *total = (int64_t)rec;
+  *n = 0;
+  const int64_t stored = std::min<int64_t>((int64_t)rec, D.mon_cap);
+  const int64_t hi = std::min<int64_t>(stored, start + cap);
+  if (hi <= start) return B2B_OK;
+  const int64_t m = hi - start;
+  CU(cudaMemcpyAsync(idx, D.mon_idx + start, 4 * m, cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaMemcpyAsync(step, D.mon_step + start, 8 * m, cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  int64_t k = 0;
+  for (int64_t r = 0; r < m; ++r) {
+    if (idx[r] < g.offset || idx[r] >= g.offset + g.n) continue;
+    idx[k] = (int32_t)(idx[r] - g.offset);
+    step[k] = step[r];
+    ++k;
+  }
+  *n = k;
+  if ((int64_t)rec > D.mon_cap)
+    return fail(net, B2B_ERR_QUEUE_OVERFLOW, "spike monitor overflowed");
+  return B2B_OK;
+}
+
+b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  CHECK(n != nullptr, B2B_ERR_INVALID_ARG, "n is NULL");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  GUARD_BEGIN
+  const Group& g = net->groups[gid];
+  const PopDev& D = net->pops[g.pop].dev;
+  *n = 0;
+  if (net->ts == 0) return B2B_OK;
+  CU(cudaStreamSynchronize(net->stream));
+  const int slot = (int)((net->ts - 1) % D.ring_len);
+  int32_t cnt = 0;
+  CU(cudaMemcpy(&cnt, D.ring_cnt + slot, 4, cudaMemcpyDeviceToHost));
+  std::vector<int32_t> h(cnt);
+  if (cnt) CU(cudaMemcpy(h.data(), D.ring_idx + (int64_t)slot * D.n, 4 * (size_t)cnt,
+                         cudaMemcpyDeviceToHost));
+  std::vector<int32_t> mine;
+  for (int32_t x : h)
+    if (x >= g.offset && x < g.offset + g.n) mine.push_back((int32_t)(x - g.offset));
+  std::sort(mine.begin(), mine.end());
+  *n = (int64_t)mine.size();
+  if (idx)
+    for (int64_t k = 0; k < (int64_t)mine.size() && k < cap; ++k) idx[k] = mine[k];
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_queue_get(b2b_net* net, int32_t sid, int64_t* n, int32_t* offset, int32_t* pre,
+                         int32_t* delay, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(sid >= 0 && sid < (int)net->syns.size(), B2B_ERR_INVALID_ARG, "bad synapses %d", sid);
+  CHECK(n != nullptr, B2B_ERR_INVALID_ARG, "n is NULL");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  GUARD_BEGIN
+  const Syn& sy = net->syns[sid];
+  const Proj& pr = net->projs[sy.proj];
+  const Group& gpre = net->groups[sy.pre_gid];
+  const PopDev& S = net->pops[gpre.pop].dev;
+  const int32_t nd = pr.dmax - pr.dmin + 1;
+  CU(cudaStreamSynchronize(net->stream));
+  const int64_t lo = gpre.offset + sy.pre_lo, hi = gpre.offset + sy.pre_hi;
+  std::vector<int64_t> off((size_t)(hi - lo) * nd + 1);
+  CU(cudaMemcpy(off.data(), pr.off + lo * (int64_t)nd, 8 * off.size(), cudaMemcpyDeviceToHost));
+  std::vector<int32_t> cnt(S.ring_len);
+  CU(cudaMemcpy(cnt.data(), S.ring_cnt, 4 * S.ring_len, cudaMemcpyDeviceToHost));
+  std::vector<std::vector<int32_t>> rows(S.ring_len);
+  struct E { int32_t a, p, d; };
+  std::vector<E> out;
+  const int64_t last = net->ts - 1;
+  for (int32_t a = 1; a <= pr.dmax && last >= 0; ++a) {
+    for (int32_t d = std::max(a, pr.dmin); d <= pr.dmax; ++d) {
+      const int64_t st = last + a - d;
+      if (st < 0) continue;
+      const int slot = (int)(st % S.ring_len);
+      if (rows[slot].empty() && cnt[slot] > 0) {
+        rows[slot].resize(cnt[slot]);
+        CU(cudaMemcpy(rows[slot].data(), S.ring_idx + (int64_t)slot * S.n, 4 * (size_t)cnt[slot],
+                      cudaMemcpyDeviceToHost));
+      }
+      for (int32_t x : rows[slot]) {
+        if (x < lo || x >= hi) continue;
+        const int64_t key = (int64_t)(x - lo) * nd + (d - pr.dmin);
+        if (off[key + 1] > off[key]) out.push_back({a, (int32_t)(x - gpre.offset), d});
+      }
+    }
+  }
+  std::sort(out.begin(), out.end(), [](const E& x, const E& y) {
+    if (x.a != y.a) return x.a < y.a;
+    if (x.p != y.p) return x.p < y.p;
+    return x.d < y.d;
+  });
+  *n = (int64_t)out.size();
+  for (int64_t k = 0; k < (int64_t)out.size() && k < cap; ++k) {
+    if (offset) offset[k] = out[k].a;
+    if (pre) pre[k] = out[k].p;
+    if (delay) delay[k] = out[k].d;
+  }
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_rng_uniforms_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
+                                int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  const Group& g = net->groups[gid];
+  CHECK(g.kind == KIND_POISSON, B2B_ERR_INVALID_ARG, "group %d is not a Poisson group", gid);
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(host && n == g.n && steps > 0 && steps <= net->last_chunk_steps, B2B_ERR_INVALID_ARG,
+        "bad shape");
+  const Pop& pop = net->pops[g.pop];
+  const size_t rs = real_size(pop.dtype);
+  CU(cudaStreamSynchronize(net->stream));
+  for (int64_t k = 0; k < steps; ++k)
+    CU(cudaMemcpy((uint8_t*)host + rs * n * k,
+                  (const uint8_t*)pop.rng_buf + rs * (k * pop.n + g.offset), rs * n,
+                  cudaMemcpyDeviceToHost));
+  return B2B_OK;
+}
+
+b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(sid >= 0 && sid < (int)net->syns.size() && n, B2B_ERR_INVALID_ARG, "bad synapses %d",
+        sid);
+  CHECK(net->finalized || !net->syns[sid].generated, B2B_ERR_STATE,
+        "generated synapses exist only after b2b_finalize");
+  *n = net->syns[sid].n;
+  return B2B_OK;
+}
+
+b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(sid >= 0 && sid < (int)net->syns.size(), B2B_ERR_INVALID_ARG, "bad synapses %d", sid);
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  const Syn& sy = net->syns[sid];
+  CHECK(host && n == sy.n, B2B_ERR_INVALID_ARG, "expected %lld values", (long long)sy.n);
+  CHECK(var >= B2B_SYN_I && var <= B2B_SYN_LASTUPDATE, B2B_ERR_INVALID_ARG, "bad variable %d",
+        var);
+  const Proj& pr = net->projs[sy.proj];
+  CHECK(var <= B2B_SYN_W || pr.effect == B2B_EFFECT_STDP, B2B_ERR_INVALID_ARG,
+        "variable %d exists only for STDP synapses", var);
+  if (n == 0) return B2B_OK;
+  const Group& gpre = net->groups[sy.pre_gid];
+  const Group& gpost = net->groups[sy.post_gid];
+  const int32_t nd = pr.dmax - pr.dmin + 1;
+  const void* arr = nullptr;
+  if (var == B2B_SYN_W) arr = pr.w;
+  if (var == B2B_SYN_APRE) arr = pr.dev.apre;
+  if (var == B2B_SYN_APOST) arr = pr.dev.apost;
+  if (var == B2B_SYN_LASTUPDATE) arr = pr.dev.lastupdate;
+  const int64_t* inv = sy.inv;  // NULL for generated synapses: positions are the numbering
+  const size_t es = (var <= B2B_SYN_DELAY) ? 4 : real_size(pr.dtype);
+  void* d_out = nullptr;
+  CU(cudaMalloc(&d_out, es * n));
+  cudaError_t e = gather_syn_var(pr, var, inv, sy.base, n,
+                                 (gpre.offset + sy.pre_lo) * (int64_t)nd,
+                                 (gpre.offset + sy.pre_hi) * (int64_t)nd, gpre.offset,
+                                 gpost.offset, arr, sy.w_scalar, d_out, net->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, d_out, es * n, cudaMemcpyDeviceToHost, net->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "syn_get: %s", cudaGetErrorString(e));
+  return B2B_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+// Internal types of libb2b shared by the host runtime (api.cu) and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <curand.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/b2b.h"
+
+namespace b2b {
+
+constexpr int kMaxVars = 8;          // v, ge, gi, m, h, n, lastspike, not_refractory
+constexpr int kPad = 128;            // population and group offsets are padded to this
+constexpr int kBlock = 256;          // threads per CTA for the per-neuron kernels
+constexpr int kChunk = 128;          // synapses one warp takes from a bundle per work item
+constexpr int kNumSMs = 148;         // B200
+
+enum Kind { KIND_LIF = 1, KIND_HH = 2, KIND_POISSON = 3, KIND_SPIKEGEN = 4 };
+
+// Per-group parameters as the kernels read them (doubles; cast to the state type in-kernel).
+struct LifDev {
+  double A, Be, Bi, De, Di, El, Vt, Vr;   // exact propagator coefficients + threshold/reset
+  int64_t ref_steps;                      // timestep(refractory, dt); -1 = no refractoriness
+  int64_t offset, n;                      // group range inside the population
+  int32_t has_threshold, has_reset, unless_refractory, pad;
+};
+struct HhDev {
+  double Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr;
+  int64_t ref_steps;
+  int64_t offset, n;
+};
+struct PoissonDev {
+  double p_spike;                         // rate * dt
+  int64_t offset, n;
+};
+
+// Device view of a population (all groups of one kind and dtype laid out back to back).
+struct PopDev {
+  void* var[kMaxVars];            // SoA state, NOT_REFRACTORY as uint8
+  const void* params;             // LifDev/HhDev/PoissonDev[n_groups]
+  const int32_t* vec_group;       // group id per 4-neuron vector (NULL when one group)
+  int64_t n;                      // padded neuron count (multiple of kPad)
+  int32_t n_groups;
+  int32_t ring_len;               // spike history slots (>= max delay + 2)
+  int32_t* ring_idx;              // [ring_len][n] spike indices per step
+  int32_t* ring_cnt;              // [ring_len] spike counts per step
+  int32_t* mon_idx;               // spike monitor (or NULL)
+  int64_t* mon_step;
+  unsigned long long* mon_cnt;
+  int64_t mon_cap;
+  const void* rng;                // uniform buffer [steps][n] (Poisson)
+  const int32_t* sg_idx;          // spike generator entries sorted by step
+  const int64_t* sg_step;
+  int64_t sg_n;
+  int32_t late_reset;             // reset must run after synaptic delivery
+  int32_t pad;
+};
+
+// Device view of a projection (merged Synapses objects with one source population, one
+// target variable and one effect).
+struct ProjDev {
+  const int32_t* src_ring_idx;
+  const int32_t* src_ring_cnt;
+  int64_t src_n;                  // ring row stride (padded source population size)
+  int32_t src_ring_len;
+  int32_t dmin, nd;               // delays dmin .. dmin+nd-1
+  int32_t chunks;                 // work items per bundle = ceil(max bundle / kChunk)
+  const int64_t* off;             // [n_src*nd + 1] bundle offsets, key = pre*nd + (d-dmin)
+  const int32_t* post;            // [n_syn] target index in the target population
+  const void* w;                  // [n_syn] weights or NULL
+  double w_scalar;
+  void* target;                   // target variable array
+  // STDP
+  void* apre; void* apost; void* lastupdate;
+  double taupre, taupost, dApre, dApost, wmin, wmax;
+  int32_t pre_adds_weight;
+  int32_t aggregate;              // warp-aggregate atomics (few targets)
+  // on_post pathway (transposed index)
+  const int32_t* post_ring_idx;
+  const int32_t* post_ring_cnt;
+  int64_t post_src_n;
+  int32_t post_ring_len;
+  int32_t post_chunks;
+  const int64_t* post_off;        // [n_post + 1]
+  const int32_t* post_syn;        // synapse positions grouped by post
+};
+
+struct Group {
+  int kind = 0, dtype = 0, pop = -1;
+  int64_t n = 0, offset = 0;
+  b2b_lif_params lif{};
+  b2b_hh_params hh{};
+  double rate = 0;
+  std::vector<int32_t> sg_idx;
+  std::vector<int64_t> sg_step;
+  std::vector<std::vector<uint8_t>> staged;   // per var host bytes staged before finalize
+  int64_t mon_cap = 0;
+};
+
+struct Pop {
+  int kind = 0, dtype = 0;
+  int64_t n = 0;
+  std::vector<int> groups;
+  PopDev dev{};
+  void* params_dev = nullptr;
+  int32_t* vec_group_dev = nullptr;
+  std::vector<void*> allocs;
+  int64_t rng_steps = 0;          // rows held by the uniform buffer
+  void* rng_buf = nullptr;
+  bool late_reset = false;
+  int max_delay = 0;
+};
+
+struct Syn {  // one user-level Synapses object
+  int pre_gid = -1, post_gid = -1, target_var = 0, effect = 0;
+  int64_t n = 0;
+  std::vector<int32_t> i, j, delay;          // host input (empty for generated)
+  std::vector<uint8_t> w;                    // host weights (dtype of target) or empty
+  double w_scalar = 0;
+  int32_t delay_scalar = 0;
+  b2b_stdp_params stdp{};
+  bool generated = false;
+  double p = 0; int32_t gdmin = 0, gdmax = 0; uint64_t gseed = 0;
+  int proj = -1;
+  int64_t base = 0;                          // first position inside the projection
+  int32_t dmin = 0, dmax = 0;
+  int64_t* inv = nullptr;                    // input index -> position (host-given synapses)
+  int32_t pre_lo = 0, pre_hi = 0;            // presynaptic subgroup (group-local)
+};
+
+struct Proj {
+  int src_pop = -1, dst_pop = -1, target_var = 0, effect = 0, dtype = 0;
+  std::vector<int> members;                  // Syn ids, sorted by source range
+  int32_t dmin = 0, dmax = 0;
+  int64_t n_syn = 0;
+  int64_t max_bundle = 0, max_post_bundle = 0;
+  ProjDev dev{};
+  int64_t* off = nullptr;
+  int32_t* post = nullptr;
+  void* w = nullptr;
+  std::vector<void*> allocs;
+};
+
+}  // namespace b2b
+
+struct b2b_net {
+  b2b_config cfg{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool finalized = false;
+  int64_t ts = 0;                          // next step to simulate
+  int64_t* d_clock = nullptr;              // device copy of ts at chunk start
+  int32_t* d_status = nullptr;
+  curandGenerator_t gen = nullptr;
+  std::vector<b2b::Group> groups;
+  std::vector<b2b::Pop> pops;
+  std::vector<b2b::Syn> syns;
+  std::vector<b2b::Proj> projs;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int64_t launches = 0;
+  int64_t graph_nodes = 0;
+  int64_t last_chunk_steps = 0;
+  std::string err;
+  std::vector<b2b_hines*> hines;
+};
+
+// Kernel launch entry points (implemented in the .cu files, called by api.cu).
+namespace b2b {
+cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
+                            int32_t* status, cudaStream_t s);
+cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k,
+                                  cudaStream_t s);
+cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,
+                            int32_t* status, cudaStream_t s);
+cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double dt,
+                             int32_t* status, cudaStream_t s);
+cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
+}  // namespace b2b

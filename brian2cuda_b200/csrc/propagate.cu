@@ -1,0 +1,280 @@
+// Spike propagation: delivery of due synapse bundles from the spike-history ring, with the
+// on_pre / on_post effects (additive, and event-driven STDP with its traces) applied in the
+// same pass.
+//
+// Reference: the per-step push of (pre, post-block, delay) bundle ids into CudaSpikeQueue
+// slots `(current_offset + delay) % num_queues` under per-post-block spin locks with
+// device-malloc growth (brian2cuda/brianlib/spikequeue.h:432-511, templates/
+// synapses_push_spikes.cu:1056-1131), then the effect kernel over the current slot
+// (templates/synapses.cu:12-164) with `_brian_atomicAdd` (cuda_generator.py:33-157).
+//
+// Here nothing is pushed.  Each population keeps the compacted spikes of its last
+// `ring_len` steps (written by the neuron kernel).  A bundle (pre, d) is due at step ts
+// exactly when pre spiked at step ts - d, so the delivery kernel enumerates, for every delay
+// d of the projection, the spikes of ring slot ts - d and walks the synapse range of bundle
+// (pre, d) in the (pre, delay)-sorted synapse arrays.  This is the same set of bundles the
+// reference's queue holds in slot `current_offset` after its push, without the push kernel,
+// the host sync on the spike count, the locks or the device heap.
+#include "kernels_common.cuh"
+
+namespace b2b {
+
+namespace {
+
+constexpr int kDeliverBlock = 256;
+
+// Loads the number of due spikes per delay into s_pref[1..nd] and turns it into an
+// inclusive prefix (s_pref[0] = 0).  Returns the number of due (spike, delay) pairs.
+__device__ __forceinline__ int due_prefix(const int32_t* ring_cnt, int ring_len, int64_t ts,
+                                          int dmin, int nd, int* s_pref) {
+  for (int di = threadIdx.x; di < nd; di += blockDim.x) {
+    const int64_t st = ts - (int64_t)(dmin + di);
+    s_pref[di + 1] = st >= 0 ? ring_cnt[ring_slot(st, ring_len)] : 0;
+  }
+  if (threadIdx.x == 0) s_pref[0] = 0;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int carry = 0;
+    for (int base = 1; base <= nd; base += 32) {
+      const int i = base + lane;
+      int x = i <= nd ? s_pref[i] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+      }
+      if (i <= nd) s_pref[i] = x + carry;
+      carry += __shfl_sync(kFull, x, 31);
+    }
+  }
+  __syncthreads();
+  return s_pref[nd];
+}
+
+// Largest di in [0, nd) with s_pref[di] <= sp.
+__device__ __forceinline__ int find_delay(const int* s_pref, int nd, int sp) {
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= sp) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Calls body(s, valid) for every synapse position s of every bundle due at step ts.  All 32
+// lanes of a warp call body together (valid marks real synapses), so bodies may use
+// warp-synchronous intrinsics.
+template <class Body>
+__device__ __forceinline__ void for_each_due(const ProjDev& P, int64_t ts, int* s_pref,
+                                             Body body) {
+  const int nspk = due_prefix(P.src_ring_cnt, P.src_ring_len, ts, P.dmin, P.nd, s_pref);
+  const int64_t items = (int64_t)nspk * P.chunks;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t it = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items;
+       it += warps) {
+    const int sp = (int)(it / P.chunks);
+    const int ch = (int)(it - (int64_t)sp * P.chunks);
+    const int di = find_delay(s_pref, P.nd, sp);
+    const int kk = sp - s_pref[di];
+    const int64_t st = ts - (int64_t)(P.dmin + di);
+    const int32_t pre =
+        P.src_ring_idx[(int64_t)ring_slot(st, P.src_ring_len) * P.src_n + kk];
+    const int64_t key = (int64_t)pre * P.nd + di;
+    const int64_t b0 = P.off[key] + (int64_t)ch * kChunk;
+    int64_t b1 = P.off[key + 1];
+    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
+    for (int64_t base = b0; base < b1; base += 32) {
+      const int64_t s = base + lane;
+      body(s, s < b1);
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void atomic_add(R* addr, R v) {
+  atomicAdd(addr, v);
+}
+
+// Sum of `v` over the lanes whose `key` equals this lane's key; valid in every lane.
+template <typename R>
+__device__ __forceinline__ R peer_sum(unsigned peers, R v) {
+  R acc = 0;
+#pragma unroll 1
+  for (int src = 0; src < 32; ++src) {
+    const R x = __shfl_sync(kFull, v, src);
+    if ((peers >> src) & 1u) acc += x;
+  }
+  return acc;
+}
+
+// ---- on_pre: target[post] += w -------------------------------------------------------------
+template <typename R, bool HAS_W, bool AGG>
+__global__ void __launch_bounds__(kDeliverBlock)
+deliver_add_kernel(ProjDev P, const int64_t* __restrict__ clock, int k) {
+  extern __shared__ int s_pref[];
+  const int64_t ts = clock[0] + k;
+  const R* __restrict__ W = static_cast<const R*>(P.w);
+  const R ws = (R)P.w_scalar;
+  R* __restrict__ T = static_cast<R*>(P.target);
+  const int lane = threadIdx.x & 31;
+  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
+    const int32_t post = valid ? __ldg(P.post + s) : -1;
+    R w = ws;
+    if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
+    if constexpr (AGG) {
+      const unsigned peers = __match_any_sync(kFull, post);
+      const R sum = peer_sum<R>(peers, w);
+      if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
+    } else {
+      if (valid) atomic_add(T + post, w);
+    }
+  });
+}
+
+// ---- on_pre of event-driven additive STDP (examples/stdp.py:125-186) ----------------------
+// Traces decay lazily from lastupdate to t (Brian2's event-driven update); in float32 the
+// elapsed time is rounded to float first, as brian2cuda does (brian2cuda/device.py:1034-1039).
+template <typename R, bool AGG>
+__global__ void __launch_bounds__(kDeliverBlock)
+deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, double dt) {
+  extern __shared__ int s_pref[];
+  const int64_t ts = clock[0] + k;
+  const double t = (double)ts * dt;
+  R* __restrict__ W = static_cast<R*>(const_cast<void*>(P.w));
+  R* __restrict__ Apre = static_cast<R*>(P.apre);
+  R* __restrict__ Apost = static_cast<R*>(P.apost);
+  R* __restrict__ LU = static_cast<R*>(P.lastupdate);
+  R* __restrict__ T = static_cast<R*>(P.target);
+  const R taupre = (R)P.taupre, taupost = (R)P.taupost, dApre = (R)P.dApre;
+  const R wmin = (R)P.wmin, wmax = (R)P.wmax;
+  const int lane = threadIdx.x & 31;
+  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
+    int32_t post = -1;
+    R w = 0;
+    if (valid) {
+      post = __ldg(P.post + s);
+      w = W[s];
+      R apre = Apre[s], apost = Apost[s];
+      const R tau = (R)(t - (double)LU[s]);
+      apre = apre * dexp(-tau / taupre);
+      apost = apost * dexp(-tau / taupost);
+      apre = apre + dApre;
+      W[s] = dclip(w + apost, wmin, wmax);
+      Apre[s] = apre;
+      Apost[s] = apost;
+      LU[s] = (R)t;
+    }
+    if (P.pre_adds_weight) {
+      if constexpr (AGG) {
+        const unsigned peers = __match_any_sync(kFull, post);
+        const R sum = peer_sum<R>(peers, w);
+        if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
+      } else {
+        if (valid) atomic_add(T + post, w);
+      }
+    }
+  });
+}
+
+// ---- on_post of event-driven additive STDP -------------------------------------------------
+// Every synapse of each neuron of the target population that spiked this step, reached
+// through the transposed (post-sorted) index.
+template <typename R>
+__global__ void __launch_bounds__(kDeliverBlock)
+deliver_stdp_post_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, double dt) {
+  const int64_t ts = clock[0] + k;
+  const double t = (double)ts * dt;
+  const int slot = ring_slot(ts, P.post_ring_len);
+  const int nspk = P.post_ring_cnt[slot];
+  const int32_t* spikes = P.post_ring_idx + (int64_t)slot * P.post_src_n;
+  R* __restrict__ W = static_cast<R*>(const_cast<void*>(P.w));
+  R* __restrict__ Apre = static_cast<R*>(P.apre);
+  R* __restrict__ Apost = static_cast<R*>(P.apost);
+  R* __restrict__ LU = static_cast<R*>(P.lastupdate);
+  const R taupre = (R)P.taupre, taupost = (R)P.taupost, dApost = (R)P.dApost;
+  const R wmin = (R)P.wmin, wmax = (R)P.wmax;
+  const int lane = threadIdx.x & 31;
+  const int64_t items = (int64_t)nspk * P.post_chunks;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t it = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items;
+       it += warps) {
+    const int sp = (int)(it / P.post_chunks);
+    const int ch = (int)(it - (int64_t)sp * P.post_chunks);
+    const int32_t j = spikes[sp];
+    const int64_t b0 = P.post_off[j] + (int64_t)ch * kChunk;
+    int64_t b1 = P.post_off[j + 1];
+    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
+    for (int64_t r = b0 + lane; r < b1; r += 32) {
+      const int64_t s = P.post_syn[r];
+      R apre = Apre[s], apost = Apost[s];
+      const R tau = (R)(t - (double)LU[s]);
+      apre = apre * dexp(-tau / taupre);
+      apost = apost * dexp(-tau / taupost);
+      apost = apost + dApost;
+      W[s] = dclip(W[s] + apre, wmin, wmax);
+      Apre[s] = apre;
+      Apost[s] = apost;
+      LU[s] = (R)t;
+    }
+  }
+}
+
+unsigned deliver_grid(const Proj& pr) {
+  const int64_t want = (pr.dev.src_n * (int64_t)pr.dev.chunks) / 64 + 1;
+  const int64_t cap = 2 * kNumSMs;
+  return (unsigned)(want < cap ? want : cap);
+}
+
+}  // namespace
+
+cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,
+                            int32_t* status, cudaStream_t s) {
+  (void)status;
+  const ProjDev& P = pr.dev;
+  const unsigned grid = deliver_grid(pr);
+  const size_t smem = sizeof(int) * (size_t)(P.nd + 1);
+  const bool f32 = pr.dtype == B2B_F32;
+  if (pr.effect == B2B_EFFECT_ADD) {
+    const bool hw = P.w != nullptr;
+    const bool ag = P.aggregate != 0;
+#define B2B_ADD(R, HW, AG) deliver_add_kernel<R, HW, AG><<<grid, kDeliverBlock, smem, s>>>(P, clock, k)
+    if (f32) {
+      if (hw) { if (ag) B2B_ADD(float, true, true); else B2B_ADD(float, true, false); }
+      else { if (ag) B2B_ADD(float, false, true); else B2B_ADD(float, false, false); }
+    } else {
+      if (hw) { if (ag) B2B_ADD(double, true, true); else B2B_ADD(double, true, false); }
+      else { if (ag) B2B_ADD(double, false, true); else B2B_ADD(double, false, false); }
+    }
+#undef B2B_ADD
+  } else if (pr.effect == B2B_EFFECT_STDP) {
+    const bool ag = P.aggregate != 0;
+    if (f32) {
+      if (ag) deliver_stdp_pre_kernel<float, true><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+      else deliver_stdp_pre_kernel<float, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+    } else {
+      if (ag) deliver_stdp_pre_kernel<double, true><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+      else deliver_stdp_pre_kernel<double, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+    }
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double dt,
+                             int32_t* status, cudaStream_t s) {
+  (void)status;
+  if (pr.effect != B2B_EFFECT_STDP) return cudaSuccess;
+  const ProjDev& P = pr.dev;
+  int64_t want = (P.post_src_n * (int64_t)P.post_chunks) / 8 + 1;
+  const unsigned grid = (unsigned)(want < 2 * kNumSMs ? want : 2 * kNumSMs);
+  if (pr.dtype == B2B_F32)
+    deliver_stdp_post_kernel<float><<<grid, kDeliverBlock, 0, s>>>(P, clock, k, dt);
+  else
+    deliver_stdp_post_kernel<double><<<grid, kDeliverBlock, 0, s>>>(P, clock, k, dt);
+  return cudaGetLastError();
+}
+
+}  // namespace b2b

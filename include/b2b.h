@@ -1,0 +1,277 @@
+/*
+ * b2b.h — C ABI of libb2b, the B200 (sm_100a) simulation backend that replaces the
+ * per-code-object CUDA kernels which brian2cuda generates for a Brian2 network.
+ *
+ * brian2cuda renders one kernel plus one host launcher `_run_<codeobject>()` per Brian2
+ * code object and calls them from `Network::run` (brian2cuda/templates/network.cu:40-137).
+ * libb2b replaces that generated hot path with a handful of fused, hand-written kernels
+ * that own the state of the whole network.  The generated host code (or ctypes) builds a
+ * network once through this header and then advances it with b2b_run().
+ *
+ * Conventions
+ *   - Every entry point returns b2b_status.  Nothing calls exit(); the message of the last
+ *     failure is kept per network (b2b_last_error).  The reference prints and exits
+ *     instead (brian2cuda/brianlib/cuda_utils.h:77-132).
+ *   - Plain C types only: pointers, sizes, int32/int64/double.  Arrays passed in are host
+ *     pointers unless the name says `dev`.
+ *   - One b2b_net per host thread; nets are independent of each other.
+ *   - All device work of a net runs on one CUDA stream (the caller's, or one the net owns).
+ *     b2b_run() is asynchronous; b2b_sync() waits and reports device-side status.
+ *   - Time: t = timestep * dt, timestep an int64 (brian2cuda/brianlib/clocks.h:33-37).
+ *     Delays are integer numbers of steps; Brian2 rounds a delay in seconds to steps as
+ *     (int)(delay/dt + 0.5) (brian2cuda/templates/synapses_push_spikes.cu:375).
+ */
+#ifndef B2B_H
+#define B2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2B_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+typedef int32_t b2b_status;
+enum {
+  B2B_OK = 0,
+  B2B_ERR_INVALID_ARG = 1,    /* bad argument (NULL, size, unknown enum, index range)  */
+  B2B_ERR_OOM = 2,            /* device or host allocation failed                      */
+  B2B_ERR_QUEUE_OVERFLOW = 3, /* a fixed-capacity device buffer (monitor) overflowed   */
+  B2B_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up                    */
+  B2B_ERR_CUDA = 5,           /* a CUDA runtime / cuRAND call failed                   */
+  B2B_ERR_STATE = 6,          /* call not valid now (e.g. adding groups after finalize)*/
+  B2B_ERR_UNSUPPORTED = 7,    /* combination not implemented                           */
+  B2B_ERR_INDEX = 8           /* out-of-range index found in input or by a checked kernel */
+};
+
+typedef struct b2b_net b2b_net;
+
+/* Numeric type of a group's state (Brian2's core.default_float_dtype). */
+enum { B2B_F32 = 1, B2B_F64 = 2 };
+
+/* Network flags (b2b_config.flags). */
+enum {
+  B2B_NET_NO_GRAPH = 1,   /* launch every step eagerly instead of replaying CUDA graphs */
+  B2B_NET_CHECKED = 2,    /* kernels check indices and record B2B_ERR_INDEX            */
+  B2B_NET_RESET_BEFORE_SYNAPSES = 4  /* schedule start, groups, thresholds, resets, synapses,
+                                        end (Brian2 prefs core.network.default_schedule);
+                                        default: resets after synapses                   */
+};
+
+typedef struct {
+  double dt;                /* time step in seconds                                      */
+  int32_t device;           /* CUDA device ordinal                                       */
+  int32_t steps_per_graph;  /* steps captured per CUDA graph; 0 selects 50               */
+  uint64_t seed;            /* seed of the cuRAND Philox generator and of b2b_connect    */
+  void* stream;             /* cudaStream_t to run on, or NULL: the net creates its own  */
+  int32_t flags;            /* B2B_NET_* bits                                            */
+  int32_t reserved;
+} b2b_config;
+
+/* Replaces the generated `brian_start()` / `_init_arrays()` pair
+ * (brian2cuda/templates/run.cu:15-32, objects.cu:340-489). */
+b2b_status b2b_create(const b2b_config* cfg, b2b_net** out);
+/* Replaces `brian_end()` / `_dealloc_arrays()` (run.cu:34-38, objects.cu:654-726). */
+b2b_status b2b_destroy(b2b_net* net);
+/* Copies the message of the net's last failure into buf (always NUL-terminated). */
+b2b_status b2b_last_error(const b2b_net* net, char* buf, size_t len);
+const char* b2b_status_string(b2b_status s);
+int32_t b2b_abi_version(void);
+
+/* ---- neuron groups ---------------------------------------------------------------- */
+/* Linear leaky integrate-and-fire, integrated with the exact (closed-form) propagator
+ * Brian2's `method='exact'` emits for
+ *     dv/dt  = (El - v + ke*ge + ki*gi)/taum   [(unless refractory)]
+ *     dge/dt = -ge/taue,  dgi/dt = -gi/taui
+ * CUBA (examples/cuba.py:125-132): ke = ki = 1.  The STDP benchmark neuron
+ * (brian2cuda/tests/features/speed.py:629-640): ke = Ee - vr, ki = 0.
+ * taum = +inf gives a non-leaky `v : 1` group.  Threshold `v > Vt` (and not_refractory
+ * when refractory > 0), reset `v = Vr` (brian2cuda/templates/threshold.cu:19-45,
+ * reset.cu:3-27).  Replaces the stateupdater/thresholder/resetter code objects. */
+typedef struct {
+  double El, taum, taue, taui, ke, ki;   /* volts, seconds, dimensionless factors */
+  double Vt, Vr, refractory;             /* refractory in seconds; 0 = none         */
+  int32_t has_threshold, has_reset, unless_refractory, reserved;
+} b2b_lif_params;
+
+/* Conductance-based Hodgkin-Huxley (examples/cobahh.py:159-180), integrated with the
+ * exponential-Euler scheme of Brian2's `method='exponential_euler'`.  Threshold
+ * `v > Vthr` and not_refractory; no reset.  All SI units. */
+typedef struct {
+  double Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, taue, taui, Vthr, refractory;
+} b2b_hh_params;
+
+b2b_status b2b_group_lif(b2b_net* net, int64_t n, int32_t dtype, const b2b_lif_params* p,
+                         int32_t* gid);
+b2b_status b2b_group_hh(b2b_net* net, int64_t n, int32_t dtype, const b2b_hh_params* p,
+                        int32_t* gid);
+/* PoissonGroup: neuron i spikes in a step when u_i < rate*dt, u_i one uniform from the
+ * net's cuRAND buffer (brian2cuda/templates/rand.cu:340-463 fills the same kind of
+ * per-step bulk buffer; `_rand` reads it in place, cuda_generator.py:938-943). */
+b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate_hz,
+                             int32_t* gid);
+/* SpikeGeneratorGroup: neuron idx[k] spikes at step[k]
+ * (brian2cuda/templates/spikegenerator.cu:41-148). */
+b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const int32_t* idx,
+                              const int64_t* step, int32_t* gid);
+
+/* State variables of a group.  Values are in the group's dtype; NOT_REFRACTORY is uint8. */
+enum {
+  B2B_VAR_V = 0, B2B_VAR_GE = 1, B2B_VAR_GI = 2, B2B_VAR_M = 3, B2B_VAR_H = 4, B2B_VAR_N = 5,
+  B2B_VAR_LASTSPIKE = 6, B2B_VAR_NOT_REFRACTORY = 7
+};
+/* Host <-> device copies of one variable (replaces the generated H2D/D2H copies of
+ * `_array_<group>_<var>`, brian2cuda/device.py:558-658, objects.cu:522-641).
+ * Before b2b_finalize the values are staged on the host. */
+b2b_status b2b_state_set(b2b_net* net, int32_t gid, int32_t var, const void* host, int64_t n);
+b2b_status b2b_state_get(b2b_net* net, int32_t gid, int32_t var, void* host, int64_t n);
+/* Device pointer to a group's variable (after b2b_finalize); the net owns the memory. */
+b2b_status b2b_state_ptr(b2b_net* net, int32_t gid, int32_t var, void** dev, int64_t* n);
+
+/* ---- synapses ---------------------------------------------------------------------- */
+/* Effect of a presynaptic spike (the on_pre code of a Synapses object). */
+enum {
+  B2B_EFFECT_ADD = 1,   /* target_var[post] += w                                         */
+  B2B_EFFECT_STDP = 2   /* event-driven additive STDP with on_pre and on_post pathways   */
+};
+
+/* examples/stdp.py:125-186, brian2cuda/tests/features/speed.py:627-663:
+ *   on_pre : Apre, Apost decayed to t; target += w (if pre_adds_weight);
+ *            Apre += dApre; w = clip(w + Apost, wmin, wmax); lastupdate = t
+ *   on_post: Apre, Apost decayed to t; Apost += dApost; w = clip(w + Apre, wmin, wmax);
+ *            lastupdate = t                                                          */
+typedef struct {
+  double taupre, taupost, dApre, dApost, wmin, wmax;
+  int32_t pre_adds_weight, reserved;
+} b2b_stdp_params;
+
+/* Adds a Synapses object with explicit connectivity (i -> j, group-local indices).
+ * w: per-synapse weights in the target group's dtype, or NULL to use w_scalar.
+ * delay_steps: per-synapse delays in steps, or NULL to use delay_scalar.
+ * stdp: required for B2B_EFFECT_STDP (w then is the initial weight), else NULL.
+ * Replaces connectivity preprocessing `_before_run_<pathway>_push_spikes`
+ * (brian2cuda/templates/synapses_push_spikes.cu:171-993). */
+b2b_status b2b_synapses(b2b_net* net, int32_t pre_gid, int32_t post_gid, int32_t target_var,
+                        int32_t effect, int64_t n_syn, const int32_t* i, const int32_t* j,
+                        const void* w, double w_scalar, const int32_t* delay_steps,
+                        int32_t delay_scalar, const b2b_stdp_params* stdp, int32_t* sid);
+
+/* Adds a Synapses object whose connectivity is generated on the GPU: every pair (i, j),
+ * i in the presynaptic subgroup [pre_lo, pre_hi) of pre_gid (Brian2's `P[lo:hi]`), j in
+ * post_gid, is connected with probability p (Brian2 `connect(p=...)`); each synapse gets a
+ * delay drawn uniformly from the integers [dmin, dmax] and weight w.  Generation is
+ * counter-based (Philox-4x32-10 keyed by seed and the group-local (i, j)), so it is
+ * reproducible and independent of launch shape.  Replaces host-serial synapse creation
+ * (brian2cuda/templates/synapses_create_generator.cu:164-271).  Synapses are numbered in
+ * (i, delay, j) order; i and j are group-local. */
+b2b_status b2b_synapses_random(b2b_net* net, int32_t pre_gid, int32_t pre_lo, int32_t pre_hi,
+                               int32_t post_gid, int32_t target_var, double p, int32_t dmin,
+                               int32_t dmax, double w, uint64_t seed, int32_t* sid);
+
+/* Synapse variables. I, J, DELAY are int32; the others use the target group's dtype. */
+enum {
+  B2B_SYN_I = 0, B2B_SYN_J = 1, B2B_SYN_DELAY = 2, B2B_SYN_W = 3, B2B_SYN_APRE = 4,
+  B2B_SYN_APOST = 5, B2B_SYN_LASTUPDATE = 6
+};
+b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n);
+/* Reads a synapse variable in the order the synapses were given (after b2b_finalize). */
+b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64_t n);
+
+/* ---- lifecycle ---------------------------------------------------------------------- */
+/* Lays out state, builds the delay-sorted connectivity on the GPU and captures the step
+ * graphs (the role of the generated before_run code). */
+b2b_status b2b_finalize(b2b_net* net);
+/* Advances the network by n_steps time steps; asynchronous (replaces the per-step loop
+ * of Network::run, brian2cuda/templates/network.cu:40-137, with no host sync per step). */
+b2b_status b2b_run(b2b_net* net, int64_t n_steps);
+/* Waits for the net's stream; *device_status receives the device status word
+ * (B2B_OK, B2B_ERR_QUEUE_OVERFLOW, B2B_ERR_INDEX, ...). */
+b2b_status b2b_sync(b2b_net* net, int32_t* device_status);
+/* Current time step (the next step to simulate) and time in seconds. */
+b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
+/* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
+b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
+/* Profiling run (the role of run(..., profile=True): per-code-object device timing,
+ * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
+ * network by n_steps with eager launches, timing every launch with a CUDA event pair on the
+ * net's stream, and returns per launch site the mean device time of one launch in ms.
+ * Sites, in order: one per population (kind 1), one per projection's on_pre delivery
+ * (kind 2), one per STDP projection's on_post delivery (kind 3), one per population with a
+ * deferred reset (kind 4).  *n_sites receives the number of sites (<= cap filled). */
+b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
+                       int32_t cap, int32_t* n_sites);
+
+/* ---- monitors and inspection ---------------------------------------------------------- */
+/* Records every spike of group gid as (step, index) into a device buffer of `capacity`
+ * entries (replaces brian2cuda/templates/spikemonitor.cu without per-step resizes).
+ * Must be called before b2b_finalize. */
+b2b_status b2b_spikemon(b2b_net* net, int32_t gid, int64_t capacity);
+/* Copies recorded spikes sorted by (step, index); *n receives the total recorded. */
+b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
+                            int64_t* step, int64_t cap);
+/* Incremental readout: *total receives the number of entries the monitor of gid's
+ * population has recorded; entries [start, min(total, start + cap)) are copied in recording
+ * order, keeping those of group gid (group-local index), and *n receives how many were kept.
+ * Lets a caller drain new spikes after every run chunk (the role of the per-run result
+ * files, brian2cuda/templates/objects.cu:522-641). */
+b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total,
+                              int64_t* n, int32_t* idx, int64_t* step, int64_t cap);
+/* Spikes of group gid in the last completed step, sorted ascending (the canonical form of
+ * the spikespace, brian2cuda/templates/objects.cu:458-479). */
+b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, int64_t cap);
+/* Delay-queue contents of Synapses object sid: every (pre, delay) bundle still due after
+ * the last completed step, with the step offset (1..max_delay) at which it is due, sorted
+ * by (offset, pre, delay).  Matches the content of the CudaSpikeQueue slots
+ * (brian2cuda/brianlib/spikequeue.h:432-516) with one post block. */
+b2b_status b2b_queue_get(b2b_net* net, int32_t sid, int64_t* n, int32_t* offset,
+                         int32_t* pre, int32_t* delay, int64_t cap);
+/* Uniform numbers the last b2b_run chunk consumed for Poisson group gid: `steps` rows of
+ * n values each (row k = step k of the chunk). */
+b2b_status b2b_rng_uniforms_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
+                                int64_t n);
+
+/* ---- multicompartment (SpatialNeuron) batch ------------------------------------------------ */
+/* A batch of independent multicompartment HH neurons, each a tree of sections (branches) of
+ * cylindrical compartments.  One b2b_hines_step advances all neurons by one dt with the
+ * Hines scheme brian2cuda runs in five kernels (brian2cuda/templates/spatialstateupdate.cu:
+ * 18-93 host matrix preparation, 108-113 channels, 128-192 per-section Thomas solves with
+ * three right-hand sides, 202-307 coupling solve, 316-351 combine, 359-387 currents).
+ *
+ * Layout per neuron b: compartments [comp_off[b], comp_off[b+1]) of the flat arrays;
+ * sections [sec_off[b], sec_off[b+1]); section s covers neuron-local compartments
+ * [sec_start[s], sec_end[s]) and hangs off section sec_parent[s] (-1 for the root section,
+ * which must be the first one of its neuron and start at compartment 0).
+ * Geometry: diameter and length (m) per compartment.  Ri in ohm*m, Cm in F/m^2. */
+typedef struct {
+  double Cm, Ri, El, EK, ENa, gl, gNa, gK;   /* F/m^2, ohm*m, V, S/m^2 */
+  double Vthr;                                /* soma spike threshold (V), upward crossing */
+  int32_t channel_dtype;                      /* B2B_F32 or B2B_F64 gating variables;
+                                                 the cable solve is always float64      */
+  int32_t reserved;
+} b2b_hines_params;
+
+typedef struct b2b_hines b2b_hines;
+b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp_off,
+                            const int32_t* sec_off, const int32_t* sec_start,
+                            const int32_t* sec_end, const int32_t* sec_parent,
+                            const double* diameter, const double* length,
+                            const b2b_hines_params* p, b2b_hines** out);
+/* Per-neuron current injected into compartment 0 (A); NULL clears it. */
+b2b_status b2b_hines_set_current(b2b_hines* h, const double* soma_current);
+/* vars: 0 = v (f64), 1 = m, 2 = h, 3 = n (channel_dtype), 4 = Ic (f64, capacitive current
+ * density of the last step, A/m^2).  Channels follow the Hodgkin-Huxley 1952 rate functions
+ * of examples/compartmental/hh_with_spikes_cuda.py:31-50 (v measured from rest). */
+b2b_status b2b_hines_state_set(b2b_hines* h, int32_t var, const void* host, int64_t n);
+b2b_status b2b_hines_state_get(b2b_hines* h, int32_t var, void* host, int64_t n);
+/* Advances all neurons by n_steps; soma spike counts accumulate per neuron. */
+b2b_status b2b_hines_run(b2b_hines* h, int64_t n_steps);
+b2b_status b2b_hines_spike_counts(b2b_hines* h, int32_t* host, int32_t n);
+b2b_status b2b_hines_destroy(b2b_hines* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B2B_H */

@@ -1,0 +1,921 @@
+// CPU oracle for the brian2cuda hot path — TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, as plain sequential C++ (OpenMP only on independent per-neuron
+// loops), the algorithm brian2cuda generates for the hot path.  It is the checker the
+// GPU library is compared against; it is never linked into or called by the product.
+// Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline arm) load it.
+//
+// It follows the reference's structure, not the GPU design:
+//   * Brian2's schedule per step: all state updates, all thresholds, every synaptic
+//     pathway (on_pre pathways, then on_post pathways; each one advance + push + deliver),
+//     all resets, then the clock tick (templates/network.cu:65-115, clocks.h:33-37).
+//   * Spike queues: `CudaSpikeQueue` with one post block (brianlib/spikequeue.h):
+//     advance() clears slot current_offset and moves to the next slot (504-511);
+//     push_bundles() appends each bundle id of a spiking neuron to slot
+//     (current_offset + delay) % num_queues (432-502); the effect code then walks the
+//     bundles of slot current_offset (peek, 513-516; templates/synapses.cu:117-162).
+//     num_queues = max_delay + 1 (templates/synapses_push_spikes.cu:392-393); bundles are
+//     the synapses of one presynaptic neuron with one delay, in synapse order
+//     (synapses_push_spikes.cu:460-544).
+//   * Spikespace: thresholder appends spiking indices (templates/threshold.cu:19-45); here
+//     in ascending order, the canonical form.
+//   * Refractoriness: not_refractory = timestep(t - lastspike) >= timestep(refractory)
+//     with timestep(t, dt) = (int64)((t + 1e-3 dt)/dt) (cuda_generator.py:997-1006);
+//     threshold `cond and not_refractory`; on a spike not_refractory = false and
+//     lastspike = t (threshold.cu:37-42).  lastspike starts at -1e4 s.
+//   * Integrators: the exact propagator of the linear LIF (examples/cuba.py:125-132) and
+//     Brian2's exponential Euler for COBAHH (examples/cobahh.py:159-180).
+//   * Event-driven STDP (examples/stdp.py:125-186) with float32 elapsed time in float32
+//     mode (brian2cuda/device.py:1034-1039); clip as cuda_generator.py:902-914.
+//   * Hines solver: brian2cuda/templates/spatialstateupdate.cu:36-77 (matrix), 128-192
+//     (Thomas), 202-307 (coupling), 316-351 (combine), 359-387 (currents), literally.
+//   * Philox-4x32-10 connectivity generation restated from Salmon et al., SC 2011.
+//
+// Arithmetic: R = double (reference mode) or float (same-precision mode).
+#include <stdint.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+enum { LIF = 1, HH = 2, POISSON = 3, SPIKEGEN = 4 };
+enum { V = 0, GE = 1, GI = 2, M = 3, H = 4, N = 5, LASTSPIKE = 6, NOT_REF = 7 };
+enum { ADD = 1, STDP = 2 };
+enum { SYN_I = 0, SYN_J = 1, SYN_DELAY = 2, SYN_W = 3, SYN_APRE = 4, SYN_APOST = 5, SYN_LU = 6 };
+
+int64_t timestep(double t, double dt) { return (int64_t)((t + 1e-3 * dt) / dt); }
+
+inline float xexp(float x) { return std::exp(x); }
+inline double xexp(double x) { return std::exp(x); }
+inline float xfma(float a, float b, float c) { return std::fma(a, b, c); }
+inline double xfma(double a, double b, double c) { return std::fma(a, b, c); }
+
+template <typename R>
+R clip(R v, R lo, R hi) {
+  if (v < lo) return lo;
+  if (v > hi) return hi;
+  return v;
+}
+
+// ---- Philox-4x32-10 ----------------------------------------------------------------------
+struct Ctr { uint32_t v[4]; };
+Ctr philox(Ctr c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.v[0];
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.v[2];
+    Ctr n;
+    n.v[0] = (uint32_t)(p1 >> 32) ^ c.v[1] ^ k0;
+    n.v[1] = (uint32_t)p1;
+    n.v[2] = (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1;
+    n.v[3] = (uint32_t)p0;
+    c = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// ---- groups --------------------------------------------------------------------------------
+template <typename R>
+struct Group {
+  int kind = 0;
+  int64_t n = 0;
+  // LIF: El taum taue taui ke ki Vt Vr refractory has_threshold has_reset unless_refractory
+  // HH : Cm gl El EK ENa gNa gK VT Ee Ei taue taui Vthr refractory
+  std::vector<double> p;
+  double rate = 0;
+  std::vector<R> var[7];
+  std::vector<uint8_t> not_ref;
+  std::vector<int32_t> spikes;  // spikespace of the current step, ascending
+  std::vector<std::pair<int64_t, int32_t>> sg;  // spike generator (step, idx), sorted
+  std::vector<std::vector<R>> uniforms;         // Poisson: queued rows, one per step
+  size_t uni_next = 0;
+  std::vector<std::pair<int64_t, int32_t>> recorded;  // (step, idx)
+  double refractory() const {
+    if (kind == LIF) return p[8];
+    if (kind == HH) return p[13];
+    return 0;
+  }
+};
+
+// ---- pathways ------------------------------------------------------------------------------
+template <typename R>
+struct Syn {
+  int pre = -1, post = -1, target = 0, effect = 0;
+  int64_t n = 0;
+  std::vector<int32_t> i, j, delay;
+  std::vector<R> w, apre, apost, lu;
+  R w_scalar = 0;
+  bool has_w = false;
+  double stdp[7] = {0};  // taupre taupost dApre dApost wmin wmax pre_adds_weight
+  // bundles: (pre, delay) -> synapse ids in synapse order
+  int max_delay = 0;
+  std::vector<int64_t> bundle_off;       // [n_pre * (max_delay+1) + 1]
+  std::vector<int64_t> bundle_syn;
+  // queue
+  int num_queues = 1;
+  int current_offset = 0;
+  std::vector<std::vector<int64_t>> queue;  // slot -> bundle ids (key = pre*(D+1)+delay)
+  // on_post (delay 0): synapses by post
+  std::vector<int64_t> post_off, post_syn;
+};
+
+template <typename R>
+struct Net {
+  double dt;
+  int64_t ts = 0;
+  std::vector<Group<R>> groups;
+  std::vector<Syn<R>> syns;
+  bool built = false;
+  bool reset_first = false;   // schedule: thresholds, resets, synapses
+  std::string err;
+};
+
+template <typename R>
+void build_syn(Net<R>& net, Syn<R>& s) {
+  const int64_t npre = net.groups[s.pre].n;
+  const int D = s.max_delay + 1;
+  s.bundle_off.assign(npre * D + 1, 0);
+  for (int64_t k = 0; k < s.n; ++k) s.bundle_off[(int64_t)s.i[k] * D + s.delay[k] + 1]++;
+  for (size_t q = 1; q < s.bundle_off.size(); ++q) s.bundle_off[q] += s.bundle_off[q - 1];
+  s.bundle_syn.assign(s.n, 0);
+  std::vector<int64_t> fill(s.bundle_off.begin(), s.bundle_off.end() - 1);
+  for (int64_t k = 0; k < s.n; ++k) s.bundle_syn[fill[(int64_t)s.i[k] * D + s.delay[k]]++] = k;
+  s.num_queues = D;
+  s.current_offset = 0;
+  s.queue.assign(D, {});
+  if (s.effect == STDP) {
+    const int64_t npost = net.groups[s.post].n;
+    s.post_off.assign(npost + 1, 0);
+    for (int64_t k = 0; k < s.n; ++k) s.post_off[s.j[k] + 1]++;
+    for (int64_t q = 1; q <= npost; ++q) s.post_off[q] += s.post_off[q - 1];
+    s.post_syn.assign(s.n, 0);
+    std::vector<int64_t> f(s.post_off.begin(), s.post_off.end() - 1);
+    for (int64_t k = 0; k < s.n; ++k) s.post_syn[f[s.j[k]]++] = k;
+    s.apre.assign(s.n, 0);
+    s.apost.assign(s.n, 0);
+    s.lu.assign(s.n, 0);
+  }
+}
+
+// ---- one step -------------------------------------------------------------------------------
+template <typename R>
+void update_lif(Group<R>& g, double t, double dt) {
+  const double El = g.p[0], taum = g.p[1], taue = g.p[2], taui = g.p[3], ke = g.p[4], ki = g.p[5];
+  const bool leak = std::isfinite(taum) && taum > 0;
+  const double A = leak ? std::exp(-dt / taum) : 1.0;
+  const double De = taue > 0 ? std::exp(-dt / taue) : 0.0;
+  const double Di = taui > 0 ? std::exp(-dt / taui) : 0.0;
+  auto coupling = [&](double k, double tau, double D) {
+    if (k == 0.0 || !leak) return 0.0;
+    if (tau == taum) return k * (dt / taum) * A;
+    return k * tau / (tau - taum) * (D - A);
+  };
+  const double Be = coupling(ke, taue, De), Bi = coupling(ki, taui, Di);
+  const R rA = (R)A, rBe = (R)Be, rBi = (R)Bi, rDe = (R)De, rDi = (R)Di, rEl = (R)El;
+  const double refr = g.p[8];
+  const int64_t ref_steps = refr > 0 ? timestep(refr, dt) : -1;
+  const bool unless = g.p[11] != 0;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < g.n; ++i) {
+    bool nr = true;
+    if (ref_steps >= 0) nr = timestep(t - (double)g.var[LASTSPIKE][i], dt) >= ref_steps;
+    const R v = g.var[V][i], ge = g.var[GE][i], gi = g.var[GI][i];
+    R vn = xfma(rBi, gi, xfma(rBe, ge, xfma(rA, (R)(v - rEl), rEl)));
+    if (unless && !nr) vn = v;
+    g.var[V][i] = vn;
+    g.var[GE][i] = rDe * ge;
+    g.var[GI][i] = rDi * gi;
+    g.not_ref[i] = nr ? 1 : 0;
+  }
+}
+
+template <typename R>
+R expeuler(R x, R A, R B, R dt) {
+  const R BA = B / A;
+  return -BA + (BA + x) * xexp(A * dt);
+}
+
+template <typename R>
+void update_hh(Group<R>& g, double t, double dt) {
+  const R Cm = (R)g.p[0], gl = (R)g.p[1], El = (R)g.p[2], EK = (R)g.p[3], ENa = (R)g.p[4];
+  const R gNa = (R)g.p[5], gK = (R)g.p[6], VT = (R)g.p[7], Ee = (R)g.p[8], Ei = (R)g.p[9];
+  const R De = (R)std::exp(-dt / g.p[10]), Di = (R)std::exp(-dt / g.p[11]);
+  const R dtR = (R)dt;
+  const double refr = g.p[13];
+  const int64_t ref_steps = refr > 0 ? timestep(refr, dt) : -1;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < g.n; ++i) {
+    bool nr = true;
+    if (ref_steps >= 0) nr = timestep(t - (double)g.var[LASTSPIKE][i], dt) >= ref_steps;
+    const R v = g.var[V][i], m = g.var[M][i], h = g.var[H][i], n = g.var[N][i];
+    const R ge = g.var[GE][i], gi = g.var[GI][i];
+    // examples/cobahh.py:169-180 in SI units
+    const R xm = (R)13e-3 - v + VT;
+    const R am = (R)0.32e6 * xm / (xexp(xm / (R)4e-3) - (R)1);
+    const R ym = v - VT - (R)40e-3;
+    const R bm = (R)0.28e6 * ym / (xexp(ym / (R)5e-3) - (R)1);
+    const R ah = (R)128 * xexp(((R)17e-3 - v + VT) / (R)18e-3);
+    const R bh = (R)4000 / ((R)1 + xexp(((R)40e-3 - v + VT) / (R)5e-3));
+    const R xn = (R)15e-3 - v + VT;
+    const R an = (R)0.032e6 * xn / (xexp(xn / (R)5e-3) - (R)1);
+    const R bn = (R)500 * xexp(((R)10e-3 - v + VT) / (R)40e-3);
+    const R gna = gNa * (m * m * m) * h;
+    const R gk = gK * (n * n * n * n);
+    const R Av = -(gl + ge + gi + gna + gk) / Cm;
+    const R Bv = (gl * El + ge * Ee + gi * Ei + gna * ENa + gk * EK) / Cm;
+    g.var[V][i] = expeuler(v, Av, Bv, dtR);
+    g.var[M][i] = expeuler(m, -(am + bm), am, dtR);
+    g.var[H][i] = expeuler(h, -(ah + bh), ah, dtR);
+    g.var[N][i] = expeuler(n, -(an + bn), an, dtR);
+    g.var[GE][i] = De * ge;
+    g.var[GI][i] = Di * gi;
+    g.not_ref[i] = nr ? 1 : 0;
+  }
+}
+
+template <typename R>
+bool threshold(Net<R>& net, Group<R>& g, double t) {
+  g.spikes.clear();
+  if (g.kind == LIF || g.kind == HH) {
+    const bool has_thr = g.kind == HH || g.p[9] != 0;
+    if (!has_thr) return true;
+    const R thr = (R)(g.kind == LIF ? g.p[6] : g.p[12]);
+    const bool refr = g.refractory() > 0;
+    for (int64_t i = 0; i < g.n; ++i) {
+      const bool cond = g.var[V][i] > thr && (!refr || g.not_ref[i]);
+      if (cond) {
+        g.spikes.push_back((int32_t)i);
+        if (refr) {
+          g.not_ref[i] = 0;
+          g.var[LASTSPIKE][i] = (R)t;
+        }
+      }
+    }
+  } else if (g.kind == POISSON) {
+    if (g.uni_next >= g.uniforms.size()) {
+      net.err = "Poisson group ran out of uniforms";
+      return false;
+    }
+    const std::vector<R>& u = g.uniforms[g.uni_next++];
+    const R thr = (R)(g.rate * net.dt);
+    for (int64_t i = 0; i < g.n; ++i)
+      if (u[i] < thr) g.spikes.push_back((int32_t)i);
+  } else if (g.kind == SPIKEGEN) {
+    auto lo = std::lower_bound(g.sg.begin(), g.sg.end(), std::make_pair(net.ts, (int32_t)-1));
+    for (auto it = lo; it != g.sg.end() && it->first == net.ts; ++it) g.spikes.push_back(it->second);
+  }
+  for (int32_t i : g.spikes) g.recorded.emplace_back(net.ts, i);
+  return true;
+}
+
+template <typename R>
+void pathway_pre(Net<R>& net, Syn<R>& s, double t) {
+  // advance
+  s.queue[s.current_offset].clear();
+  s.current_offset = (s.current_offset + 1) % s.num_queues;
+  // push
+  const int D = s.max_delay + 1;
+  for (int32_t pre : net.groups[s.pre].spikes) {
+    for (int d = 0; d < D; ++d) {
+      const int64_t key = (int64_t)pre * D + d;
+      if (s.bundle_off[key + 1] > s.bundle_off[key])
+        s.queue[(s.current_offset + d) % s.num_queues].push_back(key);
+    }
+  }
+  // deliver
+  Group<R>& tgt = net.groups[s.post];
+  std::vector<R>& T = tgt.var[s.target];
+  const R taupre = (R)s.stdp[0], taupost = (R)s.stdp[1], dApre = (R)s.stdp[2];
+  const R wmin = (R)s.stdp[4], wmax = (R)s.stdp[5];
+  const bool adds = s.stdp[6] != 0;
+  for (int64_t key : s.queue[s.current_offset]) {
+    for (int64_t q = s.bundle_off[key]; q < s.bundle_off[key + 1]; ++q) {
+      const int64_t k = s.bundle_syn[q];
+      if (s.effect == ADD) {
+        T[s.j[k]] += s.has_w ? s.w[k] : s.w_scalar;
+      } else {
+        const R tau = (R)(t - (double)s.lu[k]);
+        R apre = s.apre[k] * xexp(-tau / taupre);
+        R apost = s.apost[k] * xexp(-tau / taupost);
+        const R w = s.w[k];
+        if (adds) T[s.j[k]] += w;
+        apre = apre + dApre;
+        s.w[k] = clip(w + apost, wmin, wmax);
+        s.apre[k] = apre;
+        s.apost[k] = apost;
+        s.lu[k] = (R)t;
+      }
+    }
+  }
+}
+
+template <typename R>
+void pathway_post(Net<R>& net, Syn<R>& s, double t) {
+  const R taupre = (R)s.stdp[0], taupost = (R)s.stdp[1], dApost = (R)s.stdp[3];
+  const R wmin = (R)s.stdp[4], wmax = (R)s.stdp[5];
+  for (int32_t j : net.groups[s.post].spikes) {
+    for (int64_t q = s.post_off[j]; q < s.post_off[j + 1]; ++q) {
+      const int64_t k = s.post_syn[q];
+      const R tau = (R)(t - (double)s.lu[k]);
+      R apre = s.apre[k] * xexp(-tau / taupre);
+      R apost = s.apost[k] * xexp(-tau / taupost);
+      apost = apost + dApost;
+      s.w[k] = clip(s.w[k] + apre, wmin, wmax);
+      s.apre[k] = apre;
+      s.apost[k] = apost;
+      s.lu[k] = (R)t;
+    }
+  }
+}
+
+template <typename R>
+bool step(Net<R>& net) {
+  const double t = (double)net.ts * net.dt;
+  for (Group<R>& g : net.groups) {
+    if (g.kind == LIF) update_lif(g, t, net.dt);
+    else if (g.kind == HH) update_hh(g, t, net.dt);
+  }
+  for (Group<R>& g : net.groups)
+    if (!threshold(net, g, t)) return false;
+  auto resets = [&]() {
+    for (Group<R>& g : net.groups)
+      if (g.kind == LIF && g.p[10] != 0)
+        for (int32_t i : g.spikes) g.var[V][i] = (R)g.p[7];
+  };
+  if (net.reset_first) resets();
+  for (Syn<R>& s : net.syns) pathway_pre(net, s, t);
+  for (Syn<R>& s : net.syns)
+    if (s.effect == STDP) pathway_post(net, s, t);
+  if (!net.reset_first) resets();
+  ++net.ts;
+  return true;
+}
+
+template <typename R>
+int add_group(Net<R>& net, Group<R>&& g) {
+  if (net.built || g.n <= 0) return -1;
+  for (auto& v : g.var) v.assign(g.n, (R)0);
+  g.not_ref.assign(g.n, 1);
+  if (g.refractory() > 0) g.var[LASTSPIKE].assign(g.n, (R)-1e4);
+  net.groups.push_back(std::move(g));
+  return (int)net.groups.size() - 1;
+}
+
+template <typename R>
+void ensure_built(Net<R>& net) {
+  if (net.built) return;
+  for (Syn<R>& s : net.syns) build_syn(net, s);
+  net.built = true;
+}
+
+// ---- Hines (SpatialNeuron), literal restatement of spatialstateupdate.cu ----------------------
+template <typename RC>
+struct Hines {
+  int nn = 0;
+  std::vector<int64_t> comp_off;
+  std::vector<int32_t> sec_off, starts, ends, parent;   // starts/ends neuron-local
+  std::vector<double> area, rl1, rl2;
+  double Cm, Ri, El, EK, ENa, gl, gNa, gK, Vthr, dt;
+  // prepared matrix (per neuron, neuron-local indices into the flat arrays)
+  std::vector<double> invr, ab0, ab1, ab2, bplus, bminus, invr0, invrn;
+  std::vector<double> v, Ic, soma_I;
+  std::vector<RC> m, h, n;
+  std::vector<int32_t> spikes, above;
+};
+
+template <typename RC>
+void hines_prepare(Hines<RC>& H) {
+  const int64_t NC = H.comp_off[H.nn];
+  H.invr.assign(NC, 0); H.ab0.assign(NC, 0); H.ab1.assign(NC, 0); H.ab2.assign(NC, 0);
+  H.bplus.assign(NC, 0); H.bminus.assign(NC, 0);
+  H.invr0.assign(H.sec_off[H.nn], 0); H.invrn.assign(H.sec_off[H.nn], 0);
+  for (int b = 0; b < H.nn; ++b) {
+    const int64_t c0 = H.comp_off[b];
+    const int _N = (int)(H.comp_off[b + 1] - c0);
+    double* invr = &H.invr[c0];
+    double* a0 = &H.ab0[c0];
+    double* a1 = &H.ab1[c0];
+    double* a2 = &H.ab2[c0];
+    const double* area = &H.area[c0];
+    const double* r1 = &H.rl1[c0];
+    const double* r2 = &H.rl2[c0];
+    const int s0 = H.sec_off[b], ns = H.sec_off[b + 1] - s0;
+    for (int _i = 1; _i < _N; _i++) invr[_i] = 1.0 / (H.Ri * (1 / r2[_i - 1] + 1 / r1[_i]));
+    for (int _i = 0; _i < ns; _i++) invr[H.starts[s0 + _i]] = 0;
+    for (int _i = 0; _i < _N; _i++) a1[_i] = (-(H.Cm / H.dt) - invr[_i] / area[_i]);
+    for (int _i = 1; _i < _N; _i++) {
+      a0[_i] = invr[_i] / area[_i - 1];
+      a2[_i - 1] = invr[_i] / area[_i];
+      a1[_i - 1] -= invr[_i] / area[_i - 1];
+    }
+    for (int c = 0; c < ns; c++) {
+      const int first = H.starts[s0 + c];
+      const int last = H.ends[s0 + c] - 1;
+      const double i0 = r1[first] / H.Ri;
+      const double in = r2[last] / H.Ri;
+      H.invr0[s0 + c] = i0;
+      H.invrn[s0 + c] = in;
+      a1[first] -= (i0 / area[first]);
+      a1[last] -= (in / area[last]);
+      H.bplus[c0 + last] = -(in / area[last]);
+      H.bminus[c0 + first] = -(i0 / area[first]);
+    }
+  }
+}
+
+template <typename RC>
+RC hh_ee(RC x, RC a, RC b, RC dt) {
+  const RC A = -(a + b);
+  const RC BA = a / A;
+  return -BA + (BA + x) * xexp(A * dt);
+}
+
+template <typename RC>
+void hines_step(Hines<RC>& H, bool write_currents) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < H.nn; ++b) {
+    const int64_t c0 = H.comp_off[b];
+    const int _N = (int)(H.comp_off[b + 1] - c0);
+    const int s0 = H.sec_off[b], ns = H.sec_off[b + 1] - s0;
+    std::vector<double> gtot(_N), I0(_N), vprev(_N), vstar(_N), up(_N), um(_N), c(_N);
+    double* v = &H.v[c0];
+    // kernel 1: conductance/current from the state at the start of the step, then gates
+    for (int j = 0; j < _N; ++j) {
+      const double md = (double)H.m[c0 + j], hd = (double)H.h[c0 + j], nd = (double)H.n[c0 + j];
+      const double gna = H.gNa * (md * md * md * hd);
+      const double gk = H.gK * (nd * nd * nd * nd);
+      gtot[j] = H.gl + gna + gk;
+      I0[j] = H.gl * H.El + gna * H.ENa + gk * H.EK;
+      if (j == 0) I0[j] += H.soma_I[b];
+      vprev[j] = v[j];
+      const RC vr = (RC)v[j], dtR = (RC)H.dt;
+      const RC xm = (RC)25e-3 - vr;
+      const RC am = (RC)1e5 * xm / (xexp(xm / (RC)10e-3) - (RC)1);
+      const RC bm = (RC)4000 * xexp(-vr / (RC)18e-3);
+      const RC ah = (RC)70 * xexp(-vr / (RC)20e-3);
+      const RC bh = (RC)1000 / (xexp(((RC)30e-3 - vr) / (RC)10e-3) + (RC)1);
+      const RC xn = (RC)10e-3 - vr;
+      const RC an = (RC)1e4 * xn / (xexp(xn / (RC)10e-3) - (RC)1);
+      const RC bn = (RC)125 * xexp(-vr / (RC)80e-3);
+      H.m[c0 + j] = hh_ee(H.m[c0 + j], am, bm, dtR);
+      H.h[c0 + j] = hh_ee(H.h[c0 + j], ah, bh, dtR);
+      H.n[c0 + j] = hh_ee(H.n[c0 + j], an, bn, dtR);
+    }
+    const double* ab0 = &H.ab0[c0];
+    const double* ab1 = &H.ab1[c0];
+    const double* ab2 = &H.ab2[c0];
+    const double* bp = &H.bplus[c0];
+    const double* bmn = &H.bminus[c0];
+    // kernel 2: Thomas for each section (spatialstateupdate.cu:128-192)
+    for (int _i = 0; _i < ns; ++_i) {
+      const int _j_start = H.starts[s0 + _i], _j_end = H.ends[s0 + _i];
+      double _ai, _bi, _m;
+      for (int _j = _j_start; _j < _j_end; _j++) {
+        vstar[_j] = -(H.Cm / H.dt * v[_j]) - I0[_j];
+        up[_j] = bp[_j];
+        um[_j] = bmn[_j];
+        _bi = ab1[_j] - gtot[_j];
+        if (_j < _N - 1) c[_j] = ab0[_j + 1];
+        if (_j > 0) {
+          _ai = ab2[_j - 1];
+          _m = 1.0 / (_bi - _ai * c[_j - 1]);
+          c[_j] = c[_j] * _m;
+          vstar[_j] = (vstar[_j] - _ai * vstar[_j - 1]) * _m;
+          up[_j] = (up[_j] - _ai * up[_j - 1]) * _m;
+          um[_j] = (um[_j] - _ai * um[_j - 1]) * _m;
+        } else {
+          c[0] = c[0] / _bi;
+          vstar[0] = vstar[0] / _bi;
+          up[0] = up[0] / _bi;
+          um[0] = um[0] / _bi;
+        }
+      }
+      for (int _j = _j_end - 2; _j >= _j_start; _j--) {
+        vstar[_j] = vstar[_j] - c[_j] * vstar[_j + 1];
+        up[_j] = up[_j] - c[_j] * up[_j + 1];
+        um[_j] = um[_j] - c[_j] * um[_j + 1];
+      }
+    }
+    // kernel 3: coupling (spatialstateupdate.cu:202-307); node i+1 = end of section i
+    const int nB = ns + 1;
+    std::vector<int> parent_i(ns), nchild(nB, 0), idxchild(ns, 0);
+    std::vector<std::vector<int>> children(nB);
+    for (int i = 0; i < ns; ++i) parent_i[i] = i == 0 ? 0 : H.parent[s0 + i] + 1;
+    for (int i = 0; i < ns; ++i) {
+      idxchild[i] = (int)children[parent_i[i]].size();
+      children[parent_i[i]].push_back(i + 1);
+    }
+    std::vector<double> Pd(nB, 0), Pp(ns, 0), B(nB, 0);
+    std::vector<std::vector<double>> Pc(nB);
+    for (int i = 0; i < nB; ++i) Pc[i].assign(children[i].size(), 0.0);
+    for (int _i = 0; _i < nB - 1; _i++) {
+      const int _i_parent = parent_i[_i];
+      const int _i_childind = idxchild[_i];
+      const int _first = H.starts[s0 + _i];
+      const int _last = H.ends[s0 + _i] - 1;
+      const double _invr0 = H.invr0[s0 + _i];
+      const double _invrn = H.invrn[s0 + _i];
+      if (_i == 0) {
+        Pd[0] = um[_first] - 1;
+        Pc[0][0] = up[_first];
+        B[0] = -vstar[_first];
+      } else {
+        Pd[_i_parent] += (1 - um[_first]) * _invr0;
+        Pc[_i_parent][_i_childind] = -up[_first] * _invr0;
+        B[_i_parent] += vstar[_first] * _invr0;
+      }
+      Pd[_i + 1] = (1 - up[_last]) * _invrn;
+      Pp[_i] = -um[_last] * _invrn;
+      B[_i + 1] = vstar[_last] * _invrn;
+    }
+    for (int _i = nB - 1; _i >= 0; _i--) {
+      for (size_t _k = 0; _k < children[_i].size(); _k++) {
+        const int _j = children[_i][_k];
+        const double _subfac = Pc[_i][_k] / Pd[_j];
+        Pd[_i] = Pd[_i] - _subfac * Pp[_j - 1];
+        B[_i] = B[_i] - _subfac * B[_j];
+      }
+    }
+    B[0] = B[0] / Pd[0];
+    for (int _i = 1; _i < nB; _i++) {
+      const int _j = parent_i[_i - 1];
+      B[_i] = B[_i] - Pp[_i - 1] * B[_j];
+      B[_i] = B[_i] / Pd[_i];
+    }
+    // kernel 4: combine; kernel 5: currents
+    for (int _i = 0; _i < ns; ++_i) {
+      const int _i_parent = parent_i[_i];
+      for (int _j = H.starts[s0 + _i]; _j < H.ends[s0 + _i]; _j++)
+        v[_j] = vstar[_j] + B[_i_parent] * um[_j] + B[_i + 1] * up[_j];
+    }
+    if (write_currents)
+      for (int j = 0; j < _N; ++j) H.Ic[c0 + j] = H.Cm * (v[j] - vprev[j]) / H.dt;
+    const int ab = v[0] > H.Vthr ? 1 : 0;
+    if (ab && !H.above[b]) H.spikes[b]++;
+    H.above[b] = ab;
+  }
+}
+
+// ---- C API ------------------------------------------------------------------------------------
+struct Handle {
+  bool f32;
+  Net<float> nf;
+  Net<double> nd;
+};
+
+#define DISPATCH(h, fn, ...) ((h)->f32 ? fn<float>((h)->nf, __VA_ARGS__) : fn<double>((h)->nd, __VA_ARGS__))
+
+template <typename R>
+int api_group(Net<R>& net, int kind, int64_t n, const double* p, int np, double rate) {
+  Group<R> g;
+  g.kind = kind;
+  g.n = n;
+  if (p) g.p.assign(p, p + np);
+  g.rate = rate;
+  return add_group(net, std::move(g));
+}
+
+template <typename R>
+int api_spikegen(Net<R>& net, int64_t n, int64_t ns, const int32_t* idx, const int64_t* st) {
+  Group<R> g;
+  g.kind = SPIKEGEN;
+  g.n = n;
+  for (int64_t k = 0; k < ns; ++k) g.sg.emplace_back(st[k], idx[k]);
+  std::sort(g.sg.begin(), g.sg.end());
+  return add_group(net, std::move(g));
+}
+
+template <typename R>
+int api_state(Net<R>& net, int gid, int var, double* vals, int64_t n, int set) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  Group<R>& g = net.groups[gid];
+  if (n != g.n || var < 0 || var > NOT_REF) return -1;
+  for (int64_t i = 0; i < n; ++i) {
+    if (var == NOT_REF) {
+      if (set) g.not_ref[i] = vals[i] != 0; else vals[i] = g.not_ref[i];
+    } else {
+      if (set) g.var[var][i] = (R)vals[i]; else vals[i] = (double)g.var[var][i];
+    }
+  }
+  return 0;
+}
+
+template <typename R>
+int api_synapses(Net<R>& net, int pre, int post, int target, int effect, int64_t n,
+                 const int32_t* i, const int32_t* j, const double* w, double w_scalar,
+                 const int32_t* delay, int32_t delay_scalar, const double* stdp) {
+  if (net.built) return -1;
+  if (pre < 0 || post < 0 || pre >= (int)net.groups.size() || post >= (int)net.groups.size())
+    return -1;
+  Syn<R> s;
+  s.pre = pre; s.post = post; s.target = target; s.effect = effect; s.n = n;
+  s.i.assign(i, i + n);
+  s.j.assign(j, j + n);
+  s.delay.assign(n, delay_scalar);
+  if (delay) s.delay.assign(delay, delay + n);
+  s.max_delay = 0;
+  for (int32_t d : s.delay) s.max_delay = std::max(s.max_delay, d);
+  s.has_w = w != nullptr || effect == STDP;
+  s.w_scalar = (R)w_scalar;
+  if (s.has_w) {
+    s.w.assign(n, (R)w_scalar);
+    if (w) for (int64_t k = 0; k < n; ++k) s.w[k] = (R)w[k];
+  }
+  if (stdp) std::copy(stdp, stdp + 7, s.stdp);
+  net.syns.push_back(std::move(s));
+  return (int)net.syns.size() - 1;
+}
+
+// connect(p) restated from the paper's Philox: pair (i, j) connects when word (j mod 4) of
+// Philox(counter = (j/4, i, 0x5EED, 0), key = seed) is below floor(p * 2^32); its delay is
+// dmin + floor(word0 * nd / 2^32) of Philox(counter = (j, i, 0xDE1A, 1), key = seed).
+// Synapses are numbered in (i, delay, j) order.
+template <typename R>
+int api_random(Net<R>& net, int pre, int lo, int hi, int post, int target, double p,
+               int32_t dmin, int32_t dmax, double w, uint64_t seed) {
+  if (pre < 0 || post < 0 || pre >= (int)net.groups.size() || post >= (int)net.groups.size())
+    return -1;
+  if (lo < 0 || hi > net.groups[pre].n || lo >= hi) return -1;
+  const int64_t npost = net.groups[post].n;
+  const uint64_t thr = p >= 1.0 ? ((uint64_t)1 << 32) : (p <= 0 ? 0 : (uint64_t)(p * 4294967296.0));
+  const int32_t nd = dmax - dmin + 1;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  std::vector<int32_t> I, J, Dl;
+  for (int64_t i = lo; i < hi; ++i) {
+    std::vector<std::pair<int32_t, int32_t>> row;  // (delay, j)
+    for (int64_t jq = 0; 4 * jq < npost; ++jq) {
+      const Ctr r = philox(Ctr{{(uint32_t)jq, (uint32_t)i, 0x5EEDu, 0u}}, k0, k1);
+      for (int e = 0; e < 4 && 4 * jq + e < npost; ++e) {
+        if ((uint64_t)r.v[e] < thr) {
+          const uint32_t j = (uint32_t)(4 * jq + e);
+          const Ctr rd = philox(Ctr{{j, (uint32_t)i, 0xDE1Au, 1u}}, k0, k1);
+          const int32_t d = dmin + (int32_t)(((uint64_t)rd.v[0] * (uint64_t)(uint32_t)nd) >> 32);
+          row.emplace_back(d, (int32_t)j);
+        }
+      }
+    }
+    std::stable_sort(row.begin(), row.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (auto& x : row) { I.push_back((int32_t)i); J.push_back(x.second); Dl.push_back(x.first); }
+  }
+  return api_synapses(net, pre, post, target, ADD, (int64_t)I.size(), I.data(), J.data(),
+                      nullptr, w, Dl.data(), 0, nullptr);
+}
+
+template <typename R>
+int64_t api_syn_count(Net<R>& net, int sid) {
+  if (sid < 0 || sid >= (int)net.syns.size()) return -1;
+  return net.syns[sid].n;
+}
+
+template <typename R>
+int api_syn_get(Net<R>& net, int sid, int var, double* out, int64_t n) {
+  if (sid < 0 || sid >= (int)net.syns.size()) return -1;
+  ensure_built(net);
+  Syn<R>& s = net.syns[sid];
+  if (n != s.n) return -1;
+  for (int64_t k = 0; k < n; ++k) {
+    switch (var) {
+      case SYN_I: out[k] = s.i[k]; break;
+      case SYN_J: out[k] = s.j[k]; break;
+      case SYN_DELAY: out[k] = s.delay[k]; break;
+      case SYN_W: out[k] = s.has_w ? (double)s.w[k] : (double)s.w_scalar; break;
+      case SYN_APRE: out[k] = s.effect == STDP ? (double)s.apre[k] : 0; break;
+      case SYN_APOST: out[k] = s.effect == STDP ? (double)s.apost[k] : 0; break;
+      case SYN_LU: out[k] = s.effect == STDP ? (double)s.lu[k] : 0; break;
+      default: return -1;
+    }
+  }
+  return 0;
+}
+
+template <typename R>
+int api_uniforms(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  Group<R>& g = net.groups[gid];
+  if (g.kind != POISSON || n != g.n) return -1;
+  for (int64_t k = 0; k < steps; ++k) g.uniforms.emplace_back(u + k * n, u + (k + 1) * n);
+  return 0;
+}
+
+template <typename R>
+int api_run(Net<R>& net, int64_t steps, int64_t) {
+  ensure_built(net);
+  for (int64_t k = 0; k < steps; ++k)
+    if (!step(net)) return -1;
+  return 0;
+}
+
+template <typename R>
+int64_t api_spikes(Net<R>& net, int gid, int32_t* idx, int64_t* st, int64_t cap) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  auto rec = net.groups[gid].recorded;
+  std::sort(rec.begin(), rec.end());
+  for (int64_t k = 0; k < (int64_t)rec.size() && k < cap; ++k) {
+    if (st) st[k] = rec[k].first;
+    if (idx) idx[k] = rec[k].second;
+  }
+  return (int64_t)rec.size();
+}
+
+// Bundles still queued after the last step: (offset a >= 1 at which it is delivered, pre,
+// delay), sorted.  Slot (current_offset + a) % num_queues is delivered a steps from now.
+template <typename R>
+int64_t api_queue(Net<R>& net, int sid, int32_t* off, int32_t* pre, int32_t* dl, int64_t cap) {
+  if (sid < 0 || sid >= (int)net.syns.size()) return -1;
+  ensure_built(net);
+  Syn<R>& s = net.syns[sid];
+  const int D = s.max_delay + 1;
+  std::vector<std::array<int32_t, 3>> out;
+  for (int a = 1; a < s.num_queues; ++a) {
+    for (int64_t key : s.queue[(s.current_offset + a) % s.num_queues])
+      out.push_back({a, (int32_t)(key / D), (int32_t)(key % D)});
+  }
+  std::sort(out.begin(), out.end());
+  for (int64_t k = 0; k < (int64_t)out.size() && k < cap; ++k) {
+    if (off) off[k] = out[k][0];
+    if (pre) pre[k] = out[k][1];
+    if (dl) dl[k] = out[k][2];
+  }
+  return (int64_t)out.size();
+}
+
+struct HinesHandle {
+  bool f32;
+  Hines<float> hf;
+  Hines<double> hd;
+};
+
+template <typename RC>
+void hines_init(Hines<RC>& H, int nn, const int64_t* comp_off, const int32_t* sec_off,
+                const int32_t* st, const int32_t* en, const int32_t* par, const double* d,
+                const double* L, const double* p, double dt) {
+  H.nn = nn;
+  H.comp_off.assign(comp_off, comp_off + nn + 1);
+  H.sec_off.assign(sec_off, sec_off + nn + 1);
+  const int32_t S = sec_off[nn];
+  const int64_t C = comp_off[nn];
+  H.starts.assign(st, st + S);
+  H.ends.assign(en, en + S);
+  H.parent.assign(par, par + S);
+  H.area.resize(C); H.rl1.resize(C); H.rl2.resize(C);
+  for (int64_t c = 0; c < C; ++c) {
+    H.area[c] = M_PI * d[c] * L[c];
+    H.rl1[c] = H.rl2[c] = M_PI * d[c] * d[c] / (2.0 * L[c]);
+  }
+  H.Cm = p[0]; H.Ri = p[1]; H.El = p[2]; H.EK = p[3]; H.ENa = p[4]; H.gl = p[5]; H.gNa = p[6];
+  H.gK = p[7]; H.Vthr = p[8]; H.dt = dt;
+  H.v.assign(C, 0); H.Ic.assign(C, 0); H.soma_I.assign(nn, 0);
+  H.m.assign(C, 0); H.h.assign(C, 0); H.n.assign(C, 0);
+  H.spikes.assign(nn, 0); H.above.assign(nn, 0);
+  hines_prepare(H);
+}
+
+}  // namespace
+
+extern "C" {
+
+// flags: bit 0 = float32 arithmetic, bit 1 = resets before synapses
+void* orc_create(double dt, int flags) {
+  Handle* h = new Handle();
+  h->f32 = (flags & 1) != 0;
+  h->nf.dt = dt;
+  h->nd.dt = dt;
+  h->nf.reset_first = h->nd.reset_first = (flags & 2) != 0;
+  return h;
+}
+void orc_destroy(void* h) { delete static_cast<Handle*>(h); }
+const char* orc_error(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return h->f32 ? h->nf.err.c_str() : h->nd.err.c_str();
+}
+// LIF params (12): El taum taue taui ke ki Vt Vr refractory has_threshold has_reset unless
+int orc_group_lif(void* hp, int64_t n, const double* p) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_group, LIF, n, p, 12, 0.0);
+}
+// HH params (14): Cm gl El EK ENa gNa gK VT Ee Ei taue taui Vthr refractory
+int orc_group_hh(void* hp, int64_t n, const double* p) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_group, HH, n, p, 14, 0.0);
+}
+int orc_group_poisson(void* hp, int64_t n, double rate) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_group, POISSON, n, nullptr, 0, rate);
+}
+int orc_group_spikegen(void* hp, int64_t n, int64_t ns, const int32_t* idx, const int64_t* st) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_spikegen, n, ns, idx, st);
+}
+int orc_state_set(void* hp, int gid, int var, const double* v, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_state, gid, var, const_cast<double*>(v), n, 1);
+}
+int orc_state_get(void* hp, int gid, int var, double* v, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_state, gid, var, v, n, 0);
+}
+// stdp (7): taupre taupost dApre dApost wmin wmax pre_adds_weight
+int orc_synapses(void* hp, int pre, int post, int target, int effect, int64_t n,
+                 const int32_t* i, const int32_t* j, const double* w, double w_scalar,
+                 const int32_t* delay, int32_t delay_scalar, const double* stdp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_synapses, pre, post, target, effect, n, i, j, w, w_scalar, delay,
+                  delay_scalar, stdp);
+}
+int orc_synapses_random(void* hp, int pre, int lo, int hi, int post, int target, double p,
+                        int32_t dmin, int32_t dmax, double w, uint64_t seed) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_random, pre, lo, hi, post, target, p, dmin, dmax, w, seed);
+}
+int64_t orc_syn_count(void* hp, int sid) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_syn_count, sid);
+}
+int orc_syn_get(void* hp, int sid, int var, double* out, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_syn_get, sid, var, out, n);
+}
+int orc_set_uniforms(void* hp, int gid, const double* u, int64_t steps, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_uniforms, gid, u, steps, n);
+}
+int orc_run(void* hp, int64_t steps) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_run, steps, 0);
+}
+int64_t orc_timestep(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return h->f32 ? h->nf.ts : h->nd.ts;
+}
+int64_t orc_spikes(void* hp, int gid, int32_t* idx, int64_t* st, int64_t cap) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_spikes, gid, idx, st, cap);
+}
+int64_t orc_queue(void* hp, int sid, int32_t* off, int32_t* pre, int32_t* dl, int64_t cap) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_queue, sid, off, pre, dl, cap);
+}
+
+// Hines. p (9): Cm Ri El EK ENa gl gNa gK Vthr
+void* orc_hines_create(int nn, const int64_t* comp_off, const int32_t* sec_off,
+                       const int32_t* st, const int32_t* en, const int32_t* par,
+                       const double* d, const double* L, const double* p, double dt, int f32) {
+  HinesHandle* h = new HinesHandle();
+  h->f32 = f32 != 0;
+  if (h->f32) hines_init(h->hf, nn, comp_off, sec_off, st, en, par, d, L, p, dt);
+  else hines_init(h->hd, nn, comp_off, sec_off, st, en, par, d, L, p, dt);
+  return h;
+}
+void orc_hines_destroy(void* h) { delete static_cast<HinesHandle*>(h); }
+int orc_hines_set_current(void* hp, const double* I) {
+  HinesHandle* h = static_cast<HinesHandle*>(hp);
+  auto set = [&](auto& H) {
+    for (int b = 0; b < H.nn; ++b) H.soma_I[b] = I ? I[b] / H.area[H.comp_off[b]] : 0.0;
+  };
+  if (h->f32) set(h->hf); else set(h->hd);
+  return 0;
+}
+// vars: 0 v, 1 m, 2 h, 3 n, 4 Ic (values as doubles)
+int orc_hines_state(void* hp, int var, double* vals, int64_t n, int set) {
+  HinesHandle* h = static_cast<HinesHandle*>(hp);
+  auto go = [&](auto& H) {
+    if (n != H.comp_off[H.nn]) return -1;
+    for (int64_t c = 0; c < n; ++c) {
+      switch (var) {
+        case 0: if (set) H.v[c] = vals[c]; else vals[c] = H.v[c]; break;
+        case 1: if (set) H.m[c] = vals[c]; else vals[c] = H.m[c]; break;
+        case 2: if (set) H.h[c] = vals[c]; else vals[c] = H.h[c]; break;
+        case 3: if (set) H.n[c] = vals[c]; else vals[c] = H.n[c]; break;
+        case 4: if (set) H.Ic[c] = vals[c]; else vals[c] = H.Ic[c]; break;
+        default: return -1;
+      }
+    }
+    return 0;
+  };
+  return h->f32 ? go(h->hf) : go(h->hd);
+}
+int orc_hines_run(void* hp, int64_t steps) {
+  HinesHandle* h = static_cast<HinesHandle*>(hp);
+  for (int64_t k = 0; k < steps; ++k) {
+    if (h->f32) hines_step(h->hf, k == steps - 1);
+    else hines_step(h->hd, k == steps - 1);
+  }
+  return 0;
+}
+int orc_hines_spikes(void* hp, int32_t* out, int n) {
+  HinesHandle* h = static_cast<HinesHandle*>(hp);
+  auto& sp = h->f32 ? h->hf.spikes : h->hd.spikes;
+  if (n != (int)sp.size()) return -1;
+  std::copy(sp.begin(), sp.end(), out);
+  return 0;
+}
+
+}  // extern "C"

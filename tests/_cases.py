@@ -1,0 +1,150 @@
+"""Known-answer cases restated from the reference's own tests, without Brian2.
+
+Each case takes `make(dt, **kw)` returning a backend with the `Network` interface (the CUDA
+library or the CPU oracle), builds the network of the reference test, runs it and checks
+the answer that test asserts.  Spike steps are exact integers here; the reference compares
+spike times t = step*dt.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from brian2cuda_b200.network import LIF
+
+DT = 1e-4  # Brian2's defaultclock.dt
+
+
+def _spike_steps(net, gid):
+    idx, st = net.spikes(gid)
+    return idx, st
+
+
+def neuron_v1():
+    """`NeuronGroup(N, 'v:1', threshold='v>1', reset='v=0')`."""
+    return LIF(El=0.0, taum=math.inf, Vt=1.0, Vr=0.0)
+
+
+def example_run(make):
+    """brian2cuda/__init__.py:50-72: dv/dt = -v/tau, v0 = i/100, 1 ms later
+    v == i/100 * exp(-1 ms / 10 ms)."""
+    net = make(DT)
+    G = net.lif_group(100, LIF(El=0.0, taum=10e-3, Vt=1.0, Vr=0.0, refractory=5e-3),
+                      "float64")
+    net.set_state(G, "v", np.arange(100) / 100.0)
+    net.finalize()
+    net.run(10)
+    v = net.get_state(G, "v")
+    np.testing.assert_allclose(v, np.arange(100) / 100 * np.exp(-1e-3 / 10e-3), rtol=1e-12)
+
+
+def push_outer_loop(make):
+    """test_synaptic_propagations.py:11-48: one input spike at t=0 to 15*1025 targets with
+    delays alternating 0 and dt; even targets spike at dt, odd ones at 2 dt."""
+    N = 1025 * 15
+    net = make(DT)
+    inp = net.spikegen_group(1, [0], [0])
+    G = net.lif_group(N, neuron_v1(), "float64")
+    j = np.arange(N)
+    net.synapses(inp, G, "v", np.zeros(N, np.int32), j, w_scalar=1.1, delay=(j % 2))
+    net.spike_monitor(G, 4 * N)
+    net.finalize()
+    net.run(3)
+    idx, st = _spike_steps(net, G)
+    assert len(idx) == N
+    np.testing.assert_array_equal(np.sort(idx[st == 1]), np.arange(0, N, 2))
+    np.testing.assert_array_equal(np.sort(idx[st == 2]), np.arange(1, N, 2))
+
+
+def push_outer_loop2(make):
+    """test_synaptic_propagations.py:51-150 with one post block: input 0 spikes in the first
+    2048 steps with zero weight, input 1 once at step 2048 with weight 1.1 and delays
+    j (j = 1024 gets 1023); target j then spikes at step 2049 + delay."""
+    npb = 2048
+    net = make(DT)
+    inp = net.spikegen_group(2, [0] * npb + [1], np.arange(npb + 1))
+    G = net.lif_group(npb, neuron_v1(), "float64")
+    i = np.repeat([0, 1], npb).astype(np.int32)
+    j = np.tile(np.arange(npb), 2).astype(np.int32)
+    w = np.where(i == 0, 0.0, 1.1)
+    d = j.copy()
+    d[(i == 1) & (j == 1024)] = 1023
+    net.synapses(inp, G, "v", i, j, w=w, delay=d)
+    net.spike_monitor(G, 4 * npb)
+    net.finalize()
+    steps = 2 * npb + 2
+    net.run(steps)
+    idx, st = _spike_steps(net, G)
+    assert len(idx) == npb
+    for n in range(steps):
+        got = np.sort(idx[st == n])
+        if n <= npb or n == steps - 1:
+            assert len(got) == 0, n
+            continue
+        s = n - (npb + 1)
+        if s == 1023:
+            exp = [1023, 1024]
+        elif s == 1024:
+            exp = []
+        else:
+            exp = [s]
+        np.testing.assert_array_equal(got, exp, err_msg=f"step {n}")
+
+
+def _circular(net, inp):
+    G = net.lif_group(5, neuron_v1(), "float64")
+    net.synapses(inp, G, "v", [0], [0], w_scalar=1.1, delay=0)
+    net.synapses(inp, G, "v", [0], [1], w_scalar=1.1, delay=2)
+    net.synapses(inp, G, "v", [0], [2], w_scalar=1.1, delay=5)
+    net.synapses(inp, G, "v", [0, 0], [3, 4], w_scalar=1.1, delay=np.array([3, 4]))
+    net.spike_monitor(G, 1000)
+    return G
+
+
+def circular_eventspaces(make):
+    """test_synaptic_propagations.py:153-184 (and :343-374): homogeneous delays 0, 2, 5 and
+    heterogeneous delays 3, 4; each target spikes the step after its effect arrives."""
+    net = make(DT)
+    inp = net.spikegen_group(1, [0], [0])
+    G = _circular(net, inp)
+    net.finalize()
+    net.run(7)
+    idx, st = _spike_steps(net, G)
+    for neuron, step in [(0, 1), (1, 3), (2, 6), (3, 4), (4, 5)]:
+        np.testing.assert_array_equal(st[idx == neuron], [step])
+
+
+def circular_eventspaces_spikegenerator(make):
+    """test_synaptic_propagations.py:187-227: input spikes in each of the first 12 steps,
+    schedule with resets before synapses."""
+    n = 12
+    net = make(DT, reset_before_synapses=True)
+    inp = net.spikegen_group(1, [0] * n, np.arange(n))
+    G = _circular(net, inp)
+    net.finalize()
+    net.run(n + 6)
+    idx, st = _spike_steps(net, G)
+    for neuron, first in [(0, 1), (1, 3), (2, 6), (3, 4), (4, 5)]:
+        np.testing.assert_array_equal(np.sort(st[idx == neuron]), np.arange(first, first + n))
+
+
+def multiple_runs_scalar_delay(make):
+    """test_network_multiple_runs.py:10-26: an always-spiking input, `v += 1` with delay dt,
+    two runs of two steps; v at the start of each step is [0, 0, 1, 2]."""
+    net = make(DT)
+    inG = net.lif_group(1, LIF(taum=math.inf, Vt=-math.inf, has_reset=False), "float64")
+    G = net.lif_group(1, LIF(taum=math.inf, has_threshold=False, has_reset=False), "float64")
+    net.set_state(G, "v", 0.0)
+    net.synapses(inG, G, "v", [0], [0], w_scalar=1.0, delay=1)
+    net.finalize()
+    trace = []
+    for _run in range(2):
+        for _ in range(2):
+            trace.append(float(net.get_state(G, "v")[0]))
+            net.run(1)
+    assert trace == [0.0, 0.0, 1.0, 2.0]
+
+
+ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
+       circular_eventspaces_spikegenerator, multiple_runs_scalar_delay]

@@ -1,0 +1,253 @@
+"""Parity of the CUDA library (through the C ABI) with the CPU oracle on seeded inputs.
+
+Tolerances: float64 state within 1e-10 relative of the float64 oracle (the exact-LIF update
+is bit-identical: both sides evaluate the same fused multiply-adds); float32 state within
+1e-5 relative (plus an absolute floor of 1e-5 of the variable's scale) of the float64
+oracle; spike indices, spike counts per step and delay-queue contents exactly.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from brian2cuda_b200 import models
+from brian2cuda_b200.network import LIF
+
+pytestmark = pytest.mark.gpu
+DT = 1e-4
+mV = 1e-3
+
+
+def _close(a, b, rtol, atol):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    bad = np.abs(a - b) > rtol * np.abs(b) + atol
+    assert not bad.any(), f"{bad.sum()} mismatches, worst {np.max(np.abs(a - b))}"
+
+
+def _random_lif_state(net, G, n, rng, t0_steps):
+    net.set_state(G, "v", rng.uniform(-62 * mV, -48 * mV, n))
+    net.set_state(G, "ge", rng.uniform(-2 * mV, 5 * mV, n))
+    net.set_state(G, "gi", rng.uniform(-9 * mV, 0, n))
+    net.set_state(G, "lastspike", (t0_steps - rng.integers(0, 100, n)) * DT)
+
+
+def test_lif_float64_step_is_bit_exact(gpu_factory, oracle_factory):
+    n = 5003
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        rng = np.random.default_rng(7)
+        net = make(DT)
+        G = net.lif_group(n, models.cuba_lif(), "float64")
+        _random_lif_state(net, G, n, rng, 0)
+        net.spike_monitor(G, 10 * n)
+        net.finalize()
+        net.run(1)
+        out[name] = {v: net.get_state(G, v) for v in ("v", "ge", "gi", "lastspike")}
+        out[name]["spk"] = np.sort(net.spikes(G)[0])
+    for v in ("v", "ge", "gi", "lastspike"):
+        np.testing.assert_array_equal(out["gpu"][v], out["orc"][v], err_msg=v)
+    np.testing.assert_array_equal(out["gpu"]["spk"], out["orc"]["spk"])
+    assert len(out["gpu"]["spk"]) > 0
+
+
+def _random_hh_state(net, P, n, rng):
+    net.set_state(P, "v", rng.uniform(-80 * mV, 10 * mV, n))
+    net.set_state(P, "m", rng.uniform(0, 1, n))
+    net.set_state(P, "h", rng.uniform(0, 1, n))
+    net.set_state(P, "n", rng.uniform(0, 1, n))
+    net.set_state(P, "ge", rng.uniform(0, 80e-9, n))
+    net.set_state(P, "gi", rng.uniform(0, 400e-9, n))
+    lastspike = -rng.integers(0, 60, n) * DT
+    net.set_state(P, "lastspike", lastspike)
+    return lastspike
+
+
+def test_hh_float32_step_within_tolerance(gpu_factory, oracle_factory):
+    n = 20000
+    res = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        rng = np.random.default_rng(11)
+        net = make(DT)
+        P = net.hh_group(n, models.cobahh_hh(), "float32")
+        ls = _random_hh_state(net, P, n, rng)
+        net.spike_monitor(P, 10 * n)
+        net.finalize()
+        net.run(1)
+        res[name] = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi")}
+        res[name]["spk"] = np.sort(net.spikes(P)[0])
+    scale = {"v": 0.1, "m": 1, "h": 1, "n": 1, "ge": 80e-9, "gi": 400e-9}
+    for v in scale:
+        _close(res["gpu"][v], res["orc"][v], 1e-5, 1e-5 * scale[v])
+    # spikes given the same state: the GPU's own post-update v decides, exactly
+    v = res["gpu"]["v"]
+    nr = ((0 - ls + 1e-3 * DT) / DT).astype(np.int64) >= 30
+    expect = np.nonzero((v > np.float32(-20 * mV)) & nr)[0]
+    np.testing.assert_array_equal(res["gpu"]["spk"], expect)
+
+
+def test_cuba_rollout_float64(gpu_factory, oracle_factory):
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        ids = models.build_cuba(net, n=1000, p=0.05, dtype="float64")
+        net.finalize()
+        net.run(300)
+        idx, st = net.spikes(ids["P"])
+        out[name] = (idx, st, net.get_state(ids["P"], "v"), net.get_state(ids["P"], "ge"))
+    gi, gs, gv, gge = out["gpu"]
+    oi, os_, ov, oge = out["orc"]
+    assert len(gi) > 100
+    np.testing.assert_array_equal(gs, os_)
+    np.testing.assert_array_equal(gi, oi)
+    _close(gv, ov, 1e-10, 1e-15)
+    _close(gge, oge, 1e-10, 1e-15)
+
+
+def _delay_net(net, n=800, p=0.05, seed=3):
+    rng = np.random.default_rng(seed)
+    G = net.lif_group(n, models.cuba_lif(), "float64")
+    net.set_state(G, "v", rng.uniform(-60 * mV, -50 * mV, n))
+    i, j = models.bernoulli_pairs(rng, n, n, p)
+    d = rng.integers(1, 17, size=len(i)).astype(np.int32)
+    ne = int(0.8 * n)
+    exc = i < ne
+    Ce = net.synapses(G, G, "ge", i[exc], j[exc], w=np.full(exc.sum(), 1.62 * mV), delay=d[exc])
+    Ci = net.synapses(G, G, "gi", i[~exc], j[~exc], w_scalar=-9 * mV, delay=d[~exc])
+    net.spike_monitor(G, 10**6)
+    return G, Ce, Ci, (i, j, d, exc)
+
+
+def test_heterogeneous_delays_rollout_and_queue(gpu_factory, oracle_factory):
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        G, Ce, Ci, _ = _delay_net(net)
+        net.finalize()
+        net.run(237)
+        idx, st = net.spikes(G)
+        out[name] = (idx, st, net.queue(Ce), net.queue(Ci), net.get_state(G, "v"))
+    for k in range(4):
+        np.testing.assert_array_equal(out["gpu"][k], out["orc"][k], err_msg=str(k))
+    assert len(out["gpu"][0]) > 100 and len(out["gpu"][2]) > 0
+    _close(out["gpu"][4], out["orc"][4], 1e-10, 1e-15)
+
+
+def test_synapse_readback_in_input_order(gpu_factory):
+    net = gpu_factory(DT)
+    G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=300)
+    net.finalize()
+    for sid, sel in ((Ce, exc), (Ci, ~exc)):
+        np.testing.assert_array_equal(net.syn_get(sid, "i"), i[sel])
+        np.testing.assert_array_equal(net.syn_get(sid, "j"), j[sel])
+        np.testing.assert_array_equal(net.syn_get(sid, "delay"), d[sel])
+    np.testing.assert_array_equal(net.syn_get(Ce, "w"), np.full(exc.sum(), 1.62 * mV))
+    np.testing.assert_array_equal(net.syn_get(Ci, "w"), np.full((~exc).sum(), -9 * mV))
+
+
+def test_generated_connectivity_matches_oracle(gpu_factory, oracle_factory):
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        A = net.lif_group(300, models.cuba_lif(), "float64")
+        B = net.lif_group(517, models.cuba_lif(), "float64")
+        s1 = net.synapses_random(A, B, "ge", 0.05, 1, 20, 1e-3, 12345, pre_range=(0, 240))
+        s2 = net.synapses_random(A, B, "gi", 0.1, 3, 3, -1e-3, 999, pre_range=(240, 300))
+        net.finalize()
+        out[name] = [net.syn_get(s, v) for s in (s1, s2) for v in ("i", "j", "delay")]
+    for a, b in zip(out["gpu"], out["orc"]):
+        np.testing.assert_array_equal(a, b)
+    assert len(out["gpu"][0]) > 1000
+
+
+def test_stdp_with_poisson_input(gpu_factory, oracle_factory):
+    K = 50
+    gpu = gpu_factory(DT, steps_per_graph=K, seed=5)
+    orc = oracle_factory(DT)
+    ids = {}
+    for name, net in (("gpu", gpu), ("orc", orc)):
+        ids[name] = models.build_stdp(net, n_in=400, n_out=60, rate=80.0, dtype="float64",
+                                      monitor_capacity=10**6)
+        net.finalize()
+    for _ in range(8):
+        gpu.run(K)
+        orc.set_uniforms(ids["orc"]["inp"], gpu.rng_uniforms(ids["gpu"]["inp"], K))
+        orc.run(K)
+    for g in ("inp", "out"):
+        a, b = gpu.spikes(ids["gpu"][g]), orc.spikes(ids["orc"][g])
+        np.testing.assert_array_equal(a[1], b[1])
+        np.testing.assert_array_equal(a[0], b[0])
+    assert len(gpu.spikes(ids["gpu"]["out"])[0]) > 0
+    for v in ("w", "Apre", "Apost", "lastupdate"):
+        _close(gpu.syn_get(ids["gpu"]["S"], v), orc.syn_get(ids["orc"]["S"], v), 1e-10, 1e-18)
+
+
+def test_poisson_spikes_follow_uniforms(gpu_factory):
+    K = 20
+    net = gpu_factory(DT, steps_per_graph=K, seed=9)
+    P = net.poisson_group(1000, 300.0, "float32")
+    net.spike_monitor(P, 10**5)
+    net.finalize()
+    net.run(K)
+    u = net.rng_uniforms(P, K)
+    idx, st = net.spikes(P)
+    exp_st, exp_idx = np.nonzero(u < np.float32(300.0 * DT))
+    np.testing.assert_array_equal(st, exp_st)
+    np.testing.assert_array_equal(idx, exp_idx)
+    assert 0.0 < u.min() and u.max() <= 1.0
+
+
+def _hines_pair(gpu_factory, channel_dtype, n_neurons=6, steps=300):
+    from oracle.oracle import OracleHines
+    net = gpu_factory(25e-6)
+    hb, morph, params, current = models.build_hines(net, n_neurons=n_neurons,
+                                                    channel_dtype=channel_dtype,
+                                                    comp_range=(40, 160))
+    orc = OracleHines(25e-6, morph["comp_off"], morph["sec_off"], morph["sec_start"],
+                      morph["sec_end"], morph["sec_parent"], morph["diameter"], morph["length"],
+                      params, f32=(channel_dtype == "float32"))
+    for k, v in models.hines_rest_state().items():
+        orc.set_state(k, v)
+    orc.set_current(current)
+    hb.run(steps)
+    orc.run(steps)
+    return hb, orc
+
+
+def test_hines_float64_channels(gpu_factory):
+    hb, orc = _hines_pair(gpu_factory, "float64")
+    for v, atol in (("v", 1e-15), ("m", 1e-15), ("h", 1e-15), ("n", 1e-15), ("Ic", 1e-12)):
+        _close(hb.get_state(v), orc.get_state(v), 1e-10, atol)
+    np.testing.assert_array_equal(hb.spike_counts(), orc.spike_counts())
+
+
+def test_hines_float32_channels(gpu_factory):
+    hb, orc = _hines_pair(gpu_factory, "float32")
+    _close(hb.get_state("v"), orc.get_state("v"), 1e-4, 1e-6)
+    for v in ("m", "h", "n"):
+        _close(hb.get_state(v), orc.get_state(v), 1e-4, 1e-5)
+
+
+def test_monitor_overflow_is_reported(gpu_factory):
+    from brian2cuda_b200 import B2BError
+    net = gpu_factory(DT)
+    G = net.lif_group(100, LIF(taum=math.inf, Vt=-math.inf, has_reset=False), "float64")
+    net.spike_monitor(G, 150)
+    net.finalize()
+    net.run(3)
+    assert net.sync() == 3  # B2B_ERR_QUEUE_OVERFLOW
+    with pytest.raises(B2BError):
+        net.spikes(G)
+
+
+def test_graph_and_eager_agree(gpu_factory):
+    res = []
+    for graphs in (True, False):
+        net = gpu_factory(DT, graphs=graphs, steps_per_graph=25)
+        G, Ce, Ci, _ = _delay_net(net, n=400)
+        net.finalize()
+        net.run(113)
+        res.append(net.spikes(G))
+        assert net.kernel_launches > 0
+    np.testing.assert_array_equal(res[0][0], res[1][0])
+    np.testing.assert_array_equal(res[0][1], res[1][1])
