@@ -1,11 +1,14 @@
 """Benchmark: COBAHH network, 100,000 Hodgkin-Huxley neurons, float32, exponential Euler,
-dt = 0.1 ms, connect(p=0.02) (about 2e8 synapses) with per-synapse delays of 1..50 steps.
+dt = 0.1 ms, connect(p=0.02) (about 2e8 synapses) with per-synapse delays of 1..50 steps,
+1 s simulated.
 
-One bench step = 100 simulation time steps (10 ms of biological time) of the whole network
-(fused neuron kernel + spike delivery), replayed from CUDA graphs.  value = synaptic
-events/s (spikes x out-degree delivered per second of wall time on the device); the line
-also carries neuron-updates/s.  Inputs (state, 1.6 GB of synapse arrays) are resident in
-HBM before timing starts; the synapse arrays alone exceed the 126 MB L2.
+One bench step = the whole configured run: restore the seeded initial state (a device-side
+checkpoint) and simulate 1 s = 10,000 time steps (fused neuron kernel + spike delivery,
+replayed from CUDA graphs).  The network fires in population bursts about every 140 ms, so
+shorter windows would sample the burst cycle unevenly.  value = synaptic events/s (spikes
+x out-degree delivered per second of device time); the line also carries
+neuron-updates/s.  Inputs (state, 1.6 GB of synapse arrays) are resident in HBM before
+timing starts; the synapse arrays alone exceed the 126 MB L2.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b2b|reference]
 Under torchrun every rank runs an independent replica (weak scaling; the network does not
@@ -31,10 +34,10 @@ DT = 1e-4
 N_NEURONS = 100_000
 P_CONNECT = 0.02
 DMIN, DMAX = 1, 50
-SIM_STEPS = 100              # simulation steps per bench step
+SIM_STEPS = 10_000           # simulation steps per bench step (1 s)
 BYTES_NEURON_UPDATE = 54     # COBAHH f32: 6 vars x 4 B x (R+W) + flag + lastspike
 BYTES_EVENT = 16             # post index 4 + weight 4 + target R/W 8
-BYTES_BUNDLE = 8             # bundle offsets read per (spike, delay)
+BYTES_BUNDLE = 8             # per (spike, delay) bundle visited
 METRIC = "synaptic events/s"
 UNIT = "events/s"
 WORKLOAD = "COBAHH 1e5 HH neurons f32 exp-Euler, p=0.02 (~2e8 synapses), delays U{1..50} steps"
@@ -152,19 +155,20 @@ def cpu_network(steps_budget_s: float, max_steps: int):
     sel = st >= 1
     events = float(outdeg[idx[sel]].sum())
     return {"events": events, "steps": steps, "seconds": el, "n_syn": n_syn,
-            "neuron_updates": float(N_NEURONS) * steps}
+            "neuron_updates": float(N_NEURONS) * steps, "spikes": int(sel.sum())}
 
 
 def reference_arm(args):
     threads = os.cpu_count()
     t0 = time.perf_counter()
-    r = cpu_network(steps_budget_s=min(60.0, 8.0 * (args.steps + args.warmup)),
-                    max_steps=20 * (args.steps + args.warmup))
+    r = cpu_network(steps_budget_s=min(120.0, 10.0 * (args.steps + args.warmup)),
+                    max_steps=SIM_STEPS)
     value = r["events"] / r["seconds"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * r["seconds"] / max(1, r["steps"]) * SIM_STEPS,
+        "firing_rate_hz": r["spikes"] / (N_NEURONS * max(1, r["steps"]) * DT),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "sim_steps_per_step": SIM_STEPS,
@@ -203,8 +207,8 @@ def main():
     from brian2cuda_b200 import Network, models
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
-    total_sim = SIM_STEPS * (args.warmup + 2 * args.steps) + 300
-    mon_cap = int(N_NEURONS * total_sim * DT * 400)  # room for a mean rate up to 400 Hz
+    runs = args.warmup + 2 * args.steps + 1
+    mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
                   stream=stream.cuda_stream)
     t_setup = time.perf_counter()
@@ -212,6 +216,7 @@ def main():
                               monitor_capacity=mon_cap)
     net.finalize()
     P = ids["P"]
+    ne = int(0.8 * N_NEURONS)
     outdeg = np.zeros(N_NEURONS, np.int64)
     n_syn = 0
     for sid in (ids["Ce"], ids["Ci"]):
@@ -219,72 +224,92 @@ def main():
         outdeg += np.bincount(i, minlength=N_NEURONS)
         n_syn += len(i)
         del i
+    net.store(0)
+    init = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi", "lastspike")}
     setup_s = time.perf_counter() - t_setup
 
-    for _ in range(args.warmup):
+    def one_run():
+        net.restore(0)
         net.run(SIM_STEPS)
+
+    for _ in range(args.warmup):
+        one_run()
     net.sync()
     barrier(world)
-    cursor = net.spikes_fetch(P, 0, cap=1 << 26)[2]
+    cursor = net.spikes_recorded(P)
 
     # ---- device-timed region: inputs resident, CUDA events on the network's stream
     launches0 = net.kernel_launches
-    ts0 = net.timestep
     clocks = Clocks(local)
     torch.cuda.synchronize()
     barrier(world)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        net.run(SIM_STEPS)
+        one_run()
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms_total = max_over_ranks(ev0.elapsed_time(ev1), world)
     launches = net.kernel_launches - launches0
-    ts1 = net.timestep
-    idx, st, cursor = net.spikes_fetch(P, cursor, cap=1 << 27)
-    sel = (st >= ts0) & (st < ts1)
-    events = float(outdeg[idx[sel]].sum()) * world
-    nspk = int(sel.sum())
+    idx, st, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
+    nspk = len(idx)
+    ev_exc = float(outdeg[idx[idx < ne]].sum())
+    ev_inh = float(outdeg[idx[idx >= ne]].sum())
+    events = (ev_exc + ev_inh) * world
     seconds = ms_total / 1e3
     value = events / seconds
-    neuron_updates = float(N_NEURONS) * (ts1 - ts0) * world / seconds
-    rate_hz = nspk / (N_NEURONS * (ts1 - ts0) * DT)
+    neuron_updates = float(N_NEURONS) * SIM_STEPS * args.steps * world / seconds
+    rate_hz = nspk / (N_NEURONS * SIM_STEPS * args.steps * DT)
 
-    # ---- end to end through the public API: run + host readback of the step's results
-    v_host = np.empty(N_NEURONS, np.float32)
+    # ---- end to end through the public API: the seeded initial state goes host -> device
+    # from pinned memory, the run executes, and the new spikes and v come back every step
+    pinned = {}
+    for k, a in init.items():
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a).dtype, pin_memory=True)
+        t.numpy()[:] = a
+        pinned[k] = t.numpy()
+    h2d = sum(a.nbytes for a in pinned.values())
     d2h = 0
     e2e_events = 0.0
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        net.restore(0)
+        for k, a in pinned.items():
+            net.set_state(P, k, a)
         net.run(SIM_STEPS)
-        v_host[:] = net.get_state(P, "v")
-        idx, st, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
-        e2e_events += float(outdeg[idx].sum())
-        d2h += v_host.nbytes + 12 * len(idx) + 8
+        v_host = net.get_state(P, "v")
+        idx_e, st_e, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
+        e2e_events += float(outdeg[idx_e].sum())
+        d2h += v_host.nbytes + 12 * len(idx_e) + 8
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = e2e_events * world / e2e_s
 
-    # ---- per-kernel device times (profiling run: every launch timed with CUDA events)
-    prof = net.profile(200)
+    # ---- per-kernel device times (profiling run of one configured 1 s simulation, every
+    # launch timed with CUDA events on the network's stream)
+    net.restore(0)
+    prof = net.profile(SIM_STEPS)
     hbm, peak_kind = peaks()
-    kinds = {1: "neuron (HH update+threshold+compaction)", 2: "delivery on_pre"}
+    names = ["neuron (HH update+threshold+compaction)", "delivery on_pre Ce (exc)",
+             "delivery on_pre Ci (inh)"]
+    kernel_ms = {names[k] if k < len(names) else f"site{k}": round(ms, 6)
+                 for k, (kd, ms) in enumerate(prof)}
+    runs_timed = args.steps
+    per_launch_bytes = [
+        BYTES_NEURON_UPDATE * N_NEURONS,
+        (BYTES_EVENT * ev_exc + BYTES_BUNDLE * (DMAX - DMIN + 1) * float((idx < ne).sum()))
+        / (SIM_STEPS * runs_timed),
+        (BYTES_EVENT * ev_inh + BYTES_BUNDLE * (DMAX - DMIN + 1) * float((idx >= ne).sum()))
+        / (SIM_STEPS * runs_timed),
+    ]
     dom = max(range(len(prof)), key=lambda k: prof[k][1])
-    dom_kind, dom_ms = prof[dom]
-    if dom_kind == 1:
-        alg = BYTES_NEURON_UPDATE * N_NEURONS
-        traffic = _traffic("hh_step_kernel")
-    else:
-        ev_per_step = events / world / max(1, ts1 - ts0)
-        spk_per_step = nspk / max(1, ts1 - ts0)
-        alg = BYTES_EVENT * ev_per_step + BYTES_BUNDLE * spk_per_step * (DMAX - DMIN + 1) / 2
-        traffic = _traffic("deliver_add_kernel")
+    dom_ms = prof[dom][1]
+    alg = per_launch_bytes[dom] if dom < len(per_launch_bytes) else 0.0
     achieved = alg / (dom_ms * 1e-3) / 1e9
-    kernel_ms = {f"site{k}:{kinds.get(kd, kd)}": round(ms, 5) for k, (kd, ms) in enumerate(prof)}
+    traffic = _traffic(["hh_step_kernel", "deliver_add_kernel", "deliver_add_kernel"][dom])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -295,26 +320,27 @@ def main():
                    "l2": "working set > L2 (1.6 GB synapse arrays)"},
         "neuron_updates_per_s": neuron_updates,
         "firing_rate_hz": rate_hz,
+        "spikes_per_run": nspk / args.steps,
         "setup_s": setup_s,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic,
-                     "kernel": kinds.get(dom_kind, str(dom_kind)), "kernel_ms": dom_ms,
-                     "peak_source": peak_kind},
-        "kernel_ms": kernel_ms,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": names[dom],
+                     "kernel_ms": dom_ms, "peak_source": peak_kind,
+                     "bytes_per_launch": alg},
+        "kernel_ms_mean_per_launch": kernel_ms,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h // max(1, args.steps),
-                "note": "run(100 steps) + readback of v and of the new spikes each step; the "
-                        "network has no per-step external input"},
+                "note": "restore + upload of the 7 initial state arrays from pinned memory, "
+                        "run of 10,000 steps, readback of v and of the run's spikes"},
         "gpu_launches": launches,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_network(steps_budget_s=20.0, max_steps=400)
+        r = cpu_network(steps_budget_s=60.0, max_steps=SIM_STEPS)
         line["cpu_baseline"] = {
             "value": r["events"] / r["seconds"], "unit": UNIT, "cores": os.cpu_count(),
             "kind": "port",
-            "sample": f"{r['steps']} simulation steps of the full 1e5-neuron network "
-                      f"({r['seconds']:.1f} s), C++ oracle with OpenMP",
+            "sample": f"the first {r['steps']} simulation steps of the configured 1 s run of the "
+                      f"full 1e5-neuron network ({r['seconds']:.1f} s), C++ oracle, OpenMP",
             "neuron_updates_per_s": r["neuron_updates"] / r["seconds"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -325,6 +351,11 @@ def main():
 
 
 def _traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, when one exists."""
+    return _traffic_lookup(kernel)
+
+
+def _traffic_lookup(kernel: str):
     """DRAM bytes per launch from the committed ncu summary, when one exists."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:

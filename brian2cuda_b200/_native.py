@@ -90,6 +90,8 @@ PROTOTYPES = {
     "b2b_finalize": (I32, [P]),
     "b2b_run": (I32, [P, I64]),
     "b2b_sync": (I32, [P, PI32]),
+    "b2b_store": (I32, [P, I32]),
+    "b2b_restore": (I32, [P, I32]),
     "b2b_time": (I32, [P, PI64, C.POINTER(DBL)]),
     "b2b_kernel_launches": (I32, [P, PI64]),
     "b2b_profile": (I32, [P, I64, C.POINTER(DBL), PI32, I32, PI32]),

@@ -520,6 +520,21 @@ b2b_status finalize_projs(b2b_net* net) {
     b2b_status st = build_proj(net, (int)p);
     if (st != B2B_OK) return st;
   }
+  // additive projections with the same kernel variant share one delivery launch
+  for (const Proj& pr : net->projs) {
+    if (pr.effect != B2B_EFFECT_ADD) continue;
+    bool placed = false;
+    for (auto& b : net->add_batches) {
+      const Proj& q = *b[0];
+      if ((int)b.size() < kMaxProjBatch && q.dtype == pr.dtype &&
+          (q.dev.w != nullptr) == (pr.dev.w != nullptr) && q.dev.aggregate == pr.dev.aggregate) {
+        b.push_back(&pr);
+        placed = true;
+        break;
+      }
+    }
+    if (!placed) net->add_batches.push_back({&pr});
+  }
   return B2B_OK;
 }
 
@@ -530,7 +545,12 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
       CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
       ++net->launches;
     }
+    for (const auto& b : net->add_batches) {
+      CU(launch_proj_add_batch(b.data(), (int)b.size(), net->d_clock, k, net->stream));
+      ++net->launches;
+    }
     for (const Proj& pr : net->projs) {
+      if (pr.effect == B2B_EFFECT_ADD) continue;
       CU(launch_proj_pre(pr, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
       ++net->launches;
     }
@@ -559,8 +579,29 @@ b2b_status refill_rng(b2b_net* net, int kk) {
                             : curandGenerateUniformDouble(net->gen, (double*)pop.rng_buf, n);
     if (st != CURAND_STATUS_SUCCESS)
       return fail(net, B2B_ERR_CUDA, "curandGenerateUniform failed (%d)", (int)st);
+    net->rng_offset += n;
   }
   return B2B_OK;
+}
+
+// Every device array that holds dynamic state, with its size in bytes.
+std::vector<std::pair<void*, size_t>> state_arrays(b2b_net* net) {
+  std::vector<std::pair<void*, size_t>> out;
+  for (Pop& pop : net->pops) {
+    for (int v = 0; v < kMaxVars; ++v)
+      if (pop.dev.var[v]) out.emplace_back(pop.dev.var[v], var_size(pop.dtype, v) * pop.n);
+    out.emplace_back(pop.dev.ring_idx, sizeof(int32_t) * (size_t)pop.dev.ring_len * pop.n);
+    out.emplace_back(pop.dev.ring_cnt, sizeof(int32_t) * (size_t)pop.dev.ring_len);
+  }
+  for (Proj& pr : net->projs) {
+    if (pr.effect != B2B_EFFECT_STDP) continue;
+    const size_t b = real_size(pr.dtype) * pr.n_syn;
+    out.emplace_back(pr.w, b);
+    out.emplace_back(pr.dev.apre, b);
+    out.emplace_back(pr.dev.apost, b);
+    out.emplace_back(pr.dev.lastupdate, b);
+  }
+  return out;
 }
 
 b2b_status capture_graph(b2b_net* net) {
@@ -651,6 +692,8 @@ b2b_status b2b_destroy(b2b_net* net) {
     for (void* a : p.allocs) cudaFree(a);
   for (Proj& p : net->projs)
     for (void* a : p.allocs) cudaFree(a);
+  for (Snapshot& sn : net->snapshots)
+    for (void* a : sn.buffers) cudaFree(a);
   cudaFree(net->d_clock);
   cudaFree(net->d_status);
   if (net->own_stream) cudaStreamDestroy(net->stream);
@@ -950,6 +993,51 @@ b2b_status b2b_sync(b2b_net* net, int32_t* device_status) {
   int32_t s = 0;
   CU(cudaMemcpy(&s, net->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (device_status) *device_status = s;
+  return B2B_OK;
+}
+
+b2b_status b2b_store(b2b_net* net, int32_t slot) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(slot >= 0 && slot < 1024, B2B_ERR_INVALID_ARG, "bad slot %d", slot);
+  GUARD_BEGIN
+  if ((int)net->snapshots.size() <= slot) net->snapshots.resize(slot + 1);
+  Snapshot& sn = net->snapshots[slot];
+  const auto arrays = state_arrays(net);
+  if (sn.buffers.size() != arrays.size()) {
+    for (void* p : sn.buffers) cudaFree(p);
+    sn.buffers.assign(arrays.size(), nullptr);
+    for (size_t k = 0; k < arrays.size(); ++k) CU(cudaMalloc(&sn.buffers[k], arrays[k].second));
+  }
+  for (size_t k = 0; k < arrays.size(); ++k)
+    CU(cudaMemcpyAsync(sn.buffers[k], arrays[k].first, arrays[k].second,
+                       cudaMemcpyDeviceToDevice, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  sn.ts = net->ts;
+  sn.rng_offset = net->rng_offset;
+  sn.valid = true;
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_restore(b2b_net* net, int32_t slot) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(slot >= 0 && slot < (int)net->snapshots.size() && net->snapshots[slot].valid,
+        B2B_ERR_INVALID_ARG, "no checkpoint in slot %d", slot);
+  const Snapshot& sn = net->snapshots[slot];
+  const auto arrays = state_arrays(net);
+  for (size_t k = 0; k < arrays.size(); ++k)
+    CU(cudaMemcpyAsync(arrays[k].first, sn.buffers[k], arrays[k].second,
+                       cudaMemcpyDeviceToDevice, net->stream));
+  net->ts = sn.ts;
+  CU(cudaMemcpyAsync(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice,
+                     net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  if (net->gen && net->rng_offset != sn.rng_offset) {
+    if (curandSetGeneratorOffset(net->gen, sn.rng_offset) != CURAND_STATUS_SUCCESS)
+      return fail(net, B2B_ERR_CUDA, "curandSetGeneratorOffset failed");
+    net->rng_offset = sn.rng_offset;
+  }
   return B2B_OK;
 }
 

@@ -17,6 +17,7 @@ constexpr int kMaxVars = 8;          // v, ge, gi, m, h, n, lastspike, not_refra
 constexpr int kPad = 128;            // population and group offsets are padded to this
 constexpr int kBlock = 256;          // threads per CTA for the per-neuron kernels
 constexpr int kChunk = 128;          // synapses one warp takes from a bundle per work item
+constexpr int kMaxProjBatch = 8;     // additive projections delivered by one launch
 constexpr int kNumSMs = 148;         // B200
 
 enum Kind { KIND_LIF = 1, KIND_HH = 2, KIND_POISSON = 3, KIND_SPIKEGEN = 4 };
@@ -147,8 +148,19 @@ struct Proj {
 
 }  // namespace b2b
 
+namespace b2b {
+struct Snapshot {
+  bool valid = false;
+  int64_t ts = 0;
+  unsigned long long rng_offset = 0;
+  std::vector<void*> buffers;      // device copies, one per entry of the state list
+};
+}  // namespace b2b
+
 struct b2b_net {
   b2b_config cfg{};
+  std::vector<b2b::Snapshot> snapshots;
+  unsigned long long rng_offset = 0;       // uniforms drawn so far from the cuRAND stream
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   bool finalized = false;
@@ -160,6 +172,7 @@ struct b2b_net {
   std::vector<b2b::Pop> pops;
   std::vector<b2b::Syn> syns;
   std::vector<b2b::Proj> projs;
+  std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   int64_t launches = 0;
@@ -179,5 +192,8 @@ cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double 
                             int32_t* status, cudaStream_t s);
 cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double dt,
                              int32_t* status, cudaStream_t s);
+// One launch for n (<= kMaxProjBatch) additive projections of equal dtype / weight mode.
+cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
+                                  cudaStream_t s);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
 }  // namespace b2b

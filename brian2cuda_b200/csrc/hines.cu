@@ -59,16 +59,14 @@ __device__ __forceinline__ RC hh_expeuler(RC x, RC a, RC b, RC dt) {
 }
 
 // Hodgkin-Huxley 1952 rates (examples/compartmental/hh_with_spikes_cuda.py:41-46), v in
-// volts measured from rest, rates in 1/s.
+// volts measured from rest, rates in 1/s; x/(exp(x/a) - 1) forms through z_over_expm1.
 template <typename RC>
 __device__ __forceinline__ void hh_gates(RC v, RC dt, RC& m, RC& h, RC& n) {
-  const RC xm = (RC)25e-3 - v;
-  const RC am = (RC)1e5 * xm / (dexp(xm / (RC)10e-3) - (RC)1);
+  const RC am = (RC)1000 * z_over_expm1(((RC)25e-3 - v) / (RC)10e-3);
   const RC bm = (RC)4000 * dexp(-v / (RC)18e-3);
   const RC ah = (RC)70 * dexp(-v / (RC)20e-3);
   const RC bh = (RC)1000 / (dexp(((RC)30e-3 - v) / (RC)10e-3) + (RC)1);
-  const RC xn = (RC)10e-3 - v;
-  const RC an = (RC)1e4 * xn / (dexp(xn / (RC)10e-3) - (RC)1);
+  const RC an = (RC)100 * z_over_expm1(((RC)10e-3 - v) / (RC)10e-3);
   const RC bn = (RC)125 * dexp(-v / (RC)80e-3);
   m = hh_expeuler(m, am, bm, dt);
   h = hh_expeuler(h, ah, bh, dt);

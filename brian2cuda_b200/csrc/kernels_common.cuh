@@ -12,6 +12,16 @@ constexpr unsigned kFull = 0xffffffffu;
 __device__ __forceinline__ float dexp(float x) { return expf(x); }
 __device__ __forceinline__ double dexp(double x) { return exp(x); }
 __device__ __forceinline__ float dfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float dexpm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double dexpm1(double x) { return expm1(x); }
+
+// z / (exp(z) - 1), i.e. 1/exprel(z) with Brian2's exprel (brian2cuda/cuda_generator.py:858-867):
+// the removable singularity at z = 0 evaluates to its limit 1 instead of 0/0.  Rate
+// functions of the form c*x/(exp(x/a) - 1) are evaluated as c*a*z_over_expm1(x/a).
+template <typename R>
+__device__ __forceinline__ R z_over_expm1(R z) {
+  return fabs(z) < (R)1e-16 ? (R)1 : z / dexpm1(z);
+}
 __device__ __forceinline__ double dfma(double a, double b, double c) { return fma(a, b, c); }
 
 // Brian2's clip(value, a_min, a_max) (brian2cuda/cuda_generator.py:902-914).

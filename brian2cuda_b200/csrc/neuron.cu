@@ -5,8 +5,9 @@
 // neurons: `_run_kernel_<group>_stateupdater` (brian2cuda/templates/common_group.cu:108-160),
 // an eventspace reset kernel (templates/threshold.cu:50-75), the thresholder that appends
 // spikes with one global atomicAdd per spike (threshold.cu:19-45), and the resetter over
-// the spiking indices (templates/reset.cu:3-27).  Here one thread owns four consecutive
-// neurons and loads each state array with one 128-bit access (two for float64); the CTA
+// the spiking indices (templates/reset.cu:3-27).  Here a thread owns E consecutive neurons:
+// E = 4 for large populations (each state array read with one 128-bit access, two for
+// float64), E = 1 when the population is too small to fill the GPU that way.  The CTA
 // compacts its spikes with warp shuffles and a shared-memory scan and reserves its output
 // range with a single atomicAdd on the step's slot of the spike-history ring.
 //
@@ -25,15 +26,18 @@ __device__ __forceinline__ int64_t timestep_of(double t, double dt) {
   return (int64_t)((t + 1e-3 * dt) / dt);
 }
 
-template <typename R>
-struct Quad {
-  R x[4];
+template <typename R, int E>
+struct Pack {
+  R x[E];
 };
 
-template <typename R>
-__device__ __forceinline__ Quad<R> load4(const void* base, int64_t q) {
-  Quad<R> r;
-  if constexpr (sizeof(R) == 4) {
+// Loads/stores the E values of thread q from one state array (vectorised for E = 4).
+template <typename R, int E>
+__device__ __forceinline__ Pack<R, E> load_pack(const void* base, int64_t q) {
+  Pack<R, E> r;
+  if constexpr (E == 1) {
+    r.x[0] = static_cast<const R*>(base)[q];
+  } else if constexpr (sizeof(R) == 4) {
     float4 a = reinterpret_cast<const float4*>(base)[q];
     r.x[0] = a.x; r.x[1] = a.y; r.x[2] = a.z; r.x[3] = a.w;
   } else {
@@ -44,9 +48,11 @@ __device__ __forceinline__ Quad<R> load4(const void* base, int64_t q) {
   return r;
 }
 
-template <typename R>
-__device__ __forceinline__ void store4(void* base, int64_t q, const Quad<R>& r) {
-  if constexpr (sizeof(R) == 4) {
+template <typename R, int E>
+__device__ __forceinline__ void store_pack(void* base, int64_t q, const Pack<R, E>& r) {
+  if constexpr (E == 1) {
+    static_cast<R*>(base)[q] = r.x[0];
+  } else if constexpr (sizeof(R) == 4) {
     reinterpret_cast<float4*>(base)[q] = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
   } else {
     double2* p = reinterpret_cast<double2*>(base) + 2 * q;
@@ -55,8 +61,22 @@ __device__ __forceinline__ void store4(void* base, int64_t q, const Quad<R>& r) 
   }
 }
 
-// Writes the spikes flagged in `fl` (bit e = neuron 4q+e) into the ring slot and the spike
+template <int E>
+__device__ __forceinline__ void store_flags(void* base, int64_t q, uint32_t packed) {
+  if constexpr (E == 1) static_cast<uint8_t*>(base)[q] = (uint8_t)packed;
+  else reinterpret_cast<uint32_t*>(base)[q] = packed;
+}
+
+// Group-parameter index of thread q (the table holds one entry per 4 neurons).
+template <int E>
+__device__ __forceinline__ int group_of(const PopDev& P, int64_t q) {
+  if (!P.vec_group) return 0;
+  return P.vec_group[E == 4 ? q : (q >> 2)];
+}
+
+// Writes the spikes flagged in `fl` (bit e = neuron E*q+e) into the ring slot and the spike
 // monitor.  Every thread of the CTA must call this (it synchronises the block).
+template <int E>
 __device__ __forceinline__ void emit_spikes(const PopDev& P, int64_t q, unsigned fl,
                                             int64_t ts, int slot, int32_t* status) {
   __shared__ int s_warp[33];
@@ -75,9 +95,9 @@ __device__ __forceinline__ void emit_spikes(const PopDev& P, int64_t q, unsigned
   int pos = s_base + excl;
   unsigned long long mpos = P.mon_cnt ? s_mbase + excl : 0;
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
+  for (int e = 0; e < E; ++e) {
     if (fl & (1u << e)) {
-      const int32_t idx = (int32_t)(4 * q + e);
+      const int32_t idx = (int32_t)(E * q + e);
       out[pos++] = idx;
       if (P.mon_cnt) {
         if (mpos < (unsigned long long)P.mon_cap) {
@@ -97,30 +117,30 @@ __device__ __forceinline__ void clear_next_slot(const PopDev& P, int64_t ts) {
 }
 
 // ---- LIF, exact integration ------------------------------------------------------------
-template <typename R>
+template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
 lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                 int32_t* status) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
   const int slot = ring_slot(ts, P.ring_len);
-  const int64_t nvec = P.n >> 2;
+  const int64_t nthr = P.n / E;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned fl = 0;
-  if (q < nvec) {
+  if (q < nthr) {
     const LifDev* prm = static_cast<const LifDev*>(P.params);
-    const LifDev g = prm[P.vec_group ? P.vec_group[q] : 0];
+    const LifDev g = prm[group_of<E>(P, q)];
     const R A = (R)g.A, Be = (R)g.Be, Bi = (R)g.Bi, De = (R)g.De, Di = (R)g.Di;
     const R El = (R)g.El, Vt = (R)g.Vt, Vr = (R)g.Vr;
     const bool refr = g.ref_steps >= 0;
-    Quad<R> V = load4<R>(P.var[B2B_VAR_V], q);
-    Quad<R> GE = load4<R>(P.var[B2B_VAR_GE], q);
-    Quad<R> GI = load4<R>(P.var[B2B_VAR_GI], q);
-    Quad<R> LS;
-    if (refr) LS = load4<R>(P.var[B2B_VAR_LASTSPIKE], q);
+    Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
+    Pack<R, E> GE = load_pack<R, E>(P.var[B2B_VAR_GE], q);
+    Pack<R, E> GI = load_pack<R, E>(P.var[B2B_VAR_GI], q);
+    Pack<R, E> LS;
+    if (refr) LS = load_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q);
     uint32_t NRout = 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < E; ++e) {
       const R v = V.x[e], ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
@@ -128,7 +148,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       if (g.unless_refractory && !nr) vn = v;
       GE.x[e] = De * ge;
       GI.x[e] = Di * gi;
-      const bool valid = (4 * q + e - g.offset) < g.n;
+      const bool valid = (E * q + e - g.offset) < g.n;
       if (g.has_threshold && valid && vn > Vt && nr) {
         nr = false;
         if (refr) LS.x[e] = (R)t;
@@ -138,67 +158,66 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       V.x[e] = vn;
       NRout |= (nr ? 1u : 0u) << (8 * e);
     }
-    store4<R>(P.var[B2B_VAR_V], q, V);
-    store4<R>(P.var[B2B_VAR_GE], q, GE);
-    store4<R>(P.var[B2B_VAR_GI], q, GI);
+    store_pack<R, E>(P.var[B2B_VAR_V], q, V);
+    store_pack<R, E>(P.var[B2B_VAR_GE], q, GE);
+    store_pack<R, E>(P.var[B2B_VAR_GI], q, GI);
     if (refr) {
-      store4<R>(P.var[B2B_VAR_LASTSPIKE], q, LS);
-      reinterpret_cast<uint32_t*>(P.var[B2B_VAR_NOT_REFRACTORY])[q] = NRout;
+      store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);
+      store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
   }
-  emit_spikes(P, q, fl, ts, slot, status);
+  emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
 }
 
 // ---- Hodgkin-Huxley (COBAHH), exponential Euler ----------------------------------------
-// Rate functions of examples/cobahh.py:169-180 in SI units; every right-hand side is
-// evaluated with the values at the start of the step, and each variable x with
-// dx/dt = A x + B advances as x' = -B/A + (x + B/A) exp(A dt).
+// Rate functions of examples/cobahh.py:169-180 in SI units (the three of the form
+// x/(exp(x/a) - 1) through z/expm1(z), see z_over_expm1); every right-hand side is evaluated
+// with the values at the start of the step, and each variable x with dx/dt = A x + B
+// advances as x' = -B/A + (x + B/A) exp(A dt).
 template <typename R>
 __device__ __forceinline__ R expeuler(R x, R A, R B, R dt) {
   const R BA = B / A;
   return -BA + (BA + x) * dexp(A * dt);
 }
 
-template <typename R>
+template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
 hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                int32_t* status) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
   const int slot = ring_slot(ts, P.ring_len);
-  const int64_t nvec = P.n >> 2;
+  const int64_t nthr = P.n / E;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned fl = 0;
-  if (q < nvec) {
+  if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
-    const HhDev g = prm[P.vec_group ? P.vec_group[q] : 0];
+    const HhDev g = prm[group_of<E>(P, q)];
     const R Cm = (R)g.Cm, gl = (R)g.gl, El = (R)g.El, EK = (R)g.EK, ENa = (R)g.ENa;
     const R gNa = (R)g.gNa, gK = (R)g.gK, VT = (R)g.VT, Ee = (R)g.Ee, Ei = (R)g.Ei;
     const R De = (R)g.De, Di = (R)g.Di, Vthr = (R)g.Vthr, dtR = (R)dt;
     const bool refr = g.ref_steps >= 0;
-    Quad<R> V = load4<R>(P.var[B2B_VAR_V], q);
-    Quad<R> M = load4<R>(P.var[B2B_VAR_M], q);
-    Quad<R> H = load4<R>(P.var[B2B_VAR_H], q);
-    Quad<R> N = load4<R>(P.var[B2B_VAR_N], q);
-    Quad<R> GE = load4<R>(P.var[B2B_VAR_GE], q);
-    Quad<R> GI = load4<R>(P.var[B2B_VAR_GI], q);
-    Quad<R> LS;
-    if (refr) LS = load4<R>(P.var[B2B_VAR_LASTSPIKE], q);
+    Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
+    Pack<R, E> M = load_pack<R, E>(P.var[B2B_VAR_M], q);
+    Pack<R, E> H = load_pack<R, E>(P.var[B2B_VAR_H], q);
+    Pack<R, E> N = load_pack<R, E>(P.var[B2B_VAR_N], q);
+    Pack<R, E> GE = load_pack<R, E>(P.var[B2B_VAR_GE], q);
+    Pack<R, E> GI = load_pack<R, E>(P.var[B2B_VAR_GI], q);
+    Pack<R, E> LS;
+    if (refr) LS = load_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q);
     uint32_t NRout = 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < E; ++e) {
       const R v = V.x[e], m = M.x[e], h = H.x[e], n = N.x[e], ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
-      const R xm = (R)13e-3 - v + VT;
-      const R am = (R)0.32e6 * xm / (dexp(xm / (R)4e-3) - (R)1);
-      const R ym = v - VT - (R)40e-3;
-      const R bm = (R)0.28e6 * ym / (dexp(ym / (R)5e-3) - (R)1);
+      // 0.32/mV*(13mV-v+VT)/(exp((13mV-v+VT)/4mV)-1)/ms = 1280 * z/expm1(z), z = (..)/4mV
+      const R am = (R)1280 * z_over_expm1(((R)13e-3 - v + VT) / (R)4e-3);
+      const R bm = (R)1400 * z_over_expm1((v - VT - (R)40e-3) / (R)5e-3);
       const R ah = (R)128 * dexp(((R)17e-3 - v + VT) / (R)18e-3);
       const R bh = (R)4000 / ((R)1 + dexp(((R)40e-3 - v + VT) / (R)5e-3));
-      const R xn = (R)15e-3 - v + VT;
-      const R an = (R)0.032e6 * xn / (dexp(xn / (R)5e-3) - (R)1);
+      const R an = (R)160 * z_over_expm1(((R)15e-3 - v + VT) / (R)5e-3);
       const R bn = (R)500 * dexp(((R)10e-3 - v + VT) / (R)40e-3);
       const R gna = gNa * (m * m * m) * h;
       const R gk = gK * (n * n * n * n);
@@ -210,7 +229,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       N.x[e] = expeuler(n, -(an + bn), an, dtR);
       GE.x[e] = De * ge;
       GI.x[e] = Di * gi;
-      const bool valid = (4 * q + e - g.offset) < g.n;
+      const bool valid = (E * q + e - g.offset) < g.n;
       if (valid && vn > Vthr && nr) {
         nr = false;
         if (refr) LS.x[e] = (R)t;
@@ -219,43 +238,43 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       V.x[e] = vn;
       NRout |= (nr ? 1u : 0u) << (8 * e);
     }
-    store4<R>(P.var[B2B_VAR_V], q, V);
-    store4<R>(P.var[B2B_VAR_M], q, M);
-    store4<R>(P.var[B2B_VAR_H], q, H);
-    store4<R>(P.var[B2B_VAR_N], q, N);
-    store4<R>(P.var[B2B_VAR_GE], q, GE);
-    store4<R>(P.var[B2B_VAR_GI], q, GI);
+    store_pack<R, E>(P.var[B2B_VAR_V], q, V);
+    store_pack<R, E>(P.var[B2B_VAR_M], q, M);
+    store_pack<R, E>(P.var[B2B_VAR_H], q, H);
+    store_pack<R, E>(P.var[B2B_VAR_N], q, N);
+    store_pack<R, E>(P.var[B2B_VAR_GE], q, GE);
+    store_pack<R, E>(P.var[B2B_VAR_GI], q, GI);
     if (refr) {
-      store4<R>(P.var[B2B_VAR_LASTSPIKE], q, LS);
-      reinterpret_cast<uint32_t*>(P.var[B2B_VAR_NOT_REFRACTORY])[q] = NRout;
+      store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);
+      store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
   }
-  emit_spikes(P, q, fl, ts, slot, status);
+  emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
 }
 
 // ---- PoissonGroup: spike when u < rate*dt, u read in place from the bulk buffer ---------
-template <typename R>
+template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
 poisson_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, int32_t* status) {
   const int64_t ts = clock[0] + k;
   const int slot = ring_slot(ts, P.ring_len);
-  const int64_t nvec = P.n >> 2;
+  const int64_t nthr = P.n / E;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned fl = 0;
-  if (q < nvec) {
+  if (q < nthr) {
     const PoissonDev* prm = static_cast<const PoissonDev*>(P.params);
-    const PoissonDev g = prm[P.vec_group ? P.vec_group[q] : 0];
+    const PoissonDev g = prm[group_of<E>(P, q)];
     const R thr = (R)g.p_spike;
     const R* row = static_cast<const R*>(P.rng) + (int64_t)k * P.n;
-    Quad<R> U = load4<R>(row, q);
+    Pack<R, E> U = load_pack<R, E>(row, q);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const bool valid = (4 * q + e - g.offset) < g.n;
+    for (int e = 0; e < E; ++e) {
+      const bool valid = (E * q + e - g.offset) < g.n;
       if (valid && U.x[e] < thr) fl |= 1u << e;
     }
   }
-  emit_spikes(P, q, fl, ts, slot, status);
+  emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
 }
 
@@ -317,33 +336,44 @@ __global__ void lif_late_reset_kernel(PopDev P, const int64_t* __restrict__ cloc
   }
 }
 
-}  // namespace
+// Four neurons per thread once that still gives every SM several CTAs' worth of warps.
+bool wide(int64_t n) { return n / 4 >= (int64_t)kNumSMs * 4 * kBlock; }
 
-cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
-                            int32_t* status, cudaStream_t s) {
+template <int E>
+cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int32_t* status,
+                     cudaStream_t s) {
   const PopDev& P = pop.dev;
-  const int64_t nvec = P.n >> 2;
-  const unsigned grid = (unsigned)((nvec + kBlock - 1) / kBlock);
+  const unsigned grid = (unsigned)((P.n / E + kBlock - 1) / kBlock);
+  const bool f32 = pop.dtype == B2B_F32;
   switch (pop.kind) {
     case KIND_LIF:
-      if (pop.dtype == B2B_F32) lif_step_kernel<float><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
-      else lif_step_kernel<double><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      if (f32) lif_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      else lif_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
       break;
     case KIND_HH:
-      if (pop.dtype == B2B_F32) hh_step_kernel<float><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
-      else hh_step_kernel<double><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      if (f32) hh_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      else hh_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
       break;
     case KIND_POISSON:
-      if (pop.dtype == B2B_F32) poisson_step_kernel<float><<<grid, kBlock, 0, s>>>(P, clock, k, status);
-      else poisson_step_kernel<double><<<grid, kBlock, 0, s>>>(P, clock, k, status);
-      break;
-    case KIND_SPIKEGEN:
-      spikegen_step_kernel<<<1, kBlock, 0, s>>>(P, clock, k, status);
+      if (f32) poisson_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, status);
+      else poisson_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, status);
       break;
     default:
       return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
+                            int32_t* status, cudaStream_t s) {
+  if (pop.kind == KIND_SPIKEGEN) {
+    spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
+    return cudaGetLastError();
+  }
+  return wide(pop.dev.n) ? launch_e<4>(pop, clock, k, dt, status, s)
+                         : launch_e<1>(pop, clock, k, dt, status, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -15,6 +15,8 @@
 // (pre, d) in the (pre, delay)-sorted synapse arrays.  This is the same set of bundles the
 // reference's queue holds in slot `current_offset` after its push, without the push kernel,
 // the host sync on the spike count, the locks or the device heap.
+#include <algorithm>
+
 #include "kernels_common.cuh"
 
 namespace b2b {
@@ -114,6 +116,37 @@ template <typename R, bool HAS_W, bool AGG>
 __global__ void __launch_bounds__(kDeliverBlock)
 deliver_add_kernel(ProjDev P, const int64_t* __restrict__ clock, int k) {
   extern __shared__ int s_pref[];
+  const int64_t ts = clock[0] + k;
+  const R* __restrict__ W = static_cast<const R*>(P.w);
+  const R ws = (R)P.w_scalar;
+  R* __restrict__ T = static_cast<R*>(P.target);
+  const int lane = threadIdx.x & 31;
+  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
+    const int32_t post = valid ? __ldg(P.post + s) : -1;
+    R w = ws;
+    if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
+    if constexpr (AGG) {
+      const unsigned peers = __match_any_sync(kFull, post);
+      const R sum = peer_sum<R>(peers, w);
+      if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
+    } else {
+      if (valid) atomic_add(T + post, w);
+    }
+  });
+}
+
+// Several additive projections in one launch: blockIdx.y picks the projection.
+struct ProjBatch {
+  ProjDev p[kMaxProjBatch];
+  int n;
+};
+
+template <typename R, bool HAS_W, bool AGG>
+__global__ void __launch_bounds__(kDeliverBlock)
+deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __restrict__ clock,
+                         int k) {
+  extern __shared__ int s_pref[];
+  const ProjDev& P = B.p[blockIdx.y];
   const int64_t ts = clock[0] + k;
   const R* __restrict__ W = static_cast<const R*>(P.w);
   const R ws = (R)P.w_scalar;
@@ -260,6 +293,36 @@ cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double 
   } else {
     return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
+                                  cudaStream_t s) {
+  if (n <= 0 || n > kMaxProjBatch) return cudaErrorInvalidValue;
+  ProjBatch B{};
+  B.n = n;
+  unsigned grid = 1;
+  int nd = 1;
+  for (int i = 0; i < n; ++i) {
+    B.p[i] = prs[i]->dev;
+    grid = std::max(grid, deliver_grid(*prs[i]));
+    nd = std::max(nd, (int)prs[i]->dev.nd);
+  }
+  const size_t smem = sizeof(int) * (size_t)(nd + 1);
+  const bool f32 = prs[0]->dtype == B2B_F32;
+  const bool hw = prs[0]->dev.w != nullptr;
+  const bool ag = prs[0]->dev.aggregate != 0;
+  const dim3 g(grid, (unsigned)n);
+#define B2B_ADDB(R, HW, AG) \
+  deliver_add_batch_kernel<R, HW, AG><<<g, kDeliverBlock, smem, s>>>(B, clock, k)
+  if (f32) {
+    if (hw) { if (ag) B2B_ADDB(float, true, true); else B2B_ADDB(float, true, false); }
+    else { if (ag) B2B_ADDB(float, false, true); else B2B_ADDB(float, false, false); }
+  } else {
+    if (hw) { if (ag) B2B_ADDB(double, true, true); else B2B_ADDB(double, true, false); }
+    else { if (ag) B2B_ADDB(double, false, true); else B2B_ADDB(double, false, false); }
+  }
+#undef B2B_ADDB
   return cudaGetLastError();
 }
 

@@ -306,6 +306,14 @@ class Network:
         self._check(self._lib.b2b_sync(self._h, C.byref(s)), "sync")
         return s.value
 
+    def store(self, slot: int = 0):
+        """Device-side checkpoint of the dynamic state (Brian2's Network.store)."""
+        self._check(self._lib.b2b_store(self._h, int(slot)), "store")
+
+    def restore(self, slot: int = 0):
+        """Restores a checkpoint taken with store() (Brian2's Network.restore)."""
+        self._check(self._lib.b2b_restore(self._h, int(slot)), "restore")
+
     @property
     def timestep(self) -> int:
         ts = C.c_int64()
@@ -351,6 +359,13 @@ class Network:
                     "spikemon_fetch")
         nxt = min(total.value, int(start) + cap)
         return idx[: n.value], stp[: n.value], nxt
+
+    def spikes_recorded(self, gid: int) -> int:
+        """Number of entries the monitor of gid's population has recorded so far."""
+        total, n = C.c_int64(), C.c_int64()
+        self._check(self._lib.b2b_spikemon_fetch(self._h, gid, 0, C.byref(total), C.byref(n),
+                                                 None, None, 0), "spikemon_fetch")
+        return total.value
 
     def spikes_last(self, gid: int) -> np.ndarray:
         n = C.c_int64()

@@ -190,6 +190,13 @@ b2b_status b2b_run(b2b_net* net, int64_t n_steps);
 /* Waits for the net's stream; *device_status receives the device status word
  * (B2B_OK, B2B_ERR_QUEUE_OVERFLOW, B2B_ERR_INDEX, ...). */
 b2b_status b2b_sync(b2b_net* net, int32_t* device_status);
+/* Device-side checkpoint of the net's dynamic state in `slot` (>= 0): state variables and
+ * spike-history rings of every population, synaptic variables of STDP projections, the
+ * clock and the cuRAND offset (spike monitors keep recording).  b2b_restore copies the
+ * checkpoint back.  Brian2's Network.store()/restore(); the reference's device raises
+ * NotImplementedError for both (brian2cuda/device.py:1783-1789). */
+b2b_status b2b_store(b2b_net* net, int32_t slot);
+b2b_status b2b_restore(b2b_net* net, int32_t slot);
 /* Current time step (the next step to simulate) and time in seconds. */
 b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */

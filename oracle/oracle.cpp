@@ -24,7 +24,9 @@
 //     threshold `cond and not_refractory`; on a spike not_refractory = false and
 //     lastspike = t (threshold.cu:37-42).  lastspike starts at -1e4 s.
 //   * Integrators: the exact propagator of the linear LIF (examples/cuba.py:125-132) and
-//     Brian2's exponential Euler for COBAHH (examples/cobahh.py:159-180).
+//     Brian2's exponential Euler for COBAHH (examples/cobahh.py:159-180); rate functions of
+//     the form c*x/(exp(x/a) - 1) through Brian2's exprel (z_over_expm1 below), which keeps
+//     their removable singularity finite (the literal form is 0/0 there).
 //   * Event-driven STDP (examples/stdp.py:125-186) with float32 elapsed time in float32
 //     mode (brian2cuda/device.py:1034-1039); clip as cuda_generator.py:902-914.
 //   * Hines solver: brian2cuda/templates/spatialstateupdate.cu:36-77 (matrix), 128-192
@@ -54,6 +56,15 @@ int64_t timestep(double t, double dt) { return (int64_t)((t + 1e-3 * dt) / dt); 
 inline float xexp(float x) { return std::exp(x); }
 inline double xexp(double x) { return std::exp(x); }
 inline float xfma(float a, float b, float c) { return std::fma(a, b, c); }
+inline float xexpm1(float x) { return std::expm1(x); }
+inline double xexpm1(double x) { return std::expm1(x); }
+// x/(exp(x) - 1) = 1/exprel(x), Brian2's exprel (brian2cuda/cuda_generator.py:858-867): the
+// removable singularity at 0 takes its limit.  The COBAHH and HH-1952 rate functions written
+// as c*x/(exp(x/a) - 1) are evaluated as c*a*z_over_expm1(x/a).
+template <typename R>
+R z_over_expm1(R z) {
+  return std::fabs(z) < (R)1e-16 ? (R)1 : z / xexpm1(z);
+}
 inline double xfma(double a, double b, double c) { return std::fma(a, b, c); }
 
 template <typename R>
@@ -217,14 +228,11 @@ void update_hh(Group<R>& g, double t, double dt) {
     const R v = g.var[V][i], m = g.var[M][i], h = g.var[H][i], n = g.var[N][i];
     const R ge = g.var[GE][i], gi = g.var[GI][i];
     // examples/cobahh.py:169-180 in SI units
-    const R xm = (R)13e-3 - v + VT;
-    const R am = (R)0.32e6 * xm / (xexp(xm / (R)4e-3) - (R)1);
-    const R ym = v - VT - (R)40e-3;
-    const R bm = (R)0.28e6 * ym / (xexp(ym / (R)5e-3) - (R)1);
+    const R am = (R)1280 * z_over_expm1(((R)13e-3 - v + VT) / (R)4e-3);
+    const R bm = (R)1400 * z_over_expm1((v - VT - (R)40e-3) / (R)5e-3);
     const R ah = (R)128 * xexp(((R)17e-3 - v + VT) / (R)18e-3);
     const R bh = (R)4000 / ((R)1 + xexp(((R)40e-3 - v + VT) / (R)5e-3));
-    const R xn = (R)15e-3 - v + VT;
-    const R an = (R)0.032e6 * xn / (xexp(xn / (R)5e-3) - (R)1);
+    const R an = (R)160 * z_over_expm1(((R)15e-3 - v + VT) / (R)5e-3);
     const R bn = (R)500 * xexp(((R)10e-3 - v + VT) / (R)40e-3);
     const R gna = gNa * (m * m * m) * h;
     const R gk = gK * (n * n * n * n);
@@ -456,13 +464,11 @@ void hines_step(Hines<RC>& H, bool write_currents) {
       if (j == 0) I0[j] += H.soma_I[b];
       vprev[j] = v[j];
       const RC vr = (RC)v[j], dtR = (RC)H.dt;
-      const RC xm = (RC)25e-3 - vr;
-      const RC am = (RC)1e5 * xm / (xexp(xm / (RC)10e-3) - (RC)1);
+      const RC am = (RC)1000 * z_over_expm1(((RC)25e-3 - vr) / (RC)10e-3);
       const RC bm = (RC)4000 * xexp(-vr / (RC)18e-3);
       const RC ah = (RC)70 * xexp(-vr / (RC)20e-3);
       const RC bh = (RC)1000 / (xexp(((RC)30e-3 - vr) / (RC)10e-3) + (RC)1);
-      const RC xn = (RC)10e-3 - vr;
-      const RC an = (RC)1e4 * xn / (xexp(xn / (RC)10e-3) - (RC)1);
+      const RC an = (RC)100 * z_over_expm1(((RC)10e-3 - vr) / (RC)10e-3);
       const RC bn = (RC)125 * xexp(-vr / (RC)80e-3);
       H.m[c0 + j] = hh_ee(H.m[c0 + j], am, bm, dtR);
       H.h[c0 + j] = hh_ee(H.h[c0 + j], ah, bh, dtR);

@@ -251,3 +251,27 @@ def test_graph_and_eager_agree(gpu_factory):
         assert net.kernel_launches > 0
     np.testing.assert_array_equal(res[0][0], res[1][0])
     np.testing.assert_array_equal(res[0][1], res[1][1])
+
+
+def test_store_restore_replays_identically(gpu_factory):
+    net = gpu_factory(DT, steps_per_graph=20)
+    G, Ce, Ci, _ = _delay_net(net, n=600)
+    net.finalize()
+    net.run(37)
+    net.store(0)
+    q0 = net.queue(Ce)
+    n0 = net.spikes_recorded(G)
+    net.run(160)
+    idx1, st1, _ = net.spikes_fetch(G, n0)
+    v1 = net.get_state(G, "v")
+    net.restore(0)
+    assert net.timestep == 37
+    np.testing.assert_array_equal(net.queue(Ce), q0)
+    n1 = net.spikes_recorded(G)
+    net.run(160)
+    idx2, st2, _ = net.spikes_fetch(G, n1)
+    order1, order2 = np.lexsort((idx1, st1)), np.lexsort((idx2, st2))
+    np.testing.assert_array_equal(st1[order1], st2[order2])
+    np.testing.assert_array_equal(idx1[order1], idx2[order2])
+    _close(net.get_state(G, "v"), v1, 1e-12, 1e-15)
+    assert len(idx1) > 50
