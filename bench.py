@@ -293,23 +293,41 @@ def main():
     net.restore(0)
     prof = net.profile(SIM_STEPS)
     hbm, peak_kind = peaks()
-    names = ["neuron (HH update+threshold+compaction)", "delivery on_pre Ce (exc)",
-             "delivery on_pre Ci (inh)"]
-    kernel_ms = {names[k] if k < len(names) else f"site{k}": round(ms, 6)
-                 for k, (kd, ms) in enumerate(prof)}
     runs_timed = args.steps
-    per_launch_bytes = [
-        BYTES_NEURON_UPDATE * N_NEURONS,
-        (BYTES_EVENT * ev_exc + BYTES_BUNDLE * (DMAX - DMIN + 1) * float((idx < ne).sum()))
-        / (SIM_STEPS * runs_timed),
-        (BYTES_EVENT * ev_inh + BYTES_BUNDLE * (DMAX - DMIN + 1) * float((idx >= ne).sum()))
-        / (SIM_STEPS * runs_timed),
-    ]
+    n_exc_spk = float((idx < ne).sum())
+    n_inh_spk = float((idx >= ne).sum())
+    nd = DMAX - DMIN + 1
+    launches_timed = SIM_STEPS * runs_timed
+    deliver_exc = (BYTES_EVENT * ev_exc + BYTES_BUNDLE * nd * n_exc_spk) / launches_timed
+    deliver_inh = (BYTES_EVENT * ev_inh + BYTES_BUNDLE * nd * n_inh_spk) / launches_timed
+    neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
+    # algorithmic bytes per launch of each launch site the profiler reports
+    site_info = {1: ("neuron (HH update+threshold+compaction)", "hh_step_kernel"),
+                 2: ("delivery on_pre", "deliver_add_kernel"),
+                 5: ("fused step (HH update + delivery, one kernel)", "fused_step_kernel")}
+    kernel_ms, per_launch_bytes, kernels = {}, [], []
+    n_deliver = 0
+    for k, (kd, ms) in enumerate(prof):
+        label, kname = site_info.get(kd, (f"site kind {kd}", None))
+        if kd == 1:
+            b = neuron_bytes
+        elif kd == 2:
+            b = deliver_exc if n_deliver == 0 else deliver_inh
+            label += " Ce (exc)" if n_deliver == 0 else " Ci (inh)"
+            n_deliver += 1
+        elif kd == 5:
+            b = neuron_bytes + deliver_exc + deliver_inh
+        else:
+            b = 0.0
+        kernel_ms[label] = round(ms, 6)
+        per_launch_bytes.append(b)
+        kernels.append((label, kname))
     dom = max(range(len(prof)), key=lambda k: prof[k][1])
     dom_ms = prof[dom][1]
-    alg = per_launch_bytes[dom] if dom < len(per_launch_bytes) else 0.0
+    alg = per_launch_bytes[dom]
     achieved = alg / (dom_ms * 1e-3) / 1e9
-    traffic = _traffic(["hh_step_kernel", "deliver_add_kernel", "deliver_add_kernel"][dom])
+    traffic = _traffic(kernels[dom][1]) if kernels[dom][1] else None
+    names = [lab for lab, _ in kernels]
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -322,6 +340,7 @@ def main():
         "firing_rate_hz": rate_hz,
         "spikes_per_run": nspk / args.steps,
         "setup_s": setup_s,
+        "run_mode": net.run_mode,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": names[dom],
                      "kernel_ms": dom_ms, "peak_source": peak_kind,

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     8: "B2B_ERR_INDEX",
 }
 F32, F64 = 1, 2
-NET_NO_GRAPH, NET_CHECKED, NET_RESET_BEFORE_SYNAPSES = 1, 2, 4
+NET_NO_GRAPH, NET_CHECKED, NET_RESET_BEFORE_SYNAPSES, NET_NO_FUSED = 1, 2, 4, 8
 EFFECT_ADD, EFFECT_STDP = 1, 2
 VARS = {"v": 0, "ge": 1, "gi": 2, "m": 3, "h": 4, "n": 5, "lastspike": 6,
         "not_refractory": 7}
@@ -94,6 +94,7 @@ PROTOTYPES = {
     "b2b_restore": (I32, [P, I32]),
     "b2b_time": (I32, [P, PI64, C.POINTER(DBL)]),
     "b2b_kernel_launches": (I32, [P, PI64]),
+    "b2b_run_mode": (I32, [P, PI32]),
     "b2b_profile": (I32, [P, I64, C.POINTER(DBL), PI32, I32, PI32]),
     "b2b_spikemon": (I32, [P, I32, I64]),
     "b2b_spikemon_get": (I32, [P, I32, PI64, P, P, I64]),

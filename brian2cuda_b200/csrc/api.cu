@@ -7,6 +7,7 @@
 // synchronisation inside a run.
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -538,8 +539,61 @@ b2b_status finalize_projs(b2b_net* net) {
   return B2B_OK;
 }
 
+// One kernel per step (fused.cu) applies when the net is one LIF/HH population whose
+// synapses are all additive onto ge/gi of that population with delays of at least one step.
+b2b_status setup_fused(b2b_net* net) {
+  if (net->cfg.flags & B2B_NET_NO_FUSED) return B2B_OK;
+  if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
+    return B2B_OK;
+  const Pop& pop = net->pops[0];
+  if (pop.kind != KIND_LIF && pop.kind != KIND_HH) return B2B_OK;
+  int32_t nd_max = 1;
+  for (const Proj& pr : net->projs) {
+    if (pr.effect != B2B_EFFECT_ADD || pr.dmin < 1) return B2B_OK;
+    if (pr.target_var != B2B_VAR_GE && pr.target_var != B2B_VAR_GI) return B2B_OK;
+    nd_max = std::max(nd_max, pr.dev.nd);
+  }
+  FusedDev& F = net->fdev;
+  F = FusedDev{};
+  F.pop = pop.dev;
+  F.n_proj = (int32_t)net->projs.size();
+  F.nd_max = nd_max;
+  const size_t rs = real_size(pop.dtype);
+  for (size_t p = 0; p < net->projs.size(); ++p) {
+    const int v = net->projs[p].target_var;
+    if (!F.acc[v]) {
+      CU(cudaMalloc(&F.acc[v], 2 * rs * pop.n));
+      net->fused_allocs.push_back(F.acc[v]);
+      CU(cudaMemset(F.acc[v], 0, 2 * rs * pop.n));
+    }
+    F.proj[p] = net->projs[p].dev;
+    F.proj[p].target = F.acc[v];
+  }
+  const int block = fused_block();
+  F.neuron_ctas = (int32_t)((pop.n + block - 1) / block);
+  int sms = kNumSMs;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+  int deliver = std::max(8, std::min(2 * sms, (int)(pop.n / 1024)));
+  if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) deliver = std::max(1, std::atoi(env));
+  net->fused_grid = F.neuron_ctas + deliver;
+  net->fused = true;
+  return B2B_OK;
+}
+
 // ---------------------------------------------------------------------------------------
 b2b_status enqueue_steps(b2b_net* net, int kk) {
+  if (net->fused) {
+    const Pop& pop = net->pops[0];
+    for (int k = 0; k < kk; ++k) {
+      CU(launch_fused_step(net->fdev, pop.kind, pop.dtype, net->fused_grid, net->d_clock, k,
+                           net->cfg.dt, net->d_status, net->stream));
+      ++net->launches;
+    }
+    CU(launch_fused_fold(net->fdev, pop.dtype, net->d_clock, kk - 1, net->stream));
+    CU(launch_tick(net->d_clock, kk, net->stream));
+    net->launches += 2;
+    return B2B_OK;
+  }
   for (int k = 0; k < kk; ++k) {
     for (const Pop& pop : net->pops) {
       CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
@@ -694,6 +748,7 @@ b2b_status b2b_destroy(b2b_net* net) {
     for (void* a : p.allocs) cudaFree(a);
   for (Snapshot& sn : net->snapshots)
     for (void* a : sn.buffers) cudaFree(a);
+  for (void* a : net->fused_allocs) cudaFree(a);
   cudaFree(net->d_clock);
   cudaFree(net->d_status);
   if (net->own_stream) cudaStreamDestroy(net->stream);
@@ -896,6 +951,7 @@ b2b_status b2b_finalize(b2b_net* net) {
   GUARD_BEGIN
   b2b_status st = finalize_pops(net);
   if (st == B2B_OK) st = finalize_projs(net);
+  if (st == B2B_OK) st = setup_fused(net);
   if (st != B2B_OK) return st;
   CU(cudaMemcpy(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice));
   CU(cudaDeviceSynchronize());
@@ -937,12 +993,16 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   GUARD_BEGIN
   struct Site { int kind; int idx; };
   std::vector<Site> sites;
-  for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
-  for (size_t p = 0; p < net->projs.size(); ++p) sites.push_back({2, (int)p});
-  for (size_t p = 0; p < net->projs.size(); ++p)
-    if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
-  for (size_t p = 0; p < net->pops.size(); ++p)
-    if (net->pops[p].late_reset) sites.push_back({4, (int)p});
+  if (net->fused) {
+    sites.push_back({5, 0});
+  } else {
+    for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
+    for (size_t p = 0; p < net->projs.size(); ++p) sites.push_back({2, (int)p});
+    for (size_t p = 0; p < net->projs.size(); ++p)
+      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      if (net->pops[p].late_reset) sites.push_back({4, (int)p});
+  }
   const size_t ns = sites.size();
   std::vector<cudaEvent_t> ev(2 * ns);
   for (auto& e : ev) CU(cudaEventCreate(&e));
@@ -959,6 +1019,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
+      if (s.kind == 5)
+        e = launch_fused_step(net->fdev, net->pops[0].kind, net->pops[0].dtype, net->fused_grid,
+                              clk, 0, net->cfg.dt, net->d_status, net->stream);
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
       ++net->launches;
@@ -977,6 +1040,11 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
     net->last_chunk_steps = 1;
   }
   for (auto& e : ev) cudaEventDestroy(e);
+  if (result == B2B_OK && net->fused) {
+    cudaError_t e = launch_fused_fold(net->fdev, net->pops[0].dtype, net->d_clock, -1, net->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+    if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile fold: %s", cudaGetErrorString(e));
+  }
   if (result != B2B_OK) return result;
   *n_sites = (int32_t)ns;
   for (size_t k = 0; k < ns && (int32_t)k < cap; ++k) {
@@ -1045,6 +1113,13 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t) {
   if (!net) return B2B_ERR_INVALID_ARG;
   if (timestep) *timestep = net->ts;
   if (t) *t = (double)net->ts * net->cfg.dt;
+  return B2B_OK;
+}
+
+b2b_status b2b_run_mode(b2b_net* net, int32_t* mode) {
+  if (!net || !mode) return B2B_ERR_INVALID_ARG;
+  if (!net->finalized) return fail(net, B2B_ERR_STATE, "call b2b_finalize first");
+  *mode = net->fused ? 1 : 0;
   return B2B_OK;
 }
 

@@ -90,6 +90,17 @@ struct ProjDev {
   const int32_t* post_syn;        // synapse positions grouped by post
 };
 
+// Device view of the one-kernel-per-step path (fused.cu): one population and its additive
+// projections, whose targets are redirected to double-buffered input accumulators.
+struct FusedDev {
+  PopDev pop;
+  ProjDev proj[kMaxProjBatch];
+  int32_t n_proj, nd_max;
+  int32_t neuron_ctas;            // CTAs [0, neuron_ctas) update neurons, the rest deliver
+  int32_t pad;
+  void* acc[3];                   // per target variable (v, ge, gi): [2][pop.n] or NULL
+};
+
 struct Group {
   int kind = 0, dtype = 0, pop = -1;
   int64_t n = 0, offset = 0;
@@ -173,6 +184,10 @@ struct b2b_net {
   std::vector<b2b::Syn> syns;
   std::vector<b2b::Proj> projs;
   std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
+  bool fused = false;                      // one kernel per step (fused.cu) in use
+  b2b::FusedDev fdev{};
+  int fused_grid = 0;
+  std::vector<void*> fused_allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   int64_t launches = 0;
@@ -196,4 +211,12 @@ cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
                                   cudaStream_t s);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
+// One kernel per step (fused.cu): the step itself, and the fold of the pending input.
+size_t fused_smem(const FusedDev& F);
+int fused_block();
+cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
+                              const int64_t* clock, int k, double dt, int32_t* status,
+                              cudaStream_t s);
+cudaError_t launch_fused_fold(const FusedDev& F, int dtype, const int64_t* clock, int k_last,
+                              cudaStream_t s);
 }  // namespace b2b

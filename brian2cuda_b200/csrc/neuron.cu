@@ -15,16 +15,11 @@
 // variable the reset writes; otherwise `late_reset` defers it to a kernel that runs after
 // the synaptic delivery, preserving Brian2's schedule (groups, thresholds, synapses,
 // resets).
-#include "kernels_common.cuh"
+#include "neuron_math.cuh"
 
 namespace b2b {
 
 namespace {
-
-// Brian2's `timestep(t, dt)` (brian2cuda/cuda_generator.py:997-1006).
-__device__ __forceinline__ int64_t timestep_of(double t, double dt) {
-  return (int64_t)((t + 1e-3 * dt) / dt);
-}
 
 template <typename R, int E>
 struct Pack {
@@ -130,8 +125,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   if (q < nthr) {
     const LifDev* prm = static_cast<const LifDev*>(P.params);
     const LifDev g = prm[group_of<E>(P, q)];
-    const R A = (R)g.A, Be = (R)g.Be, Bi = (R)g.Bi, De = (R)g.De, Di = (R)g.Di;
-    const R El = (R)g.El, Vt = (R)g.Vt, Vr = (R)g.Vr;
+    const R Vt = (R)g.Vt, Vr = (R)g.Vr;
     const bool refr = g.ref_steps >= 0;
     Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
     Pack<R, E> GE = load_pack<R, E>(P.var[B2B_VAR_GE], q);
@@ -141,13 +135,12 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     uint32_t NRout = 0;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const R v = V.x[e], ge = GE.x[e], gi = GI.x[e];
+      R ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
-      R vn = dfma(Bi, gi, dfma(Be, ge, dfma(A, v - El, El)));
-      if (g.unless_refractory && !nr) vn = v;
-      GE.x[e] = De * ge;
-      GI.x[e] = Di * gi;
+      R vn = lif_advance<R>(g, V.x[e], ge, gi, nr);
+      GE.x[e] = ge;
+      GI.x[e] = gi;
       const bool valid = (E * q + e - g.offset) < g.n;
       if (g.has_threshold && valid && vn > Vt && nr) {
         nr = false;
@@ -170,17 +163,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   clear_next_slot(P, ts);
 }
 
-// ---- Hodgkin-Huxley (COBAHH), exponential Euler ----------------------------------------
-// Rate functions of examples/cobahh.py:169-180 in SI units (the three of the form
-// x/(exp(x/a) - 1) through z/expm1(z), see z_over_expm1); every right-hand side is evaluated
-// with the values at the start of the step, and each variable x with dx/dt = A x + B
-// advances as x' = -B/A + (x + B/A) exp(A dt).
-template <typename R>
-__device__ __forceinline__ R expeuler(R x, R A, R B, R dt) {
-  const R BA = B / A;
-  return -BA + (BA + x) * dexp(A * dt);
-}
-
+// ---- Hodgkin-Huxley (COBAHH), exponential Euler (hh_advance) ------------------------
 template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
 hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
@@ -194,9 +177,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
     const HhDev g = prm[group_of<E>(P, q)];
-    const R Cm = (R)g.Cm, gl = (R)g.gl, El = (R)g.El, EK = (R)g.EK, ENa = (R)g.ENa;
-    const R gNa = (R)g.gNa, gK = (R)g.gK, VT = (R)g.VT, Ee = (R)g.Ee, Ei = (R)g.Ei;
-    const R De = (R)g.De, Di = (R)g.Di, Vthr = (R)g.Vthr, dtR = (R)dt;
+    const R Vthr = (R)g.Vthr, dtR = (R)dt;
     const bool refr = g.ref_steps >= 0;
     Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
     Pack<R, E> M = load_pack<R, E>(P.var[B2B_VAR_M], q);
@@ -209,26 +190,9 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     uint32_t NRout = 0;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const R v = V.x[e], m = M.x[e], h = H.x[e], n = N.x[e], ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
-      // 0.32/mV*(13mV-v+VT)/(exp((13mV-v+VT)/4mV)-1)/ms = 1280 * z/expm1(z), z = (..)/4mV
-      const R am = (R)1280 * z_over_expm1(((R)13e-3 - v + VT) / (R)4e-3);
-      const R bm = (R)1400 * z_over_expm1((v - VT - (R)40e-3) / (R)5e-3);
-      const R ah = (R)128 * dexp(((R)17e-3 - v + VT) / (R)18e-3);
-      const R bh = (R)4000 / ((R)1 + dexp(((R)40e-3 - v + VT) / (R)5e-3));
-      const R an = (R)160 * z_over_expm1(((R)15e-3 - v + VT) / (R)5e-3);
-      const R bn = (R)500 * dexp(((R)10e-3 - v + VT) / (R)40e-3);
-      const R gna = gNa * (m * m * m) * h;
-      const R gk = gK * (n * n * n * n);
-      const R Av = -(gl + ge + gi + gna + gk) / Cm;
-      const R Bv = (gl * El + ge * Ee + gi * Ei + gna * ENa + gk * EK) / Cm;
-      const R vn = expeuler(v, Av, Bv, dtR);
-      M.x[e] = expeuler(m, -(am + bm), am, dtR);
-      H.x[e] = expeuler(h, -(ah + bh), ah, dtR);
-      N.x[e] = expeuler(n, -(an + bn), an, dtR);
-      GE.x[e] = De * ge;
-      GI.x[e] = Di * gi;
+      const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR);
       const bool valid = (E * q + e - g.offset) < g.n;
       if (valid && vn > Vthr && nr) {
         nr = false;

@@ -140,7 +140,7 @@ class Network:
 
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
-                 stream: int | None = None):
+                 stream: int | None = None, fused: bool = True):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
         default the network creates its own non-blocking stream."""
         self._lib = N.lib()
@@ -148,6 +148,8 @@ class Network:
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
         if reset_before_synapses:
             flags |= N.NET_RESET_BEFORE_SYNAPSES
+        if not fused:
+            flags |= N.NET_NO_FUSED
         cfg = N.Config(self.dt, device, steps_per_graph, seed, stream, flags, 0)
         h = C.c_void_p()
         st = self._lib.b2b_create(C.byref(cfg), C.byref(h))
@@ -319,6 +321,13 @@ class Network:
         ts = C.c_int64()
         self._lib.b2b_time(self._h, C.byref(ts), None)
         return ts.value
+
+    @property
+    def run_mode(self) -> str:
+        """'fused' (persistent multi-step kernel) or 'per-step' (graph-replayed kernels)."""
+        m = C.c_int32()
+        self._check(self._lib.b2b_run_mode(self._h, C.byref(m)), "run_mode")
+        return "fused" if m.value == 1 else "per-step"
 
     @property
     def kernel_launches(self) -> int:

@@ -56,9 +56,12 @@ enum { B2B_F32 = 1, B2B_F64 = 2 };
 enum {
   B2B_NET_NO_GRAPH = 1,   /* launch every step eagerly instead of replaying CUDA graphs */
   B2B_NET_CHECKED = 2,    /* kernels check indices and record B2B_ERR_INDEX            */
-  B2B_NET_RESET_BEFORE_SYNAPSES = 4  /* schedule start, groups, thresholds, resets, synapses,
+  B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
+  B2B_NET_NO_FUSED = 8    /* never run one kernel per step (neuron update and delivery side
+                             by side), which a net with one population, additive synapses
+                             onto ge/gi and all delays >= 1 step otherwise uses          */
 };
 
 typedef struct {
@@ -201,13 +204,17 @@ b2b_status b2b_restore(b2b_net* net, int32_t slot);
 b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
 b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
+/* How b2b_run advances the net (after b2b_finalize): *mode = 1 for the persistent
+ * multi-step kernel, 0 for per-step kernels replayed from CUDA graphs. */
+b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
  * network by n_steps with eager launches, timing every launch with a CUDA event pair on the
  * net's stream, and returns per launch site the mean device time of one launch in ms.
  * Sites, in order: one per population (kind 1), one per projection's on_pre delivery
  * (kind 2), one per STDP projection's on_post delivery (kind 3), one per population with a
- * deferred reset (kind 4).  *n_sites receives the number of sites (<= cap filled). */
+ * deferred reset (kind 4); or, when the net runs one kernel per step (b2b_run_mode 1), that
+ * kernel alone (kind 5).  *n_sites receives the number of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
 
