@@ -191,6 +191,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2b", choices=["b2b", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", type=int, default=0, metavar="STEPS",
+                    help="profiling case: build the workload, simulate STEPS steps, print "
+                         "nothing (for ncu captures of the step kernels)")
+    ap.add_argument("--per-step", action="store_true",
+                    help="use the per-step kernels even where one kernel per step applies")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
 
@@ -210,7 +215,7 @@ def main():
     runs = args.warmup + 2 * args.steps + 1
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
-                  stream=stream.cuda_stream)
+                  stream=stream.cuda_stream, fused=not args.per_step)
     t_setup = time.perf_counter()
     ids = models.build_cobahh(net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
                               monitor_capacity=mon_cap)
@@ -227,6 +232,12 @@ def main():
     net.store(0)
     init = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi", "lastspike")}
     setup_s = time.perf_counter() - t_setup
+
+    if args.ncu_case:
+        net.run(args.ncu_case)
+        net.sync()
+        net.close()
+        return
 
     def one_run():
         net.restore(0)

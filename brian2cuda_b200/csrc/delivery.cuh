@@ -1,0 +1,139 @@
+// Enumeration of the synapse bundles due at a step, shared by every delivery kernel.
+//
+// A bundle (pre, d) is due at step ts when pre spiked at step ts - d.  The due work of a
+// projection is therefore the spikes of ring slots ts - dmin .. ts - dmin - nd + 1, each
+// split into `chunks` work items of up to kChunk synapses.  An item is located by a prefix
+// sum over the per-delay spike counts.  With nd <= 64 every warp computes that prefix in two
+// registers per lane (two coalesced loads and a warp scan) and finds an item's delay with two
+// ballots, so no shared memory or block barrier is involved; larger delay ranges use a
+// per-CTA prefix in shared memory.
+#pragma once
+#include "kernels_common.cuh"
+
+namespace b2b {
+
+constexpr int kWarpPrefixMaxDelays = 64;
+
+// Slot of step (ts - d) given ts's slot, for 0 <= d < ring_len.
+__device__ __forceinline__ int ring_back(int base, int d, int ring_len) {
+  const int s = base - d;
+  return s < 0 ? s + ring_len : s;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// Per-warp inclusive prefix of the due spike counts of up to 64 delays: lane l holds the
+// prefix through delay index l (incl0) and through 32 + l (incl1).
+struct DuePrefix {
+  int incl0, incl1, total;
+};
+
+__device__ __forceinline__ DuePrefix due_prefix_warp(const int32_t* __restrict__ ring_cnt,
+                                                     int ring_len, int64_t ts, int dmin, int nd) {
+  const int lane = threadIdx.x & 31;
+  const int base = ring_slot(ts, ring_len);
+  int c0 = 0, c1 = 0;
+  if (lane < nd && ts - (dmin + lane) >= 0) c0 = ring_cnt[ring_back(base, dmin + lane, ring_len)];
+  if (32 + lane < nd && ts - (dmin + 32 + lane) >= 0)
+    c1 = ring_cnt[ring_back(base, dmin + 32 + lane, ring_len)];
+  DuePrefix p;
+  p.incl0 = warp_incl_scan(c0);
+  const int t0 = __shfl_sync(kFull, p.incl0, 31);
+  p.incl1 = warp_incl_scan(c1) + t0;
+  p.total = __shfl_sync(kFull, p.incl1, 31);
+  return p;
+}
+
+// Delay index of due spike number sp (0 <= sp < total) and its rank within its slot.
+__device__ __forceinline__ int find_delay_warp(const DuePrefix& p, int sp, int* rank) {
+  const int di = __popc(__ballot_sync(kFull, p.incl0 <= sp)) +
+                 __popc(__ballot_sync(kFull, p.incl1 <= sp));
+  const int src = (di - 1) & 31;
+  const int v0 = __shfl_sync(kFull, p.incl0, src);
+  const int v1 = __shfl_sync(kFull, p.incl1, src);
+  const int excl = di == 0 ? 0 : (di - 1 < 32 ? v0 : v1);
+  *rank = sp - excl;
+  return di;
+}
+
+// Per-CTA prefix in shared memory (any nd): s_pref[0] = 0, s_pref[i] = counts of delay
+// indices < i.  Every thread of the CTA must call this.
+__device__ __forceinline__ int due_prefix_block(const int32_t* __restrict__ ring_cnt,
+                                                int ring_len, int64_t ts, int dmin, int nd,
+                                                int* s_pref) {
+  const int base = ring_slot(ts, ring_len);
+  for (int di = threadIdx.x; di < nd; di += blockDim.x)
+    s_pref[di + 1] = ts - (dmin + di) >= 0 ? ring_cnt[ring_back(base, dmin + di, ring_len)] : 0;
+  if (threadIdx.x == 0) s_pref[0] = 0;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int carry = 0;
+    for (int b0 = 1; b0 <= nd; b0 += 32) {
+      const int i = b0 + lane;
+      int x = warp_incl_scan(i <= nd ? s_pref[i] : 0);
+      if (i <= nd) s_pref[i] = x + carry;
+      carry += __shfl_sync(kFull, x, 31);
+    }
+  }
+  __syncthreads();
+  return s_pref[nd];
+}
+
+__device__ __forceinline__ int find_delay_block(const int* s_pref, int nd, int sp, int* rank) {
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_pref[mid] <= sp) lo = mid; else hi = mid - 1;
+  }
+  *rank = sp - s_pref[lo];
+  return lo;
+}
+
+// Calls body(s, valid) for every synapse position s of every bundle of projection J due at
+// step ts, over warps warp0, warp0 + nwarps, ...  All 32 lanes of a warp call body together
+// (valid marks real synapses).  WARP_PREFIX requires J.nd <= 64; otherwise every thread of
+// the CTA must call this (block prefix in s_pref, J.nd + 1 ints).
+template <bool WARP_PREFIX, class Body>
+__device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64_t warp0,
+                                             int64_t nwarps, int* s_pref, Body body) {
+  const int lane = threadIdx.x & 31;
+  DuePrefix wp{};
+  int nspk;
+  if constexpr (WARP_PREFIX) {
+    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd);
+    nspk = wp.total;
+  } else {
+    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, s_pref);
+  }
+  const int64_t items = (int64_t)nspk * J.chunks;
+  const int base = ring_slot(ts, J.src_ring_len);
+  for (int64_t it = warp0; it < items; it += nwarps) {
+    const int sp = (int)(it / J.chunks);
+    const int ch = (int)(it - (int64_t)sp * J.chunks);
+    int kk;
+    int di;
+    if constexpr (WARP_PREFIX) di = find_delay_warp(wp, sp, &kk);
+    else di = find_delay_block(s_pref, J.nd, sp, &kk);
+    const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
+    const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
+    const int64_t key = (int64_t)pre * J.nd + di;
+    const int64_t b0 = J.off[key] + (int64_t)ch * kChunk;
+    int64_t b1 = J.off[key + 1];
+    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
+    for (int64_t s0 = b0; s0 < b1; s0 += 32) {
+      const int64_t s = s0 + lane;
+      body(s, s < b1);
+    }
+  }
+}
+
+}  // namespace b2b

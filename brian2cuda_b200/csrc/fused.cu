@@ -20,6 +20,7 @@
 // (griddepcontrol.wait) for its predecessor's memory before touching state, so the launch of
 // step t+1 overlaps the tail of step t.  Measured on B200: a graph kernel boundary costs
 // about 1.1 us, 0.9 us with programmatic dependent launch, a software grid barrier 1.2-1.4 us.
+#include "delivery.cuh"
 #include "neuron_math.cuh"
 
 namespace b2b {
@@ -89,7 +90,7 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
   uint8_t* NR = static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
   bool spk = false;
   if constexpr (KIND == KIND_HH) {
-    const HhDev& g = static_cast<const HhDev*>(P.params)[gidx];
+    const HhDev g = static_cast<const HhDev*>(P.params)[gidx];  // by value: no reloads
     const bool refr = g.ref_steps >= 0;
     bool nr = true;
     if (refr) nr = timestep_of(t - (double)LS[q], dt) >= g.ref_steps;
@@ -109,7 +110,7 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
     N[q] = n;
     if (refr) NR[q] = nr ? 1 : 0;
   } else {
-    const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
+    const LifDev g = static_cast<const LifDev*>(P.params)[gidx];  // by value: no reloads
     const bool refr = g.ref_steps >= 0;
     bool nr = true;
     if (refr) nr = timestep_of(t - (double)LS[q], dt) >= g.ref_steps;
@@ -128,12 +129,11 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
   return spk;
 }
 
-template <typename R, int KIND>
+template <typename R, int KIND, bool WARP_PREFIX>
 __global__ void __launch_bounds__(kFusedBlock)
 fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict__ clock, int k,
                   double dt, int32_t* status) {
-  extern __shared__ int s_pref[];  // F.n_proj x (F.nd_max + 1)
-  __shared__ int s_base[kMaxProjBatch + 1];
+  extern __shared__ int s_pref[];  // F.nd_max + 1 ints when !WARP_PREFIX
   wait_for_predecessor();
   allow_successor_launch();
   const PopDev& P = F.pop;
@@ -150,76 +150,20 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
     return;
   }
   // ---- delivery half: bundles due at step ts (spikes of steps ts - d, d >= 1) into acc[ts & 1]
-  const int lane = threadIdx.x & 31;
+  const int64_t warp0 = ((int64_t)(blockIdx.x - F.neuron_ctas) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)(gridDim.x - F.neuron_ctas) * blockDim.x) >> 5;
+  const int par = (int)(ts & 1);
   for (int p = 0; p < F.n_proj; ++p) {
     const ProjDev& J = F.proj[p];
-    int* pref = s_pref + p * (F.nd_max + 1);
-    for (int di = threadIdx.x; di < J.nd; di += blockDim.x) {
-      const int64_t st = ts - (int64_t)(J.dmin + di);
-      pref[di + 1] = st >= 0 ? J.src_ring_cnt[ring_slot(st, J.src_ring_len)] : 0;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int total = 0;
-    for (int p = 0; p < F.n_proj; ++p) {
-      const ProjDev& J = F.proj[p];
-      int* pref = s_pref + p * (F.nd_max + 1);
-      int carry = 0;
-      for (int b0 = 1; b0 <= J.nd; b0 += 32) {
-        const int i = b0 + lane;
-        int x = i <= J.nd ? pref[i] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(kFull, x, o);
-          if (lane >= o) x += y;
-        }
-        if (i <= J.nd) pref[i] = x + carry;
-        carry += __shfl_sync(kFull, x, 31);
-      }
-      if (lane == 0) {
-        pref[0] = 0;
-        s_base[p] = total;
-      }
-      total += carry * J.chunks;
-    }
-    if (lane == 0) s_base[F.n_proj] = total;
-  }
-  __syncthreads();
-  const int64_t items = s_base[F.n_proj];
-  const int dctas = gridDim.x - F.neuron_ctas;
-  const int64_t warps = (int64_t)dctas * (blockDim.x >> 5);
-  const int par = (int)(ts & 1);
-  for (int64_t it = (int64_t)(blockIdx.x - F.neuron_ctas) * (blockDim.x >> 5) +
-                    (threadIdx.x >> 5);
-       it < items; it += warps) {
-    int p = 0;
-    while (p + 1 < F.n_proj && s_base[p + 1] <= it) ++p;
-    const ProjDev& J = F.proj[p];
-    const int* pref = s_pref + p * (F.nd_max + 1);
-    const int64_t local = it - s_base[p];
-    const int sp = (int)(local / J.chunks);
-    const int ch = (int)(local - (int64_t)sp * J.chunks);
-    int lo = 0, hi = J.nd - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (pref[mid] <= sp) lo = mid; else hi = mid - 1;
-    }
-    const int kk = sp - pref[lo];
-    const int64_t st = ts - (int64_t)(J.dmin + lo);
-    const int32_t pre = J.src_ring_idx[(int64_t)ring_slot(st, J.src_ring_len) * J.src_n + kk];
-    const int64_t key = (int64_t)pre * J.nd + lo;
-    const int64_t b0 = J.off[key] + (int64_t)ch * kChunk;
-    int64_t b1 = J.off[key + 1];
-    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
     R* T = static_cast<R*>(J.target) + (int64_t)par * P.n;
     const R* W = static_cast<const R*>(J.w);
     const R ws = (R)J.w_scalar;
-    for (int64_t s = b0 + lane; s < b1; s += 32) {
+    for_each_due<WARP_PREFIX>(J, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+      if (!valid) return;
       const int32_t post = __ldg(J.post + s);
       const R w = W ? __ldg(W + s) : ws;
       atomicAdd(T + post, w);
-    }
+    });
   }
 }
 
@@ -261,7 +205,7 @@ cudaError_t launch_pdl(KernelT kernel, dim3 grid, size_t smem, cudaStream_t s, A
 }  // namespace
 
 size_t fused_smem(const FusedDev& F) {
-  return sizeof(int) * (size_t)F.n_proj * (size_t)(F.nd_max + 1);
+  return F.nd_max <= kWarpPrefixMaxDelays ? 0 : sizeof(int) * (size_t)(F.nd_max + 1);
 }
 
 int fused_block() { return kFusedBlock; }
@@ -271,14 +215,16 @@ cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
                               cudaStream_t s) {
   const size_t smem = fused_smem(F);
   const dim3 g(grid);
+  const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
+#define B2B_FS(R, KD, WP) \
+  launch_pdl(fused_step_kernel<R, KD, WP>, g, smem, s, F, clock, k, dt, status)
   if (kind == KIND_HH) {
-    if (dtype == B2B_F32)
-      return launch_pdl(fused_step_kernel<float, KIND_HH>, g, smem, s, F, clock, k, dt, status);
-    return launch_pdl(fused_step_kernel<double, KIND_HH>, g, smem, s, F, clock, k, dt, status);
+    if (dtype == B2B_F32) return wp ? B2B_FS(float, KIND_HH, true) : B2B_FS(float, KIND_HH, false);
+    return wp ? B2B_FS(double, KIND_HH, true) : B2B_FS(double, KIND_HH, false);
   }
-  if (dtype == B2B_F32)
-    return launch_pdl(fused_step_kernel<float, KIND_LIF>, g, smem, s, F, clock, k, dt, status);
-  return launch_pdl(fused_step_kernel<double, KIND_LIF>, g, smem, s, F, clock, k, dt, status);
+  if (dtype == B2B_F32) return wp ? B2B_FS(float, KIND_LIF, true) : B2B_FS(float, KIND_LIF, false);
+  return wp ? B2B_FS(double, KIND_LIF, true) : B2B_FS(double, KIND_LIF, false);
+#undef B2B_FS
 }
 
 cudaError_t launch_fused_fold(const FusedDev& F, int dtype, const int64_t* clock, int k_last,

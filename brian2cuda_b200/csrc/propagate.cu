@@ -10,14 +10,14 @@
 //
 // Here nothing is pushed.  Each population keeps the compacted spikes of its last
 // `ring_len` steps (written by the neuron kernel).  A bundle (pre, d) is due at step ts
-// exactly when pre spiked at step ts - d, so the delivery kernel enumerates, for every delay
-// d of the projection, the spikes of ring slot ts - d and walks the synapse range of bundle
-// (pre, d) in the (pre, delay)-sorted synapse arrays.  This is the same set of bundles the
-// reference's queue holds in slot `current_offset` after its push, without the push kernel,
-// the host sync on the spike count, the locks or the device heap.
+// exactly when pre spiked at step ts - d, so the delivery kernels enumerate, for every delay
+// d of the projection, the spikes of ring slot ts - d and walk the synapse range of bundle
+// (pre, d) in the (pre, delay)-sorted synapse arrays (delivery.cuh).  This is the same set of
+// bundles the reference's queue holds in slot `current_offset` after its push, without the
+// push kernel, the host sync on the spike count, the locks or the device heap.
 #include <algorithm>
 
-#include "kernels_common.cuh"
+#include "delivery.cuh"
 
 namespace b2b {
 
@@ -25,81 +25,7 @@ namespace {
 
 constexpr int kDeliverBlock = 256;
 
-// Loads the number of due spikes per delay into s_pref[1..nd] and turns it into an
-// inclusive prefix (s_pref[0] = 0).  Returns the number of due (spike, delay) pairs.
-__device__ __forceinline__ int due_prefix(const int32_t* ring_cnt, int ring_len, int64_t ts,
-                                          int dmin, int nd, int* s_pref) {
-  for (int di = threadIdx.x; di < nd; di += blockDim.x) {
-    const int64_t st = ts - (int64_t)(dmin + di);
-    s_pref[di + 1] = st >= 0 ? ring_cnt[ring_slot(st, ring_len)] : 0;
-  }
-  if (threadIdx.x == 0) s_pref[0] = 0;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    int carry = 0;
-    for (int base = 1; base <= nd; base += 32) {
-      const int i = base + lane;
-      int x = i <= nd ? s_pref[i] : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += y;
-      }
-      if (i <= nd) s_pref[i] = x + carry;
-      carry += __shfl_sync(kFull, x, 31);
-    }
-  }
-  __syncthreads();
-  return s_pref[nd];
-}
-
-// Largest di in [0, nd) with s_pref[di] <= sp.
-__device__ __forceinline__ int find_delay(const int* s_pref, int nd, int sp) {
-  int lo = 0, hi = nd - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (s_pref[mid] <= sp) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Calls body(s, valid) for every synapse position s of every bundle due at step ts.  All 32
-// lanes of a warp call body together (valid marks real synapses), so bodies may use
-// warp-synchronous intrinsics.
-template <class Body>
-__device__ __forceinline__ void for_each_due(const ProjDev& P, int64_t ts, int* s_pref,
-                                             Body body) {
-  const int nspk = due_prefix(P.src_ring_cnt, P.src_ring_len, ts, P.dmin, P.nd, s_pref);
-  const int64_t items = (int64_t)nspk * P.chunks;
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t it = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items;
-       it += warps) {
-    const int sp = (int)(it / P.chunks);
-    const int ch = (int)(it - (int64_t)sp * P.chunks);
-    const int di = find_delay(s_pref, P.nd, sp);
-    const int kk = sp - s_pref[di];
-    const int64_t st = ts - (int64_t)(P.dmin + di);
-    const int32_t pre =
-        P.src_ring_idx[(int64_t)ring_slot(st, P.src_ring_len) * P.src_n + kk];
-    const int64_t key = (int64_t)pre * P.nd + di;
-    const int64_t b0 = P.off[key] + (int64_t)ch * kChunk;
-    int64_t b1 = P.off[key + 1];
-    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
-    for (int64_t base = b0; base < b1; base += 32) {
-      const int64_t s = base + lane;
-      body(s, s < b1);
-    }
-  }
-}
-
-template <typename R>
-__device__ __forceinline__ void atomic_add(R* addr, R v) {
-  atomicAdd(addr, v);
-}
-
-// Sum of `v` over the lanes whose `key` equals this lane's key; valid in every lane.
+// Sum of `v` over the lanes whose key equals this lane's key; valid in every lane.
 template <typename R>
 __device__ __forceinline__ R peer_sum(unsigned peers, R v) {
   R acc = 0;
@@ -111,28 +37,16 @@ __device__ __forceinline__ R peer_sum(unsigned peers, R v) {
   return acc;
 }
 
-// ---- on_pre: target[post] += w -------------------------------------------------------------
-template <typename R, bool HAS_W, bool AGG>
-__global__ void __launch_bounds__(kDeliverBlock)
-deliver_add_kernel(ProjDev P, const int64_t* __restrict__ clock, int k) {
-  extern __shared__ int s_pref[];
-  const int64_t ts = clock[0] + k;
-  const R* __restrict__ W = static_cast<const R*>(P.w);
-  const R ws = (R)P.w_scalar;
-  R* __restrict__ T = static_cast<R*>(P.target);
-  const int lane = threadIdx.x & 31;
-  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
-    const int32_t post = valid ? __ldg(P.post + s) : -1;
-    R w = ws;
-    if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
-    if constexpr (AGG) {
-      const unsigned peers = __match_any_sync(kFull, post);
-      const R sum = peer_sum<R>(peers, w);
-      if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
-    } else {
-      if (valid) atomic_add(T + post, w);
-    }
-  });
+// target[post] += w for one synapse per lane; AGG sums lanes hitting the same target first.
+template <typename R, bool AGG>
+__device__ __forceinline__ void add_to_target(R* T, int32_t post, R w, bool valid) {
+  if constexpr (AGG) {
+    const unsigned peers = __match_any_sync(kFull, valid ? post : -1);
+    const R sum = peer_sum<R>(peers, valid ? w : (R)0);
+    if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(T + post, sum);
+  } else {
+    if (valid) atomicAdd(T + post, w);
+  }
 }
 
 // Several additive projections in one launch: blockIdx.y picks the projection.
@@ -141,7 +55,8 @@ struct ProjBatch {
   int n;
 };
 
-template <typename R, bool HAS_W, bool AGG>
+// ---- on_pre: target[post] += w -------------------------------------------------------------
+template <typename R, bool HAS_W, bool AGG, bool WARP_PREFIX>
 __global__ void __launch_bounds__(kDeliverBlock)
 deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __restrict__ clock,
                          int k) {
@@ -151,25 +66,20 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   const R* __restrict__ W = static_cast<const R*>(P.w);
   const R ws = (R)P.w_scalar;
   R* __restrict__ T = static_cast<R*>(P.target);
-  const int lane = threadIdx.x & 31;
-  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
-    const int32_t post = valid ? __ldg(P.post + s) : -1;
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+    const int32_t post = valid ? __ldg(P.post + s) : 0;
     R w = ws;
     if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
-    if constexpr (AGG) {
-      const unsigned peers = __match_any_sync(kFull, post);
-      const R sum = peer_sum<R>(peers, w);
-      if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
-    } else {
-      if (valid) atomic_add(T + post, w);
-    }
+    add_to_target<R, AGG>(T, post, w, valid);
   });
 }
 
 // ---- on_pre of event-driven additive STDP (examples/stdp.py:125-186) ----------------------
 // Traces decay lazily from lastupdate to t (Brian2's event-driven update); in float32 the
 // elapsed time is rounded to float first, as brian2cuda does (brian2cuda/device.py:1034-1039).
-template <typename R, bool AGG>
+template <typename R, bool AGG, bool WARP_PREFIX>
 __global__ void __launch_bounds__(kDeliverBlock)
 deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, double dt) {
   extern __shared__ int s_pref[];
@@ -182,9 +92,10 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
   R* __restrict__ T = static_cast<R*>(P.target);
   const R taupre = (R)P.taupre, taupost = (R)P.taupost, dApre = (R)P.dApre;
   const R wmin = (R)P.wmin, wmax = (R)P.wmax;
-  const int lane = threadIdx.x & 31;
-  for_each_due(P, ts, s_pref, [&](int64_t s, bool valid) {
-    int32_t post = -1;
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+    int32_t post = 0;
     R w = 0;
     if (valid) {
       post = __ldg(P.post + s);
@@ -199,15 +110,7 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
       Apost[s] = apost;
       LU[s] = (R)t;
     }
-    if (P.pre_adds_weight) {
-      if constexpr (AGG) {
-        const unsigned peers = __match_any_sync(kFull, post);
-        const R sum = peer_sum<R>(peers, w);
-        if (valid && lane == __ffs(peers) - 1) atomic_add(T + post, sum);
-      } else {
-        if (valid) atomic_add(T + post, w);
-      }
-    }
+    if (P.pre_adds_weight) add_to_target<R, AGG>(T, post, w, valid);
   });
 }
 
@@ -260,41 +163,40 @@ unsigned deliver_grid(const Proj& pr) {
   return (unsigned)(want < cap ? want : cap);
 }
 
-}  // namespace
-
-cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,
-                            int32_t* status, cudaStream_t s) {
-  (void)status;
-  const ProjDev& P = pr.dev;
-  const unsigned grid = deliver_grid(pr);
-  const size_t smem = sizeof(int) * (size_t)(P.nd + 1);
-  const bool f32 = pr.dtype == B2B_F32;
-  if (pr.effect == B2B_EFFECT_ADD) {
-    const bool hw = P.w != nullptr;
-    const bool ag = P.aggregate != 0;
-#define B2B_ADD(R, HW, AG) deliver_add_kernel<R, HW, AG><<<grid, kDeliverBlock, smem, s>>>(P, clock, k)
-    if (f32) {
-      if (hw) { if (ag) B2B_ADD(float, true, true); else B2B_ADD(float, true, false); }
-      else { if (ag) B2B_ADD(float, false, true); else B2B_ADD(float, false, false); }
-    } else {
-      if (hw) { if (ag) B2B_ADD(double, true, true); else B2B_ADD(double, true, false); }
-      else { if (ag) B2B_ADD(double, false, true); else B2B_ADD(double, false, false); }
-    }
-#undef B2B_ADD
-  } else if (pr.effect == B2B_EFFECT_STDP) {
-    const bool ag = P.aggregate != 0;
-    if (f32) {
-      if (ag) deliver_stdp_pre_kernel<float, true><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
-      else deliver_stdp_pre_kernel<float, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
-    } else {
-      if (ag) deliver_stdp_pre_kernel<double, true><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
-      else deliver_stdp_pre_kernel<double, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
-    }
-  } else {
-    return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
+template <typename R, bool HAS_W, bool AGG>
+void launch_add(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem, const int64_t* clock,
+                int k, cudaStream_t s) {
+  if (warp_prefix)
+    deliver_add_batch_kernel<R, HAS_W, AGG, true><<<g, kDeliverBlock, 0, s>>>(B, clock, k);
+  else
+    deliver_add_batch_kernel<R, HAS_W, AGG, false><<<g, kDeliverBlock, smem, s>>>(B, clock, k);
 }
+
+template <typename R>
+void launch_add_r(const ProjBatch& B, dim3 g, bool hw, bool ag, bool wp, size_t smem,
+                  const int64_t* clock, int k, cudaStream_t s) {
+  if (hw) {
+    if (ag) launch_add<R, true, true>(B, g, wp, smem, clock, k, s);
+    else launch_add<R, true, false>(B, g, wp, smem, clock, k, s);
+  } else {
+    if (ag) launch_add<R, false, true>(B, g, wp, smem, clock, k, s);
+    else launch_add<R, false, false>(B, g, wp, smem, clock, k, s);
+  }
+}
+
+template <typename R>
+void launch_stdp_pre(const ProjDev& P, unsigned grid, bool ag, bool wp, size_t smem,
+                     const int64_t* clock, int k, double dt, cudaStream_t s) {
+  if (wp) {
+    if (ag) deliver_stdp_pre_kernel<R, true, true><<<grid, kDeliverBlock, 0, s>>>(P, clock, k, dt);
+    else deliver_stdp_pre_kernel<R, false, true><<<grid, kDeliverBlock, 0, s>>>(P, clock, k, dt);
+  } else {
+    if (ag) deliver_stdp_pre_kernel<R, true, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+    else deliver_stdp_pre_kernel<R, false, false><<<grid, kDeliverBlock, smem, s>>>(P, clock, k, dt);
+  }
+}
+
+}  // namespace
 
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
                                   cudaStream_t s) {
@@ -308,21 +210,31 @@ cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* 
     grid = std::max(grid, deliver_grid(*prs[i]));
     nd = std::max(nd, (int)prs[i]->dev.nd);
   }
+  const bool wp = nd <= kWarpPrefixMaxDelays;
   const size_t smem = sizeof(int) * (size_t)(nd + 1);
-  const bool f32 = prs[0]->dtype == B2B_F32;
+  const dim3 g(grid, (unsigned)n);
   const bool hw = prs[0]->dev.w != nullptr;
   const bool ag = prs[0]->dev.aggregate != 0;
-  const dim3 g(grid, (unsigned)n);
-#define B2B_ADDB(R, HW, AG) \
-  deliver_add_batch_kernel<R, HW, AG><<<g, kDeliverBlock, smem, s>>>(B, clock, k)
-  if (f32) {
-    if (hw) { if (ag) B2B_ADDB(float, true, true); else B2B_ADDB(float, true, false); }
-    else { if (ag) B2B_ADDB(float, false, true); else B2B_ADDB(float, false, false); }
-  } else {
-    if (hw) { if (ag) B2B_ADDB(double, true, true); else B2B_ADDB(double, true, false); }
-    else { if (ag) B2B_ADDB(double, false, true); else B2B_ADDB(double, false, false); }
+  if (prs[0]->dtype == B2B_F32) launch_add_r<float>(B, g, hw, ag, wp, smem, clock, k, s);
+  else launch_add_r<double>(B, g, hw, ag, wp, smem, clock, k, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,
+                            int32_t* status, cudaStream_t s) {
+  (void)status;
+  if (pr.effect == B2B_EFFECT_ADD) {
+    const Proj* one = &pr;
+    return launch_proj_add_batch(&one, 1, clock, k, s);
   }
-#undef B2B_ADDB
+  if (pr.effect != B2B_EFFECT_STDP) return cudaErrorInvalidValue;
+  const ProjDev& P = pr.dev;
+  const unsigned grid = deliver_grid(pr);
+  const bool wp = P.nd <= kWarpPrefixMaxDelays;
+  const size_t smem = sizeof(int) * (size_t)(P.nd + 1);
+  const bool ag = P.aggregate != 0;
+  if (pr.dtype == B2B_F32) launch_stdp_pre<float>(P, grid, ag, wp, smem, clock, k, dt, s);
+  else launch_stdp_pre<double>(P, grid, ag, wp, smem, clock, k, dt, s);
   return cudaGetLastError();
 }
 
