@@ -573,9 +573,12 @@ b2b_status setup_fused(b2b_net* net) {
   F.neuron_ctas = (int32_t)((pop.n + block - 1) / block);
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
-  int deliver = std::max(8, std::min(2 * sms, (int)(pop.n / 1024)));
+  // delivery CTAs fill what one wave leaves after the neuron CTAs, at least 16
+  const int resident = fused_resident_ctas(pop.kind, pop.dtype, F, sms);
+  int deliver = std::min(2 * sms, std::max(16, resident - F.neuron_ctas));
   if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) deliver = std::max(1, std::atoi(env));
-  net->fused_grid = F.neuron_ctas + deliver;
+  F.deliver_ctas = deliver;
+  net->fused_grid = F.neuron_ctas + F.deliver_ctas;
   net->fused = true;
   return B2B_OK;
 }

@@ -96,8 +96,8 @@ struct FusedDev {
   PopDev pop;
   ProjDev proj[kMaxProjBatch];
   int32_t n_proj, nd_max;
-  int32_t neuron_ctas;            // CTAs [0, neuron_ctas) update neurons, the rest deliver
-  int32_t pad;
+  int32_t deliver_ctas;           // CTAs [0, deliver_ctas) deliver, the rest update neurons
+  int32_t neuron_ctas;
   void* acc[3];                   // per target variable (v, ge, gi): [2][pop.n] or NULL
 };
 
@@ -214,6 +214,7 @@ cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
 // One kernel per step (fused.cu): the step itself, and the fold of the pending input.
 size_t fused_smem(const FusedDev& F);
 int fused_block();
+int fused_resident_ctas(int kind, int dtype, const FusedDev& F, int sms);
 cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
                               const int64_t* clock, int k, double dt, int32_t* status,
                               cudaStream_t s);

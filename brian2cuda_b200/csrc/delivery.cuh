@@ -99,13 +99,18 @@ __device__ __forceinline__ int find_delay_block(const int* s_pref, int nd, int s
 }
 
 // Calls body(s, valid) for every synapse position s of every bundle of projection J due at
-// step ts, over warps warp0, warp0 + nwarps, ...  All 32 lanes of a warp call body together
+// step ts.  Work items go to warps warp0, warp0 + nwarps, ...; inside a warp, groups of
+// GROUP lanes take one item each, so 32/GROUP items' dependent loads (spike index, bundle
+// offsets, synapse data) are in flight together.  All 32 lanes of a warp call body together
 // (valid marks real synapses).  WARP_PREFIX requires J.nd <= 64; otherwise every thread of
 // the CTA must call this (block prefix in s_pref, J.nd + 1 ints).
-template <bool WARP_PREFIX, class Body>
+template <bool WARP_PREFIX, int GROUP = 32, class Body>
 __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64_t warp0,
                                              int64_t nwarps, int* s_pref, Body body) {
+  static_assert(GROUP == 32 || GROUP == 16 || GROUP == 8 || GROUP == 4, "group size");
+  constexpr int G = 32 / GROUP;  // items per warp per round
   const int lane = threadIdx.x & 31;
+  const int grp = lane / GROUP, glane = lane % GROUP;
   DuePrefix wp{};
   int nspk;
   if constexpr (WARP_PREFIX) {
@@ -116,21 +121,37 @@ __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64
   }
   const int64_t items = (int64_t)nspk * J.chunks;
   const int base = ring_slot(ts, J.src_ring_len);
-  for (int64_t it = warp0; it < items; it += nwarps) {
-    const int sp = (int)(it / J.chunks);
-    const int ch = (int)(it - (int64_t)sp * J.chunks);
-    int kk;
-    int di;
-    if constexpr (WARP_PREFIX) di = find_delay_warp(wp, sp, &kk);
-    else di = find_delay_block(s_pref, J.nd, sp, &kk);
-    const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
-    const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
-    const int64_t key = (int64_t)pre * J.nd + di;
-    const int64_t b0 = J.off[key] + (int64_t)ch * kChunk;
-    int64_t b1 = J.off[key + 1];
-    if (b1 > b0 + kChunk) b1 = b0 + kChunk;
-    for (int64_t s0 = b0; s0 < b1; s0 += 32) {
-      const int64_t s = s0 + lane;
+  for (int64_t r0 = warp0 * G; r0 < items; r0 += nwarps * G) {
+    const int64_t it = r0 + grp;
+    const bool have = it < items;
+    const int sp = have ? (int)(it / J.chunks) : 0;
+    const int ch = have ? (int)(it - (int64_t)sp * J.chunks) : 0;
+    int kk = 0, di = 0;
+    if constexpr (WARP_PREFIX) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        int r;
+        const int d = find_delay_warp(wp, __shfl_sync(kFull, sp, g * GROUP), &r);
+        if (grp == g) { di = d; kk = r; }
+      }
+    } else {
+      di = find_delay_block(s_pref, J.nd, sp, &kk);
+    }
+    int64_t b0 = 0, b1 = 0;
+    if (have) {
+      const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
+      const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
+      const int64_t key = (int64_t)pre * J.nd + di;
+      b0 = J.off[key] + (int64_t)ch * kChunk;
+      b1 = J.off[key + 1];
+      if (b1 > b0 + kChunk) b1 = b0 + kChunk;
+    }
+    // rounds until the longest bundle of this warp's groups is done (warp-uniform)
+    int64_t len = b1 - b0;
+#pragma unroll
+    for (int o = 16; o >= GROUP; o >>= 1) len = max(len, __shfl_xor_sync(kFull, len, o));
+    for (int64_t off = 0; off < len; off += GROUP) {
+      const int64_t s = b0 + off + glane;
       body(s, s < b1);
     }
   }

@@ -6,11 +6,12 @@
 // delivery of step t only reads spikes of steps t - d <= t - 1, so its one dependence on the
 // update of step t is the target variable itself.  Double-buffering that input removes it:
 //
-//   step t (one launch):  CTAs [0, neuron_ctas) update one neuron per thread, reading the
-//                         input that arrived during step t-1 from acc[(t-1) & 1] (and
-//                         zeroing it), and compact their spikes into ring slot t;
-//                         the remaining CTAs deliver the bundles due at step t into
-//                         acc[t & 1].
+//   step t (one launch):  CTAs [0, deliver_ctas) deliver the bundles due at step t into
+//                         acc[t & 1]; the remaining CTAs update one neuron per thread,
+//                         reading the input that arrived during step t-1 from
+//                         acc[(t-1) & 1] (and zeroing it), and compact their spikes into
+//                         ring slot t.  Delivery CTAs come first so the block scheduler
+//                         starts them with the first wave.
 //
 // Both halves run concurrently; the update of step t+1 sees exactly the value Brian2's
 // schedule produces (state after step t's update plus every effect of step t's synapses
@@ -138,27 +139,28 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
   allow_successor_launch();
   const PopDev& P = F.pop;
   const int64_t ts = clock[0] + k;
-  if ((int)blockIdx.x < F.neuron_ctas) {
-    // ---- neuron half: one neuron per thread
+  if ((int)blockIdx.x >= F.deliver_ctas) {
+    // ---- neuron half: one neuron per thread (scheduled after the delivery CTAs)
     const int slot = ring_slot(ts, P.ring_len);
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < P.n) {  // P.n is a multiple of the block size: whole warps take this branch
+    const int64_t nb = (int64_t)blockIdx.x - F.deliver_ctas;
+    const int64_t q = nb * blockDim.x + threadIdx.x;
+    if (q < P.n) {  // P.n is a multiple of 32: whole warps take this branch
       const bool spk = update_neuron<R, KIND>(F, q, (double)ts * dt, dt, (int)((ts & 1) ^ 1));
       warp_emit(P, spk, (int32_t)q, ts, slot, status);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
+    if (nb == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
     return;
   }
   // ---- delivery half: bundles due at step ts (spikes of steps ts - d, d >= 1) into acc[ts & 1]
-  const int64_t warp0 = ((int64_t)(blockIdx.x - F.neuron_ctas) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)(gridDim.x - F.neuron_ctas) * blockDim.x) >> 5;
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)F.deliver_ctas * blockDim.x) >> 5;
   const int par = (int)(ts & 1);
   for (int p = 0; p < F.n_proj; ++p) {
     const ProjDev& J = F.proj[p];
     R* T = static_cast<R*>(J.target) + (int64_t)par * P.n;
     const R* W = static_cast<const R*>(J.w);
     const R ws = (R)J.w_scalar;
-    for_each_due<WARP_PREFIX>(J, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+    for_each_due<WARP_PREFIX, 8>(J, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
       if (!valid) return;
       const int32_t post = __ldg(J.post + s);
       const R w = W ? __ldg(W + s) : ws;
@@ -209,6 +211,23 @@ size_t fused_smem(const FusedDev& F) {
 }
 
 int fused_block() { return kFusedBlock; }
+
+int fused_resident_ctas(int kind, int dtype, const FusedDev& F, int sms) {
+  const size_t smem = fused_smem(F);
+  const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
+  int occ = 0;
+#define B2B_OCC(R, KD, WP) \
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_step_kernel<R, KD, WP>, kFusedBlock, smem)
+  if (kind == KIND_HH) {
+    if (dtype == B2B_F32) { if (wp) B2B_OCC(float, KIND_HH, true); else B2B_OCC(float, KIND_HH, false); }
+    else { if (wp) B2B_OCC(double, KIND_HH, true); else B2B_OCC(double, KIND_HH, false); }
+  } else {
+    if (dtype == B2B_F32) { if (wp) B2B_OCC(float, KIND_LIF, true); else B2B_OCC(float, KIND_LIF, false); }
+    else { if (wp) B2B_OCC(double, KIND_LIF, true); else B2B_OCC(double, KIND_LIF, false); }
+  }
+#undef B2B_OCC
+  return occ * sms;
+}
 
 cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
                               const int64_t* clock, int k, double dt, int32_t* status,

@@ -68,7 +68,7 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   R* __restrict__ T = static_cast<R*>(P.target);
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+  for_each_due<WARP_PREFIX, 8>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
     const int32_t post = valid ? __ldg(P.post + s) : 0;
     R w = ws;
     if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
