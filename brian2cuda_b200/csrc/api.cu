@@ -441,6 +441,26 @@ b2b_status build_proj(b2b_net* net, int pj) {
   D.w = pr.w;
   D.w_scalar = net->syns[pr.members[0]].w_scalar;
   D.target = dst.dev.var[pr.target_var];
+  for (int v = 0; v < 3; ++v) D.targets[v] = dst.dev.var[v];
+  D.n_mem = 1;
+  if (pr.multi_target) {
+    std::vector<int64_t> hi;
+    std::vector<int8_t> var;
+    for (int m : pr.members) {
+      const Syn& sy = net->syns[m];
+      hi.push_back(net->groups[sy.pre_gid].offset + sy.pre_hi);
+      var.push_back((int8_t)sy.target_var);
+    }
+    int64_t* dhi = nullptr;
+    int8_t* dvar = nullptr;
+    CU(dalloc(pr, &dhi, hi.size()));
+    CU(dalloc(pr, &dvar, var.size()));
+    CU(cudaMemcpy(dhi, hi.data(), 8 * hi.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(dvar, var.data(), var.size(), cudaMemcpyHostToDevice));
+    D.n_mem = (int32_t)hi.size();
+    D.mem_hi = dhi;
+    D.mem_var = dvar;
+  }
   int64_t n_dst_valid = 0;
   for (int gi : dst.groups) n_dst_valid += net->groups[gi].n;
   D.aggregate = n_dst_valid < 64 ? 1 : 0;
@@ -482,9 +502,11 @@ b2b_status finalize_projs(b2b_net* net) {
     int pj = -1;
     for (size_t p = 0; p < net->projs.size() && pj < 0; ++p) {
       Proj& pr = net->projs[p];
-      if (pr.src_pop != gpre.pop || pr.dst_pop != gpost.pop || pr.target_var != sy.target_var ||
-          pr.effect != sy.effect)
+      // additive Synapses objects of one source population share a projection whatever
+      // their target variable (one spike ring walk); STDP ones need the same target
+      if (pr.src_pop != gpre.pop || pr.dst_pop != gpost.pop || pr.effect != sy.effect)
         continue;
+      if (sy.effect != B2B_EFFECT_ADD && pr.target_var != sy.target_var) continue;
       if (sy.effect == B2B_EFFECT_STDP && !same_stdp(net->syns[pr.members[0]].stdp, sy.stdp))
         continue;
       bool clash = false;
@@ -507,6 +529,7 @@ b2b_status finalize_projs(b2b_net* net) {
       pj = (int)net->projs.size() - 1;
     }
     Proj& pr = net->projs[pj];
+    if (pr.target_var != sy.target_var) pr.multi_target = true;
     pr.members.push_back((int)si);
     pr.dmin = std::min(pr.dmin, sy.dmin);
     pr.dmax = std::max(pr.dmax, sy.dmax);
@@ -550,7 +573,10 @@ b2b_status setup_fused(b2b_net* net) {
   int32_t nd_max = 1;
   for (const Proj& pr : net->projs) {
     if (pr.effect != B2B_EFFECT_ADD || pr.dmin < 1) return B2B_OK;
-    if (pr.target_var != B2B_VAR_GE && pr.target_var != B2B_VAR_GI) return B2B_OK;
+    for (int m : pr.members) {
+      const int v = net->syns[m].target_var;
+      if (v != B2B_VAR_GE && v != B2B_VAR_GI) return B2B_OK;
+    }
     nd_max = std::max(nd_max, pr.dev.nd);
   }
   FusedDev& F = net->fdev;
@@ -560,14 +586,18 @@ b2b_status setup_fused(b2b_net* net) {
   F.nd_max = nd_max;
   const size_t rs = real_size(pop.dtype);
   for (size_t p = 0; p < net->projs.size(); ++p) {
-    const int v = net->projs[p].target_var;
-    if (!F.acc[v]) {
-      CU(cudaMalloc(&F.acc[v], 2 * rs * pop.n));
-      net->fused_allocs.push_back(F.acc[v]);
-      CU(cudaMemset(F.acc[v], 0, 2 * rs * pop.n));
+    const Proj& pr = net->projs[p];
+    F.proj[p] = pr.dev;
+    for (int m : pr.members) {
+      const int v = net->syns[m].target_var;
+      if (!F.acc[v]) {
+        CU(cudaMalloc(&F.acc[v], 2 * rs * pop.n));
+        net->fused_allocs.push_back(F.acc[v]);
+        CU(cudaMemset(F.acc[v], 0, 2 * rs * pop.n));
+      }
+      F.proj[p].targets[v] = F.acc[v];
     }
-    F.proj[p] = net->projs[p].dev;
-    F.proj[p].target = F.acc[v];
+    F.proj[p].target = F.acc[pr.target_var];
   }
   const int block = fused_block();
   F.neuron_ctas = (int32_t)((pop.n + block - 1) / block);

@@ -74,7 +74,14 @@ struct ProjDev {
   const int32_t* post;            // [n_syn] target index in the target population
   const void* w;                  // [n_syn] weights or NULL
   double w_scalar;
-  void* target;                   // target variable array
+  void* target;                   // target variable array (all members share it: n_mem == 1)
+  // Members with different target variables (additive projections): member m covers
+  // presynaptic indices below mem_hi[m] and adds into targets[mem_var[m]].
+  int32_t n_mem;
+  int32_t pad_mem;
+  const int64_t* mem_hi;
+  const int8_t* mem_var;
+  void* targets[3];               // per variable v, ge, gi
   // STDP
   void* apre; void* apost; void* lastupdate;
   double taupre, taupost, dApre, dApost, wmin, wmax;
@@ -146,6 +153,7 @@ struct Syn {  // one user-level Synapses object
 
 struct Proj {
   int src_pop = -1, dst_pop = -1, target_var = 0, effect = 0, dtype = 0;
+  bool multi_target = false;                 // members add into different variables
   std::vector<int> members;                  // Syn ids, sorted by source range
   int32_t dmin = 0, dmax = 0;
   int64_t n_syn = 0;

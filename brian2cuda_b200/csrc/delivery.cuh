@@ -98,8 +98,8 @@ __device__ __forceinline__ int find_delay_block(const int* s_pref, int nd, int s
   return lo;
 }
 
-// Calls body(s, valid) for every synapse position s of every bundle of projection J due at
-// step ts.  Work items go to warps warp0, warp0 + nwarps, ...; inside a warp, groups of
+// Calls body(s, valid, pre) for every synapse position s of every bundle of projection J
+// due at step ts (pre: its presynaptic neuron).  Work items go to warps warp0, warp0 + nwarps, ...; inside a warp, groups of
 // GROUP lanes take one item each, so 32/GROUP items' dependent loads (spike index, bundle
 // offsets, synapse data) are in flight together.  All 32 lanes of a warp call body together
 // (valid marks real synapses).  WARP_PREFIX requires J.nd <= 64; otherwise every thread of
@@ -138,9 +138,10 @@ __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64
       di = find_delay_block(s_pref, J.nd, sp, &kk);
     }
     int64_t b0 = 0, b1 = 0;
+    int32_t pre = 0;
     if (have) {
       const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
-      const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
+      pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
       const int64_t key = (int64_t)pre * J.nd + di;
       b0 = J.off[key] + (int64_t)ch * kChunk;
       b1 = J.off[key + 1];
@@ -152,9 +153,21 @@ __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64
     for (int o = 16; o >= GROUP; o >>= 1) len = max(len, __shfl_xor_sync(kFull, len, o));
     for (int64_t off = 0; off < len; off += GROUP) {
       const int64_t s = b0 + off + glane;
-      body(s, s < b1);
+      body(s, s < b1, pre);
     }
   }
+}
+
+// Target array of presynaptic neuron pre in a projection whose members add into
+// different variables (binary search over the members' upper bounds).
+__device__ __forceinline__ void* member_target(const ProjDev& J, int32_t pre) {
+  if (J.n_mem <= 1) return J.target;
+  int lo = 0, hi = J.n_mem - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (pre < J.mem_hi[mid]) hi = mid; else lo = mid + 1;
+  }
+  return J.targets[J.mem_var[lo]];
 }
 
 }  // namespace b2b

@@ -157,14 +157,14 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
   const int par = (int)(ts & 1);
   for (int p = 0; p < F.n_proj; ++p) {
     const ProjDev& J = F.proj[p];
-    R* T = static_cast<R*>(J.target) + (int64_t)par * P.n;
     const R* W = static_cast<const R*>(J.w);
     const R ws = (R)J.w_scalar;
-    for_each_due<WARP_PREFIX, 8>(J, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+    for_each_due<WARP_PREFIX, 8>(J, ts, warp0, nwarps, s_pref,
+                                 [&](int64_t s, bool valid, int32_t pre) {
       if (!valid) return;
       const int32_t post = __ldg(J.post + s);
       const R w = W ? __ldg(W + s) : ws;
-      atomicAdd(T + post, w);
+      atomicAdd(static_cast<R*>(member_target(J, pre)) + (int64_t)par * P.n + post, w);
     });
   }
 }

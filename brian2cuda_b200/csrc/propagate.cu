@@ -65,13 +65,14 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   const int64_t ts = clock[0] + k;
   const R* __restrict__ W = static_cast<const R*>(P.w);
   const R ws = (R)P.w_scalar;
-  R* __restrict__ T = static_cast<R*>(P.target);
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for_each_due<WARP_PREFIX, 8>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+  for_each_due<WARP_PREFIX, 8>(P, ts, warp0, nwarps, s_pref,
+                               [&](int64_t s, bool valid, int32_t pre) {
     const int32_t post = valid ? __ldg(P.post + s) : 0;
     R w = ws;
     if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
+    R* T = static_cast<R*>(member_target(P, pre));
     add_to_target<R, AGG>(T, post, w, valid);
   });
 }
@@ -94,7 +95,7 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
   const R wmin = (R)P.wmin, wmax = (R)P.wmax;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid) {
+  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid, int32_t) {
     int32_t post = 0;
     R w = 0;
     if (valid) {
