@@ -194,8 +194,8 @@ def main():
     ap.add_argument("--ncu-case", type=int, default=0, metavar="STEPS",
                     help="profiling case: build the workload, simulate STEPS steps, print "
                          "nothing (for ncu captures of the step kernels)")
-    ap.add_argument("--per-step", action="store_true",
-                    help="use the per-step kernels even where one kernel per step applies")
+    ap.add_argument("--fused", action="store_true",
+                    help="run one kernel per step (neuron update and delivery side by side)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
 
@@ -215,7 +215,7 @@ def main():
     runs = args.warmup + 2 * args.steps + 1
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
-                  stream=stream.cuda_stream, fused=not args.per_step)
+                  stream=stream.cuda_stream, fused=args.fused)
     t_setup = time.perf_counter()
     ids = models.build_cobahh(net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
                               monitor_capacity=mon_cap)

@@ -565,7 +565,7 @@ b2b_status finalize_projs(b2b_net* net) {
 // One kernel per step (fused.cu) applies when the net is one LIF/HH population whose
 // synapses are all additive onto ge/gi of that population with delays of at least one step.
 b2b_status setup_fused(b2b_net* net) {
-  if (net->cfg.flags & B2B_NET_NO_FUSED) return B2B_OK;
+  if (!(net->cfg.flags & B2B_NET_FUSED)) return B2B_OK;
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
     return B2B_OK;
   const Pop& pop = net->pops[0];

@@ -140,16 +140,17 @@ class Network:
 
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
-                 stream: int | None = None, fused: bool = True):
+                 stream: int | None = None, fused: bool = False):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
-        default the network creates its own non-blocking stream."""
+        default the network creates its own non-blocking stream.  `fused`: run one kernel per
+        step (neuron update and delivery side by side) where the net allows it."""
         self._lib = N.lib()
         self.dt = float(dt)
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
         if reset_before_synapses:
             flags |= N.NET_RESET_BEFORE_SYNAPSES
-        if not fused:
-            flags |= N.NET_NO_FUSED
+        if fused:
+            flags |= N.NET_FUSED
         cfg = N.Config(self.dt, device, steps_per_graph, seed, stream, flags, 0)
         h = C.c_void_p()
         st = self._lib.b2b_create(C.byref(cfg), C.byref(h))

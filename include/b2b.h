@@ -59,9 +59,9 @@ enum {
   B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
-  B2B_NET_NO_FUSED = 8    /* never run one kernel per step (neuron update and delivery side
-                             by side), which a net with one population, additive synapses
-                             onto ge/gi and all delays >= 1 step otherwise uses          */
+  B2B_NET_FUSED = 8       /* run one kernel per step (neuron update and delivery side by
+                             side) when the net has one population, additive synapses onto
+                             ge/gi and all delays >= 1 step; otherwise per-step kernels  */
 };
 
 typedef struct {

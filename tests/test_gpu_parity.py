@@ -297,7 +297,7 @@ def test_fused_and_per_step_paths_agree(gpu_factory):
 def test_fused_cobahh_float32_matches_oracle(gpu_factory, oracle_factory):
     out = {}
     for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
-        net = make(DT, f32=True) if name == "orc" else make(DT)
+        net = make(DT, f32=True) if name == "orc" else make(DT, fused=True)
         ids = models.build_cobahh(net, n=3000, p=0.02, generated=False, monitor_capacity=10**6)
         net.finalize()
         if name == "gpu":
