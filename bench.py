@@ -314,7 +314,7 @@ def main():
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     # algorithmic bytes per launch of each launch site the profiler reports
     site_info = {1: ("neuron (HH update+threshold+compaction)", "hh_step_kernel"),
-                 2: ("delivery on_pre", "deliver_add_kernel"),
+                 2: ("delivery on_pre", "deliver_add_batch_kernel"),
                  5: ("fused step (HH update + delivery, one kernel)", "fused_step_kernel")}
     kernel_ms, per_launch_bytes, kernels = {}, [], []
     n_deliver = 0
