@@ -85,6 +85,8 @@ PROTOTYPES = {
     "b2b_synapses": (I32, [P, I32, I32, I32, I32, I64, P, P, P, DBL, P, I32,
                            C.POINTER(StdpParams), PI32]),
     "b2b_synapses_random": (I32, [P, I32, I32, I32, I32, I32, DBL, I32, I32, DBL, U64, PI32]),
+    "b2b_connect_random_static": (I32, [I32, P, I32, I32, I32, DBL, I32, I32, U64, P, P, P, I64,
+                                        PI64]),
     "b2b_syn_count": (I32, [P, I32, PI64]),
     "b2b_syn_get": (I32, [P, I32, I32, P, I64]),
     "b2b_finalize": (I32, [P]),
