@@ -112,7 +112,22 @@ PROTOTYPES = {
     "b2b_hines_run": (I32, [P, I64]),
     "b2b_hines_spike_counts": (I32, [P, P, I32]),
     "b2b_hines_destroy": (I32, [P]),
+    "b2b_mlp_create": (I32, [I32, P, U64, C.POINTER(P)]),
+    "b2b_mlp_destroy": (I32, [P]),
+    "b2b_mlp_params_get": (I32, [P, P, I64]),
+    "b2b_mlp_params_set": (I32, [P, P, I64]),
+    "b2b_mlp_scaling_get": (I32, [P, P]),
+    "b2b_mlp_scaling_set": (I32, [P, P]),
+    "b2b_mlp_fit_scaling": (I32, [P, P, P, I64]),
+    "b2b_mlp_forward": (I32, [P, P, P, I64, I32]),
+    "b2b_mlp_grad": (I32, [P, P, P, I64, P, I64, C.POINTER(DBL)]),
+    "b2b_mlp_train": (I32, [P, P, P, I64, I32, I32, DBL, P]),
+    "b2b_hh_gating_exact": (I32, [C.POINTER(HhParams), DBL, P, P, I64, I32, P]),
+    "b2b_hh_gating_sample": (I32, [P, I32, P, I64]),
+    "b2b_group_hh_surrogate": (I32, [P, I32, P, DBL, I32]),
+    "b2b_surrogate_stats": (I32, [P, I32, PI64, PI64]),
 }
+MLP_NPARAMS = 4675
 
 _lib = None
 

@@ -253,6 +253,27 @@ b2b_status finalize_pops(b2b_net* net) {
       CU(cudaMemcpy(pop.params_dev, prm.data(), prm.size(), cudaMemcpyHostToDevice));
       D.params = pop.params_dev;
     }
+    // gating surrogate: every HH group of a float32 population shares one network
+    if (pop.kind == KIND_HH) {
+      const Group& g0 = net->groups[pop.groups[0]];
+      bool any = false;
+      for (int gi : pop.groups) {
+        const Group& g = net->groups[gi];
+        any = any || g.surr;
+        CHECK(g.surr == g0.surr && g.surr_tol == g0.surr_tol && g.surr_judge == g0.surr_judge,
+              B2B_ERR_UNSUPPORTED, "HH groups of one population must share one surrogate");
+      }
+      if (any) {
+        CHECK(pop.dtype == B2B_F32, B2B_ERR_UNSUPPORTED, "the gating surrogate is float32 only");
+        CHECK(mlp_device(g0.surr) == net->cfg.device, B2B_ERR_INVALID_ARG,
+              "surrogate and net are on different devices");
+        pop.surr_img = mlp_image(g0.surr);
+        pop.surr_tol = (float)g0.surr_tol;
+        pop.surr_judge = g0.surr_judge;
+        CU(dalloc(pop, &pop.surr_cnt, 2));
+        CU(cudaMemset(pop.surr_cnt, 0, 2 * sizeof(unsigned long long)));
+      }
+    }
     if (pop.groups.size() > 1) {
       std::vector<int32_t> vg(pop.n / 4, (int32_t)pop.groups.size() - 1);
       for (size_t k = 0; k < pop.groups.size(); ++k) {
@@ -570,6 +591,7 @@ b2b_status setup_fused(b2b_net* net) {
     return B2B_OK;
   const Pop& pop = net->pops[0];
   if (pop.kind != KIND_LIF && pop.kind != KIND_HH) return B2B_OK;
+  if (pop.surr_img) return B2B_OK;
   int32_t nd_max = 1;
   for (const Proj& pr : net->projs) {
     if (pr.effect != B2B_EFFECT_ADD || pr.dmin < 1) return B2B_OK;
@@ -813,6 +835,56 @@ b2b_status b2b_group_hh(b2b_net* net, int64_t n, int32_t dtype, const b2b_hh_par
   g.kind = KIND_HH; g.n = n; g.dtype = dtype; g.hh = *p;
   return add_group(net, std::move(g), gid);
   GUARD_END
+}
+
+b2b_status b2b_group_hh_surrogate(b2b_net* net, int32_t gid, b2b_mlp* m, double tol,
+                                  int32_t judge) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "attach the surrogate before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int32_t)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group id");
+  CHECK(m != nullptr && tol >= 0 && std::isfinite(tol) && (judge == 0 || judge == 1),
+        B2B_ERR_INVALID_ARG, "bad surrogate arguments");
+  Group& g0 = net->groups[gid];
+  CHECK(g0.kind == KIND_HH && g0.dtype == B2B_F32, B2B_ERR_UNSUPPORTED,
+        "the gating surrogate applies to float32 HH groups");
+  for (Group& g : net->groups) {
+    if (g.kind != KIND_HH || g.dtype != B2B_F32) continue;
+    g.surr = m;
+    g.surr_tol = tol;
+    g.surr_judge = judge;
+  }
+  return B2B_OK;
+}
+
+b2b_status b2b_surrogate_stats(b2b_net* net, int32_t gid, int64_t* updates, int64_t* fallbacks) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(gid >= 0 && gid < (int32_t)net->groups.size() && updates && fallbacks,
+        B2B_ERR_INVALID_ARG, "bad arguments");
+  const Pop& pop = net->pops[net->groups[gid].pop];
+  CHECK(pop.surr_cnt != nullptr, B2B_ERR_STATE, "no surrogate attached to this group");
+  unsigned long long c[2] = {0, 0};
+  CU(cudaMemcpyAsync(c, pop.surr_cnt, sizeof c, cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaStreamSynchronize(net->stream));
+  *updates = (int64_t)c[0];
+  *fallbacks = (int64_t)c[1];
+  return B2B_OK;
+}
+
+b2b_status b2b_hh_gating_sample(b2b_net* net, int32_t gid, float* dev_x, int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(gid >= 0 && gid < (int32_t)net->groups.size() && dev_x != nullptr, B2B_ERR_INVALID_ARG,
+        "bad arguments");
+  CHECK((reinterpret_cast<uintptr_t>(dev_x) & 15) == 0, B2B_ERR_INVALID_ARG,
+        "dev_x must be 16-byte aligned");
+  const Group& g = net->groups[gid];
+  CHECK(g.kind == KIND_HH && g.dtype == B2B_F32, B2B_ERR_UNSUPPORTED,
+        "sampling applies to float32 HH groups");
+  CHECK(n >= 0 && n <= g.n, B2B_ERR_INVALID_ARG, "n exceeds the group size");
+  if (n == 0) return B2B_OK;
+  CU(launch_hh_sample(net->pops[g.pop], g.offset, n, dev_x, net->stream));
+  return B2B_OK;
 }
 
 b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate_hz,

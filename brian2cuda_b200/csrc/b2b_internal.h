@@ -118,6 +118,9 @@ struct Group {
   std::vector<int64_t> sg_step;
   std::vector<std::vector<uint8_t>> staged;   // per var host bytes staged before finalize
   int64_t mon_cap = 0;
+  b2b_mlp* surr = nullptr;                    // gating surrogate (HH float32), or none
+  double surr_tol = 0;
+  int32_t surr_judge = 1;
 };
 
 struct Pop {
@@ -132,6 +135,11 @@ struct Pop {
   void* rng_buf = nullptr;
   bool late_reset = false;
   int max_delay = 0;
+  // gating surrogate of a float32 HH population (surrogate.cu), or none
+  const void* surr_img = nullptr;
+  unsigned long long* surr_cnt = nullptr;     // [0] neuron-updates, [1] exact fallbacks
+  float surr_tol = 0.f;
+  int32_t surr_judge = 1;
 };
 
 struct Syn {  // one user-level Synapses object
@@ -219,6 +227,15 @@ cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
                                   cudaStream_t s);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
+// COBAHH step of a population with a gating surrogate attached (surrogate.cu).
+cudaError_t launch_hh_surrogate(const Pop& pop, const int64_t* clock, int k, double dt,
+                                int32_t* status, cudaStream_t s);
+// (v, m, h, n) rows of neurons [off, off + n) of a float32 HH population.
+cudaError_t launch_hh_sample(const Pop& pop, int64_t off, int64_t n, float* dev_x,
+                             cudaStream_t s);
+// Packed device image and device ordinal of a surrogate network.
+const void* mlp_image(const b2b_mlp* m);
+int mlp_device(const b2b_mlp* m);
 // One kernel per step (fused.cu): the step itself, and the fold of the pending input.
 size_t fused_smem(const FusedDev& F);
 int fused_block();

@@ -15,102 +15,11 @@
 // variable the reset writes; otherwise `late_reset` defers it to a kernel that runs after
 // the synaptic delivery, preserving Brian2's schedule (groups, thresholds, synapses,
 // resets).
-#include "neuron_math.cuh"
+#include "neuron_common.cuh"
 
 namespace b2b {
 
 namespace {
-
-template <typename R, int E>
-struct Pack {
-  R x[E];
-};
-
-// Loads/stores the E values of thread q from one state array (vectorised for E = 4).
-template <typename R, int E>
-__device__ __forceinline__ Pack<R, E> load_pack(const void* base, int64_t q) {
-  Pack<R, E> r;
-  if constexpr (E == 1) {
-    r.x[0] = static_cast<const R*>(base)[q];
-  } else if constexpr (sizeof(R) == 4) {
-    float4 a = reinterpret_cast<const float4*>(base)[q];
-    r.x[0] = a.x; r.x[1] = a.y; r.x[2] = a.z; r.x[3] = a.w;
-  } else {
-    const double2* p = reinterpret_cast<const double2*>(base) + 2 * q;
-    double2 a = p[0], b = p[1];
-    r.x[0] = a.x; r.x[1] = a.y; r.x[2] = b.x; r.x[3] = b.y;
-  }
-  return r;
-}
-
-template <typename R, int E>
-__device__ __forceinline__ void store_pack(void* base, int64_t q, const Pack<R, E>& r) {
-  if constexpr (E == 1) {
-    static_cast<R*>(base)[q] = r.x[0];
-  } else if constexpr (sizeof(R) == 4) {
-    reinterpret_cast<float4*>(base)[q] = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
-  } else {
-    double2* p = reinterpret_cast<double2*>(base) + 2 * q;
-    p[0] = make_double2(r.x[0], r.x[1]);
-    p[1] = make_double2(r.x[2], r.x[3]);
-  }
-}
-
-template <int E>
-__device__ __forceinline__ void store_flags(void* base, int64_t q, uint32_t packed) {
-  if constexpr (E == 1) static_cast<uint8_t*>(base)[q] = (uint8_t)packed;
-  else reinterpret_cast<uint32_t*>(base)[q] = packed;
-}
-
-// Group-parameter index of thread q (the table holds one entry per 4 neurons).
-template <int E>
-__device__ __forceinline__ int group_of(const PopDev& P, int64_t q) {
-  if (!P.vec_group) return 0;
-  return P.vec_group[E == 4 ? q : (q >> 2)];
-}
-
-// Writes the spikes flagged in `fl` (bit e = neuron E*q+e) into the ring slot and the spike
-// monitor.  Every thread of the CTA must call this (it synchronises the block).
-template <int E>
-__device__ __forceinline__ void emit_spikes(const PopDev& P, int64_t q, unsigned fl,
-                                            int64_t ts, int slot, int32_t* status) {
-  __shared__ int s_warp[33];
-  __shared__ int s_base;
-  __shared__ unsigned long long s_mbase;
-  int total;
-  const int c = __popc(fl);
-  const int excl = block_exclusive_scan(c, s_warp, &total);
-  if (threadIdx.x == 0 && total > 0) {
-    s_base = atomicAdd(&P.ring_cnt[slot], total);
-    if (P.mon_cnt) s_mbase = atomicAdd(P.mon_cnt, (unsigned long long)total);
-  }
-  __syncthreads();
-  if (total == 0 || c == 0) return;
-  int32_t* out = P.ring_idx + (int64_t)slot * P.n;
-  int pos = s_base + excl;
-  unsigned long long mpos = P.mon_cnt ? s_mbase + excl : 0;
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    if (fl & (1u << e)) {
-      const int32_t idx = (int32_t)(E * q + e);
-      out[pos++] = idx;
-      if (P.mon_cnt) {
-        if (mpos < (unsigned long long)P.mon_cap) {
-          P.mon_idx[mpos] = idx;
-          P.mon_step[mpos] = ts;
-        } else {
-          set_status(status, B2B_ERR_QUEUE_OVERFLOW);
-        }
-        ++mpos;
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ void clear_next_slot(const PopDev& P, int64_t ts) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
-}
-
 // ---- LIF, exact integration ------------------------------------------------------------
 template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
@@ -332,6 +241,7 @@ cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int
 
 cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
                             int32_t* status, cudaStream_t s) {
+  if (pop.kind == KIND_HH && pop.surr_img) return launch_hh_surrogate(pop, clock, k, dt, status, s);
   if (pop.kind == KIND_SPIKEGEN) {
     spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
     return cudaGetLastError();

@@ -29,13 +29,11 @@ __device__ __forceinline__ R expeuler(R x, R A, R B, R dt) {
   return -BA + (BA + x) * dexp(A * dt);
 }
 
-// COBAHH (examples/cobahh.py:159-180) over one dt: rates in SI units, the three of the form
-// x/(exp(x/a) - 1) through z/expm1(z) (see z_over_expm1); every right-hand side uses the
-// values at the start of the step.  Returns the new v; advances m, h, n, ge, gi in place.
+// Gating part of the COBAHH update (examples/cobahh.py:159-180): the exponential-Euler step
+// of m, h, n over one dt at membrane potential v.  Rates in SI units; the three of the form
+// x/(exp(x/a) - 1) go through z/expm1(z) (see z_over_expm1).
 template <typename R>
-__device__ __forceinline__ R hh_advance(const HhDev& g, R v, R& m, R& h, R& n, R& ge, R& gi,
-                                        R dt) {
-  const R VT = (R)g.VT;
+__device__ __forceinline__ void hh_gating(R VT, R v, R& m, R& h, R& n, R dt) {
   // 0.32/mV*(13mV-v+VT)/(exp((13mV-v+VT)/4mV)-1)/ms = 1280 * z/expm1(z), z = (..)/4mV
   const R am = (R)1280 * z_over_expm1(((R)13e-3 - v + VT) / (R)4e-3);
   const R bm = (R)1400 * z_over_expm1((v - VT - (R)40e-3) / (R)5e-3);
@@ -43,15 +41,30 @@ __device__ __forceinline__ R hh_advance(const HhDev& g, R v, R& m, R& h, R& n, R
   const R bh = (R)4000 / ((R)1 + dexp(((R)40e-3 - v + VT) / (R)5e-3));
   const R an = (R)160 * z_over_expm1(((R)15e-3 - v + VT) / (R)5e-3);
   const R bn = (R)500 * dexp(((R)10e-3 - v + VT) / (R)40e-3);
+  m = expeuler(m, -(am + bm), am, dt);
+  h = expeuler(h, -(ah + bh), ah, dt);
+  n = expeuler(n, -(an + bn), an, dt);
+}
+
+// Membrane part of the COBAHH update: exponential Euler for v with the conductances of the
+// gating state at the start of the step.  Returns the new v.
+template <typename R>
+__device__ __forceinline__ R hh_membrane(const HhDev& g, R v, R m, R h, R n, R ge, R gi, R dt) {
   const R gl = (R)g.gl, Cm = (R)g.Cm;
   const R gna = (R)g.gNa * (m * m * m) * h;
   const R gk = (R)g.gK * (n * n * n * n);
   const R Av = -(gl + ge + gi + gna + gk) / Cm;
   const R Bv = (gl * (R)g.El + ge * (R)g.Ee + gi * (R)g.Ei + gna * (R)g.ENa + gk * (R)g.EK) / Cm;
-  const R vn = expeuler(v, Av, Bv, dt);
-  m = expeuler(m, -(am + bm), am, dt);
-  h = expeuler(h, -(ah + bh), ah, dt);
-  n = expeuler(n, -(an + bn), an, dt);
+  return expeuler(v, Av, Bv, dt);
+}
+
+// COBAHH over one dt: every right-hand side uses the values at the start of the step.
+// Returns the new v; advances m, h, n, ge, gi in place.
+template <typename R>
+__device__ __forceinline__ R hh_advance(const HhDev& g, R v, R& m, R& h, R& n, R& ge, R& gi,
+                                        R dt) {
+  const R vn = hh_membrane<R>(g, v, m, h, n, ge, gi, dt);
+  hh_gating<R>((R)g.VT, v, m, h, n, dt);
   ge = (R)g.De * ge;
   gi = (R)g.Di * gi;
   return vn;

@@ -306,6 +306,59 @@ b2b_status b2b_hines_run(b2b_hines* h, int64_t n_steps);
 b2b_status b2b_hines_spike_counts(b2b_hines* h, int32_t* host, int32_t n);
 b2b_status b2b_hines_destroy(b2b_hines* h);
 
+/* ---- gating surrogate (no counterpart in the reference) ------------------------------------
+ * A 4 -> 64 -> 64 -> 3 perceptron (tanh hidden units, BF16 weights and activations, FP32
+ * accumulation on the sm_100a tensor cores) that predicts the exponential-Euler step of the
+ * COBAHH gating variables (m, h, n) over one dt from (v, m, h, n).  brian2cuda integrates the
+ * gates only with the code Brian2 generates for method='exponential_euler'
+ * (examples/cobahh.py:159-180); that integrator stays here as the fallback and the judge.
+ * Samples are float32 rows (v, m, h, n) in SI units; targets and predictions are rows
+ * (m', h', n').  The network computes y = W3 tanh(W2 tanh(W1 xh + b1) + b2) + b3 with
+ * xh = ((v, m, h, n) - in_shift) * in_scale and predicts clip(x + out_scale * y, 0, 1). */
+typedef struct b2b_mlp b2b_mlp;
+#define B2B_MLP_NPARAMS 4675  /* W1[64][4], b1[64], W2[64][64], b2[64], W3[3][64], b3[3] */
+
+/* Creates a network with seeded Xavier-uniform weights and zero biases on `device`; all its
+ * work runs on `stream` (a cudaStream_t, or NULL for one it owns). */
+b2b_status b2b_mlp_create(int32_t device, void* stream, uint64_t seed, b2b_mlp** out);
+b2b_status b2b_mlp_destroy(b2b_mlp* m);
+/* fp32 master parameters, B2B_MLP_NPARAMS values in the order above. */
+b2b_status b2b_mlp_params_get(b2b_mlp* m, float* host, int64_t n);
+b2b_status b2b_mlp_params_set(b2b_mlp* m, const float* host, int64_t n);
+/* Input/output scaling: 11 floats in_shift[4], in_scale[4], out_scale[3]. */
+b2b_status b2b_mlp_scaling_get(b2b_mlp* m, float* host11);
+b2b_status b2b_mlp_scaling_set(b2b_mlp* m, const float* host11);
+/* Sets the scaling from a dataset: v's range maps to [-1, 1], m/h/n's [0, 1] to [-1, 1],
+ * out_scale = the largest |target - input| per gate. */
+b2b_status b2b_mlp_fit_scaling(b2b_mlp* m, const float* dev_x, const float* dev_t, int64_t n);
+/* n predictions (raw = 0: clip(x + out_scale * y, 0, 1); raw = 1: the outputs y). */
+b2b_status b2b_mlp_forward(b2b_mlp* m, const float* dev_x, float* dev_out, int64_t n,
+                           int32_t raw);
+/* Gradient of the mean loss mean_s sum_o (y_o - (t_o - x_o)/out_scale_o)^2 over the n
+ * samples, in parameter order, and the loss itself. */
+b2b_status b2b_mlp_grad(b2b_mlp* m, const float* dev_x, const float* dev_t, int64_t n,
+                        float* host_grad, int64_t n_grad, double* loss);
+/* Adam (beta 0.9/0.999) with a cosine-decayed learning rate over `epochs` passes of
+ * minibatches of `batch` samples (a multiple of 128) in a fresh pseudo-random order per
+ * epoch; loss_per_epoch (epochs values, or NULL) receives each epoch's mean loss. */
+b2b_status b2b_mlp_train(b2b_mlp* m, const float* dev_x, const float* dev_t, int64_t n,
+                         int32_t epochs, int32_t batch, double lr, double* loss_per_epoch);
+/* Training targets: the exact exponential-Euler gating step (the kernel's own integrator) of
+ * n samples for the COBAHH parameters p and time step dt, on `stream` of `device`. */
+b2b_status b2b_hh_gating_exact(const b2b_hh_params* p, double dt, const float* dev_x,
+                               float* dev_t, int64_t n, int32_t device, void* stream);
+/* Copies (v, m, h, n) of the first n neurons of float32 HH group gid into dev_x (device rows
+ * of 4 floats), on the net's stream: trajectory samples for training. */
+b2b_status b2b_hh_gating_sample(b2b_net* net, int32_t gid, float* dev_x, int64_t n);
+/* Steps every HH group of gid's (float32) population with the surrogate's gating update
+ * (before b2b_finalize; m must outlive the net).  A neuron is re-stepped exactly when its v
+ * lies outside the range the scaling maps to [-1, 1], or, with judge = 1, when a predicted
+ * gate differs from the exact update by more than tol. */
+b2b_status b2b_group_hh_surrogate(b2b_net* net, int32_t gid, b2b_mlp* m, double tol,
+                                  int32_t judge);
+/* Neuron-updates made with the surrogate attached and how many of them fell back. */
+b2b_status b2b_surrogate_stats(b2b_net* net, int32_t gid, int64_t* updates, int64_t* fallbacks);
+
 #ifdef __cplusplus
 }
 #endif
