@@ -118,7 +118,7 @@ LifDev lif_dev(const Group& g, double dt) {
 HhDev hh_dev(const Group& g, double dt) {
   const b2b_hh_params& p = g.hh;
   HhDev d{};
-  d.Cm = p.Cm; d.gl = p.gl; d.El = p.El; d.EK = p.EK; d.ENa = p.ENa; d.gNa = p.gNa;
+  d.Cm = p.Cm; d.inv_Cm = 1.0 / p.Cm; d.gl = p.gl; d.El = p.El; d.EK = p.EK; d.ENa = p.ENa; d.gNa = p.gNa;
   d.gK = p.gK; d.VT = p.VT; d.Ee = p.Ee; d.Ei = p.Ei;
   d.De = p.taue > 0 ? std::exp(-dt / p.taue) : 0.0;
   d.Di = p.taui > 0 ? std::exp(-dt / p.taui) : 0.0;

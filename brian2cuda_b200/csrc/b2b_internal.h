@@ -33,6 +33,7 @@ struct HhDev {
   double Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr;
   int64_t ref_steps;
   int64_t offset, n;
+  double inv_Cm;                          // 1/Cm (the float32 update multiplies by it)
 };
 struct PoissonDev {
   double p_spike;                         // rate * dt

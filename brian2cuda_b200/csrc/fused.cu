@@ -70,7 +70,7 @@ __device__ __forceinline__ void warp_emit(const PopDev& P, bool spk, int32_t q, 
 // Neuron q of step ts: fold the pending input, integrate, threshold, reset.
 template <typename R, int KIND>
 __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, double t, double dt,
-                                              int prev) {
+                                              double inv_dt, int prev) {
   const PopDev& P = F.pop;
   const int gidx = P.vec_group ? P.vec_group[q >> 2] : 0;
   R* V = static_cast<R*>(P.var[B2B_VAR_V]);
@@ -94,7 +94,7 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
     const HhDev g = static_cast<const HhDev*>(P.params)[gidx];  // by value: no reloads
     const bool refr = g.ref_steps >= 0;
     bool nr = true;
-    if (refr) nr = timestep_of(t - (double)LS[q], dt) >= g.ref_steps;
+    if (refr) nr = timestep_of(t - (double)LS[q], dt, inv_dt) >= g.ref_steps;
     R* M = static_cast<R*>(P.var[B2B_VAR_M]);
     R* H = static_cast<R*>(P.var[B2B_VAR_H]);
     R* N = static_cast<R*>(P.var[B2B_VAR_N]);
@@ -114,7 +114,7 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
     const LifDev g = static_cast<const LifDev*>(P.params)[gidx];  // by value: no reloads
     const bool refr = g.ref_steps >= 0;
     bool nr = true;
-    if (refr) nr = timestep_of(t - (double)LS[q], dt) >= g.ref_steps;
+    if (refr) nr = timestep_of(t - (double)LS[q], dt, inv_dt) >= g.ref_steps;
     R vn = lif_advance<R>(g, V[q], ge, gi, nr);
     if (g.has_threshold && (q - g.offset) < g.n && vn > (R)g.Vt && nr) {
       nr = false;
@@ -145,7 +145,8 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
     const int64_t nb = (int64_t)blockIdx.x - F.deliver_ctas;
     const int64_t q = nb * blockDim.x + threadIdx.x;
     if (q < P.n) {  // P.n is a multiple of 32: whole warps take this branch
-      const bool spk = update_neuron<R, KIND>(F, q, (double)ts * dt, dt, (int)((ts & 1) ^ 1));
+      const bool spk = update_neuron<R, KIND>(F, q, (double)ts * dt, dt, 1.0 / dt,
+                                              (int)((ts & 1) ^ 1));
       warp_emit(P, spk, (int32_t)q, ts, slot, status);
     }
     if (nb == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;

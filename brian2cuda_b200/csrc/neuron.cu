@@ -15,6 +15,8 @@
 // variable the reset writes; otherwise `late_reset` defers it to a kernel that runs after
 // the synaptic delivery, preserving Brian2's schedule (groups, thresholds, synapses,
 // resets).
+#include <algorithm>
+
 #include "neuron_common.cuh"
 
 namespace b2b {
@@ -27,6 +29,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                 int32_t* status) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
+  const double inv_dt = 1.0 / dt;
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t nthr = P.n / E;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -46,7 +49,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     for (int e = 0; e < E; ++e) {
       R ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
-      if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
+      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
       R vn = lif_advance<R>(g, V.x[e], ge, gi, nr);
       GE.x[e] = ge;
       GI.x[e] = gi;
@@ -79,6 +82,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                int32_t* status) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
+  const double inv_dt = 1.0 / dt;
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t nthr = P.n / E;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -100,7 +104,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       bool nr = true;
-      if (refr) nr = timestep_of(t - (double)LS.x[e], dt) >= g.ref_steps;
+      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
       const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR);
       const bool valid = (E * q + e - g.offset) < g.n;
       if (valid && vn > Vthr && nr) {
@@ -123,6 +127,85 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     }
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
+  clear_next_slot(P, ts);
+}
+
+// Large HH populations: a persistent grid (resident CTAs only) walks the population in
+// strides, and every thread loads the state of its next four neurons before it updates the
+// current four, so the loads of one pack overlap the arithmetic of the previous one.  The
+// per-neuron arithmetic is hh_step_kernel's.
+template <typename R>
+struct HhPack {
+  Pack<R, 4> V, M, H, N, GE, GI, LS;
+  int grp;
+};
+
+template <typename R>
+__device__ __forceinline__ void hh_pack_load(const PopDev& P, const HhDev* prm, int64_t q,
+                                             HhPack<R>& s) {
+  s.grp = group_of<4>(P, q);
+  s.V = load_pack<R, 4>(P.var[B2B_VAR_V], q);
+  s.M = load_pack<R, 4>(P.var[B2B_VAR_M], q);
+  s.H = load_pack<R, 4>(P.var[B2B_VAR_H], q);
+  s.N = load_pack<R, 4>(P.var[B2B_VAR_N], q);
+  s.GE = load_pack<R, 4>(P.var[B2B_VAR_GE], q);
+  s.GI = load_pack<R, 4>(P.var[B2B_VAR_GI], q);
+  if (prm[s.grp].ref_steps >= 0) s.LS = load_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock, 2)
+hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
+                 int32_t* status) {
+  const int64_t ts = clock[0] + k;
+  const double t = (double)ts * dt;
+  const double inv_dt = 1.0 / dt;
+  const int slot = ring_slot(ts, P.ring_len);
+  const int64_t nthr = P.n / 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t iters = (nthr + stride - 1) / stride;   // the same for every thread
+  const HhDev* prm = static_cast<const HhDev*>(P.params);
+  const R dtR = (R)dt;
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  HhPack<R> cur;
+  if (q < nthr) hh_pack_load<R>(P, prm, q, cur);
+  for (int64_t it = 0; it < iters; ++it, q += stride) {
+    HhPack<R> nxt;
+    if (q + stride < nthr) hh_pack_load<R>(P, prm, q + stride, nxt);
+    unsigned fl = 0;
+    if (q < nthr) {
+      const HhDev g = prm[cur.grp];
+      const bool refr = g.ref_steps >= 0;
+      uint32_t NRout = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        bool nr = true;
+        if (refr) nr = timestep_of(t - (double)cur.LS.x[e], dt, inv_dt) >= g.ref_steps;
+        const R vn = hh_advance<R>(g, cur.V.x[e], cur.M.x[e], cur.H.x[e], cur.N.x[e],
+                                   cur.GE.x[e], cur.GI.x[e], dtR);
+        const bool valid = (4 * q + e - g.offset) < g.n;
+        if (valid && vn > (R)g.Vthr && nr) {
+          nr = false;
+          if (refr) cur.LS.x[e] = (R)t;
+          fl |= 1u << e;
+        }
+        cur.V.x[e] = vn;
+        NRout |= (nr ? 1u : 0u) << (8 * e);
+      }
+      store_pack<R, 4>(P.var[B2B_VAR_V], q, cur.V);
+      store_pack<R, 4>(P.var[B2B_VAR_M], q, cur.M);
+      store_pack<R, 4>(P.var[B2B_VAR_H], q, cur.H);
+      store_pack<R, 4>(P.var[B2B_VAR_N], q, cur.N);
+      store_pack<R, 4>(P.var[B2B_VAR_GE], q, cur.GE);
+      store_pack<R, 4>(P.var[B2B_VAR_GI], q, cur.GI);
+      if (refr) {
+        store_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q, cur.LS);
+        store_flags<4>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
+      }
+    }
+    emit_spikes<4>(P, q, fl, ts, slot, status);
+    cur = nxt;
+  }
   clear_next_slot(P, ts);
 }
 
@@ -224,8 +307,16 @@ cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int
       else lif_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
       break;
     case KIND_HH:
-      if (f32) hh_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
-      else hh_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      if (E == 4 && f32) {
+        // resident CTAs only (2 per SM by the launch bounds); float64 keeps one pack per
+        // thread (two packs of doubles do not fit the register budget)
+        const unsigned g2 = std::min<unsigned>(grid, 2 * kNumSMs);
+        hh_stream_kernel<float><<<g2, kBlock, 0, s>>>(P, clock, k, dt, status);
+      } else if (f32) {
+        hh_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      } else {
+        hh_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      }
       break;
     case KIND_POISSON:
       if (f32) poisson_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, status);

@@ -5,9 +5,12 @@
 
 namespace b2b {
 
-// Brian2's `timestep(t, dt)` (brian2cuda/cuda_generator.py:997-1006).
-__device__ __forceinline__ int64_t timestep_of(double t, double dt) {
-  return (int64_t)((t + 1e-3 * dt) / dt);
+// Brian2's `timestep(t, dt)` = (int64)((t + 1e-3 dt) / dt) (brian2cuda/cuda_generator.py:
+// 997-1006), with the division replaced by a product with inv_dt = 1/dt: the quotient is an
+// integer plus 1e-3 (plus the rounding of a float32 lastspike, below 1e-3 of a step for
+// t < 100 s), so the one-ulp difference between the two forms never changes the truncation.
+__device__ __forceinline__ int64_t timestep_of(double t, double dt, double inv_dt) {
+  return (int64_t)((t + 1e-3 * dt) * inv_dt);
 }
 
 // Exact propagator of dv/dt = (El - v + ke ge + ki gi)/taum, dge/dt = -ge/taue,
@@ -22,39 +25,71 @@ __device__ __forceinline__ R lif_advance(const LifDev& g, R v, R& ge, R& gi, boo
   return vn;
 }
 
+// Arithmetic of the COBAHH update.  float64 keeps the correctly rounded library forms.
+// float32 uses the hardware units: exp through ex2 (__expf, relative error ~1e-6 for the
+// |x| <= 25 the rates reach), division through the reciprocal unit (__fdividef, 2 ulp), and
+// division by a literal constant as multiplication by its rounded reciprocal; all of it is
+// far inside the 1e-5 relative tolerance against the float64 oracle, at a quarter of the
+// instructions of the precise forms.
+__device__ __forceinline__ float hexp(float x) { return __expf(x); }
+__device__ __forceinline__ double hexp(double x) { return exp(x); }
+__device__ __forceinline__ float hdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double hdiv(double a, double b) { return a / b; }
+// x / c for a literal c.
+__device__ __forceinline__ float hdivc(float x, double c) { return x * (float)(1.0 / c); }
+__device__ __forceinline__ double hdivc(double x, double c) { return x / c; }
+// z / (exp(z) - 1) with its z = 0 limit.  float32: near 0 the Taylor series of the
+// generating function of the Bernoulli numbers, sum_k B_k z^k / k!
+// (1 - z/2 + z^2/12 - z^4/720 + z^6/30240 - z^8/1209600, truncation < 1e-10 for |z| < 1/2);
+// elsewhere exp(z) - 1 >= 0.39 in magnitude, so ex2's error is not amplified by more than 2.5.
+__device__ __forceinline__ float hz_over_expm1(float z) {
+  if (fabsf(z) < 0.5f) {
+    const float z2 = z * z;
+    const float even = fmaf(z2, fmaf(z2, fmaf(z2, fmaf(z2, -1.f / 1209600.f, 1.f / 30240.f),
+                                               -1.f / 720.f), 1.f / 12.f), 1.f);
+    return fmaf(z, -0.5f, even);
+  }
+  return __fdividef(z, __expf(z) - 1.f);
+}
+__device__ __forceinline__ double hz_over_expm1(double z) { return z_over_expm1(z); }
+
 // Exponential Euler: x' = -B/A + (x + B/A) exp(A dt) for dx/dt = A x + B.
 template <typename R>
 __device__ __forceinline__ R expeuler(R x, R A, R B, R dt) {
-  const R BA = B / A;
-  return -BA + (BA + x) * dexp(A * dt);
+  const R BA = hdiv(B, A);
+  return -BA + (BA + x) * hexp(A * dt);
 }
 
 // Gating part of the COBAHH update (examples/cobahh.py:159-180): the exponential-Euler step
 // of m, h, n over one dt at membrane potential v.  Rates in SI units; the three of the form
-// x/(exp(x/a) - 1) go through z/expm1(z) (see z_over_expm1).
+// x/(exp(x/a) - 1) go through z/(exp(z) - 1) (hz_over_expm1, Brian2's exprel).
 template <typename R>
 __device__ __forceinline__ void hh_gating(R VT, R v, R& m, R& h, R& n, R dt) {
   // 0.32/mV*(13mV-v+VT)/(exp((13mV-v+VT)/4mV)-1)/ms = 1280 * z/expm1(z), z = (..)/4mV
-  const R am = (R)1280 * z_over_expm1(((R)13e-3 - v + VT) / (R)4e-3);
-  const R bm = (R)1400 * z_over_expm1((v - VT - (R)40e-3) / (R)5e-3);
-  const R ah = (R)128 * dexp(((R)17e-3 - v + VT) / (R)18e-3);
-  const R bh = (R)4000 / ((R)1 + dexp(((R)40e-3 - v + VT) / (R)5e-3));
-  const R an = (R)160 * z_over_expm1(((R)15e-3 - v + VT) / (R)5e-3);
-  const R bn = (R)500 * dexp(((R)10e-3 - v + VT) / (R)40e-3);
+  const R am = (R)1280 * hz_over_expm1(hdivc((R)13e-3 - v + VT, 4e-3));
+  const R bm = (R)1400 * hz_over_expm1(hdivc(v - VT - (R)40e-3, 5e-3));
+  const R ah = (R)128 * hexp(hdivc((R)17e-3 - v + VT, 18e-3));
+  const R bh = hdiv((R)4000, (R)1 + hexp(hdivc((R)40e-3 - v + VT, 5e-3)));
+  const R an = (R)160 * hz_over_expm1(hdivc((R)15e-3 - v + VT, 5e-3));
+  const R bn = (R)500 * hexp(hdivc((R)10e-3 - v + VT, 40e-3));
   m = expeuler(m, -(am + bm), am, dt);
   h = expeuler(h, -(ah + bh), ah, dt);
   n = expeuler(n, -(an + bn), an, dt);
 }
 
+// 1/Cm (float32, from the group's precomputed reciprocal) or division by Cm (float64).
+__device__ __forceinline__ float per_cm(float x, const HhDev& g) { return x * (float)g.inv_Cm; }
+__device__ __forceinline__ double per_cm(double x, const HhDev& g) { return x / g.Cm; }
+
 // Membrane part of the COBAHH update: exponential Euler for v with the conductances of the
 // gating state at the start of the step.  Returns the new v.
 template <typename R>
 __device__ __forceinline__ R hh_membrane(const HhDev& g, R v, R m, R h, R n, R ge, R gi, R dt) {
-  const R gl = (R)g.gl, Cm = (R)g.Cm;
+  const R gl = (R)g.gl;
   const R gna = (R)g.gNa * (m * m * m) * h;
   const R gk = (R)g.gK * (n * n * n * n);
-  const R Av = -(gl + ge + gi + gna + gk) / Cm;
-  const R Bv = (gl * (R)g.El + ge * (R)g.Ee + gi * (R)g.Ei + gna * (R)g.ENa + gk * (R)g.EK) / Cm;
+  const R Av = -per_cm(gl + ge + gi + gna + gk, g);
+  const R Bv = per_cm(gl * (R)g.El + ge * (R)g.Ee + gi * (R)g.Ei + gna * (R)g.ENa + gk * (R)g.EK, g);
   return expeuler(v, Av, Bv, dt);
 }
 

@@ -327,6 +327,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
   const MlpImage* I = image_of(S);
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
+  const double inv_dt = 1.0 / dt;
   const int slot = ring_slot(ts, P.ring_len);
   const float dtR = (float)dt;
   const HhDev* prm = static_cast<const HhDev*>(P.params);
@@ -373,7 +374,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
     float ls = 0.f;
     if (refr) {
       ls = LSv[q];
-      nr = timestep_of(t - (double)ls, dt) >= g.ref_steps;
+      nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
     }
     const float vn = hh_membrane<float>(g, v, m, h, n, ge, gi, dtR);
     unsigned fl = 0;
