@@ -376,12 +376,16 @@ b2b_status build_proj(b2b_net* net, int pj) {
     ~Cleanup() { for (auto& m : *t) m.release(); }
   } cleanup{&tmp};
   const size_t rs = real_size(pr.dtype);
+  // per-synapse weights only for STDP and host-given weights; members with different scalar
+  // weights keep one weight per member
   bool need_w = pr.effect == B2B_EFFECT_STDP;
+  bool member_w = false;
   for (int sid : pr.members) {
     const Syn& sy = net->syns[sid];
     if (!sy.w.empty()) need_w = true;
-    if (net->syns[pr.members[0]].w_scalar != sy.w_scalar) need_w = true;
+    if (net->syns[pr.members[0]].w_scalar != sy.w_scalar) member_w = true;
   }
+  member_w = member_w && !need_w;
   // 1) upload or generate, keys, histogram
   for (size_t m = 0; m < pr.members.size(); ++m) {
     Syn& sy = net->syns[pr.members[m]];
@@ -464,13 +468,15 @@ b2b_status build_proj(b2b_net* net, int pj) {
   D.target = dst.dev.var[pr.target_var];
   for (int v = 0; v < 3; ++v) D.targets[v] = dst.dev.var[v];
   D.n_mem = 1;
-  if (pr.multi_target) {
+  if (pr.multi_target || member_w) {
     std::vector<int64_t> hi;
     std::vector<int8_t> var;
+    std::vector<double> mw;
     for (int m : pr.members) {
       const Syn& sy = net->syns[m];
       hi.push_back(net->groups[sy.pre_gid].offset + sy.pre_hi);
       var.push_back((int8_t)sy.target_var);
+      mw.push_back(sy.w_scalar);
     }
     int64_t* dhi = nullptr;
     int8_t* dvar = nullptr;
@@ -481,6 +487,12 @@ b2b_status build_proj(b2b_net* net, int pj) {
     D.n_mem = (int32_t)hi.size();
     D.mem_hi = dhi;
     D.mem_var = dvar;
+    if (member_w) {
+      double* dw = nullptr;
+      CU(dalloc(pr, &dw, mw.size()));
+      CU(cudaMemcpy(dw, mw.data(), 8 * mw.size(), cudaMemcpyHostToDevice));
+      D.mem_w = dw;
+    }
   }
   int64_t n_dst_valid = 0;
   for (int gi : dst.groups) n_dst_valid += net->groups[gi].n;

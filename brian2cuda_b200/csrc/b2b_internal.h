@@ -82,6 +82,7 @@ struct ProjDev {
   int32_t pad_mem;
   const int64_t* mem_hi;
   const int8_t* mem_var;
+  const double* mem_w;            // per-member scalar weight (members differ), or NULL
   void* targets[3];               // per variable v, ge, gi
   // STDP
   void* apre; void* apost; void* lastupdate;

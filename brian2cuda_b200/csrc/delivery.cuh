@@ -158,16 +158,38 @@ __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64
   }
 }
 
-// Target array of presynaptic neuron pre in a projection whose members add into
-// different variables (binary search over the members' upper bounds).
-__device__ __forceinline__ void* member_target(const ProjDev& J, int32_t pre) {
-  if (J.n_mem <= 1) return J.target;
+// Member of presynaptic neuron pre in a projection of several Synapses objects (binary
+// search over the members' upper bounds).
+__device__ __forceinline__ int member_of(const ProjDev& J, int32_t pre) {
   int lo = 0, hi = J.n_mem - 1;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     if (pre < J.mem_hi[mid]) hi = mid; else lo = mid + 1;
   }
-  return J.targets[J.mem_var[lo]];
+  return lo;
+}
+
+// Target array and scalar weight of presynaptic neuron pre.  A lane keeps its last lookup:
+// the synapses a lane visits for one work item share their pre.
+template <typename R>
+struct MemberCache {
+  int32_t pre = -1;
+  R* target = nullptr;
+  R w = 0;
+};
+
+template <typename R>
+__device__ __forceinline__ void member_lookup(const ProjDev& J, int32_t pre, MemberCache<R>& c) {
+  if (pre == c.pre) return;
+  c.pre = pre;
+  if (J.n_mem <= 1) {
+    c.target = static_cast<R*>(J.target);
+    c.w = (R)J.w_scalar;
+    return;
+  }
+  const int m = member_of(J, pre);
+  c.target = static_cast<R*>(J.targets[J.mem_var[m]]);
+  c.w = J.mem_w ? (R)J.mem_w[m] : (R)J.w_scalar;
 }
 
 }  // namespace b2b

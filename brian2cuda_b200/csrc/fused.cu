@@ -159,13 +159,14 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
   for (int p = 0; p < F.n_proj; ++p) {
     const ProjDev& J = F.proj[p];
     const R* W = static_cast<const R*>(J.w);
-    const R ws = (R)J.w_scalar;
+    MemberCache<R> mc;
     for_each_due<WARP_PREFIX, 8>(J, ts, warp0, nwarps, s_pref,
                                  [&](int64_t s, bool valid, int32_t pre) {
       if (!valid) return;
       const int32_t post = __ldg(J.post + s);
-      const R w = W ? __ldg(W + s) : ws;
-      atomicAdd(static_cast<R*>(member_target(J, pre)) + (int64_t)par * P.n + post, w);
+      member_lookup<R>(J, pre, mc);
+      const R w = W ? __ldg(W + s) : mc.w;
+      atomicAdd(mc.target + (int64_t)par * P.n + post, w);
     });
   }
 }

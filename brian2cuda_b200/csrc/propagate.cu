@@ -64,16 +64,16 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   const ProjDev& P = B.p[blockIdx.y];
   const int64_t ts = clock[0] + k;
   const R* __restrict__ W = static_cast<const R*>(P.w);
-  const R ws = (R)P.w_scalar;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  MemberCache<R> mc;
   for_each_due<WARP_PREFIX, 8>(P, ts, warp0, nwarps, s_pref,
                                [&](int64_t s, bool valid, int32_t pre) {
     const int32_t post = valid ? __ldg(P.post + s) : 0;
-    R w = ws;
+    member_lookup<R>(P, pre, mc);
+    R w = mc.w;
     if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
-    R* T = static_cast<R*>(member_target(P, pre));
-    add_to_target<R, AGG>(T, post, w, valid);
+    add_to_target<R, AGG>(mc.target, post, w, valid);
   });
 }
 

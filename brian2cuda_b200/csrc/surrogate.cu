@@ -319,7 +319,7 @@ struct SurrDev {
 // gating state at the start of the step, as the exact kernel does.  A neuron is re-stepped
 // exactly when its normalised v lies outside the training range or, with `judge`, when a
 // predicted gate differs from the exact exponential-Euler value by more than `tol`.
-__global__ void __launch_bounds__(kTile)
+__global__ void __launch_bounds__(kTile, 6)
 hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock, int k,
                          double dt, int32_t* status) {
   __shared__ FwdSmem S;
@@ -342,15 +342,27 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
   uint32_t phase = 0;
   unsigned long long n_upd = 0, n_fb = 0;
   const int64_t ntiles = P.n / kTile;   // populations are padded to a multiple of 128
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const int64_t tstride = (int64_t)gridDim.x * kTile;
+  int64_t tile = blockIdx.x;
+  float v = 0.f, m = 0.f, h = 0.f, n = 0.f, ge = 0.f, gi = 0.f, ls = 0.f;
+  if (tile < ntiles) {
     const int64_t q = tile * kTile + threadIdx.x;
-    const HhDev g = prm[group_of<1>(P, q)];
-    const bool refr = g.ref_steps >= 0;
-    const float v = Vv[q], m = Mv[q], h = Hv[q], n = Nv[q];
-    float ge = GEv[q], gi = GIv[q];
+    v = Vv[q]; m = Mv[q]; h = Hv[q]; n = Nv[q]; ge = GEv[q]; gi = GIv[q]; ls = LSv[q];
+  }
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int64_t q = tile * kTile + threadIdx.x;
     float xh[4], y[3];
     normalise(I, v, m, h, n, xh);
+    // the next tile's state loads are in flight during this tile's tensor-core chain
+    float nv = 0.f, nm = 0.f, nh = 0.f, nn_ = 0.f, nge = 0.f, ngi = 0.f, nls = 0.f;
+    if (tile + gridDim.x < ntiles) {
+      const int64_t qn = q + tstride;
+      nv = Vv[qn]; nm = Mv[qn]; nh = Hv[qn]; nn_ = Nv[qn]; nge = GEv[qn]; ngi = GIv[qn];
+      nls = LSv[qn];
+    }
     if (!mlp_tile_forward(S, phase, xh, y, status)) break;
+    const HhDev& g = prm[group_of<1>(P, q)];
+    const bool refr = g.ref_steps >= 0;
     float mn = dclip(m + I->out_scale[0] * y[0], 0.f, 1.f);
     float hn = dclip(h + I->out_scale[1] * y[1], 0.f, 1.f);
     float nn = dclip(n + I->out_scale[2] * y[2], 0.f, 1.f);
@@ -371,11 +383,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
       n_fb += __popc(fb);
     }
     bool nr = true;
-    float ls = 0.f;
-    if (refr) {
-      ls = LSv[q];
-      nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
-    }
+    if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
     const float vn = hh_membrane<float>(g, v, m, h, n, ge, gi, dtR);
     unsigned fl = 0;
     if (valid && vn > (float)g.Vthr && nr) {
@@ -394,6 +402,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
       NRv[q] = nr ? 1 : 0;
     }
     emit_spikes<1>(P, q, fl, ts, slot, status);
+    v = nv; m = nm; h = nh; n = nn_; ge = nge; gi = ngi; ls = nls;
   }
   clear_next_slot(P, ts);
   if ((threadIdx.x & 31) == 0 && D.counters) {
@@ -769,16 +778,34 @@ int64_t gcd64(int64_t a, int64_t b) {
   return a;
 }
 
-// Resident CTAs of the surrogate step kernel per SM (shared memory and 64 TMEM columns each).
+// Resident CTAs per SM of a 128-thread inference kernel, from its registers and shared
+// memory (carveout set to the largest shared-memory share) and its 64 TMEM columns (at most
+// 8 per SM).  The runtime's occupancy query answers 1 for these kernels on this toolchain
+// although 6 fit (the profiler's limits agree with this computation), so it is not used.
+template <class K>
+int inference_ctas_per_sm(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || fa.numRegs <= 0) {
+    cudaGetLastError();
+    return 1;
+  }
+  const int regs = (fa.numRegs + 7) / 8 * 8;                      // allocation granule
+  const int by_regs = 65536 / (regs * kTile);
+  const int by_smem = (int)((228 * 1024) / (fa.sharedSizeBytes + 1024));  // +1 KB per CTA
+  return std::max(1, std::min(std::min(by_regs, by_smem), 8));
+}
+
 int surrogate_ctas_per_sm() {
   static int cached = 0;
-  if (cached == 0) {
-    int occ = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, hh_surrogate_step_kernel, kTile, 0) !=
-        cudaSuccess)
-      occ = 1;
-    cached = std::max(1, std::min(occ, 8));
-  }
+  if (cached == 0) cached = inference_ctas_per_sm(hh_surrogate_step_kernel);
+  return cached;
+}
+
+int forward_ctas_per_sm() {
+  static int cached = 0;
+  if (cached == 0) cached = inference_ctas_per_sm(mlp_forward_kernel);
   return cached;
 }
 
@@ -960,7 +987,7 @@ b2b_status b2b_mlp_forward(b2b_mlp* m, const float* dev_x, float* dev_out, int64
   if (n == 0) return B2B_OK;
   DeviceScope ds(m->device);
   const int64_t ntiles = (n + kTile - 1) / kTile;
-  const int64_t resident = (int64_t)surrogate_ctas_per_sm() * sm_count(m->device);
+  const int64_t resident = (int64_t)forward_ctas_per_sm() * sm_count(m->device);
   const unsigned grid = (unsigned)std::min(ntiles, resident);
   mlp_forward_kernel<<<grid, kTile, 0, m->stream>>>(m->img, reinterpret_cast<const float4*>(dev_x),
                                                    dev_out, n, raw ? 1 : 0, m->status);

@@ -117,6 +117,40 @@ def build_cobahh(net, n: int = 100_000, p: float = 0.02, dmin: int = 1, dmax: in
     return {"P": P, "Ce": Ce, "Ci": Ci}
 
 
+def batch_sizes(n_instances: int = 256, lo: int = 1000, hi: int = 64000,
+                seed_offset: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Sizes round(exp(U[ln lo, ln hi])) and excitatory weights U[4, 8] nS of the batched
+    COBAHH instances (seeded)."""
+    rng = rng_for(5 + seed_offset)
+    sizes = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), n_instances))).astype(np.int64)
+    we = rng.uniform(4 * nS, 8 * nS, n_instances)
+    return sizes, we
+
+
+def build_cobahh_batch(net, sizes, we, p: float = 0.02, dmin: int = 1, dmax: int = 50,
+                       wi: float = 67 * nS, dtype="float32", seed_offset: int = 0,
+                       monitor_capacity: int = 0):
+    """Independent COBAHH instances in one network: instance k is build_cobahh's network with
+    sizes[k] neurons and excitatory weight we[k].  The instances' groups share one population
+    and their 2 x len(sizes) Synapses objects one projection, so every step is one neuron
+    launch and one delivery launch whatever the number of instances."""
+    rng = rng_for(5 + seed_offset)
+    groups, syns = [], []
+    for k, (n, w) in enumerate(zip(np.asarray(sizes).tolist(), np.asarray(we).tolist())):
+        P = net.hh_group(int(n), cobahh_hh(), dtype)
+        cobahh_init(net, P, int(n), rng)
+        ne = int(0.8 * n)
+        seed = SEED_BASE + 1000 + 2 * k + 1000 * seed_offset
+        syns.append(net.synapses_random(P, P, "ge", p, dmin, dmax, float(w), seed,
+                                        pre_range=(0, ne)))
+        syns.append(net.synapses_random(P, P, "gi", p, dmin, dmax, wi, seed + 1,
+                                        pre_range=(ne, int(n))))
+        if monitor_capacity:
+            net.spike_monitor(P, monitor_capacity)
+        groups.append(P)
+    return {"groups": groups, "syns": syns}
+
+
 # ---- STDP (configuration: 1e4 Poisson @ 15 Hz -> 1e3 LIF, all-to-all, float32) ----------------
 def stdp_lif() -> LIF:
     # dv/dt = (ge*(Ee - vr) + El - v)/taum, dge/dt = -ge/taue; threshold v > vt, reset v = vr
