@@ -196,8 +196,18 @@ def main():
                          "nothing (for ncu captures of the step kernels)")
     ap.add_argument("--fused", action="store_true",
                     help="run one kernel per step (neuron update and delivery side by side)")
+    ap.add_argument("--workload", default="cobahh", choices=["cobahh", "batched"],
+                    help="cobahh: the 1e5-neuron COBAHH network (default line); batched: 256 "
+                         "COBAHH instances, plain vs batched vs batched + gating surrogate")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
+
+    if args.workload == "batched" and args.impl == "b2b":
+        bench_batched(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank == 0:
@@ -378,6 +388,181 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ---- batched COBAHH instances (plain, batched, batched + gating surrogate) -------------------
+BATCH_STEPS = 1000           # simulation steps per bench step of the batched workload (0.1 s)
+BATCH_WORKLOAD = ("256 COBAHH instances, sizes round(exp(U[ln 1e3, ln 6.4e4])) (3.93e6 neurons), "
+                  "p=0.02 (2.65e9 synapses), we~U[4,8] nS, delays U{1..50} steps, f32")
+SURR_TOL = 1e-3
+
+
+def _spike_match(a, b):
+    """Fraction of spikes (neuron, step) of a that b has within one step."""
+    keys = set(zip(b[0].tolist(), b[1].tolist()))
+    if len(a[0]) == 0:
+        return 1.0
+    hit = sum(1 for i, t in zip(a[0].tolist(), a[1].tolist())
+              if (i, t) in keys or (i, t - 1) in keys or (i, t + 1) in keys)
+    return hit / len(a[0])
+
+
+def bench_batched(args, world, rank, local):
+    import torch
+
+    from brian2cuda_b200 import Network, models
+    from brian2cuda_b200.surrogate import (GatingSurrogate, gating_targets, sample_states,
+                                           surrogate_stats)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    sizes, we = models.batch_sizes()
+    n_total = int(sizes.sum())
+    runs = args.warmup + args.steps + 2
+
+    def build(surr=None, judge=True, mon_entries=0):
+        net = Network(DT, seed=models.SEED_BASE + 5, device=local, steps_per_graph=50,
+                      stream=stream.cuda_stream)
+        # one monitor buffer per population: the groups' capacities add up
+        cap = -(-mon_entries // len(sizes)) if mon_entries else 0
+        ids = models.build_cobahh_batch(net, sizes, we, monitor_capacity=cap)
+        if surr is not None:
+            surr.attach(net, ids["groups"][0], tol=SURR_TOL, judge=judge)
+        net.finalize()
+        net.store(0)
+        return net, ids
+
+    def timed(net, steps):
+        for _ in range(args.warmup):
+            net.restore(0)
+            net.run(BATCH_STEPS)
+        net.sync()
+        barrier(world)
+        torch.cuda.synchronize()
+        launches0 = net.kernel_launches
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            net.restore(0)
+            net.run(BATCH_STEPS)
+        ev1.record(stream)
+        ev1.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1), world), net.kernel_launches - launches0
+
+    # ---- batched, exact integrator (the headline line)
+    t0 = time.perf_counter()
+    net, ids = build(mon_entries=int(n_total * BATCH_STEPS * DT * 40.0 * runs + n_total * 0.03 * 40))
+    setup_s = time.perf_counter() - t0
+    n_syn = sum(net.syn_count(s_) for s_ in ids["syns"])
+    offs = [net.group_offset(g) for g in ids["groups"]]
+    outdeg = np.zeros(max(o + int(n) for o, n in zip(offs, sizes)), np.int64)
+    for g, o, n in zip(ids["groups"], offs, sizes):
+        outdeg[o:o + int(n)] = net.out_degree(g)
+    net.run(300)
+    tune = net.autotune(trial_steps=20)
+    start = net.spikes_recorded(ids["groups"][0])
+    clocks = Clocks(local)
+    ms_total, launches = timed(net, args.steps)
+    clk = clocks.stop()
+    # synaptic events of the timed runs (the warm-up runs repeat the same run from the same
+    # checkpoint): recorded spikes x out-degree, per run
+    idx, _, _ = net.spikes_fetch_population(ids["groups"][0], start, cap=1 << 27)
+    per_run = 1.0 / max(1, args.warmup + args.steps)
+    nspk = len(idx) * per_run * args.steps
+    events = float(outdeg[idx].sum()) * per_run * args.steps
+    del idx
+    seconds = ms_total / 1e3
+    value = float(n_total) * BATCH_STEPS * args.steps * world / seconds
+    events_per_s = events * world / seconds
+    net.restore(0)
+    prof = net.profile(200)
+    hbm, peak_kind = peaks()
+    neuron_ms = [ms for k, ms in prof if k == 1][0]
+    neuron_bytes = float(BYTES_NEURON_UPDATE * n_total)
+    achieved = neuron_bytes / (neuron_ms * 1e-3) / 1e9
+    # raster of the exact form, first 300 steps, for the surrogate comparison
+    net.close()
+    ref_net, ref_ids = build(mon_entries=int(n_total * 300 * DT * 200.0))
+    ref_net.run(300)
+    ref_ras = {g: ref_net.spikes(g) for g in ref_ids["groups"][-16:]}
+    # ---- gating surrogate: training data from the batched net's own trajectories (the three
+    # largest instances every 5 steps of the first 500), 1e7 transitions, exact targets
+    ref_net.restore(0)
+    big = [ref_ids["groups"][int(k)] for k in np.argsort(sizes)[-3:]]
+    xs = []
+    for _ in range(100):
+        ref_net.run(5)
+        xs.extend(sample_states(ref_net, g) for g in big)
+    ref_net.close()
+    x = torch.cat(xs)
+    x = x[torch.randperm(len(x), device=x.device)[:10_000_000]].contiguous()
+    t = gating_targets(models.cobahh_hh(), DT, x)
+    surr = GatingSurrogate(device=local, seed=3)
+    t0 = time.perf_counter()
+    losses = surr.fit(x, t, epochs=100, batch=32768, lr=1e-2)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del x, t
+    snet, sids = build(surr, judge=True, mon_entries=int(n_total * 300 * DT * 200.0))
+    snet.run(300)
+    s_ras = {g: snet.spikes(g) for g in sids["groups"][-16:]}
+    match = min(_spike_match(ref_ras[g], s_ras[g2]) for g, g2 in zip(ref_ras, s_ras))
+    snet.restore(0)
+    u0, f0 = surrogate_stats(snet, sids["groups"][0])
+    s_ms, _ = timed(snet, args.steps)
+    u1, f1 = surrogate_stats(snet, sids["groups"][0])
+    snet.close()
+    surr_value = float(n_total) * BATCH_STEPS * args.steps * world / (s_ms / 1e3)
+    # ---- plain exact form: every instance its own network, one after another
+    plain_ms = 0.0
+    plain_steps = 200
+    for k, (n_k, w_k) in enumerate(zip(sizes.tolist(), we.tolist())):
+        pn = Network(DT, seed=models.SEED_BASE + 5, device=local, stream=stream.cuda_stream)
+        models.build_cobahh(pn, n=int(n_k), we=float(w_k), seed_offset=100 + k)
+        pn.finalize()
+        pn.run(50)
+        pn.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pn.run(plain_steps)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        pn.close()
+    plain_value = float(n_total) * plain_steps / (plain_ms / 1e3)
+    line = {
+        "metric": "neuron-updates/s", "value": value, "unit": "neuron-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "sim_steps_per_step": BATCH_STEPS,
+                   "instances": len(sizes), "neurons": n_total, "synapses": n_syn,
+                   "parallelism": f"replicas x{world}", "l2": "working set > L2 (21 GB)"},
+        "synaptic_events_per_s": events_per_s,
+        "spikes_per_run": nspk / max(1, args.steps),
+        "setup_s": setup_s,
+        "autotune": tune,
+        "plain": {"neuron_updates_per_s": plain_value,
+                  "how": f"each instance its own network, {plain_steps} steps each, "
+                         "one after another (the unbatched exact-integrator form)"},
+        "surrogate": {"neuron_updates_per_s": surr_value, "vs_plain": surr_value / plain_value,
+                      "vs_batched_exact": surr_value / value, "tol": SURR_TOL, "judge": True,
+                      "fallback_frac": (f1 - f0) / max(1, u1 - u0),
+                      "raster_match_within_1dt_300_steps_last_16_instances": match,
+                      "train_s": train_s, "train_loss": losses[-1],
+                      "dataset": "1e7 exact transitions from the batched net's trajectories"},
+        "batched_vs_plain": value / plain_value,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": _traffic_lookup("hh_stream_kernel"),
+                     "kernel": "neuron (HH update+threshold+compaction, hh_stream_kernel)",
+                     "kernel_ms": neuron_ms, "peak_source": peak_kind,
+                     "bytes_per_launch": neuron_bytes},
+        "kernel_ms_mean_per_launch": {("neuron" if k == 1 else "delivery" if k == 2 else
+                                       f"site {k}"): ms for k, ms in prof},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def _traffic(kernel: str):

@@ -64,6 +64,11 @@ class HinesParams(C.Structure):
                [("channel_dtype", C.c_int32), ("reserved", C.c_int32)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("site_kind", C.c_int32), ("site_index", C.c_int32), ("choice_a", C.c_int32),
+                ("choice_b", C.c_int32), ("best_ms", C.c_double), ("default_ms", C.c_double)]
+
+
 P = C.c_void_p
 I32, I64, U64, DBL = C.c_int32, C.c_int64, C.c_uint64, C.c_double
 PI32, PI64 = C.POINTER(C.c_int32), C.POINTER(C.c_int64)
@@ -112,6 +117,10 @@ PROTOTYPES = {
     "b2b_hines_run": (I32, [P, I64]),
     "b2b_hines_spike_counts": (I32, [P, P, I32]),
     "b2b_hines_destroy": (I32, [P]),
+    "b2b_autotune": (I32, [P, I32, C.POINTER(TuneResult), I32, PI32]),
+    "b2b_out_degree": (I32, [P, I32, P, I64]),
+    "b2b_spikemon_fetch_population": (I32, [P, I32, I64, PI64, PI64, P, P, I64]),
+    "b2b_group_offset": (I32, [P, I32, PI64]),
     "b2b_mlp_create": (I32, [I32, P, U64, C.POINTER(P)]),
     "b2b_mlp_destroy": (I32, [P]),
     "b2b_mlp_params_get": (I32, [P, P, I64]),

@@ -666,8 +666,10 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
       CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
       ++net->launches;
     }
-    for (const auto& b : net->add_batches) {
-      CU(launch_proj_add_batch(b.data(), (int)b.size(), net->d_clock, k, net->stream));
+    for (size_t b = 0; b < net->add_batches.size(); ++b) {
+      const auto& B = net->add_batches[b];
+      CU(launch_proj_add_batch(B.data(), (int)B.size(), net->d_clock, k, net->stream,
+                               b < net->add_tune.size() ? &net->add_tune[b] : nullptr));
       ++net->launches;
     }
     for (const Proj& pr : net->projs) {
@@ -1172,6 +1174,174 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   GUARD_END
 }
 
+// ---- autotuner ------------------------------------------------------------------------------
+namespace {
+
+struct TuneSite {
+  int kind;   // 1 population, 6 additive delivery launch
+  int idx;
+};
+
+// Advances the net by n_steps with eager launches, timing the launch of `site` with a CUDA
+// event pair on the net's stream; *mean_ms receives its mean device time.
+b2b_status time_site(b2b_net* net, int64_t n_steps, const TuneSite& site, double* mean_ms) {
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  double acc = 0.0;
+  b2b_status result = B2B_OK;
+  const int64_t* clk = net->d_clock;
+  for (int64_t step = 0; step < n_steps && result == B2B_OK; ++step) {
+    if ((result = refill_rng(net, 1)) != B2B_OK) break;
+    cudaError_t e = cudaSuccess;
+    for (size_t p = 0; p < net->pops.size() && e == cudaSuccess; ++p) {
+      const bool timed = site.kind == 1 && site.idx == (int)p;
+      if (timed) cudaEventRecord(e0, net->stream);
+      e = launch_pop_step(net->pops[p], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (timed) cudaEventRecord(e1, net->stream);
+    }
+    for (size_t b = 0; b < net->add_batches.size() && e == cudaSuccess; ++b) {
+      const bool timed = site.kind == 6 && site.idx == (int)b;
+      if (timed) cudaEventRecord(e0, net->stream);
+      e = launch_proj_add_batch(net->add_batches[b].data(), (int)net->add_batches[b].size(), clk,
+                                0, net->stream, &net->add_tune[b]);
+      if (timed) cudaEventRecord(e1, net->stream);
+    }
+    for (const Proj& pr : net->projs) {
+      if (e != cudaSuccess || pr.effect == B2B_EFFECT_ADD) continue;
+      e = launch_proj_pre(pr, clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (e == cudaSuccess && pr.effect == B2B_EFFECT_STDP)
+        e = launch_proj_post(pr, clk, 0, net->cfg.dt, net->d_status, net->stream);
+    }
+    for (const Pop& pop : net->pops)
+      if (e == cudaSuccess && pop.late_reset)
+        e = launch_pop_late_reset(pop, clk, 0, net->stream);
+    if (e == cudaSuccess) e = launch_tick(net->d_clock, 1, net->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+    if (e != cudaSuccess) {
+      result = fail(net, B2B_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    acc += ms;
+    net->ts += 1;
+    net->last_chunk_steps = 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (result == B2B_OK) *mean_ms = acc / (double)n_steps;
+  return result;
+}
+
+}  // namespace
+
+b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out, int32_t cap,
+                        int32_t* n_out) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(trial_steps > 0 && trial_steps <= 100000 && n_out, B2B_ERR_INVALID_ARG, "bad arguments");
+  CHECK(!net->fused, B2B_ERR_UNSUPPORTED, "the one-kernel-per-step path has no tunable shapes");
+  GUARD_BEGIN
+  CU(cudaStreamSynchronize(net->stream));
+  // the state to start every trial from, in a slot of its own; monitor counts to put back
+  const int slot = (int)net->snapshots.size();
+  if (b2b_status st = b2b_store(net, slot)) return st;
+  std::vector<unsigned long long> mon(net->pops.size(), 0);
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    if (net->pops[p].dev.mon_cnt)
+      CU(cudaMemcpy(&mon[p], net->pops[p].dev.mon_cnt, sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost));
+  net->add_tune.resize(net->add_batches.size());
+  std::vector<b2b_tune_result> res;
+  b2b_status st = B2B_OK;
+  auto trial = [&](const TuneSite& site, double* ms) {
+    if (b2b_status s2 = b2b_restore(net, slot)) return s2;
+    return time_site(net, trial_steps, site, ms);
+  };
+  for (size_t p = 0; p < net->pops.size() && st == B2B_OK; ++p) {
+    Pop& pop = net->pops[p];
+    if (pop.kind == KIND_SPIKEGEN) continue;
+    std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
+    if (pop.surr_img) {
+      cands = {{0, 0}, {2, 0}, {3, 0}, {4, 0}, {6, 0}};
+    } else {
+      cands = {{0, 0}, {1, 128}, {1, 256}, {4, 128}, {4, 256}};
+    }
+    b2b_tune_result r{1, (int32_t)p, 0, 0, 0.0, 0.0};
+    double best = 1e30;
+    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+      if (pop.surr_img) {
+        pop.tune_ctas = cands[c].first;
+      } else {
+        pop.tune_e = cands[c].first;
+        pop.tune_block = cands[c].second;
+      }
+      double ms = 0;
+      st = trial({1, (int)p}, &ms);
+      if (c == 0) r.default_ms = ms;
+      if (st == B2B_OK && ms < best) {
+        best = ms;
+        r.choice_a = cands[c].first;
+        r.choice_b = cands[c].second;
+      }
+    }
+    if (pop.surr_img) {
+      pop.tune_ctas = r.choice_a;
+    } else {
+      pop.tune_e = r.choice_a;
+      pop.tune_block = r.choice_b;
+    }
+    r.best_ms = best;
+    res.push_back(r);
+  }
+  int sms = kNumSMs;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK; ++b) {
+    AddTune& t = net->add_tune[b];
+    std::vector<std::pair<int, int>> cands = {{0, 0}};
+    for (int g : {8, 16, 32})
+      for (int mult : {1, 2, 4, 8}) cands.push_back({g, mult * sms / 2});
+    b2b_tune_result r{6, (int32_t)b, 0, 0, 0.0, 0.0};
+    double best = 1e30;
+    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+      t.group = cands[c].first;
+      t.grid = cands[c].second;
+      double ms = 0;
+      st = trial({6, (int)b}, &ms);
+      if (c == 0) r.default_ms = ms;
+      if (st == B2B_OK && ms < best) {
+        best = ms;
+        r.choice_a = cands[c].first;
+        r.choice_b = cands[c].second;
+      }
+    }
+    t.group = r.choice_a;
+    t.grid = r.choice_b;
+    r.best_ms = best;
+    res.push_back(r);
+  }
+  // back to the starting state; the next b2b_run captures a graph with the chosen shapes
+  b2b_status st2 = b2b_restore(net, slot);
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    if (net->pops[p].dev.mon_cnt)
+      CU(cudaMemcpy(net->pops[p].dev.mon_cnt, &mon[p], sizeof(unsigned long long),
+                    cudaMemcpyHostToDevice));
+  for (void* a : net->snapshots[slot].buffers) cudaFree(a);
+  net->snapshots.resize(slot);
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  if (st != B2B_OK) return st;
+  if (st2 != B2B_OK) return st2;
+  *n_out = (int32_t)res.size();
+  for (size_t k = 0; k < res.size() && (int32_t)k < cap; ++k)
+    if (out) out[k] = res[k];
+  return B2B_OK;
+  GUARD_END
+}
+
 b2b_status b2b_sync(b2b_net* net, int32_t* device_status) {
   if (b2b_status st = check_net(net)) return st;
   CU(cudaStreamSynchronize(net->stream));
@@ -1283,8 +1453,33 @@ b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
   GUARD_END
 }
 
+namespace {
+b2b_status spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total, int64_t* n,
+                          int32_t* idx, int64_t* step, int64_t cap, bool whole_population);
+}  // namespace
+
 b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total,
                               int64_t* n, int32_t* idx, int64_t* step, int64_t cap) {
+  return spikemon_fetch(net, gid, start, total, n, idx, step, cap, false);
+}
+
+b2b_status b2b_spikemon_fetch_population(b2b_net* net, int32_t gid, int64_t start,
+                                         int64_t* total, int64_t* n, int32_t* idx,
+                                         int64_t* step, int64_t cap) {
+  return spikemon_fetch(net, gid, start, total, n, idx, step, cap, true);
+}
+
+b2b_status b2b_group_offset(b2b_net* net, int32_t gid, int64_t* offset) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(gid >= 0 && gid < (int)net->groups.size() && offset, B2B_ERR_INVALID_ARG, "bad arguments");
+  *offset = net->groups[gid].offset;
+  return B2B_OK;
+}
+
+namespace {
+b2b_status spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total, int64_t* n,
+                          int32_t* idx, int64_t* step, int64_t cap, bool whole_population) {
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   CHECK(total && n && start >= 0 && cap >= 0, B2B_ERR_INVALID_ARG, "bad arguments");
@@ -1304,18 +1499,22 @@ b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t*
   CU(cudaMemcpyAsync(idx, D.mon_idx + start, 4 * m, cudaMemcpyDeviceToHost, net->stream));
   CU(cudaMemcpyAsync(step, D.mon_step + start, 8 * m, cudaMemcpyDeviceToHost, net->stream));
   CU(cudaStreamSynchronize(net->stream));
-  int64_t k = 0;
-  for (int64_t r = 0; r < m; ++r) {
-    if (idx[r] < g.offset || idx[r] >= g.offset + g.n) continue;
-    idx[k] = (int32_t)(idx[r] - g.offset);
-    step[k] = step[r];
-    ++k;
+  int64_t k = m;
+  if (!whole_population) {
+    k = 0;
+    for (int64_t r = 0; r < m; ++r) {
+      if (idx[r] < g.offset || idx[r] >= g.offset + g.n) continue;
+      idx[k] = (int32_t)(idx[r] - g.offset);
+      step[k] = step[r];
+      ++k;
+    }
   }
   *n = k;
   if ((int64_t)rec > D.mon_cap)
     return fail(net, B2B_ERR_QUEUE_OVERFLOW, "spike monitor overflowed");
   return B2B_OK;
 }
+}  // namespace
 
 b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, int64_t cap) {
   if (b2b_status st = check_net(net)) return st;
@@ -1416,6 +1615,29 @@ b2b_status b2b_rng_uniforms_get(b2b_net* net, int32_t gid, void* host, int64_t s
                   (const uint8_t*)pop.rng_buf + rs * (k * pop.n + g.offset), rs * n,
                   cudaMemcpyDeviceToHost));
   return B2B_OK;
+}
+
+b2b_status b2b_out_degree(b2b_net* net, int32_t gid, int32_t* host, int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(gid >= 0 && gid < (int32_t)net->groups.size() && host != nullptr, B2B_ERR_INVALID_ARG,
+        "bad arguments");
+  const Group& g = net->groups[gid];
+  CHECK(n == g.n, B2B_ERR_INVALID_ARG, "n must be the group size");
+  GUARD_BEGIN
+  int32_t* d = nullptr;
+  CU(cudaMalloc(&d, sizeof(int32_t) * std::max<int64_t>(n, 1)));
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(int32_t) * n, net->stream);
+  for (const Proj& pr : net->projs)
+    if (e == cudaSuccess && pr.src_pop == g.pop && n > 0)
+      e = add_out_degree(pr.off, pr.dev.nd, g.offset, n, d, net->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host, d, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, net->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+  cudaFree(d);
+  CU(e);
+  return B2B_OK;
+  GUARD_END
 }
 
 b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n) {

@@ -31,4 +31,7 @@ cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_
                            int64_t n, int64_t key_lo, int64_t key_hi, int64_t src_offset,
                            int64_t dst_offset, const void* d_arr, double w_scalar,
                            void* d_out, cudaStream_t s);
+// Adds the out-degree (all delays) of source neurons [first, first + n) into d_out.
+cudaError_t add_out_degree(const int64_t* d_off, int32_t nd, int64_t first, int64_t n,
+                           int32_t* d_out, cudaStream_t s);
 }  // namespace b2b

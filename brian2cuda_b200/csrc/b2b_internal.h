@@ -142,6 +142,16 @@ struct Pop {
   unsigned long long* surr_cnt = nullptr;     // [0] neuron-updates, [1] exact fallbacks
   float surr_tol = 0.f;
   int32_t surr_judge = 1;
+  // launch shape chosen by b2b_autotune (0: the built-in heuristic)
+  int32_t tune_e = 0;             // neurons per thread, 1 or 4
+  int32_t tune_block = 0;         // threads per CTA, 128 or 256
+  int32_t tune_ctas = 0;          // surrogate kernel: CTAs per SM
+};
+
+// Launch shape of one additive delivery launch (b2b_autotune; 0: built-in heuristic).
+struct AddTune {
+  int32_t grid = 0;               // CTAs per projection
+  int32_t group = 0;              // lanes per work item: 8, 16 or 32
 };
 
 struct Syn {  // one user-level Synapses object
@@ -202,6 +212,7 @@ struct b2b_net {
   std::vector<b2b::Syn> syns;
   std::vector<b2b::Proj> projs;
   std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
+  std::vector<b2b::AddTune> add_tune;      // launch shape per add batch (b2b_autotune)
   bool fused = false;                      // one kernel per step (fused.cu) in use
   b2b::FusedDev fdev{};
   int fused_grid = 0;
@@ -227,7 +238,7 @@ cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double
                              int32_t* status, cudaStream_t s);
 // One launch for n (<= kMaxProjBatch) additive projections of equal dtype / weight mode.
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
-                                  cudaStream_t s);
+                                  cudaStream_t s, const AddTune* tune = nullptr);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
 // COBAHH step of a population with a gating surrogate attached (surrogate.cu).
 cudaError_t launch_hh_surrogate(const Pop& pop, const int64_t* clock, int k, double dt,

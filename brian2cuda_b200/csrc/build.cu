@@ -1,3 +1,4 @@
+#include <algorithm>
 // Connectivity build on the GPU (the role of `_before_run_<pathway>_push_spikes`,
 // brian2cuda/templates/synapses_push_spikes.cu:171-993, which buckets synapses by (pre,
 // post-block), sorts each bucket by delay on the host and copies every bundle with its own
@@ -334,6 +335,25 @@ cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_
                                                       src_offset, pr.post, dst_offset,
                                                       static_cast<const double*>(d_arr),
                                                       w_scalar, d_out);
+  return cudaGetLastError();
+}
+
+// Out-degree of neurons [first, first + n) of a projection's source population:
+// off[(first + i + 1) * nd] - off[(first + i) * nd] (all delays of neuron first + i), added
+// into out[i].
+namespace {
+__global__ void out_degree_kernel(const int64_t* __restrict__ off, int32_t nd, int64_t first,
+                                  int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] += (int32_t)(off[(first + i + 1) * nd] - off[(first + i) * nd]);
+}
+}  // namespace
+
+cudaError_t add_out_degree(const int64_t* d_off, int32_t nd, int64_t first, int64_t n,
+                           int32_t* d_out, cudaStream_t s) {
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096));
+  out_degree_kernel<<<(unsigned)blocks, 256, 0, s>>>(d_off, nd, first, n, d_out);
   return cudaGetLastError();
 }
 

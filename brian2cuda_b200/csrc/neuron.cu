@@ -299,28 +299,29 @@ template <int E>
 cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int32_t* status,
                      cudaStream_t s) {
   const PopDev& P = pop.dev;
-  const unsigned grid = (unsigned)((P.n / E + kBlock - 1) / kBlock);
+  const int block = pop.tune_block > 0 ? pop.tune_block : kBlock;   // <= kBlock
+  const unsigned grid = (unsigned)((P.n / E + block - 1) / block);
   const bool f32 = pop.dtype == B2B_F32;
   switch (pop.kind) {
     case KIND_LIF:
-      if (f32) lif_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
-      else lif_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      if (f32) lif_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+      else lif_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       break;
     case KIND_HH:
       if (E == 4 && f32) {
-        // resident CTAs only (2 per SM by the launch bounds); float64 keeps one pack per
-        // thread (two packs of doubles do not fit the register budget)
-        const unsigned g2 = std::min<unsigned>(grid, 2 * kNumSMs);
-        hh_stream_kernel<float><<<g2, kBlock, 0, s>>>(P, clock, k, dt, status);
+        // resident CTAs only (2 per SM of 256 threads by the launch bounds); float64 keeps
+        // one pack per thread (two packs of doubles do not fit the register budget)
+        const unsigned g2 = std::min<unsigned>(grid, 2 * kNumSMs * (kBlock / block));
+        hh_stream_kernel<float><<<g2, block, 0, s>>>(P, clock, k, dt, status);
       } else if (f32) {
-        hh_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+        hh_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       } else {
-        hh_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+        hh_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       }
       break;
     case KIND_POISSON:
-      if (f32) poisson_step_kernel<float, E><<<grid, kBlock, 0, s>>>(P, clock, k, status);
-      else poisson_step_kernel<double, E><<<grid, kBlock, 0, s>>>(P, clock, k, status);
+      if (f32) poisson_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, status);
+      else poisson_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, status);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -337,8 +338,9 @@ cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double 
     spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
     return cudaGetLastError();
   }
-  return wide(pop.dev.n) ? launch_e<4>(pop, clock, k, dt, status, s)
-                         : launch_e<1>(pop, clock, k, dt, status, s);
+  const bool four = pop.tune_e > 0 ? pop.tune_e == 4 : wide(pop.dev.n);
+  return four ? launch_e<4>(pop, clock, k, dt, status, s)
+              : launch_e<1>(pop, clock, k, dt, status, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

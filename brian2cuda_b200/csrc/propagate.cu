@@ -56,7 +56,7 @@ struct ProjBatch {
 };
 
 // ---- on_pre: target[post] += w -------------------------------------------------------------
-template <typename R, bool HAS_W, bool AGG, bool WARP_PREFIX>
+template <typename R, bool HAS_W, bool AGG, bool WARP_PREFIX, int GROUP>
 __global__ void __launch_bounds__(kDeliverBlock)
 deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __restrict__ clock,
                          int k) {
@@ -67,7 +67,7 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   MemberCache<R> mc;
-  for_each_due<WARP_PREFIX, 8>(P, ts, warp0, nwarps, s_pref,
+  for_each_due<WARP_PREFIX, GROUP>(P, ts, warp0, nwarps, s_pref,
                                [&](int64_t s, bool valid, int32_t pre) {
     const int32_t post = valid ? __ldg(P.post + s) : 0;
     member_lookup<R>(P, pre, mc);
@@ -164,24 +164,34 @@ unsigned deliver_grid(const Proj& pr) {
   return (unsigned)(want < cap ? want : cap);
 }
 
+template <typename R, bool HAS_W, bool AGG, int GROUP>
+void launch_add_g(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem,
+                  const int64_t* clock, int k, cudaStream_t s) {
+  if (warp_prefix)
+    deliver_add_batch_kernel<R, HAS_W, AGG, true, GROUP><<<g, kDeliverBlock, 0, s>>>(B, clock, k);
+  else
+    deliver_add_batch_kernel<R, HAS_W, AGG, false, GROUP><<<g, kDeliverBlock, smem, s>>>(B, clock,
+                                                                                         k);
+}
+
+// Lanes per work item: 8 (four items in flight per warp, the default), 16 or 32.
 template <typename R, bool HAS_W, bool AGG>
 void launch_add(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem, const int64_t* clock,
-                int k, cudaStream_t s) {
-  if (warp_prefix)
-    deliver_add_batch_kernel<R, HAS_W, AGG, true><<<g, kDeliverBlock, 0, s>>>(B, clock, k);
-  else
-    deliver_add_batch_kernel<R, HAS_W, AGG, false><<<g, kDeliverBlock, smem, s>>>(B, clock, k);
+                int k, cudaStream_t s, int group) {
+  if (group == 32) launch_add_g<R, HAS_W, AGG, 32>(B, g, warp_prefix, smem, clock, k, s);
+  else if (group == 16) launch_add_g<R, HAS_W, AGG, 16>(B, g, warp_prefix, smem, clock, k, s);
+  else launch_add_g<R, HAS_W, AGG, 8>(B, g, warp_prefix, smem, clock, k, s);
 }
 
 template <typename R>
 void launch_add_r(const ProjBatch& B, dim3 g, bool hw, bool ag, bool wp, size_t smem,
-                  const int64_t* clock, int k, cudaStream_t s) {
+                  const int64_t* clock, int k, cudaStream_t s, int group) {
   if (hw) {
-    if (ag) launch_add<R, true, true>(B, g, wp, smem, clock, k, s);
-    else launch_add<R, true, false>(B, g, wp, smem, clock, k, s);
+    if (ag) launch_add<R, true, true>(B, g, wp, smem, clock, k, s, group);
+    else launch_add<R, true, false>(B, g, wp, smem, clock, k, s, group);
   } else {
-    if (ag) launch_add<R, false, true>(B, g, wp, smem, clock, k, s);
-    else launch_add<R, false, false>(B, g, wp, smem, clock, k, s);
+    if (ag) launch_add<R, false, true>(B, g, wp, smem, clock, k, s, group);
+    else launch_add<R, false, false>(B, g, wp, smem, clock, k, s, group);
   }
 }
 
@@ -200,7 +210,7 @@ void launch_stdp_pre(const ProjDev& P, unsigned grid, bool ag, bool wp, size_t s
 }  // namespace
 
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, const AddTune* tune) {
   if (n <= 0 || n > kMaxProjBatch) return cudaErrorInvalidValue;
   ProjBatch B{};
   B.n = n;
@@ -213,11 +223,13 @@ cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* 
   }
   const bool wp = nd <= kWarpPrefixMaxDelays;
   const size_t smem = sizeof(int) * (size_t)(nd + 1);
+  if (tune && tune->grid > 0) grid = (unsigned)tune->grid;
+  const int group = tune && tune->group > 0 ? tune->group : 8;
   const dim3 g(grid, (unsigned)n);
   const bool hw = prs[0]->dev.w != nullptr;
   const bool ag = prs[0]->dev.aggregate != 0;
-  if (prs[0]->dtype == B2B_F32) launch_add_r<float>(B, g, hw, ag, wp, smem, clock, k, s);
-  else launch_add_r<double>(B, g, hw, ag, wp, smem, clock, k, s);
+  if (prs[0]->dtype == B2B_F32) launch_add_r<float>(B, g, hw, ag, wp, smem, clock, k, s, group);
+  else launch_add_r<double>(B, g, hw, ag, wp, smem, clock, k, s, group);
   return cudaGetLastError();
 }
 

@@ -820,7 +820,9 @@ cudaError_t launch_hh_surrogate(const Pop& pop, const int64_t* clock, int k, dou
   D.vmax_hat = 1.0f;
   D.judge = pop.surr_judge;
   const int64_t ntiles = pop.dev.n / kTile;
-  const int64_t resident = (int64_t)surrogate_ctas_per_sm() * kNumSMs;
+  const int per_sm = pop.tune_ctas > 0 ? std::min(pop.tune_ctas, surrogate_ctas_per_sm())
+                                       : surrogate_ctas_per_sm();
+  const int64_t resident = (int64_t)per_sm * kNumSMs;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min(ntiles, resident));
   hh_surrogate_step_kernel<<<grid, kTile, 0, s>>>(pop.dev, D, clock, k, dt, status);
   return cudaGetLastError();

@@ -282,6 +282,13 @@ class Network:
         self._syns.append((pre, post, self._groups[post][2]))
         return sid.value
 
+    def out_degree(self, gid: int) -> np.ndarray:
+        """Outgoing synapses of every neuron of the group, over all its Synapses objects."""
+        n = self.group_size(gid)
+        a = np.empty(n, dtype=np.int32)
+        self._check(self._lib.b2b_out_degree(self._h, gid, _ptr(a), n), "out_degree")
+        return a
+
     def syn_count(self, sid: int) -> int:
         n = C.c_int64()
         self._check(self._lib.b2b_syn_count(self._h, sid, C.byref(n)), "syn_count")
@@ -347,6 +354,18 @@ class Network:
                     "profile")
         return [(kinds[k], ms[k]) for k in range(n.value)]
 
+    def autotune(self, trial_steps: int = 50) -> list[dict]:
+        """Times candidate launch shapes of every launch site on the current state and keeps
+        the fastest (state, clock and monitors are left as they were)."""
+        cap = 256
+        res = (N.TuneResult * cap)()
+        n = C.c_int32()
+        self._check(self._lib.b2b_autotune(self._h, int(trial_steps), res, cap, C.byref(n)),
+                    "autotune")
+        return [{"site_kind": r.site_kind, "site_index": r.site_index, "choice_a": r.choice_a,
+                 "choice_b": r.choice_b, "best_ms": r.best_ms, "default_ms": r.default_ms}
+                for r in res[: n.value]]
+
     def spikes(self, gid: int) -> tuple[np.ndarray, np.ndarray]:
         """All recorded spikes of a monitored group as (indices, steps), sorted by step."""
         n = C.c_int64()
@@ -369,6 +388,24 @@ class Network:
                     "spikemon_fetch")
         nxt = min(total.value, int(start) + cap)
         return idx[: n.value], stp[: n.value], nxt
+
+    def spikes_fetch_population(self, gid: int, start: int, cap: int = 1 << 24):
+        """Like spikes_fetch, for every monitored group of gid's population at once, with
+        population indices (see group_offset)."""
+        total, n = C.c_int64(), C.c_int64()
+        idx = np.empty(cap, dtype=np.int32)
+        stp = np.empty(cap, dtype=np.int64)
+        self._check(self._lib.b2b_spikemon_fetch_population(
+            self._h, gid, int(start), C.byref(total), C.byref(n), _ptr(idx), _ptr(stp), cap),
+            "spikemon_fetch_population")
+        nxt = min(total.value, int(start) + cap)
+        return idx[: n.value], stp[: n.value], nxt
+
+    def group_offset(self, gid: int) -> int:
+        """Index of the group's first neuron in its population."""
+        o = C.c_int64()
+        self._check(self._lib.b2b_group_offset(self._h, gid, C.byref(o)), "group_offset")
+        return o.value
 
     def spikes_recorded(self, gid: int) -> int:
         """Number of entries the monitor of gid's population has recorded so far."""

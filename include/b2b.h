@@ -204,6 +204,11 @@ b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n);
 /* Reads a synapse variable in the order the synapses were given (after b2b_finalize). */
 b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64_t n);
 
+/* Number of outgoing synapses of every neuron of group gid over all Synapses objects that
+ * leave it (Brian2's Synapses.N_outgoing summed over pathways; brian2cuda computes it on the
+ * host in synapses_create templates); host receives n = group size int32 counts. */
+b2b_status b2b_out_degree(b2b_net* net, int32_t gid, int32_t* host, int64_t n);
+
 /* ---- lifecycle ---------------------------------------------------------------------- */
 /* Lays out state, builds the delay-sorted connectivity on the GPU and captures the step
  * graphs (the role of the generated before_run code). */
@@ -239,6 +244,25 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
 
+/* Autotuner (no counterpart in the reference, which picks launch shapes from fixed rules,
+ * brian2cuda/device.py:383-394): for every launch site of the net it times candidate launch
+ * shapes on the net's own current state, each over `trial_steps` eager steps started from
+ * the same checkpoint, and keeps the fastest.  Populations: neurons per thread (1 or 4) x
+ * threads per CTA (128 or 256), or, with a gating surrogate, CTAs per SM (2..6); additive
+ * delivery launches: lanes per work item (8, 16, 32) x CTAs (1/2, 1, 2, 4 per SM).  Afterwards
+ * the state, clock and monitor counts are as before the call, and the next b2b_run captures
+ * its graph with the chosen shapes.  A choice of 0 means the built-in rule won. */
+typedef struct {
+  int32_t site_kind;     /* 1 population, 6 additive delivery launch                    */
+  int32_t site_index;    /* population index / delivery launch index                    */
+  int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item */
+  int32_t choice_b;      /* threads per CTA / CTAs                                       */
+  double best_ms;        /* mean device time of one launch with the chosen shape         */
+  double default_ms;     /* the same with the built-in rule                              */
+} b2b_tune_result;
+b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out, int32_t cap,
+                        int32_t* n_out);
+
 /* ---- monitors and inspection ---------------------------------------------------------- */
 /* Records every spike of group gid as (step, index) into a device buffer of `capacity`
  * entries (replaces brian2cuda/templates/spikemonitor.cu without per-step resizes).
@@ -254,6 +278,13 @@ b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
  * files, brian2cuda/templates/objects.cu:522-641). */
 b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total,
                               int64_t* n, int32_t* idx, int64_t* step, int64_t cap);
+/* b2b_spikemon_fetch without the group filter: entries of every monitored group of gid's
+ * population, with population indices (group k's neuron i is b2b_group_offset(k) + i). */
+b2b_status b2b_spikemon_fetch_population(b2b_net* net, int32_t gid, int64_t start,
+                                         int64_t* total, int64_t* n, int32_t* idx,
+                                         int64_t* step, int64_t cap);
+/* Index of group gid's first neuron in its population (after b2b_finalize). */
+b2b_status b2b_group_offset(b2b_net* net, int32_t gid, int64_t* offset);
 /* Spikes of group gid in the last completed step, sorted ascending (the canonical form of
  * the spikespace, brian2cuda/templates/objects.cu:458-479). */
 b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, int64_t cap);

@@ -331,3 +331,40 @@ def test_fused_cobahh_float32_matches_oracle(gpu_factory, oracle_factory):
         a, b = gstate[v].astype(np.float64), ostate[v]
         ok = np.abs(a - b) <= 1e-4 * np.abs(b) + 1e-4 * sc
         assert ok.mean() >= 0.98, (v, ok.mean())
+
+
+def test_autotune_keeps_state_and_results(gpu_factory):
+    """b2b_autotune leaves state, clock and monitors as they were, and the shapes it picks
+    compute the same network (CUBA float64: every delivered weight of one target variable
+    is equal, so the order of the atomic additions cannot change a sum)."""
+    out = {}
+    for tuned in (False, True):
+        net = gpu_factory(DT)
+        ids = models.build_cuba(net, n=1000, p=0.05, dtype="float64")
+        net.finalize()
+        net.run(100)
+        before = (net.timestep, net.get_state(ids["P"], "v").copy(), len(net.spikes(ids["P"])[0]))
+        if tuned:
+            res = net.autotune(trial_steps=10)
+            kinds = {r["site_kind"] for r in res}
+            assert kinds == {1, 6}
+            assert all(r["best_ms"] <= r["default_ms"] for r in res)
+            after = (net.timestep, net.get_state(ids["P"], "v"), len(net.spikes(ids["P"])[0]))
+            assert after[0] == before[0] and after[2] == before[2]
+            np.testing.assert_array_equal(after[1], before[1])
+        net.run(300)
+        idx, st = net.spikes(ids["P"])
+        out[tuned] = (idx, st, net.get_state(ids["P"], "v"))
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    np.testing.assert_array_equal(out[True][1], out[False][1])
+    np.testing.assert_array_equal(out[True][2], out[False][2])
+
+
+def test_out_degree_matches_synapses(gpu_factory):
+    net = gpu_factory(DT)
+    ids = models.build_cobahh(net, n=3000, p=0.03)
+    net.finalize()
+    want = np.zeros(3000, np.int64)
+    for sid in (ids["Ce"], ids["Ci"]):
+        want += np.bincount(net.syn_get(sid, "i"), minlength=3000)
+    np.testing.assert_array_equal(net.out_degree(ids["P"]), want)
