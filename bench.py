@@ -196,10 +196,19 @@ def main():
                          "nothing (for ncu captures of the step kernels)")
     ap.add_argument("--fused", action="store_true",
                     help="run one kernel per step (neuron update and delivery side by side)")
+    ap.add_argument("--tune-from", default=None, metavar="FILE",
+                    help="apply the launch shapes of the JSON line in FILE (an earlier bench "
+                         "output) instead of autotuning; used by the profiling case")
     ap.add_argument("--workload", default="cobahh", choices=["cobahh", "batched"],
                     help="cobahh: the 1e5-neuron COBAHH network (default line); batched: 256 "
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
+    ap.add_argument("--kernel-case", default=None,
+                    choices=["hh4m", "surrogate1m", "mlp_train"],
+                    help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args.kernel_case)
+        return
     world, rank, local = dist_setup(args.gpus)
 
     if args.workload == "batched" and args.impl == "b2b":
@@ -242,6 +251,17 @@ def main():
     net.store(0)
     init = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi", "lastspike")}
     setup_s = time.perf_counter() - t_setup
+    # launch shapes tuned on the network's own state, 150 steps into the run (after the first
+    # population burst); the autotuner leaves the state where it found it
+    tune = None
+    if args.tune_from:
+        with open(args.tune_from) as f:
+            tune = json.loads([ln for ln in f if ln.startswith("{")][-1])["autotune"]
+        net.tune_apply(tune)
+    elif not args.fused:
+        net.run(150)
+        tune = net.autotune(trial_steps=50)
+        net.restore(0)
 
     if args.ncu_case:
         net.run(args.ncu_case)
@@ -367,6 +387,7 @@ def main():
                      "kernel_ms": dom_ms, "peak_source": peak_kind,
                      "bytes_per_launch": alg},
         "kernel_ms_mean_per_launch": kernel_ms,
+        "autotune": tune,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h // max(1, args.steps),
                 "note": "restore + upload of the 7 initial state arrays from pinned memory, "
@@ -563,6 +584,38 @@ def bench_batched(args, world, rank, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def kernel_case(name: str):
+    """Small cases for ncu captures of single kernels (inputs above the L2 size, a few GB at
+    most): hh4m = 4e6 HH neurons (hh_stream_kernel), surrogate1m = 1e6 HH neurons with the
+    gating surrogate attached (hh_surrogate_step_kernel), mlp_train = one epoch of surrogate
+    training on 2e6 transitions (mlp_grad_kernel, mlp_adam_kernel)."""
+    import torch
+
+    from brian2cuda_b200 import Network, models
+    from brian2cuda_b200.surrogate import GatingSurrogate, gating_targets
+    if name in ("hh4m", "surrogate1m"):
+        n = 4_000_000 if name == "hh4m" else 1_000_000
+        net = Network(DT, seed=1, graphs=False)
+        P = net.hh_group(n, models.cobahh_hh(), "float32")
+        models.cobahh_init(net, P, n, np.random.default_rng(0))
+        s = None
+        if name == "surrogate1m":
+            s = GatingSurrogate(seed=3)
+            s.attach(net, P, tol=SURR_TOL, judge=True)
+        net.finalize()
+        net.run(6)
+        net.sync()
+        net.close()
+    elif name == "mlp_train":
+        g = torch.Generator(device="cuda").manual_seed(0)
+        x = torch.rand((2_000_000, 4), device="cuda", generator=g)
+        x[:, 0] = x[:, 0] * 0.13 - 0.085
+        t = gating_targets(models.cobahh_hh(), DT, x)
+        s = GatingSurrogate(seed=3)
+        s.fit(x, t, epochs=1, batch=32768, lr=1e-2)
+        torch.cuda.synchronize()
 
 
 def _traffic(kernel: str):

@@ -119,6 +119,7 @@ PROTOTYPES = {
     "b2b_hines_destroy": (I32, [P]),
     "b2b_autotune": (I32, [P, I32, C.POINTER(TuneResult), I32, PI32]),
     "b2b_out_degree": (I32, [P, I32, P, I64]),
+    "b2b_tune_apply": (I32, [P, C.POINTER(TuneResult), I32]),
     "b2b_spikemon_fetch_population": (I32, [P, I32, I64, PI64, PI64, P, P, I64]),
     "b2b_group_offset": (I32, [P, I32, PI64]),
     "b2b_mlp_create": (I32, [I32, P, U64, C.POINTER(P)]),

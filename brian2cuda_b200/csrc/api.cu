@@ -1342,6 +1342,46 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   GUARD_END
 }
 
+b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(n >= 0 && (r || n == 0), B2B_ERR_INVALID_ARG, "bad arguments");
+  net->add_tune.resize(net->add_batches.size());
+  for (int32_t k = 0; k < n; ++k) {
+    const b2b_tune_result& t = r[k];
+    if (t.site_kind == 1) {
+      CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->pops.size(), B2B_ERR_INVALID_ARG,
+            "bad population index %d", t.site_index);
+      Pop& pop = net->pops[t.site_index];
+      if (pop.surr_img) {
+        CHECK(t.choice_a >= 0 && t.choice_a <= 8, B2B_ERR_INVALID_ARG, "bad CTAs per SM");
+        pop.tune_ctas = t.choice_a;
+      } else {
+        CHECK((t.choice_a == 0 || t.choice_a == 1 || t.choice_a == 4) &&
+                  (t.choice_b == 0 || t.choice_b == 128 || t.choice_b == 256),
+              B2B_ERR_INVALID_ARG, "bad neuron launch shape");
+        pop.tune_e = t.choice_a;
+        pop.tune_block = t.choice_b;
+      }
+    } else if (t.site_kind == 6) {
+      CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->add_batches.size(),
+            B2B_ERR_INVALID_ARG, "bad delivery launch index %d", t.site_index);
+      CHECK((t.choice_a == 0 || t.choice_a == 8 || t.choice_a == 16 || t.choice_a == 32) &&
+                t.choice_b >= 0 && t.choice_b <= 65535,
+            B2B_ERR_INVALID_ARG, "bad delivery launch shape");
+      net->add_tune[t.site_index].group = t.choice_a;
+      net->add_tune[t.site_index].grid = t.choice_b;
+    } else {
+      return fail(net, B2B_ERR_INVALID_ARG, "bad site kind %d", t.site_kind);
+    }
+  }
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  return B2B_OK;
+}
+
 b2b_status b2b_sync(b2b_net* net, int32_t* device_status) {
   if (b2b_status st = check_net(net)) return st;
   CU(cudaStreamSynchronize(net->stream));

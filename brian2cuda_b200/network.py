@@ -366,6 +366,14 @@ class Network:
                  "choice_b": r.choice_b, "best_ms": r.best_ms, "default_ms": r.default_ms}
                 for r in res[: n.value]]
 
+    def tune_apply(self, results: list[dict]):
+        """Applies the launch shapes of an earlier autotune() of a net built the same way."""
+        arr = (N.TuneResult * max(1, len(results)))()
+        for k, r in enumerate(results):
+            arr[k] = N.TuneResult(r["site_kind"], r["site_index"], r["choice_a"], r["choice_b"],
+                                  r.get("best_ms", 0.0), r.get("default_ms", 0.0))
+        self._check(self._lib.b2b_tune_apply(self._h, arr, len(results)), "tune_apply")
+
     def spikes(self, gid: int) -> tuple[np.ndarray, np.ndarray]:
         """All recorded spikes of a monitored group as (indices, steps), sorted by step."""
         n = C.c_int64()

@@ -262,6 +262,9 @@ typedef struct {
 } b2b_tune_result;
 b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out, int32_t cap,
                         int32_t* n_out);
+/* Applies launch shapes an earlier b2b_autotune chose (of a net built the same way), so that
+ * a run can reuse a tuning without repeating its trials. */
+b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n);
 
 /* ---- monitors and inspection ---------------------------------------------------------- */
 /* Records every spike of group gid as (step, index) into a device buffer of `capacity`
