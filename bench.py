@@ -199,7 +199,8 @@ def main():
     ap.add_argument("--tune-from", default=None, metavar="FILE",
                     help="apply the launch shapes of the JSON line in FILE (an earlier bench "
                          "output) instead of autotuning; used by the profiling case")
-    ap.add_argument("--workload", default="cobahh", choices=["cobahh", "batched"],
+    ap.add_argument("--workload", default="cobahh",
+                    choices=["cobahh", "batched", "cuba", "stdp", "hines"],
                     help="cobahh: the 1e5-neuron COBAHH network (default line); batched: 256 "
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
@@ -211,8 +212,11 @@ def main():
         return
     world, rank, local = dist_setup(args.gpus)
 
-    if args.workload == "batched" and args.impl == "b2b":
-        bench_batched(args, world, rank, local)
+    if args.workload != "cobahh" and args.impl == "b2b":
+        if args.workload == "batched":
+            bench_batched(args, world, rank, local)
+        else:
+            bench_small(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -583,6 +587,218 @@ def bench_batched(args, world, rank, local):
         "clocks": clk,
     }
     if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---- CUBA, STDP and multicompartment workloads ------------------------------------------------
+WORKLOADS = {
+    "cuba": "CUBA 4000 LIF (3200 exc / 800 inh), f64, exact integration, p=0.02 (~3.2e5 "
+            "synapses), no delay, 1 s simulated",
+    "stdp": "1e4 Poisson inputs at 15 Hz -> 1e3 LIF all-to-all (1e7 synapses), additive STDP "
+            "(on_pre + on_post), f32, 1 s simulated per step (the configured run is 10 s)",
+    "hines": "1024 multicompartment HH neurons, random binary trees of 200-1000 compartments, "
+             "f64 cable solve, f32 channels, dt=0.025 ms, 200 ms simulated (8000 steps)",
+}
+BYTES = {"cuba_neuron": 58, "cuba_event": 20, "stdp_neuron": 16, "poisson": 4,
+         "stdp_pre": 40, "stdp_post": 32, "hines_comp": 136}
+
+
+def _line_base(args, world, metric, value, unit, ms_per_step, workload, config, dtype):
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic", "config": dict({"workload": workload}, **config)}
+
+
+def _roofline(bytes_per_launch, ms, kernel):
+    hbm, kind = peaks()
+    achieved = bytes_per_launch / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": _traffic_lookup(kernel), "kernel": kernel,
+            "kernel_ms": ms, "peak_source": kind, "bytes_per_launch": bytes_per_launch}
+
+
+def _timed_net_runs(net, stream, args, world, local, steps_per_run):
+    import torch
+    for _ in range(args.warmup):
+        net.restore(0)
+        net.run(steps_per_run)
+    net.sync()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = net.kernel_launches
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        net.restore(0)
+        net.run(steps_per_run)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    return max_over_ranks(ev0.elapsed_time(ev1), world), net.kernel_launches - launches0, clk
+
+
+def bench_small(args, world, rank, local):
+    """CUBA, STDP or the multicompartment batch (args.workload), with the oracle port timed
+    on the host cores beside it."""
+    import torch
+
+    from brian2cuda_b200 import Network, models
+    from oracle.oracle import OracleHines, OracleNet
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    wl = args.workload
+    line = None
+    if wl == "cuba":
+        steps_run = 10_000
+        net = Network(DT, seed=models.SEED_BASE, device=local, stream=stream.cuda_stream)
+        ids = models.build_cuba(net, n=4000, dtype="float64")
+        net.finalize()
+        net.store(0)
+        P = ids["P"]
+        outdeg = net.out_degree(P).astype(np.int64)
+        net.run(500)
+        tune = net.autotune(trial_steps=50)
+        start = net.spikes_recorded(P)
+        ms, launches, clk = _timed_net_runs(net, stream, args, world, local, steps_run)
+        idx, _, _ = net.spikes_fetch(P, start, cap=1 << 26)
+        runs = args.warmup + args.steps
+        events = float(outdeg[idx].sum()) / runs * args.steps
+        nspk = len(idx) / runs
+        net.restore(0)
+        prof = net.profile(2000)
+        sec = ms / 1e3
+        value = events * world / sec
+        nb = BYTES["cuba_neuron"] * 4000.0
+        db = BYTES["cuba_event"] * events / (args.steps * steps_run)
+        dom = max(prof, key=lambda kv: kv[1])
+        roof = (_roofline(nb, dom[1], "lif_step_kernel") if dom[0] == 1 else
+                _roofline(db, dom[1], "deliver_add_batch_kernel"))
+        line = _line_base(args, world, "synaptic events/s", value, "events/s",
+                          ms / args.steps, WORKLOADS[wl],
+                          {"sim_steps_per_step": steps_run, "neurons": 4000,
+                           "synapses": ids["n_syn"], "parallelism": f"replicas x{world}",
+                           "l2": "working set < L2 (the net is 2.6 MB): no flush, see DESIGN.md"},
+                          "f64")
+        line.update({"neuron_updates_per_s": 4000.0 * steps_run * args.steps * world / sec,
+                     "firing_rate_hz": nspk / (4000 * steps_run * DT), "roofline": roof,
+                     "kernel_ms_mean_per_launch": {f"site {k}": v for k, v in prof},
+                     "autotune": tune, "gpu_launches": launches, "clocks": clk})
+        net.close()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            orc = OracleNet(DT, f32=False)
+            oids = models.build_cuba(orc, n=4000, dtype="float64")
+            orc.finalize()
+            t0 = time.perf_counter()
+            orc.run(steps_run)
+            el = time.perf_counter() - t0
+            oi, _ = orc.spikes(oids["P"])
+            line["cpu_baseline"] = {"value": float(outdeg[oi].sum()) / el, "unit": "events/s",
+                                    "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"the full 1 s run ({el:.1f} s), C++ oracle"}
+    elif wl == "stdp":
+        steps_run = 10_000
+        net = Network(DT, seed=models.SEED_BASE + 2, device=local, stream=stream.cuda_stream)
+        # per population; the output neurons (no refractory period) can fire every step
+        cap = int(1000 * steps_run * 1.05 * (args.warmup + args.steps + 1))
+        ids = models.build_stdp(net, monitor_capacity=cap)
+        net.finalize()
+        net.store(0)
+        tune = net.autotune(trial_steps=50)
+        s_in = net.spikes_recorded(ids["inp"])
+        ms, launches, clk = _timed_net_runs(net, stream, args, world, local, steps_run)
+        runs = args.warmup + args.steps
+        n_in = len(net.spikes_fetch(ids["inp"], s_in, cap=1 << 26)[0]) / runs * args.steps
+        n_out = len(net.spikes_fetch(ids["out"], s_in, cap=1 << 26)[0]) / runs * args.steps
+        ev_pre, ev_post = n_in * 1000.0, n_out * 10_000.0
+        net.restore(0)
+        prof = net.profile(2000)
+        sec = ms / 1e3
+        value = (ev_pre + ev_post) * world / sec
+        per_launch = {1: None, 2: BYTES["stdp_pre"] * ev_pre / (args.steps * steps_run),
+                      3: BYTES["stdp_post"] * ev_post / (args.steps * steps_run)}
+        dom = max(prof, key=lambda kv: kv[1])
+        kname = {1: "poisson/lif step", 2: "deliver_stdp_pre_kernel",
+                 3: "deliver_stdp_post_kernel"}.get(dom[0], "site")
+        b = per_launch.get(dom[0]) or (BYTES["stdp_neuron"] * 1000 + BYTES["poisson"] * 10_000)
+        line = _line_base(args, world, "synaptic events/s", value, "events/s",
+                          ms / args.steps, WORKLOADS[wl],
+                          {"sim_steps_per_step": steps_run, "neurons": 11_000,
+                           "synapses": 10_000_000, "parallelism": f"replicas x{world}",
+                           "l2": "working set > L2 (1e7 synapses x 4 f32 variables = 160 MB)"},
+                          "f32")
+        line.update({"on_pre_events_per_s": ev_pre / sec, "on_post_events_per_s": ev_post / sec,
+                     "neuron_updates_per_s": 11_000.0 * steps_run * args.steps * world / sec,
+                     "roofline": _roofline(b, dom[1], kname),
+                     "kernel_ms_mean_per_launch": {f"site {k}": v for k, v in prof},
+                     "autotune": tune, "gpu_launches": launches, "clocks": clk})
+        net.close()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            orc = OracleNet(DT, f32=True)
+            oids = models.build_stdp(orc, monitor_capacity=cap)
+            orc.finalize()
+            # the oracle's Poisson group reads supplied uniforms (the GPU draws them with cuRAND)
+            orc.set_uniforms(oids["inp"], np.random.default_rng(7).random((1000, 10_000),
+                                                                          dtype=np.float32))
+            t0 = time.perf_counter()
+            orc.run(1000)
+            el = time.perf_counter() - t0
+            oin = len(orc.spikes(oids["inp"])[0])
+            oout = len(orc.spikes(oids["out"])[0])
+            line["cpu_baseline"] = {"value": (oin * 1000.0 + oout * 10_000.0) / el,
+                                    "unit": "events/s", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"the first 1000 steps of the run ({el:.1f} s), "
+                                              "C++ oracle"}
+    elif wl == "hines":
+        steps_run = 8000
+        net = Network(25e-6, seed=models.SEED_BASE + 3, device=local, stream=stream.cuda_stream)
+        hb, morph, params, current = models.build_hines(net, n_neurons=1024)
+        for _ in range(args.warmup):
+            hb.run(steps_run)
+        net.sync()
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            hb.run(steps_run)
+        net.sync()
+        el = max_over_ranks(time.perf_counter() - t0, world)
+        clk = clocks.stop()
+        n_comp = hb.n_comp
+        value = float(n_comp) * steps_run * args.steps * world / el
+        line = _line_base(args, world, "compartment-updates/s", value, "compartment-updates/s",
+                          1e3 * el / args.steps, WORKLOADS[wl],
+                          {"sim_steps_per_step": steps_run, "neurons": 1024,
+                           "compartments": n_comp, "parallelism": f"replicas x{world}",
+                           "l2": "state held in shared memory across chunks of up to 1000 "
+                                 "steps; per chunk it moves through HBM once"},
+                          "f64")
+        line.update({"neuron_updates_per_s": 1024.0 * steps_run * args.steps * world / el,
+                     "roofline": _roofline(BYTES["hines_comp"] * n_comp * steps_run,
+                                           1e3 * el / args.steps, "hines_kernel"),
+                     "timing": "wall clock around b2b_hines_run with a device sync (one "
+                               "kernel per 1000-step chunk)",
+                     "gpu_launches": args.steps * (steps_run // 1000), "clocks": clk})
+        line["roofline"]["note"] = ("achieved = algorithmic 136 B per compartment-step / time; "
+                                    "the kernel keeps the state in shared memory, so HBM is "
+                                    "not what bounds it")
+        net.close()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            orc = OracleHines(25e-6, morph["comp_off"], morph["sec_off"], morph["sec_start"],
+                              morph["sec_end"], morph["sec_parent"], morph["diameter"],
+                              morph["length"], params, f32=True)
+            for k_, v_ in models.hines_rest_state().items():
+                orc.set_state(k_, v_)
+            orc.set_current(current)
+            t0 = time.perf_counter()
+            orc.run(200)
+            el2 = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": float(n_comp) * 200 / el2,
+                                    "unit": "compartment-updates/s", "cores": os.cpu_count(),
+                                    "kind": "port",
+                                    "sample": f"200 of the 8000 steps ({el2:.1f} s), C++ oracle"}
+    if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
 
 

@@ -500,12 +500,14 @@ b2b_status build_proj(b2b_net* net, int pj) {
   if (pr.effect == B2B_EFFECT_STDP) {
     const b2b_stdp_params& sp = net->syns[pr.members[0]].stdp;
     CHECK(pr.n_syn < (1ll << 31), B2B_ERR_UNSUPPORTED, "STDP projection above 2^31 synapses");
-    CU(dalloc(pr, (uint8_t**)&D.apre, rs * (size_t)pr.n_syn));
-    CU(dalloc(pr, (uint8_t**)&D.apost, rs * (size_t)pr.n_syn));
-    CU(dalloc(pr, (uint8_t**)&D.lastupdate, rs * (size_t)pr.n_syn));
-    CU(cudaMemsetAsync(D.apre, 0, rs * pr.n_syn, s));
-    CU(cudaMemsetAsync(D.apost, 0, rs * pr.n_syn, s));
-    CU(cudaMemsetAsync(D.lastupdate, 0, rs * pr.n_syn, s));
+    // one interleaved record per synapse; the scattered initial weights move into it
+    CU(dalloc(pr, (uint8_t**)&D.syn4, 4 * rs * (size_t)pr.n_syn));
+    CU(pack_stdp(pr.w, D.syn4, pr.dtype, pr.n_syn, s));
+    CU(cudaStreamSynchronize(s));
+    pr.allocs.erase(std::remove(pr.allocs.begin(), pr.allocs.end(), pr.w), pr.allocs.end());
+    cudaFree(pr.w);
+    pr.w = nullptr;
+    D.w = nullptr;
     D.taupre = sp.taupre; D.taupost = sp.taupost; D.dApre = sp.dApre; D.dApost = sp.dApost;
     D.wmin = sp.wmin; D.wmax = sp.wmax; D.pre_adds_weight = sp.pre_adds_weight;
     int64_t* poff = nullptr;
@@ -718,11 +720,7 @@ std::vector<std::pair<void*, size_t>> state_arrays(b2b_net* net) {
   }
   for (Proj& pr : net->projs) {
     if (pr.effect != B2B_EFFECT_STDP) continue;
-    const size_t b = real_size(pr.dtype) * pr.n_syn;
-    out.emplace_back(pr.w, b);
-    out.emplace_back(pr.dev.apre, b);
-    out.emplace_back(pr.dev.apost, b);
-    out.emplace_back(pr.dev.lastupdate, b);
+    out.emplace_back(pr.dev.syn4, 4 * real_size(pr.dtype) * pr.n_syn);
   }
   return out;
 }
@@ -1706,10 +1704,14 @@ b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64
   const Group& gpost = net->groups[sy.post_gid];
   const int32_t nd = pr.dmax - pr.dmin + 1;
   const void* arr = nullptr;
-  if (var == B2B_SYN_W) arr = pr.w;
-  if (var == B2B_SYN_APRE) arr = pr.dev.apre;
-  if (var == B2B_SYN_APOST) arr = pr.dev.apost;
-  if (var == B2B_SYN_LASTUPDATE) arr = pr.dev.lastupdate;
+  int64_t stride = 1;
+  if (pr.effect == B2B_EFFECT_STDP && var >= B2B_SYN_W) {
+    // component (var - W) of the interleaved {w, Apre, Apost, lastupdate} records
+    arr = static_cast<const uint8_t*>(pr.dev.syn4) + real_size(pr.dtype) * (var - B2B_SYN_W);
+    stride = 4;
+  } else if (var == B2B_SYN_W) {
+    arr = pr.w;
+  }
   const int64_t* inv = sy.inv;  // NULL for generated synapses: positions are the numbering
   const size_t es = (var <= B2B_SYN_DELAY) ? 4 : real_size(pr.dtype);
   void* d_out = nullptr;
@@ -1717,7 +1719,7 @@ b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64
   cudaError_t e = gather_syn_var(pr, var, inv, sy.base, n,
                                  (gpre.offset + sy.pre_lo) * (int64_t)nd,
                                  (gpre.offset + sy.pre_hi) * (int64_t)nd, gpre.offset,
-                                 gpost.offset, arr, sy.w_scalar, d_out, net->stream);
+                                 gpost.offset, arr, stride, sy.w_scalar, d_out, net->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(host, d_out, es * n, cudaMemcpyDeviceToHost, net->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
   cudaFree(d_out);

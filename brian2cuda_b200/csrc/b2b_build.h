@@ -29,9 +29,11 @@ cudaError_t build_post_index(const int32_t* d_post, int64_t n_syn, int64_t dst_l
                              int64_t* max_count, cudaStream_t s);
 cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_t pos_base,
                            int64_t n, int64_t key_lo, int64_t key_hi, int64_t src_offset,
-                           int64_t dst_offset, const void* d_arr, double w_scalar,
-                           void* d_out, cudaStream_t s);
+                           int64_t dst_offset, const void* d_arr, int64_t stride,
+                           double w_scalar, void* d_out, cudaStream_t s);
 // Adds the out-degree (all delays) of source neurons [first, first + n) into d_out.
 cudaError_t add_out_degree(const int64_t* d_off, int32_t nd, int64_t first, int64_t n,
                            int32_t* d_out, cudaStream_t s);
+// Interleaved STDP records {w, Apre = 0, Apost = 0, lastupdate = 0} from initial weights.
+cudaError_t pack_stdp(const void* d_w, void* d_syn4, int dtype, int64_t n, cudaStream_t s);
 }  // namespace b2b

@@ -85,7 +85,8 @@ struct ProjDev {
   const double* mem_w;            // per-member scalar weight (members differ), or NULL
   void* targets[3];               // per variable v, ge, gi
   // STDP
-  void* apre; void* apost; void* lastupdate;
+  void* syn4;                     // per synapse {w, Apre, Apost, lastupdate}, interleaved so
+                                  // that a strided (on_post) visit touches one sector
   double taupre, taupost, dApre, dApost, wmin, wmax;
   int32_t pre_adds_weight;
   int32_t aggregate;              // warp-aggregate atomics (few targets)

@@ -152,7 +152,8 @@ __global__ void gather_kernel(int var, int64_t n, int64_t pos_base, const int64_
                               const int64_t* __restrict__ off, int64_t key_lo, int64_t key_hi,
                               int32_t nd, int32_t dmin, int64_t src_offset,
                               const int32_t* __restrict__ post, int64_t dst_offset,
-                              const R* __restrict__ arr, double w_scalar, void* out) {
+                              const R* __restrict__ arr, int64_t stride, double w_scalar,
+                              void* out) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pos = inv ? inv[q] : pos_base + q;
@@ -169,7 +170,7 @@ __global__ void gather_kernel(int var, int64_t n, int64_t pos_base, const int64_
                                            : (int32_t)(lo % nd + dmin);
       static_cast<int32_t*>(out)[q] = val;
     } else {
-      static_cast<R*>(out)[q] = arr ? arr[pos] : (R)w_scalar;
+      static_cast<R*>(out)[q] = arr ? arr[pos * stride] : (R)w_scalar;
     }
   }
 }
@@ -320,21 +321,21 @@ cudaError_t build_post_index(const int32_t* d_post, int64_t n_syn, int64_t dst_l
 
 cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_t pos_base,
                            int64_t n, int64_t key_lo, int64_t key_hi, int64_t src_offset,
-                           int64_t dst_offset, const void* d_arr, double w_scalar,
-                           void* d_out, cudaStream_t s) {
+                           int64_t dst_offset, const void* d_arr, int64_t stride,
+                           double w_scalar, void* d_out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   if (pr.dtype == B2B_F32)
     gather_kernel<float><<<grid_for(n), 256, 0, s>>>(var, n, pos_base, d_inv, pr.off, key_lo,
                                                      key_hi, pr.dmax - pr.dmin + 1, pr.dmin,
                                                      src_offset, pr.post, dst_offset,
                                                      static_cast<const float*>(d_arr),
-                                                     w_scalar, d_out);
+                                                     stride, w_scalar, d_out);
   else
     gather_kernel<double><<<grid_for(n), 256, 0, s>>>(var, n, pos_base, d_inv, pr.off, key_lo,
                                                       key_hi, pr.dmax - pr.dmin + 1, pr.dmin,
                                                       src_offset, pr.post, dst_offset,
                                                       static_cast<const double*>(d_arr),
-                                                      w_scalar, d_out);
+                                                      stride, w_scalar, d_out);
   return cudaGetLastError();
 }
 
@@ -354,6 +355,32 @@ cudaError_t add_out_degree(const int64_t* d_off, int32_t nd, int64_t first, int6
                            int32_t* d_out, cudaStream_t s) {
   const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096));
   out_degree_kernel<<<(unsigned)blocks, 256, 0, s>>>(d_off, nd, first, n, d_out);
+  return cudaGetLastError();
+}
+
+// STDP synapse records {w, 0, 0, 0} from the per-synapse initial weights.
+namespace {
+template <typename R>
+__global__ void pack_stdp_kernel(const R* __restrict__ w, R* __restrict__ syn4, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    syn4[4 * i] = w[i];
+    syn4[4 * i + 1] = (R)0;
+    syn4[4 * i + 2] = (R)0;
+    syn4[4 * i + 3] = (R)0;
+  }
+}
+}  // namespace
+
+cudaError_t pack_stdp(const void* d_w, void* d_syn4, int dtype, int64_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8192));
+  if (dtype == B2B_F32)
+    pack_stdp_kernel<float><<<g, 256, 0, s>>>(static_cast<const float*>(d_w),
+                                              static_cast<float*>(d_syn4), n);
+  else
+    pack_stdp_kernel<double><<<g, 256, 0, s>>>(static_cast<const double*>(d_w),
+                                               static_cast<double*>(d_syn4), n);
   return cudaGetLastError();
 }
 

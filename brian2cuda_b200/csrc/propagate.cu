@@ -80,16 +80,19 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
 // ---- on_pre of event-driven additive STDP (examples/stdp.py:125-186) ----------------------
 // Traces decay lazily from lastupdate to t (Brian2's event-driven update); in float32 the
 // elapsed time is rounded to float first, as brian2cuda does (brian2cuda/device.py:1034-1039).
+// A synapse's four variables are one interleaved record (one 16-byte access in float32).
+template <typename R>
+struct __align__(4 * sizeof(R)) SynRec {
+  R w, apre, apost, lu;
+};
+
 template <typename R, bool AGG, bool WARP_PREFIX>
 __global__ void __launch_bounds__(kDeliverBlock)
 deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, double dt) {
   extern __shared__ int s_pref[];
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
-  R* __restrict__ W = static_cast<R*>(const_cast<void*>(P.w));
-  R* __restrict__ Apre = static_cast<R*>(P.apre);
-  R* __restrict__ Apost = static_cast<R*>(P.apost);
-  R* __restrict__ LU = static_cast<R*>(P.lastupdate);
+  SynRec<R>* __restrict__ S = static_cast<SynRec<R>*>(P.syn4);
   R* __restrict__ T = static_cast<R*>(P.target);
   const R taupre = (R)P.taupre, taupost = (R)P.taupost, dApre = (R)P.dApre;
   const R wmin = (R)P.wmin, wmax = (R)P.wmax;
@@ -100,16 +103,17 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
     R w = 0;
     if (valid) {
       post = __ldg(P.post + s);
-      w = W[s];
-      R apre = Apre[s], apost = Apost[s];
-      const R tau = (R)(t - (double)LU[s]);
-      apre = apre * dexp(-tau / taupre);
-      apost = apost * dexp(-tau / taupost);
+      SynRec<R> r = S[s];
+      w = r.w;
+      const R tau = (R)(t - (double)r.lu);
+      R apre = r.apre * dexp(-tau / taupre);
+      const R apost = r.apost * dexp(-tau / taupost);
       apre = apre + dApre;
-      W[s] = dclip(w + apost, wmin, wmax);
-      Apre[s] = apre;
-      Apost[s] = apost;
-      LU[s] = (R)t;
+      r.w = dclip(w + apost, wmin, wmax);
+      r.apre = apre;
+      r.apost = apost;
+      r.lu = (R)t;
+      S[s] = r;
     }
     if (P.pre_adds_weight) add_to_target<R, AGG>(T, post, w, valid);
   });
@@ -126,10 +130,7 @@ deliver_stdp_post_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, do
   const int slot = ring_slot(ts, P.post_ring_len);
   const int nspk = P.post_ring_cnt[slot];
   const int32_t* spikes = P.post_ring_idx + (int64_t)slot * P.post_src_n;
-  R* __restrict__ W = static_cast<R*>(const_cast<void*>(P.w));
-  R* __restrict__ Apre = static_cast<R*>(P.apre);
-  R* __restrict__ Apost = static_cast<R*>(P.apost);
-  R* __restrict__ LU = static_cast<R*>(P.lastupdate);
+  SynRec<R>* __restrict__ S = static_cast<SynRec<R>*>(P.syn4);
   const R taupre = (R)P.taupre, taupost = (R)P.taupost, dApost = (R)P.dApost;
   const R wmin = (R)P.wmin, wmax = (R)P.wmax;
   const int lane = threadIdx.x & 31;
@@ -145,15 +146,16 @@ deliver_stdp_post_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, do
     if (b1 > b0 + kChunk) b1 = b0 + kChunk;
     for (int64_t r = b0 + lane; r < b1; r += 32) {
       const int64_t s = P.post_syn[r];
-      R apre = Apre[s], apost = Apost[s];
-      const R tau = (R)(t - (double)LU[s]);
-      apre = apre * dexp(-tau / taupre);
-      apost = apost * dexp(-tau / taupost);
+      SynRec<R> q = S[s];
+      const R tau = (R)(t - (double)q.lu);
+      const R apre = q.apre * dexp(-tau / taupre);
+      R apost = q.apost * dexp(-tau / taupost);
       apost = apost + dApost;
-      W[s] = dclip(W[s] + apre, wmin, wmax);
-      Apre[s] = apre;
-      Apost[s] = apost;
-      LU[s] = (R)t;
+      q.w = dclip(q.w + apre, wmin, wmax);
+      q.apre = apre;
+      q.apost = apost;
+      q.lu = (R)t;
+      S[s] = q;
     }
   }
 }
