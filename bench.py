@@ -436,8 +436,8 @@ def bench_batched(args, world, rank, local):
     import torch
 
     from brian2cuda_b200 import Network, models
-    from brian2cuda_b200.surrogate import (GatingSurrogate, gating_targets, sample_states,
-                                           surrogate_stats)
+    from brian2cuda_b200.surrogate import (GatingSurrogate, gating_targets, physiological,
+                                           sample_states, surrogate_stats)
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
     sizes, we = models.batch_sizes()
@@ -518,7 +518,7 @@ def bench_batched(args, world, rank, local):
         ref_net.run(5)
         xs.extend(sample_states(ref_net, g) for g in big)
     ref_net.close()
-    x = torch.cat(xs)
+    x = physiological(torch.cat(xs))
     x = x[torch.randperm(len(x), device=x.device)[:10_000_000]].contiguous()
     t = gating_targets(models.cobahh_hh(), DT, x)
     surr = GatingSurrogate(device=local, seed=3)

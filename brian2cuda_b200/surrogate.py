@@ -186,6 +186,17 @@ def trajectory_states(net: Network, gid: int, n_samples: int, every: int = 10,
     return torch.cat(chunks)
 
 
+def physiological(x, v_lo: float = -0.15, v_hi: float = 0.1):
+    """The rows of x whose values are finite and whose v lies in [v_lo, v_hi] volts.  Training
+    data should pass through this: b2b_mlp_fit_scaling maps the data's v range to the
+    network's input range, so a few runaway states (a neuron with a negative conductance and
+    no input drifts to volts) would leave the physiological range a sliver of it; states
+    outside the training range are stepped exactly by the surrogate kernel."""
+    import torch
+    ok = torch.isfinite(x).all(dim=1) & (x[:, 0] >= v_lo) & (x[:, 0] <= v_hi)
+    return x[ok].contiguous()
+
+
 def surrogate_stats(net: Network, gid: int) -> tuple[int, int]:
     """(neuron-updates made with the surrogate, exact fallbacks among them)."""
     u, f = C.c_int64(), C.c_int64()

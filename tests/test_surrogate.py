@@ -171,12 +171,17 @@ def _trajectories(n_neurons, n_samples, seed, **kw):
 
 def _dataset():
     """States of COBAHH trajectories (coupled, and pseudo-coupled with 1e-9 nS weights) and
-    their exact gating steps."""
+    their exact gating steps.  The reference's initial conductances (N(0,1) x 12 + 20 x 10 nS
+    for gi) are negative for a few neurons; without synaptic input such a neuron's v runs away
+    (-1.6 V after ~120 steps) until its rates overflow float32.  Such states would stretch the
+    input scaling over volts, so only states with v in [-150, 100] mV are kept (the surrogate
+    steps states outside its training range exactly)."""
     from brian2cuda_b200 import models
-    from brian2cuda_b200.surrogate import gating_targets
+    from brian2cuda_b200.surrogate import gating_targets, physiological
     torch = _torch()
     x = torch.cat([_trajectories(20000, 1_800_000, 1),
-                   _trajectories(20000, 1_200_000, 5, we=1e-18, wi=1e-18)])
+                   _trajectories(20000, 1_000_000, 5, we=1e-18, wi=1e-18)])
+    x = physiological(x)
     return x, gating_targets(models.cobahh_hh(), DT, x)
 
 
