@@ -599,6 +599,41 @@ b2b_status finalize_projs(b2b_net* net) {
 
 // One kernel per step (fused.cu) applies when the net is one LIF/HH population whose
 // synapses are all additive onto ge/gi of that population with delays of at least one step.
+// A small network (small.cu, opt-in with B2B_NET_SMALL) runs every step of a chunk in one
+// CTA: one LIF/HH population of at most 4096 neurons (no gating surrogate) whose Synapses
+// objects are all additive and target it, with the state fitting the CTA's shared memory.
+b2b_status setup_small(b2b_net* net) {
+  if (!(net->cfg.flags & B2B_NET_SMALL) || (net->cfg.flags & (B2B_NET_CHECKED | B2B_NET_FUSED)))
+    return B2B_OK;
+  if (net->pops.size() != 1 || net->projs.size() > kMaxProjBatch) return B2B_OK;
+  const Pop& pop = net->pops[0];
+  if ((pop.kind != KIND_LIF && pop.kind != KIND_HH) || pop.surr_img || pop.n > 4096)
+    return B2B_OK;
+  SmallDev& D = net->sdev;
+  D = SmallDev{};
+  D.pop = pop.dev;
+  D.n_proj = (int32_t)net->projs.size();
+  D.nd_max = 1;
+  D.warp_prefix = 1;
+  for (size_t p = 0; p < net->projs.size(); ++p) {
+    const Proj& pr = net->projs[p];
+    if (pr.effect != B2B_EFFECT_ADD || pr.src_pop != 0 || pr.dst_pop != 0) return B2B_OK;
+    for (int m : pr.members) {
+      const int v = net->syns[m].target_var;
+      if (v != B2B_VAR_V && v != B2B_VAR_GE && v != B2B_VAR_GI) return B2B_OK;
+    }
+    D.proj[p] = pr.dev;
+    D.proj_target[p] = pr.target_var;
+    D.nd_max = std::max<int32_t>(D.nd_max, pr.dev.nd);
+    if (pr.dev.nd > 64) D.warp_prefix = 0;
+  }
+  if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) return B2B_OK;
+  D.ring_in_smem = 1;
+  if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) D.ring_in_smem = 0;
+  net->small = true;
+  return B2B_OK;
+}
+
 b2b_status setup_fused(b2b_net* net) {
   if (!(net->cfg.flags & B2B_NET_FUSED)) return B2B_OK;
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
@@ -651,6 +686,14 @@ b2b_status setup_fused(b2b_net* net) {
 
 // ---------------------------------------------------------------------------------------
 b2b_status enqueue_steps(b2b_net* net, int kk) {
+  if (net->small) {
+    const Pop& pop = net->pops[0];
+    CU(launch_small(net->sdev, pop.kind, pop.dtype, net->d_clock, kk, net->cfg.dt,
+                    net->d_status, net->stream));
+    CU(launch_tick(net->d_clock, kk, net->stream));
+    net->launches += 2;
+    return B2B_OK;
+  }
   if (net->fused) {
     const Pop& pop = net->pops[0];
     for (int k = 0; k < kk; ++k) {
@@ -1069,6 +1112,7 @@ b2b_status b2b_finalize(b2b_net* net) {
   b2b_status st = finalize_pops(net);
   if (st == B2B_OK) st = finalize_projs(net);
   if (st == B2B_OK) st = setup_fused(net);
+  if (st == B2B_OK) st = setup_small(net);
   if (st != B2B_OK) return st;
   CU(cudaMemcpy(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice));
   CU(cudaDeviceSynchronize());
@@ -1110,7 +1154,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   GUARD_BEGIN
   struct Site { int kind; int idx; };
   std::vector<Site> sites;
-  if (net->fused) {
+  if (net->small) {
+    sites.push_back({7, 0});
+  } else if (net->fused) {
     sites.push_back({5, 0});
   } else {
     for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
@@ -1136,6 +1182,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
+      if (s.kind == 7)
+        e = launch_small(net->sdev, net->pops[0].kind, net->pops[0].dtype, clk, 1, net->cfg.dt,
+                         net->d_status, net->stream);
       if (s.kind == 5)
         e = launch_fused_step(net->fdev, net->pops[0].kind, net->pops[0].dtype, net->fused_grid,
                               clk, 0, net->cfg.dt, net->d_status, net->stream);
@@ -1240,6 +1289,10 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   CHECK(trial_steps > 0 && trial_steps <= 100000 && n_out, B2B_ERR_INVALID_ARG, "bad arguments");
   CHECK(!net->fused, B2B_ERR_UNSUPPORTED, "the one-kernel-per-step path has no tunable shapes");
+  if (net->small) {  // one CTA with a fixed shape: nothing to tune
+    *n_out = 0;
+    return B2B_OK;
+  }
   GUARD_BEGIN
   CU(cudaStreamSynchronize(net->stream));
   // the state to start every trial from, in a slot of its own; monitor counts to put back
@@ -1444,7 +1497,7 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t) {
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode) {
   if (!net || !mode) return B2B_ERR_INVALID_ARG;
   if (!net->finalized) return fail(net, B2B_ERR_STATE, "call b2b_finalize first");
-  *mode = net->fused ? 1 : 0;
+  *mode = net->small ? 2 : (net->fused ? 1 : 0);
   return B2B_OK;
 }
 

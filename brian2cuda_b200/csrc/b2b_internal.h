@@ -111,6 +111,17 @@ struct FusedDev {
   void* acc[3];                   // per target variable (v, ge, gi): [2][pop.n] or NULL
 };
 
+// Device view of the one-CTA path for small networks (small.cu): one LIF/HH population of at
+// most 4096 neurons and its additive projections onto itself.
+struct SmallDev {
+  PopDev pop;
+  ProjDev proj[kMaxProjBatch];
+  int32_t proj_target[kMaxProjBatch];   // target variable of each projection's first member
+  int32_t n_proj, nd_max;
+  int32_t warp_prefix;                  // every projection has <= 64 delays
+  int32_t ring_in_smem;                 // the spike-history ring is mirrored in shared memory
+};
+
 struct Group {
   int kind = 0, dtype = 0, pop = -1;
   int64_t n = 0, offset = 0;
@@ -214,6 +225,8 @@ struct b2b_net {
   std::vector<b2b::Proj> projs;
   std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
   std::vector<b2b::AddTune> add_tune;      // launch shape per add batch (b2b_autotune)
+  bool small = false;                      // one CTA runs every step (small.cu)
+  b2b::SmallDev sdev{};
   bool fused = false;                      // one kernel per step (fused.cu) in use
   b2b::FusedDev fdev{};
   int fused_grid = 0;
@@ -250,6 +263,10 @@ cudaError_t launch_hh_sample(const Pop& pop, int64_t off, int64_t n, float* dev_
 // Packed device image and device ordinal of a surrogate network.
 const void* mlp_image(const b2b_mlp* m);
 int mlp_device(const b2b_mlp* m);
+// Small networks (small.cu): `steps` steps of the net in one one-CTA launch.
+size_t small_smem(const SmallDev& D, int kind, int dtype);
+cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
+                         int steps, double dt, int32_t* status, cudaStream_t s);
 // One kernel per step (fused.cu): the step itself, and the fold of the pending input.
 size_t fused_smem(const FusedDev& F);
 int fused_block();

@@ -1,0 +1,309 @@
+// Small networks: every step of a chunk inside one CTA, with the neuron state in shared
+// memory.
+//
+// A network of a few thousand neurons (the CUBA example: 4000 LIF neurons, about two spikes
+// per step) leaves the per-step path launch-bound: each step is a neuron launch and a delivery
+// launch of a few microseconds, nearly all of it launch and synchronisation latency (the
+// reference is bound the same way at a larger scale: one launch per code object per step,
+// brian2cuda/templates/network.cu:65-115).  When the net is one LIF or HH population of at
+// most 4096 neurons whose synapses are all additive and target it, and the caller opts in
+// (B2B_NET_SMALL), one CTA of 1024 threads runs a whole chunk of steps: it loads the state into shared memory once, then per step
+// updates four neurons per thread, compacts the spikes with a block scan into the same
+// spike-history ring and monitor the per-step kernels write, delivers the due bundles
+// (every warp of the CTA, 32 synapses per warp and item) with atomic additions into the
+// shared-memory targets,
+// applies a deferred reset if the schedule needs one, and writes the state back at the end.
+// Block barriers separate the phases, so Brian2's order within a step (groups, thresholds,
+// synapses, resets) is kept, delays of zero steps included.  Measured on B200 against the
+// per-step kernels: CUBA-type LIF nets of 500 / 1000 / 2000 neurons 3.8 / 4.4 / 5.8 us per
+// step against 4.9 / 5.5 / 6.6 us; at 4000 neurons, or with many delays (COBAHH with delays
+// of 1-50 steps), one SM's issue rate loses to the whole GPU, so the path is opt-in.
+#include <algorithm>
+
+#include "delivery.cuh"
+#include "neuron_common.cuh"
+
+namespace b2b {
+
+namespace {
+
+constexpr int kSmallThreads = 1024;
+
+// Shared-memory image of the population: one array per real-valued variable of the kind,
+// then the not_refractory flags, then the delivery prefix of the block path.
+struct SmallLayout {
+  int nvars;              // real-valued variables held
+  int var[kMaxVars];      // their B2B_VAR_* ids
+};
+
+__host__ __device__ inline SmallLayout small_layout(int kind) {
+  SmallLayout L{};
+  const int lif[] = {B2B_VAR_V, B2B_VAR_GE, B2B_VAR_GI, B2B_VAR_LASTSPIKE};
+  const int hh[] = {B2B_VAR_V, B2B_VAR_GE, B2B_VAR_GI, B2B_VAR_M, B2B_VAR_H, B2B_VAR_N,
+                    B2B_VAR_LASTSPIKE};
+  if (kind == KIND_LIF) {
+    L.nvars = 4;
+    for (int i = 0; i < 4; ++i) L.var[i] = lif[i];
+  } else {
+    L.nvars = 7;
+    for (int i = 0; i < 7; ++i) L.var[i] = hh[i];
+  }
+  return L;
+}
+
+// Delivery of the bundles of projection J due at step ts by every warp of the CTA: a work
+// item is 32 synapses of one due bundle (one synapse per lane), items go to the warps in
+// turn, so the few bundles of a small network's step are spread over the whole CTA rather
+// than walked by one warp while the others wait at the next barrier.
+template <typename R, bool WP>
+__device__ __forceinline__ void small_deliver(const ProjDev& J, int64_t ts, int* s_pref) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  DuePrefix wp{};
+  int nspk;
+  if constexpr (WP) {
+    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd);
+    nspk = wp.total;
+  } else {
+    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, s_pref);
+  }
+  const int sub = J.chunks * (kChunk / 32);
+  const int64_t items = (int64_t)nspk * sub;
+  const int base = ring_slot(ts, J.src_ring_len);
+  const R* W = static_cast<const R*>(J.w);
+  MemberCache<R> mc;
+  for (int64_t it = warp; it < items; it += nwarps) {   // warp-uniform
+    const int sp = (int)(it / sub);
+    const int ch = (int)(it - (int64_t)sp * sub);
+    int kk;
+    int di;
+    if constexpr (WP) di = find_delay_warp(wp, sp, &kk);
+    else di = find_delay_block(s_pref, J.nd, sp, &kk);
+    const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
+    const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
+    const int64_t key = (int64_t)pre * J.nd + di;
+    const int64_t s = J.off[key] + (int64_t)ch * 32 + lane;
+    if (s < J.off[key + 1]) {
+      const int32_t post = __ldg(J.post + s);
+      member_lookup<R>(J, pre, mc);
+      const R w = W ? __ldg(W + s) : mc.w;
+      atomicAdd(mc.target + post, w);
+    }
+  }
+}
+
+template <typename R, int KIND>
+__global__ void __launch_bounds__(kSmallThreads, 1)
+small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
+                 int steps, double dt, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const PopDev& P = D.pop;
+  const SmallLayout L = small_layout(KIND);
+  const int64_t n = P.n;   // padded population size, <= 4 * kSmallThreads
+  // column c of the image holds variable L.var[c]; v, ge, gi are columns 0-2 for both kinds,
+  // lastspike the last one, m, h, n columns 3-5 of HH
+  R* const base = reinterpret_cast<R*>(smem);
+  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const sV = base;
+  R* const sGE = base + n;
+  R* const sGI = base + 2 * n;
+  R* const sLS = base + kLS * n;
+  R* const sM = base + 3 * n;   // HH only
+  R* const sH = base + 4 * n;
+  R* const sN = base + 5 * n;
+  uint8_t* snr = smem + sizeof(R) * L.nvars * n;
+  int* s_pref = reinterpret_cast<int*>(smem + ((sizeof(R) * L.nvars * n + n + 15) & ~15));
+  // the spike-history ring's counts, and its indices when they fit, mirrored in shared memory
+  // (every write goes to both; delivery reads the mirror)
+  int32_t* s_ring_cnt = s_pref + D.nd_max + 2;
+  int32_t* s_ring = D.ring_in_smem ? s_ring_cnt + ((P.ring_len + 3) & ~3) : nullptr;
+  __shared__ int s_warp[33];
+  __shared__ unsigned long long s_mbase, s_mon;
+  const int tid = threadIdx.x;
+  const int64_t ts0 = clock[0];
+
+  // state -> shared memory
+  for (int i = 0; i < L.nvars; ++i) {
+    const R* g = static_cast<const R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < n; q += blockDim.x) base[i * n + q] = g[q];
+  }
+  {
+    const uint8_t* g = static_cast<const uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < n; q += blockDim.x) snr[q] = g[q];
+  }
+  for (int r = tid; r < P.ring_len; r += blockDim.x) s_ring_cnt[r] = P.ring_cnt[r];
+  if (s_ring)
+    for (int64_t r = tid; r < (int64_t)P.ring_len * n; r += blockDim.x) s_ring[r] = P.ring_idx[r];
+  if (tid == 0) s_mon = P.mon_cnt ? *P.mon_cnt : 0ull;
+  // the delivery targets of every projection are the shared-memory arrays, and its source
+  // ring the shared-memory mirror
+  __shared__ ProjDev J[kMaxProjBatch];
+  if (tid < D.n_proj) {
+    J[tid] = D.proj[tid];
+    for (int v = 0; v < 3; ++v) J[tid].targets[v] = base + v * n;   // v, ge, gi
+    J[tid].target = base + D.proj_target[tid] * n;
+    J[tid].src_ring_cnt = s_ring_cnt;
+    if (s_ring) J[tid].src_ring_idx = s_ring;
+  }
+  __syncthreads();
+
+  const double inv_dt = 1.0 / dt;
+  for (int k = 0; k < steps; ++k) {
+    const int64_t ts = ts0 + k;
+    const double t = (double)ts * dt;
+    const int slot = ring_slot(ts, P.ring_len);
+    // ---- groups and thresholds: neurons 4*tid .. 4*tid + 3
+    unsigned fl = 0;
+    const int64_t q4 = (int64_t)tid;
+    if (4 * q4 < n) {
+      const int gidx = P.vec_group ? P.vec_group[q4] : 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t i = 4 * q4 + e;
+        R v = sV[i], ge = sGE[i], gi = sGI[i];
+        R ls = sLS[i];
+        bool nr = true;
+        if constexpr (KIND == KIND_LIF) {
+          const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R vn = lif_advance<R>(g, v, ge, gi, nr);
+          if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
+            fl |= 1u << e;
+          }
+          v = vn;
+          if (refr) {
+            sLS[i] = ls;
+            snr[i] = nr ? 1 : 0;
+          }
+        } else {
+          const HhDev& g = static_cast<const HhDev*>(P.params)[gidx];
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R m = sM[i], h = sH[i], nn = sN[i];
+          const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt);
+          if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            fl |= 1u << e;
+          }
+          v = vn;
+          sM[i] = m;
+          sH[i] = h;
+          sN[i] = nn;
+          if (refr) {
+            sLS[i] = ls;
+            snr[i] = nr ? 1 : 0;
+          }
+        }
+        sV[i] = v;
+        sGE[i] = ge;
+        sGI[i] = gi;
+      }
+    }
+    // ---- compaction into ring slot ts (ascending neuron order) and the monitor
+    int total;
+    const int c = __popc(fl);
+    const int excl = block_exclusive_scan(c, s_warp, &total);
+    if (tid == 0) {
+      const int next = ring_slot(ts + 1, P.ring_len);
+      P.ring_cnt[slot] = total;
+      P.ring_cnt[next] = 0;
+      s_ring_cnt[slot] = total;
+      s_ring_cnt[next] = 0;
+      s_mbase = s_mon;     // this kernel is the monitor's only writer while it runs
+      s_mon += (unsigned long long)total;
+    }
+    if (c) {
+      int pos = excl;
+      int32_t* out = P.ring_idx + (int64_t)slot * P.n;
+      int32_t* sout = s_ring ? s_ring + (int64_t)slot * n : nullptr;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!(fl & (1u << e))) continue;
+        out[pos] = (int32_t)(4 * q4 + e);
+        if (sout) sout[pos] = (int32_t)(4 * q4 + e);
+        ++pos;
+      }
+    }
+    __syncthreads();
+    if (c && P.mon_cnt) {
+      unsigned long long mpos = s_mbase + (unsigned long long)excl;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!(fl & (1u << e))) continue;
+        if (mpos < (unsigned long long)P.mon_cap) {
+          P.mon_idx[mpos] = (int32_t)(4 * q4 + e);
+          P.mon_step[mpos] = ts;
+        } else {
+          set_status(status, B2B_ERR_QUEUE_OVERFLOW);
+        }
+        ++mpos;
+      }
+    }
+    // ---- synapses: bundles due at step ts, effects into the shared-memory targets
+    for (int p = 0; p < D.n_proj; ++p) {
+      if (D.warp_prefix) small_deliver<R, true>(J[p], ts, s_pref);
+      else small_deliver<R, false>(J[p], ts, s_pref);
+      __syncthreads();
+    }
+    // ---- resets deferred after the synapses (a synapse writes the reset variable)
+    if constexpr (KIND == KIND_LIF) {
+      if (P.late_reset) {
+        const int32_t* idx = s_ring ? s_ring + (int64_t)slot * n : P.ring_idx + (int64_t)slot * P.n;
+        for (int r = tid; r < total; r += blockDim.x) {
+          const int32_t i = idx[r];
+          const LifDev& g = static_cast<const LifDev*>(P.params)[P.vec_group ? P.vec_group[i >> 2] : 0];
+          if (g.has_reset) sV[i] = (R)g.Vr;
+        }
+        __syncthreads();
+      }
+    }
+  }
+  // shared memory -> state
+  for (int i = 0; i < L.nvars; ++i) {
+    R* g = static_cast<R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < n; q += blockDim.x) g[q] = base[i * n + q];
+  }
+  {
+    uint8_t* g = static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < n; q += blockDim.x) g[q] = snr[q];
+  }
+  if (tid == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
+}
+
+}  // namespace
+
+size_t small_smem(const SmallDev& D, int kind, int dtype) {
+  const SmallLayout L = small_layout(kind);
+  const size_t rs = dtype == B2B_F32 ? 4 : 8;
+  const size_t base = (rs * L.nvars * (size_t)D.pop.n + (size_t)D.pop.n + 15) & ~(size_t)15;
+  size_t bytes = base + sizeof(int) * (size_t)(D.nd_max + 2) +
+                 sizeof(int) * (size_t)((D.pop.ring_len + 3) & ~3);
+  if (D.ring_in_smem) bytes += sizeof(int32_t) * (size_t)D.pop.ring_len * (size_t)D.pop.n;
+  return bytes;
+}
+
+cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
+                         int steps, double dt, int32_t* status, cudaStream_t s) {
+  const size_t smem = small_smem(D, kind, dtype);
+  cudaError_t e = cudaSuccess;
+#define B2B_SMALL(R, K)                                                                       \
+  do {                                                                                        \
+    e = cudaFuncSetAttribute(small_net_kernel<R, K>,                                          \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);         \
+    if (e == cudaSuccess)                                                                     \
+      small_net_kernel<R, K><<<1, kSmallThreads, smem, s>>>(D, clock, steps, dt, status);     \
+  } while (0)
+  if (kind == KIND_LIF && dtype == B2B_F32) B2B_SMALL(float, KIND_LIF);
+  else if (kind == KIND_LIF) B2B_SMALL(double, KIND_LIF);
+  else if (dtype == B2B_F32) B2B_SMALL(float, KIND_HH);
+  else B2B_SMALL(double, KIND_HH);
+#undef B2B_SMALL
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+}  // namespace b2b

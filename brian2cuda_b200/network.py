@@ -140,10 +140,13 @@ class Network:
 
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
-                 stream: int | None = None, fused: bool = False):
+                 stream: int | None = None, fused: bool = False, small: bool = False):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
         default the network creates its own non-blocking stream.  `fused`: run one kernel per
-        step (neuron update and delivery side by side) where the net allows it."""
+        step (neuron update and delivery side by side) where the net allows it.  `small`: run
+        a small network (one LIF/HH population of <= 4096 neurons, additive synapses onto
+        itself) in one CTA per chunk of steps with the state in shared memory; it pays off for
+        nets of a few hundred to ~2000 neurons with few delays."""
         self._lib = N.lib()
         self.dt = float(dt)
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
@@ -151,6 +154,8 @@ class Network:
             flags |= N.NET_RESET_BEFORE_SYNAPSES
         if fused:
             flags |= N.NET_FUSED
+        if small:
+            flags |= N.NET_SMALL
         cfg = N.Config(self.dt, device, steps_per_graph, seed, stream, flags, 0)
         h = C.c_void_p()
         st = self._lib.b2b_create(C.byref(cfg), C.byref(h))
@@ -332,10 +337,11 @@ class Network:
 
     @property
     def run_mode(self) -> str:
-        """'fused' (persistent multi-step kernel) or 'per-step' (graph-replayed kernels)."""
+        """'fused' (one kernel per step), 'small' (one CTA runs every step of a chunk) or
+        'per-step' (graph-replayed kernels)."""
         m = C.c_int32()
         self._check(self._lib.b2b_run_mode(self._h, C.byref(m)), "run_mode")
-        return "fused" if m.value == 1 else "per-step"
+        return {1: "fused", 2: "small"}.get(m.value, "per-step")
 
     @property
     def kernel_launches(self) -> int:

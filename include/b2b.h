@@ -59,9 +59,15 @@ enum {
   B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
-  B2B_NET_FUSED = 8       /* run one kernel per step (neuron update and delivery side by
+  B2B_NET_FUSED = 8,      /* run one kernel per step (neuron update and delivery side by
                              side) when the net has one population, additive synapses onto
                              ge/gi and all delays >= 1 step; otherwise per-step kernels  */
+  B2B_NET_SMALL = 16      /* run a small network (one LIF/HH population of <= 4096 neurons
+                             with additive synapses onto itself) in one CTA per chunk of
+                             steps, with the state in shared memory; faster than the
+                             per-step kernels only for nets of a few hundred to ~2000
+                             neurons with few delays (measured: 500-neuron CUBA 3.8 vs
+                             4.9 us per step); otherwise per-step kernels                */
 };
 
 typedef struct {
@@ -230,8 +236,9 @@ b2b_status b2b_restore(b2b_net* net, int32_t slot);
 b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
 b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
-/* How b2b_run advances the net (after b2b_finalize): *mode = 1 for the persistent
- * multi-step kernel, 0 for per-step kernels replayed from CUDA graphs. */
+/* How b2b_run advances the net (after b2b_finalize): *mode = 1 for one kernel per step
+ * (B2B_NET_FUSED), 2 for a small network run by one CTA per chunk of steps, 0 for per-step
+ * kernels replayed from CUDA graphs. */
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
@@ -240,7 +247,8 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * Sites, in order: one per population (kind 1), one per projection's on_pre delivery
  * (kind 2), one per STDP projection's on_post delivery (kind 3), one per population with a
  * deferred reset (kind 4); or, when the net runs one kernel per step (b2b_run_mode 1), that
- * kernel alone (kind 5).  *n_sites receives the number of sites (<= cap filled). */
+ * kernel alone (kind 5); or, for a small network run by one CTA (b2b_run_mode 2), that kernel
+ * advancing one step (kind 7).  *n_sites receives the number of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
 

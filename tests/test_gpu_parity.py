@@ -358,6 +358,11 @@ def test_autotune_keeps_state_and_results(gpu_factory):
     np.testing.assert_array_equal(out[True][0], out[False][0])
     np.testing.assert_array_equal(out[True][1], out[False][1])
     np.testing.assert_array_equal(out[True][2], out[False][2])
+    # a small network run by one CTA has a fixed shape: nothing to tune
+    net = gpu_factory(DT, small=True)
+    models.build_cuba(net, n=1000, p=0.05, dtype="float64")
+    net.finalize()
+    assert net.run_mode == "small" and net.autotune(trial_steps=5) == []
 
 
 def test_out_degree_matches_synapses(gpu_factory):
@@ -368,3 +373,37 @@ def test_out_degree_matches_synapses(gpu_factory):
     for sid in (ids["Ce"], ids["Ci"]):
         want += np.bincount(net.syn_get(sid, "i"), minlength=3000)
     np.testing.assert_array_equal(net.out_degree(ids["P"]), want)
+
+
+@pytest.mark.parametrize("case", ["cobahh_delays", "lif_onto_v_late_reset"])
+def test_small_network_path_matches_per_step(gpu_factory, case):
+    """The opt-in small-network path runs every step of a chunk in one CTA with the state in
+    shared memory; the result must be the per-step kernels' result exactly (every delivered weight of one
+    target variable is equal, so the order of the additions cannot change a sum)."""
+    out = {}
+    for small in (True, False):
+        net = gpu_factory(DT, small=small)
+        if case == "cobahh_delays":
+            ids = models.build_cobahh(net, n=3000, p=0.05, monitor_capacity=10**6)
+            G, steps = ids["P"], 300
+        else:
+            rng = np.random.default_rng(5)
+            n = 700
+            G = net.lif_group(n, models.cuba_lif(), "float64")
+            net.set_state(G, "v", rng.uniform(-60 * mV, -50 * mV, n))
+            i, j = models.bernoulli_pairs(rng, n, n, 0.05)
+            d = rng.integers(0, 4, size=len(i)).astype(np.int32)
+            net.synapses(G, G, "v", i, j, w_scalar=0.6 * mV, delay=d)
+            net.spike_monitor(G, 10**6)
+            steps = 200
+        net.finalize()
+        assert net.run_mode == ("small" if small else "per-step")
+        net.run(steps)
+        assert net.sync() == 0
+        idx, st = net.spikes(G)
+        out[small] = (idx, st, {v: net.get_state(G, v) for v in ("v", "ge", "gi", "lastspike")})
+    assert len(out[True][0]) > 50
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    np.testing.assert_array_equal(out[True][1], out[False][1])
+    for v in ("v", "ge", "gi", "lastspike"):
+        np.testing.assert_array_equal(out[True][2][v], out[False][2][v], err_msg=v)
