@@ -126,6 +126,9 @@ HhDev hh_dev(const Group& g, double dt) {
   d.ref_steps = p.refractory > 0 ? timestep_host(p.refractory, dt) : -1;
   d.offset = g.offset;
   d.n = g.n;
+  d.f = HhFloat{(float)d.Cm, (float)d.gl, (float)d.El, (float)d.EK, (float)d.ENa, (float)d.gNa,
+                (float)d.gK, (float)d.VT, (float)d.Ee, (float)d.Ei, (float)d.De, (float)d.Di,
+                (float)d.Vthr, (float)d.inv_Cm};
   return d;
 }
 

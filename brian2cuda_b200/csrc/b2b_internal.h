@@ -29,11 +29,17 @@ struct LifDev {
   int64_t offset, n;                      // group range inside the population
   int32_t has_threshold, has_reset, unless_refractory, pad;
 };
+// float32 copies of the HH constants (rounded on the host as the device would round them),
+// so a float32 update loads 4-byte values and converts nothing.
+struct HhFloat {
+  float Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr, inv_Cm;
+};
 struct HhDev {
   double Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr;
   int64_t ref_steps;
   int64_t offset, n;
   double inv_Cm;                          // 1/Cm (the float32 update multiplies by it)
+  HhFloat f;
 };
 struct PoissonDev {
   double p_spike;                         // rate * dt

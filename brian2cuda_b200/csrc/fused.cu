@@ -91,7 +91,7 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
   uint8_t* NR = static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
   bool spk = false;
   if constexpr (KIND == KIND_HH) {
-    const HhDev g = static_cast<const HhDev*>(P.params)[gidx];  // by value: no reloads
+    const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());  // no reloads
     const bool refr = g.ref_steps >= 0;
     bool nr = true;
     if (refr) nr = timestep_of(t - (double)LS[q], dt, inv_dt) >= g.ref_steps;

@@ -89,7 +89,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   unsigned fl = 0;
   if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
-    const HhDev g = prm[group_of<E>(P, q)];
+    const HhRun<R> g = hh_run(prm[group_of<E>(P, q)], R());
     const R Vthr = (R)g.Vthr, dtR = (R)dt;
     const bool refr = g.ref_steps >= 0;
     Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
@@ -174,7 +174,7 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     if (q + stride < nthr) hh_pack_load<R>(P, prm, q + stride, nxt);
     unsigned fl = 0;
     if (q < nthr) {
-      const HhDev g = prm[cur.grp];
+      const HhRun<R> g = hh_run(prm[cur.grp], R());
       const bool refr = g.ref_steps >= 0;
       uint32_t NRout = 0;
 #pragma unroll

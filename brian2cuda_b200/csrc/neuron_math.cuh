@@ -77,14 +77,32 @@ __device__ __forceinline__ void hh_gating(R VT, R v, R& m, R& h, R& n, R dt) {
   n = expeuler(n, -(an + bn), an, dt);
 }
 
+// A group's HH constants in the arithmetic type R of the update (float32: the host-rounded
+// copies, float64: the originals) with its refractory period and range.
+template <typename R>
+struct HhRun {
+  R Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr, inv_Cm;
+  int64_t ref_steps, offset, n;
+};
+__device__ __forceinline__ HhRun<float> hh_run(const HhDev& g, float) {
+  const HhFloat& f = g.f;
+  return {f.Cm, f.gl, f.El, f.EK, f.ENa, f.gNa, f.gK, f.VT, f.Ee, f.Ei, f.De, f.Di, f.Vthr,
+          f.inv_Cm, g.ref_steps, g.offset, g.n};
+}
+__device__ __forceinline__ HhRun<double> hh_run(const HhDev& g, double) {
+  return {g.Cm, g.gl, g.El, g.EK, g.ENa, g.gNa, g.gK, g.VT, g.Ee, g.Ei, g.De, g.Di, g.Vthr,
+          g.inv_Cm, g.ref_steps, g.offset, g.n};
+}
+
 // 1/Cm (float32, from the group's precomputed reciprocal) or division by Cm (float64).
-__device__ __forceinline__ float per_cm(float x, const HhDev& g) { return x * (float)g.inv_Cm; }
-__device__ __forceinline__ double per_cm(double x, const HhDev& g) { return x / g.Cm; }
+__device__ __forceinline__ float per_cm(float x, const HhRun<float>& g) { return x * g.inv_Cm; }
+__device__ __forceinline__ double per_cm(double x, const HhRun<double>& g) { return x / g.Cm; }
 
 // Membrane part of the COBAHH update: exponential Euler for v with the conductances of the
 // gating state at the start of the step.  Returns the new v.
 template <typename R>
-__device__ __forceinline__ R hh_membrane(const HhDev& g, R v, R m, R h, R n, R ge, R gi, R dt) {
+__device__ __forceinline__ R hh_membrane(const HhRun<R>& g, R v, R m, R h, R n, R ge, R gi,
+                                         R dt) {
   const R gl = (R)g.gl;
   const R gna = (R)g.gNa * (m * m * m) * h;
   const R gk = (R)g.gK * (n * n * n * n);
@@ -96,7 +114,7 @@ __device__ __forceinline__ R hh_membrane(const HhDev& g, R v, R m, R h, R n, R g
 // COBAHH over one dt: every right-hand side uses the values at the start of the step.
 // Returns the new v; advances m, h, n, ge, gi in place.
 template <typename R>
-__device__ __forceinline__ R hh_advance(const HhDev& g, R v, R& m, R& h, R& n, R& ge, R& gi,
+__device__ __forceinline__ R hh_advance(const HhRun<R>& g, R v, R& m, R& h, R& n, R& ge, R& gi,
                                         R dt) {
   const R vn = hh_membrane<R>(g, v, m, h, n, ge, gi, dt);
   hh_gating<R>((R)g.VT, v, m, h, n, dt);

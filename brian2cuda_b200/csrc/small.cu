@@ -179,7 +179,7 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
             snr[i] = nr ? 1 : 0;
           }
         } else {
-          const HhDev& g = static_cast<const HhDev*>(P.params)[gidx];
+          const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
           const bool refr = g.ref_steps >= 0;
           if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
           R m = sM[i], h = sH[i], nn = sN[i];

@@ -361,7 +361,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
       nls = LSv[qn];
     }
     if (!mlp_tile_forward(S, phase, xh, y, status)) break;
-    const HhDev& g = prm[group_of<1>(P, q)];
+    const HhRun<float> g = hh_run(prm[group_of<1>(P, q)], 0.f);
     const bool refr = g.ref_steps >= 0;
     float mn = dclip(m + I->out_scale[0] * y[0], 0.f, 1.f);
     float hn = dclip(h + I->out_scale[1] * y[1], 0.f, 1.f);
