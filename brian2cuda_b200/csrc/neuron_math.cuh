@@ -26,14 +26,26 @@ __device__ __forceinline__ R lif_advance(const LifDev& g, R v, R& ge, R& gi, boo
 }
 
 // Arithmetic of the COBAHH update.  float64 keeps the correctly rounded library forms.
-// float32 uses the hardware units: exp through ex2 (__expf, relative error ~1e-6 for the
-// |x| <= 25 the rates reach), division through the reciprocal unit (__fdividef, 2 ulp), and
-// division by a literal constant as multiplication by its rounded reciprocal; all of it is
-// far inside the 1e-5 relative tolerance against the float64 oracle, at a quarter of the
-// instructions of the precise forms.
-__device__ __forceinline__ float hexp(float x) { return __expf(x); }
+// float32 uses the hardware units in their flush-to-zero forms (a result below 1.2e-38
+// becomes 0; no operand or result of the update comes near that range otherwise): exp(x) as
+// 2^(x log2 e) on the ex2 unit (relative error ~1e-6 for the |x| <= 25 the rates reach, from
+// the rounding of x log2 e), division as a product with the reciprocal unit's 1/b, and
+// division by a literal constant as a product with its rounded reciprocal; all of it is far
+// inside the 1e-5 relative tolerance against the float64 oracle.  The flush-to-zero forms
+// need no subnormal handling around each ex2 and reciprocal.
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float hexp(float x) { return ex2_ftz(x * 1.4426950408889634f); }
 __device__ __forceinline__ double hexp(double x) { return exp(x); }
-__device__ __forceinline__ float hdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float hdiv(float a, float b) { return a * rcp_ftz(b); }
 __device__ __forceinline__ double hdiv(double a, double b) { return a / b; }
 // x / c for a literal c.
 __device__ __forceinline__ float hdivc(float x, double c) { return x * (float)(1.0 / c); }
@@ -49,7 +61,7 @@ __device__ __forceinline__ float hz_over_expm1(float z) {
                                                -1.f / 720.f), 1.f / 12.f), 1.f);
     return fmaf(z, -0.5f, even);
   }
-  return __fdividef(z, __expf(z) - 1.f);
+  return z * rcp_ftz(hexp(z) - 1.f);
 }
 __device__ __forceinline__ double hz_over_expm1(double z) { return z_over_expm1(z); }
 
