@@ -271,17 +271,16 @@ def main():
     net.store(0)
     init = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi", "lastspike")}
     setup_s = time.perf_counter() - t_setup
-    # launch shapes tuned on the network's own state, 150 steps into the run (after the first
-    # population burst); the autotuner leaves the state where it found it
+    # launch shapes tuned on the network's own run: every trial covers the first 300 steps
+    # from the initial state (the first population burst and the quiet phase after it); the
+    # autotuner leaves the state where it found it
     tune = None
     if args.tune_from:
         with open(args.tune_from) as f:
             tune = json.loads([ln for ln in f if ln.startswith("{")][-1])["autotune"]
         net.tune_apply(tune)
     elif not args.fused:
-        net.run(150)
-        tune = net.autotune(trial_steps=50)
-        net.restore(0)
+        tune = net.autotune(trial_steps=300)
 
     if args.ncu_case:
         net.run(args.ncu_case)

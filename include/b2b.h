@@ -259,7 +259,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
  * threads per CTA (128 or 256), or, with a gating surrogate, CTAs per SM (2..6); additive
  * delivery launches: lanes per work item (8, 16, 32) x CTAs (1/2, 1, 2, 4 per SM).  Afterwards
  * the state, clock and monitor counts are as before the call, and the next b2b_run captures
- * its graph with the chosen shapes.  A choice of 0 means the built-in rule won. */
+ * its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far
+ * (starting from the built-in rule) to be chosen.  A choice of 0 means the built-in rule won.
+ * The trials should cover a representative stretch of the run (bursts included). */
 typedef struct {
   int32_t site_kind;     /* 1 population, 6 additive delivery launch                    */
   int32_t site_index;    /* population index / delivery launch index                    */
