@@ -67,7 +67,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     store_pack<R, E>(P.var[B2B_VAR_GE], q, GE);
     store_pack<R, E>(P.var[B2B_VAR_GI], q, GI);
     if (refr) {
-      store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);
+      if (fl) store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);   // changes only on a spike
       store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
   }
@@ -122,7 +122,7 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     store_pack<R, E>(P.var[B2B_VAR_GE], q, GE);
     store_pack<R, E>(P.var[B2B_VAR_GI], q, GI);
     if (refr) {
-      store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);
+      if (fl) store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);   // changes only on a spike
       store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
   }
@@ -199,7 +199,7 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       store_pack<R, 4>(P.var[B2B_VAR_GE], q, cur.GE);
       store_pack<R, 4>(P.var[B2B_VAR_GI], q, cur.GI);
       if (refr) {
-        store_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q, cur.LS);
+        if (fl) store_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q, cur.LS);   // changes on a spike
         store_flags<4>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
       }
     }

@@ -63,6 +63,8 @@ __device__ __forceinline__ void emit_spikes(const PopDev& P, int64_t q, unsigned
   __shared__ int s_warp[33];
   __shared__ int s_base;
   __shared__ unsigned long long s_mbase;
+  // most CTAs of most steps have no spike: one barrier decides that for the whole CTA
+  if (!__syncthreads_or(fl != 0)) return;
   int total;
   const int c = __popc(fl);
   const int excl = block_exclusive_scan(c, s_warp, &total);
