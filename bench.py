@@ -36,7 +36,7 @@ P_CONNECT = 0.02
 DMIN, DMAX = 1, 50
 SIM_STEPS = 10_000           # simulation steps per bench step (1 s)
 BYTES_NEURON_UPDATE = 54     # COBAHH f32: 6 vars x 4 B x (R+W) + flag + lastspike
-BYTES_EVENT = 16             # post index 4 + weight 4 + target R/W 8
+BYTES_EVENT = 12             # post index 4 + target R/W 8 (we, wi: one value per Synapses)
 BYTES_BUNDLE = 8             # per (spike, delay) bundle visited
 METRIC = "synaptic events/s"
 UNIT = "events/s"
@@ -363,18 +363,15 @@ def main():
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     # algorithmic bytes per launch of each launch site the profiler reports
     site_info = {1: ("neuron (HH update+threshold+compaction)", "hh_step_kernel"),
-                 2: ("delivery on_pre", "deliver_add_batch_kernel"),
+                 6: ("delivery on_pre (Ce and Ci, one launch)", "deliver_add_batch_kernel"),
                  5: ("fused step (HH update + delivery, one kernel)", "fused_step_kernel")}
     kernel_ms, per_launch_bytes, kernels = {}, [], []
-    n_deliver = 0
     for k, (kd, ms) in enumerate(prof):
         label, kname = site_info.get(kd, (f"site kind {kd}", None))
         if kd == 1:
             b = neuron_bytes
-        elif kd == 2:
-            b = deliver_exc if n_deliver == 0 else deliver_inh
-            label += " Ce (exc)" if n_deliver == 0 else " Ci (inh)"
-            n_deliver += 1
+        elif kd == 6:
+            b = deliver_exc + deliver_inh
         elif kd == 5:
             b = neuron_bytes + deliver_exc + deliver_inh
         else:
@@ -608,7 +605,7 @@ def bench_batched(args, world, rank, local):
                      "kernel": "neuron (HH update+threshold+compaction, hh_stream_kernel)",
                      "kernel_ms": neuron_ms, "peak_source": peak_kind,
                      "bytes_per_launch": neuron_bytes},
-        "kernel_ms_mean_per_launch": {("neuron" if k == 1 else "delivery" if k == 2 else
+        "kernel_ms_mean_per_launch": {("neuron" if k == 1 else "delivery" if k == 6 else
                                        f"site {k}"): ms for k, ms in prof},
         "gpu_launches": launches,
         "clocks": clk,

@@ -1163,7 +1163,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
     sites.push_back({5, 0});
   } else {
     for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
-    for (size_t p = 0; p < net->projs.size(); ++p) sites.push_back({2, (int)p});
+    for (size_t b = 0; b < net->add_batches.size(); ++b) sites.push_back({6, (int)b});
+    for (size_t p = 0; p < net->projs.size(); ++p)
+      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({2, (int)p});
     for (size_t p = 0; p < net->projs.size(); ++p)
       if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
     for (size_t p = 0; p < net->pops.size(); ++p)
@@ -1182,6 +1184,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       cudaError_t e = cudaSuccess;
       const int64_t* clk = net->d_clock;
       if (s.kind == 1) e = launch_pop_step(net->pops[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 6)
+        e = launch_proj_add_batch(net->add_batches[s.idx].data(), (int)net->add_batches[s.idx].size(),
+                                  clk, 0, net->stream, &net->add_tune[s.idx]);
       if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
@@ -1229,61 +1234,33 @@ namespace {
 
 constexpr double kTuneMargin = 0.98;
 
-struct TuneSite {
-  int kind;   // 1 population, 6 additive delivery launch
-  int idx;
-};
-
-// Advances the net by n_steps with eager launches, timing the launch of `site` with a CUDA
-// event pair on the net's stream; *mean_ms receives its mean device time.
-b2b_status time_site(b2b_net* net, int64_t n_steps, const TuneSite& site, double* mean_ms) {
+// Advances the net by n_steps the way b2b_run does (CUDA-graph replays of the current launch
+// shapes, captured afresh before the timing starts), timed with a CUDA event pair on the
+// net's stream; *mean_ms receives the mean device time of one whole step.  A shape is judged
+// by the step it produces, so its effect on the neighbouring launches (a larger grid delays
+// the next kernel's start) counts too.
+b2b_status time_steps(b2b_net* net, int64_t n_steps, double* mean_ms) {
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  if (!(net->cfg.flags & B2B_NET_NO_GRAPH))
+    if (b2b_status st = capture_graph(net)) return st;
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  double acc = 0.0;
-  b2b_status result = B2B_OK;
-  const int64_t* clk = net->d_clock;
-  for (int64_t step = 0; step < n_steps && result == B2B_OK; ++step) {
-    if ((result = refill_rng(net, 1)) != B2B_OK) break;
-    cudaError_t e = cudaSuccess;
-    for (size_t p = 0; p < net->pops.size() && e == cudaSuccess; ++p) {
-      const bool timed = site.kind == 1 && site.idx == (int)p;
-      if (timed) cudaEventRecord(e0, net->stream);
-      e = launch_pop_step(net->pops[p], clk, 0, net->cfg.dt, net->d_status, net->stream);
-      if (timed) cudaEventRecord(e1, net->stream);
-    }
-    for (size_t b = 0; b < net->add_batches.size() && e == cudaSuccess; ++b) {
-      const bool timed = site.kind == 6 && site.idx == (int)b;
-      if (timed) cudaEventRecord(e0, net->stream);
-      e = launch_proj_add_batch(net->add_batches[b].data(), (int)net->add_batches[b].size(), clk,
-                                0, net->stream, &net->add_tune[b]);
-      if (timed) cudaEventRecord(e1, net->stream);
-    }
-    for (const Proj& pr : net->projs) {
-      if (e != cudaSuccess || pr.effect == B2B_EFFECT_ADD) continue;
-      e = launch_proj_pre(pr, clk, 0, net->cfg.dt, net->d_status, net->stream);
-      if (e == cudaSuccess && pr.effect == B2B_EFFECT_STDP)
-        e = launch_proj_post(pr, clk, 0, net->cfg.dt, net->d_status, net->stream);
-    }
-    for (const Pop& pop : net->pops)
-      if (e == cudaSuccess && pop.late_reset)
-        e = launch_pop_late_reset(pop, clk, 0, net->stream);
-    if (e == cudaSuccess) e = launch_tick(net->d_clock, 1, net->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
-    if (e != cudaSuccess) {
-      result = fail(net, B2B_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
-      break;
-    }
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    acc += ms;
-    net->ts += 1;
-    net->last_chunk_steps = 1;
-  }
+  cudaEventRecord(e0, net->stream);
+  b2b_status st = b2b_run(net, n_steps);
+  cudaEventRecord(e1, net->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (st == B2B_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (result == B2B_OK) *mean_ms = acc / (double)n_steps;
-  return result;
+  if (st != B2B_OK) return st;
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+  *mean_ms = ms / (double)n_steps;
+  return B2B_OK;
 }
 
 }  // namespace
@@ -1311,15 +1288,24 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   net->add_tune.resize(net->add_batches.size());
   std::vector<b2b_tune_result> res;
   b2b_status st = B2B_OK;
-  auto trial = [&](const TuneSite& site, double* ms) {
+  auto put_back_monitors = [&]() -> b2b_status {
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      if (net->pops[p].dev.mon_cnt)
+        CU(cudaMemcpy(net->pops[p].dev.mon_cnt, &mon[p], sizeof(unsigned long long),
+                      cudaMemcpyHostToDevice));
+    return B2B_OK;
+  };
+  // every trial starts from the same state, with the monitors' counts of that state
+  auto trial = [&](double* ms) {
     if (b2b_status s2 = b2b_restore(net, slot)) return s2;
-    return time_site(net, trial_steps, site, ms);
+    if (b2b_status s2 = put_back_monitors()) return s2;
+    return time_steps(net, trial_steps, ms);
   };
   // one discarded trial first, so that no candidate pays for a cold start (first launches,
   // caches, clocks ramping up)
   {
     double ms = 0;
-    st = trial({net->pops.empty() ? 6 : 1, 0}, &ms);
+    st = trial(&ms);
   }
   for (size_t p = 0; p < net->pops.size() && st == B2B_OK; ++p) {
     Pop& pop = net->pops[p];
@@ -1340,7 +1326,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         pop.tune_block = cands[c].second;
       }
       double ms = 0;
-      st = trial({1, (int)p}, &ms);
+      st = trial(&ms);
       if (c == 0) r.default_ms = ms;
       // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
       // near-equal shapes differ by noise, and noise should not pick the shape
@@ -1364,15 +1350,15 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK; ++b) {
     AddTune& t = net->add_tune[b];
     std::vector<std::pair<int, int>> cands = {{0, 0}};
-    for (int g : {8, 16, 32})
-      for (int mult : {1, 2, 4, 8}) cands.push_back({g, mult * sms / 2});
+    for (int g : {4, 8, 16, 32})
+      for (int mult : {1, 2, 4, 8, 16}) cands.push_back({g, mult * sms / 2});
     b2b_tune_result r{6, (int32_t)b, 0, 0, 0.0, 0.0};
     double best = 1e30;
     for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
       t.group = cands[c].first;
       t.grid = cands[c].second;
       double ms = 0;
-      st = trial({6, (int)b}, &ms);
+      st = trial(&ms);
       if (c == 0) r.default_ms = ms;
       // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
       // near-equal shapes differ by noise, and noise should not pick the shape
@@ -1389,10 +1375,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
-  for (size_t p = 0; p < net->pops.size(); ++p)
-    if (net->pops[p].dev.mon_cnt)
-      CU(cudaMemcpy(net->pops[p].dev.mon_cnt, &mon[p], sizeof(unsigned long long),
-                    cudaMemcpyHostToDevice));
+  if (st2 == B2B_OK) st2 = put_back_monitors();
   for (void* a : net->snapshots[slot].buffers) cudaFree(a);
   net->snapshots.resize(slot);
   if (net->graph) {
@@ -1432,7 +1415,8 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
     } else if (t.site_kind == 6) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->add_batches.size(),
             B2B_ERR_INVALID_ARG, "bad delivery launch index %d", t.site_index);
-      CHECK((t.choice_a == 0 || t.choice_a == 8 || t.choice_a == 16 || t.choice_a == 32) &&
+      CHECK((t.choice_a == 0 || t.choice_a == 4 || t.choice_a == 8 || t.choice_a == 16 ||
+             t.choice_a == 32) &&
                 t.choice_b >= 0 && t.choice_b <= 65535,
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       net->add_tune[t.site_index].group = t.choice_a;

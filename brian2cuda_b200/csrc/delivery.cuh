@@ -98,19 +98,21 @@ __device__ __forceinline__ int find_delay_block(const int* s_pref, int nd, int s
   return lo;
 }
 
-// Calls body(s, valid, pre) for every synapse position s of every bundle of projection J
-// due at step ts (pre: its presynaptic neuron).  Work items go to warps warp0, warp0 + nwarps, ...; inside a warp, groups of
-// GROUP lanes take one item each, so 32/GROUP items' dependent loads (spike index, bundle
-// offsets, synapse data) are in flight together.  All 32 lanes of a warp call body together
-// (valid marks real synapses).  WARP_PREFIX requires J.nd <= 64; otherwise every thread of
-// the CTA must call this (block prefix in s_pref, J.nd + 1 ints).
-template <bool WARP_PREFIX, int GROUP = 32, class Body>
-__device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64_t warp0,
-                                             int64_t nwarps, int* s_pref, Body body) {
+// Calls item(b0, b1, len, pre) for every work item of projection J due at step ts: the
+// synapse positions [b0, b1) of one chunk of the bundle of presynaptic neuron pre (b1 == b0
+// for a lane group without an item).  Work items go to warps warp0, warp0 + nwarps, ...;
+// inside a warp, groups of GROUP lanes take one item each, so 32/GROUP items' dependent loads
+// (spike index, bundle offsets, synapse data) are in flight together.  All 32 lanes of a warp
+// call item together; len, the longest b1 - b0 of the warp's groups, is the same in every
+// lane.  WARP_PREFIX requires J.nd <= 64; otherwise every thread of the CTA must call this
+// (block prefix in s_pref, J.nd + 1 ints).
+template <bool WARP_PREFIX, int GROUP = 32, class Item>
+__device__ __forceinline__ void for_each_due_item(const ProjDev& J, int64_t ts, int64_t warp0,
+                                                  int64_t nwarps, int* s_pref, Item item) {
   static_assert(GROUP == 32 || GROUP == 16 || GROUP == 8 || GROUP == 4, "group size");
   constexpr int G = 32 / GROUP;  // items per warp per round
   const int lane = threadIdx.x & 31;
-  const int grp = lane / GROUP, glane = lane % GROUP;
+  const int grp = lane / GROUP;
   DuePrefix wp{};
   int nspk;
   if constexpr (WARP_PREFIX) {
@@ -151,11 +153,24 @@ __device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64
     int64_t len = b1 - b0;
 #pragma unroll
     for (int o = 16; o >= GROUP; o >>= 1) len = max(len, __shfl_xor_sync(kFull, len, o));
+    item(b0, b1, len, pre);
+  }
+}
+
+// Calls body(s, valid, pre) for every synapse position s of every bundle of projection J
+// due at step ts, GROUP lanes to a work item (for_each_due_item); all 32 lanes of a warp call
+// body together, valid marking real synapses.
+template <bool WARP_PREFIX, int GROUP = 32, class Body>
+__device__ __forceinline__ void for_each_due(const ProjDev& J, int64_t ts, int64_t warp0,
+                                             int64_t nwarps, int* s_pref, Body body) {
+  const int glane = (threadIdx.x & 31) % GROUP;
+  for_each_due_item<WARP_PREFIX, GROUP>(J, ts, warp0, nwarps, s_pref,
+                                        [&](int64_t b0, int64_t b1, int64_t len, int32_t pre) {
     for (int64_t off = 0; off < len; off += GROUP) {
       const int64_t s = b0 + off + glane;
       body(s, s < b1, pre);
     }
-  }
+  });
 }
 
 // Member of presynaptic neuron pre in a projection of several Synapses objects (binary

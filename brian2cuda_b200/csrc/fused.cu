@@ -30,13 +30,6 @@ namespace {
 
 constexpr int kFusedBlock = 256;
 
-__device__ __forceinline__ void wait_for_predecessor() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-__device__ __forceinline__ void allow_successor_launch() {
-  asm volatile("griddepcontrol.launch_dependents;");
-}
-
 // Appends this warp's spikes (flag per lane, neuron q) to ring slot `slot` and the monitor.
 __device__ __forceinline__ void warp_emit(const PopDev& P, bool spk, int32_t q, int64_t ts,
                                           int slot, int32_t* status) {
@@ -135,8 +128,8 @@ __global__ void __launch_bounds__(kFusedBlock)
 fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict__ clock, int k,
                   double dt, int32_t* status) {
   extern __shared__ int s_pref[];  // F.nd_max + 1 ints when !WARP_PREFIX
-  wait_for_predecessor();
-  allow_successor_launch();
+  chain_wait();
+  chain_trigger();
   const PopDev& P = F.pop;
   const int64_t ts = clock[0] + k;
   if ((int)blockIdx.x >= F.deliver_ctas) {
@@ -175,8 +168,8 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
 template <typename R>
 __global__ void fused_fold_kernel(const __grid_constant__ FusedDev F,
                                   const int64_t* __restrict__ clock, int k_last) {
-  wait_for_predecessor();
-  allow_successor_launch();
+  chain_wait();
+  chain_trigger();
   const int last = (int)((clock[0] + k_last) & 1);
   const int64_t n = F.pop.n;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -189,21 +182,6 @@ __global__ void fused_fold_kernel(const __grid_constant__ FusedDev F,
       A[q] = (R)0;
     }
   }
-}
-
-template <typename KernelT, typename... Args>
-cudaError_t launch_pdl(KernelT kernel, dim3 grid, size_t smem, cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = dim3(kFusedBlock);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 }  // namespace
@@ -237,8 +215,9 @@ cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
   const size_t smem = fused_smem(F);
   const dim3 g(grid);
   const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
-#define B2B_FS(R, KD, WP) \
-  launch_pdl(fused_step_kernel<R, KD, WP>, g, smem, s, F, clock, k, dt, status)
+#define B2B_FS(R, KD, WP)                                                                   \
+  launch_chained(fused_step_kernel<R, KD, WP>, g, dim3(kFusedBlock), smem, s, F, clock, k, dt, \
+                 status)
   if (kind == KIND_HH) {
     if (dtype == B2B_F32) return wp ? B2B_FS(float, KIND_HH, true) : B2B_FS(float, KIND_HH, false);
     return wp ? B2B_FS(double, KIND_HH, true) : B2B_FS(double, KIND_HH, false);
@@ -254,8 +233,9 @@ cudaError_t launch_fused_fold(const FusedDev& F, int dtype, const int64_t* clock
   int64_t blocks = (n + kFusedBlock - 1) / kFusedBlock;
   if (blocks > 4 * kNumSMs) blocks = 4 * kNumSMs;
   const dim3 g((unsigned)blocks);
-  if (dtype == B2B_F32) return launch_pdl(fused_fold_kernel<float>, g, 0, s, F, clock, k_last);
-  return launch_pdl(fused_fold_kernel<double>, g, 0, s, F, clock, k_last);
+  const dim3 b(kFusedBlock);
+  if (dtype == B2B_F32) return launch_chained(fused_fold_kernel<float>, g, b, 0, s, F, clock, k_last);
+  return launch_chained(fused_fold_kernel<double>, g, b, 0, s, F, clock, k_last);
 }
 
 }  // namespace b2b

@@ -24,6 +24,7 @@ namespace b2b {
 namespace {
 
 constexpr int kDeliverBlock = 256;
+constexpr int kAddUnroll = 4;
 
 // Sum of `v` over the lanes whose key equals this lane's key; valid in every lane.
 template <typename R>
@@ -37,11 +38,14 @@ __device__ __forceinline__ R peer_sum(unsigned peers, R v) {
   return acc;
 }
 
-// target[post] += w for one synapse per lane; AGG sums lanes hitting the same target first.
+// T[post] += w for one synapse per lane; AGG sums lanes hitting the same element first.  The
+// lanes of a warp may write different target arrays (the members of a projection that merges
+// several Synapses objects), so lanes are matched on the element's address.
 template <typename R, bool AGG>
 __device__ __forceinline__ void add_to_target(R* T, int32_t post, R w, bool valid) {
   if constexpr (AGG) {
-    const unsigned peers = __match_any_sync(kFull, valid ? post : -1);
+    const unsigned peers =
+        __match_any_sync(kFull, valid ? (unsigned long long)(T + post) : 0ull);
     const R sum = peer_sum<R>(peers, valid ? w : (R)0);
     if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(T + post, sum);
   } else {
@@ -66,14 +70,30 @@ deliver_add_batch_kernel(const __grid_constant__ ProjBatch B, const int64_t* __r
   const R* __restrict__ W = static_cast<const R*>(P.w);
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int glane = (threadIdx.x & 31) % GROUP;
   MemberCache<R> mc;
-  for_each_due<WARP_PREFIX, GROUP>(P, ts, warp0, nwarps, s_pref,
-                               [&](int64_t s, bool valid, int32_t pre) {
-    const int32_t post = valid ? __ldg(P.post + s) : 0;
+  for_each_due_item<WARP_PREFIX, GROUP>(P, ts, warp0, nwarps, s_pref,
+                                        [&](int64_t b0, int64_t b1, int64_t len, int32_t pre) {
     member_lookup<R>(P, pre, mc);
-    R w = mc.w;
-    if constexpr (HAS_W) w = valid ? __ldg(W + s) : (R)0;
-    add_to_target<R, AGG>(mc.target, post, w, valid);
+    // kAddUnroll rounds of the bundle per pass: their loads are all issued before the first
+    // atomic, so each lane keeps several independent loads in flight
+    for (int64_t off = 0; off < len; off += kAddUnroll * GROUP) {
+      int32_t post[kAddUnroll];
+      R w[kAddUnroll];
+      bool v[kAddUnroll];
+#pragma unroll
+      for (int u = 0; u < kAddUnroll; ++u) {
+        const int64_t s = b0 + off + u * GROUP + glane;
+        v[u] = s < b1;
+        post[u] = v[u] ? __ldg(P.post + s) : 0;
+        w[u] = mc.w;
+        if constexpr (HAS_W) w[u] = v[u] ? __ldg(W + s) : (R)0;
+      }
+#pragma unroll
+      for (int u = 0; u < kAddUnroll; ++u)
+        if (off + u * GROUP < len)  // warp-uniform
+          add_to_target<R, AGG>(mc.target, post[u], w[u], v[u]);
+    }
   });
 }
 
@@ -162,7 +182,7 @@ deliver_stdp_post_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, do
 
 unsigned deliver_grid(const Proj& pr) {
   const int64_t want = (pr.dev.src_n * (int64_t)pr.dev.chunks) / 64 + 1;
-  const int64_t cap = 2 * kNumSMs;
+  const int64_t cap = 4 * kNumSMs;
   return (unsigned)(want < cap ? want : cap);
 }
 
@@ -176,12 +196,13 @@ void launch_add_g(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem,
                                                                                          k);
 }
 
-// Lanes per work item: 8 (four items in flight per warp, the default), 16 or 32.
+// Lanes per work item: 8 (four items in flight per warp, the default), 4, 16 or 32.
 template <typename R, bool HAS_W, bool AGG>
 void launch_add(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem, const int64_t* clock,
                 int k, cudaStream_t s, int group) {
   if (group == 32) launch_add_g<R, HAS_W, AGG, 32>(B, g, warp_prefix, smem, clock, k, s);
   else if (group == 16) launch_add_g<R, HAS_W, AGG, 16>(B, g, warp_prefix, smem, clock, k, s);
+  else if (group == 4) launch_add_g<R, HAS_W, AGG, 4>(B, g, warp_prefix, smem, clock, k, s);
   else launch_add_g<R, HAS_W, AGG, 8>(B, g, warp_prefix, smem, clock, k, s);
 }
 

@@ -351,7 +351,8 @@ class Network:
 
     def profile(self, steps: int) -> list[tuple[int, float]]:
         """Advances `steps` steps with every launch timed; returns (site kind, mean ms) per
-        launch site (1 population, 2 on_pre delivery, 3 on_post delivery, 4 late reset)."""
+        launch site (1 population, 6 additive on_pre delivery launch, 2 STDP on_pre delivery,
+        3 on_post delivery, 4 late reset, 5 one-kernel step, 7 one-CTA step)."""
         cap = 256
         ms = (C.c_double * cap)()
         kinds = (C.c_int32 * cap)()

@@ -244,30 +244,34 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
  * network by n_steps with eager launches, timing every launch with a CUDA event pair on the
  * net's stream, and returns per launch site the mean device time of one launch in ms.
- * Sites, in order: one per population (kind 1), one per projection's on_pre delivery
- * (kind 2), one per STDP projection's on_post delivery (kind 3), one per population with a
- * deferred reset (kind 4); or, when the net runs one kernel per step (b2b_run_mode 1), that
+ * Sites, in order: one per population (kind 1), one per launch of additive on_pre delivery
+ * (kind 6: the additive projections that share a kernel variant are delivered by one launch,
+ * with its tuned shape), one per STDP projection's on_pre delivery (kind 2), one per STDP
+ * projection's on_post delivery (kind 3), one per population with a deferred reset (kind 4);
+ * or, when the net runs one kernel per step (b2b_run_mode 1), that
  * kernel alone (kind 5); or, for a small network run by one CTA (b2b_run_mode 2), that kernel
  * advancing one step (kind 7).  *n_sites receives the number of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
 
 /* Autotuner (no counterpart in the reference, which picks launch shapes from fixed rules,
- * brian2cuda/device.py:383-394): for every launch site of the net it times candidate launch
- * shapes on the net's own current state, each over `trial_steps` eager steps started from
- * the same checkpoint, and keeps the fastest.  Populations: neurons per thread (1 or 4) x
- * threads per CTA (128 or 256), or, with a gating surrogate, CTAs per SM (2..6); additive
- * delivery launches: lanes per work item (8, 16, 32) x CTAs (1/2, 1, 2, 4 per SM).  Afterwards
- * the state, clock and monitor counts are as before the call, and the next b2b_run captures
- * its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far
- * (starting from the built-in rule) to be chosen.  A choice of 0 means the built-in rule won.
- * The trials should cover a representative stretch of the run (bursts included). */
+ * brian2cuda/device.py:383-394): launch site by launch site it times candidate launch shapes
+ * on the net's own current state and keeps the fastest.  A trial restores the same
+ * checkpoint, captures the step graph with the candidate shape and times `trial_steps` whole
+ * steps run as b2b_run runs them (graph replays), so a shape is judged by the step time it
+ * gives.  Populations: neurons per thread (1 or 4) x threads per CTA (128 or 256), or, with a
+ * gating surrogate, CTAs per SM (2..6); additive delivery launches: lanes per work item
+ * (4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM).  Afterwards the state, clock and monitor
+ * counts are as before the call, and the next b2b_run captures its graph with the chosen
+ * shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
+ * rule) to be chosen.  A choice of 0 means the built-in rule won.  The trials should cover a
+ * representative stretch of the run (bursts included). */
 typedef struct {
   int32_t site_kind;     /* 1 population, 6 additive delivery launch                    */
   int32_t site_index;    /* population index / delivery launch index                    */
   int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item */
   int32_t choice_b;      /* threads per CTA / CTAs                                       */
-  double best_ms;        /* mean device time of one launch with the chosen shape         */
+  double best_ms;        /* mean device time of one whole step with the chosen shape     */
   double default_ms;     /* the same with the built-in rule                              */
 } b2b_tune_result;
 b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out, int32_t cap,

@@ -133,6 +133,37 @@ def test_heterogeneous_delays_rollout_and_queue(gpu_factory, oracle_factory):
     _close(out["gpu"][4], out["orc"][4], 1e-10, 1e-15)
 
 
+def test_merged_synapses_onto_two_variables_of_few_targets(gpu_factory, oracle_factory):
+    """Two Synapses objects from disjoint halves of one source onto ge and onto gi of a
+    40-neuron target: one projection with two members, delivered with warp-aggregated atomics
+    (fewer than 64 targets), so lanes of one warp add to the same index of different
+    variables."""
+    n_src, n_dst, half = 256, 40, 128
+    sg_idx = np.tile(np.arange(n_src), 10)
+    sg_step = np.repeat(np.arange(0, 20, 2), n_src)
+    i = np.repeat(np.arange(n_src), n_dst).astype(np.int32)
+    j = np.tile(np.arange(n_dst), n_src).astype(np.int32)
+    e = i < half
+    prm = LIF(El=-49 * mV, taum=20e-3, taue=5e-3, taui=10e-3, ke=1.0, ki=1.0,
+              has_threshold=False, has_reset=False)
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        S = net.spikegen_group(n_src, sg_idx, sg_step)
+        G = net.lif_group(n_dst, prm, "float64")
+        net.set_state(G, "v", np.full(n_dst, -49 * mV))
+        net.synapses(S, G, "ge", i[e], j[e], w_scalar=0.5 * mV,
+                     delay=np.ones(int(e.sum()), np.int32))
+        net.synapses(S, G, "gi", i[~e], j[~e], w_scalar=-0.25 * mV,
+                     delay=np.full(int((~e).sum()), 2, np.int32))
+        net.finalize()
+        net.run(25)
+        out[name] = {v: net.get_state(G, v) for v in ("ge", "gi", "v")}
+    assert np.all(out["orc"]["ge"] > 0) and np.all(out["orc"]["gi"] < 0)
+    for v in ("ge", "gi", "v"):
+        _close(out["gpu"][v], out["orc"][v], 1e-10, 1e-15)
+
+
 def test_synapse_readback_in_input_order(gpu_factory):
     net = gpu_factory(DT)
     G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=300)
