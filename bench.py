@@ -216,11 +216,12 @@ def main():
                     help="apply the launch shapes of the JSON line in FILE (an earlier bench "
                          "output) instead of autotuning; used by the profiling case")
     ap.add_argument("--workload", default="cobahh",
-                    choices=["cobahh", "batched", "cuba", "stdp", "hines"],
+                    choices=["cobahh", "batched", "cuba", "stdp", "hines", "propagation"],
                     help="cobahh: the 1e5-neuron COBAHH network (default line); batched: 256 "
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
-                    choices=["hh4m", "surrogate1m", "mlp_train"],
+                    choices=["hh4m", "surrogate1m", "mlp_train", "propagation",
+                             "propagation3000"],
                     help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
     if args.kernel_case:
@@ -622,9 +623,31 @@ WORKLOADS = {
             "(on_pre + on_post), f32, 1 s simulated per step (the configured run is 10 s)",
     "hines": "1024 multicompartment HH neurons, random binary trees of 200-1000 compartments, "
              "f64 cable solve, f32 channels, dt=0.025 ms, 200 ms simulated (8000 steps)",
+    "propagation": "spike propagation at high load: 1e5 Poisson neurons at 300 Hz -> 1e5 "
+                   "COBAHH neurons (first 80 % -> ge += 6 nS, last 20 % -> gi += 67 nS), "
+                   "p=0.02 (2e8 synapses), delays U{1..50} steps, f32; ~6e6 synaptic events "
+                   "per step, 0.1 s simulated per step",
 }
+PROP_RATE = 300.0
 BYTES = {"cuba_neuron": 58, "cuba_event": 20, "stdp_neuron": 16, "poisson": 4,
          "stdp_pre": 40, "stdp_post": 32, "hines_comp": 136}
+
+
+def build_propagation(net, monitor_capacity=0, rate=PROP_RATE):
+    """The propagation workload: Poisson input population S (rate in Hz) driving a COBAHH
+    population P through COBAHH's synapse shapes (no recurrent synapses)."""
+    from brian2cuda_b200 import models
+    n = N_NEURONS
+    S = net.poisson_group(n, rate, "float32")
+    P = net.hh_group(n, models.cobahh_hh(), "float32")
+    models.cobahh_init(net, P, n, models.rng_for(5))
+    ne = int(0.8 * n)
+    seed = models.SEED_BASE + 5
+    net.synapses_random(S, P, "ge", P_CONNECT, DMIN, DMAX, 6e-9, seed, pre_range=(0, ne))
+    net.synapses_random(S, P, "gi", P_CONNECT, DMIN, DMAX, 67e-9, seed + 7, pre_range=(ne, n))
+    if monitor_capacity:
+        net.spike_monitor(S, monitor_capacity)
+    return {"S": S, "P": P}
 
 
 def _line_base(args, world, metric, value, unit, ms_per_step, workload, config, dtype):
@@ -774,6 +797,70 @@ def bench_small(args, world, rank, local):
                                     "unit": "events/s", "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"the first 1000 steps of the run ({el:.1f} s), "
                                               "C++ oracle"}
+    elif wl == "propagation":
+        steps_run = 1000
+        runs = args.warmup + args.steps
+        cap = int(N_NEURONS * PROP_RATE * DT * steps_run * 1.1 * (runs + 2)) + 100_000
+        net = Network(DT, seed=models.SEED_BASE + 5, device=local, stream=stream.cuda_stream)
+        ids = build_propagation(net, monitor_capacity=cap)
+        net.finalize()
+        S = ids["S"]
+        outdeg = net.out_degree(S).astype(np.int64)
+        net.run(2 * DMAX)   # every delay slot of the ring holds spikes from here on
+        net.store(0)
+        tune = net.autotune(trial_steps=100)
+        start = net.spikes_recorded(S)
+        ms, launches, clk = _timed_net_runs(net, stream, args, world, local, steps_run)
+        idx, st, _ = net.spikes_fetch(S, start, cap=net.spikes_recorded(S) - start + 16)
+        events = float(outdeg[idx].sum()) / runs * args.steps
+        nspk = len(idx) / runs * args.steps
+        del idx, st
+        net.restore(0)
+        prof = net.profile(200)
+        sec = ms / 1e3
+        value = events * world / sec
+        per_step_events = events / (args.steps * steps_run)
+        per_step_bundles = nspk / (args.steps * steps_run) * (DMAX - DMIN + 1)
+        db = BYTES_EVENT * per_step_events + BYTES_BUNDLE * per_step_bundles
+        dmsk = [m for k, m in prof if k == 6]
+        roof = _roofline(db, dmsk[0], "deliver_add_batch_kernel")
+        roof["traffic"] = _traffic_lookup("deliver_add_batch_kernel@propagation")
+        roof["note"] = ("12 B per event (target index 4 B + target read/write 8 B) + 8 B per "
+                        "(spike, delay) bundle; bound: one L2 atomic per event")
+        line = _line_base(args, world, "synaptic events/s", value, "events/s",
+                          ms / args.steps, WORKLOADS[wl],
+                          {"sim_steps_per_step": steps_run, "neurons": 2 * N_NEURONS,
+                           "synapses": int(outdeg.sum()), "parallelism": f"replicas x{world}",
+                           "l2": "working set > L2 (0.8 GB of synapse targets)"},
+                          "f32")
+        line.update({"events_per_sim_step": per_step_events,
+                     "input_spikes_per_sim_step": nspk / (args.steps * steps_run),
+                     "roofline": roof, "autotune": tune,
+                     "kernel_ms_mean_per_launch": {
+                         ("delivery" if k == 6 else f"site {k}"): v for k, v in prof},
+                     "gpu_launches": launches, "clocks": clk})
+        net.close()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            sample = 20
+            orc = OracleNet(DT, f32=True)
+            oids = build_propagation(orc, monitor_capacity=N_NEURONS * sample)
+            orc.finalize()
+            orc.set_uniforms(oids["S"], np.random.default_rng(9).random(
+                (2 * DMAX + sample, N_NEURONS), dtype=np.float32))
+            orc.run(2 * DMAX)
+            n0 = len(orc.spikes(oids["S"])[0])
+            t0 = time.perf_counter()
+            orc.run(sample)
+            el = time.perf_counter() - t0
+            oi = orc.spikes(oids["S"])[0]
+            # events delivered in the sample: the due bundles of the last 50 steps' spikes,
+            # about the steady per-step count of the GPU run
+            line["cpu_baseline"] = {"value": per_step_events * sample / el, "unit": "events/s",
+                                    "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"{sample} steps after a {2 * DMAX}-step fill "
+                                              f"({el:.1f} s, {len(oi) - n0} input spikes), "
+                                              "C++ oracle; events counted at the GPU run's "
+                                              "mean per step"}
     elif wl == "hines":
         steps_run = 8000
         net = Network(25e-6, seed=models.SEED_BASE + 3, device=local, stream=stream.cuda_stream)
@@ -830,7 +917,9 @@ def kernel_case(name: str):
     """Small cases for ncu captures of single kernels (inputs above the L2 size, a few GB at
     most): hh4m = 4e6 HH neurons (hh_stream_kernel), surrogate1m = 1e6 HH neurons with the
     gating surrogate attached (hh_surrogate_step_kernel), mlp_train = one epoch of surrogate
-    training on 2e6 transitions (mlp_grad_kernel, mlp_adam_kernel)."""
+    training on 2e6 transitions (mlp_grad_kernel, mlp_adam_kernel), propagation /
+    propagation3000 = the propagation workload at 300 / 3000 Hz of input, 100 filling steps
+    then 20 profiled ones (deliver_add_batch_kernel, 6e6 / 6e7 events per step)."""
     import torch
 
     from brian2cuda_b200 import Network, models
@@ -846,6 +935,14 @@ def kernel_case(name: str):
             s.attach(net, P, tol=SURR_TOL, judge=True)
         net.finalize()
         net.run(6)
+        net.sync()
+        net.close()
+    elif name in ("propagation", "propagation3000"):
+        net = Network(DT, seed=models.SEED_BASE + 5)
+        build_propagation(net, rate=PROP_RATE if name == "propagation" else 3000.0)
+        net.finalize()
+        net.run(2 * DMAX)       # 100 delivery launches before the profiled ones
+        net.profile(20)
         net.sync()
         net.close()
     elif name == "mlp_train":
