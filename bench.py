@@ -221,7 +221,7 @@ def main():
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
                     choices=["hh4m", "surrogate1m", "mlp_train", "propagation",
-                             "propagation3000"],
+                             "propagation3000", "stdp", "stdp_synorder"],
                     help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
     if args.kernel_case:
@@ -775,9 +775,13 @@ def bench_small(args, world, rank, local):
                            "synapses": 10_000_000, "parallelism": f"replicas x{world}",
                            "l2": "working set > L2 (1e7 synapses x 4 f32 variables = 160 MB)"},
                           "f32")
+        roof = _roofline(b, dom[1], kname)
+        if kname == "deliver_stdp_post_kernel":
+            post_grouped = any(t["site_kind"] == 8 and t["choice_a"] == 1 for t in tune)
+            roof["traffic"] = _traffic_lookup(kname + ("" if post_grouped else "@synorder"))
         line.update({"on_pre_events_per_s": ev_pre / sec, "on_post_events_per_s": ev_post / sec,
                      "neuron_updates_per_s": 11_000.0 * steps_run * args.steps * world / sec,
-                     "roofline": _roofline(b, dom[1], kname),
+                     "roofline": roof,
                      "kernel_ms_mean_per_launch": {f"site {k}": v for k, v in prof},
                      "autotune": tune, "gpu_launches": launches, "clocks": clk})
         net.close()
@@ -786,17 +790,18 @@ def bench_small(args, world, rank, local):
             oids = models.build_stdp(orc, monitor_capacity=cap)
             orc.finalize()
             # the oracle's Poisson group reads supplied uniforms (the GPU draws them with cuRAND)
-            orc.set_uniforms(oids["inp"], np.random.default_rng(7).random((1000, 10_000),
+            sample = 250
+            orc.set_uniforms(oids["inp"], np.random.default_rng(7).random((sample, 10_000),
                                                                           dtype=np.float32))
             t0 = time.perf_counter()
-            orc.run(1000)
+            orc.run(sample)
             el = time.perf_counter() - t0
             oin = len(orc.spikes(oids["inp"])[0])
             oout = len(orc.spikes(oids["out"])[0])
             line["cpu_baseline"] = {"value": (oin * 1000.0 + oout * 10_000.0) / el,
                                     "unit": "events/s", "cores": os.cpu_count(), "kind": "port",
-                                    "sample": f"the first 1000 steps of the run ({el:.1f} s), "
-                                              "C++ oracle"}
+                                    "sample": f"the first {sample} steps of the run "
+                                              f"({el:.1f} s), C++ oracle"}
     elif wl == "propagation":
         steps_run = 1000
         runs = args.warmup + args.steps
@@ -919,7 +924,9 @@ def kernel_case(name: str):
     gating surrogate attached (hh_surrogate_step_kernel), mlp_train = one epoch of surrogate
     training on 2e6 transitions (mlp_grad_kernel, mlp_adam_kernel), propagation /
     propagation3000 = the propagation workload at 300 / 3000 Hz of input, 100 filling steps
-    then 20 profiled ones (deliver_add_batch_kernel, 6e6 / 6e7 events per step)."""
+    then 20 profiled ones (deliver_add_batch_kernel, 6e6 / 6e7 events per step), stdp /
+    stdp_synorder = the STDP workload with its records grouped by postsynaptic neuron / in
+    synapse order, 200 steps then 20 profiled ones (deliver_stdp_post_kernel)."""
     import torch
 
     from brian2cuda_b200 import Network, models
@@ -935,6 +942,16 @@ def kernel_case(name: str):
             s.attach(net, P, tol=SURR_TOL, judge=True)
         net.finalize()
         net.run(6)
+        net.sync()
+        net.close()
+    elif name in ("stdp", "stdp_synorder"):
+        net = Network(DT, seed=models.SEED_BASE + 2)
+        models.build_stdp(net)
+        net.finalize()
+        net.tune_apply([{"site_kind": 8, "site_index": 0, "choice_b": 0,
+                         "choice_a": 1 if name == "stdp" else 0}])
+        net.run(200)            # 200 launches of each kernel before the profiled ones
+        net.profile(20)
         net.sync()
         net.close()
     elif name in ("propagation", "propagation3000"):

@@ -1232,6 +1232,44 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
 // ---- autotuner ------------------------------------------------------------------------------
 namespace {
 
+// Puts the STDP records of a projection in post-grouped order (on_post walks contiguous
+// records, on_pre reaches them through rec_of) or back in synapse order.  The live records
+// and every stored copy of them (snapshots) are permuted together, so a later restore
+// finds them in the order in use.
+b2b_status set_record_order(b2b_net* net, Proj& pr, bool post_grouped) {
+  if ((pr.dev.rec_of != nullptr) == post_grouped) return B2B_OK;
+  cudaStream_t s = net->stream;
+  if (post_grouped && !pr.rec_buf) {
+    CU(dalloc(pr, &pr.rec_buf, (size_t)pr.n_syn));
+    CU(build_rec_of(pr.dev.post_syn, pr.n_syn, pr.rec_buf, s));
+  }
+  const size_t bytes = 4 * real_size(pr.dtype) * (size_t)pr.n_syn;
+  std::vector<void*> copies = {pr.dev.syn4};
+  const auto state = state_arrays(net);
+  for (size_t k = 0; k < state.size(); ++k) {
+    if (state[k].first != pr.dev.syn4) continue;
+    for (const Snapshot& sn : net->snapshots)
+      if (sn.valid && k < sn.buffers.size()) copies.push_back(sn.buffers[k]);
+  }
+  void* tmp = nullptr;
+  CU(cudaMalloc(&tmp, bytes ? bytes : 1));
+  cudaError_t e = cudaSuccess;
+  for (void* a : copies) {
+    if (e == cudaSuccess)
+      e = permute_stdp_records(a, tmp, pr.dev.post_syn, pr.n_syn, pr.dtype, post_grouped, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a, tmp, bytes, cudaMemcpyDeviceToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "record order: %s", cudaGetErrorString(e));
+  pr.dev.rec_of = post_grouped ? pr.rec_buf : nullptr;
+  if (net->graph) {   // the graph holds the projection's parameters
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  return B2B_OK;
+}
+
 constexpr double kTuneMargin = 0.98;
 
 // Advances the net by n_steps the way b2b_run does (CUDA-graph replays of the current launch
@@ -1373,6 +1411,26 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
+  // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
+  for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
+    Proj& pr = net->projs[p];
+    if (pr.effect != B2B_EFFECT_STDP) continue;
+    b2b_tune_result r{8, (int32_t)p, 0, 0, 0.0, 0.0};
+    double best = 1e30;
+    for (int c = 0; c < 2 && st == B2B_OK; ++c) {
+      st = set_record_order(net, pr, c == 1);
+      double ms = 0;
+      if (st == B2B_OK) st = trial(&ms);
+      if (c == 0) r.default_ms = ms;
+      if (st == B2B_OK && (c == 0 || ms < kTuneMargin * best)) {
+        best = ms;
+        r.choice_a = c;
+      }
+    }
+    if (st == B2B_OK) st = set_record_order(net, pr, r.choice_a == 1);
+    r.best_ms = best;
+    res.push_back(r);
+  }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
   if (st2 == B2B_OK) st2 = put_back_monitors();
@@ -1421,6 +1479,13 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       net->add_tune[t.site_index].group = t.choice_a;
       net->add_tune[t.site_index].grid = t.choice_b;
+    } else if (t.site_kind == 8) {
+      CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
+                net->projs[t.site_index].effect == B2B_EFFECT_STDP,
+            B2B_ERR_INVALID_ARG, "bad STDP projection index %d", t.site_index);
+      CHECK(t.choice_a == 0 || t.choice_a == 1, B2B_ERR_INVALID_ARG, "bad record order");
+      if (b2b_status st = set_record_order(net, net->projs[t.site_index], t.choice_a == 1))
+        return st;
     } else {
       return fail(net, B2B_ERR_INVALID_ARG, "bad site kind %d", t.site_kind);
     }

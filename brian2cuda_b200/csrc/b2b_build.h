@@ -34,6 +34,13 @@ cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_
 // Adds the out-degree (all delays) of source neurons [first, first + n) into d_out.
 cudaError_t add_out_degree(const int64_t* d_off, int32_t nd, int64_t first, int64_t n,
                            int32_t* d_out, cudaStream_t s);
+// STDP records from synapse order into post-grouped order (record r = synapse post_syn[r]) or
+// back, d_in -> d_out (distinct buffers).
+cudaError_t permute_stdp_records(const void* d_in, void* d_out, const int32_t* d_post_syn,
+                                 int64_t n, int dtype, bool to_post, cudaStream_t s);
+// rec_of[post_syn[r]] = r: the post-grouped record of each synapse position.
+cudaError_t build_rec_of(const int32_t* d_post_syn, int64_t n, int32_t* d_rec_of,
+                         cudaStream_t s);
 // Interleaved STDP records {w, Apre = 0, Apost = 0, lastupdate = 0} from initial weights.
 cudaError_t pack_stdp(const void* d_w, void* d_syn4, int dtype, int64_t n, cudaStream_t s);
 }  // namespace b2b

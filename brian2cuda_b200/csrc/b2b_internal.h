@@ -104,6 +104,10 @@ struct ProjDev {
   int32_t post_chunks;
   const int64_t* post_off;        // [n_post + 1]
   const int32_t* post_syn;        // synapse positions grouped by post
+  // Order of the STDP records: NULL, record s belongs to synapse position s; otherwise the
+  // records follow the post-grouped index (record r is synapse post_syn[r], so on_post walks
+  // contiguous records) and rec_of[s] is the record of synapse position s.
+  const int32_t* rec_of;
 };
 
 // Device view of the one-kernel-per-step path (fused.cu): one population and its additive
@@ -201,6 +205,7 @@ struct Proj {
   int32_t* post = nullptr;
   void* w = nullptr;
   std::vector<void*> allocs;
+  int32_t* rec_buf = nullptr;                // STDP: record of each synapse, post-grouped order
 };
 
 }  // namespace b2b

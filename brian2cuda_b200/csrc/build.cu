@@ -152,8 +152,8 @@ __global__ void gather_kernel(int var, int64_t n, int64_t pos_base, const int64_
                               const int64_t* __restrict__ off, int64_t key_lo, int64_t key_hi,
                               int32_t nd, int32_t dmin, int64_t src_offset,
                               const int32_t* __restrict__ post, int64_t dst_offset,
-                              const R* __restrict__ arr, int64_t stride, double w_scalar,
-                              void* out) {
+                              const R* __restrict__ arr, int64_t stride,
+                              const int32_t* __restrict__ rec, double w_scalar, void* out) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pos = inv ? inv[q] : pos_base + q;
@@ -170,7 +170,7 @@ __global__ void gather_kernel(int var, int64_t n, int64_t pos_base, const int64_
                                            : (int32_t)(lo % nd + dmin);
       static_cast<int32_t*>(out)[q] = val;
     } else {
-      static_cast<R*>(out)[q] = arr ? arr[pos * stride] : (R)w_scalar;
+      static_cast<R*>(out)[q] = arr ? arr[(rec ? (int64_t)rec[pos] : pos) * stride] : (R)w_scalar;
     }
   }
 }
@@ -240,6 +240,49 @@ cudaError_t member_sort_scatter(uint32_t* d_keys, uint32_t* d_vals, int64_t n,
   cudaFree(k2);
   cudaFree(v2);
   return e;
+}
+
+namespace {
+// STDP records between synapse order and post-grouped order (record r of the post-grouped
+// order is synapse post_syn[r]).
+template <typename R>
+__global__ void permute_records_kernel(const R* __restrict__ in, R* __restrict__ out,
+                                       const int32_t* __restrict__ post_syn, int64_t n,
+                                       bool to_post) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = post_syn[r];
+    const R* src = in + 4 * (to_post ? s : r);
+    R* dst = out + 4 * (to_post ? r : s);
+    for (int c = 0; c < 4; ++c) dst[c] = src[c];
+  }
+}
+
+__global__ void rec_of_kernel(const int32_t* __restrict__ post_syn, int64_t n,
+                              int32_t* __restrict__ rec_of) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x)
+    rec_of[post_syn[r]] = (int32_t)r;
+}
+}  // namespace
+
+cudaError_t permute_stdp_records(const void* d_in, void* d_out, const int32_t* d_post_syn,
+                                 int64_t n, int dtype, bool to_post, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  if (dtype == B2B_F32)
+    permute_records_kernel<float><<<grid_for(n), 256, 0, s>>>(
+        static_cast<const float*>(d_in), static_cast<float*>(d_out), d_post_syn, n, to_post);
+  else
+    permute_records_kernel<double><<<grid_for(n), 256, 0, s>>>(
+        static_cast<const double*>(d_in), static_cast<double*>(d_out), d_post_syn, n, to_post);
+  return cudaGetLastError();
+}
+
+cudaError_t build_rec_of(const int32_t* d_post_syn, int64_t n, int32_t* d_rec_of,
+                         cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  rec_of_kernel<<<grid_for(n), 256, 0, s>>>(d_post_syn, n, d_rec_of);
+  return cudaGetLastError();
 }
 
 cudaError_t fill_value(void* d, int dtype, int64_t n, double v, cudaStream_t s) {
@@ -324,18 +367,20 @@ cudaError_t gather_syn_var(const Proj& pr, int var, const int64_t* d_inv, int64_
                            int64_t dst_offset, const void* d_arr, int64_t stride,
                            double w_scalar, void* d_out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
+  // STDP record components are read through the record order
+  const int32_t* rec = stride == 4 ? pr.dev.rec_of : nullptr;
   if (pr.dtype == B2B_F32)
     gather_kernel<float><<<grid_for(n), 256, 0, s>>>(var, n, pos_base, d_inv, pr.off, key_lo,
                                                      key_hi, pr.dmax - pr.dmin + 1, pr.dmin,
                                                      src_offset, pr.post, dst_offset,
                                                      static_cast<const float*>(d_arr),
-                                                     stride, w_scalar, d_out);
+                                                     stride, rec, w_scalar, d_out);
   else
     gather_kernel<double><<<grid_for(n), 256, 0, s>>>(var, n, pos_base, d_inv, pr.off, key_lo,
                                                       key_hi, pr.dmax - pr.dmin + 1, pr.dmin,
                                                       src_offset, pr.post, dst_offset,
                                                       static_cast<const double*>(d_arr),
-                                                      stride, w_scalar, d_out);
+                                                      stride, rec, w_scalar, d_out);
   return cudaGetLastError();
 }
 

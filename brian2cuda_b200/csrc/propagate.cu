@@ -123,7 +123,8 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
     R w = 0;
     if (valid) {
       post = __ldg(P.post + s);
-      SynRec<R> r = S[s];
+      const int64_t q = P.rec_of ? (int64_t)__ldg(P.rec_of + s) : s;
+      SynRec<R> r = S[q];
       w = r.w;
       const R tau = (R)(t - (double)r.lu);
       R apre = r.apre * dexp(-tau / taupre);
@@ -133,7 +134,7 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
       r.apre = apre;
       r.apost = apost;
       r.lu = (R)t;
-      S[s] = r;
+      S[q] = r;
     }
     if (P.pre_adds_weight) add_to_target<R, AGG>(T, post, w, valid);
   });
@@ -164,18 +165,31 @@ deliver_stdp_post_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, do
     const int64_t b0 = P.post_off[j] + (int64_t)ch * kChunk;
     int64_t b1 = P.post_off[j + 1];
     if (b1 > b0 + kChunk) b1 = b0 + kChunk;
-    for (int64_t r = b0 + lane; r < b1; r += 32) {
-      const int64_t s = P.post_syn[r];
-      SynRec<R> q = S[s];
-      const R tau = (R)(t - (double)q.lu);
-      const R apre = q.apre * dexp(-tau / taupre);
-      R apost = q.apost * dexp(-tau / taupost);
+    // the lane's (up to) kChunk/32 records of the item, all loaded before any is updated so
+    // that their loads are in flight together (distinct records: no ordering between them)
+    static_assert(kChunk % 32 == 0, "an item is whole rounds of the warp");
+    constexpr int kPer = kChunk / 32;
+    SynRec<R> q[kPer];
+    int64_t at[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t r = b0 + lane + 32 * u;
+      // post-grouped records: record r itself (contiguous); otherwise its synapse's record
+      at[u] = r < b1 ? (P.rec_of ? r : (int64_t)P.post_syn[r]) : -1;
+      if (at[u] >= 0) q[u] = S[at[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (at[u] < 0) continue;
+      const R tau = (R)(t - (double)q[u].lu);
+      const R apre = q[u].apre * dexp(-tau / taupre);
+      R apost = q[u].apost * dexp(-tau / taupost);
       apost = apost + dApost;
-      q.w = dclip(q.w + apre, wmin, wmax);
-      q.apre = apre;
-      q.apost = apost;
-      q.lu = (R)t;
-      S[s] = q;
+      q[u].w = dclip(q[u].w + apre, wmin, wmax);
+      q[u].apre = apre;
+      q[u].apost = apost;
+      q[u].lu = (R)t;
+      S[at[u]] = q[u];
     }
   }
 }

@@ -261,15 +261,18 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
  * steps run as b2b_run runs them (graph replays), so a shape is judged by the step time it
  * gives.  Populations: neurons per thread (1 or 4) x threads per CTA (128 or 256), or, with a
  * gating surrogate, CTAs per SM (2..6); additive delivery launches: lanes per work item
- * (4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM).  Afterwards the state, clock and monitor
- * counts are as before the call, and the next b2b_run captures its graph with the chosen
- * shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
+ * (4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM); STDP projections: the order of the synapse
+ * records (0 synapse order, 1 grouped by postsynaptic neuron, where on_post reads contiguous
+ * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
+ * through the order).  Afterwards the state, clock and monitor counts are as before the call,
+ * and the next b2b_run captures its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
  * rule) to be chosen.  A choice of 0 means the built-in rule won.  The trials should cover a
  * representative stretch of the run (bursts included). */
 typedef struct {
-  int32_t site_kind;     /* 1 population, 6 additive delivery launch                    */
-  int32_t site_index;    /* population index / delivery launch index                    */
-  int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item */
+  int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records     */
+  int32_t site_index;    /* population / delivery launch / projection index              */
+  int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item /
+                            record order                                                  */
   int32_t choice_b;      /* threads per CTA / CTAs                                       */
   double best_ms;        /* mean device time of one whole step with the chosen shape     */
   double default_ms;     /* the same with the built-in rule                              */

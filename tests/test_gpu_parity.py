@@ -191,7 +191,13 @@ def test_generated_connectivity_matches_oracle(gpu_factory, oracle_factory):
     assert len(out["gpu"][0]) > 1000
 
 
-def test_stdp_with_poisson_input(gpu_factory, oracle_factory):
+# STDP projection 0: records grouped by postsynaptic neuron (autotuner site kind 8)
+POST_GROUPED = [{"site_kind": 8, "site_index": 0, "choice_a": 1, "choice_b": 0}]
+SYNAPSE_ORDER = [{"site_kind": 8, "site_index": 0, "choice_a": 0, "choice_b": 0}]
+
+
+@pytest.mark.parametrize("post_grouped", [False, True])
+def test_stdp_with_poisson_input(gpu_factory, oracle_factory, post_grouped):
     K = 50
     gpu = gpu_factory(DT, steps_per_graph=K, seed=5)
     orc = oracle_factory(DT)
@@ -200,6 +206,8 @@ def test_stdp_with_poisson_input(gpu_factory, oracle_factory):
         ids[name] = models.build_stdp(net, n_in=400, n_out=60, rate=80.0, dtype="float64",
                                       monitor_capacity=10**6)
         net.finalize()
+    if post_grouped:
+        gpu.tune_apply(POST_GROUPED)
     for _ in range(8):
         gpu.run(K)
         orc.set_uniforms(ids["orc"]["inp"], gpu.rng_uniforms(ids["gpu"]["inp"], K))
@@ -211,6 +219,33 @@ def test_stdp_with_poisson_input(gpu_factory, oracle_factory):
     assert len(gpu.spikes(ids["gpu"]["out"])[0]) > 0
     for v in ("w", "Apre", "Apost", "lastupdate"):
         _close(gpu.syn_get(ids["gpu"]["S"], v), orc.syn_get(ids["orc"]["S"], v), 1e-10, 1e-18)
+
+
+def test_stdp_record_order_keeps_snapshots(gpu_factory):
+    """Changing the record order permutes the stored snapshot with the live records: runs
+    from one snapshot agree whatever order was in use when it was taken or restored."""
+    net = gpu_factory(DT, steps_per_graph=25, seed=5)
+    ids = models.build_stdp(net, n_in=300, n_out=40, rate=80.0, dtype="float64",
+                            monitor_capacity=10**6)
+    net.finalize()
+    net.run(60)
+    w0 = net.syn_get(ids["S"], "w")
+    net.store(0)
+    res = []
+    for order in (SYNAPSE_ORDER, POST_GROUPED, SYNAPSE_ORDER):
+        net.tune_apply(order)
+        net.restore(0)
+        np.testing.assert_array_equal(net.syn_get(ids["S"], "w"), w0)
+        start = net.spikes_recorded(ids["out"])
+        net.run(90)
+        idx, st, _ = net.spikes_fetch(ids["out"], start)
+        res.append((idx, st, net.syn_get(ids["S"], "w"), net.syn_get(ids["S"], "Apost")))
+    assert len(res[0][0]) > 0
+    for r in res[1:]:
+        np.testing.assert_array_equal(r[1], res[0][1])
+        np.testing.assert_array_equal(np.sort(r[0]), np.sort(res[0][0]))
+        _close(r[2], res[0][2], 1e-12, 1e-18)
+        _close(r[3], res[0][3], 1e-12, 1e-18)
 
 
 def test_poisson_spikes_follow_uniforms(gpu_factory):
