@@ -118,25 +118,42 @@ deliver_stdp_pre_kernel(ProjDev P, const int64_t* __restrict__ clock, int k, dou
   const R wmin = (R)P.wmin, wmax = (R)P.wmax;
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for_each_due<WARP_PREFIX>(P, ts, warp0, nwarps, s_pref, [&](int64_t s, bool valid, int32_t) {
-    int32_t post = 0;
-    R w = 0;
-    if (valid) {
-      post = __ldg(P.post + s);
-      const int64_t q = P.rec_of ? (int64_t)__ldg(P.rec_of + s) : s;
-      SynRec<R> r = S[q];
-      w = r.w;
-      const R tau = (R)(t - (double)r.lu);
-      R apre = r.apre * dexp(-tau / taupre);
-      const R apost = r.apost * dexp(-tau / taupost);
-      apre = apre + dApre;
-      r.w = dclip(w + apost, wmin, wmax);
-      r.apre = apre;
-      r.apost = apost;
-      r.lu = (R)t;
-      S[q] = r;
+  const int lane = threadIdx.x & 31;
+  for_each_due_item<WARP_PREFIX, 32>(P, ts, warp0, nwarps, s_pref,
+                                     [&](int64_t b0, int64_t b1, int64_t len, int32_t) {
+    // the item's (at most kChunk) synapses, kChunk/32 per lane: every load of the lane is
+    // issued before the first record is updated (distinct records: no ordering between them)
+    static_assert(kChunk % 32 == 0, "an item is whole rounds of the warp");
+    constexpr int kPer = kChunk / 32;
+    SynRec<R> r[kPer];
+    int64_t at[kPer];
+    int32_t post[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int64_t s = b0 + lane + 32 * u;
+      const bool ok = s < b1;
+      post[u] = ok ? __ldg(P.post + s) : 0;
+      at[u] = ok ? (P.rec_of ? (int64_t)__ldg(P.rec_of + s) : s) : -1;
+      if (ok) r[u] = S[at[u]];
     }
-    if (P.pre_adds_weight) add_to_target<R, AGG>(T, post, w, valid);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      R w = 0;
+      if (at[u] >= 0) {
+        w = r[u].w;
+        const R tau = (R)(t - (double)r[u].lu);
+        R apre = r[u].apre * dexp(-tau / taupre);
+        const R apost = r[u].apost * dexp(-tau / taupost);
+        apre = apre + dApre;
+        r[u].w = dclip(w + apost, wmin, wmax);
+        r[u].apre = apre;
+        r[u].apost = apost;
+        r[u].lu = (R)t;
+        S[at[u]] = r[u];
+      }
+      if (P.pre_adds_weight && 32 * u < len)  // warp-uniform
+        add_to_target<R, AGG>(T, post[u], w, at[u] >= 0);
+    }
   });
 }
 
