@@ -122,6 +122,10 @@ PROTOTYPES = {
     "b2b_tune_apply": (I32, [P, C.POINTER(TuneResult), I32]),
     "b2b_spikemon_fetch_population": (I32, [P, I32, I64, PI64, PI64, P, P, I64]),
     "b2b_group_offset": (I32, [P, I32, PI64]),
+    "b2b_statemon": (I32, [P, I32, I32, PI64, I64, I32, I64, PI32]),
+    "b2b_statemon_get": (I32, [P, I32, PI64, PI64, P, I64]),
+    "b2b_ratemon": (I32, [P, I32, I64, PI32]),
+    "b2b_ratemon_get": (I32, [P, I32, PI64, PI64, PI32, I64]),
     "b2b_mlp_create": (I32, [I32, P, U64, C.POINTER(P)]),
     "b2b_mlp_destroy": (I32, [P]),
     "b2b_mlp_params_get": (I32, [P, P, I64]),

@@ -600,6 +600,78 @@ b2b_status finalize_projs(b2b_net* net) {
   return B2B_OK;
 }
 
+// Buffers and device views of the state and rate monitors (after the populations exist).
+b2b_status setup_monitors(b2b_net* net) {
+  auto mal = [&](void** p, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 1);
+    if (e == cudaSuccess) net->mon_allocs.push_back(*p);
+    return e;
+  };
+  std::vector<StateMonDev> sd;
+  for (StateMon& m : net->smons) {
+    const Group& g = net->groups[m.gid];
+    const Pop& pop = net->pops[g.pop];
+    StateMonDev& D = m.dev;
+    D.es = (int32_t)var_size(pop.dtype, m.var);
+    D.src = static_cast<const uint8_t*>(pop.dev.var[m.var]);
+    D.n_idx = (int64_t)m.idx.size();
+    D.cap = m.cap;
+    D.every = m.every;
+    std::vector<int64_t> rows(m.idx);
+    for (int64_t& r : rows) r += g.offset;
+    void *idx = nullptr, *buf = nullptr, *steps = nullptr, *cnt = nullptr, *tk = nullptr;
+    CU(mal(&idx, sizeof(int64_t) * rows.size()));
+    CU(mal(&buf, (size_t)D.es * (size_t)D.n_idx * (size_t)m.cap));
+    CU(mal(&steps, sizeof(int64_t) * (size_t)m.cap));
+    CU(mal(&cnt, sizeof(unsigned long long)));
+    CU(mal(&tk, sizeof(unsigned int)));
+    CU(cudaMemcpy(idx, rows.data(), sizeof(int64_t) * rows.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemset(cnt, 0, sizeof(unsigned long long)));
+    CU(cudaMemset(tk, 0, sizeof(unsigned int)));
+    D.idx = static_cast<const int64_t*>(idx);
+    D.buf = static_cast<uint8_t*>(buf);
+    D.steps = static_cast<int64_t*>(steps);
+    D.cnt = static_cast<unsigned long long*>(cnt);
+    D.ticket = static_cast<unsigned int*>(tk);
+    net->smon_max_idx = std::max(net->smon_max_idx, D.n_idx);
+    sd.push_back(D);
+  }
+  std::vector<RateMonDev> rd;
+  for (RateMon& m : net->rmons) {
+    const Group& g = net->groups[m.gid];
+    const Pop& pop = net->pops[g.pop];
+    RateMonDev& D = m.dev;
+    D.ring_idx = pop.dev.ring_idx;
+    D.ring_cnt = pop.dev.ring_cnt;
+    D.ring_n = pop.n;
+    D.ring_len = pop.dev.ring_len;
+    D.lo = g.offset;
+    D.hi = g.offset + g.n;
+    D.whole = pop.groups.size() == 1 ? 1 : 0;
+    D.cap = m.cap;
+    void *buf = nullptr, *steps = nullptr, *cnt = nullptr;
+    CU(mal(&buf, sizeof(int32_t) * (size_t)m.cap));
+    CU(mal(&steps, sizeof(int64_t) * (size_t)m.cap));
+    CU(mal(&cnt, sizeof(unsigned long long)));
+    CU(cudaMemset(cnt, 0, sizeof(unsigned long long)));
+    D.buf = static_cast<int32_t*>(buf);
+    D.steps = static_cast<int64_t*>(steps);
+    D.cnt = static_cast<unsigned long long*>(cnt);
+    rd.push_back(D);
+  }
+  if (!sd.empty()) {
+    CU(mal((void**)&net->d_smons, sizeof(StateMonDev) * sd.size()));
+    CU(cudaMemcpy(net->d_smons, sd.data(), sizeof(StateMonDev) * sd.size(),
+                  cudaMemcpyHostToDevice));
+  }
+  if (!rd.empty()) {
+    CU(mal((void**)&net->d_rmons, sizeof(RateMonDev) * rd.size()));
+    CU(cudaMemcpy(net->d_rmons, rd.data(), sizeof(RateMonDev) * rd.size(),
+                  cudaMemcpyHostToDevice));
+  }
+  return B2B_OK;
+}
+
 // One kernel per step (fused.cu) applies when the net is one LIF/HH population whose
 // synapses are all additive onto ge/gi of that population with delays of at least one step.
 // A small network (small.cu, opt-in with B2B_NET_SMALL) runs every step of a chunk in one
@@ -608,6 +680,7 @@ b2b_status finalize_projs(b2b_net* net) {
 b2b_status setup_small(b2b_net* net) {
   if (!(net->cfg.flags & B2B_NET_SMALL) || (net->cfg.flags & (B2B_NET_CHECKED | B2B_NET_FUSED)))
     return B2B_OK;
+  if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.size() > kMaxProjBatch) return B2B_OK;
   const Pop& pop = net->pops[0];
   if ((pop.kind != KIND_LIF && pop.kind != KIND_HH) || pop.surr_img || pop.n > 4096)
@@ -639,6 +712,7 @@ b2b_status setup_small(b2b_net* net) {
 
 b2b_status setup_fused(b2b_net* net) {
   if (!(net->cfg.flags & B2B_NET_FUSED)) return B2B_OK;
+  if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
     return B2B_OK;
   const Pop& pop = net->pops[0];
@@ -710,6 +784,11 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     return B2B_OK;
   }
   for (int k = 0; k < kk; ++k) {
+    if (!net->smons.empty()) {
+      CU(launch_statemon(net->d_smons, (int)net->smons.size(), net->smon_max_idx, net->d_clock,
+                         k, net->d_status, net->stream));
+      ++net->launches;
+    }
     for (const Pop& pop : net->pops) {
       CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
       ++net->launches;
@@ -733,6 +812,11 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     for (const Pop& pop : net->pops) {
       if (!pop.late_reset) continue;
       CU(launch_pop_late_reset(pop, net->d_clock, k, net->stream));
+      ++net->launches;
+    }
+    if (!net->rmons.empty()) {
+      CU(launch_ratemon(net->d_rmons, (int)net->rmons.size(), net->d_clock, k, net->d_status,
+                        net->stream));
       ++net->launches;
     }
   }
@@ -862,6 +946,7 @@ b2b_status b2b_destroy(b2b_net* net) {
   for (Snapshot& sn : net->snapshots)
     for (void* a : sn.buffers) cudaFree(a);
   for (void* a : net->fused_allocs) cudaFree(a);
+  for (void* a : net->mon_allocs) cudaFree(a);
   cudaFree(net->d_clock);
   cudaFree(net->d_status);
   if (net->own_stream) cudaStreamDestroy(net->stream);
@@ -1108,12 +1193,88 @@ b2b_status b2b_spikemon(b2b_net* net, int32_t gid, int64_t capacity) {
   return B2B_OK;
 }
 
+b2b_status b2b_statemon(b2b_net* net, int32_t gid, int32_t var, const int64_t* idx, int64_t n,
+                        int32_t every, int64_t capacity, int32_t* mid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "monitors must be added before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size() && mid, B2B_ERR_INVALID_ARG,
+        "bad group %d", gid);
+  const Group& g = net->groups[gid];
+  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(n >= 0 && (idx || n == 0) && every >= 1 && capacity > 0, B2B_ERR_INVALID_ARG,
+        "bad indices, interval or capacity");
+  StateMon m;
+  m.gid = gid;
+  m.var = var;
+  m.every = every;
+  m.cap = capacity;
+  for (int64_t k = 0; k < n; ++k) {
+    CHECK(idx[k] >= 0 && idx[k] < g.n, B2B_ERR_INDEX, "index %lld outside group %d",
+          (long long)idx[k], gid);
+    m.idx.push_back(idx[k]);
+  }
+  net->smons.push_back(std::move(m));
+  *mid = (int32_t)net->smons.size() - 1;
+  return B2B_OK;
+}
+
+b2b_status b2b_statemon_get(b2b_net* net, int32_t mid, int64_t* n_records, int64_t* steps,
+                            void* values, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(mid >= 0 && mid < (int)net->smons.size() && n_records && cap >= 0,
+        B2B_ERR_INVALID_ARG, "bad state monitor %d", mid);
+  const StateMonDev& D = net->smons[mid].dev;
+  CU(cudaStreamSynchronize(net->stream));
+  unsigned long long cnt = 0;
+  CU(cudaMemcpy(&cnt, D.cnt, sizeof(cnt), cudaMemcpyDeviceToHost));
+  *n_records = (int64_t)cnt;
+  const int64_t m = std::min<int64_t>((int64_t)cnt, cap);
+  if (m > 0 && steps) CU(cudaMemcpy(steps, D.steps, sizeof(int64_t) * m, cudaMemcpyDeviceToHost));
+  if (m > 0 && values)
+    CU(cudaMemcpy(values, D.buf, (size_t)D.es * (size_t)D.n_idx * (size_t)m,
+                  cudaMemcpyDeviceToHost));
+  return B2B_OK;
+}
+
+b2b_status b2b_ratemon(b2b_net* net, int32_t gid, int64_t capacity, int32_t* mid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "monitors must be added before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size() && mid, B2B_ERR_INVALID_ARG,
+        "bad group %d", gid);
+  CHECK(capacity > 0, B2B_ERR_INVALID_ARG, "capacity must be positive");
+  RateMon m;
+  m.gid = gid;
+  m.cap = capacity;
+  net->rmons.push_back(m);
+  *mid = (int32_t)net->rmons.size() - 1;
+  return B2B_OK;
+}
+
+b2b_status b2b_ratemon_get(b2b_net* net, int32_t mid, int64_t* n_records, int64_t* steps,
+                           int32_t* counts, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(mid >= 0 && mid < (int)net->rmons.size() && n_records && cap >= 0,
+        B2B_ERR_INVALID_ARG, "bad rate monitor %d", mid);
+  const RateMonDev& D = net->rmons[mid].dev;
+  CU(cudaStreamSynchronize(net->stream));
+  unsigned long long cnt = 0;
+  CU(cudaMemcpy(&cnt, D.cnt, sizeof(cnt), cudaMemcpyDeviceToHost));
+  *n_records = (int64_t)cnt;
+  const int64_t m = std::min<int64_t>((int64_t)cnt, cap);
+  if (m > 0 && steps) CU(cudaMemcpy(steps, D.steps, sizeof(int64_t) * m, cudaMemcpyDeviceToHost));
+  if (m > 0 && counts) CU(cudaMemcpy(counts, D.buf, sizeof(int32_t) * m, cudaMemcpyDeviceToHost));
+  return B2B_OK;
+}
+
 b2b_status b2b_finalize(b2b_net* net) {
   if (b2b_status st = check_net(net)) return st;
   CHECK(!net->finalized, B2B_ERR_STATE, "already finalized");
   GUARD_BEGIN
   b2b_status st = finalize_pops(net);
   if (st == B2B_OK) st = finalize_projs(net);
+  if (st == B2B_OK) st = setup_monitors(net);
   if (st == B2B_OK) st = setup_fused(net);
   if (st == B2B_OK) st = setup_small(net);
   if (st != B2B_OK) return st;
@@ -1162,6 +1323,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   } else if (net->fused) {
     sites.push_back({5, 0});
   } else {
+    if (!net->smons.empty()) sites.push_back({9, 0});
     for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
     for (size_t b = 0; b < net->add_batches.size(); ++b) sites.push_back({6, (int)b});
     for (size_t p = 0; p < net->projs.size(); ++p)
@@ -1170,6 +1332,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
     for (size_t p = 0; p < net->pops.size(); ++p)
       if (net->pops[p].late_reset) sites.push_back({4, (int)p});
+    if (!net->rmons.empty()) sites.push_back({10, 0});
   }
   const size_t ns = sites.size();
   std::vector<cudaEvent_t> ev(2 * ns);
@@ -1190,6 +1353,12 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
+      if (s.kind == 9)
+        e = launch_statemon(net->d_smons, (int)net->smons.size(), net->smon_max_idx, clk, 0,
+                            net->d_status, net->stream);
+      if (s.kind == 10)
+        e = launch_ratemon(net->d_rmons, (int)net->rmons.size(), clk, 0, net->d_status,
+                           net->stream);
       if (s.kind == 7)
         e = launch_small(net->sdev, net->pops[0].kind, net->pops[0].dtype, clk, 1, net->cfg.dt,
                          net->d_status, net->stream);
@@ -1323,6 +1492,13 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     if (net->pops[p].dev.mon_cnt)
       CU(cudaMemcpy(&mon[p], net->pops[p].dev.mon_cnt, sizeof(unsigned long long),
                     cudaMemcpyDeviceToHost));
+  std::vector<unsigned long long> smon(net->smons.size()), rmon(net->rmons.size());
+  for (size_t m = 0; m < net->smons.size(); ++m)
+    CU(cudaMemcpy(&smon[m], net->smons[m].dev.cnt, sizeof(unsigned long long),
+                  cudaMemcpyDeviceToHost));
+  for (size_t m = 0; m < net->rmons.size(); ++m)
+    CU(cudaMemcpy(&rmon[m], net->rmons[m].dev.cnt, sizeof(unsigned long long),
+                  cudaMemcpyDeviceToHost));
   net->add_tune.resize(net->add_batches.size());
   std::vector<b2b_tune_result> res;
   b2b_status st = B2B_OK;
@@ -1331,6 +1507,12 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
       if (net->pops[p].dev.mon_cnt)
         CU(cudaMemcpy(net->pops[p].dev.mon_cnt, &mon[p], sizeof(unsigned long long),
                       cudaMemcpyHostToDevice));
+    for (size_t m = 0; m < net->smons.size(); ++m)
+      CU(cudaMemcpy(net->smons[m].dev.cnt, &smon[m], sizeof(unsigned long long),
+                    cudaMemcpyHostToDevice));
+    for (size_t m = 0; m < net->rmons.size(); ++m)
+      CU(cudaMemcpy(net->rmons[m].dev.cnt, &rmon[m], sizeof(unsigned long long),
+                    cudaMemcpyHostToDevice));
     return B2B_OK;
   };
   // every trial starts from the same state, with the monitors' counts of that state

@@ -110,6 +110,33 @@ struct ProjDev {
   const int32_t* rec_of;
 };
 
+// Device view of a state monitor (monitor.cu): variable src (es-byte elements) of the
+// population rows idx[0..n_idx), one record [n_idx] per step divisible by `every`.
+struct StateMonDev {
+  const uint8_t* src;
+  const int64_t* idx;             // population-level rows
+  uint8_t* buf;                   // [cap][n_idx]
+  int64_t* steps;                 // [cap] step of each record
+  unsigned long long* cnt;        // records written
+  unsigned int* ticket;           // CTAs done with the current record
+  int64_t n_idx, cap;
+  int32_t every, es;
+};
+
+// Device view of a population-rate monitor: spike count per step of the population rows
+// [lo, hi) (the whole population when `whole`), from the spike-history ring.
+struct RateMonDev {
+  const int32_t* ring_idx;
+  const int32_t* ring_cnt;
+  int64_t ring_n;                 // ring row stride (padded population size)
+  int32_t ring_len, whole;
+  int64_t lo, hi;
+  int32_t* buf;                   // [cap] spike counts
+  int64_t* steps;                 // [cap]
+  unsigned long long* cnt;
+  int64_t cap;
+};
+
 // Device view of the one-kernel-per-step path (fused.cu): one population and its additive
 // projections, whose targets are redirected to double-buffered input accumulators.
 struct FusedDev {
@@ -176,6 +203,19 @@ struct AddTune {
   int32_t group = 0;              // lanes per work item: 8, 16 or 32
 };
 
+struct StateMon {  // one StateMonitor (b2b_statemon)
+  int gid = -1, var = 0, every = 1;
+  std::vector<int64_t> idx;       // group-local
+  int64_t cap = 0;
+  StateMonDev dev{};
+};
+
+struct RateMon {  // one PopulationRateMonitor (b2b_ratemon)
+  int gid = -1;
+  int64_t cap = 0;
+  RateMonDev dev{};
+};
+
 struct Syn {  // one user-level Synapses object
   int pre_gid = -1, post_gid = -1, target_var = 0, effect = 0;
   int64_t n = 0;
@@ -236,6 +276,12 @@ struct b2b_net {
   std::vector<b2b::Proj> projs;
   std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
   std::vector<b2b::AddTune> add_tune;      // launch shape per add batch (b2b_autotune)
+  std::vector<b2b::StateMon> smons;        // state monitors, recorded at the start of a step
+  std::vector<b2b::RateMon> rmons;         // rate monitors, recorded at the end of a step
+  b2b::StateMonDev* d_smons = nullptr;     // device copies of smons[].dev / rmons[].dev
+  b2b::RateMonDev* d_rmons = nullptr;
+  int64_t smon_max_idx = 0;                // largest recorded index count
+  std::vector<void*> mon_allocs;
   bool small = false;                      // one CTA runs every step (small.cu)
   b2b::SmallDev sdev{};
   bool fused = false;                      // one kernel per step (fused.cu) in use
@@ -265,6 +311,11 @@ cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
                                   cudaStream_t s, const AddTune* tune = nullptr);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
+// All state monitors (start of step k of the chunk) / all rate monitors (end of the step).
+cudaError_t launch_statemon(const StateMonDev* d_mons, int n_mons, int64_t max_idx,
+                            const int64_t* clock, int k, int32_t* status, cudaStream_t s);
+cudaError_t launch_ratemon(const RateMonDev* d_mons, int n_mons, const int64_t* clock, int k,
+                           int32_t* status, cudaStream_t s);
 // COBAHH step of a population with a gating surrogate attached (surrogate.cu).
 cudaError_t launch_hh_surrogate(const Pop& pop, const int64_t* clock, int k, double dt,
                                 int32_t* status, cudaStream_t s);

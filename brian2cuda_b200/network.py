@@ -165,6 +165,7 @@ class Network:
         self._groups: list[tuple[str, int, int]] = []   # (kind, n, dtype code)
         self._syns: list[tuple[int, int, int]] = []     # (pre, post, dtype code)
         self._hines: list[HinesBatch] = []
+        self._smons: dict[int, tuple[int, type]] = {}   # state monitor: (width, dtype)
 
     # -- plumbing ---------------------------------------------------------------------------
     def _check(self, st: int, what: str):
@@ -309,6 +310,54 @@ class Network:
     # -- monitors and run -----------------------------------------------------------------------
     def spike_monitor(self, gid: int, capacity: int):
         self._check(self._lib.b2b_spikemon(self._h, gid, int(capacity)), "spikemon")
+
+    def state_monitor(self, gid: int, var: str, indices=None, every: int = 1,
+                      capacity: int = 0) -> int:
+        """Brian2's StateMonitor(G, var, record=indices, dt=every*dt): records `var` of the
+        given neurons (all when None) at the start of every step divisible by `every`, into
+        a device buffer of `capacity` records.  Returns the monitor index."""
+        n = self.group_size(gid)
+        idx = (np.arange(n, dtype=np.int64) if indices is None
+               else np.ascontiguousarray(indices, dtype=np.int64))
+        mid = C.c_int32()
+        self._check(self._lib.b2b_statemon(self._h, gid, N.VARS[var],
+                                           idx.ctypes.data_as(C.POINTER(C.c_int64)), len(idx),
+                                           int(every), int(capacity), C.byref(mid)),
+                    "statemon")
+        self._smons[mid.value] = (len(idx), self._var_dtype(gid, var))
+        return mid.value
+
+    def state_values(self, mid: int) -> tuple[np.ndarray, np.ndarray]:
+        """(steps, values[records, indices]) a state monitor has recorded so far."""
+        width, dt = self._smons[mid]
+        n = C.c_int64()
+        self._check(self._lib.b2b_statemon_get(self._h, mid, C.byref(n), None, None, 0),
+                    "statemon_get")
+        steps = np.empty(n.value, dtype=np.int64)
+        vals = np.empty((n.value, width), dtype=dt)
+        self._check(self._lib.b2b_statemon_get(
+            self._h, mid, C.byref(n), steps.ctypes.data_as(C.POINTER(C.c_int64)),
+            _ptr(vals), len(steps)), "statemon_get")
+        return steps, vals
+
+    def rate_monitor(self, gid: int, capacity: int) -> int:
+        """Brian2's PopulationRateMonitor(G): the group's spike count of every step (rate =
+        count / (N dt)), into a device buffer of `capacity` records."""
+        mid = C.c_int32()
+        self._check(self._lib.b2b_ratemon(self._h, gid, int(capacity), C.byref(mid)), "ratemon")
+        return mid.value
+
+    def rate_counts(self, mid: int) -> tuple[np.ndarray, np.ndarray]:
+        """(steps, spike counts) a rate monitor has recorded so far."""
+        n = C.c_int64()
+        self._check(self._lib.b2b_ratemon_get(self._h, mid, C.byref(n), None, None, 0),
+                    "ratemon_get")
+        steps = np.empty(n.value, dtype=np.int64)
+        counts = np.empty(n.value, dtype=np.int32)
+        self._check(self._lib.b2b_ratemon_get(
+            self._h, mid, C.byref(n), steps.ctypes.data_as(C.POINTER(C.c_int64)),
+            counts.ctypes.data_as(C.POINTER(C.c_int32)), len(steps)), "ratemon_get")
+        return steps, counts
 
     def finalize(self):
         self._check(self._lib.b2b_finalize(self._h), "finalize")

@@ -244,11 +244,13 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
  * network by n_steps with eager launches, timing every launch with a CUDA event pair on the
  * net's stream, and returns per launch site the mean device time of one launch in ms.
- * Sites, in order: one per population (kind 1), one per launch of additive on_pre delivery
- * (kind 6: the additive projections that share a kernel variant are delivered by one launch,
- * with its tuned shape), one per STDP projection's on_pre delivery (kind 2), one per STDP
- * projection's on_post delivery (kind 3), one per population with a deferred reset (kind 4);
- * or, when the net runs one kernel per step (b2b_run_mode 1), that
+ * Sites, in order: the state monitors (kind 9, one launch for all, when there are any), one
+ * per population (kind 1), one per launch of additive on_pre delivery (kind 6: the additive
+ * projections that share a kernel variant are delivered by one launch, with its tuned
+ * shape), one per STDP projection's on_pre delivery (kind 2), one per STDP projection's
+ * on_post delivery (kind 3), one per population with a deferred reset (kind 4), the rate
+ * monitors (kind 10, one launch for all); or, when the net runs one kernel per step
+ * (b2b_run_mode 1), that
  * kernel alone (kind 5); or, for a small network run by one CTA (b2b_run_mode 2), that kernel
  * advancing one step (kind 7).  *n_sites receives the number of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
@@ -305,6 +307,27 @@ b2b_status b2b_spikemon_fetch_population(b2b_net* net, int32_t gid, int64_t star
                                          int64_t* step, int64_t cap);
 /* Index of group gid's first neuron in its population (after b2b_finalize). */
 b2b_status b2b_group_offset(b2b_net* net, int32_t gid, int64_t* offset);
+/* StateMonitor (brian2cuda/templates/statemonitor.cu; Brian2's StateMonitor(G, var,
+ * record=idx, dt=every*dt), when='start'): at the start of every step divisible by `every`,
+ * before any group updates, copies variable `var` of neurons idx[0..n) of group gid into a
+ * device buffer of `capacity` records.  A record is one value per recorded neuron, in the
+ * variable's type (the group's dtype; uint8 for NOT_REFRACTORY).  Records beyond the
+ * capacity are dropped and b2b_sync reports B2B_ERR_QUEUE_OVERFLOW.  Recording appends
+ * across b2b_run calls and b2b_restore, as the spike monitor does.  Before b2b_finalize;
+ * *mid receives the monitor's index. */
+b2b_status b2b_statemon(b2b_net* net, int32_t gid, int32_t var, const int64_t* idx, int64_t n,
+                        int32_t every, int64_t capacity, int32_t* mid);
+/* *n_records receives the number of records so far; the first min(*n_records, cap) are
+ * copied: their steps (int64, may be NULL) and values (cap x n elements, may be NULL). */
+b2b_status b2b_statemon_get(b2b_net* net, int32_t mid, int64_t* n_records, int64_t* steps,
+                            void* values, int64_t cap);
+/* PopulationRateMonitor (templates/ratemonitor.cu): the number of spikes of group gid in
+ * every step, recorded at the end of the step (after synaptic effects and resets, Brian2's
+ * when='end'); the rate is count / (group size * dt).  Capacity and overflow as for
+ * b2b_statemon.  Before b2b_finalize. */
+b2b_status b2b_ratemon(b2b_net* net, int32_t gid, int64_t capacity, int32_t* mid);
+b2b_status b2b_ratemon_get(b2b_net* net, int32_t mid, int64_t* n_records, int64_t* steps,
+                           int32_t* counts, int64_t cap);
 /* Spikes of group gid in the last completed step, sorted ascending (the canonical form of
  * the spikespace, brian2cuda/templates/objects.cu:458-479). */
 b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, int64_t cap);

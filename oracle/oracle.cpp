@@ -137,12 +137,31 @@ struct Syn {
   std::vector<int64_t> post_off, post_syn;
 };
 
+// StateMonitor (brian2cuda/templates/statemonitor.cu: one value per recorded index per tick
+// of the monitor's clock) recording at the start of a step, before the groups update
+// (Brian2's default when='start'), at every step divisible by `every`.
+struct StateMon {
+  int gid = -1, var = 0, every = 1;
+  std::vector<int64_t> idx;
+  std::vector<int64_t> steps;
+  std::vector<double> vals;   // [records][idx]
+};
+// PopulationRateMonitor (templates/ratemonitor.cu): the group's spike count of every step,
+// after the synaptic effects and resets (when='end'); rate = count / (N dt).
+struct RateMon {
+  int gid = -1;
+  std::vector<int64_t> steps;
+  std::vector<int64_t> counts;
+};
+
 template <typename R>
 struct Net {
   double dt;
   int64_t ts = 0;
   std::vector<Group<R>> groups;
   std::vector<Syn<R>> syns;
+  std::vector<StateMon> smons;
+  std::vector<RateMon> rmons;
   bool built = false;
   bool reset_first = false;   // schedule: thresholds, resets, synapses
   std::string err;
@@ -346,6 +365,13 @@ void pathway_post(Net<R>& net, Syn<R>& s, double t) {
 template <typename R>
 bool step(Net<R>& net) {
   const double t = (double)net.ts * net.dt;
+  for (StateMon& m : net.smons) {
+    if (net.ts % m.every != 0) continue;
+    const Group<R>& g = net.groups[m.gid];
+    m.steps.push_back(net.ts);
+    for (int64_t i : m.idx)
+      m.vals.push_back(m.var == NOT_REF ? (double)g.not_ref[i] : (double)g.var[m.var][i]);
+  }
   for (Group<R>& g : net.groups) {
     if (g.kind == LIF) update_lif(g, t, net.dt);
     else if (g.kind == HH) update_hh(g, t, net.dt);
@@ -362,6 +388,10 @@ bool step(Net<R>& net) {
   for (Syn<R>& s : net.syns)
     if (s.effect == STDP) pathway_post(net, s, t);
   if (!net.reset_first) resets();
+  for (RateMon& m : net.rmons) {
+    m.steps.push_back(net.ts);
+    m.counts.push_back((int64_t)net.groups[m.gid].spikes.size());
+  }
   ++net.ts;
   return true;
 }
@@ -731,6 +761,53 @@ int64_t api_spikes(Net<R>& net, int gid, int32_t* idx, int64_t* st, int64_t cap)
   return (int64_t)rec.size();
 }
 
+template <typename R>
+int api_statemon(Net<R>& net, int gid, int var, const int64_t* idx, int64_t n, int every) {
+  if (gid < 0 || gid >= (int)net.groups.size() || var < 0 || var > NOT_REF || every < 1)
+    return -1;
+  StateMon m;
+  m.gid = gid; m.var = var; m.every = every;
+  for (int64_t k = 0; k < n; ++k) {
+    if (idx[k] < 0 || idx[k] >= net.groups[gid].n) return -1;
+    m.idx.push_back(idx[k]);
+  }
+  net.smons.push_back(std::move(m));
+  return (int)net.smons.size() - 1;
+}
+
+template <typename R>
+int64_t api_statemon_get(Net<R>& net, int mid, int64_t* steps, double* vals, int64_t cap) {
+  if (mid < 0 || mid >= (int)net.smons.size()) return -1;
+  const StateMon& m = net.smons[mid];
+  const int64_t n = (int64_t)m.steps.size(), ni = (int64_t)m.idx.size();
+  for (int64_t r = 0; r < n && r < cap; ++r) {
+    if (steps) steps[r] = m.steps[r];
+    if (vals) std::copy(m.vals.begin() + r * ni, m.vals.begin() + (r + 1) * ni, vals + r * ni);
+  }
+  return n;
+}
+
+template <typename R>
+int api_ratemon(Net<R>& net, int gid) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  RateMon m;
+  m.gid = gid;
+  net.rmons.push_back(std::move(m));
+  return (int)net.rmons.size() - 1;
+}
+
+template <typename R>
+int64_t api_ratemon_get(Net<R>& net, int mid, int64_t* steps, int64_t* counts, int64_t cap) {
+  if (mid < 0 || mid >= (int)net.rmons.size()) return -1;
+  const RateMon& m = net.rmons[mid];
+  const int64_t n = (int64_t)m.steps.size();
+  for (int64_t r = 0; r < n && r < cap; ++r) {
+    if (steps) steps[r] = m.steps[r];
+    if (counts) counts[r] = m.counts[r];
+  }
+  return n;
+}
+
 // Bundles still queued after the last step: (offset a >= 1 at which it is delivered, pre,
 // delay), sorted.  Slot (current_offset + a) % num_queues is delivered a steps from now.
 template <typename R>
@@ -864,6 +941,22 @@ int64_t orc_timestep(void* hp) {
 int64_t orc_spikes(void* hp, int gid, int32_t* idx, int64_t* st, int64_t cap) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_spikes, gid, idx, st, cap);
+}
+int orc_statemon(void* hp, int gid, int var, const int64_t* idx, int64_t n, int every) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_statemon, gid, var, idx, n, every);
+}
+int64_t orc_statemon_get(void* hp, int mid, int64_t* steps, double* vals, int64_t cap) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_statemon_get, mid, steps, vals, cap);
+}
+int orc_ratemon(void* hp, int gid) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_ratemon, gid);
+}
+int64_t orc_ratemon_get(void* hp, int mid, int64_t* steps, int64_t* counts, int64_t cap) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_ratemon_get, mid, steps, counts, cap);
 }
 int64_t orc_queue(void* hp, int sid, int32_t* off, int32_t* pre, int32_t* dl, int64_t cap) {
   Handle* h = static_cast<Handle*>(hp);

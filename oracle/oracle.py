@@ -57,6 +57,10 @@ def lib() -> C.CDLL:
             "orc_run": (C.c_int, [P, I64]),
             "orc_timestep": (I64, [P]),
             "orc_spikes": (I64, [P, C.c_int, P, P, I64]),
+            "orc_statemon": (C.c_int, [P, C.c_int, C.c_int, P, I64, C.c_int]),
+            "orc_statemon_get": (I64, [P, C.c_int, P, P, I64]),
+            "orc_ratemon": (C.c_int, [P, C.c_int]),
+            "orc_ratemon_get": (I64, [P, C.c_int, P, P, I64]),
             "orc_queue": (I64, [P, C.c_int, P, P, P, I64]),
             "orc_hines_create": (P, [C.c_int, P, P, P, P, P, P, P, P, D, C.c_int]),
             "orc_hines_destroy": (None, [P]),
@@ -93,6 +97,7 @@ class OracleNet:
                                        (2 if reset_before_synapses else 0))
         self._sizes: list[int] = []
         self._kinds: list[str] = []
+        self._smon_n: dict[int, int] = {}
 
     def close(self):
         if self._h:
@@ -184,6 +189,35 @@ class OracleNet:
     # -- run ------------------------------------------------------------------------------------
     def spike_monitor(self, gid, capacity):
         pass  # the oracle records every spike
+
+    def state_monitor(self, gid, var, indices=None, every=1, capacity=0):
+        idx = (np.arange(self._sizes[gid], dtype=np.int64) if indices is None
+               else np.ascontiguousarray(indices, dtype=np.int64))
+        mid = self._ok(self._lib.orc_statemon(self._h, gid, VARS[var], _p(idx), len(idx),
+                                              int(every)), "state_monitor")
+        self._smon_n[mid] = len(idx)
+        return mid
+
+    def state_values(self, mid):
+        """(steps, values[records, indices]) recorded so far."""
+        n = self._ok(self._lib.orc_statemon_get(self._h, mid, None, None, 0), "state_values")
+        ni = self._smon_n[mid]
+        steps = np.empty(n, dtype=np.int64)
+        vals = np.empty((n, ni), dtype=np.float64)
+        if n:
+            self._lib.orc_statemon_get(self._h, mid, _p(steps), _p(vals), n)
+        return steps, vals
+
+    def rate_monitor(self, gid, capacity=0):
+        return self._ok(self._lib.orc_ratemon(self._h, gid), "rate_monitor")
+
+    def rate_counts(self, mid):
+        n = self._ok(self._lib.orc_ratemon_get(self._h, mid, None, None, 0), "rate_counts")
+        steps = np.empty(n, dtype=np.int64)
+        counts = np.empty(n, dtype=np.int64)
+        if n:
+            self._lib.orc_ratemon_get(self._h, mid, _p(steps), _p(counts), n)
+        return steps, counts
 
     def finalize(self):
         pass

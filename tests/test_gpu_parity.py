@@ -306,6 +306,55 @@ def test_monitor_overflow_is_reported(gpu_factory):
         net.spikes(G)
 
 
+def test_state_and_rate_monitors_match_oracle(gpu_factory, oracle_factory):
+    """StateMonitor (start of the step, every k steps) and PopulationRateMonitor (spike count
+    at the end of the step) against the oracle, across two runs: CUBA 1000 float64, and two
+    groups of one population (the rate monitor of each counts only its own neurons)."""
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        ids = models.build_cuba(net, n=1000, p=0.05, dtype="float64")
+        P = ids["P"]
+        A = net.lif_group(300, models.cuba_lif(), "float64")
+        B = net.lif_group(200, models.cuba_lif(), "float64")
+        rng = np.random.default_rng(4)
+        for G, n in ((A, 300), (B, 200)):
+            net.set_state(G, "v", rng.uniform(-60 * mV, -48 * mV, n))
+        net.synapses(A, B, "ge", np.arange(300, dtype=np.int32) % 200,
+                     np.arange(300, dtype=np.int32) % 200, w_scalar=2 * mV, delay=3)
+        mons = [net.state_monitor(P, "v", [0, 17, 999], every=1, capacity=400),
+                net.state_monitor(P, "ge", None, every=7, capacity=100),
+                net.state_monitor(B, "v", [5, 199], every=3, capacity=100)]
+        rates = [net.rate_monitor(G, capacity=400) for G in (P, A, B)]
+        net.finalize()
+        net.run(120)
+        net.run(130)
+        out[name] = ([net.state_values(m) for m in mons], [net.rate_counts(r) for r in rates])
+    for (gs, gv), (os_, ov) in zip(out["gpu"][0], out["orc"][0]):
+        np.testing.assert_array_equal(gs, os_)
+        assert gv.shape == ov.shape and len(gs) > 0
+        _close(gv, ov, 1e-10, 1e-15)
+    assert list(out["gpu"][0][0][0]) == list(range(250))
+    assert list(out["gpu"][0][1][0]) == list(range(0, 250, 7))
+    for (gs, gc), (os_, oc) in zip(out["gpu"][1], out["orc"][1]):
+        np.testing.assert_array_equal(gs, os_)
+        np.testing.assert_array_equal(gc, oc)
+    assert out["gpu"][1][0][1].sum() > 100 and out["gpu"][1][2][1].sum() > 0
+
+
+def test_state_monitor_overflow_is_reported(gpu_factory):
+    net = gpu_factory(DT)
+    G = net.lif_group(100, models.cuba_lif(), "float64")
+    m = net.state_monitor(G, "v", None, every=1, capacity=10)
+    r = net.rate_monitor(G, capacity=40)
+    net.finalize()
+    net.run(30)
+    assert net.sync() == 3  # B2B_ERR_QUEUE_OVERFLOW
+    steps, vals = net.state_values(m)
+    assert list(steps) == list(range(10)) and vals.shape == (10, 100)
+    assert list(net.rate_counts(r)[0]) == list(range(30))
+
+
 def test_graph_and_eager_agree(gpu_factory):
     res = []
     for graphs in (True, False):
