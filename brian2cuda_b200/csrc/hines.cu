@@ -7,13 +7,22 @@
 // 1>>>` (316-351) and `_currents` (359-387).  One neuron is one code object, so a batch of
 // neurons costs five launches per neuron per step.
 //
-// Here one CTA owns one neuron and keeps its whole morphology (matrix diagonals, state,
+// The method (domain decomposition of the backward-Euler cable equation), restated from the
+// mathematics: compartment j couples to compartment j-1 of its section through the axial
+// conductance g[j] (0 at a section's first compartment), a section's first and last
+// compartments to its start and end nodes through g0 and gn.  Per section, three
+// tridiagonal solves with one matrix give x* (both node voltages 0) and the responses u_start,
+// u_end to a unit voltage at either node, so that v = x* + V_start u_start + V_end u_end;
+// Kirchhoff's current law at the nodes (node 0: the sealed start of the root section, node
+// s+1: the end of section s) gives a tree-shaped system in the node voltages.
+//
+// Here one CTA owns one neuron and keeps its whole morphology (matrix rows, state,
 // per-section and per-node arrays) in shared memory across a chunk of steps; the only
 // global traffic inside the chunk is the soma spike count.  Per step: compartment-parallel
-// channels, section-parallel Thomas solves, node-parallel assembly of the coupling system,
-// then elimination and substitution level by level over the section tree (nodes of equal
-// depth are independent), and a compartment-parallel combine.  The arithmetic of each
-// step follows the reference's formulas term by term.
+// channels, section-parallel tridiagonal solves, node-parallel assembly of the node
+// equations, then elimination (each node pulls in its children) and substitution level by
+// level over the section tree (nodes of equal depth are independent), and a
+// compartment-parallel combination.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,10 +43,14 @@ struct HinesDev {
   const int64_t* comp_off;
   const int32_t* sec_off;
   const int32_t* lvl_base;
-  const double *ab0, *ab1, *ab2;
+  // per compartment: matrix row without the membrane conductance (low couples j to j-1, up
+  // couples j to j+1; both 0 across section boundaries)
+  const double *low, *diag, *up;
   const int32_t* sec_of_comp;
   const int32_t *sec_start, *sec_end, *sec_pnode;
-  const double *invr0, *invrn, *bplus, *bminus;
+  // per section: node couplings, and the right-hand side of the unit-node solves at the
+  // first (-g0/area) and last (-gn/area) compartment
+  const double *g0, *gn, *rhs_first, *rhs_last;
   const int32_t* child_off;   // per node (global node index = sec_off[b] + b + i), global edges
   const int32_t* child_sec;   // neuron-local section index per edge
   const int32_t* level_order; // per node slot: neuron-local node ids sorted by depth
@@ -90,23 +103,23 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
   const int NC = H.nc_max, NS = H.ns_max, NB = H.ns_max + 1;
 
   double* V = reinterpret_cast<double*>(sm);
-  double* RHS = V + NC;
-  double* UP = RHS + NC;
-  double* UM = UP + NC;
-  double* C = UM + NC;
-  double* DIAG = C + NC;
-  double* AB0 = DIAG + NC;
-  double* AB1 = AB0 + NC;
-  double* AB2 = AB1 + NC;
-  double* PD = AB2 + NC;
-  double* PP = PD + NB;
-  double* BB = PP + NB;
-  double* PCH = BB + NB;
-  double* INVR0 = PCH + NS;
-  double* INVRN = INVR0 + NS;
-  double* BPL = INVRN + NS;
-  double* BMI = BPL + NS;
-  RC* M = reinterpret_cast<RC*>(BMI + NS);
+  double* X = V + NC;          // x*, first the right-hand side of the membrane solve
+  double* UE = X + NC;         // u_end
+  double* US = UE + NC;        // u_start
+  double* C = US + NC;         // eliminated super-diagonal
+  double* DG = C + NC;         // diagonal with the membrane conductance of the step
+  double* LOW = DG + NC;
+  double* DIAG0 = LOW + NC;
+  double* UPR = DIAG0 + NC;
+  double* DN = UPR + NC;       // node equations: diagonal,
+  double* TOWARD = DN + NB;    // coefficient of the parent node (node >= 1),
+  double* RHSN = TOWARD + NB;  // right-hand side,
+  double* INTO = RHSN + NB;    // per child edge: coefficient of the child's end node
+  double* G0 = INTO + NS;
+  double* GN = G0 + NS;
+  double* RF = GN + NS;
+  double* RL = RF + NS;
+  RC* M = reinterpret_cast<RC*>(RL + NS);
   RC* Hh = M + NC;
   RC* N = Hh + NC;
   int32_t* SOC = reinterpret_cast<int32_t*>(N + NC);
@@ -123,9 +136,9 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
   const RC* gn = static_cast<const RC*>(H.n);
   for (int j = tid; j < nc; j += bs) {
     V[j] = H.v[c0 + j];
-    AB0[j] = H.ab0[c0 + j];
-    AB1[j] = H.ab1[c0 + j];
-    AB2[j] = H.ab2[c0 + j];
+    LOW[j] = H.low[c0 + j];
+    DIAG0[j] = H.diag[c0 + j];
+    UPR[j] = H.up[c0 + j];
     M[j] = gm[c0 + j];
     Hh[j] = gh[c0 + j];
     N[j] = gn[c0 + j];
@@ -135,10 +148,10 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
     SST[s] = H.sec_start[s0 + s];
     SEN[s] = H.sec_end[s0 + s];
     SPN[s] = H.sec_pnode[s0 + s];
-    INVR0[s] = H.invr0[s0 + s];
-    INVRN[s] = H.invrn[s0 + s];
-    BPL[s] = H.bplus[s0 + s];
-    BMI[s] = H.bminus[s0 + s];
+    G0[s] = H.g0[s0 + s];
+    GN[s] = H.gn[s0 + s];
+    RF[s] = H.rhs_first[s0 + s];
+    RL[s] = H.rhs_last[s0 + s];
   }
   const int e0 = H.child_off[nb0];
   for (int i = tid; i <= nB; i += bs) COFF[i] = H.child_off[nb0 + i] - e0;
@@ -164,102 +177,97 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
       const double gtot = H.gl + gna + gk;
       double I0 = H.gl * H.El + gna * H.ENa + gk * H.EK;
       if (j == 0) I0 += Isoma;
-      DIAG[j] = AB1[j] - gtot;
-      RHS[j] = -cdt * v - I0;
+      DG[j] = DIAG0[j] - gtot;
+      X[j] = -cdt * v - I0;
       hh_gates<RC>((RC)v, dtR, m, h, n);
       M[j] = m;
       Hh[j] = h;
       N[j] = n;
     }
     __syncthreads();
-    // (2) Thomas solve of each section for v*, u+ and u-
+    // (2) per section, one pass of forward elimination (reciprocal pivot) and back
+    // substitution for the three right-hand sides
     for (int s = tid; s < ns; s += bs) {
       const int j0 = SST[s], j1 = SEN[s];
+      double cprev = 0.0, xprev = 0.0, sprev = 0.0, eprev = 0.0;
       for (int j = j0; j < j1; ++j) {
-        const double bi = DIAG[j];
-        const double cj = (j + 1 < j1) ? AB0[j + 1] : 0.0;
-        const double vs = RHS[j];
-        const double upj = (j == j1 - 1) ? BPL[s] : 0.0;
-        const double umj = (j == j0) ? BMI[s] : 0.0;
-        if (j == 0) {
-          C[j] = cj / bi; RHS[j] = vs / bi; UP[j] = upj / bi; UM[j] = umj / bi;
-        } else if (j == j0) {
-          const double mm = 1.0 / bi;
-          C[j] = cj * mm; RHS[j] = vs * mm; UP[j] = upj * mm; UM[j] = umj * mm;
-        } else {
-          const double ai = AB2[j - 1];
-          const double mm = 1.0 / (bi - ai * C[j - 1]);
-          C[j] = cj * mm;
-          RHS[j] = (vs - ai * RHS[j - 1]) * mm;
-          UP[j] = (upj - ai * UP[j - 1]) * mm;
-          UM[j] = (umj - ai * UM[j - 1]) * mm;
-        }
+        const double lw = j > j0 ? LOW[j] : 0.0;
+        const double piv = 1.0 / (DG[j] - lw * cprev);
+        C[j] = UPR[j] * piv;
+        X[j] = (X[j] - lw * xprev) * piv;
+        US[j] = ((j == j0 ? RF[s] : 0.0) - lw * sprev) * piv;
+        UE[j] = ((j == j1 - 1 ? RL[s] : 0.0) - lw * eprev) * piv;
+        cprev = C[j];
+        xprev = X[j];
+        sprev = US[j];
+        eprev = UE[j];
       }
       for (int j = j1 - 2; j >= j0; --j) {
-        RHS[j] = RHS[j] - C[j] * RHS[j + 1];
-        UP[j] = UP[j] - C[j] * UP[j + 1];
-        UM[j] = UM[j] - C[j] * UM[j + 1];
+        X[j] -= C[j] * X[j + 1];
+        US[j] -= C[j] * US[j + 1];
+        UE[j] -= C[j] * UE[j + 1];
       }
     }
     __syncthreads();
-    // (3) coupling system, one row per node
+    // (3) node equations: node i's current balance in its own voltage (DN), its parent
+    // node's (TOWARD) and its children's end nodes' (INTO, per edge)
     for (int i = tid; i < nB; i += bs) {
-      double pd, bb;
+      double dn, rh;
       if (i == 0) {
+        // the root's start takes the voltage of the root's first compartment
         const int f = SST[0];
-        pd = UM[f] - 1.0;
-        bb = -RHS[f];
-        PCH[COFF[0]] = UP[f];
+        dn = US[f] - 1.0;
+        rh = -X[f];
+        INTO[COFF[0]] = UE[f];
       } else {
         const int s = i - 1;
-        const int last = SEN[s] - 1;
-        pd = (1.0 - UP[last]) * INVRN[s];
-        PP[s] = -UM[last] * INVRN[s];
-        bb = RHS[last] * INVRN[s];
+        const int l = SEN[s] - 1;
+        dn = GN[s] * (1.0 - UE[l]);
+        TOWARD[i] = -GN[s] * US[l];
+        rh = GN[s] * X[l];
         for (int e = COFF[i]; e < COFF[i + 1]; ++e) {
           const int cs = CSEC[e];
           const int f = SST[cs];
-          pd += (1.0 - UM[f]) * INVR0[cs];
-          PCH[e] = -UP[f] * INVR0[cs];
-          bb += RHS[f] * INVR0[cs];
+          dn += G0[cs] * (1.0 - US[f]);
+          INTO[e] = -G0[cs] * UE[f];
+          rh += G0[cs] * X[f];
         }
       }
-      PD[i] = pd;
-      BB[i] = bb;
+      DN[i] = dn;
+      RHSN[i] = rh;
     }
     __syncthreads();
-    // (4) elimination, deepest level first
+    // (4) elimination, deepest level first: each node takes in its children's equations
     for (int L = nlev - 1; L >= 0; --L) {
       for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += bs) {
         const int i = LORD[k];
-        double pd = PD[i], bb = BB[i];
+        double dn = DN[i], rh = RHSN[i];
         for (int e = COFF[i]; e < COFF[i + 1]; ++e) {
-          const int j = CSEC[e] + 1;
-          const double sub = PCH[e] / PD[j];
-          pd = pd - sub * PP[j - 1];
-          bb = bb - sub * BB[j];
+          const int c = CSEC[e] + 1;   // the child section's end node
+          const double f = INTO[e] / DN[c];
+          dn -= f * TOWARD[c];
+          rh -= f * RHSN[c];
         }
-        PD[i] = pd;
-        BB[i] = bb;
+        DN[i] = dn;
+        RHSN[i] = rh;
       }
       __syncthreads();
     }
-    // (5) substitution, root first
-    if (tid == 0) BB[0] = BB[0] / PD[0];
+    // (5) substitution, root first: RHSN becomes the node voltage
+    if (tid == 0) RHSN[0] = RHSN[0] / DN[0];
     __syncthreads();
     for (int L = 1; L < nlev; ++L) {
       for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += bs) {
         const int i = LORD[k];
-        const int j = SPN[i - 1];
-        BB[i] = (BB[i] - PP[i - 1] * BB[j]) / PD[i];
+        RHSN[i] = (RHSN[i] - TOWARD[i] * RHSN[SPN[i - 1]]) / DN[i];
       }
       __syncthreads();
     }
-    // (6) combine the particular and homogeneous solutions; capacitive current
+    // (6) v = x* + V_start u_start + V_end u_end; capacitive current
     const bool last_step = step == n_steps - 1;
     for (int j = tid; j < nc; j += bs) {
       const int s = SOC[j];
-      const double vn = RHS[j] + BB[SPN[s]] * UM[j] + BB[s + 1] * UP[j];
+      const double vn = X[j] + RHSN[SPN[s]] * US[j] + RHSN[s + 1] * UE[j];
       if (last_step && write_currents) H.Ic[c0 + j] = H.Cm * (vn - V[j]) / H.dt;
       V[j] = vn;
     }
@@ -342,11 +350,12 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     if (comp_off[0] != 0 || sec_off[0] != 0) return B2B_ERR_INVALID_ARG;
     const int64_t n_comp = comp_off[n_neurons];
     const int32_t n_sec = sec_off[n_neurons];
-    std::vector<double> ab0(n_comp, 0.0), ab1(n_comp, 0.0), ab2(n_comp, 0.0);
+    std::vector<double> low(n_comp, 0.0), diag(n_comp, 0.0), upr(n_comp, 0.0);
     std::vector<int32_t> soc(n_comp), sst(n_sec), sen(n_sec), spn(n_sec);
-    std::vector<double> invr0(n_sec), invrn(n_sec), bpl(n_sec), bmi(n_sec);
+    std::vector<double> g0(n_sec), gn(n_sec), rfirst(n_sec), rlast(n_sec);
     std::vector<int32_t> child_off, child_sec, level_order, level_off, lvl_base;
-    std::vector<double> area(n_comp), rl(n_comp), invr(n_comp, 0.0);
+    // r: cross section over half the length; g: axial conductance into c from c - 1
+    std::vector<double> area(n_comp), rl(n_comp), g(n_comp + 1, 0.0);
     std::vector<double> soma_area(n_neurons);
     int nc_max = 0, ns_max = 0, nlev_max = 0;
     const double Ri = p->Ri, Cm = p->Cm;
@@ -371,25 +380,26 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
         rl[c] = M_PI * diameter[c] * diameter[c] / (2.0 * length[c]);
       }
       soma_area[b] = area[c0];
-      // matrix (brian2cuda/templates/spatialstateupdate.cu:36-77, neuron-local indices)
-      for (int64_t c = c0 + 1; c < c1; ++c) invr[c] = 1.0 / (Ri * (1.0 / rl[c - 1] + 1.0 / rl[c]));
-      for (int s = 0; s < ns; ++s) invr[c0 + sec_start[s0 + s]] = 0.0;
-      for (int64_t c = c0; c < c1; ++c) ab1[c] = (-(Cm / dt) - invr[c] / area[c]);
-      for (int64_t c = c0 + 1; c < c1; ++c) {
-        ab0[c] = invr[c] / area[c - 1];
-        ab2[c - 1] = invr[c] / area[c];
-        ab1[c - 1] -= invr[c] / area[c - 1];
+      // matrix rows (the cable matrix of spatialstateupdate.cu:36-77)
+      std::vector<char> first_of_sec(nc, 0);
+      for (int s = 0; s < ns; ++s) first_of_sec[sec_start[s0 + s]] = 1;
+      for (int64_t c = c0; c < c1; ++c)
+        g[c] = first_of_sec[c - c0] ? 0.0 : 1.0 / (Ri * (1.0 / rl[c - 1] + 1.0 / rl[c]));
+      g[c1] = 0.0;
+      for (int64_t c = c0; c < c1; ++c) {
+        low[c] = g[c] / area[c];
+        upr[c] = g[c + 1] / area[c];
+        diag[c] = -(Cm / dt) - (g[c] + g[c + 1]) / area[c];
       }
       for (int s = 0; s < ns; ++s) {
         const int64_t first = c0 + sec_start[s0 + s];
         const int64_t last = c0 + sec_end[s0 + s] - 1;
-        const double i0 = rl[first] / Ri, in = rl[last] / Ri;
-        invr0[s0 + s] = i0;
-        invrn[s0 + s] = in;
-        ab1[first] -= (i0 / area[first]);
-        ab1[last] -= (in / area[last]);
-        bpl[s0 + s] = -(in / area[last]);
-        bmi[s0 + s] = -(i0 / area[first]);
+        g0[s0 + s] = rl[first] / Ri;
+        gn[s0 + s] = rl[last] / Ri;
+        diag[first] -= g0[s0 + s] / area[first];
+        diag[last] -= gn[s0 + s] / area[last];
+        rfirst[s0 + s] = -g0[s0 + s] / area[first];
+        rlast[s0 + s] = -gn[s0 + s] / area[last];
         sst[s0 + s] = sec_start[s0 + s];
         sen[s0 + s] = sec_end[s0 + s];
         spn[s0 + s] = s == 0 ? 0 : sec_parent[s0 + s] + 1;
@@ -451,9 +461,9 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       if (e == cudaSuccess) e = upload(h, dst, src);
     };
     up(&D.comp_off, co); up(&D.sec_off, so); up(&D.lvl_base, lvl_base);
-    up(&D.ab0, ab0); up(&D.ab1, ab1); up(&D.ab2, ab2); up(&D.sec_of_comp, soc);
+    up(&D.low, low); up(&D.diag, diag); up(&D.up, upr); up(&D.sec_of_comp, soc);
     up(&D.sec_start, sst); up(&D.sec_end, sen); up(&D.sec_pnode, spn);
-    up(&D.invr0, invr0); up(&D.invrn, invrn); up(&D.bplus, bpl); up(&D.bminus, bmi);
+    up(&D.g0, g0); up(&D.gn, gn); up(&D.rhs_first, rfirst); up(&D.rhs_last, rlast);
     up(&D.child_off, child_off); up(&D.child_sec, child_sec);
     up(&D.level_order, level_order); up(&D.level_off, level_off);
     std::vector<double> zeros_d(n_comp, 0.0), zero_I(n_neurons, 0.0);

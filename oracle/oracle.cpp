@@ -29,8 +29,10 @@
 //     their removable singularity finite (the literal form is 0/0 there).
 //   * Event-driven STDP (examples/stdp.py:125-186) with float32 elapsed time in float32
 //     mode (brian2cuda/device.py:1034-1039); clip as cuda_generator.py:902-914.
-//   * Hines solver: brian2cuda/templates/spatialstateupdate.cu:36-77 (matrix), 128-192
-//     (Thomas), 202-307 (coupling), 316-351 (combine), 359-387 (currents), literally.
+//   * Hines solver: the domain-decomposition method of brian2cuda/templates/
+//     spatialstateupdate.cu (matrix 36-77, per-section solves 128-192, branch-point system
+//     202-307, combination 316-351, currents 359-387), restated from the cable equation
+//     (see the Hines section below).
 //   * Philox-4x32-10 connectivity generation restated from Salmon et al., SC 2011.
 //
 // Arithmetic: R = double (reference mode) or float (same-precision mode).
@@ -413,16 +415,36 @@ void ensure_built(Net<R>& net) {
   net.built = true;
 }
 
-// ---- Hines (SpatialNeuron), literal restatement of spatialstateupdate.cu ----------------------
+// ---- Hines (SpatialNeuron) --------------------------------------------------------------------
+// Backward-Euler step of the cable equation of a branched neuron, solved by domain
+// decomposition: the method of brian2cuda/templates/spatialstateupdate.cu (matrix 18-93,
+// per-section solves 128-192, branch-point system 202-307, combination 316-351), restated
+// here from the mathematics.
+//  - Compartment j of a neuron couples to compartment j-1 of the same section through the
+//    axial conductance g[j] = 1 / (Ri (1/r_end[j-1] + 1/r_start[j])) (r: cross section over
+//    half length); g is 0 at the first compartment of every section.  A section's first
+//    compartment couples to the section's start node through g0 = r_start/Ri, its last one
+//    to its end node through gn = r_end/Ri.
+//  - Per section: three tridiagonal solves with the same matrix, x* for the membrane
+//    equation with both node voltages 0, u_start and u_end with a unit voltage at one node.
+//    Any solution of the section is v = x* + V_start u_start + V_end u_end.
+//  - Node 0 is the start of the root section (sealed: its voltage is that of the first
+//    compartment); node k+1 is the end of section k, where its child sections start.
+//    Kirchhoff's current law at every node gives one equation per node in the node voltages;
+//    the system is a tree (a node couples to its parent node and to its children's end
+//    nodes), eliminated from the leaves to the root and then substituted back.  Sections are
+//    numbered so that a parent precedes its children.
 template <typename RC>
 struct Hines {
   int nn = 0;
   std::vector<int64_t> comp_off;
   std::vector<int32_t> sec_off, starts, ends, parent;   // starts/ends neuron-local
-  std::vector<double> area, rl1, rl2;
+  std::vector<double> area, r_start, r_end;             // per compartment
   double Cm, Ri, El, EK, ENa, gl, gNa, gK, Vthr, dt;
-  // prepared matrix (per neuron, neuron-local indices into the flat arrays)
-  std::vector<double> invr, ab0, ab1, ab2, bplus, bminus, invr0, invrn;
+  // per compartment: matrix row without the membrane conductance (low couples j to j-1,
+  // up couples j to j+1), and the right-hand sides of the two unit-node solves
+  std::vector<double> low, diag, up, rhs_start, rhs_end;
+  std::vector<double> g0, gn;                           // per section: node couplings
   std::vector<double> v, Ic, soma_I;
   std::vector<RC> m, h, n;
   std::vector<int32_t> spikes, above;
@@ -431,39 +453,30 @@ struct Hines {
 template <typename RC>
 void hines_prepare(Hines<RC>& H) {
   const int64_t NC = H.comp_off[H.nn];
-  H.invr.assign(NC, 0); H.ab0.assign(NC, 0); H.ab1.assign(NC, 0); H.ab2.assign(NC, 0);
-  H.bplus.assign(NC, 0); H.bminus.assign(NC, 0);
-  H.invr0.assign(H.sec_off[H.nn], 0); H.invrn.assign(H.sec_off[H.nn], 0);
+  H.low.assign(NC, 0); H.diag.assign(NC, 0); H.up.assign(NC, 0);
+  H.rhs_start.assign(NC, 0); H.rhs_end.assign(NC, 0);
+  H.g0.assign(H.sec_off[H.nn], 0); H.gn.assign(H.sec_off[H.nn], 0);
+  std::vector<double> g(NC + 1, 0.0);   // axial conductance into compartment j from j-1
   for (int b = 0; b < H.nn; ++b) {
-    const int64_t c0 = H.comp_off[b];
-    const int _N = (int)(H.comp_off[b + 1] - c0);
-    double* invr = &H.invr[c0];
-    double* a0 = &H.ab0[c0];
-    double* a1 = &H.ab1[c0];
-    double* a2 = &H.ab2[c0];
-    const double* area = &H.area[c0];
-    const double* r1 = &H.rl1[c0];
-    const double* r2 = &H.rl2[c0];
-    const int s0 = H.sec_off[b], ns = H.sec_off[b + 1] - s0;
-    for (int _i = 1; _i < _N; _i++) invr[_i] = 1.0 / (H.Ri * (1 / r2[_i - 1] + 1 / r1[_i]));
-    for (int _i = 0; _i < ns; _i++) invr[H.starts[s0 + _i]] = 0;
-    for (int _i = 0; _i < _N; _i++) a1[_i] = (-(H.Cm / H.dt) - invr[_i] / area[_i]);
-    for (int _i = 1; _i < _N; _i++) {
-      a0[_i] = invr[_i] / area[_i - 1];
-      a2[_i - 1] = invr[_i] / area[_i];
-      a1[_i - 1] -= invr[_i] / area[_i - 1];
+    const int64_t c0 = H.comp_off[b], c1 = H.comp_off[b + 1];
+    std::vector<char> first(c1 - c0, 0);
+    for (int k = H.sec_off[b]; k < H.sec_off[b + 1]; ++k) first[H.starts[k]] = 1;
+    for (int64_t j = c0; j < c1; ++j)
+      g[j] = first[j - c0] ? 0.0 : 1.0 / (H.Ri * (1.0 / H.r_end[j - 1] + 1.0 / H.r_start[j]));
+    g[c1] = 0.0;
+    for (int64_t j = c0; j < c1; ++j) {
+      H.low[j] = g[j] / H.area[j];
+      H.up[j] = g[j + 1] / H.area[j];
+      H.diag[j] = -(H.Cm / H.dt) - (g[j] + g[j + 1]) / H.area[j];
     }
-    for (int c = 0; c < ns; c++) {
-      const int first = H.starts[s0 + c];
-      const int last = H.ends[s0 + c] - 1;
-      const double i0 = r1[first] / H.Ri;
-      const double in = r2[last] / H.Ri;
-      H.invr0[s0 + c] = i0;
-      H.invrn[s0 + c] = in;
-      a1[first] -= (i0 / area[first]);
-      a1[last] -= (in / area[last]);
-      H.bplus[c0 + last] = -(in / area[last]);
-      H.bminus[c0 + first] = -(i0 / area[first]);
+    for (int k = H.sec_off[b]; k < H.sec_off[b + 1]; ++k) {
+      const int64_t f = c0 + H.starts[k], l = c0 + H.ends[k] - 1;
+      H.g0[k] = H.r_start[f] / H.Ri;
+      H.gn[k] = H.r_end[l] / H.Ri;
+      H.diag[f] -= H.g0[k] / H.area[f];
+      H.diag[l] -= H.gn[k] / H.area[l];
+      H.rhs_start[f] = -H.g0[k] / H.area[f];
+      H.rhs_end[l] = -H.gn[k] / H.area[l];
     }
   }
 }
@@ -480,12 +493,12 @@ void hines_step(Hines<RC>& H, bool write_currents) {
 #pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < H.nn; ++b) {
     const int64_t c0 = H.comp_off[b];
-    const int _N = (int)(H.comp_off[b + 1] - c0);
+    const int nc = (int)(H.comp_off[b + 1] - c0);
     const int s0 = H.sec_off[b], ns = H.sec_off[b + 1] - s0;
-    std::vector<double> gtot(_N), I0(_N), vprev(_N), vstar(_N), up(_N), um(_N), c(_N);
+    std::vector<double> gtot(nc), I0(nc), vprev(nc), xs(nc), us(nc), ue(nc), c(nc);
     double* v = &H.v[c0];
-    // kernel 1: conductance/current from the state at the start of the step, then gates
-    for (int j = 0; j < _N; ++j) {
+    // membrane conductance and current from the state at the start of the step, then gates
+    for (int j = 0; j < nc; ++j) {
       const double md = (double)H.m[c0 + j], hd = (double)H.h[c0 + j], nd = (double)H.n[c0 + j];
       const double gna = H.gNa * (md * md * md * hd);
       const double gk = H.gK * (nd * nd * nd * nd);
@@ -504,95 +517,73 @@ void hines_step(Hines<RC>& H, bool write_currents) {
       H.h[c0 + j] = hh_ee(H.h[c0 + j], ah, bh, dtR);
       H.n[c0 + j] = hh_ee(H.n[c0 + j], an, bn, dtR);
     }
-    const double* ab0 = &H.ab0[c0];
-    const double* ab1 = &H.ab1[c0];
-    const double* ab2 = &H.ab2[c0];
-    const double* bp = &H.bplus[c0];
-    const double* bmn = &H.bminus[c0];
-    // kernel 2: Thomas for each section (spatialstateupdate.cu:128-192)
-    for (int _i = 0; _i < ns; ++_i) {
-      const int _j_start = H.starts[s0 + _i], _j_end = H.ends[s0 + _i];
-      double _ai, _bi, _m;
-      for (int _j = _j_start; _j < _j_end; _j++) {
-        vstar[_j] = -(H.Cm / H.dt * v[_j]) - I0[_j];
-        up[_j] = bp[_j];
-        um[_j] = bmn[_j];
-        _bi = ab1[_j] - gtot[_j];
-        if (_j < _N - 1) c[_j] = ab0[_j + 1];
-        if (_j > 0) {
-          _ai = ab2[_j - 1];
-          _m = 1.0 / (_bi - _ai * c[_j - 1]);
-          c[_j] = c[_j] * _m;
-          vstar[_j] = (vstar[_j] - _ai * vstar[_j - 1]) * _m;
-          up[_j] = (up[_j] - _ai * up[_j - 1]) * _m;
-          um[_j] = (um[_j] - _ai * um[_j - 1]) * _m;
-        } else {
-          c[0] = c[0] / _bi;
-          vstar[0] = vstar[0] / _bi;
-          up[0] = up[0] / _bi;
-          um[0] = um[0] / _bi;
-        }
+    // per section: one Thomas pass (forward elimination with the reciprocal pivot, then
+    // back substitution) for the three right-hand sides x*, u_start, u_end
+    for (int k = 0; k < ns; ++k) {
+      const int lo = H.starts[s0 + k], hi = H.ends[s0 + k];
+      double cprev = 0.0;
+      for (int j = lo; j < hi; ++j) {
+        const int64_t q = c0 + j;
+        const double lw = j > lo ? H.low[q] : 0.0;
+        const double piv = 1.0 / (H.diag[q] - gtot[j] - lw * cprev);
+        c[j] = H.up[q] * piv;
+        xs[j] = (-(H.Cm / H.dt) * v[j] - I0[j] - (j > lo ? lw * xs[j - 1] : 0.0)) * piv;
+        us[j] = (H.rhs_start[q] - (j > lo ? lw * us[j - 1] : 0.0)) * piv;
+        ue[j] = (H.rhs_end[q] - (j > lo ? lw * ue[j - 1] : 0.0)) * piv;
+        cprev = c[j];
       }
-      for (int _j = _j_end - 2; _j >= _j_start; _j--) {
-        vstar[_j] = vstar[_j] - c[_j] * vstar[_j + 1];
-        up[_j] = up[_j] - c[_j] * up[_j + 1];
-        um[_j] = um[_j] - c[_j] * um[_j + 1];
+      for (int j = hi - 2; j >= lo; --j) {
+        xs[j] -= c[j] * xs[j + 1];
+        us[j] -= c[j] * us[j + 1];
+        ue[j] -= c[j] * ue[j + 1];
       }
     }
-    // kernel 3: coupling (spatialstateupdate.cu:202-307); node i+1 = end of section i
-    const int nB = ns + 1;
-    std::vector<int> parent_i(ns), nchild(nB, 0), idxchild(ns, 0);
-    std::vector<std::vector<int>> children(nB);
-    for (int i = 0; i < ns; ++i) parent_i[i] = i == 0 ? 0 : H.parent[s0 + i] + 1;
-    for (int i = 0; i < ns; ++i) {
-      idxchild[i] = (int)children[parent_i[i]].size();
-      children[parent_i[i]].push_back(i + 1);
-    }
-    std::vector<double> Pd(nB, 0), Pp(ns, 0), B(nB, 0);
-    std::vector<std::vector<double>> Pc(nB);
-    for (int i = 0; i < nB; ++i) Pc[i].assign(children[i].size(), 0.0);
-    for (int _i = 0; _i < nB - 1; _i++) {
-      const int _i_parent = parent_i[_i];
-      const int _i_childind = idxchild[_i];
-      const int _first = H.starts[s0 + _i];
-      const int _last = H.ends[s0 + _i] - 1;
-      const double _invr0 = H.invr0[s0 + _i];
-      const double _invrn = H.invrn[s0 + _i];
-      if (_i == 0) {
-        Pd[0] = um[_first] - 1;
-        Pc[0][0] = up[_first];
-        B[0] = -vstar[_first];
+    // node system: node n's equation D[n] V_n + toward_parent[n] V_parent(n)
+    // + sum over child nodes c of into_parent[c] V_c = rhs[n]
+    const int nodes = ns + 1;
+    std::vector<int> parent_node(nodes, -1);
+    std::vector<double> D(nodes, 0.0), rhs(nodes, 0.0), toward_parent(nodes, 0.0),
+        into_parent(nodes, 0.0), V(nodes, 0.0);
+    auto start_node = [&](int k) { return k == 0 ? 0 : H.parent[s0 + k] + 1; };
+    for (int k = 0; k < ns; ++k) {
+      const int f = H.starts[s0 + k], l = H.ends[s0 + k] - 1;
+      const int sn = start_node(k), en = k + 1;
+      const double g0 = H.g0[s0 + k], gn = H.gn[s0 + k];
+      parent_node[en] = sn;
+      // end node: current from the section's last compartment
+      D[en] += gn * (1.0 - ue[l]);
+      toward_parent[en] = -gn * us[l];
+      rhs[en] += gn * xs[l];
+      if (k == 0) {
+        // node 0 takes the voltage of the root's first compartment
+        D[0] = us[f] - 1.0;
+        into_parent[en] = ue[f];
+        rhs[0] = -xs[f];
       } else {
-        Pd[_i_parent] += (1 - um[_first]) * _invr0;
-        Pc[_i_parent][_i_childind] = -up[_first] * _invr0;
-        B[_i_parent] += vstar[_first] * _invr0;
-      }
-      Pd[_i + 1] = (1 - up[_last]) * _invrn;
-      Pp[_i] = -um[_last] * _invrn;
-      B[_i + 1] = vstar[_last] * _invrn;
-    }
-    for (int _i = nB - 1; _i >= 0; _i--) {
-      for (size_t _k = 0; _k < children[_i].size(); _k++) {
-        const int _j = children[_i][_k];
-        const double _subfac = Pc[_i][_k] / Pd[_j];
-        Pd[_i] = Pd[_i] - _subfac * Pp[_j - 1];
-        B[_i] = B[_i] - _subfac * B[_j];
+        // start node: current into the section's first compartment
+        D[sn] += g0 * (1.0 - us[f]);
+        into_parent[en] = -g0 * ue[f];
+        rhs[sn] += g0 * xs[f];
       }
     }
-    B[0] = B[0] / Pd[0];
-    for (int _i = 1; _i < nB; _i++) {
-      const int _j = parent_i[_i - 1];
-      B[_i] = B[_i] - Pp[_i - 1] * B[_j];
-      B[_i] = B[_i] / Pd[_i];
-    }
-    // kernel 4: combine; kernel 5: currents
-    for (int _i = 0; _i < ns; ++_i) {
-      const int _i_parent = parent_i[_i];
-      for (int _j = H.starts[s0 + _i]; _j < H.ends[s0 + _i]; _j++)
-        v[_j] = vstar[_j] + B[_i_parent] * um[_j] + B[_i + 1] * up[_j];
-    }
+    // elimination from the leaves: a node's children have larger numbers, so going down
+    // from the last node every child is complete when its parent takes it in
+    std::vector<std::vector<int>> child_nodes(nodes);
+    for (int nd = 1; nd < nodes; ++nd) child_nodes[parent_node[nd]].push_back(nd);
+    for (int p = nodes - 1; p >= 0; --p)
+      for (int nd : child_nodes[p]) {
+        const double f = into_parent[nd] / D[nd];
+        D[p] -= f * toward_parent[nd];
+        rhs[p] -= f * rhs[nd];
+      }
+    V[0] = rhs[0] / D[0];
+    for (int nd = 1; nd < nodes; ++nd)
+      V[nd] = (rhs[nd] - toward_parent[nd] * V[parent_node[nd]]) / D[nd];
+    for (int k = 0; k < ns; ++k)
+      for (int j = H.starts[s0 + k]; j < H.ends[s0 + k]; ++j)
+        v[j] = xs[j] + V[start_node(k)] * us[j] + V[k + 1] * ue[j];
     if (write_currents)
-      for (int j = 0; j < _N; ++j) H.Ic[c0 + j] = H.Cm * (v[j] - vprev[j]) / H.dt;
+      for (int j = 0; j < nc; ++j) H.Ic[c0 + j] = H.Cm * (v[j] - vprev[j]) / H.dt;
     const int ab = v[0] > H.Vthr ? 1 : 0;
     if (ab && !H.above[b]) H.spikes[b]++;
     H.above[b] = ab;
@@ -848,10 +839,11 @@ void hines_init(Hines<RC>& H, int nn, const int64_t* comp_off, const int32_t* se
   H.starts.assign(st, st + S);
   H.ends.assign(en, en + S);
   H.parent.assign(par, par + S);
-  H.area.resize(C); H.rl1.resize(C); H.rl2.resize(C);
+  H.area.resize(C); H.r_start.resize(C); H.r_end.resize(C);
   for (int64_t c = 0; c < C; ++c) {
     H.area[c] = M_PI * d[c] * L[c];
-    H.rl1[c] = H.rl2[c] = M_PI * d[c] * d[c] / (2.0 * L[c]);
+    // cross section over half the length, towards either end of a cylinder
+    H.r_start[c] = H.r_end[c] = M_PI * d[c] * d[c] / (2.0 * L[c]);
   }
   H.Cm = p[0]; H.Ri = p[1]; H.El = p[2]; H.EK = p[3]; H.ENa = p[4]; H.gl = p[5]; H.gNa = p[6];
   H.gK = p[7]; H.Vthr = p[8]; H.dt = dt;
