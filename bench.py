@@ -435,14 +435,18 @@ BATCH_WORKLOAD = ("256 COBAHH instances, sizes round(exp(U[ln 1e3, ln 6.4e4])) (
 SURR_TOL = 1e-3
 
 
-def _spike_match(a, b):
-    """Fraction of spikes (neuron, step) of a that b has within one step."""
+def _spike_hits(a, b):
+    """(spikes (neuron, step) of a that b has within one step, spikes of a)."""
     keys = set(zip(b[0].tolist(), b[1].tolist()))
-    if len(a[0]) == 0:
-        return 1.0
     hit = sum(1 for i, t in zip(a[0].tolist(), a[1].tolist())
               if (i, t) in keys or (i, t - 1) in keys or (i, t + 1) in keys)
-    return hit / len(a[0])
+    return hit, len(a[0])
+
+
+def _spike_match(a, b):
+    """Fraction of spikes (neuron, step) of a that b has within one step."""
+    hit, n = _spike_hits(a, b)
+    return hit / n if n else 1.0
 
 
 def bench_batched(args, world, rank, local):
@@ -544,15 +548,25 @@ def bench_batched(args, world, rank, local):
     t = gating_targets(models.cobahh_hh(), DT, x)
     surr = GatingSurrogate(device=local, seed=3)
     t0 = time.perf_counter()
-    losses = surr.fit(x, t, epochs=100, batch=32768, lr=1e-2)
+    losses = surr.fit(x, t, epochs=400, batch=32768, lr=3e-3)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     del x, t
     snet, sids = build(surr, judge=True, mon_entries=int(n_total * 300 * DT * 200.0))
     snet.run(300)
     s_ras = {g: snet.spikes(g) for g in sids["groups"][-16:]}
-    match = min(_spike_match(ref_ras[g], s_ras[g2]) for g, g2 in zip(ref_ras, s_ras))
-    match = 1.0 - max_over_ranks(1.0 - match, world)
+    # pooled over the instances, in both directions (exact spikes the surrogate run has, and
+    # surrogate spikes the exact run has), and the worst single instance
+    hits = np.zeros((2, 2))
+    worst = 1.0
+    for g, g2 in zip(ref_ras, s_ras):
+        for d, (a, b) in enumerate(((ref_ras[g], s_ras[g2]), (s_ras[g2], ref_ras[g]))):
+            h, n = _spike_hits(a, b)
+            hits[d] += (h, n)
+            worst = min(worst, h / n if n else 1.0)
+    hits = np.array([[sum_over_ranks(float(v), world) for v in row] for row in hits])
+    match = float(min(hits[0, 0] / max(1.0, hits[0, 1]), hits[1, 0] / max(1.0, hits[1, 1])))
+    worst = 1.0 - max_over_ranks(1.0 - worst, world)
     snet.restore(0)
     u0, f0 = surrogate_stats(snet, sids["groups"][0])
     s_ms, _ = timed(snet, args.steps)
@@ -598,8 +612,11 @@ def bench_batched(args, world, rank, local):
                       "vs_batched_exact": surr_value / value, "tol": SURR_TOL, "judge": True,
                       "fallback_frac": f_all / max(1.0, u_all),
                       "raster_match_within_1dt_300_steps_last_16_instances": match,
+                      "raster_match_worst_instance": worst,
+                      "raster_spikes_exact": hits[0, 1],
                       "train_s": train_s, "train_loss": losses[-1],
-                      "dataset": "1e7 exact transitions from the batched net's trajectories"},
+                      "dataset": "1e7 exact transitions from the batched net's trajectories",
+                      "training": "400 epochs, batch 32768, Adam lr 3e-3 with cosine decay"},
         "batched_vs_plain": value / plain_value,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": _traffic_lookup("hh_stream_kernel"),

@@ -130,7 +130,7 @@ class GatingSurrogate:
                                        int(epochs), int(batch), float(lr), losses), "mlp_train")
         return [losses[i] for i in range(epochs)]
 
-    def fit(self, x, t, epochs: int = 300, batch: int = 32768, lr: float = 1e-2,
+    def fit(self, x, t, epochs: int = 400, batch: int = 32768, lr: float = 3e-3,
             out_scale: float = 0.01) -> list[float]:
         """The training recipe: input scaling from the data, one output scale for all gates
         (it weights the loss towards absolute gate error, which the fallback bound tests),
