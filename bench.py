@@ -221,7 +221,7 @@ def main():
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
                     choices=["hh4m", "surrogate1m", "mlp_train", "propagation",
-                             "propagation3000", "stdp", "stdp_synorder"],
+                             "propagation3000", "stdp", "stdp_synorder", "hines"],
                     help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
     if args.kernel_case:
@@ -943,7 +943,8 @@ def kernel_case(name: str):
     propagation3000 = the propagation workload at 300 / 3000 Hz of input, 100 filling steps
     then 20 profiled ones (deliver_add_batch_kernel, 6e6 / 6e7 events per step), stdp /
     stdp_synorder = the STDP workload with its records grouped by postsynaptic neuron / in
-    synapse order, 200 steps then 20 profiled ones (deliver_stdp_post_kernel)."""
+    synapse order, 200 steps then 20 profiled ones (deliver_stdp_post_kernel), hines = the
+    1024-neuron multicompartment batch for one 1000-step launch (hines_kernel)."""
     import torch
 
     from brian2cuda_b200 import Network, models
@@ -959,6 +960,12 @@ def kernel_case(name: str):
             s.attach(net, P, tol=SURR_TOL, judge=True)
         net.finalize()
         net.run(6)
+        net.sync()
+        net.close()
+    elif name == "hines":
+        net = Network(25e-6, seed=models.SEED_BASE + 3)
+        hb, _, _, _ = models.build_hines(net, n_neurons=1024)
+        hb.run(1000)            # one launch of the 1000-step chunk
         net.sync()
         net.close()
     elif name in ("stdp", "stdp_synorder"):

@@ -53,8 +53,10 @@ struct HinesDev {
   const double *g0, *gn, *rhs_first, *rhs_last;
   const int32_t* child_off;   // per node (global node index = sec_off[b] + b + i), global edges
   const int32_t* child_sec;   // neuron-local section index per edge
-  const int32_t* level_order; // per node slot: neuron-local node ids sorted by depth
-  const int32_t* level_off;   // per neuron at lvl_base[b]: nlev+1 offsets into level_order
+  // per node slot, nodes sorted by depth: {node, parent node (-1 for node 0), first child
+  // edge, end of its child edges} (neuron-local), 4 ints
+  const int32_t* level_rec;
+  const int32_t* level_off;   // per neuron at lvl_base[b]: nlev+1 offsets into level_rec
   double* v;
   void *m, *h, *n;
   double* Ic;
@@ -86,6 +88,20 @@ __device__ __forceinline__ void hh_gates(RC v, RC dt, RC& m, RC& h, RC& n) {
   n = hh_expeuler(n, an, bn, dt);
 }
 
+// 1/x for a finite, normal, nonzero x: the reciprocal unit's approximation refined by two
+// Newton-Raphson steps (y <- y + y (1 - x y), each step doubling the correct bits), within
+// an ulp or two of the correctly rounded quotient.  The solver's serial chains (the pivots of
+// a section, the node system level by level) take one reciprocal per link; the IEEE
+// division's longer sequence made them several times longer.
+__device__ __forceinline__ double recip(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
 template <typename RC>
 __global__ void __launch_bounds__(kHinesBlock)
 hines_kernel(HinesDev H, int n_steps, int write_currents) {
@@ -102,47 +118,43 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
   const int nlev = H.lvl_base[b + 1] - l0 - 1;
   const int NC = H.nc_max, NS = H.ns_max, NB = H.ns_max + 1;
 
-  double* V = reinterpret_cast<double*>(sm);
+  int4* REC = reinterpret_cast<int4*>(sm);   // level records, first (16-byte aligned)
+  // The constant matrix rows (low, diag, up) and the compartment-to-section map are read
+  // through the read-only cache rather than kept here, so that three CTAs fit an SM and one
+  // neuron's serial phases overlap other neurons' parallel ones.
+  double* V = reinterpret_cast<double*>(REC + NB);
   double* X = V + NC;          // x*, first the right-hand side of the membrane solve
   double* UE = X + NC;         // u_end
   double* US = UE + NC;        // u_start
-  double* C = US + NC;         // eliminated super-diagonal
-  double* DG = C + NC;         // diagonal with the membrane conductance of the step
-  double* LOW = DG + NC;
-  double* DIAG0 = LOW + NC;
-  double* UPR = DIAG0 + NC;
-  double* DN = UPR + NC;       // node equations: diagonal,
+  double* DG = US + NC;        // diagonal with the membrane conductance of the step, then
+                               // the eliminated super-diagonal
+  double* DN = DG + NC;        // node equations: diagonal,
   double* TOWARD = DN + NB;    // coefficient of the parent node (node >= 1),
   double* RHSN = TOWARD + NB;  // right-hand side,
-  double* INTO = RHSN + NB;    // per child edge: coefficient of the child's end node
-  double* G0 = INTO + NS;
+  double* INTO = RHSN + NB;    // per node >= 1: its coefficient in its parent's equation
+  double* INV = INTO + NB;     // 1 / final diagonal, per node
+  double* G0 = INV + NB;
   double* GN = G0 + NS;
   double* RF = GN + NS;
   double* RL = RF + NS;
   RC* M = reinterpret_cast<RC*>(RL + NS);
   RC* Hh = M + NC;
   RC* N = Hh + NC;
-  int32_t* SOC = reinterpret_cast<int32_t*>(N + NC);
-  int32_t* SST = SOC + NC;
+  int32_t* SST = reinterpret_cast<int32_t*>(N + NC);
   int32_t* SEN = SST + NS;
   int32_t* SPN = SEN + NS;
   int32_t* COFF = SPN + NS;
   int32_t* CSEC = COFF + NB + 1;
-  int32_t* LORD = CSEC + NS;
-  int32_t* LOFF = LORD + NB;
+  int32_t* LOFF = CSEC + NS;
 
   const RC* gm = static_cast<const RC*>(H.m);
   const RC* gh = static_cast<const RC*>(H.h);
   const RC* gn = static_cast<const RC*>(H.n);
   for (int j = tid; j < nc; j += bs) {
     V[j] = H.v[c0 + j];
-    LOW[j] = H.low[c0 + j];
-    DIAG0[j] = H.diag[c0 + j];
-    UPR[j] = H.up[c0 + j];
     M[j] = gm[c0 + j];
     Hh[j] = gh[c0 + j];
     N[j] = gn[c0 + j];
-    SOC[j] = H.sec_of_comp[c0 + j];
   }
   for (int s = tid; s < ns; s += bs) {
     SST[s] = H.sec_start[s0 + s];
@@ -156,7 +168,9 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
   const int e0 = H.child_off[nb0];
   for (int i = tid; i <= nB; i += bs) COFF[i] = H.child_off[nb0 + i] - e0;
   for (int e = tid; e < ns; e += bs) CSEC[e] = H.child_sec[e0 + e];
-  for (int k = tid; k < nB; k += bs) LORD[k] = H.level_order[nb0 + k];
+  for (int k = tid; k < nB; k += bs)
+    REC[k] = make_int4(H.level_rec[4 * (nb0 + k)], H.level_rec[4 * (nb0 + k) + 1],
+                       H.level_rec[4 * (nb0 + k) + 2], H.level_rec[4 * (nb0 + k) + 3]);
   for (int L = tid; L <= nlev; L += bs) LOFF[L] = H.level_off[l0 + L];
   __syncthreads();
 
@@ -177,7 +191,7 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
       const double gtot = H.gl + gna + gk;
       double I0 = H.gl * H.El + gna * H.ENa + gk * H.EK;
       if (j == 0) I0 += Isoma;
-      DG[j] = DIAG0[j] - gtot;
+      DG[j] = __ldg(H.diag + c0 + j) - gtot;
       X[j] = -cdt * v - I0;
       hh_gates<RC>((RC)v, dtR, m, h, n);
       M[j] = m;
@@ -191,26 +205,26 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
       const int j0 = SST[s], j1 = SEN[s];
       double cprev = 0.0, xprev = 0.0, sprev = 0.0, eprev = 0.0;
       for (int j = j0; j < j1; ++j) {
-        const double lw = j > j0 ? LOW[j] : 0.0;
-        const double piv = 1.0 / (DG[j] - lw * cprev);
-        C[j] = UPR[j] * piv;
+        const double lw = j > j0 ? __ldg(H.low + c0 + j) : 0.0;
+        const double piv = recip(DG[j] - lw * cprev);
+        cprev = __ldg(H.up + c0 + j) * piv;
+        DG[j] = cprev;   // the diagonal is not needed again
         X[j] = (X[j] - lw * xprev) * piv;
         US[j] = ((j == j0 ? RF[s] : 0.0) - lw * sprev) * piv;
         UE[j] = ((j == j1 - 1 ? RL[s] : 0.0) - lw * eprev) * piv;
-        cprev = C[j];
         xprev = X[j];
         sprev = US[j];
         eprev = UE[j];
       }
       for (int j = j1 - 2; j >= j0; --j) {
-        X[j] -= C[j] * X[j + 1];
-        US[j] -= C[j] * US[j + 1];
-        UE[j] -= C[j] * UE[j + 1];
+        X[j] -= DG[j] * X[j + 1];
+        US[j] -= DG[j] * US[j + 1];
+        UE[j] -= DG[j] * UE[j + 1];
       }
     }
     __syncthreads();
     // (3) node equations: node i's current balance in its own voltage (DN), its parent
-    // node's (TOWARD) and its children's end nodes' (INTO, per edge)
+    // node's (TOWARD) and its children's end nodes' (INTO, stored with the child node)
     for (int i = tid; i < nB; i += bs) {
       double dn, rh;
       if (i == 0) {
@@ -218,7 +232,7 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
         const int f = SST[0];
         dn = US[f] - 1.0;
         rh = -X[f];
-        INTO[COFF[0]] = UE[f];
+        INTO[1] = UE[f];
       } else {
         const int s = i - 1;
         const int l = SEN[s] - 1;
@@ -229,7 +243,7 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
           const int cs = CSEC[e];
           const int f = SST[cs];
           dn += G0[cs] * (1.0 - US[f]);
-          INTO[e] = -G0[cs] * UE[f];
+          INTO[cs + 1] = -G0[cs] * UE[f];
           rh += G0[cs] * X[f];
         }
       }
@@ -237,41 +251,60 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
       RHSN[i] = rh;
     }
     __syncthreads();
-    // (4) elimination, deepest level first: each node takes in its children's equations
-    for (int L = nlev - 1; L >= 0; --L) {
-      for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += bs) {
-        const int i = LORD[k];
-        double dn = DN[i], rh = RHSN[i];
-        for (int e = COFF[i]; e < COFF[i + 1]; ++e) {
-          const int c = CSEC[e] + 1;   // the child section's end node
-          const double f = INTO[e] / DN[c];
-          dn -= f * TOWARD[c];
-          rh -= f * RHSN[c];
+    // (4)-(5) the node system on the first warp alone, level by level with warp barriers (a
+    // level holds few nodes; CTA-wide barriers per level would idle every other warp)
+    if (tid < 32) {
+      // (4) elimination, deepest level first: each node takes in its children's equations;
+      // a record gives the node and its child edges at once, and children are taken in
+      // pairs so that their loads and divisions overlap (the order of the updates is the
+      // children's order)
+      for (int L = nlev - 1; L >= 0; --L) {
+        for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += 32) {
+          const int4 r = REC[k];
+          double dn = DN[r.x], rh = RHSN[r.x];
+          int e = r.z;
+          for (; e + 1 < r.w; e += 2) {
+            const int ca = CSEC[e] + 1, cb = CSEC[e + 1] + 1;   // the children's end nodes
+            const double fa = INTO[ca] * INV[ca], fb = INTO[cb] * INV[cb];
+            dn -= fa * TOWARD[ca];
+            rh -= fa * RHSN[ca];
+            dn -= fb * TOWARD[cb];
+            rh -= fb * RHSN[cb];
+          }
+          if (e < r.w) {
+            const int c = CSEC[e] + 1;
+            const double f = INTO[c] * INV[c];
+            dn -= f * TOWARD[c];
+            rh -= f * RHSN[c];
+          }
+          DN[r.x] = dn;
+          RHSN[r.x] = rh;
+          INV[r.x] = recip(dn);   // the node's equation is final here
         }
-        DN[i] = dn;
-        RHSN[i] = rh;
+        __syncwarp();
       }
-      __syncthreads();
+      // (5) substitution, root first: RHSN becomes the node voltage
+      if (tid == 0) RHSN[0] = RHSN[0] * INV[0];
+      __syncwarp();
+      for (int L = 1; L < nlev; ++L) {
+        for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += 32) {
+          const int4 r = REC[k];
+          RHSN[r.x] = (RHSN[r.x] - TOWARD[r.x] * RHSN[r.y]) * INV[r.x];
+        }
+        __syncwarp();
+      }
     }
-    // (5) substitution, root first: RHSN becomes the node voltage
-    if (tid == 0) RHSN[0] = RHSN[0] / DN[0];
     __syncthreads();
-    for (int L = 1; L < nlev; ++L) {
-      for (int k = LOFF[L] + tid; k < LOFF[L + 1]; k += bs) {
-        const int i = LORD[k];
-        RHSN[i] = (RHSN[i] - TOWARD[i] * RHSN[SPN[i - 1]]) / DN[i];
-      }
-      __syncthreads();
-    }
     // (6) v = x* + V_start u_start + V_end u_end; capacitive current
     const bool last_step = step == n_steps - 1;
     for (int j = tid; j < nc; j += bs) {
-      const int s = SOC[j];
+      const int s = __ldg(H.sec_of_comp + c0 + j);
       const double vn = X[j] + RHSN[SPN[s]] * US[j] + RHSN[s + 1] * UE[j];
       if (last_step && write_currents) H.Ic[c0 + j] = H.Cm * (vn - V[j]) / H.dt;
       V[j] = vn;
     }
-    __syncthreads();
+    // no barrier: a thread owns the same compartments here and in the next step's channel
+    // phase (and thread 0 owns compartment 0); the next step's first barrier orders the rest
     if (tid == 0) {
       const int ab = V[0] > H.Vthr ? 1 : 0;
       if (ab && !above) ++spikes;
@@ -295,8 +328,8 @@ hines_kernel(HinesDev H, int n_steps, int write_currents) {
 
 size_t hines_smem(int nc, int ns, int nlev, int rc_size) {
   const size_t NB = (size_t)ns + 1;
-  return sizeof(double) * (9 * (size_t)nc + 3 * NB + 5 * (size_t)ns) + rc_size * 3 * (size_t)nc +
-         sizeof(int32_t) * ((size_t)nc + 4 * (size_t)ns + NB + 1 + NB + (size_t)nlev + 1);
+  return 16 * NB + sizeof(double) * (5 * (size_t)nc + 5 * NB + 4 * (size_t)ns) +
+         rc_size * 3 * (size_t)nc + sizeof(int32_t) * (4 * (size_t)ns + NB + 1 + (size_t)nlev + 1);
 }
 
 }  // namespace
@@ -353,7 +386,7 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     std::vector<double> low(n_comp, 0.0), diag(n_comp, 0.0), upr(n_comp, 0.0);
     std::vector<int32_t> soc(n_comp), sst(n_sec), sen(n_sec), spn(n_sec);
     std::vector<double> g0(n_sec), gn(n_sec), rfirst(n_sec), rlast(n_sec);
-    std::vector<int32_t> child_off, child_sec, level_order, level_off, lvl_base;
+    std::vector<int32_t> child_off, child_sec, level_rec, level_off, lvl_base;
     // r: cross section over half the length; g: axial conductance into c from c - 1
     std::vector<double> area(n_comp), rl(n_comp), g(n_comp + 1, 0.0);
     std::vector<double> soma_area(n_neurons);
@@ -415,16 +448,23 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       const int nlev = *std::max_element(depth.begin(), depth.end()) + 1;
       nlev_max = std::max(nlev_max, nlev);
       const int edge_base = (int)child_sec.size();
+      std::vector<int> first_edge(nB + 1);
       for (int i = 0; i < nB; ++i) {
         child_off.push_back((int)child_sec.size());
+        first_edge[i] = (int)child_sec.size() - edge_base;
         for (int s : kids[i]) child_sec.push_back(s);
       }
-      (void)edge_base;
+      first_edge[nB] = (int)child_sec.size() - edge_base;
       std::vector<int> order(nB);
       for (int i = 0; i < nB; ++i) order[i] = i;
       std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return depth[a] < depth[c]; });
       lvl_base.push_back((int)level_off.size());
-      for (int i = 0; i < nB; ++i) level_order.push_back(order[i]);
+      for (int i : order) {
+        level_rec.push_back(i);
+        level_rec.push_back(i == 0 ? -1 : spn[s0 + i - 1]);
+        level_rec.push_back(first_edge[i]);
+        level_rec.push_back(first_edge[i + 1]);
+      }
       int k = 0;
       for (int L = 0; L <= nlev; ++L) {
         while (k < nB && depth[order[k]] < L) ++k;
@@ -465,7 +505,7 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     up(&D.sec_start, sst); up(&D.sec_end, sen); up(&D.sec_pnode, spn);
     up(&D.g0, g0); up(&D.gn, gn); up(&D.rhs_first, rfirst); up(&D.rhs_last, rlast);
     up(&D.child_off, child_off); up(&D.child_sec, child_sec);
-    up(&D.level_order, level_order); up(&D.level_off, level_off);
+    up(&D.level_rec, level_rec); up(&D.level_off, level_off);
     std::vector<double> zeros_d(n_comp, 0.0), zero_I(n_neurons, 0.0);
     std::vector<int32_t> zeros_i(n_neurons, 0);
     const double* cv = nullptr;
