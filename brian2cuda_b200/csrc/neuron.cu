@@ -140,9 +140,11 @@ struct HhPack {
   int grp;
 };
 
+// lastspike is loaded whatever the group's refractoriness (every HH population holds it):
+// deciding on the group's flag first would make the prefetch wait for the group id and the
+// group's constants, two dependent loads, when a population holds many groups.
 template <typename R>
-__device__ __forceinline__ void hh_pack_load(const PopDev& P, const HhDev* prm, int64_t q,
-                                             HhPack<R>& s) {
+__device__ __forceinline__ void hh_pack_load(const PopDev& P, int64_t q, HhPack<R>& s) {
   s.grp = group_of<4>(P, q);
   s.V = load_pack<R, 4>(P.var[B2B_VAR_V], q);
   s.M = load_pack<R, 4>(P.var[B2B_VAR_M], q);
@@ -150,7 +152,7 @@ __device__ __forceinline__ void hh_pack_load(const PopDev& P, const HhDev* prm, 
   s.N = load_pack<R, 4>(P.var[B2B_VAR_N], q);
   s.GE = load_pack<R, 4>(P.var[B2B_VAR_GE], q);
   s.GI = load_pack<R, 4>(P.var[B2B_VAR_GI], q);
-  if (prm[s.grp].ref_steps >= 0) s.LS = load_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q);
+  s.LS = load_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q);
 }
 
 template <typename R>
@@ -168,10 +170,10 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   const R dtR = (R)dt;
   int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   HhPack<R> cur;
-  if (q < nthr) hh_pack_load<R>(P, prm, q, cur);
+  if (q < nthr) hh_pack_load<R>(P, q, cur);
   for (int64_t it = 0; it < iters; ++it, q += stride) {
     HhPack<R> nxt;
-    if (q + stride < nthr) hh_pack_load<R>(P, prm, q + stride, nxt);
+    if (q + stride < nthr) hh_pack_load<R>(P, q + stride, nxt);
     unsigned fl = 0;
     if (q < nthr) {
       const HhRun<R> g = hh_run(prm[cur.grp], R());
