@@ -211,7 +211,11 @@ def main():
                     help="profiling case: build the workload, simulate STEPS steps, print "
                          "nothing (for ncu captures of the step kernels)")
     ap.add_argument("--fused", action="store_true",
-                    help="run one kernel per step (neuron update and delivery side by side)")
+                    help="run every step as two concurrent launches (neuron update, delivery "
+                         "of earlier spikes) where the net allows it")
+    ap.add_argument("--per-step", action="store_true",
+                    help="always the per-step kernels (default: the library's choice, which "
+                         "the autotuner settles)")
     ap.add_argument("--tune-from", default=None, metavar="FILE",
                     help="apply the launch shapes of the JSON line in FILE (an earlier bench "
                          "output) instead of autotuning; used by the profiling case")
@@ -255,7 +259,8 @@ def main():
     runs = args.warmup + 2 * args.steps + 1
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
-                  stream=stream.cuda_stream, fused=args.fused)
+                  stream=stream.cuda_stream,
+                  fused=True if args.fused else (False if args.per_step else None))
     t_setup = time.perf_counter()
     ids = models.build_cobahh(net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
                               monitor_capacity=mon_cap)
@@ -280,7 +285,7 @@ def main():
         with open(args.tune_from) as f:
             tune = json.loads([ln for ln in f if ln.startswith("{")][-1])["autotune"]
         net.tune_apply(tune)
-    elif not args.fused:
+    else:
         tune = net.autotune(trial_steps=300)
 
     if args.ncu_case:
@@ -365,7 +370,8 @@ def main():
     # algorithmic bytes per launch of each launch site the profiler reports
     site_info = {1: ("neuron (HH update+threshold+compaction)", "hh_step_kernel"),
                  6: ("delivery on_pre (Ce and Ci, one launch)", "deliver_add_batch_kernel"),
-                 5: ("fused step (HH update + delivery, one kernel)", "fused_step_kernel")}
+                 5: ("step as two concurrent launches (HH update, delivery)",
+                     "fused_step_kernel")}
     kernel_ms, per_launch_bytes, kernels = {}, [], []
     for k, (kd, ms) in enumerate(prof):
         label, kname = site_info.get(kd, (f"site kind {kd}", None))

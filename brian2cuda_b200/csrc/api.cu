@@ -710,8 +710,16 @@ b2b_status setup_small(b2b_net* net) {
   return B2B_OK;
 }
 
+// Populations up to this size run the two concurrent launches unless tuned otherwise
+// (measured: 1e5 HH neurons 42.5 vs 50.9 ms per simulated second; 3.9e6 HH neurons in 256
+// groups 5.6x slower, its one-neuron-per-thread update being no match for the per-step
+// kernels' packed, prefetched one).
+constexpr int64_t kAutoFusedMaxNeurons = 1 << 18;
+
 b2b_status setup_fused(b2b_net* net) {
-  if (!(net->cfg.flags & B2B_NET_FUSED)) return B2B_OK;
+  const int32_t flags = net->cfg.flags;
+  if (flags & (B2B_NET_PER_STEP | B2B_NET_SMALL)) return B2B_OK;
+  if ((flags & B2B_NET_CHECKED) && !(flags & B2B_NET_FUSED)) return B2B_OK;
   if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
     return B2B_OK;
@@ -757,7 +765,20 @@ b2b_status setup_fused(b2b_net* net) {
   if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) deliver = std::max(1, std::atoi(env));
   F.deliver_ctas = deliver;
   net->fused_grid = F.neuron_ctas + F.deliver_ctas;
-  net->fused = true;
+  // the same kernel as two launches: every CTA of one delivers, every CTA of the other updates
+  net->fused_dgrid = 2 * sms;
+  if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) net->fused_dgrid = deliver;
+  net->fused_ngrid = F.neuron_ctas;
+  net->fdev_d = F;
+  net->fdev_d.deliver_ctas = net->fused_dgrid;
+  net->fdev_n = F;
+  net->fdev_n.deliver_ctas = 0;
+  CU(cudaStreamCreateWithFlags(&net->stream2, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&net->ev_n, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&net->ev_d[0], cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&net->ev_d[1], cudaEventDisableTiming));
+  net->fused_ok = true;
+  net->fused = (flags & B2B_NET_FUSED) || pop.n <= kAutoFusedMaxNeurons;
   return B2B_OK;
 }
 
@@ -772,14 +793,28 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     return B2B_OK;
   }
   if (net->fused) {
+    // Step k's delivery (spikes of steps <= k-1 into acc[k & 1]) and step k's neuron update
+    // (which folds in acc[(k-1) & 1]) are independent: the delivery of step k waits for the
+    // update of step k-1, the update of step k for the update and the delivery of step k-1.
+    // The deliveries run on the second stream; under stream capture this is a graph with
+    // two branches per step.
     const Pop& pop = net->pops[0];
+    cudaStream_t s = net->stream, s2 = net->stream2;
+    CU(cudaEventRecord(net->ev_n, s));
     for (int k = 0; k < kk; ++k) {
-      CU(launch_fused_step(net->fdev, pop.kind, pop.dtype, net->fused_grid, net->d_clock, k,
-                           net->cfg.dt, net->d_status, net->stream));
-      ++net->launches;
+      CU(cudaStreamWaitEvent(s2, net->ev_n, 0));
+      CU(launch_fused_step(net->fdev_d, pop.kind, pop.dtype, net->fused_dgrid, net->d_clock, k,
+                           net->cfg.dt, net->d_status, s2));
+      CU(cudaEventRecord(net->ev_d[k & 1], s2));
+      if (k > 0) CU(cudaStreamWaitEvent(s, net->ev_d[(k - 1) & 1], 0));
+      CU(launch_fused_step(net->fdev_n, pop.kind, pop.dtype, net->fused_ngrid, net->d_clock, k,
+                           net->cfg.dt, net->d_status, s));
+      CU(cudaEventRecord(net->ev_n, s));
+      net->launches += 2;
     }
-    CU(launch_fused_fold(net->fdev, pop.dtype, net->d_clock, kk - 1, net->stream));
-    CU(launch_tick(net->d_clock, kk, net->stream));
+    CU(cudaStreamWaitEvent(s, net->ev_d[(kk - 1) & 1], 0));
+    CU(launch_fused_fold(net->fdev, pop.dtype, net->d_clock, kk - 1, s));
+    CU(launch_tick(net->d_clock, kk, s));
     net->launches += 2;
     return B2B_OK;
   }
@@ -946,6 +981,9 @@ b2b_status b2b_destroy(b2b_net* net) {
   for (Snapshot& sn : net->snapshots)
     for (void* a : sn.buffers) cudaFree(a);
   for (void* a : net->fused_allocs) cudaFree(a);
+  if (net->stream2) cudaStreamDestroy(net->stream2);
+  for (cudaEvent_t ev : {net->ev_n, net->ev_d[0], net->ev_d[1]})
+    if (ev) cudaEventDestroy(ev);
   for (void* a : net->mon_allocs) cudaFree(a);
   cudaFree(net->d_clock);
   cudaFree(net->d_status);
@@ -1362,9 +1400,14 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 7)
         e = launch_small(net->sdev, net->pops[0].kind, net->pops[0].dtype, clk, 1, net->cfg.dt,
                          net->d_status, net->stream);
-      if (s.kind == 5)
-        e = launch_fused_step(net->fdev, net->pops[0].kind, net->pops[0].dtype, net->fused_grid,
-                              clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 5) {  // the step's two launches, one after the other
+        e = launch_fused_step(net->fdev_d, net->pops[0].kind, net->pops[0].dtype,
+                              net->fused_dgrid, clk, 0, net->cfg.dt, net->d_status, net->stream);
+        if (e == cudaSuccess)
+          e = launch_fused_step(net->fdev_n, net->pops[0].kind, net->pops[0].dtype,
+                                net->fused_ngrid, clk, 0, net->cfg.dt, net->d_status,
+                                net->stream);
+      }
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
       ++net->launches;
@@ -1441,6 +1484,20 @@ b2b_status set_record_order(b2b_net* net, Proj& pr, bool post_grouped) {
 
 constexpr double kTuneMargin = 0.98;
 
+// Launch shape of the delivery launch of a net run with two launches per step (fused.cu):
+// lanes per work item (0: 8) and CTAs (0: two per SM).
+void set_fused_shape(b2b_net* net, int group, int grid) {
+  int sms = kNumSMs;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+  net->fused_dgrid = grid > 0 ? grid : 2 * sms;
+  net->fdev_d.deliver_ctas = net->fused_dgrid;
+  net->fdev_d.group = group > 0 ? group : 8;
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+}
+
 // Advances the net by n_steps the way b2b_run does (CUDA-graph replays of the current launch
 // shapes, captured afresh before the timing starts), timed with a CUDA event pair on the
 // net's stream; *mean_ms receives the mean device time of one whole step.  A shape is judged
@@ -1477,7 +1534,6 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   if (b2b_status st = check_net(net)) return st;
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   CHECK(trial_steps > 0 && trial_steps <= 100000 && n_out, B2B_ERR_INVALID_ARG, "bad arguments");
-  CHECK(!net->fused, B2B_ERR_UNSUPPORTED, "the one-kernel-per-step path has no tunable shapes");
   if (net->small) {  // one CTA with a fixed shape: nothing to tune
     *n_out = 0;
     return B2B_OK;
@@ -1527,7 +1583,13 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     double ms = 0;
     st = trial(&ms);
   }
-  for (size_t p = 0; p < net->pops.size() && st == B2B_OK; ++p) {
+  int sms = kNumSMs;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+  // a net that allows both forms of the step tunes the per-step kernels first, then the two
+  // concurrent launches, and keeps the faster form
+  const bool builtin_fused = net->fused;
+  if (net->fused_ok) net->fused = false;
+  for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->fused; ++p) {
     Pop& pop = net->pops[p];
     if (pop.kind == KIND_SPIKEGEN) continue;
     std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
@@ -1565,9 +1627,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
-  int sms = kNumSMs;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
-  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK; ++b) {
+  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->fused; ++b) {
     AddTune& t = net->add_tune[b];
     std::vector<std::pair<int, int>> cands = {{0, 0}};
     for (int g : {4, 8, 16, 32})
@@ -1593,6 +1653,38 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
+  if (net->fused_ok && st == B2B_OK) {
+    const double per_step_ms = res.empty() ? 1e30 : res.back().best_ms;
+    net->fused = true;
+    // the step's delivery launch: lanes per work item x CTAs (the neuron launch has one
+    // thread per neuron)
+    std::vector<std::pair<int, int>> cands = {{0, 0}};
+    for (int g : {4, 8, 16})
+      for (int mult : {1, 2, 4}) cands.push_back({g, mult * sms / 2});
+    b2b_tune_result r{5, 0, 0, 0, 0.0, 0.0};
+    double best = 1e30;
+    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+      set_fused_shape(net, cands[c].first, cands[c].second);
+      double ms = 0;
+      st = trial(&ms);
+      if (c == 0) r.default_ms = ms;
+      if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
+        best = ms;
+        r.choice_a = cands[c].first;
+        r.choice_b = cands[c].second;
+      }
+    }
+    set_fused_shape(net, r.choice_a, r.choice_b);
+    r.best_ms = best;
+    res.push_back(r);
+    const double fused_ms = res.back().best_ms;
+    // the built-in form stays unless the other is 2 % faster
+    const bool use_fused = builtin_fused ? !(per_step_ms < kTuneMargin * fused_ms)
+                                         : fused_ms < kTuneMargin * per_step_ms;
+    net->fused = use_fused;
+    res.push_back(b2b_tune_result{11, 0, use_fused ? 1 : 0, 0, std::min(per_step_ms, fused_ms),
+                                  builtin_fused ? fused_ms : per_step_ms});
+  }
   // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
   for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
     Proj& pr = net->projs[p];
@@ -1613,6 +1705,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
+  if (st != B2B_OK && net->fused_ok) net->fused = builtin_fused;
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
   if (st2 == B2B_OK) st2 = put_back_monitors();
@@ -1661,6 +1754,17 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       net->add_tune[t.site_index].group = t.choice_a;
       net->add_tune[t.site_index].grid = t.choice_b;
+    } else if (t.site_kind == 11) {
+      CHECK(net->fused_ok && t.site_index == 0 && (t.choice_a == 0 || t.choice_a == 1),
+            B2B_ERR_INVALID_ARG, "site kind 11 exists only for nets that allow both step forms");
+      net->fused = t.choice_a == 1;
+    } else if (t.site_kind == 5) {
+      CHECK(net->fused_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
+            "site kind 5 exists only for nets that allow two launches per step");
+      CHECK((t.choice_a == 0 || t.choice_a == 4 || t.choice_a == 8 || t.choice_a == 16) &&
+                t.choice_b >= 0 && t.choice_b <= 65535,
+            B2B_ERR_INVALID_ARG, "bad delivery launch shape");
+      set_fused_shape(net, t.choice_a, t.choice_b);
     } else if (t.site_kind == 8) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
                 net->projs[t.site_index].effect == B2B_EFFECT_STDP,

@@ -146,6 +146,8 @@ struct FusedDev {
   int32_t deliver_ctas;           // CTAs [0, deliver_ctas) deliver, the rest update neurons
   int32_t neuron_ctas;
   void* acc[3];                   // per target variable (v, ge, gi): [2][pop.n] or NULL
+  int32_t group;                  // delivery: lanes per work item (4, 8 or 16)
+  int32_t pad_group;
 };
 
 // Device view of the one-CTA path for small networks (small.cu): one LIF/HH population of at
@@ -284,9 +286,16 @@ struct b2b_net {
   std::vector<void*> mon_allocs;
   bool small = false;                      // one CTA runs every step (small.cu)
   b2b::SmallDev sdev{};
-  bool fused = false;                      // one kernel per step (fused.cu) in use
+  bool fused = false;                      // the step as two concurrent launches (fused.cu)
+  bool fused_ok = false;                   // the net allows them (their buffers exist)
   b2b::FusedDev fdev{};
   int fused_grid = 0;
+  // the step as two concurrent launches: delivery-only and neuron-only views of fdev, the
+  // delivery on a second stream, ordered by events (see enqueue_steps)
+  b2b::FusedDev fdev_d{}, fdev_n{};
+  int fused_dgrid = 0, fused_ngrid = 0;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
   std::vector<void*> fused_allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;

@@ -123,7 +123,9 @@ __device__ __forceinline__ bool update_neuron(const FusedDev& F, int64_t q, doub
   return spk;
 }
 
-template <typename R, int KIND, bool WARP_PREFIX>
+constexpr int kFusedUnroll = 4;   // rounds of a bundle whose loads a lane issues together
+
+template <typename R, int KIND, bool WARP_PREFIX, int GROUP>
 __global__ void __launch_bounds__(kFusedBlock)
 fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict__ clock, int k,
                   double dt, int32_t* status) {
@@ -149,17 +151,30 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
   const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)F.deliver_ctas * blockDim.x) >> 5;
   const int par = (int)(ts & 1);
+  const int glane = (threadIdx.x & 31) % GROUP;
   for (int p = 0; p < F.n_proj; ++p) {
     const ProjDev& J = F.proj[p];
     const R* W = static_cast<const R*>(J.w);
     MemberCache<R> mc;
-    for_each_due<WARP_PREFIX, 8>(J, ts, warp0, nwarps, s_pref,
-                                 [&](int64_t s, bool valid, int32_t pre) {
-      if (!valid) return;
-      const int32_t post = __ldg(J.post + s);
+    for_each_due_item<WARP_PREFIX, GROUP>(J, ts, warp0, nwarps, s_pref,
+                                          [&](int64_t b0, int64_t b1, int64_t len, int32_t pre) {
       member_lookup<R>(J, pre, mc);
-      const R w = W ? __ldg(W + s) : mc.w;
-      atomicAdd(mc.target + (int64_t)par * P.n + post, w);
+      // the loads of kFusedUnroll rounds first, then their atomics
+      for (int64_t off = 0; off < len; off += kFusedUnroll * GROUP) {
+        int32_t post[kFusedUnroll];
+        R w[kFusedUnroll];
+        bool v[kFusedUnroll];
+#pragma unroll
+        for (int u = 0; u < kFusedUnroll; ++u) {
+          const int64_t s = b0 + off + u * GROUP + glane;
+          v[u] = s < b1;
+          post[u] = v[u] ? __ldg(J.post + s) : 0;
+          w[u] = v[u] && W ? __ldg(W + s) : mc.w;
+        }
+#pragma unroll
+        for (int u = 0; u < kFusedUnroll; ++u)
+          if (v[u]) atomicAdd(mc.target + (int64_t)par * P.n + post[u], w[u]);
+      }
     });
   }
 }
@@ -197,7 +212,7 @@ int fused_resident_ctas(int kind, int dtype, const FusedDev& F, int sms) {
   const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
   int occ = 0;
 #define B2B_OCC(R, KD, WP) \
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_step_kernel<R, KD, WP>, kFusedBlock, smem)
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_step_kernel<R, KD, WP, 8>, kFusedBlock, smem)
   if (kind == KIND_HH) {
     if (dtype == B2B_F32) { if (wp) B2B_OCC(float, KIND_HH, true); else B2B_OCC(float, KIND_HH, false); }
     else { if (wp) B2B_OCC(double, KIND_HH, true); else B2B_OCC(double, KIND_HH, false); }
@@ -215,9 +230,13 @@ cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
   const size_t smem = fused_smem(F);
   const dim3 g(grid);
   const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
-#define B2B_FS(R, KD, WP)                                                                   \
-  launch_chained(fused_step_kernel<R, KD, WP>, g, dim3(kFusedBlock), smem, s, F, clock, k, dt, \
-                 status)
+#define B2B_FS(R, KD, WP)                                                                    \
+  (F.group == 16 ? (fused_step_kernel<R, KD, WP, 16><<<g, kFusedBlock, smem, s>>>(F, clock, k, dt, \
+                                                                              status), 0)   \
+   : F.group == 4 ? (fused_step_kernel<R, KD, WP, 4><<<g, kFusedBlock, smem, s>>>(F, clock, k, dt, \
+                                                                              status), 0)   \
+   : (fused_step_kernel<R, KD, WP, 8><<<g, kFusedBlock, smem, s>>>(F, clock, k, dt, status), 0), \
+   cudaGetLastError())
   if (kind == KIND_HH) {
     if (dtype == B2B_F32) return wp ? B2B_FS(float, KIND_HH, true) : B2B_FS(float, KIND_HH, false);
     return wp ? B2B_FS(double, KIND_HH, true) : B2B_FS(double, KIND_HH, false);
@@ -234,8 +253,9 @@ cudaError_t launch_fused_fold(const FusedDev& F, int dtype, const int64_t* clock
   if (blocks > 4 * kNumSMs) blocks = 4 * kNumSMs;
   const dim3 g((unsigned)blocks);
   const dim3 b(kFusedBlock);
-  if (dtype == B2B_F32) return launch_chained(fused_fold_kernel<float>, g, b, 0, s, F, clock, k_last);
-  return launch_chained(fused_fold_kernel<double>, g, b, 0, s, F, clock, k_last);
+  if (dtype == B2B_F32) fused_fold_kernel<float><<<g, b, 0, s>>>(F, clock, k_last);
+  else fused_fold_kernel<double><<<g, b, 0, s>>>(F, clock, k_last);
+  return cudaGetLastError();
 }
 
 }  // namespace b2b

@@ -140,10 +140,13 @@ class Network:
 
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
-                 stream: int | None = None, fused: bool = False, small: bool = False):
+                 stream: int | None = None, fused: bool | None = None, small: bool = False):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
-        default the network creates its own non-blocking stream.  `fused`: run one kernel per
-        step (neuron update and delivery side by side) where the net allows it.  `small`: run
+        default the network creates its own non-blocking stream.  `fused`: True runs every
+        step as two concurrent launches (the neuron update, and the delivery of earlier
+        steps' spikes into a double-buffered input) where the net allows it, False always
+        the per-step kernels, None (default) the two launches for nets that allow them with at
+        most 2^18 neurons, until autotune() picks the faster form.  `small`: run
         a small network (one LIF/HH population of <= 4096 neurons, additive synapses onto
         itself) in one CTA per chunk of steps with the state in shared memory; it pays off for
         nets of a few hundred to ~2000 neurons with few delays."""
@@ -152,8 +155,10 @@ class Network:
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
         if reset_before_synapses:
             flags |= N.NET_RESET_BEFORE_SYNAPSES
-        if fused:
+        if fused is True:
             flags |= N.NET_FUSED
+        elif fused is False:
+            flags |= N.NET_PER_STEP
         if small:
             flags |= N.NET_SMALL
         cfg = N.Config(self.dt, device, steps_per_graph, seed, stream, flags, 0)
@@ -386,8 +391,8 @@ class Network:
 
     @property
     def run_mode(self) -> str:
-        """'fused' (one kernel per step), 'small' (one CTA runs every step of a chunk) or
-        'per-step' (graph-replayed kernels)."""
+        """'fused' (two concurrent launches per step), 'small' (one CTA runs every step of a
+        chunk) or 'per-step' (graph-replayed kernels)."""
         m = C.c_int32()
         self._check(self._lib.b2b_run_mode(self._h, C.byref(m)), "run_mode")
         return {1: "fused", 2: "small"}.get(m.value, "per-step")

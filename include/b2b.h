@@ -59,15 +59,21 @@ enum {
   B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
-  B2B_NET_FUSED = 8,      /* run one kernel per step (neuron update and delivery side by
-                             side) when the net has one population, additive synapses onto
-                             ge/gi and all delays >= 1 step; otherwise per-step kernels  */
-  B2B_NET_SMALL = 16      /* run a small network (one LIF/HH population of <= 4096 neurons
+  B2B_NET_FUSED = 8,      /* run every step as two concurrent launches (neuron update, and
+                             the delivery of spikes of earlier steps into a double-buffered
+                             input) whenever the net allows it: one LIF/HH population, additive
+                             synapses onto ge/gi only, all delays >= 1 step, no state or rate
+                             monitor.  Without this flag or B2B_NET_PER_STEP such a net uses
+                             the two launches when its population has at most 2^18 neurons,
+                             and b2b_autotune picks the faster of the two forms             */
+  B2B_NET_SMALL = 16,     /* run a small network (one LIF/HH population of <= 4096 neurons
                              with additive synapses onto itself) in one CTA per chunk of
                              steps, with the state in shared memory; faster than the
                              per-step kernels only for nets of a few hundred to ~2000
                              neurons with few delays (measured: 500-neuron CUBA 3.8 vs
                              4.9 us per step); otherwise per-step kernels                */
+  B2B_NET_PER_STEP = 32   /* always the per-step kernels (one launch per population, then
+                             the delivery), never the two concurrent launches             */
 };
 
 typedef struct {

@@ -480,6 +480,41 @@ def test_autotune_keeps_state_and_results(gpu_factory):
     assert net.run_mode == "small" and net.autotune(trial_steps=5) == []
 
 
+def test_autotune_chooses_step_form(gpu_factory):
+    """A net that allows both forms of the step (one population, additive synapses onto ge
+    and gi, delays >= 1): the tuner tunes the per-step kernels and the two concurrent
+    launches, keeps the faster form (site kind 11), leaves the state as it was, and either
+    form computes the same network; tune_apply reproduces each form."""
+    out = {}
+    for mode in ("untuned", "tuned", "per-step", "two launches"):
+        net = gpu_factory(DT)
+        G, Ce, Ci, _ = _delay_net(net, n=800)
+        net.finalize()
+        assert net.run_mode == "fused"   # <= 2^18 neurons: the two launches until tuned
+        net.run(60)
+        v0 = net.get_state(G, "v").copy()
+        if mode == "tuned":
+            res = net.autotune(trial_steps=20)
+            kinds = [r["site_kind"] for r in res]
+            assert {1, 6, 5, 11} <= set(kinds), kinds
+            form = [r for r in res if r["site_kind"] == 11][0]
+            assert net.run_mode == ("fused" if form["choice_a"] == 1 else "per-step")
+            np.testing.assert_array_equal(net.get_state(G, "v"), v0)
+            assert net.timestep == 60
+        elif mode != "untuned":
+            net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_b": 0,
+                             "choice_a": 1 if mode == "two launches" else 0}])
+            assert net.run_mode == ("fused" if mode == "two launches" else "per-step")
+        net.run(240)
+        idx, st = net.spikes(G)
+        out[mode] = (idx, st, net.get_state(G, "v"))
+    assert len(out["untuned"][0]) > 100
+    for mode in ("tuned", "per-step", "two launches"):
+        np.testing.assert_array_equal(out[mode][1], out["untuned"][1])
+        np.testing.assert_array_equal(out[mode][0], out["untuned"][0])
+        _close(out[mode][2], out["untuned"][2], 1e-10, 1e-15)
+
+
 def test_out_degree_matches_synapses(gpu_factory):
     net = gpu_factory(DT)
     ids = models.build_cobahh(net, n=3000, p=0.03)
@@ -497,7 +532,7 @@ def test_small_network_path_matches_per_step(gpu_factory, case):
     target variable is equal, so the order of the additions cannot change a sum)."""
     out = {}
     for small in (True, False):
-        net = gpu_factory(DT, small=small)
+        net = gpu_factory(DT, small=small, fused=None if small else False)
         if case == "cobahh_delays":
             ids = models.build_cobahh(net, n=3000, p=0.05, monitor_capacity=10**6)
             G, steps = ids["P"], 300
