@@ -1,4 +1,5 @@
-// One kernel per time step for networks whose every synaptic delay is at least one step.
+// The step as two concurrent launches, for networks whose every synaptic delay is at least
+// one step.
 //
 // The per-step path (neuron.cu then propagate.cu) runs the neuron update and the spike
 // delivery of a step as two dependent launches, because Brian2's schedule applies the
@@ -6,21 +7,20 @@
 // delivery of step t only reads spikes of steps t - d <= t - 1, so its one dependence on the
 // update of step t is the target variable itself.  Double-buffering that input removes it:
 //
-//   step t (one launch):  CTAs [0, deliver_ctas) deliver the bundles due at step t into
-//                         acc[t & 1]; the remaining CTAs update one neuron per thread,
-//                         reading the input that arrived during step t-1 from
-//                         acc[(t-1) & 1] (and zeroing it), and compact their spikes into
-//                         ring slot t.  Delivery CTAs come first so the block scheduler
-//                         starts them with the first wave.
+//   delivery of step t:  the bundles due at step t are added into acc[t & 1];
+//   update of step t:    one neuron per thread, reading the input that arrived during step
+//                        t-1 from acc[(t-1) & 1] (and zeroing it), spikes compacted into
+//                        ring slot t.
 //
-// Both halves run concurrently; the update of step t+1 sees exactly the value Brian2's
-// schedule produces (state after step t's update plus every effect of step t's synapses
-// slot).  A fold kernel at the end of every chunk of steps adds the pending accumulator into
-// the target variables, so between chunks the state is the ordinary one.  Consecutive step
-// kernels are chained with programmatic dependent launch: each kernel waits
-// (griddepcontrol.wait) for its predecessor's memory before touching state, so the launch of
-// step t+1 overlaps the tail of step t.  Measured on B200: a graph kernel boundary costs
-// about 1.1 us, 0.9 us with programmatic dependent launch, a software grid barrier 1.2-1.4 us.
+// fused_step_kernel takes either role by CTA (CTAs below deliver_ctas deliver, the rest
+// update), so one launch can hold both halves; the library launches it twice per step, once
+// per role, the delivery on a second stream: the delivery of step t waits for the update of
+// step t-1, the update of step t for the update and the delivery of step t-1, and the two
+// launches of a step run side by side (api.cu, enqueue_steps).  The update of step t+1 sees
+// exactly the value Brian2's schedule produces (state after step t's update plus every
+// effect of step t's synapses slot).  A fold kernel at the end of every chunk of steps adds
+// the pending accumulator into the target variables, so between chunks the state is the
+// ordinary one.
 #include "delivery.cuh"
 #include "neuron_math.cuh"
 
@@ -130,8 +130,6 @@ __global__ void __launch_bounds__(kFusedBlock)
 fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict__ clock, int k,
                   double dt, int32_t* status) {
   extern __shared__ int s_pref[];  // F.nd_max + 1 ints when !WARP_PREFIX
-  chain_wait();
-  chain_trigger();
   const PopDev& P = F.pop;
   const int64_t ts = clock[0] + k;
   if ((int)blockIdx.x >= F.deliver_ctas) {
@@ -183,8 +181,6 @@ fused_step_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict_
 template <typename R>
 __global__ void fused_fold_kernel(const __grid_constant__ FusedDev F,
                                   const int64_t* __restrict__ clock, int k_last) {
-  chain_wait();
-  chain_trigger();
   const int last = (int)((clock[0] + k_last) & 1);
   const int64_t n = F.pop.n;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;

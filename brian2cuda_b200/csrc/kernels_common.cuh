@@ -65,36 +65,6 @@ __device__ __forceinline__ int block_exclusive_scan(int c, int* s_warp, int* tot
   return s_warp[warp] + x - c;
 }
 
-// Chained launches (programmatic dependent launch): a kernel launched with launch_chained
-// may be scheduled while its predecessor in the stream is still running, which hides part of
-// the launch latency between consecutive kernels.  Used by the persistent multi-step path;
-// the per-step kernels measured slower with it (COBAHH, 4000 neurons: 6.1 against 5.2 us a
-// step), so they keep ordinary launches.  chain_wait() blocks until the predecessor
-// has completed and its memory is visible, so it comes before the kernel touches anything;
-// chain_trigger() then lets the successor start launching (it launches only once every CTA
-// of this grid has triggered or finished, so its waiting CTAs never keep this grid's CTAs
-// off the SMs).  Both are no-ops for ordinary launches.
-__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void chain_trigger() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-template <typename KernelT, typename... Args>
-cudaError_t launch_chained(KernelT kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                           Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 // Floor modulo of a (possibly negative) step by the ring length.
 __device__ __forceinline__ int ring_slot(int64_t step, int ring_len) {
   int64_t r = step % ring_len;
