@@ -36,6 +36,7 @@ P_CONNECT = 0.02
 DMIN, DMAX = 1, 50
 SIM_STEPS = 10_000           # simulation steps per bench step (1 s)
 BYTES_NEURON_UPDATE = 54     # COBAHH f32: 6 vars x 4 B x (R+W) + flag + lastspike
+BYTES_NEURON_FOLD = 16       # two-launch step: pending ge, gi input read and cleared, 4 B each way
 BYTES_EVENT = 12             # post index 4 + target R/W 8 (we, wi: one value per Synapses)
 BYTES_BUNDLE = 8             # per (spike, delay) bundle visited
 METRIC = "synaptic events/s"
@@ -368,29 +369,36 @@ def main():
     deliver_inh = (BYTES_EVENT * ev_inh + BYTES_BUNDLE * nd * n_inh_spk) / launches_timed
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     # algorithmic bytes per launch of each launch site the profiler reports
-    site_info = {1: ("neuron (HH update+threshold+compaction)", "hh_step_kernel"),
+    two_launch = net.run_mode == "fused"
+    if two_launch:
+        # the update also adds in and clears the pending input of ge and gi
+        neuron_bytes += BYTES_NEURON_FOLD * N_NEURONS
+    site_info = {1: ("neuron (HH update+threshold+compaction"
+                     + (", folding in the pending input)" if two_launch else ")"),
+                     "hh_step_kernel@fold" if two_launch else "hh_step_kernel"),
                  6: ("delivery on_pre (Ce and Ci, one launch)", "deliver_add_batch_kernel"),
-                 5: ("step as two concurrent launches (HH update, delivery)",
-                     "fused_step_kernel")}
+                 5: ("delivery on_pre into the pending input (Ce and Ci, one launch)",
+                     "deliver_pending_kernel")}
     kernel_ms, per_launch_bytes, kernels = {}, [], []
     for k, (kd, ms) in enumerate(prof):
         label, kname = site_info.get(kd, (f"site kind {kd}", None))
         if kd == 1:
             b = neuron_bytes
-        elif kd == 6:
+        elif kd in (5, 6):
             b = deliver_exc + deliver_inh
-        elif kd == 5:
-            b = neuron_bytes + deliver_exc + deliver_inh
         else:
             b = 0.0
         kernel_ms[label] = round(ms, 6)
         per_launch_bytes.append(b)
         kernels.append((label, kname))
-    dom = max(range(len(prof)), key=lambda k: prof[k][1])
+    # the roofline names the neuron update: the largest share of device time in the launch
+    # list in either form of the step (the eager per-launch times of this profiling run are
+    # a few us each and mostly launch latency, so they do not rank the kernels)
+    dom = [k for k, (kd, _) in enumerate(prof) if kd == 1][0]
     dom_ms = prof[dom][1]
     alg = per_launch_bytes[dom]
     achieved = alg / (dom_ms * 1e-3) / 1e9
-    traffic = _traffic(kernels[dom][1]) if kernels[dom][1] else None
+    traffic = _traffic_lookup(kernels[dom][1]) if kernels[dom][1] else None
     names = [lab for lab, _ in kernels]
 
     line = {
@@ -1000,11 +1008,6 @@ def kernel_case(name: str):
         s = GatingSurrogate(seed=3)
         s.fit(x, t, epochs=1, batch=32768, lr=1e-2)
         torch.cuda.synchronize()
-
-
-def _traffic(kernel: str):
-    """DRAM bytes per launch from the committed ncu summary, when one exists."""
-    return _traffic_lookup(kernel)
 
 
 def _traffic_lookup(kernel: str):

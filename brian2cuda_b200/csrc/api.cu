@@ -236,15 +236,26 @@ b2b_status finalize_pops(b2b_net* net) {
         D.var[v] = d;
       }
     }
-    // parameters
+    // parameters, with each group's TimedArray input in the population's dtype
     std::vector<uint8_t> prm;
     for (int gi : pop.groups) {
       const Group& g = net->groups[gi];
+      TimedInput ta{};
+      if (!g.ta.empty()) {
+        std::vector<uint8_t> host(rs * g.ta.size());
+        for (size_t k = 0; k < g.ta.size(); ++k) put_real(host, pop.dtype, (int64_t)k, g.ta[k]);
+        uint8_t* d = nullptr;
+        CU(dalloc(pop, &d, host.size()));
+        CU(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
+        ta = TimedInput{d, g.ta_rows, g.ta_cols, g.ta_mul, g.ta_div};
+      }
       if (pop.kind == KIND_LIF) {
         LifDev d = lif_dev(g, dt);
+        d.ta = ta;
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       } else if (pop.kind == KIND_HH) {
         HhDev d = hh_dev(g, dt);
+        d.ta = ta;
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       } else if (pop.kind == KIND_POISSON) {
         PoissonDev d{g.rate * dt, g.offset, g.n};
@@ -266,6 +277,9 @@ b2b_status finalize_pops(b2b_net* net) {
         CHECK(g.surr == g0.surr && g.surr_tol == g0.surr_tol && g.surr_judge == g0.surr_judge,
               B2B_ERR_UNSUPPORTED, "HH groups of one population must share one surrogate");
       }
+      for (int gi : pop.groups)
+        CHECK(!any || net->groups[gi].ta.empty(), B2B_ERR_UNSUPPORTED,
+              "a TimedArray input and the gating surrogate cannot drive one population");
       if (any) {
         CHECK(pop.dtype == B2B_F32, B2B_ERR_UNSUPPORTED, "the gating surrogate is float32 only");
         CHECK(mlp_device(g0.surr) == net->cfg.device, B2B_ERR_INVALID_ARG,
@@ -597,6 +611,7 @@ b2b_status finalize_projs(b2b_net* net) {
     }
     if (!placed) net->add_batches.push_back({&pr});
   }
+  net->add_tune.assign(net->add_batches.size(), AddTune{});  // built-in shapes until tuned
   return B2B_OK;
 }
 
@@ -711,9 +726,9 @@ b2b_status setup_small(b2b_net* net) {
 }
 
 // Populations up to this size run the two concurrent launches unless tuned otherwise
-// (measured: 1e5 HH neurons 42.5 vs 50.9 ms per simulated second; 3.9e6 HH neurons in 256
-// groups 5.6x slower, its one-neuron-per-thread update being no match for the per-step
-// kernels' packed, prefetched one).
+// (measured: 1e5 HH neurons 38.6 vs 50.9 ms per simulated second).  Above it the pending
+// input's read and clear (16 B per neuron and step for ge and gi in float32) costs more HBM
+// time than the overlap saves: 3.9e6 HH neurons 70.1 vs 62.2 us per step.
 constexpr int64_t kAutoFusedMaxNeurons = 1 << 18;
 
 b2b_status setup_fused(b2b_net* net) {
@@ -755,24 +770,14 @@ b2b_status setup_fused(b2b_net* net) {
     }
     F.proj[p].target = F.acc[pr.target_var];
   }
-  const int block = fused_block();
-  F.neuron_ctas = (int32_t)((pop.n + block - 1) / block);
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
-  // delivery CTAs fill what one wave leaves after the neuron CTAs, at least 16
-  const int resident = fused_resident_ctas(pop.kind, pop.dtype, F, sms);
-  int deliver = std::min(2 * sms, std::max(16, resident - F.neuron_ctas));
-  if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) deliver = std::max(1, std::atoi(env));
-  F.deliver_ctas = deliver;
-  net->fused_grid = F.neuron_ctas + F.deliver_ctas;
-  // the same kernel as two launches: every CTA of one delivers, every CTA of the other updates
+  F.group = 8;
   net->fused_dgrid = 2 * sms;
-  if (const char* env = std::getenv("B2B_FUSED_DELIVERY_CTAS")) net->fused_dgrid = deliver;
-  net->fused_ngrid = F.neuron_ctas;
-  net->fdev_d = F;
-  net->fdev_d.deliver_ctas = net->fused_dgrid;
-  net->fdev_n = F;
-  net->fdev_n.deliver_ctas = 0;
+  // the update launch is the per-step neuron kernel, adding in the input that the previous
+  // step's delivery left in acc
+  net->fold_dev = pop.dev;
+  for (int v = 0; v < 3; ++v) net->fold_dev.fold[v] = F.acc[v];
   CU(cudaStreamCreateWithFlags(&net->stream2, cudaStreamNonBlocking));
   CU(cudaEventCreateWithFlags(&net->ev_n, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&net->ev_d[0], cudaEventDisableTiming));
@@ -803,17 +808,16 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     CU(cudaEventRecord(net->ev_n, s));
     for (int k = 0; k < kk; ++k) {
       CU(cudaStreamWaitEvent(s2, net->ev_n, 0));
-      CU(launch_fused_step(net->fdev_d, pop.kind, pop.dtype, net->fused_dgrid, net->d_clock, k,
-                           net->cfg.dt, net->d_status, s2));
+      CU(launch_pending_delivery(net->fdev, pop.dtype, net->fused_dgrid, net->d_clock, k, s2));
       CU(cudaEventRecord(net->ev_d[k & 1], s2));
       if (k > 0) CU(cudaStreamWaitEvent(s, net->ev_d[(k - 1) & 1], 0));
-      CU(launch_fused_step(net->fdev_n, pop.kind, pop.dtype, net->fused_ngrid, net->d_clock, k,
-                           net->cfg.dt, net->d_status, s));
+      CU(launch_pop_step_dev(pop, net->fold_dev, net->d_clock, k, net->cfg.dt, net->d_status,
+                             s));
       CU(cudaEventRecord(net->ev_n, s));
       net->launches += 2;
     }
     CU(cudaStreamWaitEvent(s, net->ev_d[(kk - 1) & 1], 0));
-    CU(launch_fused_fold(net->fdev, pop.dtype, net->d_clock, kk - 1, s));
+    CU(launch_fold_pending(net->fdev, pop.dtype, net->d_clock, kk - 1, s));
     CU(launch_tick(net->d_clock, kk, s));
     net->launches += 2;
     return B2B_OK;
@@ -1103,6 +1107,39 @@ b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const i
   GUARD_END
 }
 
+b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64_t rows,
+                          int64_t cols, double dt_array) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "TimedArrays must be set before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  Group& g = net->groups[gid];
+  CHECK(g.kind == KIND_LIF || g.kind == KIND_HH, B2B_ERR_INVALID_ARG,
+        "a TimedArray drives a LIF or HH group");
+  CHECK(values && rows > 0 && (cols == 1 || cols == g.n), B2B_ERR_INVALID_ARG,
+        "values must be [rows >= 1][1 or the group's %lld neurons]", (long long)g.n);
+  CHECK(std::isfinite(dt_array) && dt_array > 0, B2B_ERR_INVALID_ARG, "bad dt_array");
+  // aligned time grids: dt_array = m dt (row = ts / m) or dt = r dt_array (row = ts * r)
+  const double dt = net->cfg.dt;
+  int64_t mul = 1, div = 1;
+  if (dt_array >= dt) {
+    div = std::llround(dt_array / dt);
+    CHECK(std::fabs(dt_array / dt - (double)div) <= 1e-6, B2B_ERR_INVALID_ARG,
+          "dt_array %g is not a multiple of dt %g", dt_array, dt);
+  } else {
+    mul = std::llround(dt / dt_array);
+    CHECK(std::fabs(dt / dt_array - (double)mul) <= 1e-6, B2B_ERR_INVALID_ARG,
+          "dt %g is not a multiple of dt_array %g", dt, dt_array);
+  }
+  GUARD_BEGIN
+  g.ta.assign(values, values + rows * cols);
+  g.ta_rows = rows;
+  g.ta_cols = cols;
+  g.ta_mul = mul;
+  g.ta_div = div;
+  return B2B_OK;
+  GUARD_END
+}
+
 b2b_status b2b_state_set(b2b_net* net, int32_t gid, int32_t var, const void* host, int64_t n) {
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
@@ -1358,8 +1395,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   std::vector<Site> sites;
   if (net->small) {
     sites.push_back({7, 0});
-  } else if (net->fused) {
+  } else if (net->fused) {  // the step's two launches, timed one after the other
     sites.push_back({5, 0});
+    sites.push_back({1, 0});
   } else {
     if (!net->smons.empty()) sites.push_back({9, 0});
     for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
@@ -1384,10 +1422,14 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       cudaEventRecord(ev[2 * k], net->stream);
       cudaError_t e = cudaSuccess;
       const int64_t* clk = net->d_clock;
-      if (s.kind == 1) e = launch_pop_step(net->pops[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
+      if (s.kind == 1)
+        e = launch_pop_step_dev(net->pops[s.idx], net->fused ? net->fold_dev : net->pops[s.idx].dev,
+                                clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 6)
         e = launch_proj_add_batch(net->add_batches[s.idx].data(), (int)net->add_batches[s.idx].size(),
-                                  clk, 0, net->stream, &net->add_tune[s.idx]);
+                                  clk, 0, net->stream,
+                                  (size_t)s.idx < net->add_tune.size() ? &net->add_tune[s.idx]
+                                                                       : nullptr);
       if (s.kind == 2) e = launch_proj_pre(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 3) e = launch_proj_post(net->projs[s.idx], clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 4) e = launch_pop_late_reset(net->pops[s.idx], clk, 0, net->stream);
@@ -1400,14 +1442,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 7)
         e = launch_small(net->sdev, net->pops[0].kind, net->pops[0].dtype, clk, 1, net->cfg.dt,
                          net->d_status, net->stream);
-      if (s.kind == 5) {  // the step's two launches, one after the other
-        e = launch_fused_step(net->fdev_d, net->pops[0].kind, net->pops[0].dtype,
-                              net->fused_dgrid, clk, 0, net->cfg.dt, net->d_status, net->stream);
-        if (e == cudaSuccess)
-          e = launch_fused_step(net->fdev_n, net->pops[0].kind, net->pops[0].dtype,
-                                net->fused_ngrid, clk, 0, net->cfg.dt, net->d_status,
-                                net->stream);
-      }
+      if (s.kind == 5)
+        e = launch_pending_delivery(net->fdev, net->pops[0].dtype, net->fused_dgrid, clk, 0,
+                                    net->stream);
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
       ++net->launches;
@@ -1427,7 +1464,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   }
   for (auto& e : ev) cudaEventDestroy(e);
   if (result == B2B_OK && net->fused) {
-    cudaError_t e = launch_fused_fold(net->fdev, net->pops[0].dtype, net->d_clock, -1, net->stream);
+    cudaError_t e = launch_fold_pending(net->fdev, net->pops[0].dtype, net->d_clock, -1, net->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
     if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile fold: %s", cudaGetErrorString(e));
   }
@@ -1490,8 +1527,7 @@ void set_fused_shape(b2b_net* net, int group, int grid) {
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
   net->fused_dgrid = grid > 0 ? grid : 2 * sms;
-  net->fdev_d.deliver_ctas = net->fused_dgrid;
-  net->fdev_d.group = group > 0 ? group : 8;
+  net->fdev.group = group > 0 ? group : 8;
   if (net->graph) {
     cudaGraphExecDestroy(net->graph);
     net->graph = nullptr;

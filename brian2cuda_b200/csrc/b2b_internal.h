@@ -23,11 +23,19 @@ constexpr int kNumSMs = 148;         // B200
 enum Kind { KIND_LIF = 1, KIND_HH = 2, KIND_POISSON = 3, KIND_SPIKEGEN = 4 };
 
 // Per-group parameters as the kernels read them (doubles; cast to the state type in-kernel).
+// TimedArray input of a group (b2b_timedarray): values[rows][cols] in the population's
+// dtype, one column for the whole group or one per neuron; step ts reads row
+// min(ts * mul / div, rows - 1).  val == NULL: no input.
+struct TimedInput {
+  const void* val;
+  int64_t rows, cols, mul, div;
+};
 struct LifDev {
   double A, Be, Bi, De, Di, El, Vt, Vr;   // exact propagator coefficients + threshold/reset
   int64_t ref_steps;                      // timestep(refractory, dt); -1 = no refractoriness
   int64_t offset, n;                      // group range inside the population
   int32_t has_threshold, has_reset, unless_refractory, pad;
+  TimedInput ta;                          // volts added to El over the step
 };
 // float32 copies of the HH constants (rounded on the host as the device would round them),
 // so a float32 update loads 4-byte values and converts nothing.
@@ -40,6 +48,7 @@ struct HhDev {
   int64_t offset, n;
   double inv_Cm;                          // 1/Cm (the float32 update multiplies by it)
   HhFloat f;
+  TimedInput ta;                          // amperes added to the membrane current
 };
 struct PoissonDev {
   double p_spike;                         // rate * dt
@@ -66,6 +75,9 @@ struct PopDev {
   int64_t sg_n;
   int32_t late_reset;             // reset must run after synaptic delivery
   int32_t pad;
+  // The step as two concurrent launches (fused.cu): per variable (v, ge, gi), [2][n] input
+  // delivered during the previous step, which the update adds in and clears (NULL: none).
+  void* fold[3];
 };
 
 // Device view of a projection (merged Synapses objects with one source population, one
@@ -137,14 +149,12 @@ struct RateMonDev {
   int64_t cap;
 };
 
-// Device view of the one-kernel-per-step path (fused.cu): one population and its additive
-// projections, whose targets are redirected to double-buffered input accumulators.
+// Device view of the delivery of the two-launch step (fused.cu): one population and its
+// additive projections, whose targets are redirected to double-buffered input accumulators.
 struct FusedDev {
   PopDev pop;
   ProjDev proj[kMaxProjBatch];
   int32_t n_proj, nd_max;
-  int32_t deliver_ctas;           // CTAs [0, deliver_ctas) deliver, the rest update neurons
-  int32_t neuron_ctas;
   void* acc[3];                   // per target variable (v, ge, gi): [2][pop.n] or NULL
   int32_t group;                  // delivery: lanes per work item (4, 8 or 16)
   int32_t pad_group;
@@ -174,6 +184,10 @@ struct Group {
   b2b_mlp* surr = nullptr;                    // gating surrogate (HH float32), or none
   double surr_tol = 0;
   int32_t surr_judge = 1;
+  // TimedArray input (b2b_timedarray): values row-major [ta_rows][ta_cols], row of step ts
+  // = min(ts * ta_mul / ta_div, ta_rows - 1)
+  std::vector<double> ta;
+  int64_t ta_rows = 0, ta_cols = 0, ta_mul = 1, ta_div = 1;
 };
 
 struct Pop {
@@ -288,12 +302,11 @@ struct b2b_net {
   b2b::SmallDev sdev{};
   bool fused = false;                      // the step as two concurrent launches (fused.cu)
   bool fused_ok = false;                   // the net allows them (their buffers exist)
+  // the step as two concurrent launches: the delivery into fdev's accumulators (on a second
+  // stream, fused_dgrid CTAs) and the update through fold_dev, ordered by events
   b2b::FusedDev fdev{};
-  int fused_grid = 0;
-  // the step as two concurrent launches: delivery-only and neuron-only views of fdev, the
-  // delivery on a second stream, ordered by events (see enqueue_steps)
-  b2b::FusedDev fdev_d{}, fdev_n{};
-  int fused_dgrid = 0, fused_ngrid = 0;
+  b2b::PopDev fold_dev{};                  // the population's view whose update folds acc in
+  int fused_dgrid = 0;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
   std::vector<void*> fused_allocs;
@@ -310,6 +323,9 @@ struct b2b_net {
 namespace b2b {
 cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
                             int32_t* status, cudaStream_t s);
+// The same with another device view of the population (its fold buffers set).
+cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t* clock, int k,
+                                double dt, int32_t* status, cudaStream_t s);
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k,
                                   cudaStream_t s);
 cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,
@@ -338,13 +354,10 @@ int mlp_device(const b2b_mlp* m);
 size_t small_smem(const SmallDev& D, int kind, int dtype);
 cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                          int steps, double dt, int32_t* status, cudaStream_t s);
-// One kernel per step (fused.cu): the step itself, and the fold of the pending input.
-size_t fused_smem(const FusedDev& F);
-int fused_block();
-int fused_resident_ctas(int kind, int dtype, const FusedDev& F, int sms);
-cudaError_t launch_fused_step(const FusedDev& F, int kind, int dtype, int grid,
-                              const int64_t* clock, int k, double dt, int32_t* status,
-                              cudaStream_t s);
-cudaError_t launch_fused_fold(const FusedDev& F, int dtype, const int64_t* clock, int k_last,
-                              cudaStream_t s);
+// The two-launch step (fused.cu): the delivery into the pending input of the step, and the
+// fold of the pending input at the end of a chunk.
+cudaError_t launch_pending_delivery(const FusedDev& F, int dtype, int grid,
+                                    const int64_t* clock, int k, cudaStream_t s);
+cudaError_t launch_fold_pending(const FusedDev& F, int dtype, const int64_t* clock, int k_last,
+                                cudaStream_t s);
 }  // namespace b2b

@@ -22,6 +22,29 @@
 namespace b2b {
 
 namespace {
+// Adds the input delivered during the previous step (fold buffer of variable v, parity
+// (ts-1) & 1) into pack X and returns the pack's address in the buffer, to be cleared after
+// the update's stores; no-op when the population has no fold buffer for v.
+template <typename R, int E>
+__device__ __forceinline__ R* fold_in(const PopDev& P, int v, int64_t ts, int64_t q,
+                                      Pack<R, E>& X) {
+  if (!P.fold[v]) return nullptr;
+  R* a = static_cast<R*>(P.fold[v]) + (int64_t)((ts & 1) ^ 1) * P.n;
+  const Pack<R, E> A = load_pack<R, E>(a, q);
+#pragma unroll
+  for (int e = 0; e < E; ++e) X.x[e] += A.x[e];
+  return a;
+}
+
+template <typename R, int E>
+__device__ __forceinline__ void fold_clear(R* a, int64_t q) {
+  if (!a) return;
+  Pack<R, E> z;
+#pragma unroll
+  for (int e = 0; e < E; ++e) z.x[e] = (R)0;
+  store_pack<R, E>(a, q, z);
+}
+
 // ---- LIF, exact integration ------------------------------------------------------------
 template <typename R, int E>
 __global__ void __launch_bounds__(kBlock)
@@ -44,13 +67,16 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     Pack<R, E> GI = load_pack<R, E>(P.var[B2B_VAR_GI], q);
     Pack<R, E> LS;
     if (refr) LS = load_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q);
+    R* fge = fold_in<R, E>(P, B2B_VAR_GE, ts, q, GE);
+    R* fgi = fold_in<R, E>(P, B2B_VAR_GI, ts, q, GI);
     uint32_t NRout = 0;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       R ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
-      R vn = lif_advance<R>(g, V.x[e], ge, gi, nr);
+      R vn = lif_advance<R>(g, V.x[e], ge, gi, nr,
+                            timed_input<R>(g.ta, ts, E * q + e - g.offset));
       GE.x[e] = ge;
       GI.x[e] = gi;
       const bool valid = (E * q + e - g.offset) < g.n;
@@ -70,6 +96,8 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       if (fl) store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);   // changes only on a spike
       store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
+    fold_clear<R, E>(fge, q);
+    fold_clear<R, E>(fgi, q);
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
@@ -100,12 +128,15 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     Pack<R, E> GI = load_pack<R, E>(P.var[B2B_VAR_GI], q);
     Pack<R, E> LS;
     if (refr) LS = load_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q);
+    R* fge = fold_in<R, E>(P, B2B_VAR_GE, ts, q, GE);
+    R* fgi = fold_in<R, E>(P, B2B_VAR_GI, ts, q, GI);
     uint32_t NRout = 0;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
-      const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR);
+      const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR,
+                                 timed_input<R>(g.ta, ts, E * q + e - g.offset));
       const bool valid = (E * q + e - g.offset) < g.n;
       if (valid && vn > Vthr && nr) {
         nr = false;
@@ -125,6 +156,8 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       if (fl) store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);   // changes only on a spike
       store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
+    fold_clear<R, E>(fge, q);
+    fold_clear<R, E>(fgi, q);
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
@@ -178,13 +211,16 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     if (q < nthr) {
       const HhRun<R> g = hh_run(prm[cur.grp], R());
       const bool refr = g.ref_steps >= 0;
+      R* fge = fold_in<R, 4>(P, B2B_VAR_GE, ts, q, cur.GE);
+      R* fgi = fold_in<R, 4>(P, B2B_VAR_GI, ts, q, cur.GI);
       uint32_t NRout = 0;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         bool nr = true;
         if (refr) nr = timestep_of(t - (double)cur.LS.x[e], dt, inv_dt) >= g.ref_steps;
         const R vn = hh_advance<R>(g, cur.V.x[e], cur.M.x[e], cur.H.x[e], cur.N.x[e],
-                                   cur.GE.x[e], cur.GI.x[e], dtR);
+                                   cur.GE.x[e], cur.GI.x[e], dtR,
+                                   timed_input<R>(g.ta, ts, 4 * q + e - g.offset));
         const bool valid = (4 * q + e - g.offset) < g.n;
         if (valid && vn > (R)g.Vthr && nr) {
           nr = false;
@@ -204,6 +240,8 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
         if (fl) store_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q, cur.LS);   // changes on a spike
         store_flags<4>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
       }
+      fold_clear<R, 4>(fge, q);
+      fold_clear<R, 4>(fgi, q);
     }
     emit_spikes<4>(P, q, fl, ts, slot, status);
     cur = nxt;
@@ -298,9 +336,8 @@ __global__ void lif_late_reset_kernel(PopDev P, const int64_t* __restrict__ cloc
 bool wide(int64_t n) { return n / 4 >= (int64_t)kNumSMs * 4 * kBlock; }
 
 template <int E>
-cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int32_t* status,
-                     cudaStream_t s) {
-  const PopDev& P = pop.dev;
+cudaError_t launch_e(const Pop& pop, const PopDev& P, const int64_t* clock, int k, double dt,
+                     int32_t* status, cudaStream_t s) {
   const int block = pop.tune_block > 0 ? pop.tune_block : kBlock;   // <= kBlock
   const unsigned grid = (unsigned)((P.n / E + block - 1) / block);
   const bool f32 = pop.dtype == B2B_F32;
@@ -335,14 +372,19 @@ cudaError_t launch_e(const Pop& pop, const int64_t* clock, int k, double dt, int
 
 cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double dt,
                             int32_t* status, cudaStream_t s) {
+  return launch_pop_step_dev(pop, pop.dev, clock, k, dt, status, s);
+}
+
+cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t* clock, int k,
+                                double dt, int32_t* status, cudaStream_t s) {
   if (pop.kind == KIND_HH && pop.surr_img) return launch_hh_surrogate(pop, clock, k, dt, status, s);
   if (pop.kind == KIND_SPIKEGEN) {
     spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
     return cudaGetLastError();
   }
   const bool four = pop.tune_e > 0 ? pop.tune_e == 4 : wide(pop.dev.n);
-  return four ? launch_e<4>(pop, clock, k, dt, status, s)
-              : launch_e<1>(pop, clock, k, dt, status, s);
+  return four ? launch_e<4>(pop, dev, clock, k, dt, status, s)
+              : launch_e<1>(pop, dev, clock, k, dt, status, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -1,5 +1,5 @@
-// Per-neuron update arithmetic shared by the per-step kernels (neuron.cu) and the
-// persistent multi-step kernel (fused.cu), so both evaluate exactly the same expressions.
+// Per-neuron update arithmetic shared by the per-step kernels (neuron.cu) and the one-CTA
+// kernel for small networks (small.cu), so both evaluate exactly the same expressions.
 #pragma once
 #include "kernels_common.cuh"
 
@@ -13,12 +13,14 @@ __device__ __forceinline__ int64_t timestep_of(double t, double dt, double inv_d
   return (int64_t)((t + 1e-3 * dt) * inv_dt);
 }
 
-// Exact propagator of dv/dt = (El - v + ke ge + ki gi)/taum, dge/dt = -ge/taue,
-// dgi/dt = -gi/taui over one dt (coefficients prepared on the host, LifDev).  Returns the new
-// v; advances ge and gi in place.
+// Exact propagator of dv/dt = (El + u - v + ke ge + ki gi)/taum, dge/dt = -ge/taue,
+// dgi/dt = -gi/taui over one dt (coefficients prepared on the host, LifDev), u held constant
+// over the step.  Returns the new v; advances ge and gi in place.
 template <typename R>
-__device__ __forceinline__ R lif_advance(const LifDev& g, R v, R& ge, R& gi, bool nr) {
-  R vn = dfma((R)g.Bi, gi, dfma((R)g.Be, ge, dfma((R)g.A, v - (R)g.El, (R)g.El)));
+__device__ __forceinline__ R lif_advance(const LifDev& g, R v, R& ge, R& gi, bool nr,
+                                         R u = R(0)) {
+  const R El = (R)g.El + u;   // u: TimedArray input (volts), constant over the step
+  R vn = dfma((R)g.Bi, gi, dfma((R)g.Be, ge, dfma((R)g.A, v - El, El)));
   if (g.unless_refractory && !nr) vn = v;
   ge = (R)g.De * ge;
   gi = (R)g.Di * gi;
@@ -95,15 +97,30 @@ template <typename R>
 struct HhRun {
   R Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr, inv_Cm;
   int64_t ref_steps, offset, n;
+  TimedInput ta;
 };
 __device__ __forceinline__ HhRun<float> hh_run(const HhDev& g, float) {
   const HhFloat& f = g.f;
   return {f.Cm, f.gl, f.El, f.EK, f.ENa, f.gNa, f.gK, f.VT, f.Ee, f.Ei, f.De, f.Di, f.Vthr,
-          f.inv_Cm, g.ref_steps, g.offset, g.n};
+          f.inv_Cm, g.ref_steps, g.offset, g.n, g.ta};
 }
 __device__ __forceinline__ HhRun<double> hh_run(const HhDev& g, double) {
   return {g.Cm, g.gl, g.El, g.EK, g.ENa, g.gNa, g.gK, g.VT, g.Ee, g.Ei, g.De, g.Di, g.Vthr,
-          g.inv_Cm, g.ref_steps, g.offset, g.n};
+          g.inv_Cm, g.ref_steps, g.offset, g.n, g.ta};
+}
+
+// TimedArray input of a group at step ts for its neuron `local` (the role of the function
+// brian2cuda/timedarray.py:10-58 generates: the array's time step holding t, clamped to the
+// last row; one column for the whole group, or one per neuron).  The row is computed from
+// the integer step, since the time grids are aligned (b2b_timedarray checks it).  Padding
+// neurons past the group's end read its last column; their results are never used.
+template <typename R>
+__device__ __forceinline__ R timed_input(const TimedInput& ta, int64_t ts, int64_t local) {
+  if (!ta.val) return (R)0;
+  int64_t row = ts * ta.mul / ta.div;
+  if (row >= ta.rows) row = ta.rows - 1;
+  const int64_t col = ta.cols == 1 ? 0 : (local < ta.cols ? local : ta.cols - 1);
+  return __ldg(static_cast<const R*>(ta.val) + row * ta.cols + col);
 }
 
 // 1/Cm (float32, from the group's precomputed reciprocal) or division by Cm (float64).
@@ -112,14 +129,15 @@ __device__ __forceinline__ double per_cm(double x, const HhRun<double>& g) { ret
 
 // Membrane part of the COBAHH update: exponential Euler for v with the conductances of the
 // gating state at the start of the step.  Returns the new v.
+// I: external current (amperes) over the step, from a TimedArray.
 template <typename R>
 __device__ __forceinline__ R hh_membrane(const HhRun<R>& g, R v, R m, R h, R n, R ge, R gi,
-                                         R dt) {
+                                         R dt, R I = R(0)) {
   const R gl = (R)g.gl;
   const R gna = (R)g.gNa * (m * m * m) * h;
   const R gk = (R)g.gK * (n * n * n * n);
   const R Av = -per_cm(gl + ge + gi + gna + gk, g);
-  const R Bv = per_cm(gl * (R)g.El + ge * (R)g.Ee + gi * (R)g.Ei + gna * (R)g.ENa + gk * (R)g.EK, g);
+  const R Bv = per_cm(gl * (R)g.El + ge * (R)g.Ee + gi * (R)g.Ei + gna * (R)g.ENa + gk * (R)g.EK + I, g);
   return expeuler(v, Av, Bv, dt);
 }
 
@@ -127,8 +145,8 @@ __device__ __forceinline__ R hh_membrane(const HhRun<R>& g, R v, R m, R h, R n, 
 // Returns the new v; advances m, h, n, ge, gi in place.
 template <typename R>
 __device__ __forceinline__ R hh_advance(const HhRun<R>& g, R v, R& m, R& h, R& n, R& ge, R& gi,
-                                        R dt) {
-  const R vn = hh_membrane<R>(g, v, m, h, n, ge, gi, dt);
+                                        R dt, R I = R(0)) {
+  const R vn = hh_membrane<R>(g, v, m, h, n, ge, gi, dt, I);
   hh_gating<R>((R)g.VT, v, m, h, n, dt);
   ge = (R)g.De * ge;
   gi = (R)g.Di * gi;

@@ -232,6 +232,18 @@ class Network:
                                                  C.byref(gid)), "spikegen")
         return self._add("spikegen", n, N.F32, gid)
 
+    def timed_array(self, gid: int, values, dt_array: float) -> None:
+        """TimedArray input of a LIF or HH group (the role of brian2cuda/timedarray.py): values
+        (rows,) for the whole group or (rows, n) per neuron, each row held for dt_array
+        seconds, the last row after the end.  LIF: volts added to El,
+        dv/dt = (El + I(t) - v + ...)/taum; HH: amperes, Cm dv/dt = ... + I(t)."""
+        v = np.asarray(values, dtype=np.float64)
+        v = np.ascontiguousarray(v[:, None] if v.ndim == 1 else v)
+        if v.ndim != 2:
+            raise ValueError("values must be (rows,) or (rows, n)")
+        self._check(self._lib.b2b_timedarray(self._h, gid, _ptr(v), v.shape[0], v.shape[1],
+                                             float(dt_array)), "timed_array")
+
     def group_size(self, gid: int) -> int:
         return self._groups[gid][1]
 
@@ -406,7 +418,8 @@ class Network:
     def profile(self, steps: int) -> list[tuple[int, float]]:
         """Advances `steps` steps with every launch timed; returns (site kind, mean ms) per
         launch site (1 population, 6 additive on_pre delivery launch, 2 STDP on_pre delivery,
-        3 on_post delivery, 4 late reset, 5 one-kernel step, 7 one-CTA step)."""
+        3 on_post delivery, 4 late reset, 5 delivery into the pending input of the two-launch
+        step, 7 one-CTA step, 9 state monitors, 10 rate monitors)."""
         cap = 256
         ms = (C.c_double * cap)()
         kinds = (C.c_int32 * cap)()

@@ -133,6 +133,19 @@ b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate
 b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const int32_t* idx,
                               const int64_t* step, int32_t* gid);
 
+/* TimedArray input of a LIF or HH group (replaces the function brian2cuda/timedarray.py:
+ * 10-58 generates for `ta(t)` / `ta(t, i)` in the group's equations).  values[rows][cols]
+ * (row-major float64, converted to the group's dtype) are sampled every dt_array seconds and
+ * held over each interval: step ts reads row floor(ts * dt / dt_array), clamped to rows - 1.
+ * cols = 1: one value for the whole group; cols = n: one per neuron.  The value I enters
+ *     LIF: dv/dt = (El + I - v + ke*ge + ki*gi)/taum     (I in volts)
+ *     HH:  Cm dv/dt = ... + I                           (I in amperes)
+ * dt_array must be an integer multiple or an integer fraction of the net's dt (aligned time
+ * grids).  Before b2b_finalize; a later call for the same group replaces the array.  Not
+ * combinable with the gating surrogate. */
+b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64_t rows,
+                          int64_t cols, double dt_array);
+
 /* State variables of a group.  Values are in the group's dtype; NOT_REFRACTORY is uint8. */
 enum {
   B2B_VAR_V = 0, B2B_VAR_GE = 1, B2B_VAR_GI = 2, B2B_VAR_M = 3, B2B_VAR_H = 4, B2B_VAR_N = 5,
@@ -242,9 +255,9 @@ b2b_status b2b_restore(b2b_net* net, int32_t slot);
 b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
 b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
-/* How b2b_run advances the net (after b2b_finalize): *mode = 1 for one kernel per step
- * (B2B_NET_FUSED), 2 for a small network run by one CTA per chunk of steps, 0 for per-step
- * kernels replayed from CUDA graphs. */
+/* How b2b_run advances the net (after b2b_finalize): *mode = 1 for every step as two
+ * concurrent launches (B2B_NET_FUSED, or chosen automatically), 2 for a small network run by
+ * one CTA per chunk of steps, 0 for per-step kernels replayed from CUDA graphs. */
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
@@ -255,10 +268,11 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * projections that share a kernel variant are delivered by one launch, with its tuned
  * shape), one per STDP projection's on_pre delivery (kind 2), one per STDP projection's
  * on_post delivery (kind 3), one per population with a deferred reset (kind 4), the rate
- * monitors (kind 10, one launch for all); or, when the net runs one kernel per step
- * (b2b_run_mode 1), that
- * kernel alone (kind 5); or, for a small network run by one CTA (b2b_run_mode 2), that kernel
- * advancing one step (kind 7).  *n_sites receives the number of sites (<= cap filled). */
+ * monitors (kind 10, one launch for all); or, when the net runs every step as two
+ * concurrent launches (b2b_run_mode 1), the delivery into the pending input (kind 5) and the
+ * neuron update folding it in (kind 1), launched one after the other; or, for a small network
+ * run by one CTA (b2b_run_mode 2), that kernel advancing one step (kind 7).  *n_sites receives the number
+ * of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
 
@@ -272,15 +286,18 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
  * (4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM); STDP projections: the order of the synapse
  * records (0 synapse order, 1 grouped by postsynaptic neuron, where on_post reads contiguous
  * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
- * through the order).  Afterwards the state, clock and monitor counts are as before the call,
+ * through the order); a net that can run every step as two concurrent launches: the pending
+ * delivery's lanes per item x CTAs (kind 5), then the form itself (kind 11: 1 two launches,
+ * 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
  * and the next b2b_run captures its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
  * rule) to be chosen.  A choice of 0 means the built-in rule won.  The trials should cover a
  * representative stretch of the run (bursts included). */
 typedef struct {
-  int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records     */
+  int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records,
+                            5 pending delivery of the two-launch step, 11 step form     */
   int32_t site_index;    /* population / delivery launch / projection index              */
   int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item /
-                            record order                                                  */
+                            record order / step form                                      */
   int32_t choice_b;      /* threads per CTA / CTAs                                       */
   double best_ms;        /* mean device time of one whole step with the chosen shape     */
   double default_ms;     /* the same with the built-in rule                              */

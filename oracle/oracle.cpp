@@ -110,6 +110,16 @@ struct Group {
   std::vector<std::vector<R>> uniforms;         // Poisson: queued rows, one per step
   size_t uni_next = 0;
   std::vector<std::pair<int64_t, int32_t>> recorded;  // (step, idx)
+  // TimedArray input (brian2cuda/timedarray.py:10-58): values [rows][cols] held over each
+  // interval of the array's dt; step ts reads row min(ts * mul / div, rows - 1), the
+  // interval holding t = ts dt on aligned time grids; one column or one per neuron.
+  std::vector<R> ta;
+  int64_t ta_rows = 0, ta_cols = 0, ta_mul = 1, ta_div = 1;
+  R input(int64_t ts, int64_t i) const {
+    if (ta.empty()) return (R)0;
+    const int64_t row = std::min(ts * ta_mul / ta_div, ta_rows - 1);
+    return ta[row * ta_cols + (ta_cols == 1 ? 0 : i)];
+  }
   double refractory() const {
     if (kind == LIF) return p[8];
     if (kind == HH) return p[13];
@@ -197,8 +207,10 @@ void build_syn(Net<R>& net, Syn<R>& s) {
 }
 
 // ---- one step -------------------------------------------------------------------------------
+// dv/dt = (El + u - v + ke ge + ki gi)/taum with u the TimedArray input, constant over the
+// step: the exact propagator with El + u in place of El.
 template <typename R>
-void update_lif(Group<R>& g, double t, double dt) {
+void update_lif(Group<R>& g, int64_t ts, double t, double dt) {
   const double El = g.p[0], taum = g.p[1], taue = g.p[2], taui = g.p[3], ke = g.p[4], ki = g.p[5];
   const bool leak = std::isfinite(taum) && taum > 0;
   const double A = leak ? std::exp(-dt / taum) : 1.0;
@@ -219,7 +231,8 @@ void update_lif(Group<R>& g, double t, double dt) {
     bool nr = true;
     if (ref_steps >= 0) nr = timestep(t - (double)g.var[LASTSPIKE][i], dt) >= ref_steps;
     const R v = g.var[V][i], ge = g.var[GE][i], gi = g.var[GI][i];
-    R vn = xfma(rBi, gi, xfma(rBe, ge, xfma(rA, (R)(v - rEl), rEl)));
+    const R El_u = rEl + g.input(ts, i);
+    R vn = xfma(rBi, gi, xfma(rBe, ge, xfma(rA, (R)(v - El_u), El_u)));
     if (unless && !nr) vn = v;
     g.var[V][i] = vn;
     g.var[GE][i] = rDe * ge;
@@ -234,8 +247,9 @@ R expeuler(R x, R A, R B, R dt) {
   return -BA + (BA + x) * xexp(A * dt);
 }
 
+// The TimedArray input enters as an external current: Cm dv/dt = ... + I.
 template <typename R>
-void update_hh(Group<R>& g, double t, double dt) {
+void update_hh(Group<R>& g, int64_t ts, double t, double dt) {
   const R Cm = (R)g.p[0], gl = (R)g.p[1], El = (R)g.p[2], EK = (R)g.p[3], ENa = (R)g.p[4];
   const R gNa = (R)g.p[5], gK = (R)g.p[6], VT = (R)g.p[7], Ee = (R)g.p[8], Ei = (R)g.p[9];
   const R De = (R)std::exp(-dt / g.p[10]), Di = (R)std::exp(-dt / g.p[11]);
@@ -258,7 +272,7 @@ void update_hh(Group<R>& g, double t, double dt) {
     const R gna = gNa * (m * m * m) * h;
     const R gk = gK * (n * n * n * n);
     const R Av = -(gl + ge + gi + gna + gk) / Cm;
-    const R Bv = (gl * El + ge * Ee + gi * Ei + gna * ENa + gk * EK) / Cm;
+    const R Bv = (gl * El + ge * Ee + gi * Ei + gna * ENa + gk * EK + g.input(ts, i)) / Cm;
     g.var[V][i] = expeuler(v, Av, Bv, dtR);
     g.var[M][i] = expeuler(m, -(am + bm), am, dtR);
     g.var[H][i] = expeuler(h, -(ah + bh), ah, dtR);
@@ -375,8 +389,8 @@ bool step(Net<R>& net) {
       m.vals.push_back(m.var == NOT_REF ? (double)g.not_ref[i] : (double)g.var[m.var][i]);
   }
   for (Group<R>& g : net.groups) {
-    if (g.kind == LIF) update_lif(g, t, net.dt);
-    else if (g.kind == HH) update_hh(g, t, net.dt);
+    if (g.kind == LIF) update_lif(g, net.ts, t, net.dt);
+    else if (g.kind == HH) update_hh(g, net.ts, t, net.dt);
   }
   for (Group<R>& g : net.groups)
     if (!threshold(net, g, t)) return false;
@@ -617,6 +631,22 @@ int api_spikegen(Net<R>& net, int64_t n, int64_t ns, const int32_t* idx, const i
   for (int64_t k = 0; k < ns; ++k) g.sg.emplace_back(st[k], idx[k]);
   std::sort(g.sg.begin(), g.sg.end());
   return add_group(net, std::move(g));
+}
+
+template <typename R>
+int api_timedarray(Net<R>& net, int gid, const double* vals, int64_t rows, int64_t cols,
+                   int64_t mul, int64_t div) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  Group<R>& g = net.groups[gid];
+  if ((g.kind != LIF && g.kind != HH) || rows < 1 || (cols != 1 && cols != g.n) || mul < 1 ||
+      div < 1)
+    return -1;
+  g.ta.assign(vals, vals + rows * cols);   // rounded to R once, as the device copy is
+  g.ta_rows = rows;
+  g.ta_cols = cols;
+  g.ta_mul = mul;
+  g.ta_div = div;
+  return 0;
 }
 
 template <typename R>
@@ -888,6 +918,12 @@ int orc_group_poisson(void* hp, int64_t n, double rate) {
 int orc_group_spikegen(void* hp, int64_t n, int64_t ns, const int32_t* idx, const int64_t* st) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_spikegen, n, ns, idx, st);
+}
+// TimedArray: values [rows][cols], step ts reads row min(ts * mul / div, rows - 1)
+int orc_timedarray(void* hp, int gid, const double* v, int64_t rows, int64_t cols, int64_t mul,
+                   int64_t div) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_timedarray, gid, v, rows, cols, mul, div);
 }
 int orc_state_set(void* hp, int gid, int var, const double* v, int64_t n) {
   Handle* h = static_cast<Handle*>(hp);

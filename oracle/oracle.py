@@ -45,6 +45,7 @@ def lib() -> C.CDLL:
             "orc_group_hh": (C.c_int, [P, I64, P]),
             "orc_group_poisson": (C.c_int, [P, I64, D]),
             "orc_group_spikegen": (C.c_int, [P, I64, I64, P, P]),
+            "orc_timedarray": (C.c_int, [P, C.c_int, P, I64, I64, I64, I64]),
             "orc_state_set": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_state_get": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_synapses": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, I64, P, P, P, D, P,
@@ -138,6 +139,16 @@ class OracleNet:
         st = np.ascontiguousarray(steps, dtype=np.int64)
         return self._add("spikegen", n,
                          self._lib.orc_group_spikegen(self._h, n, len(idx), _p(idx), _p(st)))
+
+    def timed_array(self, gid, values, dt_array):
+        """TimedArray input of a LIF (volts) or HH (amperes) group: values (rows,) for the
+        whole group or (rows, n) per neuron, each row held for dt_array seconds."""
+        v = np.asarray(values, dtype=np.float64)
+        v = np.ascontiguousarray(v[:, None] if v.ndim == 1 else v)
+        r = float(dt_array) / self.dt
+        mul, div = (1, int(round(r))) if r >= 1 else (int(round(1 / r)), 1)
+        self._ok(self._lib.orc_timedarray(self._h, gid, _p(v), v.shape[0], v.shape[1], mul, div),
+                 "timed_array")
 
     def group_size(self, gid):
         return self._sizes[gid]

@@ -409,6 +409,36 @@ def test_fused_and_per_step_paths_agree(gpu_factory):
     _close(res[True][3], res[False][3], 1e-10, 1e-15)
 
 
+def test_profile_advances_like_run(gpu_factory):
+    """The profiling run launches every kernel eagerly and times it; in either form of the
+    step it reports the form's launch sites and leaves the net where b2b_run would."""
+    for fused in (True, False):
+        out = {}
+        for how in ("run", "profile"):
+            net = gpu_factory(DT, fused=fused)
+            G, Ce, Ci, _ = _delay_net(net, n=1000)
+            net.finalize()
+            net.run(40)
+            if how == "run":
+                net.run(130)
+            else:
+                prof = net.profile(130)
+                kinds = [k for k, _ in prof]
+                # per-step: Ce (a weight per synapse) and Ci (one scalar weight) are two
+                # kernel variants, so two delivery launches
+                assert kinds == ([5, 1] if fused else [1, 6, 6]), kinds
+                assert all(ms > 0 for _, ms in prof)
+            assert net.timestep == 170
+            net.run(30)
+            idx, st = net.spikes(G)
+            out[how] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
+        assert len(out["run"][0]) > 50
+        for k in (0, 1, 4):
+            np.testing.assert_array_equal(out["profile"][k], out["run"][k])
+        _close(out["profile"][2], out["run"][2], 1e-12, 1e-15)
+        _close(out["profile"][3], out["run"][3], 1e-12, 1e-15)
+
+
 def _spikes_within_one_step(a_idx, a_stp, b_idx, b_stp):
     """Fraction of spikes of a that b has at the same neuron within one step."""
     keys = set(zip(b_idx.tolist(), b_stp.tolist()))
