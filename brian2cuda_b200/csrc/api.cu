@@ -236,8 +236,10 @@ b2b_status finalize_pops(b2b_net* net) {
         D.var[v] = d;
       }
     }
-    // parameters, with each group's TimedArray input in the population's dtype
+    // parameters, and the groups' inputs (TimedArray tables in the population's dtype,
+    // PoissonInputs) in an array of their own
     std::vector<uint8_t> prm;
+    std::vector<GroupInputs> gins;
     for (int gi : pop.groups) {
       const Group& g = net->groups[gi];
       TimedInput ta{};
@@ -249,13 +251,17 @@ b2b_status finalize_pops(b2b_net* net) {
         CU(cudaMemcpy(d, host.data(), host.size(), cudaMemcpyHostToDevice));
         ta = TimedInput{d, g.ta_rows, g.ta_cols, g.ta_mul, g.ta_div};
       }
+      pop.inputs = pop.inputs || !g.ta.empty() || !g.pins.empty();
+      PoissonInputs pin{};
+      pin.count = (int32_t)g.pins.size();
+      pin.after_reset = (net->cfg.flags & B2B_NET_RESET_BEFORE_SYNAPSES) ? 1 : 0;
+      for (size_t k = 0; k < g.pins.size(); ++k) pin.in[k] = g.pins[k];
+      gins.push_back(GroupInputs{ta, pin});
       if (pop.kind == KIND_LIF) {
         LifDev d = lif_dev(g, dt);
-        d.ta = ta;
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       } else if (pop.kind == KIND_HH) {
         HhDev d = hh_dev(g, dt);
-        d.ta = ta;
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       } else if (pop.kind == KIND_POISSON) {
         PoissonDev d{g.rate * dt, g.offset, g.n};
@@ -266,6 +272,12 @@ b2b_status finalize_pops(b2b_net* net) {
       CU(dalloc(pop, (uint8_t**)&pop.params_dev, prm.size()));
       CU(cudaMemcpy(pop.params_dev, prm.data(), prm.size(), cudaMemcpyHostToDevice));
       D.params = pop.params_dev;
+    }
+    if (pop.inputs) {
+      GroupInputs* d = nullptr;
+      CU(dalloc(pop, &d, gins.size()));
+      CU(cudaMemcpy(d, gins.data(), sizeof(GroupInputs) * gins.size(), cudaMemcpyHostToDevice));
+      D.inputs = d;
     }
     // gating surrogate: every HH group of a float32 population shares one network
     if (pop.kind == KIND_HH) {
@@ -278,8 +290,10 @@ b2b_status finalize_pops(b2b_net* net) {
               B2B_ERR_UNSUPPORTED, "HH groups of one population must share one surrogate");
       }
       for (int gi : pop.groups)
-        CHECK(!any || net->groups[gi].ta.empty(), B2B_ERR_UNSUPPORTED,
-              "a TimedArray input and the gating surrogate cannot drive one population");
+        CHECK(!any || (net->groups[gi].ta.empty() && net->groups[gi].pins.empty()),
+              B2B_ERR_UNSUPPORTED,
+              "TimedArray and PoissonInput inputs cannot drive a population with the gating "
+              "surrogate");
       if (any) {
         CHECK(pop.dtype == B2B_F32, B2B_ERR_UNSUPPORTED, "the gating surrogate is float32 only");
         CHECK(mlp_device(g0.surr) == net->cfg.device, B2B_ERR_INVALID_ARG,
@@ -700,6 +714,8 @@ b2b_status setup_small(b2b_net* net) {
   const Pop& pop = net->pops[0];
   if ((pop.kind != KIND_LIF && pop.kind != KIND_HH) || pop.surr_img || pop.n > 4096)
     return B2B_OK;
+  for (int gi : pop.groups)
+    if (!net->groups[gi].pins.empty()) return B2B_OK;   // the one-CTA kernel draws none
   SmallDev& D = net->sdev;
   D = SmallDev{};
   D.pop = pop.dev;
@@ -1104,6 +1120,42 @@ b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const i
           ent[k].second, (long long)ent[k].first);
   for (auto& e : ent) { g.sg_step.push_back(e.first); g.sg_idx.push_back(e.second); }
   return add_group(net, std::move(g), gid);
+  GUARD_END
+}
+
+b2b_status b2b_poisson_input(b2b_net* net, int32_t gid, int32_t var, int64_t n_inputs,
+                             double rate_hz, double weight, int32_t* pid) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "PoissonInputs must be added before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  Group& g = net->groups[gid];
+  CHECK(g.kind == KIND_LIF || g.kind == KIND_HH, B2B_ERR_INVALID_ARG,
+        "a PoissonInput targets a LIF or HH group");
+  CHECK(var == B2B_VAR_V || var == B2B_VAR_GE || var == B2B_VAR_GI, B2B_ERR_INVALID_ARG,
+        "a PoissonInput targets v, ge or gi");
+  CHECK((int)g.pins.size() < kMaxPoissonInputs, B2B_ERR_UNSUPPORTED,
+        "at most %d PoissonInputs per group", kMaxPoissonInputs);
+  const double p = rate_hz * net->cfg.dt;
+  CHECK(n_inputs >= 0 && std::isfinite(p) && p >= 0 && p <= 1 && std::isfinite(weight),
+        B2B_ERR_INVALID_ARG, "bad PoissonInput (N %lld, rate*dt %g)", (long long)n_inputs, p);
+  GUARD_BEGIN
+  PoissonIn in{};
+  in.n = n_inputs;
+  in.reverse = p > 0.5 ? 1 : 0;
+  const double pp = in.reverse ? 1.0 - p : p;
+  const double q = 1.0 - pp;
+  in.qn = std::pow(q, (double)n_inputs);
+  in.s = q > 0 ? pp / q : 0.0;
+  in.a = (double)(n_inputs + 1) * in.s;
+  in.weight = weight;
+  in.var = var;
+  in.id = (uint32_t)net->n_pins;
+  in.k0 = (uint32_t)net->cfg.seed;
+  in.k1 = (uint32_t)(net->cfg.seed >> 32) ^ 0xB1A0u;
+  g.pins.push_back(in);
+  if (pid) *pid = net->n_pins;
+  ++net->n_pins;
+  return B2B_OK;
   GUARD_END
 }
 

@@ -30,12 +30,33 @@ struct TimedInput {
   const void* val;
   int64_t rows, cols, mul, div;
 };
+// PoissonInput of a group (b2b_poisson_input): every step each neuron adds weight * X to
+// variable `var`, X ~ Binomial(n, p) drawn by inversion (neuron_math.cuh) from one Philox
+// word of counter (group-local index, step low, step high, id), key (k0, k1).  qn = q^n,
+// s = p/q, a = (n + 1) s with p = min(rate dt, 1 - rate dt) (reverse: X = n - draw).
+constexpr int kMaxPoissonInputs = 2;
+struct PoissonIn {
+  int64_t n;
+  double qn, s, a, weight;
+  int32_t var, reverse;
+  uint32_t id, k0, k1, pad;
+};
+struct PoissonInputs {
+  int32_t count;
+  int32_t after_reset;                    // the schedule resets before the synapses slot
+  PoissonIn in[kMaxPoissonInputs];
+};
+// Inputs of one group, in an array beside the groups' parameters (PopDev::inputs) so that
+// the parameters keep their size and populations without inputs never read it.
+struct GroupInputs {
+  TimedInput ta;                          // LIF: volts added to El; HH: amperes
+  PoissonInputs pin;
+};
 struct LifDev {
   double A, Be, Bi, De, Di, El, Vt, Vr;   // exact propagator coefficients + threshold/reset
   int64_t ref_steps;                      // timestep(refractory, dt); -1 = no refractoriness
   int64_t offset, n;                      // group range inside the population
   int32_t has_threshold, has_reset, unless_refractory, pad;
-  TimedInput ta;                          // volts added to El over the step
 };
 // float32 copies of the HH constants (rounded on the host as the device would round them),
 // so a float32 update loads 4-byte values and converts nothing.
@@ -48,7 +69,6 @@ struct HhDev {
   int64_t offset, n;
   double inv_Cm;                          // 1/Cm (the float32 update multiplies by it)
   HhFloat f;
-  TimedInput ta;                          // amperes added to the membrane current
 };
 struct PoissonDev {
   double p_spike;                         // rate * dt
@@ -60,6 +80,7 @@ struct PopDev {
   void* var[kMaxVars];            // SoA state, NOT_REFRACTORY as uint8
   const void* params;             // LifDev/HhDev/PoissonDev[n_groups]
   const int32_t* vec_group;       // group id per 4-neuron vector (NULL when one group)
+  const GroupInputs* inputs;      // [n_groups] TimedArray / PoissonInput inputs, or NULL
   int64_t n;                      // padded neuron count (multiple of kPad)
   int32_t n_groups;
   int32_t ring_len;               // spike history slots (>= max delay + 2)
@@ -188,6 +209,7 @@ struct Group {
   // = min(ts * ta_mul / ta_div, ta_rows - 1)
   std::vector<double> ta;
   int64_t ta_rows = 0, ta_cols = 0, ta_mul = 1, ta_div = 1;
+  std::vector<PoissonIn> pins;                // PoissonInputs (b2b_poisson_input)
 };
 
 struct Pop {
@@ -201,6 +223,7 @@ struct Pop {
   int64_t rng_steps = 0;          // rows held by the uniform buffer
   void* rng_buf = nullptr;
   bool late_reset = false;
+  bool inputs = false;            // some group has a TimedArray or PoissonInput input
   int max_delay = 0;
   // gating surrogate of a float32 HH population (surrogate.cu), or none
   const void* surr_img = nullptr;
@@ -291,6 +314,7 @@ struct b2b_net {
   std::vector<b2b::Syn> syns;
   std::vector<b2b::Proj> projs;
   std::vector<std::vector<const b2b::Proj*>> add_batches;  // additive projections per launch
+  int32_t n_pins = 0;                      // PoissonInputs added (their Philox stream ids)
   std::vector<b2b::AddTune> add_tune;      // launch shape per add batch (b2b_autotune)
   std::vector<b2b::StateMon> smons;        // state monitors, recorded at the start of a step
   std::vector<b2b::RateMon> rmons;         // rate monitors, recorded at the end of a step

@@ -46,7 +46,8 @@ __device__ __forceinline__ void fold_clear(R* a, int64_t q) {
 }
 
 // ---- LIF, exact integration ------------------------------------------------------------
-template <typename R, int E>
+// INPUTS: the population has TimedArray or PoissonInput inputs (compiled out otherwise).
+template <typename R, int E, bool INPUTS>
 __global__ void __launch_bounds__(kBlock)
 lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                 int32_t* status) {
@@ -59,7 +60,10 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   unsigned fl = 0;
   if (q < nthr) {
     const LifDev* prm = static_cast<const LifDev*>(P.params);
-    const LifDev g = prm[group_of<E>(P, q)];
+    const int grp = group_of<E>(P, q);
+    const LifDev g = prm[grp];
+    const GroupInputs* gin = INPUTS ? P.inputs + grp : nullptr;
+    const bool after_reset = INPUTS && gin->pin.after_reset;
     const R Vt = (R)g.Vt, Vr = (R)g.Vr;
     const bool refr = g.ref_steps >= 0;
     Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
@@ -76,16 +80,24 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
       R vn = lif_advance<R>(g, V.x[e], ge, gi, nr,
-                            timed_input<R>(g.ta, ts, E * q + e - g.offset));
+                            INPUTS ? timed_input<R>(gin->ta, ts, E * q + e - g.offset) : R(0));
       GE.x[e] = ge;
       GI.x[e] = gi;
-      const bool valid = (E * q + e - g.offset) < g.n;
+      const int64_t local = E * q + e - g.offset;
+      const bool valid = local < g.n;
+      bool reset_now = false;
       if (g.has_threshold && valid && vn > Vt && nr) {
         nr = false;
         if (refr) LS.x[e] = (R)t;
-        if (g.has_reset && !P.late_reset) vn = Vr;
+        reset_now = g.has_reset && !P.late_reset;
         fl |= 1u << e;
       }
+      // PoissonInputs act in the synapses slot: after the threshold, and before the reset
+      // unless the schedule resets first
+      if (reset_now && after_reset) vn = Vr;
+      if (INPUTS && gin->pin.count && valid)
+        add_poisson_inputs<R>(gin->pin, ts, local, vn, GE.x[e], GI.x[e]);
+      if (reset_now && !after_reset) vn = Vr;
       V.x[e] = vn;
       NRout |= (nr ? 1u : 0u) << (8 * e);
     }
@@ -104,7 +116,7 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 }
 
 // ---- Hodgkin-Huxley (COBAHH), exponential Euler (hh_advance) ------------------------
-template <typename R, int E>
+template <typename R, int E, bool INPUTS>
 __global__ void __launch_bounds__(kBlock)
 hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                int32_t* status) {
@@ -117,7 +129,9 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   unsigned fl = 0;
   if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
-    const HhRun<R> g = hh_run(prm[group_of<E>(P, q)], R());
+    const int grp = group_of<E>(P, q);
+    const HhRun<R> g = hh_run(prm[grp], R());
+    const GroupInputs* gin = INPUTS ? P.inputs + grp : nullptr;
     const R Vthr = (R)g.Vthr, dtR = (R)dt;
     const bool refr = g.ref_steps >= 0;
     Pack<R, E> V = load_pack<R, E>(P.var[B2B_VAR_V], q);
@@ -135,14 +149,17 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     for (int e = 0; e < E; ++e) {
       bool nr = true;
       if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
-      const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR,
-                                 timed_input<R>(g.ta, ts, E * q + e - g.offset));
-      const bool valid = (E * q + e - g.offset) < g.n;
+      const int64_t local = E * q + e - g.offset;
+      R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR,
+                           INPUTS ? timed_input<R>(gin->ta, ts, local) : R(0));
+      const bool valid = local < g.n;
       if (valid && vn > Vthr && nr) {
         nr = false;
         if (refr) LS.x[e] = (R)t;
         fl |= 1u << e;
       }
+      if (INPUTS && gin->pin.count && valid)
+        add_poisson_inputs<R>(gin->pin, ts, local, vn, GE.x[e], GI.x[e]);
       V.x[e] = vn;
       NRout |= (nr ? 1u : 0u) << (8 * e);
     }
@@ -188,7 +205,7 @@ __device__ __forceinline__ void hh_pack_load(const PopDev& P, int64_t q, HhPack<
   s.LS = load_pack<R, 4>(P.var[B2B_VAR_LASTSPIKE], q);
 }
 
-template <typename R>
+template <typename R, bool INPUTS>
 __global__ void __launch_bounds__(kBlock, 2)
 hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                  int32_t* status) {
@@ -210,6 +227,7 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     unsigned fl = 0;
     if (q < nthr) {
       const HhRun<R> g = hh_run(prm[cur.grp], R());
+      const GroupInputs* gin = INPUTS ? P.inputs + cur.grp : nullptr;
       const bool refr = g.ref_steps >= 0;
       R* fge = fold_in<R, 4>(P, B2B_VAR_GE, ts, q, cur.GE);
       R* fgi = fold_in<R, 4>(P, B2B_VAR_GI, ts, q, cur.GI);
@@ -218,15 +236,18 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       for (int e = 0; e < 4; ++e) {
         bool nr = true;
         if (refr) nr = timestep_of(t - (double)cur.LS.x[e], dt, inv_dt) >= g.ref_steps;
-        const R vn = hh_advance<R>(g, cur.V.x[e], cur.M.x[e], cur.H.x[e], cur.N.x[e],
-                                   cur.GE.x[e], cur.GI.x[e], dtR,
-                                   timed_input<R>(g.ta, ts, 4 * q + e - g.offset));
-        const bool valid = (4 * q + e - g.offset) < g.n;
+        const int64_t local = 4 * q + e - g.offset;
+        R vn = hh_advance<R>(g, cur.V.x[e], cur.M.x[e], cur.H.x[e], cur.N.x[e],
+                             cur.GE.x[e], cur.GI.x[e], dtR,
+                             INPUTS ? timed_input<R>(gin->ta, ts, local) : R(0));
+        const bool valid = local < g.n;
         if (valid && vn > (R)g.Vthr && nr) {
           nr = false;
           if (refr) cur.LS.x[e] = (R)t;
           fl |= 1u << e;
         }
+        if (INPUTS && gin->pin.count && valid)
+          add_poisson_inputs<R>(gin->pin, ts, local, vn, cur.GE.x[e], cur.GI.x[e]);
         cur.V.x[e] = vn;
         NRout |= (nr ? 1u : 0u) << (8 * e);
       }
@@ -335,7 +356,7 @@ __global__ void lif_late_reset_kernel(PopDev P, const int64_t* __restrict__ cloc
 // Four neurons per thread once that still gives every SM several CTAs' worth of warps.
 bool wide(int64_t n) { return n / 4 >= (int64_t)kNumSMs * 4 * kBlock; }
 
-template <int E>
+template <int E, bool IN>
 cudaError_t launch_e(const Pop& pop, const PopDev& P, const int64_t* clock, int k, double dt,
                      int32_t* status, cudaStream_t s) {
   const int block = pop.tune_block > 0 ? pop.tune_block : kBlock;   // <= kBlock
@@ -343,19 +364,19 @@ cudaError_t launch_e(const Pop& pop, const PopDev& P, const int64_t* clock, int 
   const bool f32 = pop.dtype == B2B_F32;
   switch (pop.kind) {
     case KIND_LIF:
-      if (f32) lif_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
-      else lif_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+      if (f32) lif_step_kernel<float, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+      else lif_step_kernel<double, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       break;
     case KIND_HH:
       if (E == 4 && f32) {
         // resident CTAs only (2 per SM of 256 threads by the launch bounds); float64 keeps
         // one pack per thread (two packs of doubles do not fit the register budget)
         const unsigned g2 = std::min<unsigned>(grid, 2 * kNumSMs * (kBlock / block));
-        hh_stream_kernel<float><<<g2, block, 0, s>>>(P, clock, k, dt, status);
+        hh_stream_kernel<float, IN><<<g2, block, 0, s>>>(P, clock, k, dt, status);
       } else if (f32) {
-        hh_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+        hh_step_kernel<float, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       } else {
-        hh_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+        hh_step_kernel<double, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       }
       break;
     case KIND_POISSON:
@@ -383,8 +404,11 @@ cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t
     return cudaGetLastError();
   }
   const bool four = pop.tune_e > 0 ? pop.tune_e == 4 : wide(pop.dev.n);
-  return four ? launch_e<4>(pop, dev, clock, k, dt, status, s)
-              : launch_e<1>(pop, dev, clock, k, dt, status, s);
+  if (pop.inputs)
+    return four ? launch_e<4, true>(pop, dev, clock, k, dt, status, s)
+                : launch_e<1, true>(pop, dev, clock, k, dt, status, s);
+  return four ? launch_e<4, false>(pop, dev, clock, k, dt, status, s)
+              : launch_e<1, false>(pop, dev, clock, k, dt, status, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -2,6 +2,7 @@
 // kernel for small networks (small.cu), so both evaluate exactly the same expressions.
 #pragma once
 #include "kernels_common.cuh"
+#include "philox.cuh"
 
 namespace b2b {
 
@@ -97,16 +98,15 @@ template <typename R>
 struct HhRun {
   R Cm, gl, El, EK, ENa, gNa, gK, VT, Ee, Ei, De, Di, Vthr, inv_Cm;
   int64_t ref_steps, offset, n;
-  TimedInput ta;
 };
 __device__ __forceinline__ HhRun<float> hh_run(const HhDev& g, float) {
   const HhFloat& f = g.f;
   return {f.Cm, f.gl, f.El, f.EK, f.ENa, f.gNa, f.gK, f.VT, f.Ee, f.Ei, f.De, f.Di, f.Vthr,
-          f.inv_Cm, g.ref_steps, g.offset, g.n, g.ta};
+          f.inv_Cm, g.ref_steps, g.offset, g.n};
 }
 __device__ __forceinline__ HhRun<double> hh_run(const HhDev& g, double) {
   return {g.Cm, g.gl, g.El, g.EK, g.ENa, g.gNa, g.gK, g.VT, g.Ee, g.Ei, g.De, g.Di, g.Vthr,
-          g.inv_Cm, g.ref_steps, g.offset, g.n, g.ta};
+          g.inv_Cm, g.ref_steps, g.offset, g.n};
 }
 
 // TimedArray input of a group at step ts for its neuron `local` (the role of the function
@@ -129,6 +129,46 @@ __device__ __forceinline__ double per_cm(double x, const HhRun<double>& g) { ret
 
 // Membrane part of the COBAHH update: exponential Euler for v with the conductances of the
 // gating state at the start of the step.  Returns the new v.
+// One Binomial(n, p) draw of a PoissonInput for the group-local neuron `local` at step ts
+// (the role of the inversion sampler brian2cuda/binomial.py:55-90 generates for
+// BinomialFunction, restated as sequential-search inversion, Devroye, "Non-Uniform Random
+// Variate Generation", 1986, ch. X.4): u uniform in (0, 1) from one Philox-4x32-10 word;
+// subtract P(X = 0), P(X = 1), ... from u until it is no longer above the next probability,
+// with P(X = x) = P(X = x - 1) (a / x - s).  Every operation is an IEEE double operation
+// (no fused multiply-add can form), and q^n, s and a come from the host, so the CPU
+// oracle's restatement draws the same X.  At most n steps; mass lost to rounding goes to n.
+static __device__ __noinline__ int64_t poisson_input_draw(const PoissonIn& p, int64_t ts,
+                                                      int64_t local) {
+  const U32x4 w = philox4x32_10(U32x4{(uint32_t)local, (uint32_t)ts,
+                                      (uint32_t)((uint64_t)ts >> 32), p.id}, p.k0, p.k1);
+  double u = ((double)w.x + 0.5) * 0x1p-32;
+  double r = p.qn;
+  int64_t x = 0;
+  while (u > r && x < p.n) {
+    u = __dsub_rn(u, r);
+    ++x;
+    r = __dmul_rn(r, __dsub_rn(__ddiv_rn(p.a, (double)x), p.s));
+  }
+  return p.reverse ? p.n - x : x;
+}
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// The group's PoissonInputs for one neuron: variable += weight * X, in the group's dtype, the
+// product rounded before the sum (as the oracle computes it; no fused multiply-add).
+template <typename R>
+__device__ __forceinline__ void add_poisson_inputs(const PoissonInputs& pin, int64_t ts,
+                                                   int64_t local, R& v, R& ge, R& gi) {
+  for (int k = 0; k < pin.count; ++k) {
+    const PoissonIn& p = pin.in[k];
+    const R add = mul_rn((R)poisson_input_draw(p, ts, local), (R)p.weight);
+    if (p.var == B2B_VAR_V) v += add;
+    else if (p.var == B2B_VAR_GE) ge += add;
+    else gi += add;
+  }
+}
+
 // I: external current (amperes) over the step, from a TimedArray.
 template <typename R>
 __device__ __forceinline__ R hh_membrane(const HhRun<R>& g, R v, R m, R h, R n, R ge, R gi,

@@ -166,7 +166,9 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
           const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
           const bool refr = g.ref_steps >= 0;
           if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
-          R vn = lif_advance<R>(g, v, ge, gi, nr, timed_input<R>(g.ta, ts, i - g.offset));
+          R vn = lif_advance<R>(
+              g, v, ge, gi, nr,
+              P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
           if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
             nr = false;
             if (refr) ls = (R)t;
@@ -184,7 +186,9 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
           if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
           R m = sM[i], h = sH[i], nn = sN[i];
           const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
-                                     timed_input<R>(g.ta, ts, i - g.offset));
+                                     P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
+                                                               i - g.offset)
+                                              : R(0));
           if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
             nr = false;
             if (refr) ls = (R)t;

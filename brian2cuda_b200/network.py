@@ -244,6 +244,14 @@ class Network:
         self._check(self._lib.b2b_timedarray(self._h, gid, _ptr(v), v.shape[0], v.shape[1],
                                              float(dt_array)), "timed_array")
 
+    def poisson_input(self, gid: int, var: str, n: int, rate: float, weight: float) -> int:
+        """PoissonInput(group, var, N=n, rate=rate, weight=weight): every step each neuron
+        adds weight * Binomial(n, rate*dt) to v, ge or gi (synapses slot)."""
+        pid = C.c_int32()
+        self._check(self._lib.b2b_poisson_input(self._h, gid, N.VARS[var], int(n), float(rate),
+                                                float(weight), C.byref(pid)), "poisson_input")
+        return pid.value
+
     def group_size(self, gid: int) -> int:
         return self._groups[gid][1]
 

@@ -146,6 +146,18 @@ b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const i
 b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64_t rows,
                           int64_t cols, double dt_array);
 
+/* PoissonInput of a LIF or HH group (Brian2's PoissonInput, whose per-step draw
+ * brian2cuda implements as a BinomialFunction, brian2cuda/binomial.py:12-121): every step,
+ * in the synapses slot (after the threshold, before the reset of the default schedule), each
+ * neuron of the group adds weight * X to variable var (B2B_VAR_V, _GE or _GI), X ~
+ * Binomial(n_inputs, rate_hz * dt) drawn independently per neuron and step from the net's
+ * seed.  The draw is exact inversion for every n * p (the reference switches to a normal
+ * approximation above n p = 5).  At most two per group; before b2b_finalize.  *pid receives
+ * the input's index (its random stream).  Not combinable with the gating surrogate; a net
+ * with one runs the per-step or two-launch form, not the one-CTA small form. */
+b2b_status b2b_poisson_input(b2b_net* net, int32_t gid, int32_t var, int64_t n_inputs,
+                             double rate_hz, double weight, int32_t* pid);
+
 /* State variables of a group.  Values are in the group's dtype; NOT_REFRACTORY is uint8. */
 enum {
   B2B_VAR_V = 0, B2B_VAR_GE = 1, B2B_VAR_GI = 2, B2B_VAR_M = 3, B2B_VAR_H = 4, B2B_VAR_N = 5,

@@ -115,6 +115,14 @@ struct Group {
   // interval holding t = ts dt on aligned time grids; one column or one per neuron.
   std::vector<R> ta;
   int64_t ta_rows = 0, ta_cols = 0, ta_mul = 1, ta_div = 1;
+  // PoissonInputs: (target variable, N, rate*dt, weight, stream id)
+  struct PIn {
+    int var;
+    int64_t n;
+    double p, w;
+    uint32_t id;
+  };
+  std::vector<PIn> pins;
   R input(int64_t ts, int64_t i) const {
     if (ta.empty()) return (R)0;
     const int64_t row = std::min(ts * ta_mul / ta_div, ta_rows - 1);
@@ -176,6 +184,8 @@ struct Net {
   std::vector<RateMon> rmons;
   bool built = false;
   bool reset_first = false;   // schedule: thresholds, resets, synapses
+  uint64_t seed = 0;          // the net's seed (PoissonInput streams)
+  int32_t n_pins = 0;
   std::string err;
 };
 
@@ -378,6 +388,42 @@ void pathway_post(Net<R>& net, Syn<R>& s, double t) {
   }
 }
 
+// Binomial(n, p) by sequential-search inversion (Devroye 1986, ch. X.4): u uniform in (0, 1)
+// from word 0 of Philox(counter = (neuron, step low, step high, id), key = (seed low,
+// seed high ^ 0xB1A0)); P(X = 0) = q^n, P(X = x) = P(X = x - 1) ((n + 1) s / x - s) with
+// s = p / q; p above 1/2 is drawn as n minus a Binomial(n, 1 - p).  Plain double
+// arithmetic in the order written (the build does not contract it into fused operations).
+int64_t binomial_draw(int64_t n, double p, uint64_t seed, uint32_t id, int64_t ts, int64_t i) {
+  const bool rev = p > 0.5;
+  const double pp = rev ? 1.0 - p : p;
+  const double q = 1.0 - pp;
+  const double qn = std::pow(q, (double)n);
+  const double s = q > 0 ? pp / q : 0.0;
+  const double a = (double)(n + 1) * s;
+  const Ctr w = philox(Ctr{{(uint32_t)i, (uint32_t)ts, (uint32_t)((uint64_t)ts >> 32), id}},
+                       (uint32_t)seed, (uint32_t)(seed >> 32) ^ 0xB1A0u);
+  double u = ((double)w.v[0] + 0.5) * 0x1p-32;
+  double r = qn;
+  int64_t x = 0;
+  while (u > r && x < n) {
+    u = u - r;
+    ++x;
+    r = r * (a / (double)x - s);
+  }
+  return rev ? n - x : x;
+}
+
+// Brian2's PoissonInput: every neuron of the group adds w * Binomial(N, rate dt) to its
+// target variable, at the start of the synapses slot.
+template <typename R>
+void poisson_inputs(Net<R>& net, Group<R>& g) {
+  for (const auto& in : g.pins)
+    for (int64_t i = 0; i < g.n; ++i) {
+      const int64_t x = binomial_draw(in.n, in.p, net.seed, in.id, net.ts, i);
+      g.var[in.var][i] += (R)x * (R)in.w;
+    }
+}
+
 template <typename R>
 bool step(Net<R>& net) {
   const double t = (double)net.ts * net.dt;
@@ -400,6 +446,7 @@ bool step(Net<R>& net) {
         for (int32_t i : g.spikes) g.var[V][i] = (R)g.p[7];
   };
   if (net.reset_first) resets();
+  for (Group<R>& g : net.groups) poisson_inputs(net, g);
   for (Syn<R>& s : net.syns) pathway_pre(net, s, t);
   for (Syn<R>& s : net.syns)
     if (s.effect == STDP) pathway_post(net, s, t);
@@ -631,6 +678,17 @@ int api_spikegen(Net<R>& net, int64_t n, int64_t ns, const int32_t* idx, const i
   for (int64_t k = 0; k < ns; ++k) g.sg.emplace_back(st[k], idx[k]);
   std::sort(g.sg.begin(), g.sg.end());
   return add_group(net, std::move(g));
+}
+
+template <typename R>
+int api_poisson_input(Net<R>& net, int gid, int var, int64_t n, double rate, double w) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  Group<R>& g = net.groups[gid];
+  if ((g.kind != LIF && g.kind != HH) || (var != V && var != GE && var != GI) || n < 0 ||
+      g.pins.size() >= 2)
+    return -1;
+  g.pins.push_back({var, n, rate * net.dt, w, (uint32_t)net.n_pins});
+  return net.n_pins++;
 }
 
 template <typename R>
@@ -896,6 +954,10 @@ void* orc_create(double dt, int flags) {
   h->nf.reset_first = h->nd.reset_first = (flags & 2) != 0;
   return h;
 }
+void orc_set_seed(void* hp, uint64_t seed) {
+  Handle* h = static_cast<Handle*>(hp);
+  h->nf.seed = h->nd.seed = seed;
+}
 void orc_destroy(void* h) { delete static_cast<Handle*>(h); }
 const char* orc_error(void* hp) {
   Handle* h = static_cast<Handle*>(hp);
@@ -918,6 +980,11 @@ int orc_group_poisson(void* hp, int64_t n, double rate) {
 int orc_group_spikegen(void* hp, int64_t n, int64_t ns, const int32_t* idx, const int64_t* st) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_spikegen, n, ns, idx, st);
+}
+// PoissonInput of group gid onto var: N inputs at rate Hz, weight w; returns its stream id
+int orc_poisson_input(void* hp, int gid, int var, int64_t n, double rate, double w) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_poisson_input, gid, var, n, rate, w);
 }
 // TimedArray: values [rows][cols], step ts reads row min(ts * mul / div, rows - 1)
 int orc_timedarray(void* hp, int gid, const double* v, int64_t rows, int64_t cols, int64_t mul,

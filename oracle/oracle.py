@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
             "orc_group_poisson": (C.c_int, [P, I64, D]),
             "orc_group_spikegen": (C.c_int, [P, I64, I64, P, P]),
             "orc_timedarray": (C.c_int, [P, C.c_int, P, I64, I64, I64, I64]),
+            "orc_poisson_input": (C.c_int, [P, C.c_int, C.c_int, I64, D, D]),
+            "orc_set_seed": (None, [P, C.c_uint64]),
             "orc_state_set": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_state_get": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_synapses": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, I64, P, P, P, D, P,
@@ -91,11 +93,12 @@ class OracleNet:
     f32=True computes in float32 (the group dtype of the GPU run), else float64."""
 
     def __init__(self, dt: float, f32: bool = False, reset_before_synapses: bool = False,
-                 **_ignored):
+                 seed: int = 0, **_ignored):
         self._lib = lib()
         self.dt = float(dt)
         self._h = self._lib.orc_create(self.dt, (1 if f32 else 0) |
                                        (2 if reset_before_synapses else 0))
+        self._lib.orc_set_seed(self._h, int(seed))
         self._sizes: list[int] = []
         self._kinds: list[str] = []
         self._smon_n: dict[int, int] = {}
@@ -139,6 +142,12 @@ class OracleNet:
         st = np.ascontiguousarray(steps, dtype=np.int64)
         return self._add("spikegen", n,
                          self._lib.orc_group_spikegen(self._h, n, len(idx), _p(idx), _p(st)))
+
+    def poisson_input(self, gid, var, n, rate, weight):
+        """PoissonInput: every step each neuron adds weight * Binomial(n, rate*dt) to var."""
+        from brian2cuda_b200._native import VARS
+        return self._ok(self._lib.orc_poisson_input(self._h, gid, VARS[var], int(n), float(rate),
+                                                    float(weight)), "poisson_input")
 
     def timed_array(self, gid, values, dt_array):
         """TimedArray input of a LIF (volts) or HH (amperes) group: values (rows,) for the
