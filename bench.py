@@ -3,8 +3,8 @@ dt = 0.1 ms, connect(p=0.02) (about 2e8 synapses) with per-synapse delays of 1..
 1 s simulated.
 
 One bench step = the whole configured run: restore the seeded initial state (a device-side
-checkpoint) and simulate 1 s = 10,000 time steps (fused neuron kernel + spike delivery,
-replayed from CUDA graphs).  The network fires in population bursts about every 140 ms, so
+checkpoint) and simulate 1 s = 10,000 time steps (the neuron update and the spike delivery
+of each step as two concurrent launches, replayed from CUDA graphs).  The network fires in population bursts about every 140 ms, so
 shorter windows would sample the burst cycle unevenly.  value = synaptic events/s (spikes
 x out-degree delivered per second of device time); the line also carries
 neuron-updates/s.  Inputs (state, 1.6 GB of synapse arrays) are resident in HBM before

@@ -701,8 +701,6 @@ b2b_status setup_monitors(b2b_net* net) {
   return B2B_OK;
 }
 
-// One kernel per step (fused.cu) applies when the net is one LIF/HH population whose
-// synapses are all additive onto ge/gi of that population with delays of at least one step.
 // A small network (small.cu, opt-in with B2B_NET_SMALL) runs every step of a chunk in one
 // CTA: one LIF/HH population of at most 4096 neurons (no gating surrogate) whose Synapses
 // objects are all additive and target it, with the state fitting the CTA's shared memory.
@@ -745,9 +743,12 @@ b2b_status setup_small(b2b_net* net) {
 // (measured: 1e5 HH neurons 38.6 vs 50.9 ms per simulated second).  Above it the pending
 // input's read and clear (16 B per neuron and step for ge and gi in float32) costs more HBM
 // time than the overlap saves: 3.9e6 HH neurons 70.1 vs 62.2 us per step.
-constexpr int64_t kAutoFusedMaxNeurons = 1 << 18;
+constexpr int64_t kAutoTwoLaunchMaxNeurons = 1 << 18;
 
-b2b_status setup_fused(b2b_net* net) {
+// The step as two concurrent launches (pending.cu) applies when the net is one LIF/HH
+// population (no gating surrogate, no state or rate monitor) whose synapses are all additive
+// onto its ge/gi with delays of at least one step.
+b2b_status setup_two_launch(b2b_net* net) {
   const int32_t flags = net->cfg.flags;
   if (flags & (B2B_NET_PER_STEP | B2B_NET_SMALL)) return B2B_OK;
   if ((flags & B2B_NET_CHECKED) && !(flags & B2B_NET_FUSED)) return B2B_OK;
@@ -766,8 +767,8 @@ b2b_status setup_fused(b2b_net* net) {
     }
     nd_max = std::max(nd_max, pr.dev.nd);
   }
-  FusedDev& F = net->fdev;
-  F = FusedDev{};
+  PendingDev& F = net->pdev;
+  F = PendingDev{};
   F.pop = pop.dev;
   F.n_proj = (int32_t)net->projs.size();
   F.nd_max = nd_max;
@@ -779,7 +780,7 @@ b2b_status setup_fused(b2b_net* net) {
       const int v = net->syns[m].target_var;
       if (!F.acc[v]) {
         CU(cudaMalloc(&F.acc[v], 2 * rs * pop.n));
-        net->fused_allocs.push_back(F.acc[v]);
+        net->pending_allocs.push_back(F.acc[v]);
         CU(cudaMemset(F.acc[v], 0, 2 * rs * pop.n));
       }
       F.proj[p].targets[v] = F.acc[v];
@@ -789,7 +790,7 @@ b2b_status setup_fused(b2b_net* net) {
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
   F.group = 8;
-  net->fused_dgrid = 2 * sms;
+  net->pending_grid = 2 * sms;
   // the update launch is the per-step neuron kernel, adding in the input that the previous
   // step's delivery left in acc
   net->fold_dev = pop.dev;
@@ -798,8 +799,8 @@ b2b_status setup_fused(b2b_net* net) {
   CU(cudaEventCreateWithFlags(&net->ev_n, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&net->ev_d[0], cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&net->ev_d[1], cudaEventDisableTiming));
-  net->fused_ok = true;
-  net->fused = (flags & B2B_NET_FUSED) || pop.n <= kAutoFusedMaxNeurons;
+  net->two_launch_ok = true;
+  net->two_launch = (flags & B2B_NET_FUSED) || pop.n <= kAutoTwoLaunchMaxNeurons;
   return B2B_OK;
 }
 
@@ -813,7 +814,7 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     net->launches += 2;
     return B2B_OK;
   }
-  if (net->fused) {
+  if (net->two_launch) {
     // Step k's delivery (spikes of steps <= k-1 into acc[k & 1]) and step k's neuron update
     // (which folds in acc[(k-1) & 1]) are independent: the delivery of step k waits for the
     // update of step k-1, the update of step k for the update and the delivery of step k-1.
@@ -824,7 +825,7 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     CU(cudaEventRecord(net->ev_n, s));
     for (int k = 0; k < kk; ++k) {
       CU(cudaStreamWaitEvent(s2, net->ev_n, 0));
-      CU(launch_pending_delivery(net->fdev, pop.dtype, net->fused_dgrid, net->d_clock, k, s2));
+      CU(launch_pending_delivery(net->pdev, pop.dtype, net->pending_grid, net->d_clock, k, s2));
       CU(cudaEventRecord(net->ev_d[k & 1], s2));
       if (k > 0) CU(cudaStreamWaitEvent(s, net->ev_d[(k - 1) & 1], 0));
       CU(launch_pop_step_dev(pop, net->fold_dev, net->d_clock, k, net->cfg.dt, net->d_status,
@@ -833,7 +834,7 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
       net->launches += 2;
     }
     CU(cudaStreamWaitEvent(s, net->ev_d[(kk - 1) & 1], 0));
-    CU(launch_fold_pending(net->fdev, pop.dtype, net->d_clock, kk - 1, s));
+    CU(launch_fold_pending(net->pdev, pop.dtype, net->d_clock, kk - 1, s));
     CU(launch_tick(net->d_clock, kk, s));
     net->launches += 2;
     return B2B_OK;
@@ -1000,7 +1001,7 @@ b2b_status b2b_destroy(b2b_net* net) {
     for (void* a : p.allocs) cudaFree(a);
   for (Snapshot& sn : net->snapshots)
     for (void* a : sn.buffers) cudaFree(a);
-  for (void* a : net->fused_allocs) cudaFree(a);
+  for (void* a : net->pending_allocs) cudaFree(a);
   if (net->stream2) cudaStreamDestroy(net->stream2);
   for (cudaEvent_t ev : {net->ev_n, net->ev_d[0], net->ev_d[1]})
     if (ev) cudaEventDestroy(ev);
@@ -1402,7 +1403,7 @@ b2b_status b2b_finalize(b2b_net* net) {
   b2b_status st = finalize_pops(net);
   if (st == B2B_OK) st = finalize_projs(net);
   if (st == B2B_OK) st = setup_monitors(net);
-  if (st == B2B_OK) st = setup_fused(net);
+  if (st == B2B_OK) st = setup_two_launch(net);
   if (st == B2B_OK) st = setup_small(net);
   if (st != B2B_OK) return st;
   CU(cudaMemcpy(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice));
@@ -1447,7 +1448,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   std::vector<Site> sites;
   if (net->small) {
     sites.push_back({7, 0});
-  } else if (net->fused) {  // the step's two launches, timed one after the other
+  } else if (net->two_launch) {  // the step's two launches, timed one after the other
     sites.push_back({5, 0});
     sites.push_back({1, 0});
   } else {
@@ -1475,7 +1476,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       cudaError_t e = cudaSuccess;
       const int64_t* clk = net->d_clock;
       if (s.kind == 1)
-        e = launch_pop_step_dev(net->pops[s.idx], net->fused ? net->fold_dev : net->pops[s.idx].dev,
+        e = launch_pop_step_dev(net->pops[s.idx], net->two_launch ? net->fold_dev : net->pops[s.idx].dev,
                                 clk, 0, net->cfg.dt, net->d_status, net->stream);
       if (s.kind == 6)
         e = launch_proj_add_batch(net->add_batches[s.idx].data(), (int)net->add_batches[s.idx].size(),
@@ -1495,7 +1496,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
         e = launch_small(net->sdev, net->pops[0].kind, net->pops[0].dtype, clk, 1, net->cfg.dt,
                          net->d_status, net->stream);
       if (s.kind == 5)
-        e = launch_pending_delivery(net->fdev, net->pops[0].dtype, net->fused_dgrid, clk, 0,
+        e = launch_pending_delivery(net->pdev, net->pops[0].dtype, net->pending_grid, clk, 0,
                                     net->stream);
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
@@ -1515,8 +1516,8 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
     net->last_chunk_steps = 1;
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  if (result == B2B_OK && net->fused) {
-    cudaError_t e = launch_fold_pending(net->fdev, net->pops[0].dtype, net->d_clock, -1, net->stream);
+  if (result == B2B_OK && net->two_launch) {
+    cudaError_t e = launch_fold_pending(net->pdev, net->pops[0].dtype, net->d_clock, -1, net->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
     if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile fold: %s", cudaGetErrorString(e));
   }
@@ -1573,13 +1574,13 @@ b2b_status set_record_order(b2b_net* net, Proj& pr, bool post_grouped) {
 
 constexpr double kTuneMargin = 0.98;
 
-// Launch shape of the delivery launch of a net run with two launches per step (fused.cu):
+// Launch shape of the delivery launch of a net run with two launches per step (pending.cu):
 // lanes per work item (0: 8) and CTAs (0: two per SM).
-void set_fused_shape(b2b_net* net, int group, int grid) {
+void set_pending_shape(b2b_net* net, int group, int grid) {
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
-  net->fused_dgrid = grid > 0 ? grid : 2 * sms;
-  net->fdev.group = group > 0 ? group : 8;
+  net->pending_grid = grid > 0 ? grid : 2 * sms;
+  net->pdev.group = group > 0 ? group : 8;
   if (net->graph) {
     cudaGraphExecDestroy(net->graph);
     net->graph = nullptr;
@@ -1675,9 +1676,9 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
   // a net that allows both forms of the step tunes the per-step kernels first, then the two
   // concurrent launches, and keeps the faster form
-  const bool builtin_fused = net->fused;
-  if (net->fused_ok) net->fused = false;
-  for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->fused; ++p) {
+  const bool builtin_two_launch = net->two_launch;
+  if (net->two_launch_ok) net->two_launch = false;
+  for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->two_launch; ++p) {
     Pop& pop = net->pops[p];
     if (pop.kind == KIND_SPIKEGEN) continue;
     std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
@@ -1715,7 +1716,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
-  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->fused; ++b) {
+  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
     AddTune& t = net->add_tune[b];
     std::vector<std::pair<int, int>> cands = {{0, 0}};
     for (int g : {4, 8, 16, 32})
@@ -1741,9 +1742,9 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
-  if (net->fused_ok && st == B2B_OK) {
+  if (net->two_launch_ok && st == B2B_OK) {
     const double per_step_ms = res.empty() ? 1e30 : res.back().best_ms;
-    net->fused = true;
+    net->two_launch = true;
     // the step's delivery launch: lanes per work item x CTAs (the neuron launch has one
     // thread per neuron)
     std::vector<std::pair<int, int>> cands = {{0, 0}};
@@ -1752,7 +1753,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     b2b_tune_result r{5, 0, 0, 0, 0.0, 0.0};
     double best = 1e30;
     for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
-      set_fused_shape(net, cands[c].first, cands[c].second);
+      set_pending_shape(net, cands[c].first, cands[c].second);
       double ms = 0;
       st = trial(&ms);
       if (c == 0) r.default_ms = ms;
@@ -1762,16 +1763,16 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         r.choice_b = cands[c].second;
       }
     }
-    set_fused_shape(net, r.choice_a, r.choice_b);
+    set_pending_shape(net, r.choice_a, r.choice_b);
     r.best_ms = best;
     res.push_back(r);
-    const double fused_ms = res.back().best_ms;
+    const double two_launch_ms = res.back().best_ms;
     // the built-in form stays unless the other is 2 % faster
-    const bool use_fused = builtin_fused ? !(per_step_ms < kTuneMargin * fused_ms)
-                                         : fused_ms < kTuneMargin * per_step_ms;
-    net->fused = use_fused;
-    res.push_back(b2b_tune_result{11, 0, use_fused ? 1 : 0, 0, std::min(per_step_ms, fused_ms),
-                                  builtin_fused ? fused_ms : per_step_ms});
+    const bool use_two_launch = builtin_two_launch ? !(per_step_ms < kTuneMargin * two_launch_ms)
+                                         : two_launch_ms < kTuneMargin * per_step_ms;
+    net->two_launch = use_two_launch;
+    res.push_back(b2b_tune_result{11, 0, use_two_launch ? 1 : 0, 0, std::min(per_step_ms, two_launch_ms),
+                                  builtin_two_launch ? two_launch_ms : per_step_ms});
   }
   // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
   for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
@@ -1793,7 +1794,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
-  if (st != B2B_OK && net->fused_ok) net->fused = builtin_fused;
+  if (st != B2B_OK && net->two_launch_ok) net->two_launch = builtin_two_launch;
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
   if (st2 == B2B_OK) st2 = put_back_monitors();
@@ -1843,16 +1844,16 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
       net->add_tune[t.site_index].group = t.choice_a;
       net->add_tune[t.site_index].grid = t.choice_b;
     } else if (t.site_kind == 11) {
-      CHECK(net->fused_ok && t.site_index == 0 && (t.choice_a == 0 || t.choice_a == 1),
+      CHECK(net->two_launch_ok && t.site_index == 0 && (t.choice_a == 0 || t.choice_a == 1),
             B2B_ERR_INVALID_ARG, "site kind 11 exists only for nets that allow both step forms");
-      net->fused = t.choice_a == 1;
+      net->two_launch = t.choice_a == 1;
     } else if (t.site_kind == 5) {
-      CHECK(net->fused_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
+      CHECK(net->two_launch_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
             "site kind 5 exists only for nets that allow two launches per step");
       CHECK((t.choice_a == 0 || t.choice_a == 4 || t.choice_a == 8 || t.choice_a == 16) &&
                 t.choice_b >= 0 && t.choice_b <= 65535,
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
-      set_fused_shape(net, t.choice_a, t.choice_b);
+      set_pending_shape(net, t.choice_a, t.choice_b);
     } else if (t.site_kind == 8) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
                 net->projs[t.site_index].effect == B2B_EFFECT_STDP,
@@ -1935,7 +1936,7 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t) {
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode) {
   if (!net || !mode) return B2B_ERR_INVALID_ARG;
   if (!net->finalized) return fail(net, B2B_ERR_STATE, "call b2b_finalize first");
-  *mode = net->small ? 2 : (net->fused ? 1 : 0);
+  *mode = net->small ? 2 : (net->two_launch ? 1 : 0);
   return B2B_OK;
 }
 

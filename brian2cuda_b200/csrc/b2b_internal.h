@@ -96,7 +96,7 @@ struct PopDev {
   int64_t sg_n;
   int32_t late_reset;             // reset must run after synaptic delivery
   int32_t pad;
-  // The step as two concurrent launches (fused.cu): per variable (v, ge, gi), [2][n] input
+  // The step as two concurrent launches (pending.cu): per variable (v, ge, gi), [2][n] input
   // delivered during the previous step, which the update adds in and clears (NULL: none).
   void* fold[3];
 };
@@ -170,9 +170,9 @@ struct RateMonDev {
   int64_t cap;
 };
 
-// Device view of the delivery of the two-launch step (fused.cu): one population and its
+// Device view of the delivery of the two-launch step (pending.cu): one population and its
 // additive projections, whose targets are redirected to double-buffered input accumulators.
-struct FusedDev {
+struct PendingDev {
   PopDev pop;
   ProjDev proj[kMaxProjBatch];
   int32_t n_proj, nd_max;
@@ -324,16 +324,16 @@ struct b2b_net {
   std::vector<void*> mon_allocs;
   bool small = false;                      // one CTA runs every step (small.cu)
   b2b::SmallDev sdev{};
-  bool fused = false;                      // the step as two concurrent launches (fused.cu)
-  bool fused_ok = false;                   // the net allows them (their buffers exist)
-  // the step as two concurrent launches: the delivery into fdev's accumulators (on a second
-  // stream, fused_dgrid CTAs) and the update through fold_dev, ordered by events
-  b2b::FusedDev fdev{};
+  bool two_launch = false;                 // the step as two concurrent launches (pending.cu)
+  bool two_launch_ok = false;              // the net allows them (their buffers exist)
+  // the step as two concurrent launches: the delivery into pdev's accumulators (on a second
+  // stream, pending_grid CTAs) and the update through fold_dev, ordered by events
+  b2b::PendingDev pdev{};
   b2b::PopDev fold_dev{};                  // the population's view whose update folds acc in
-  int fused_dgrid = 0;
+  int pending_grid = 0;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
-  std::vector<void*> fused_allocs;
+  std::vector<void*> pending_allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   int64_t launches = 0;
@@ -378,10 +378,10 @@ int mlp_device(const b2b_mlp* m);
 size_t small_smem(const SmallDev& D, int kind, int dtype);
 cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                          int steps, double dt, int32_t* status, cudaStream_t s);
-// The two-launch step (fused.cu): the delivery into the pending input of the step, and the
+// The two-launch step (pending.cu): the delivery into the pending input of the step, and the
 // fold of the pending input at the end of a chunk.
-cudaError_t launch_pending_delivery(const FusedDev& F, int dtype, int grid,
+cudaError_t launch_pending_delivery(const PendingDev& F, int dtype, int grid,
                                     const int64_t* clock, int k, cudaStream_t s);
-cudaError_t launch_fold_pending(const FusedDev& F, int dtype, const int64_t* clock, int k_last,
+cudaError_t launch_fold_pending(const PendingDev& F, int dtype, const int64_t* clock, int k_last,
                                 cudaStream_t s);
 }  // namespace b2b

@@ -29,7 +29,7 @@ constexpr int kPendingUnroll = 4;   // rounds of a bundle whose loads a lane iss
 // Bundles due at step clock+k (spikes of steps ts - d, d >= 1) added into acc[ts & 1].
 template <typename R, bool WARP_PREFIX, int GROUP>
 __global__ void __launch_bounds__(kPendingBlock)
-deliver_pending_kernel(const __grid_constant__ FusedDev F, const int64_t* __restrict__ clock,
+deliver_pending_kernel(const __grid_constant__ PendingDev F, const int64_t* __restrict__ clock,
                        int k) {
   extern __shared__ int s_pref[];  // F.nd_max + 1 ints when !WARP_PREFIX
   const int64_t ts = clock[0] + k;
@@ -66,7 +66,7 @@ deliver_pending_kernel(const __grid_constant__ FusedDev F, const int64_t* __rest
 
 // Adds the input delivered in step clock+k_last into the target variables and zeroes it.
 template <typename R>
-__global__ void fold_pending_kernel(const __grid_constant__ FusedDev F,
+__global__ void fold_pending_kernel(const __grid_constant__ PendingDev F,
                                     const int64_t* __restrict__ clock, int k_last) {
   const int last = (int)((clock[0] + k_last) & 1);
   const int64_t n = F.pop.n;
@@ -83,7 +83,7 @@ __global__ void fold_pending_kernel(const __grid_constant__ FusedDev F,
 }
 
 template <typename R, bool WP>
-cudaError_t launch_pending_r(const FusedDev& F, dim3 g, size_t smem, const int64_t* clock,
+cudaError_t launch_pending_r(const PendingDev& F, dim3 g, size_t smem, const int64_t* clock,
                              int k, cudaStream_t s) {
   if (F.group == 16)
     deliver_pending_kernel<R, WP, 16><<<g, kPendingBlock, smem, s>>>(F, clock, k);
@@ -96,7 +96,7 @@ cudaError_t launch_pending_r(const FusedDev& F, dim3 g, size_t smem, const int64
 
 }  // namespace
 
-cudaError_t launch_pending_delivery(const FusedDev& F, int dtype, int grid,
+cudaError_t launch_pending_delivery(const PendingDev& F, int dtype, int grid,
                                     const int64_t* clock, int k, cudaStream_t s) {
   const bool wp = F.nd_max <= kWarpPrefixMaxDelays;
   const size_t smem = wp ? 0 : sizeof(int) * (size_t)(F.nd_max + 1);
@@ -108,7 +108,7 @@ cudaError_t launch_pending_delivery(const FusedDev& F, int dtype, int grid,
             : launch_pending_r<double, false>(F, g, smem, clock, k, s);
 }
 
-cudaError_t launch_fold_pending(const FusedDev& F, int dtype, const int64_t* clock, int k_last,
+cudaError_t launch_fold_pending(const PendingDev& F, int dtype, const int64_t* clock, int k_last,
                                 cudaStream_t s) {
   const int64_t n = F.pop.n;
   int64_t blocks = (n + kPendingBlock - 1) / kPendingBlock;
