@@ -1166,8 +1166,8 @@ b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64
   CHECK(!net->finalized, B2B_ERR_STATE, "TimedArrays must be set before b2b_finalize");
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   Group& g = net->groups[gid];
-  CHECK(g.kind == KIND_LIF || g.kind == KIND_HH, B2B_ERR_INVALID_ARG,
-        "a TimedArray drives a LIF or HH group");
+  CHECK(g.kind == KIND_LIF || g.kind == KIND_HH || g.kind == KIND_POISSON, B2B_ERR_INVALID_ARG,
+        "a TimedArray drives a LIF, HH or Poisson group");
   CHECK(values && rows > 0 && (cols == 1 || cols == g.n), B2B_ERR_INVALID_ARG,
         "values must be [rows >= 1][1 or the group's %lld neurons]", (long long)g.n);
   CHECK(std::isfinite(dt_array) && dt_array > 0, B2B_ERR_INVALID_ARG, "bad dt_array");

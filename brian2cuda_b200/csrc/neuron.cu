@@ -271,9 +271,10 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 }
 
 // ---- PoissonGroup: spike when u < rate*dt, u read in place from the bulk buffer ---------
-template <typename R, int E>
+template <typename R, int E, bool INPUTS>
 __global__ void __launch_bounds__(kBlock)
-poisson_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, int32_t* status) {
+poisson_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
+                    int32_t* status) {
   const int64_t ts = clock[0] + k;
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t nthr = P.n / E;
@@ -281,14 +282,20 @@ poisson_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, int32_t*
   unsigned fl = 0;
   if (q < nthr) {
     const PoissonDev* prm = static_cast<const PoissonDev*>(P.params);
-    const PoissonDev g = prm[group_of<E>(P, q)];
+    const int grp = group_of<E>(P, q);
+    const PoissonDev g = prm[grp];
+    const GroupInputs* gin = INPUTS ? P.inputs + grp : nullptr;
     const R thr = (R)g.p_spike;
     const R* row = static_cast<const R*>(P.rng) + (int64_t)k * P.n;
     Pack<R, E> U = load_pack<R, E>(row, q);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const bool valid = (E * q + e - g.offset) < g.n;
-      if (valid && U.x[e] < thr) fl |= 1u << e;
+      const int64_t local = E * q + e - g.offset;
+      const bool valid = local < g.n;
+      // a TimedArray gives the rate in Hz (PoissonGroup(rates='ta(t)')): u < rate dt
+      const R th = INPUTS && gin->ta.val
+                       ? (R)((double)timed_input<R>(gin->ta, ts, local) * dt) : thr;
+      if (valid && U.x[e] < th) fl |= 1u << e;
     }
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
@@ -380,8 +387,8 @@ cudaError_t launch_e(const Pop& pop, const PopDev& P, const int64_t* clock, int 
       }
       break;
     case KIND_POISSON:
-      if (f32) poisson_step_kernel<float, E><<<grid, block, 0, s>>>(P, clock, k, status);
-      else poisson_step_kernel<double, E><<<grid, block, 0, s>>>(P, clock, k, status);
+      if (f32) poisson_step_kernel<float, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
+      else poisson_step_kernel<double, E, IN><<<grid, block, 0, s>>>(P, clock, k, dt, status);
       break;
     default:
       return cudaErrorInvalidValue;

@@ -233,10 +233,11 @@ class Network:
         return self._add("spikegen", n, N.F32, gid)
 
     def timed_array(self, gid: int, values, dt_array: float) -> None:
-        """TimedArray input of a LIF or HH group (the role of brian2cuda/timedarray.py): values
-        (rows,) for the whole group or (rows, n) per neuron, each row held for dt_array
-        seconds, the last row after the end.  LIF: volts added to El,
-        dv/dt = (El + I(t) - v + ...)/taum; HH: amperes, Cm dv/dt = ... + I(t)."""
+        """TimedArray input of a LIF, HH or Poisson group (the role of brian2cuda/timedarray.py):
+        values (rows,) for the whole group or (rows, n) per neuron, each row held for
+        dt_array seconds, the last row after the end.  LIF: volts added to El,
+        dv/dt = (El + I(t) - v + ...)/taum; HH: amperes, Cm dv/dt = ... + I(t); Poisson: the
+        rate in Hz (PoissonGroup(N, rates='ta(t)'))."""
         v = np.asarray(values, dtype=np.float64)
         v = np.ascontiguousarray(v[:, None] if v.ndim == 1 else v)
         if v.ndim != 2:

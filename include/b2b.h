@@ -133,13 +133,15 @@ b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate
 b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const int32_t* idx,
                               const int64_t* step, int32_t* gid);
 
-/* TimedArray input of a LIF or HH group (replaces the function brian2cuda/timedarray.py:
+/* TimedArray input of a LIF, HH or Poisson group (replaces the function brian2cuda/timedarray.py:
  * 10-58 generates for `ta(t)` / `ta(t, i)` in the group's equations).  values[rows][cols]
  * (row-major float64, converted to the group's dtype) are sampled every dt_array seconds and
  * held over each interval: step ts reads row floor(ts * dt / dt_array), clamped to rows - 1.
  * cols = 1: one value for the whole group; cols = n: one per neuron.  The value I enters
  *     LIF: dv/dt = (El + I - v + ke*ge + ki*gi)/taum     (I in volts)
  *     HH:  Cm dv/dt = ... + I                           (I in amperes)
+ *     PoissonGroup: the rate in Hz, replacing the group's constant rate
+ *                   (PoissonGroup(N, rates='ta(t)')): spike when u < I dt
  * dt_array must be an integer multiple or an integer fraction of the net's dt (aligned time
  * grids).  Before b2b_finalize; a later call for the same group replaces the array.  Not
  * combinable with the gating surrogate. */

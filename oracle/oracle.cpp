@@ -318,8 +318,11 @@ bool threshold(Net<R>& net, Group<R>& g, double t) {
     }
     const std::vector<R>& u = g.uniforms[g.uni_next++];
     const R thr = (R)(g.rate * net.dt);
-    for (int64_t i = 0; i < g.n; ++i)
-      if (u[i] < thr) g.spikes.push_back((int32_t)i);
+    for (int64_t i = 0; i < g.n; ++i) {
+      // a TimedArray gives the rate in Hz: u < rate(t) dt
+      const R th = g.ta.empty() ? thr : (R)((double)g.input(net.ts, i) * net.dt);
+      if (u[i] < th) g.spikes.push_back((int32_t)i);
+    }
   } else if (g.kind == SPIKEGEN) {
     auto lo = std::lower_bound(g.sg.begin(), g.sg.end(), std::make_pair(net.ts, (int32_t)-1));
     for (auto it = lo; it != g.sg.end() && it->first == net.ts; ++it) g.spikes.push_back(it->second);
@@ -696,7 +699,8 @@ int api_timedarray(Net<R>& net, int gid, const double* vals, int64_t rows, int64
                    int64_t mul, int64_t div) {
   if (gid < 0 || gid >= (int)net.groups.size()) return -1;
   Group<R>& g = net.groups[gid];
-  if ((g.kind != LIF && g.kind != HH) || rows < 1 || (cols != 1 && cols != g.n) || mul < 1 ||
+  if ((g.kind != LIF && g.kind != HH && g.kind != POISSON) || rows < 1 ||
+      (cols != 1 && cols != g.n) || mul < 1 ||
       div < 1)
     return -1;
   g.ta.assign(vals, vals + rows * cols);   // rounded to R once, as the device copy is

@@ -150,8 +150,9 @@ class OracleNet:
                                                     float(weight)), "poisson_input")
 
     def timed_array(self, gid, values, dt_array):
-        """TimedArray input of a LIF (volts) or HH (amperes) group: values (rows,) for the
-        whole group or (rows, n) per neuron, each row held for dt_array seconds."""
+        """TimedArray input of a LIF (volts), HH (amperes) or Poisson (rate in Hz) group:
+        values (rows,) for the whole group or (rows, n) per neuron, each row held for
+        dt_array seconds."""
         v = np.asarray(values, dtype=np.float64)
         v = np.ascontiguousarray(v[:, None] if v.ndim == 1 else v)
         r = float(dt_array) / self.dt

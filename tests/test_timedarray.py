@@ -164,14 +164,75 @@ def test_hh_timedarray_float32_matches_oracle(gpu_factory, oracle_factory):
 def test_timedarray_rejects_bad_arguments(gpu_factory):
     net = gpu_factory(DT)
     G = net.lif_group(10, models.cuba_lif(), "float64")
-    P = net.poisson_group(10, 5.0)
+    S = net.spikegen_group(10, [1], [3])
     with pytest.raises(Exception):
         net.timed_array(G, np.zeros((4, 3)), DT)         # neither 1 nor 10 columns
     with pytest.raises(Exception):
         net.timed_array(G, np.zeros(4), 2.5 * DT)         # time grids not aligned
     with pytest.raises(Exception):
-        net.timed_array(P, np.zeros(4), DT)               # not a LIF or HH group
+        net.timed_array(S, np.zeros(4), DT)               # not a LIF, HH or Poisson group
     net.timed_array(G, np.zeros(4), DT)
     net.finalize()
     with pytest.raises(Exception):
         net.timed_array(G, np.zeros(4), DT)               # after finalize
+
+
+def test_oracle_poisson_rate_timedarray_known_answer(oracle_factory):
+    """PoissonGroup(N, rates='ta(t)'): neuron i spikes at step t when u < rate(t, i) dt; rate
+    0 never spikes, rate 1/dt always does."""
+    n, steps = 300, 16
+    rng = np.random.default_rng(3)
+    rates = np.stack([np.zeros(n), rng.uniform(0, 8000, n), np.full(n, 1 / DT),
+                      rng.uniform(0, 3000, n)])
+    u = rng.uniform(0, 1, size=(steps, n))
+    net = oracle_factory(DT)
+    P = net.poisson_group(n, 123.0)
+    net.timed_array(P, rates, 4 * DT)
+    net.spike_monitor(P, 10**6)
+    net.finalize()
+    net.set_uniforms(P, u)
+    net.run(steps)
+    idx, st = net.spikes(P)
+    want = u < rates[_drive_rows(steps, len(rates), 1, 4)] * DT
+    wst, widx = np.nonzero(want)
+    np.testing.assert_array_equal(st, wst)
+    np.testing.assert_array_equal(idx, widx)
+    assert not np.any((st >= 0) & (st < 4))          # rate 0
+    assert np.sum((st >= 8) & (st < 12)) == 4 * n     # rate 1/dt
+
+
+@pytest.mark.gpu
+def test_poisson_rate_timedarray_matches_oracle(gpu_factory, oracle_factory):
+    """A PoissonGroup whose per-neuron rates follow a TimedArray drives a LIF group; the
+    oracle consumes the GPU's uniforms: both spike trains equal, state within 1e-10."""
+    K = 50
+    rng = np.random.default_rng(8)
+    rates = rng.uniform(0, 400, size=(6, 400))
+    rates[2] = 0.0
+    gpu = gpu_factory(DT, steps_per_graph=K, seed=3)
+    orc = oracle_factory(DT)
+    ids = {}
+    for name, net in (("gpu", gpu), ("orc", orc)):
+        P = net.poisson_group(400, 50.0, "float64")
+        net.timed_array(P, rates, 30 * DT)
+        G = net.lif_group(100, models.cuba_lif(), "float64")
+        i, j = models.bernoulli_pairs(np.random.default_rng(1), 400, 100, 0.1)
+        net.synapses(P, G, "ge", i, j, w_scalar=0.6 * mV,
+                     delay=np.random.default_rng(2).integers(0, 5, len(i)).astype(np.int32))
+        net.spike_monitor(P, 10**6)
+        net.spike_monitor(G, 10**6)
+        net.finalize()
+        ids[name] = (P, G)
+    for _ in range(5):
+        gpu.run(K)
+        orc.set_uniforms(ids["orc"][0], gpu.rng_uniforms(ids["gpu"][0], K))
+        orc.run(K)
+    for k in (0, 1):
+        a, b = gpu.spikes(ids["gpu"][k]), orc.spikes(ids["orc"][k])
+        np.testing.assert_array_equal(a[1], b[1])
+        np.testing.assert_array_equal(a[0], b[0])
+    ip, sp = gpu.spikes(ids["gpu"][0])
+    assert len(ip) > 500 and not np.any((sp >= 60) & (sp < 90))   # the rate-0 row
+    assert len(gpu.spikes(ids["gpu"][1])[0]) > 0
+    np.testing.assert_allclose(gpu.get_state(ids["gpu"][1], "v"),
+                               orc.get_state(ids["orc"][1], "v"), rtol=1e-10, atol=1e-15)
