@@ -264,7 +264,7 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
       fold_clear<R, 4>(fge, q);
       fold_clear<R, 4>(fgi, q);
     }
-    emit_spikes<4>(P, q, fl, ts, slot, status);
+    emit_spikes_warp<4>(P, q, fl, ts, slot, status);
     cur = nxt;
   }
   clear_next_slot(P, ts);

@@ -95,6 +95,58 @@ __device__ __forceinline__ void emit_spikes(const PopDev& P, int64_t q, unsigned
   }
 }
 
+// emit_spikes for kernels that call it in a loop (hh_stream_kernel): every lane of a warp
+// must call this, which synchronises the warp, not the block, so the warps of a CTA are not
+// held in step once per iteration.  A warp with spikes reserves its range in the slot (and
+// the monitor) with one atomicAdd from its last lane after a warp-wide scan of the counts;
+// a warp without spikes returns after one ballot.  The order of spikes within a slot is
+// arbitrary (the monitor is read sorted, and delivery sums commute).  One-shot kernels keep
+// the block form: at 1e5 neurons a burst step reaches ~3000 warps with spikes, whose
+// atomics on the one slot counter would serialise where ~400 CTAs' do not.
+template <int E>
+__device__ __forceinline__ void emit_spikes_warp(const PopDev& P, int64_t q, unsigned fl,
+                                            int64_t ts, int slot, int32_t* status) {
+  constexpr unsigned kAll = 0xffffffffu;
+  if (!__ballot_sync(kAll, fl != 0)) return;
+  const int lane = threadIdx.x & 31;
+  const int c = __popc(fl);
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kAll, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(kAll, incl, 31);
+  int base = 0;
+  unsigned long long mbase = 0;
+  if (lane == 31) {
+    base = atomicAdd(&P.ring_cnt[slot], total);
+    if (P.mon_cnt) mbase = atomicAdd(P.mon_cnt, (unsigned long long)total);
+  }
+  base = __shfl_sync(kAll, base, 31);
+  mbase = __shfl_sync(kAll, mbase, 31);
+  if (c == 0) return;
+  int32_t* out = P.ring_idx + (int64_t)slot * P.n;
+  int pos = base + incl - c;
+  unsigned long long mpos = P.mon_cnt ? mbase + (unsigned long long)(incl - c) : 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    if (fl & (1u << e)) {
+      const int32_t idx = (int32_t)(E * q + e);
+      out[pos++] = idx;
+      if (P.mon_cnt) {
+        if (mpos < (unsigned long long)P.mon_cap) {
+          P.mon_idx[mpos] = idx;
+          P.mon_step[mpos] = ts;
+        } else {
+          set_status(status, B2B_ERR_QUEUE_OVERFLOW);
+        }
+        ++mpos;
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void clear_next_slot(const PopDev& P, int64_t ts) {
   if (blockIdx.x == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
 }

@@ -587,3 +587,29 @@ def test_small_network_path_matches_per_step(gpu_factory, case):
     np.testing.assert_array_equal(out[True][1], out[False][1])
     for v in ("v", "ge", "gi", "lastspike"):
         np.testing.assert_array_equal(out[True][2][v], out[False][2][v], err_msg=v)
+
+
+@pytest.mark.parametrize("inputs", [False, True])
+def test_hh_stream_kernel_matches_per_step_kernel(gpu_factory, inputs):
+    """A float32 HH population large enough for the streaming kernel (four neurons per
+    thread, resident CTAs walking the population, warp-level spike compaction) gives the
+    same spikes and state, bit for bit, as the one-neuron-per-thread kernel: the per-neuron
+    arithmetic is shared.  With inputs, a PoissonInput onto ge exercises that variant."""
+    n = 640_000
+    out = {}
+    for e in (4, 1):
+        net = gpu_factory(DT, seed=2)
+        P = net.hh_group(n, models.cobahh_hh(), "float32")
+        rng = np.random.default_rng(4)
+        net.set_state(P, "v", rng.uniform(-70e-3, -40e-3, n))
+        if inputs:
+            net.poisson_input(P, "ge", 100, 50.0, 3e-9)
+        net.spike_monitor(P, 4 * n)
+        net.finalize()
+        net.tune_apply([{"site_kind": 1, "site_index": 0, "choice_a": e, "choice_b": 256}])
+        net.run(40)
+        idx, st = net.spikes(P)
+        out[e] = (idx, st, net.get_state(P, "v"), net.get_state(P, "ge"), net.get_state(P, "m"))
+    assert len(out[1][0]) > 1000
+    for k in range(5):
+        np.testing.assert_array_equal(out[4][k], out[1][k], err_msg=str(k))
