@@ -9,7 +9,8 @@
 // E = 4 for large populations (each state array read with one 128-bit access, two for
 // float64), E = 1 when the population is too small to fill the GPU that way.  The CTA
 // compacts its spikes with warp shuffles and a shared-memory scan and reserves its output
-// range with a single atomicAdd on the step's slot of the spike-history ring.
+// range with a single atomicAdd on the step's slot of the spike-history ring (the streaming
+// kernel, which compacts once per pack iteration, does this per warp instead).
 //
 // The reset is applied in the same pass when no synaptic effect of the population writes a
 // variable the reset writes; otherwise `late_reset` defers it to a kernel that runs after
