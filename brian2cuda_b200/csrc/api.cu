@@ -349,8 +349,11 @@ b2b_status finalize_pops(b2b_net* net) {
     // spike generator entries
     if (pop.kind == KIND_SPIKEGEN) {
       std::vector<std::pair<int64_t, int32_t>> ent;
+      D.sg_period = net->groups[pop.groups[0]].sg_period;
       for (int gi : pop.groups) {
         const Group& g = net->groups[gi];
+        CHECK(g.sg_period == D.sg_period, B2B_ERR_UNSUPPORTED,
+              "SpikeGeneratorGroups of one net must share one period");
         for (size_t k = 0; k < g.sg_idx.size(); ++k)
           ent.emplace_back(g.sg_step[k], (int32_t)(g.sg_idx[k] + g.offset));
       }
@@ -1191,6 +1194,22 @@ b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64
   g.ta_div = div;
   return B2B_OK;
   GUARD_END
+}
+
+b2b_status b2b_spikegen_period(b2b_net* net, int32_t gid, int64_t period_steps) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(!net->finalized, B2B_ERR_STATE, "the period must be set before b2b_finalize");
+  CHECK(gid >= 0 && gid < (int)net->groups.size() &&
+            net->groups[gid].kind == KIND_SPIKEGEN,
+        B2B_ERR_INVALID_ARG, "group %d is not a SpikeGeneratorGroup", gid);
+  Group& g = net->groups[gid];
+  CHECK(period_steps >= 0, B2B_ERR_INVALID_ARG, "negative period");
+  for (int64_t s : g.sg_step)
+    CHECK(period_steps == 0 || s < period_steps, B2B_ERR_INVALID_ARG,
+          "spike at step %lld is not inside the period of %lld steps", (long long)s,
+          (long long)period_steps);
+  g.sg_period = period_steps;
+  return B2B_OK;
 }
 
 b2b_status b2b_state_set(b2b_net* net, int32_t gid, int32_t var, const void* host, int64_t n) {

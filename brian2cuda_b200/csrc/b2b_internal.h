@@ -94,6 +94,7 @@ struct PopDev {
   const int32_t* sg_idx;          // spike generator entries sorted by step
   const int64_t* sg_step;
   int64_t sg_n;
+  int64_t sg_period;              // > 0: the entries repeat every sg_period steps
   int32_t late_reset;             // reset must run after synaptic delivery
   int32_t pad;
   // The step as two concurrent launches (pending.cu): per variable (v, ge, gi), [2][n] input
@@ -200,6 +201,7 @@ struct Group {
   double rate = 0;
   std::vector<int32_t> sg_idx;
   std::vector<int64_t> sg_step;
+  int64_t sg_period = 0;                      // steps; 0: no repetition
   std::vector<std::vector<uint8_t>> staged;   // per var host bytes staged before finalize
   int64_t mon_cap = 0;
   b2b_mlp* surr = nullptr;                    // gating surrogate (HH float32), or none

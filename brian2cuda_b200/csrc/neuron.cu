@@ -320,8 +320,11 @@ __global__ void spikegen_step_kernel(PopDev P, const int64_t* __restrict__ clock
   __shared__ int64_t s_lo, s_hi;
   __shared__ unsigned long long s_mbase;
   if (threadIdx.x == 0) {
-    s_lo = lower_bound_i64(P.sg_step, P.sg_n, ts);
-    s_hi = lower_bound_i64(P.sg_step, P.sg_n, ts + 1);
+    // with a period, step ts emits the entries of bin ts mod period
+    // (brian2cuda/templates/spikegenerator.cu:42-49)
+    const int64_t bin = P.sg_period > 0 ? ts % P.sg_period : ts;
+    s_lo = lower_bound_i64(P.sg_step, P.sg_n, bin);
+    s_hi = lower_bound_i64(P.sg_step, P.sg_n, bin + 1);
     const int cnt = (int)(s_hi - s_lo);
     P.ring_cnt[slot] = cnt;
     P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;

@@ -134,6 +134,14 @@ class HinesParams:
                          self.gK, self.Vthr])
 
 
+def spike_steps(times, dt: float) -> np.ndarray:
+    """Steps of spike times for a SpikeGeneratorGroup: the bin [k dt, (k+1) dt) holding each
+    time, by Brian2's timestep(t, dt) = int((t + 1e-3 dt) / dt) (brian2cuda/cuda_generator.py:
+    997-1006), so that times computed as k*dt land in bin k despite rounding."""
+    t = np.asarray(times, dtype=np.float64)
+    return ((t + 1e-3 * dt) / dt).astype(np.int64)
+
+
 class Network:
     """A network on one GPU.  Build it (groups, synapses, monitors), call `finalize()`,
     then `run(steps)`; state can be read and written between runs."""
@@ -224,12 +232,17 @@ class Network:
                     "poisson")
         return self._add("poisson", n, code, gid)
 
-    def spikegen_group(self, n: int, indices, steps) -> int:
+    def spikegen_group(self, n: int, indices, steps, period: int = 0) -> int:
+        """SpikeGeneratorGroup: neuron indices[k] spikes at step steps[k] (spike_steps()
+        turns times into steps); period > 0 repeats the pattern every `period` steps."""
         idx = np.ascontiguousarray(indices, dtype=np.int32)
         stp = np.ascontiguousarray(steps, dtype=np.int64)
         gid = C.c_int32()
         self._check(self._lib.b2b_group_spikegen(self._h, n, len(idx), _ptr(idx), _ptr(stp),
                                                  C.byref(gid)), "spikegen")
+        if period:
+            self._check(self._lib.b2b_spikegen_period(self._h, gid.value, int(period)),
+                        "spikegen period")
         return self._add("spikegen", n, N.F32, gid)
 
     def timed_array(self, gid: int, values, dt_array: float) -> None:

@@ -132,6 +132,11 @@ b2b_status b2b_group_poisson(b2b_net* net, int64_t n, int32_t dtype, double rate
  * (brian2cuda/templates/spikegenerator.cu:41-148). */
 b2b_status b2b_group_spikegen(b2b_net* net, int64_t n, int64_t n_spikes, const int32_t* idx,
                               const int64_t* step, int32_t* gid);
+/* SpikeGeneratorGroup(..., period=P): the entries repeat every period_steps steps (step ts
+ * emits the entries of step ts mod period_steps; every entry must lie inside the period),
+ * brian2cuda/templates/spikegenerator.cu:42-49, 88-96.  0 = no repetition.  Before
+ * b2b_finalize; the SpikeGeneratorGroups of one net share one period. */
+b2b_status b2b_spikegen_period(b2b_net* net, int32_t gid, int64_t period_steps);
 
 /* TimedArray input of a LIF, HH or Poisson group (replaces the function brian2cuda/timedarray.py:
  * 10-58 generates for `ta(t)` / `ta(t, i)` in the group's equations).  values[rows][cols]

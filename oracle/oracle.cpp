@@ -107,6 +107,7 @@ struct Group {
   std::vector<uint8_t> not_ref;
   std::vector<int32_t> spikes;  // spikespace of the current step, ascending
   std::vector<std::pair<int64_t, int32_t>> sg;  // spike generator (step, idx), sorted
+  int64_t sg_period = 0;                        // > 0: the entries repeat every period steps
   std::vector<std::vector<R>> uniforms;         // Poisson: queued rows, one per step
   size_t uni_next = 0;
   std::vector<std::pair<int64_t, int32_t>> recorded;  // (step, idx)
@@ -324,8 +325,10 @@ bool threshold(Net<R>& net, Group<R>& g, double t) {
       if (u[i] < th) g.spikes.push_back((int32_t)i);
     }
   } else if (g.kind == SPIKEGEN) {
-    auto lo = std::lower_bound(g.sg.begin(), g.sg.end(), std::make_pair(net.ts, (int32_t)-1));
-    for (auto it = lo; it != g.sg.end() && it->first == net.ts; ++it) g.spikes.push_back(it->second);
+    // with a period, step ts emits the entries of step ts mod period
+    const int64_t bin = g.sg_period > 0 ? net.ts % g.sg_period : net.ts;
+    auto lo = std::lower_bound(g.sg.begin(), g.sg.end(), std::make_pair(bin, (int32_t)-1));
+    for (auto it = lo; it != g.sg.end() && it->first == bin; ++it) g.spikes.push_back(it->second);
   }
   for (int32_t i : g.spikes) g.recorded.emplace_back(net.ts, i);
   return true;
@@ -712,6 +715,18 @@ int api_timedarray(Net<R>& net, int gid, const double* vals, int64_t rows, int64
 }
 
 template <typename R>
+int api_spikegen_period(Net<R>& net, int gid, int64_t period) {
+  if (gid < 0 || gid >= (int)net.groups.size() || net.groups[gid].kind != SPIKEGEN ||
+      period < 0)
+    return -1;
+  Group<R>& g = net.groups[gid];
+  for (const auto& e : g.sg)
+    if (period > 0 && e.first >= period) return -1;
+  g.sg_period = period;
+  return 0;
+}
+
+template <typename R>
 int api_state(Net<R>& net, int gid, int var, double* vals, int64_t n, int set) {
   if (gid < 0 || gid >= (int)net.groups.size()) return -1;
   Group<R>& g = net.groups[gid];
@@ -995,6 +1010,11 @@ int orc_timedarray(void* hp, int gid, const double* v, int64_t rows, int64_t col
                    int64_t div) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_timedarray, gid, v, rows, cols, mul, div);
+}
+// SpikeGeneratorGroup period in steps (0: none); every entry must lie inside it
+int orc_spikegen_period(void* hp, int gid, int64_t period) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_spikegen_period, gid, period);
 }
 int orc_state_set(void* hp, int gid, int var, const double* v, int64_t n) {
   Handle* h = static_cast<Handle*>(hp);

@@ -48,6 +48,7 @@ def lib() -> C.CDLL:
             "orc_timedarray": (C.c_int, [P, C.c_int, P, I64, I64, I64, I64]),
             "orc_poisson_input": (C.c_int, [P, C.c_int, C.c_int, I64, D, D]),
             "orc_set_seed": (None, [P, C.c_uint64]),
+            "orc_spikegen_period": (C.c_int, [P, C.c_int, I64]),
             "orc_state_set": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_state_get": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_synapses": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, I64, P, P, P, D, P,
@@ -137,11 +138,14 @@ class OracleNet:
     def poisson_group(self, n, rate, dtype=None):
         return self._add("poisson", n, self._lib.orc_group_poisson(self._h, n, float(rate)))
 
-    def spikegen_group(self, n, indices, steps):
+    def spikegen_group(self, n, indices, steps, period=0):
         idx = np.ascontiguousarray(indices, dtype=np.int32)
         st = np.ascontiguousarray(steps, dtype=np.int64)
-        return self._add("spikegen", n,
-                         self._lib.orc_group_spikegen(self._h, n, len(idx), _p(idx), _p(st)))
+        gid = self._add("spikegen", n,
+                        self._lib.orc_group_spikegen(self._h, n, len(idx), _p(idx), _p(st)))
+        if period:
+            self._ok(self._lib.orc_spikegen_period(self._h, gid, int(period)), "period")
+        return gid
 
     def poisson_input(self, gid, var, n, rate, weight):
         """PoissonInput: every step each neuron adds weight * Binomial(n, rate*dt) to var."""

@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from brian2cuda_b200.network import LIF
+from brian2cuda_b200.network import LIF, spike_steps
 
 DT = 1e-4  # Brian2's defaultclock.dt
 
@@ -146,5 +146,68 @@ def multiple_runs_scalar_delay(make):
     assert trace == [0.0, 0.0, 1.0, 2.0]
 
 
+def spikegenerator_extreme_period(make):
+    """test_spikegenerator.py:12-27: SpikeGeneratorGroup(5, [0, 1, 2], [0, 1, 2] ms,
+    period=1e6 s) run for 10 ms spikes i = [0, 1, 2] at t = [0, 1, 2] ms."""
+    net = make(DT)
+    SG = net.spikegen_group(5, [0, 1, 2], spike_steps(np.array([0, 1, 2]) * 1e-3, DT),
+                            period=int(spike_steps(1e6, DT)))
+    net.spike_monitor(SG, 100)
+    net.finalize()
+    net.run(100)
+    idx, st = net.spikes(SG)
+    np.testing.assert_array_equal(idx, [0, 1, 2])
+    np.testing.assert_array_equal(st, [0, 10, 20])
+
+
+def spikegenerator_period_repeat(make):
+    """test_spikegenerator.py:30-66: one neuron with ten spikes 0.1 ms apart inside a 1 ms
+    period; five runs of 1 ms each record all ten."""
+    net = make(DT)
+    SG = net.spikegen_group(1, np.zeros(10, np.int32), spike_steps(np.arange(0, 1, 0.1) * 1e-3, DT),
+                            period=int(spike_steps(1e-3, DT)))
+    net.spike_monitor(SG, 100)
+    net.finalize()
+    counts, seen = [], 0
+    for _ in range(5):
+        net.run(10)
+        n = len(net.spikes(SG)[0])
+        counts.append(n - seen)
+        seen = n
+    assert counts == [10] * 5
+    _, st = net.spikes(SG)
+    np.testing.assert_array_equal(st, np.arange(50))
+
+
+def spikegenerator_rounding(make):
+    """test_spikegenerator.py:69-104: 100 spike times spread over [0, dt) all fall into the
+    first step; 10000 spikes at times k*dt fall into separate steps, so a target that counts
+    its inputs (threshold always true, reset count = 0, resets before synapses) holds 1 at
+    the end of every step."""
+    net = make(DT)
+    times = np.linspace(0, 0.1, 100, endpoint=False) * 1e-3
+    SG = net.spikegen_group(100, np.arange(100), spike_steps(times, DT))
+    net.spike_monitor(SG, 1000)
+    net.finalize()
+    net.run(1)
+    idx, st = net.spikes(SG)
+    np.testing.assert_array_equal(np.sort(idx), np.arange(100))
+    assert np.all(st == 0)
+
+    net = make(DT, reset_before_synapses=True)
+    SG = net.spikegen_group(1, np.zeros(10000, np.int32), spike_steps(np.arange(10000) * DT, DT))
+    T = net.lif_group(1, LIF(taum=math.inf, Vt=-math.inf, Vr=0.0), "float64")
+    net.synapses(SG, T, "v", [0], [0], w_scalar=1.0, delay=0)
+    mon = net.state_monitor(T, "v", capacity=10001)
+    net.finalize()
+    net.run(10000)
+    steps, vals = net.state_values(mon)
+    # recorded at the start of each step, i.e. the count at the end of the step before
+    np.testing.assert_array_equal(steps, np.arange(10000))
+    np.testing.assert_array_equal(vals[1:, 0], np.ones(9999))
+    assert net.get_state(T, "v")[0] == 1.0
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
-       circular_eventspaces_spikegenerator, multiple_runs_scalar_delay]
+       circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
+       spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding]
