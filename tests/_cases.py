@@ -208,6 +208,62 @@ def spikegenerator_rounding(make):
     assert net.get_state(T, "v")[0] == 1.0
 
 
+def state_monitor_more_threads_than_single_block(make):
+    """test_monitor.py:7-20: NeuronGroup(2000, 'v:1') with v = arange(2000), StateMonitor of
+    every neuron over three steps: every record equals the initial values."""
+    net = make(DT)
+    n = 2000
+    G = net.lif_group(n, LIF(taum=math.inf, has_threshold=False, has_reset=False), "float64")
+    net.set_state(G, "v", np.arange(n, dtype=np.float64))
+    mon = net.state_monitor(G, "v", capacity=3)
+    net.finalize()
+    net.run(3)
+    steps, vals = net.state_values(mon)
+    np.testing.assert_array_equal(steps, [0, 1, 2])
+    for t in range(3):
+        np.testing.assert_array_equal(vals[t], np.arange(n))
+
+
+def spike_monitor_all_attr(make):
+    """test_monitor.py:23-45 (the whole-group monitor): threshold 'do_spike' with
+    do_spike = [T, F, F, F, T, T]: one step records i = [0, 4, 5] at t = 0, counts
+    [1, 0, 0, 0, 1, 1], N = 3."""
+    net = make(DT)
+    G = net.lif_group(6, LIF(taum=math.inf, Vt=0.5, has_reset=False), "float64")
+    net.set_state(G, "v", np.array([1, 0, 0, 0, 1, 1], dtype=np.float64))
+    net.spike_monitor(G, 100)
+    net.finalize()
+    net.run(1)
+    idx, st = net.spikes(G)
+    np.testing.assert_array_equal(idx, [0, 4, 5])
+    np.testing.assert_array_equal(st, [0, 0, 0])
+    np.testing.assert_array_equal(np.bincount(idx, minlength=6), [1, 0, 0, 0, 1, 1])
+
+
+def binomial_values_seeds(make):
+    """test_random_number_generation.py:367-466, for the binomial of a PoissonInput
+    (Binomial(100, 0.1) per neuron and step): two draws differ, the same seed reproduces
+    the values, another seed changes them."""
+    def draws(seed):
+        net = make(DT, seed=seed)
+        G = net.lif_group(10, LIF(taum=math.inf, has_threshold=False, has_reset=False),
+                          "float64")
+        net.poisson_input(G, "v", 100, 0.1 / DT, 1.0)
+        net.finalize()
+        out = []
+        for _ in range(2):
+            before = net.get_state(G, "v").copy()
+            net.run(1)
+            out.append(net.get_state(G, "v") - before)
+        return np.array(out)
+    a, b, c = draws(11400), draws(11400), draws(13579)
+    assert not np.array_equal(a[0], a[1])
+    np.testing.assert_array_equal(a, b)
+    assert not np.array_equal(a, c)
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
-       spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding]
+       spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
+       state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
+       binomial_values_seeds]
