@@ -262,8 +262,50 @@ def binomial_values_seeds(make):
     assert not np.array_equal(a, c)
 
 
+def threads_per_synapse_bundle(make):
+    """test_synaptic_propagations.py:343-374: whatever the threads per synapse bundle, a
+    spike at t = 0 with delays j*dt onto neurons 3 and 4 (v += 1.1, threshold v > 1) makes
+    them spike at steps 4 and 5.  The launch-shape counterpart here is the delivery's lanes
+    per work item (4, 8, 16, 32; the oracle has one form)."""
+    shapes = [4, 8, 16, 32]
+    for lanes in shapes:
+        net = make(DT)
+        inp = net.spikegen_group(1, [0], [0])
+        G = net.lif_group(5, neuron_v1(), "float64")
+        net.synapses(inp, G, "v", [0, 0], [3, 4], w_scalar=1.1, delay=np.array([3, 4], np.int32))
+        net.spike_monitor(G, 100)
+        net.finalize()
+        if not hasattr(net, "tune_apply"):
+            shapes = shapes[:1]
+        else:
+            net.tune_apply([{"site_kind": 6, "site_index": 0, "choice_a": lanes,
+                             "choice_b": 148}])
+        net.run(6)
+        idx, st = net.spikes(G)
+        np.testing.assert_array_equal(idx, [3, 4])
+        np.testing.assert_array_equal(st, [4, 5])
+        if len(shapes) == 1:
+            break
+
+
+def synaptic_effects_onto_one_target(make):
+    """test_synaptic_propagations.py:316-340, its on_pre half: 15 x 1024 neurons spiking
+    every step, each adding 1 to the v of one neuron with no delay; after two steps v holds
+    exactly 2 x 15360 (every one of the same-address additions lands; the on_post half of
+    that test needs an additive on_post pathway, which this library does not have)."""
+    N = 15 * 1024
+    net = make(DT)
+    src = net.lif_group(N, LIF(taum=math.inf, Vt=-math.inf, has_reset=False), "float64")
+    tgt = net.lif_group(1, LIF(taum=math.inf, has_threshold=False, has_reset=False), "float64")
+    net.synapses(src, tgt, "v", np.arange(N, dtype=np.int32), np.zeros(N, np.int32),
+                 w_scalar=1.0, delay=0)
+    net.finalize()
+    net.run(2)
+    assert net.get_state(tgt, "v")[0] == 2.0 * N
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
        spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
-       binomial_values_seeds]
+       binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target]
