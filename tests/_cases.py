@@ -304,8 +304,30 @@ def synaptic_effects_onto_one_target(make):
     assert net.get_state(tgt, "v")[0] == 2.0 * N
 
 
+def poisson_input_schedule(make):
+    """PoissonInput acts in the synapses slot (the BinomialFunction of brian2cuda/binomial.py
+    runs there): with rate 1/dt every draw is N, so v += N w each step.  A LIF with
+    threshold v > 1 and reset v = 0 (N w = 1.5) spikes every second step in the default
+    schedule, where the reset follows the synapses and overwrites the input, and every step
+    from step 1 when resets come first and the input lands after them."""
+    out = {}
+    for reset_first in (False, True):
+        net = make(DT, reset_before_synapses=reset_first)
+        G = net.lif_group(1, LIF(taum=math.inf, Vt=1.0, Vr=0.0), "float64")
+        net.poisson_input(G, "v", 3, 1.0 / DT, 0.5)
+        net.spike_monitor(G, 100)
+        net.finalize()
+        net.run(8)
+        out[reset_first] = (net.spikes(G)[1], float(net.get_state(G, "v")[0]))
+    np.testing.assert_array_equal(out[False][0], [1, 3, 5, 7])
+    assert out[False][1] == 0.0          # step 7 spiked: reset after the input
+    np.testing.assert_array_equal(out[True][0], np.arange(1, 8))
+    assert out[True][1] == 1.5           # reset, then the input
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
        spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
-       binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target]
+       binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target,
+       poisson_input_schedule]
