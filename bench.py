@@ -11,8 +11,8 @@ neuron-updates/s.  Inputs (state, 1.6 GB of synapse arrays) are resident in HBM 
 timing starts; the synapse arrays alone exceed the 126 MB L2.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b2b|reference]
-Under torchrun every rank runs an independent replica (weak scaling; the network does not
-shard) and rank 0 reports the max time over ranks.
+Under torchrun every rank runs an independent replica (weak scaling; the network fits one
+GPU and is not sharded) and rank 0 reports the max time over ranks.
 """
 from __future__ import annotations
 
@@ -757,7 +757,7 @@ def bench_small(args, world, rank, local):
                           ms / args.steps, WORKLOADS[wl],
                           {"sim_steps_per_step": steps_run, "neurons": 4000,
                            "synapses": ids["n_syn"], "parallelism": f"replicas x{world}",
-                           "l2": "working set < L2 (the net is 2.6 MB): no flush, see DESIGN.md"},
+                           "l2": "working set < L2 (the net is 2.6 MB): no flush"},
                           "f64")
         line.update({"neuron_updates_per_s": 4000.0 * steps_run * args.steps * world / sec,
                      "firing_rate_hz": nspk / (4000 * steps_run * DT), "roofline": roof,
