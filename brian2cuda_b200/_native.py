@@ -85,6 +85,7 @@ PROTOTYPES = {
     "b2b_group_hh": (I32, [P, I64, I32, C.POINTER(HhParams), PI32]),
     "b2b_group_poisson": (I32, [P, I64, I32, DBL, PI32]),
     "b2b_group_spikegen": (I32, [P, I64, I64, P, P, PI32]),
+    "b2b_spikemon_get_range": (I32, [P, I32, I64, I64, PI64, P, P, I64]),
     "b2b_spikegen_period": (I32, [P, I32, I64]),
     "b2b_timedarray": (I32, [P, I32, P, I64, I64, DBL]),
     "b2b_poisson_input": (I32, [P, I32, I32, I64, DBL, DBL, PI32]),

@@ -1969,26 +1969,36 @@ b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
                             int64_t* step, int64_t cap) {
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  return b2b_spikemon_get_range(net, gid, 0, net->groups[gid].n, n, idx, step, cap);
+}
+
+b2b_status b2b_spikemon_get_range(b2b_net* net, int32_t gid, int64_t lo, int64_t hi,
+                                  int64_t* n, int32_t* idx, int64_t* step, int64_t cap) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   CHECK(n != nullptr, B2B_ERR_INVALID_ARG, "n is NULL");
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   const Group& g = net->groups[gid];
   CHECK(g.mon_cap > 0, B2B_ERR_STATE, "group %d has no spike monitor", gid);
+  CHECK(0 <= lo && lo <= hi && hi <= g.n, B2B_ERR_INVALID_ARG,
+        "bad subgroup [%lld, %lld) of a %lld-neuron group", (long long)lo, (long long)hi,
+        (long long)g.n);
   GUARD_BEGIN
   const PopDev& D = net->pops[g.pop].dev;
   CU(cudaStreamSynchronize(net->stream));
   unsigned long long total = 0;
   CU(cudaMemcpy(&total, D.mon_cnt, sizeof(total), cudaMemcpyDeviceToHost));
   const int64_t m = std::min<int64_t>((int64_t)total, D.mon_cap);
-  std::vector<int32_t> hi(m);
-  std::vector<int64_t> hs(m);
+  std::vector<int32_t> midx(m);
+  std::vector<int64_t> mstep(m);
   if (m) {
-    CU(cudaMemcpy(hi.data(), D.mon_idx, 4 * m, cudaMemcpyDeviceToHost));
-    CU(cudaMemcpy(hs.data(), D.mon_step, 8 * m, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(midx.data(), D.mon_idx, 4 * m, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(mstep.data(), D.mon_step, 8 * m, cudaMemcpyDeviceToHost));
   }
   std::vector<std::pair<int64_t, int32_t>> ent;
   for (int64_t k = 0; k < m; ++k)
-    if (hi[k] >= g.offset && hi[k] < g.offset + g.n)
-      ent.emplace_back(hs[k], (int32_t)(hi[k] - g.offset));
+    if (midx[k] >= g.offset + lo && midx[k] < g.offset + hi)
+      ent.emplace_back(mstep[k], (int32_t)(midx[k] - g.offset - lo));
   std::sort(ent.begin(), ent.end());
   *n = (int64_t)ent.size();
   for (int64_t k = 0; k < (int64_t)ent.size() && k < cap; ++k) {

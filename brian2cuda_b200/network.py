@@ -470,15 +470,19 @@ class Network:
                                   r.get("best_ms", 0.0), r.get("default_ms", 0.0))
         self._check(self._lib.b2b_tune_apply(self._h, arr, len(results)), "tune_apply")
 
-    def spikes(self, gid: int) -> tuple[np.ndarray, np.ndarray]:
-        """All recorded spikes of a monitored group as (indices, steps), sorted by step."""
+    def spikes(self, gid: int, sub: tuple[int, int] | None = None
+               ) -> tuple[np.ndarray, np.ndarray]:
+        """All recorded spikes of a monitored group as (indices, steps), sorted by step; with
+        sub = (lo, hi), those of the subgroup G[lo:hi] with indices relative to lo."""
+        lo, hi = sub if sub is not None else (0, self.group_size(gid))
         n = C.c_int64()
-        self._check(self._lib.b2b_spikemon_get(self._h, gid, C.byref(n), None, None, 0),
-                    "spikemon_get")
+        self._check(self._lib.b2b_spikemon_get_range(self._h, gid, lo, hi, C.byref(n), None,
+                                                     None, 0), "spikemon_get")
         idx = np.empty(n.value, dtype=np.int32)
         stp = np.empty(n.value, dtype=np.int64)
-        self._check(self._lib.b2b_spikemon_get(self._h, gid, C.byref(n), _ptr(idx), _ptr(stp),
-                                               len(idx)), "spikemon_get")
+        self._check(self._lib.b2b_spikemon_get_range(self._h, gid, lo, hi, C.byref(n),
+                                                     _ptr(idx), _ptr(stp), len(idx)),
+                    "spikemon_get")
         return idx, stp
 
     def spikes_fetch(self, gid: int, start: int, cap: int = 1 << 22):

@@ -335,6 +335,10 @@ b2b_status b2b_spikemon(b2b_net* net, int32_t gid, int64_t capacity);
 /* Copies recorded spikes sorted by (step, index); *n receives the total recorded. */
 b2b_status b2b_spikemon_get(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx,
                             int64_t* step, int64_t cap);
+/* The same for the subgroup G[lo:hi] (SpikeMonitor(G[lo:hi]), indices relative to lo, as
+ * brian2cuda/tests/test_monitor.py:23-45 expects), read from the group's monitor. */
+b2b_status b2b_spikemon_get_range(b2b_net* net, int32_t gid, int64_t lo, int64_t hi,
+                                  int64_t* n, int32_t* idx, int64_t* step, int64_t cap);
 /* Incremental readout: *total receives the number of entries the monitor of gid's
  * population has recorded; entries [start, min(total, start + cap)) are copied in recording
  * order, keeping those of group gid (group-local index), and *n receives how many were kept.

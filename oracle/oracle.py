@@ -262,11 +262,14 @@ class OracleNet:
     def timestep(self):
         return self._lib.orc_timestep(self._h)
 
-    def spikes(self, gid):
+    def spikes(self, gid, sub=None):
         n = self._ok(self._lib.orc_spikes(self._h, gid, None, None, 0), "spikes")
         idx = np.empty(n, dtype=np.int32)
         st = np.empty(n, dtype=np.int64)
         self._lib.orc_spikes(self._h, gid, _p(idx), _p(st), n)
+        if sub is not None:
+            keep = (idx >= sub[0]) & (idx < sub[1])
+            idx, st = idx[keep] - sub[0], st[keep]
         return idx, st
 
     def spikes_last(self, gid):

@@ -225,9 +225,9 @@ def state_monitor_more_threads_than_single_block(make):
 
 
 def spike_monitor_all_attr(make):
-    """test_monitor.py:23-45 (the whole-group monitor): threshold 'do_spike' with
-    do_spike = [T, F, F, F, T, T]: one step records i = [0, 4, 5] at t = 0, counts
-    [1, 0, 0, 0, 1, 1], N = 3."""
+    """test_monitor.py:23-45: threshold 'do_spike' with do_spike = [T, F, F, F, T, T]: one
+    step records i = [0, 4, 5] at t = 0, counts [1, 0, 0, 0, 1, 1], N = 3; the subgroup
+    monitors G[:2], G[2:4], G[4:] hold [0], nothing and [0, 1] (relative indices)."""
     net = make(DT)
     G = net.lif_group(6, LIF(taum=math.inf, Vt=0.5, has_reset=False), "float64")
     net.set_state(G, "v", np.array([1, 0, 0, 0, 1, 1], dtype=np.float64))
@@ -238,6 +238,13 @@ def spike_monitor_all_attr(make):
     np.testing.assert_array_equal(idx, [0, 4, 5])
     np.testing.assert_array_equal(st, [0, 0, 0])
     np.testing.assert_array_equal(np.bincount(idx, minlength=6), [1, 0, 0, 0, 1, 1])
+    for (lo, hi), want in (((0, 2), [0]), ((2, 4), []), ((4, 6), [0, 1])):
+        i, t = net.spikes(G, sub=(lo, hi))
+        np.testing.assert_array_equal(i, want)
+        np.testing.assert_array_equal(t, np.zeros(len(want)))
+        np.testing.assert_array_equal(np.bincount(i, minlength=hi - lo),
+                                      np.bincount(np.array(want, dtype=np.int64),
+                                                  minlength=hi - lo))
 
 
 def binomial_values_seeds(make):
