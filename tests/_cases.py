@@ -332,9 +332,26 @@ def poisson_input_schedule(make):
     assert out[True][1] == 1.5           # reset, then the input
 
 
+def refractory_without_spikes(make):
+    """test_stateupdaters.py:169-194, for the exact integrator: dv/dt = -v/(10 ms) with
+    v = (i+1)/11, with and without (unless refractory) and refractory = 1 ms; a group that
+    never spikes is never refractory, so both give v = (i+1)/11 exp(-1) after 10 ms."""
+    net = make(DT)
+    plain = net.lif_group(10, LIF(taum=10e-3, has_threshold=False, has_reset=False), "float64")
+    refr = net.lif_group(10, LIF(taum=10e-3, has_threshold=False, has_reset=False,
+                                 refractory=1e-3, unless_refractory=True), "float64")
+    v0 = (np.arange(10) + 1) / 11.0
+    net.set_state(plain, "v", v0)
+    net.set_state(refr, "v", v0)
+    net.finalize()
+    net.run(100)
+    np.testing.assert_array_equal(net.get_state(refr, "v"), net.get_state(plain, "v"))
+    np.testing.assert_allclose(net.get_state(plain, "v"), v0 * math.exp(-1.0), rtol=1e-12)
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
        spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
        binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target,
-       poisson_input_schedule]
+       poisson_input_schedule, refractory_without_spikes]
