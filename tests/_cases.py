@@ -349,9 +349,27 @@ def refractory_without_spikes(make):
     np.testing.assert_allclose(net.get_state(plain, "v"), v0 * math.exp(-1.0), rtol=1e-12)
 
 
+def multiple_runs_heterogeneous_delay(make):
+    """test_network_multiple_runs.py:89-108: an always-spiking input, `v += 1` with delays
+    0 and dt onto two neurons, two runs of two steps; v at the start of each step is
+    [0, 1, 2, 3] and [0, 0, 1, 2]."""
+    net = make(DT)
+    inG = net.lif_group(1, LIF(taum=math.inf, Vt=-math.inf, has_reset=False), "float64")
+    G = net.lif_group(2, LIF(taum=math.inf, has_threshold=False, has_reset=False), "float64")
+    net.synapses(inG, G, "v", [0, 0], [0, 1], w_scalar=1.0, delay=np.array([0, 1], np.int32))
+    mon = net.state_monitor(G, "v", capacity=4)
+    net.finalize()
+    net.run(2)
+    net.run(2)
+    steps, vals = net.state_values(mon)
+    np.testing.assert_array_equal(steps, [0, 1, 2, 3])
+    np.testing.assert_array_equal(vals[:, 0], [0, 1, 2, 3])
+    np.testing.assert_array_equal(vals[:, 1], [0, 0, 1, 2])
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
        spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
        binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target,
-       poisson_input_schedule, refractory_without_spikes]
+       poisson_input_schedule, refractory_without_spikes, multiple_runs_heterogeneous_delay]
