@@ -424,6 +424,13 @@ class Network:
         return ts.value
 
     @property
+    def t(self) -> float:
+        """Time of the next step in seconds (Brian2's net.t / defaultclock.t after a run)."""
+        t = C.c_double()
+        self._lib.b2b_time(self._h, None, C.byref(t))
+        return t.value
+
+    @property
     def run_mode(self) -> str:
         """'fused' (two concurrent launches per step), 'small' (one CTA runs every step of a
         chunk) or 'per-step' (graph-replayed kernels)."""

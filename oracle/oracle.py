@@ -262,6 +262,10 @@ class OracleNet:
     def timestep(self):
         return self._lib.orc_timestep(self._h)
 
+    @property
+    def t(self):
+        return self.timestep * self.dt
+
     def spikes(self, gid, sub=None):
         n = self._ok(self._lib.orc_spikes(self._h, gid, None, None, 0), "spikes")
         idx = np.empty(n, dtype=np.int32)

@@ -367,9 +367,25 @@ def multiple_runs_heterogeneous_delay(make):
     np.testing.assert_array_equal(vals[:, 1], [0, 0, 1, 2])
 
 
+def time_after_run(make):
+    """test_cuda_standalone.py:139-167: t is 0 before a run, 10 ms after run(10 ms) and
+    20 ms after a second one (dt = 0.1 ms)."""
+    net = make(DT)
+    net.lif_group(10, LIF(taum=10e-3, has_threshold=False, has_reset=False), "float64")
+    net.finalize()
+    assert net.timestep == 0 and net.t == 0.0
+    net.run(100)
+    assert net.timestep == 100
+    np.testing.assert_allclose(net.t, 10e-3, rtol=1e-12)
+    net.run(100)
+    assert net.timestep == 200
+    np.testing.assert_allclose(net.t, 20e-3, rtol=1e-12)
+
+
 ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        circular_eventspaces_spikegenerator, multiple_runs_scalar_delay,
        spikegenerator_extreme_period, spikegenerator_period_repeat, spikegenerator_rounding,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
        binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target,
-       poisson_input_schedule, refractory_without_spikes, multiple_runs_heterogeneous_delay]
+       poisson_input_schedule, refractory_without_spikes, multiple_runs_heterogeneous_delay,
+       time_after_run]
