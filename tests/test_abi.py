@@ -55,6 +55,23 @@ def test_null_arguments_are_rejected_without_touching_the_gpu():
     assert lib.b2b_destroy(None) == 1
     assert lib.b2b_run(None, 1) == 1
     assert lib.b2b_hines_run(None, 1) == 1
+    # the group inputs and monitor readers
+    assert lib.b2b_timedarray(None, 0, None, 1, 1, 1e-4) == 1
+    assert lib.b2b_poisson_input(None, 0, 0, 10, 5.0, 1.0, None) == 1
+    assert lib.b2b_spikegen_period(None, 0, 10) == 1
+    assert lib.b2b_spikemon_get_range(None, 0, 0, 1, None, None, None, 0) == 1
+
+
+def test_spike_steps_bins_times_like_brian2_timestep():
+    """Times become steps by timestep(t, dt) = int((t + 1e-3 dt) / dt): [k dt, (k+1) dt)
+    lands in step k, and k*dt computed in floating point stays in step k."""
+    import numpy as np
+    from brian2cuda_b200.network import spike_steps
+    dt = 1e-4
+    k = np.arange(100000)
+    np.testing.assert_array_equal(spike_steps(k * dt, dt), k)
+    np.testing.assert_array_equal(spike_steps(np.linspace(0, dt, 100, endpoint=False), dt), 0)
+    np.testing.assert_array_equal(spike_steps([0.5 * dt, 1.5 * dt, 2.9 * dt], dt), [0, 1, 2])
 
 
 def _have_gpu():
