@@ -34,6 +34,14 @@
 //     202-307, combination 316-351, currents 359-387), restated from the cable equation
 //     (see the Hines section below).
 //   * Philox-4x32-10 connectivity generation restated from Salmon et al., SC 2011.
+//   * Inputs: TimedArray values held over each interval of the array's dt, clamped to the
+//     last row (brian2cuda/timedarray.py:10-58), as a LIF drive, an HH current or a
+//     PoissonGroup rate; PoissonInput as weight * Binomial(N, rate dt) per neuron and step
+//     in the synapses slot (the BinomialFunction of brian2cuda/binomial.py:12-121), drawn
+//     by sequential-search inversion from one Philox word; SpikeGeneratorGroup periods
+//     (templates/spikegenerator.cu:42-49: step t emits the entries of step t mod period).
+//   * Monitors: StateMonitor at the start of a step, PopulationRateMonitor at its end
+//     (templates/statemonitor.cu, templates/ratemonitor.cu).
 //
 // Arithmetic: R = double (reference mode) or float (same-precision mode).
 #include <stdint.h>
