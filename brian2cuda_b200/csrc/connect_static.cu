@@ -2,16 +2,19 @@
 //
 // The same generator as b2b_synapses_random (Philox-4x32-10 counter-based connect(p) with
 // uniform integer delays, philox.cuh), for callers that must not allocate device memory:
-// code running while a CUDA graph is being captured (cudaMalloc cannot be captured and
-// synchronises the device), applications whose device memory is owned by a pooling
-// allocator (PyTorch's caching allocator, RMM) that a library's own cudaMalloc would bypass
-// and fragment, and host loops with latency budgets that an implicit device-wide
-// synchronisation of cudaMalloc/cudaFree would break.  Its only scratch — the per-row
-// synapse counts and their prefix sum — lives in a file-scope __device__ array of
-// B2B_STATIC_MAX_ROWS + 1 int64 entries (8 MiB), which every GPU that loads the library holds
-// until exit.  All calls share that array, so calls that overlap on the GPU (different
-// streams, or different host threads) race; each call writes every entry it reads before
-// reading it.
+// applications whose device memory is owned by a pooling allocator (PyTorch's caching
+// allocator, RMM) that a library's own cudaMalloc would bypass and fragment, and host loops
+// with latency budgets that the implicit device-wide synchronisation of cudaMalloc/cudaFree
+// would break.  Its only scratch — the per-row synapse counts and their prefix sum — lives
+// in a file-scope __device__ array of B2B_STATIC_MAX_ROWS + 1 int64 entries (8 MiB), which
+// every GPU that loads the library holds until exit.  All calls share that array, so calls
+// that overlap on the GPU (different streams, or different host threads) race; each call
+// writes every entry it reads before reading it.
+//
+// The device address of the array is looked up with cudaGetSymbolAddress once per device
+// and CUDA context: the lookup is repeated when the device's current context is another
+// one than at the last lookup (after cudaDeviceReset, or a primary context released and
+// created again), so a cached address never outlives the context it belongs to.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -29,6 +32,12 @@ __device__ __align__(256) int64_t g_row_scratch[B2B_STATIC_MAX_ROWS + 1];
 
 std::mutex g_setup_mutex;
 int64_t* g_scratch_addr[kMaxDevices] = {};
+void* g_scratch_ctx[kMaxDevices] = {};
+
+// cuCtxGetCurrent, fetched through the runtime so that the library needs no link against
+// the driver library (the CPU-only test machines load it without a driver).
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 __global__ void static_count_kernel(int64_t pre_lo, int64_t rows, int64_t n_post, uint64_t thr,
                                     uint64_t seed, int64_t* __restrict__ counts) {
@@ -121,14 +130,27 @@ __global__ void static_fill_kernel(int64_t pre_lo, int64_t rows, int64_t n_post,
   }
 }
 
-// Device address of the scratch array on `device` (the current device), looked up once.
+// Device address of the scratch array on `device` (the current device, whose primary
+// context cudaSetDevice has made current), looked up once per device and context.
 cudaError_t scratch_for(int device, int64_t** out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[device]) {
+  cudaError_t e = cudaSuccess;
+  if (!g_ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+  }
+  void* ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
+  if (!g_scratch_addr[device] || g_scratch_ctx[device] != ctx) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_row_scratch);
+    e = cudaGetSymbolAddress(&p, g_row_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_addr[device] = static_cast<int64_t*>(p);
+    g_scratch_ctx[device] = ctx;
   }
   *out = g_scratch_addr[device];
   return cudaSuccess;
@@ -151,6 +173,9 @@ extern "C" b2b_status b2b_connect_random_static(int32_t device, void* stream, in
       dmax < dmin)
     return B2B_ERR_INVALID_ARG;
   if ((int64_t)pre_hi - pre_lo > B2B_STATIC_MAX_ROWS) return B2B_ERR_INVALID_ARG;
+  // An error left pending by earlier work of the caller is reported as it is and not
+  // consumed: a launch error of this call must not be confused with it.
+  if (cudaPeekAtLastError() != cudaSuccess) return B2B_ERR_CUDA;
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return B2B_ERR_CUDA;
   if (cudaSetDevice(device) != cudaSuccess) return B2B_ERR_CUDA;
@@ -164,7 +189,15 @@ extern "C" b2b_status b2b_connect_random_static(int32_t device, void* stream, in
     int64_t grid = (rows + 7) / 8;
     if (grid > 16 * kNumSMs) grid = 16 * kNumSMs;
     static_count_kernel<<<(unsigned)grid, 256, 0, s>>>(pre_lo, rows, n_post, thr, seed, row);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
     static_scan_kernel<<<1, 1024, 0, s>>>(row, rows + 1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    int64_t grid = (rows + 7) / 8;
+    if (grid > 16 * kNumSMs) grid = 16 * kNumSMs;
     static_fill_kernel<<<(unsigned)grid, 256, 0, s>>>(pre_lo, rows, n_post, thr, seed, dmin,
                                                       dmax - dmin + 1, row, capacity, dev_i,
                                                       dev_j, dev_delay);

@@ -220,19 +220,20 @@ b2b_status b2b_synapses_random(b2b_net* net, int32_t pre_gid, int32_t pre_lo, in
 
 /* The same generator as b2b_synapses_random, writing into caller-provided device arrays and
  * allocating nothing (no counterpart in the reference).  For callers that cannot allocate
- * device memory: code running under CUDA graph capture (cudaMalloc is not capturable and
- * synchronises the device), applications whose device memory belongs to a pooling allocator
- * (PyTorch's caching allocator, RMM) that a library cudaMalloc would bypass, and host loops
- * that cannot afford the implicit device synchronisation of cudaMalloc/cudaFree.
+ * device memory: applications whose device memory belongs to a pooling allocator (PyTorch's
+ * caching allocator, RMM) that a library cudaMalloc would bypass, and host loops that cannot
+ * afford the implicit device synchronisation of cudaMalloc/cudaFree.
  * Rows i in [pre_lo, pre_hi) (at most B2B_STATIC_MAX_ROWS of them, else B2B_ERR_INVALID_ARG)
  * against posts j in [0, n_post); synapses are written in (i, j) order as int32 i, j and delay
  * (steps, uniform on [dmin, dmax]) up to `capacity` entries; *n_syn receives the number
  * generated, and B2B_ERR_QUEUE_OVERFLOW is returned when it exceeds capacity.  Runs on
  * `stream` of `device` and waits for it.  Scratch: a file-scope device array of
  * B2B_STATIC_MAX_ROWS + 1 int64 (8 MiB) that every GPU loading the library holds until exit;
- * its device address is looked up (cudaGetSymbolAddress) on the first call on each device, so
- * make that first call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race. */
+ * its device address is looked up (cudaGetSymbolAddress) on the first call on each device, and
+ * again on the first call after the device's context changed (cudaDeviceReset), so make that
+ * first call before any stream capture.  A CUDA error already pending on entry is returned as
+ * B2B_ERR_CUDA without being cleared.  All calls share the array: calls that overlap on the
+ * GPU race. */
 #define B2B_STATIC_MAX_ROWS (1 << 20)
 b2b_status b2b_connect_random_static(int32_t device, void* stream, int32_t pre_lo,
                                      int32_t pre_hi, int32_t n_post, double p, int32_t dmin,

@@ -1,9 +1,9 @@
 """b2b_connect_random_static: the allocation-free connectivity generator.
 
-Some callers of this library cannot allocate device memory: code running while a CUDA graph
-is captured, applications whose device memory belongs to a pooling allocator, and host loops
-that cannot afford the device-wide synchronisation of cudaMalloc.  This entry point keeps its
-scratch in a static device array instead.  The test calls it twice in a row through the C ABI
+Some callers of this library cannot allocate device memory: applications whose device memory
+belongs to a pooling allocator, and host loops that cannot afford the device-wide
+synchronisation of cudaMalloc.  This entry point keeps its scratch in a static device array
+instead.  The test calls it twice in a row through the C ABI
 and compares each result with the generator behind b2b_synapses_random (the existing entry
 point), which numbers synapses in (i, delay, j) order while this one writes (i, j) order.
 This file sorts last so that a run stopping at the first failure has run every other test.
@@ -28,10 +28,11 @@ def _reference(pre_range, n_pre, n_post, p, dmin, dmax, seed):
     return out
 
 
-def _static(lib, torch, pre_range, n_post, p, dmin, dmax, seed, capacity):
+def _static(lib, torch, pre_range, n_post, p, dmin, dmax, seed, capacity, alloc=None):
     dev = torch.cuda.current_device()
     stream = torch.cuda.current_stream()
-    bufs = [torch.full((capacity,), -1, dtype=torch.int32, device="cuda") for _ in range(3)]
+    size = capacity if alloc is None else alloc
+    bufs = [torch.full((size,), -1, dtype=torch.int32, device="cuda") for _ in range(3)]
     n = C.c_int64(-1)
     st = lib.b2b_connect_random_static(dev, C.c_void_p(stream.cuda_stream), pre_range[0],
                                        pre_range[1], n_post, p, dmin, dmax, seed,
@@ -72,7 +73,17 @@ def test_static_generator_limits():
     # more rows than the static scratch holds: rejected before any device work
     st, _, _ = _static(lib, torch, (0, (1 << 20) + 1), 10, 0.1, 1, 2, 1, capacity=16)
     assert st == 1
-    # too small an output: the count comes back with B2B_ERR_QUEUE_OVERFLOW
-    st, n, (i, j, d) = _static(lib, torch, (0, 200), 200, 0.5, 1, 2, 5, capacity=64)
-    assert st == 3 and n > 64
-    assert (i[:64] >= 0).all()
+    # too small an output: the count comes back with B2B_ERR_QUEUE_OVERFLOW, the first
+    # `capacity` synapses in (i, j) order are written and nothing beyond them
+    cap = 64
+    st, n, (i, j, d) = _static(lib, torch, (0, 200), 200, 0.5, 1, 2, 5, capacity=cap,
+                               alloc=4 * cap)
+    assert st == 3 and n > cap
+    ri, rj, rd = _reference((0, 200), 200, 200, 0.5, 1, 2, 5)
+    assert len(ri) == n
+    order = np.lexsort((rj, ri))              # the existing entry point's synapses in (i, j) order
+    np.testing.assert_array_equal(i[:cap], ri[order][:cap])
+    np.testing.assert_array_equal(j[:cap], rj[order][:cap])
+    np.testing.assert_array_equal(d[:cap], rd[order][:cap])
+    for a in (i, j, d):
+        assert (a[cap:] == -1).all()
