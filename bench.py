@@ -142,59 +142,113 @@ def barrier(world):
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_network(steps_budget_s: float, max_steps: int):
-    """The oracle port (C++, OpenMP over all host threads) on the same model: same size,
-    parameters and connectivity distribution (numpy-drawn instance), timed per step."""
-    from brian2cuda_b200 import models
-    from oracle.oracle import OracleNet
+def cpu_info():
+    """CPU model and the threads the oracle's OpenMP loops use on this host."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                model = ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    threads = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or os.cpu_count()
+    return {"cpu_model": model, "omp_threads": threads, "host_cpus": os.cpu_count()}
 
-    rng = np.random.default_rng(models.SEED_BASE + 101)
-    net = OracleNet(DT, f32=True)
-    P = net.hh_group(N_NEURONS, models.cobahh_hh())
-    models.cobahh_init(net, P, N_NEURONS, rng)
-    i, j = models.bernoulli_pairs(rng, N_NEURONS, N_NEURONS, P_CONNECT)
-    d = rng.integers(DMIN, DMAX + 1, size=len(i)).astype(np.int32)
-    ne = int(0.8 * N_NEURONS)
-    exc = i < ne
-    net.synapses(P, P, "ge", i[exc], j[exc], w_scalar=6e-9, delay=d[exc])
-    net.synapses(P, P, "gi", i[~exc], j[~exc], w_scalar=67e-9, delay=d[~exc])
-    outdeg = np.bincount(i, minlength=N_NEURONS)
-    n_syn = len(i)
-    del i, j, d, exc
-    net.run(1)  # builds the bundles and queues
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < max_steps and time.perf_counter() - t0 < steps_budget_s:
-        net.run(5)
-        steps += 5
-    el = time.perf_counter() - t0
-    idx, st = net.spikes(P)
-    sel = st >= 1
-    events = float(outdeg[idx[sel]].sum())
-    return {"events": events, "steps": steps, "seconds": el, "n_syn": n_syn,
-            "neuron_updates": float(N_NEURONS) * steps, "spikes": int(sel.sum())}
+
+def delivery_table(net, sids, n_pre: int) -> np.ndarray:
+    """cum[n, k] = synapses of presynaptic neuron n (over the Synapses objects sids) whose
+    delay is at most k steps; a spike of n at step s of a run of E steps has
+    cum[n, min(E - 1 - s, DMAX)] of its synaptic events delivered inside the run."""
+    w = DMAX + 1
+    cnt = np.zeros(n_pre * w, np.int64)
+    for sid in sids:
+        key = net.syn_get(sid, "i").astype(np.int64) * w
+        key += net.syn_get(sid, "delay").astype(np.int64)
+        cnt += np.bincount(key, minlength=n_pre * w)
+        del key
+    return np.cumsum(cnt.reshape(n_pre, w), axis=1)
+
+
+def delivered_events(cum: np.ndarray, idx, st, end: int) -> float:
+    """Synaptic events of spikes (idx at steps st, relative to the run start) delivered
+    before step `end` (events whose delay carries them past the run are not counted)."""
+    if len(idx) == 0:
+        return 0.0
+    k = np.minimum(end - 1 - np.asarray(st, np.int64), cum.shape[1] - 1)
+    return float(cum[np.asarray(idx, np.int64), k].sum())
+
+
+class CpuCobahh:
+    """The oracle port (C++, OpenMP over the host threads) on the configured network: the
+    same connect(p) (Philox, the same seeds and synapse order as the GPU run), parameters and
+    initial state as the GPU arm, so both arms simulate the identical network."""
+
+    def __init__(self):
+        from brian2cuda_b200 import models
+        from oracle.oracle import OracleNet
+        t0 = time.perf_counter()
+        self.net = OracleNet(DT, f32=True)
+        self.ids = models.build_cobahh(self.net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
+                                       generated=True)
+        self.net.run(0)             # builds the bundle tables and the delay queues
+        self.net.store(0)
+        self.n_syn = sum(self.net.syn_count(s) for s in (self.ids["Ce"], self.ids["Ci"]))
+        self.cum = delivery_table(self.net, (self.ids["Ce"], self.ids["Ci"]), N_NEURONS)
+        self.setup_s = time.perf_counter() - t0
+
+    def run_window(self, chunks: int, chunk_steps: int, budget_s: float | None = None):
+        """From the initial state, `chunks` chunks of chunk_steps steps, each timed (stops
+        early past budget_s); returns (seconds per chunk, steps run, events, spikes)."""
+        net, P = self.net, self.ids["P"]
+        net.restore(0)
+        net.clear_spikes()
+        times = []
+        t_all = time.perf_counter()
+        for _ in range(chunks):
+            t0 = time.perf_counter()
+            net.run(chunk_steps)
+            times.append(time.perf_counter() - t0)
+            if budget_s is not None and time.perf_counter() - t_all > budget_s:
+                break
+        steps = chunk_steps * len(times)
+        idx, st = net.spikes(P)
+        return times, steps, delivered_events(self.cum, idx, st, steps), len(idx)
 
 
 def reference_arm(args):
-    threads = os.cpu_count()
+    """The reference's CPU path on the host cores: the oracle port of the reference's
+    algorithm (the reference itself is a code generator that needs Brian2, absent here).
+    One step = a sample of S = ceil(10,000 / K) simulation steps; the K timed steps cover
+    the configured 1 s run from its initial state (simulation steps [0, K*S)), the W warm-up
+    steps repeat its first sample from the initial state."""
     t0 = time.perf_counter()
-    r = cpu_network(steps_budget_s=min(120.0, 10.0 * (args.steps + args.warmup)),
-                    max_steps=SIM_STEPS)
-    value = r["events"] / r["seconds"]
+    cpu = CpuCobahh()
+    S = -(-SIM_STEPS // args.steps)
+    for _ in range(args.warmup):
+        cpu.run_window(1, S)
+    times, steps, events, nspk = cpu.run_window(args.steps, S)
+    seconds = sum(times)
+    value = events / seconds
+    info = cpu_info()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * r["seconds"] / max(1, r["steps"]) * SIM_STEPS,
-        "firing_rate_hz": r["spikes"] / (N_NEURONS * max(1, r["steps"]) * DT),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps,
+        "firing_rate_hz": nspk / (N_NEURONS * steps * DT),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sim_steps_per_step": SIM_STEPS,
-                   "neurons": N_NEURONS, "synapses": r["n_syn"]},
-        "neuron_updates_per_s": r["neuron_updates"] / r["seconds"],
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{r['steps']} simulation steps of the full network after "
-                                   f"setup ({r['seconds']:.1f} s); C++ oracle, OpenMP"},
+        "config": {"workload": WORKLOAD, "sim_steps_per_step": S, "neurons": N_NEURONS,
+                   "synapses": cpu.n_syn,
+                   "window": f"simulation steps [0, {steps}) of the configured run"},
+        "neuron_updates_per_s": float(N_NEURONS) * steps / seconds,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["omp_threads"],
+                         "kind": "port",
+                         "sample": f"{args.steps} steps of {S} simulation steps = simulation "
+                                   f"steps [0, {steps}) of the configured 1 s run of the "
+                                   f"identical 1e5-neuron network ({seconds:.1f} s); C++ "
+                                   "oracle, OpenMP", **info},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": cpu.setup_s,
         "wall_s": time.perf_counter() - t0,
     }
     print(json.dumps(line), flush=True)
@@ -208,6 +262,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2b", choices=["b2b", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="only the COBAHH line, without the other configurations' entries")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="STEPS",
                     help="profiling case: build the workload, simulate STEPS steps, print "
                          "nothing (for ncu captures of the step kernels)")
@@ -236,9 +292,11 @@ def main():
 
     if args.workload != "cobahh" and args.impl == "b2b":
         if args.workload == "batched":
-            bench_batched(args, world, rank, local)
+            line = bench_batched(args, world, rank, local)
         else:
-            bench_small(args, world, rank, local)
+            line = bench_small(args, world, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -252,12 +310,41 @@ def main():
             dist.destroy_process_group()
         return
 
+    line = bench_cobahh(args, world, rank, local)
+    if line is None:            # the profiling case prints nothing
+        return
+    if rank == 0 and world == 1 and not args.no_configs:
+        # the other configurations, each a shorter timed window (their own lines'
+        # value, unit, roofline and CPU baseline), so the default run stays a few minutes
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = min(args.steps, 5), 3
+        configs = {}
+        for wl in ("cuba", "stdp", "hines", "propagation", "batched"):
+            sub.workload = wl
+            t0 = time.perf_counter()
+            try:
+                entry = (bench_batched if wl == "batched" else bench_small)(sub, world, rank,
+                                                                            local)
+            except Exception as exc:     # keep the headline line if one entry fails
+                entry = {"error": f"{type(exc).__name__}: {exc}"}
+            entry["wall_s"] = time.perf_counter() - t0
+            configs[wl] = entry
+        line["configs"] = configs
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def bench_cobahh(args, world, rank, local):
     import torch
 
     from brian2cuda_b200 import Network, models
+    from brian2cuda_b200.network import atomic_rate
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
-    runs = args.warmup + 2 * args.steps + 1
+    runs = args.warmup + 2 * args.steps + 2
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
                   stream=stream.cuda_stream,
@@ -268,13 +355,9 @@ def main():
     net.finalize()
     P = ids["P"]
     ne = int(0.8 * N_NEURONS)
-    outdeg = np.zeros(N_NEURONS, np.int64)
-    n_syn = 0
-    for sid in (ids["Ce"], ids["Ci"]):
-        i = net.syn_get(sid, "i")
-        outdeg += np.bincount(i, minlength=N_NEURONS)
-        n_syn += len(i)
-        del i
+    n_syn = sum(net.syn_count(s) for s in (ids["Ce"], ids["Ci"]))
+    cum = delivery_table(net, (ids["Ce"], ids["Ci"]), N_NEURONS)
+    outdeg = cum[:, -1]
     net.store(0)
     init = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi", "lastspike")}
     setup_s = time.perf_counter() - t_setup
@@ -293,7 +376,7 @@ def main():
         net.run(args.ncu_case)
         net.sync()
         net.close()
-        return
+        return None
 
     def one_run():
         net.restore(0)
@@ -322,8 +405,10 @@ def main():
     launches = net.kernel_launches - launches0
     idx, st, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
     nspk = len(idx)
-    ev_exc = float(outdeg[idx[idx < ne]].sum())
-    ev_inh = float(outdeg[idx[idx >= ne]].sum())
+    # every run starts at step 0 from the checkpoint: st is the step within its run
+    exc = idx < ne
+    ev_exc = delivered_events(cum, idx[exc], st[exc], SIM_STEPS)
+    ev_inh = delivered_events(cum, idx[~exc], st[~exc], SIM_STEPS)
     events = (ev_exc + ev_inh) * world
     seconds = ms_total / 1e3
     value = events / seconds
@@ -350,25 +435,21 @@ def main():
         net.run(SIM_STEPS)
         v_host = net.get_state(P, "v")
         idx_e, st_e, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
-        e2e_events += float(outdeg[idx_e].sum())
+        e2e_events += delivered_events(cum, idx_e, st_e, SIM_STEPS)
         d2h += v_host.nbytes + 12 * len(idx_e) + 8
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = e2e_events * world / e2e_s
 
-    # ---- per-kernel device times (profiling run of one configured 1 s simulation, every
-    # launch timed with CUDA events on the network's stream)
+    # ---- per-kernel device times inside the replayed step graphs: one configured 1 s run
+    # from the checkpoint with an event-record node before and after every launch
     net.restore(0)
-    prof = net.profile(SIM_STEPS)
+    prof, prof_step_ms = net.profile_graph(SIM_STEPS)
+    pidx, pst, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
     hbm, peak_kind = peaks()
-    runs_timed = args.steps
-    n_exc_spk = float((idx < ne).sum())
-    n_inh_spk = float((idx >= ne).sum())
+    p_ev = delivered_events(cum, pidx, pst, SIM_STEPS)
     nd = DMAX - DMIN + 1
-    launches_timed = SIM_STEPS * runs_timed
-    deliver_exc = (BYTES_EVENT * ev_exc + BYTES_BUNDLE * nd * n_exc_spk) / launches_timed
-    deliver_inh = (BYTES_EVENT * ev_inh + BYTES_BUNDLE * nd * n_inh_spk) / launches_timed
+    deliver_bytes = (BYTES_EVENT * p_ev + BYTES_BUNDLE * nd * float(len(pidx))) / SIM_STEPS
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
-    # algorithmic bytes per launch of each launch site the profiler reports
     two_launch = net.run_mode == "fused"
     if two_launch:
         # the update also adds in and clears the pending input of ge and gi
@@ -382,23 +463,23 @@ def main():
     kernel_ms, per_launch_bytes, kernels = {}, [], []
     for k, (kd, ms) in enumerate(prof):
         label, kname = site_info.get(kd, (f"site kind {kd}", None))
-        if kd == 1:
-            b = neuron_bytes
-        elif kd in (5, 6):
-            b = deliver_exc + deliver_inh
-        else:
-            b = 0.0
+        b = neuron_bytes if kd == 1 else (deliver_bytes if kd in (5, 6) else 0.0)
         kernel_ms[label] = round(ms, 6)
         per_launch_bytes.append(b)
         kernels.append((label, kname))
-    # the roofline names the neuron update: the largest share of device time in the launch
-    # list in either form of the step (the eager per-launch times of this profiling run are
-    # a few us each and mostly launch latency, so they do not rank the kernels)
-    dom = [k for k, (kd, _) in enumerate(prof) if kd == 1][0]
+    # the dominant launch site: the largest device time per step inside the graphs
+    dom = max(range(len(prof)), key=lambda k: prof[k][1])
     dom_ms = prof[dom][1]
     alg = per_launch_bytes[dom]
     achieved = alg / (dom_ms * 1e-3) / 1e9
     traffic = _traffic_lookup(kernels[dom][1]) if kernels[dom][1] else None
+    dsite = [k for k, (kd, _) in enumerate(prof) if kd in (5, 6)][0]
+    d_ms = prof[dsite][1]
+    # the delivery's own ceiling: scattered f32 atomics into the population's ge and gi
+    # (2e5 floats), one index load per event from HBM
+    loaded, hashed = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
+                                 stream=stream.cuda_stream)
+    d_rate = p_ev / (d_ms * 1e-3 * SIM_STEPS)
     names = [lab for lab, _ in kernels]
 
     line = {
@@ -407,17 +488,35 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sim_steps_per_step": SIM_STEPS, "neurons": N_NEURONS,
                    "synapses": n_syn, "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2 (1.6 GB synapse arrays)"},
+                   "l2": "working set > L2 (1.6 GB synapse arrays); the 5.4 MB of neuron "
+                         "state stays L2-resident between steps"},
         "neuron_updates_per_s": neuron_updates,
         "firing_rate_hz": rate_hz,
         "spikes_per_run": nspk / args.steps,
+        "events_per_run": (ev_exc + ev_inh) / args.steps,
+        "events_counted": "spikes x their synapses whose delay lands inside the run",
         "setup_s": setup_s,
         "run_mode": net.run_mode,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": names[dom],
                      "kernel_ms": dom_ms, "peak_source": peak_kind,
-                     "bytes_per_launch": alg},
-        "kernel_ms_mean_per_launch": kernel_ms,
+                     "bytes_per_launch": alg,
+                     "timing": "mean device time per step inside the replayed step graphs "
+                               "(event-record nodes around the launch, one configured run)",
+                     "note": "the neuron state (5.4 MB) is L2-resident, so the update is "
+                             "latency-bound, not HBM-bound"},
+        "kernel_ms_per_step_in_graph": kernel_ms,
+        "profiled_step_ms": prof_step_ms,
+        "delivery": {"kernel": names[dsite], "kernel_ms": d_ms,
+                     "bytes_per_launch": deliver_bytes,
+                     "achieved_gbs": deliver_bytes / (d_ms * 1e-3) / 1e9,
+                     "frac_hbm": deliver_bytes / (d_ms * 1e-3) / 1e9 / hbm,
+                     "events_per_s_in_kernel": d_rate,
+                     "atomic_ceiling_events_per_s": {"index_loaded": loaded,
+                                                     "index_in_registers": hashed},
+                     "frac_of_atomic_ceiling": d_rate / loaded,
+                     "note": "at the network's ~3 Hz a step delivers ~6e4 events: the "
+                             "kernel is latency-bound; see configs.propagation for load"},
         "autotune": tune,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h // max(1, args.steps),
@@ -426,20 +525,19 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_network(steps_budget_s=60.0, max_steps=SIM_STEPS)
-        line["cpu_baseline"] = {
-            "value": r["events"] / r["seconds"], "unit": UNIT, "cores": os.cpu_count(),
-            "kind": "port",
-            "sample": f"the first {r['steps']} simulation steps of the configured 1 s run of the "
-                      f"full 1e5-neuron network ({r['seconds']:.1f} s), C++ oracle, OpenMP",
-            "neuron_updates_per_s": r["neuron_updates"] / r["seconds"]}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     net.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = CpuCobahh()
+        times, steps, ev, _ = cpu.run_window(SIM_STEPS // 500, 500, budget_s=30.0)
+        info = cpu_info()
+        line["cpu_baseline"] = {
+            "value": ev / sum(times), "unit": UNIT, "cores": info["omp_threads"],
+            "kind": "port",
+            "sample": f"the first {steps} simulation steps of the configured 1 s run of the "
+                      f"identical network ({sum(times):.1f} s), C++ oracle, OpenMP",
+            "neuron_updates_per_s": float(N_NEURONS) * steps / sum(times), **info}
+        del cpu
+    return line
 
 
 # ---- batched COBAHH instances (plain, batched, batched + gating surrogate) -------------------
@@ -538,7 +636,7 @@ def bench_batched(args, world, rank, local):
     nspk = sum_over_ranks(nspk, world)
     n_syn = int(sum_over_ranks(float(n_syn), world))
     net.restore(0)
-    prof = net.profile(200)
+    prof, _ = net.profile_graph(200)
     hbm, peak_kind = peaks()
     neuron_ms = [ms for k, ms in prof if k == 1][0]
     neuron_bytes = float(BYTES_NEURON_UPDATE * n_total)
@@ -642,8 +740,7 @@ def bench_batched(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 # ---- CUBA, STDP and multicompartment workloads ------------------------------------------------
@@ -745,7 +842,7 @@ def bench_small(args, world, rank, local):
         events = float(outdeg[idx].sum()) / runs * args.steps
         nspk = len(idx) / runs
         net.restore(0)
-        prof = net.profile(2000)
+        prof, _ = net.profile_graph(2000)
         sec = ms / 1e3
         value = events * world / sec
         nb = BYTES["cuba_neuron"] * 4000.0
@@ -791,7 +888,7 @@ def bench_small(args, world, rank, local):
         n_out = len(net.spikes_fetch(ids["out"], s_in, cap=1 << 26)[0]) / runs * args.steps
         ev_pre, ev_post = n_in * 1000.0, n_out * 10_000.0
         net.restore(0)
-        prof = net.profile(2000)
+        prof, _ = net.profile_graph(2000)
         sec = ms / 1e3
         value = (ev_pre + ev_post) * world / sec
         per_launch = {1: None, 2: BYTES["stdp_pre"] * ev_pre / (args.steps * steps_run),
@@ -852,7 +949,7 @@ def bench_small(args, world, rank, local):
         nspk = len(idx) / runs * args.steps
         del idx, st
         net.restore(0)
-        prof = net.profile(200)
+        prof, _ = net.profile_graph(200)
         sec = ms / 1e3
         value = events * world / sec
         per_step_events = events / (args.steps * steps_run)
@@ -863,6 +960,14 @@ def bench_small(args, world, rank, local):
         roof["traffic"] = _traffic_lookup("deliver_add_batch_kernel@propagation")
         roof["note"] = ("12 B per event (target index 4 B + target read/write 8 B) + 8 B per "
                         "(spike, delay) bundle; bound: one L2 atomic per event")
+        from brian2cuda_b200.network import atomic_rate
+        loaded, hashed = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
+                                     stream=stream.cuda_stream)
+        d_rate = per_step_events / (dmsk[0] * 1e-3)
+        roof["events_per_s_in_kernel"] = d_rate
+        roof["atomic_ceiling_events_per_s"] = {"index_loaded": loaded,
+                                               "index_in_registers": hashed}
+        roof["frac_of_atomic_ceiling"] = d_rate / loaded
         line = _line_base(args, world, "synaptic events/s", value, "events/s",
                           ms / args.steps, WORKLOADS[wl],
                           {"sim_steps_per_step": steps_run, "neurons": 2 * N_NEURONS,
@@ -945,8 +1050,7 @@ def bench_small(args, world, rank, local):
                                     "unit": "compartment-updates/s", "cores": os.cpu_count(),
                                     "kind": "port",
                                     "sample": f"200 of the 8000 steps ({el2:.1f} s), C++ oracle"}
-    if rank == 0 and line is not None:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def kernel_case(name: str):

@@ -808,11 +808,23 @@ b2b_status setup_two_launch(b2b_net* net) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Records profiling event `which` (0 before, 1 after) of launch site `site` of step k on s,
+// when b2b_profile_graph has set the net's event table; under stream capture the record is
+// an event-record node of the graph (an external event), so the replayed graph times the
+// launch in its own schedule.
+cudaError_t prof_mark(b2b_net* net, int k, int site, int which, cudaStream_t s) {
+  if (!net->prof_ev) return cudaSuccess;
+  return cudaEventRecordWithFlags(net->prof_ev[((size_t)k * net->prof_sites + site) * 2 + which],
+                                  s, cudaEventRecordExternal);
+}
+
 b2b_status enqueue_steps(b2b_net* net, int kk) {
   if (net->small) {
     const Pop& pop = net->pops[0];
+    CU(prof_mark(net, 0, 0, 0, net->stream));
     CU(launch_small(net->sdev, pop.kind, pop.dtype, net->d_clock, kk, net->cfg.dt,
                     net->d_status, net->stream));
+    CU(prof_mark(net, 0, 0, 1, net->stream));
     CU(launch_tick(net->d_clock, kk, net->stream));
     net->launches += 2;
     return B2B_OK;
@@ -822,17 +834,21 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     // (which folds in acc[(k-1) & 1]) are independent: the delivery of step k waits for the
     // update of step k-1, the update of step k for the update and the delivery of step k-1.
     // The deliveries run on the second stream; under stream capture this is a graph with
-    // two branches per step.
+    // two branches per step.  Profiling sites: 0 the delivery, 1 the update.
     const Pop& pop = net->pops[0];
     cudaStream_t s = net->stream, s2 = net->stream2;
     CU(cudaEventRecord(net->ev_n, s));
     for (int k = 0; k < kk; ++k) {
       CU(cudaStreamWaitEvent(s2, net->ev_n, 0));
+      CU(prof_mark(net, k, 0, 0, s2));
       CU(launch_pending_delivery(net->pdev, pop.dtype, net->pending_grid, net->d_clock, k, s2));
+      CU(prof_mark(net, k, 0, 1, s2));
       CU(cudaEventRecord(net->ev_d[k & 1], s2));
       if (k > 0) CU(cudaStreamWaitEvent(s, net->ev_d[(k - 1) & 1], 0));
+      CU(prof_mark(net, k, 1, 0, s));
       CU(launch_pop_step_dev(pop, net->fold_dev, net->d_clock, k, net->cfg.dt, net->d_status,
                              s));
+      CU(prof_mark(net, k, 1, 1, s));
       CU(cudaEventRecord(net->ev_n, s));
       net->launches += 2;
     }
@@ -842,44 +858,60 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     net->launches += 2;
     return B2B_OK;
   }
+  cudaStream_t s = net->stream;
   for (int k = 0; k < kk; ++k) {
+    int si = 0;   // profiling site, in the order of b2b_profile's site list
     if (!net->smons.empty()) {
+      CU(prof_mark(net, k, si, 0, s));
       CU(launch_statemon(net->d_smons, (int)net->smons.size(), net->smon_max_idx, net->d_clock,
-                         k, net->d_status, net->stream));
+                         k, net->d_status, s));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
     for (const Pop& pop : net->pops) {
-      CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      CU(prof_mark(net, k, si, 0, s));
+      CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, s));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
     for (size_t b = 0; b < net->add_batches.size(); ++b) {
       const auto& B = net->add_batches[b];
-      CU(launch_proj_add_batch(B.data(), (int)B.size(), net->d_clock, k, net->stream,
+      CU(prof_mark(net, k, si, 0, s));
+      CU(launch_proj_add_batch(B.data(), (int)B.size(), net->d_clock, k, s,
                                b < net->add_tune.size() ? &net->add_tune[b] : nullptr));
-      ++net->launches;
-    }
-    for (const Proj& pr : net->projs) {
-      if (pr.effect == B2B_EFFECT_ADD) continue;
-      CU(launch_proj_pre(pr, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
     for (const Proj& pr : net->projs) {
       if (pr.effect != B2B_EFFECT_STDP) continue;
-      CU(launch_proj_post(pr, net->d_clock, k, net->cfg.dt, net->d_status, net->stream));
+      CU(prof_mark(net, k, si, 0, s));
+      CU(launch_proj_pre(pr, net->d_clock, k, net->cfg.dt, net->d_status, s));
+      CU(prof_mark(net, k, si++, 1, s));
+      ++net->launches;
+    }
+    for (const Proj& pr : net->projs) {
+      if (pr.effect != B2B_EFFECT_STDP) continue;
+      CU(prof_mark(net, k, si, 0, s));
+      CU(launch_proj_post(pr, net->d_clock, k, net->cfg.dt, net->d_status, s));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
     for (const Pop& pop : net->pops) {
       if (!pop.late_reset) continue;
-      CU(launch_pop_late_reset(pop, net->d_clock, k, net->stream));
+      CU(prof_mark(net, k, si, 0, s));
+      CU(launch_pop_late_reset(pop, net->d_clock, k, s));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
     if (!net->rmons.empty()) {
+      CU(prof_mark(net, k, si, 0, s));
       CU(launch_ratemon(net->d_rmons, (int)net->rmons.size(), net->d_clock, k, net->d_status,
-                        net->stream));
+                        s));
+      CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
   }
-  CU(launch_tick(net->d_clock, kk, net->stream));
+  CU(launch_tick(net->d_clock, kk, s));
   ++net->launches;
   return B2B_OK;
 }
@@ -931,6 +963,33 @@ b2b_status capture_graph(b2b_net* net) {
   net->graph_nodes = (int64_t)nodes;
   net->graph_steps = net->cfg.steps_per_graph;
   return B2B_OK;
+}
+
+// Launch sites of one step, in the order enqueue_steps marks them for profiling: the state
+// monitors (kind 9), each population (1), each additive delivery launch (6), each STDP
+// projection's on_pre (2) and on_post (3), each deferred reset (4), the rate monitors (10);
+// the two-launch step: its delivery (5) and update (1); the one-CTA small path: its kernel (7).
+struct ProfSite { int kind; int idx; };
+std::vector<ProfSite> profile_sites(const b2b_net* net) {
+  std::vector<ProfSite> sites;
+  if (net->small) {
+    sites.push_back({7, 0});
+  } else if (net->two_launch) {
+    sites.push_back({5, 0});
+    sites.push_back({1, 0});
+  } else {
+    if (!net->smons.empty()) sites.push_back({9, 0});
+    for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
+    for (size_t b = 0; b < net->add_batches.size(); ++b) sites.push_back({6, (int)b});
+    for (size_t p = 0; p < net->projs.size(); ++p)
+      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({2, (int)p});
+    for (size_t p = 0; p < net->projs.size(); ++p)
+      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      if (net->pops[p].late_reset) sites.push_back({4, (int)p});
+    if (!net->rmons.empty()) sites.push_back({10, 0});
+  }
+  return sites;
 }
 
 }  // namespace
@@ -1463,25 +1522,8 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   CHECK(n_steps > 0 && n_sites, B2B_ERR_INVALID_ARG, "bad arguments");
   GUARD_BEGIN
-  struct Site { int kind; int idx; };
-  std::vector<Site> sites;
-  if (net->small) {
-    sites.push_back({7, 0});
-  } else if (net->two_launch) {  // the step's two launches, timed one after the other
-    sites.push_back({5, 0});
-    sites.push_back({1, 0});
-  } else {
-    if (!net->smons.empty()) sites.push_back({9, 0});
-    for (size_t p = 0; p < net->pops.size(); ++p) sites.push_back({1, (int)p});
-    for (size_t b = 0; b < net->add_batches.size(); ++b) sites.push_back({6, (int)b});
-    for (size_t p = 0; p < net->projs.size(); ++p)
-      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({2, (int)p});
-    for (size_t p = 0; p < net->projs.size(); ++p)
-      if (net->projs[p].effect == B2B_EFFECT_STDP) sites.push_back({3, (int)p});
-    for (size_t p = 0; p < net->pops.size(); ++p)
-      if (net->pops[p].late_reset) sites.push_back({4, (int)p});
-    if (!net->rmons.empty()) sites.push_back({10, 0});
-  }
+  using Site = ProfSite;
+  const std::vector<Site> sites = profile_sites(net);
   const size_t ns = sites.size();
   std::vector<cudaEvent_t> ev(2 * ns);
   for (auto& e : ev) CU(cudaEventCreate(&e));
@@ -1546,6 +1588,104 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
     if (mean_ms) mean_ms[k] = acc[k] / (double)n_steps;
     if (site_kind) site_kind[k] = sites[k].kind;
   }
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms,
+                             int32_t* site_kind, int32_t cap, int32_t* n_sites,
+                             double* step_ms) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  const int K = net->cfg.steps_per_graph;
+  CHECK(n_steps > 0 && n_steps % K == 0 && n_sites, B2B_ERR_INVALID_ARG,
+        "n_steps must be a positive multiple of steps_per_graph (%d)", K);
+  GUARD_BEGIN
+  const std::vector<ProfSite> sites = profile_sites(net);
+  const size_t ns = sites.size();
+  // the one-CTA path advances all K steps in one launch: one timed launch per chunk
+  const int marked_steps = net->small ? 1 : K;
+  std::vector<cudaEvent_t> ev(2 * ns * (size_t)K, nullptr);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t nodes = 0;
+  b2b_status result = B2B_OK;
+  std::vector<double> acc(ns, 0.0);
+  double total_ms = 0.0;
+  auto cleanup = [&]() {
+    net->prof_ev = nullptr;
+    net->prof_sites = 0;
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  cudaError_t e = cudaSuccess;
+  for (auto& x : ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&x);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(net, B2B_ERR_CUDA, "profile events: %s", cudaGetErrorString(e));
+  }
+  net->prof_ev = ev.data();
+  net->prof_sites = (int)ns;
+  const bool use_graph = !(net->cfg.flags & B2B_NET_NO_GRAPH);
+  if (use_graph) {
+    const int64_t before = net->launches;
+    e = cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      result = enqueue_steps(net, K);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(net->stream, &g);
+      net->launches = before;
+      if (result == B2B_OK && ee != cudaSuccess) e = ee;
+      if (result == B2B_OK && e == cudaSuccess) {
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        nodes = (int64_t)nn;
+        e = cudaGraphInstantiate(&exec, g, 0);
+      }
+      if (g) cudaGraphDestroy(g);
+    }
+  }
+  for (int64_t r = 0; result == B2B_OK && e == cudaSuccess && r < n_steps / K; ++r) {
+    if ((result = refill_rng(net, K)) != B2B_OK) break;
+    e = cudaEventRecord(e0, net->stream);
+    if (e != cudaSuccess) break;
+    if (use_graph) {
+      e = cudaGraphLaunch(exec, net->stream);
+      net->launches += nodes;
+    } else {
+      result = enqueue_steps(net, K);
+    }
+    if (result != B2B_OK || e != cudaSuccess) break;
+    e = cudaEventRecord(e1, net->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) break;
+    float ms = 0.f;
+    e = cudaEventElapsedTime(&ms, e0, e1);
+    total_ms += ms;
+    for (int k = 0; e == cudaSuccess && k < marked_steps; ++k)
+      for (size_t si = 0; e == cudaSuccess && si < ns; ++si) {
+        const size_t q = ((size_t)k * ns + si) * 2;
+        e = cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
+        acc[si] += ms;
+      }
+    net->ts += K;
+    net->last_chunk_steps = K;
+  }
+  cleanup();
+  if (result != B2B_OK) return result;
+  if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "profile_graph: %s", cudaGetErrorString(e));
+  *n_sites = (int32_t)ns;
+  for (size_t k = 0; k < ns && (int32_t)k < cap; ++k) {
+    if (mean_ms) mean_ms[k] = acc[k] / (double)n_steps;
+    if (site_kind) site_kind[k] = sites[k].kind;
+  }
+  if (step_ms) *step_ms = total_ms / (double)n_steps;
   return B2B_OK;
   GUARD_END
 }

@@ -338,6 +338,10 @@ struct b2b_net {
   std::vector<void*> pending_allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  // b2b_profile_graph: while set, enqueue_steps records prof_ev[(k * prof_sites + site) * 2]
+  // before and [.. + 1] after every launch site of step k (event-record nodes when captured)
+  cudaEvent_t* prof_ev = nullptr;
+  int prof_sites = 0;
   int64_t launches = 0;
   int64_t graph_nodes = 0;
   int64_t last_chunk_steps = 0;

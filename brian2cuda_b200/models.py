@@ -129,14 +129,23 @@ def batch_sizes(n_instances: int = 256, lo: int = 1000, hi: int = 64000,
 
 def build_cobahh_batch(net, sizes, we, p: float = 0.02, dmin: int = 1, dmax: int = 50,
                        wi: float = 67 * nS, dtype="float32", seed_offset: int = 0,
-                       monitor_capacity: int = 0):
+                       monitor_capacity: int = 0, instances=None):
     """Independent COBAHH instances in one network: instance k is build_cobahh's network with
     sizes[k] neurons and excitatory weight we[k].  The instances' groups share one population
     and their 2 x len(sizes) Synapses objects one projection, so every step is one neuron
-    launch and one delivery launch whatever the number of instances."""
+    launch and one delivery launch whatever the number of instances.  `instances` (indices
+    into sizes) builds only those instances, each with the seeds and initial state it has in
+    the whole batch."""
     rng = rng_for(5 + seed_offset)
+    keep = None if instances is None else set(int(k) for k in instances)
     groups, syns = [], []
     for k, (n, w) in enumerate(zip(np.asarray(sizes).tolist(), np.asarray(we).tolist())):
+        if keep is not None and k not in keep:
+            # consume this instance's draws of the initial state, as cobahh_init would
+            rng.standard_normal(int(n))
+            rng.standard_normal(int(n))
+            rng.standard_normal(int(n))
+            continue
         P = net.hh_group(int(n), cobahh_hh(), dtype)
         cobahh_init(net, P, int(n), rng)
         ne = int(0.8 * n)

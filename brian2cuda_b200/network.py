@@ -142,6 +142,20 @@ def spike_steps(times, dt: float) -> np.ndarray:
     return ((t + 1e-3 * dt) / dt).astype(np.int64)
 
 
+def atomic_rate(n_targets: int, n_events: int, device: int = 0, stream: int | None = None,
+                reps: int = 5) -> tuple[float, float]:
+    """Scattered float32 atomic additions per second that the GPU sustains into an array of
+    n_targets floats at uniform indices: (index loaded from device memory per event, index
+    computed in registers).  The ceiling of the additive spike delivery."""
+    lib = N.lib()
+    a, b = C.c_double(), C.c_double()
+    st = lib.b2b_atomic_rate(int(device), stream, int(n_targets), int(n_events), int(reps),
+                             C.byref(a), C.byref(b))
+    if st != N.B2B_OK:
+        raise B2BError(st, "b2b_atomic_rate")
+    return a.value, b.value
+
+
 class Network:
     """A network on one GPU.  Build it (groups, synapses, monitors), call `finalize()`,
     then `run(steps)`; state can be read and written between runs."""
@@ -456,6 +470,20 @@ class Network:
         self._check(self._lib.b2b_profile(self._h, int(steps), ms, kinds, cap, C.byref(n)),
                     "profile")
         return [(kinds[k], ms[k]) for k in range(n.value)]
+
+    def profile_graph(self, steps: int) -> tuple[list[tuple[int, float]], float]:
+        """Advances `steps` steps (a multiple of steps_per_graph) by replaying step graphs
+        that carry an event-record node before and after every launch site; returns
+        ((site kind, mean ms per simulated step inside the graphs) per site, mean ms of one
+        whole step).  Same sites as profile()."""
+        cap = 256
+        ms = (C.c_double * cap)()
+        kinds = (C.c_int32 * cap)()
+        n = C.c_int32()
+        step = C.c_double()
+        self._check(self._lib.b2b_profile_graph(self._h, int(steps), ms, kinds, cap, C.byref(n),
+                                                C.byref(step)), "profile_graph")
+        return [(kinds[k], ms[k]) for k in range(n.value)], step.value
 
     def autotune(self, trial_steps: int = 50) -> list[dict]:
         """Times candidate launch shapes of every launch site on the current state and keeps

@@ -240,6 +240,16 @@ b2b_status b2b_connect_random_static(int32_t device, void* stream, int32_t pre_l
                                      int32_t dmax, uint64_t seed, int32_t* dev_i, int32_t* dev_j,
                                      int32_t* dev_delay, int64_t capacity, int64_t* n_syn);
 
+/* Measures the ceiling of the additive delivery on `device`: the rate of scattered float32
+ * atomic additions (one per synaptic event, as brian2cuda's effect kernels do with atomicAdd,
+ * brian2cuda/templates/synapses.cu:117-162; no counterpart as a measurement) into an array of
+ * n_targets floats, at indices uniform over the array.  *loaded_per_s: every event's index
+ * loaded from an n_events-entry int32 array in device memory first (the delivery's form);
+ * *hashed_per_s: the index computed in registers (the atomics alone).  Best of `reps` timed
+ * launches after one warm-up each.  Allocates and frees its own buffers; runs on `stream`. */
+b2b_status b2b_atomic_rate(int32_t device, void* stream, int64_t n_targets, int64_t n_events,
+                           int32_t reps, double* loaded_per_s, double* hashed_per_s);
+
 /* Synapse variables. I, J, DELAY are int32; the others use the target group's dtype. */
 enum {
   B2B_SYN_I = 0, B2B_SYN_J = 1, B2B_SYN_DELAY = 2, B2B_SYN_W = 3, B2B_SYN_APRE = 4,
@@ -295,6 +305,17 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
+/* The same sites timed where b2b_run runs them: the step graph of steps_per_graph steps is
+ * captured with a CUDA event-record node before and after every launch site of every step,
+ * and replayed to advance the net by n_steps (a multiple of steps_per_graph).  mean_ms[k]
+ * receives site k's mean device time per simulated step inside the replayed graphs (in the
+ * two-launch form the two sites overlap in time; the one-CTA path's one launch covers a whole
+ * graph of steps), *step_ms the mean time of one whole step (replays timed by an event pair on
+ * the net's stream; the added event nodes are part of it).  Same site order and kinds as
+ * b2b_profile.  The profiling variant of the per-code-object timers of run(profile=True)
+ * (brian2cuda/templates/common_group.cu:170-174), which synchronise after every launch. */
+b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
+                             int32_t cap, int32_t* n_sites, double* step_ms);
 
 /* Autotuner (no counterpart in the reference, which picks launch shapes from fixed rules,
  * brian2cuda/device.py:383-394): launch site by launch site it times candidate launch shapes

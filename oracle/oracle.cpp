@@ -183,6 +183,22 @@ struct RateMon {
   std::vector<int64_t> counts;
 };
 
+// Dynamic state of a net (Network.store()/restore()): group variables and spikespaces,
+// Poisson read positions, delay queues and STDP synapse variables.  Monitors keep their
+// records across a restore, as the GPU library's do.
+template <typename R>
+struct NetSnap {
+  bool valid = false;
+  int64_t ts = 0;
+  std::vector<std::array<std::vector<R>, 7>> var;
+  std::vector<std::vector<uint8_t>> not_ref;
+  std::vector<std::vector<int32_t>> spikes;
+  std::vector<size_t> uni_next;
+  std::vector<std::vector<std::vector<int64_t>>> queue;
+  std::vector<int> current_offset;
+  std::vector<std::vector<R>> w, apre, apost, lu;
+};
+
 template <typename R>
 struct Net {
   double dt;
@@ -195,6 +211,7 @@ struct Net {
   bool reset_first = false;   // schedule: thresholds, resets, synapses
   uint64_t seed = 0;          // the net's seed (PoissonInput streams)
   int32_t n_pins = 0;
+  NetSnap<R> snap;
   std::string err;
 };
 
@@ -387,7 +404,12 @@ template <typename R>
 void pathway_post(Net<R>& net, Syn<R>& s, double t) {
   const R taupre = (R)s.stdp[0], taupost = (R)s.stdp[1], dApost = (R)s.stdp[3];
   const R wmin = (R)s.stdp[4], wmax = (R)s.stdp[5];
-  for (int32_t j : net.groups[s.post].spikes) {
+  // Each synapse has one postsynaptic neuron, so the spiking neurons' synapse sets are
+  // disjoint and the per-synapse updates are the same in any order of the neurons.
+  const std::vector<int32_t>& spk = net.groups[s.post].spikes;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t x = 0; x < (int64_t)spk.size(); ++x) {
+    const int32_t j = spk[x];
     for (int64_t q = s.post_off[j]; q < s.post_off[j + 1]; ++q) {
       const int64_t k = s.post_syn[q];
       const R tau = (R)(t - (double)s.lu[k]);
@@ -789,15 +811,40 @@ int api_random(Net<R>& net, int pre, int lo, int hi, int post, int target, doubl
   const uint64_t thr = p >= 1.0 ? ((uint64_t)1 << 32) : (p <= 0 ? 0 : (uint64_t)(p * 4294967296.0));
   const int32_t nd = dmax - dmin + 1;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  std::vector<int32_t> I, J, Dl;
-  for (int64_t i = lo; i < hi; ++i) {
+  // Rows are independent: each row's synapses are drawn in (j) order and stably sorted by
+  // delay; a first pass counts the synapses of every row so that the rows can be written in
+  // parallel straight into the synapse arrays (the 2e8-synapse network needs this).
+  const int64_t rows = hi - lo;
+  std::vector<int64_t> row_off(rows + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t r = 0; r < rows; ++r) {
+    const uint32_t i = (uint32_t)(lo + r);
+    int64_t c = 0;
+    for (int64_t jq = 0; 4 * jq < npost; ++jq) {
+      const Ctr x = philox(Ctr{{(uint32_t)jq, i, 0x5EEDu, 0u}}, k0, k1);
+      for (int e = 0; e < 4 && 4 * jq + e < npost; ++e) c += (uint64_t)x.v[e] < thr;
+    }
+    row_off[r + 1] = c;
+  }
+  for (int64_t r = 0; r < rows; ++r) row_off[r + 1] += row_off[r];
+  const int64_t n = row_off[rows];
+  if (net.built) return -1;
+  Syn<R> s;
+  s.pre = pre; s.post = post; s.target = target; s.effect = ADD; s.n = n;
+  s.i.resize(n);
+  s.j.resize(n);
+  s.delay.resize(n);
+  int32_t max_d = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(max : max_d)
+  for (int64_t r = 0; r < rows; ++r) {
+    const uint32_t i = (uint32_t)(lo + r);
     std::vector<std::pair<int32_t, int32_t>> row;  // (delay, j)
     for (int64_t jq = 0; 4 * jq < npost; ++jq) {
-      const Ctr r = philox(Ctr{{(uint32_t)jq, (uint32_t)i, 0x5EEDu, 0u}}, k0, k1);
+      const Ctr x = philox(Ctr{{(uint32_t)jq, i, 0x5EEDu, 0u}}, k0, k1);
       for (int e = 0; e < 4 && 4 * jq + e < npost; ++e) {
-        if ((uint64_t)r.v[e] < thr) {
+        if ((uint64_t)x.v[e] < thr) {
           const uint32_t j = (uint32_t)(4 * jq + e);
-          const Ctr rd = philox(Ctr{{j, (uint32_t)i, 0xDE1Au, 1u}}, k0, k1);
+          const Ctr rd = philox(Ctr{{j, i, 0xDE1Au, 1u}}, k0, k1);
           const int32_t d = dmin + (int32_t)(((uint64_t)rd.v[0] * (uint64_t)(uint32_t)nd) >> 32);
           row.emplace_back(d, (int32_t)j);
         }
@@ -805,10 +852,18 @@ int api_random(Net<R>& net, int pre, int lo, int hi, int post, int target, doubl
     }
     std::stable_sort(row.begin(), row.end(),
                      [](const auto& a, const auto& b) { return a.first < b.first; });
-    for (auto& x : row) { I.push_back((int32_t)i); J.push_back(x.second); Dl.push_back(x.first); }
+    int64_t k = row_off[r];
+    for (auto& y : row) {
+      s.i[k] = (int32_t)i; s.j[k] = y.second; s.delay[k] = y.first;
+      max_d = std::max(max_d, y.first);
+      ++k;
+    }
   }
-  return api_synapses(net, pre, post, target, ADD, (int64_t)I.size(), I.data(), J.data(),
-                      nullptr, w, Dl.data(), 0, nullptr);
+  s.max_delay = max_d;
+  s.has_w = false;
+  s.w_scalar = (R)w;
+  net.syns.push_back(std::move(s));
+  return (int)net.syns.size() - 1;
 }
 
 template <typename R>
@@ -844,6 +899,57 @@ int api_uniforms(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n
   Group<R>& g = net.groups[gid];
   if (g.kind != POISSON || n != g.n) return -1;
   for (int64_t k = 0; k < steps; ++k) g.uniforms.emplace_back(u + k * n, u + (k + 1) * n);
+  return 0;
+}
+
+template <typename R>
+int api_store(Net<R>& net) {
+  ensure_built(net);
+  NetSnap<R>& S = net.snap;
+  S.ts = net.ts;
+  S.var.clear(); S.not_ref.clear(); S.spikes.clear(); S.uni_next.clear();
+  for (const Group<R>& g : net.groups) {
+    std::array<std::vector<R>, 7> v;
+    for (int k = 0; k < 7; ++k) v[k] = g.var[k];
+    S.var.push_back(std::move(v));
+    S.not_ref.push_back(g.not_ref);
+    S.spikes.push_back(g.spikes);
+    S.uni_next.push_back(g.uni_next);
+  }
+  S.queue.clear(); S.current_offset.clear(); S.w.clear(); S.apre.clear(); S.apost.clear();
+  S.lu.clear();
+  for (const Syn<R>& sy : net.syns) {
+    S.queue.push_back(sy.queue);
+    S.current_offset.push_back(sy.current_offset);
+    S.w.push_back(sy.effect == STDP ? sy.w : std::vector<R>());
+    S.apre.push_back(sy.apre);
+    S.apost.push_back(sy.apost);
+    S.lu.push_back(sy.lu);
+  }
+  S.valid = true;
+  return 0;
+}
+
+template <typename R>
+int api_restore(Net<R>& net) {
+  const NetSnap<R>& S = net.snap;
+  if (!S.valid) return -1;
+  net.ts = S.ts;
+  for (size_t g = 0; g < net.groups.size(); ++g) {
+    for (int k = 0; k < 7; ++k) net.groups[g].var[k] = S.var[g][k];
+    net.groups[g].not_ref = S.not_ref[g];
+    net.groups[g].spikes = S.spikes[g];
+    net.groups[g].uni_next = S.uni_next[g];
+  }
+  for (size_t q = 0; q < net.syns.size(); ++q) {
+    Syn<R>& sy = net.syns[q];
+    sy.queue = S.queue[q];
+    sy.current_offset = S.current_offset[q];
+    if (sy.effect == STDP) sy.w = S.w[q];
+    sy.apre = S.apre[q];
+    sy.apost = S.apost[q];
+    sy.lu = S.lu[q];
+  }
   return 0;
 }
 
@@ -1060,6 +1166,19 @@ int orc_set_uniforms(void* hp, int gid, const double* u, int64_t steps, int64_t 
 int orc_run(void* hp, int64_t steps) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_run, steps, 0);
+}
+void orc_clear_spikes(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (h->f32) { for (auto& g : h->nf.groups) g.recorded.clear(); }
+  else { for (auto& g : h->nd.groups) g.recorded.clear(); }
+}
+int orc_store(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return h->f32 ? api_store(h->nf) : api_store(h->nd);
+}
+int orc_restore(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return h->f32 ? api_restore(h->nf) : api_restore(h->nd);
 }
 int64_t orc_timestep(void* hp) {
   Handle* h = static_cast<Handle*>(hp);

@@ -59,6 +59,9 @@ def lib() -> C.CDLL:
             "orc_syn_get": (C.c_int, [P, C.c_int, C.c_int, P, I64]),
             "orc_set_uniforms": (C.c_int, [P, C.c_int, P, I64, I64]),
             "orc_run": (C.c_int, [P, I64]),
+            "orc_store": (C.c_int, [P]),
+            "orc_clear_spikes": (None, [P]),
+            "orc_restore": (C.c_int, [P]),
             "orc_timestep": (I64, [P]),
             "orc_spikes": (I64, [P, C.c_int, P, P, I64]),
             "orc_statemon": (C.c_int, [P, C.c_int, C.c_int, P, I64, C.c_int]),
@@ -257,6 +260,18 @@ class OracleNet:
 
     def sync(self):
         return 0
+
+    def store(self, slot=0):
+        """Checkpoint of the dynamic state (one slot): group state and spikespaces, delay
+        queues, STDP synapse variables; monitors keep their records across a restore."""
+        self._ok(self._lib.orc_store(self._h), "store")
+
+    def restore(self, slot=0):
+        self._ok(self._lib.orc_restore(self._h), "restore")
+
+    def clear_spikes(self):
+        """Drops every recorded spike (a fresh spike record for the next window)."""
+        self._lib.orc_clear_spikes(self._h)
 
     @property
     def timestep(self):

@@ -1,0 +1,288 @@
+"""Parity of the CUDA library with the CPU oracle at the sizes of the five benchmark
+configurations (not stand-ins): CUBA 4000 LIF for the whole simulated second, COBAHH 1e5 HH
+with its 2.0e8 generated synapses, STDP 1e4 -> 1e3 all-to-all, the 1024-neuron Hines batch,
+and sampled instances of the 256-instance batched COBAHH population.
+
+Tolerances (stated per test): spike indices, spike steps and delay-queue contents exactly
+where both sides do the same arithmetic; float64 state within 1e-10 relative; float32 state
+within 1e-5 relative of the float64 oracle after one step from the same state; float32
+rollouts every spike within one dt of the oracle's, both ways.
+"""
+import numpy as np
+import pytest
+
+from brian2cuda_b200 import models
+
+pytestmark = pytest.mark.gpu
+DT = 1e-4
+mV, nS = 1e-3, 1e-9
+
+
+def _close(a, b, rtol, atol, what=""):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    bad = np.abs(a - b) > rtol * np.abs(b) + atol
+    assert not bad.any(), f"{what}: {bad.sum()} mismatches, worst {np.max(np.abs(a - b))}"
+
+
+def _within_one_step(a_idx, a_stp, b_idx, b_stp):
+    """Fraction of spikes of a that b has at the same neuron within one step."""
+    keys = set(zip(b_idx.tolist(), b_stp.tolist()))
+    hit = sum(1 for i, s in zip(a_idx.tolist(), a_stp.tolist())
+              if (i, s) in keys or (i, s - 1) in keys or (i, s + 1) in keys)
+    return hit / max(1, len(a_idx))
+
+
+def _sorted(idx, st):
+    o = np.lexsort((idx, st))
+    return idx[o], st[o]
+
+
+# ---- CUBA: 4000 LIF, float64, p = 0.02, the configured 1 s (10,000 steps) ----------------------
+def test_cuba_config_full_run_float64(gpu_factory, oracle_factory):
+    """Every delivered weight of one target variable is the same value, so the order of the
+    GPU's atomic additions cannot change a sum: spikes exact over all 10,000 steps, state
+    within 1e-10."""
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        ids = models.build_cuba(net, n=4000, p=0.02, dtype="float64")
+        net.finalize()
+        net.run(10_000)
+        P = ids["P"]
+        out[name] = (*net.spikes(P), {v: net.get_state(P, v) for v in ("v", "ge", "gi")},
+                     ids["n_syn"])
+    gi, gs, gst, ns = out["gpu"]
+    oi, os_, ost, _ = out["orc"]
+    assert 3.0e5 < ns < 3.4e5
+    assert len(gi) > 10_000
+    np.testing.assert_array_equal(gs, os_)
+    np.testing.assert_array_equal(gi, oi)
+    for v in ("v", "ge", "gi"):
+        _close(gst[v], ost[v], 1e-10, 1e-15, v)
+
+
+# ---- COBAHH: 1e5 HH, 2.0e8 synapses, delays 1..50 steps --------------------------------------
+def test_cobahh_config_step_float32_from_injected_state(gpu_factory, oracle_factory):
+    """One step of the configured 1e5-neuron population (float32 on the GPU) from the same
+    injected state as the float64 oracle: state within 1e-5 relative (plus 1e-5 of each
+    variable's scale), spikes exactly those the GPU's own updated v implies."""
+    n = 100_000
+    res = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        rng = np.random.default_rng(models.SEED_BASE + 101)
+        net = make(DT)
+        P = net.hh_group(n, models.cobahh_hh(), "float32")
+        net.set_state(P, "v", rng.uniform(-80 * mV, 10 * mV, n))
+        net.set_state(P, "m", rng.uniform(0, 1, n))
+        net.set_state(P, "h", rng.uniform(0, 1, n))
+        net.set_state(P, "n", rng.uniform(0, 1, n))
+        net.set_state(P, "ge", rng.uniform(0, 80 * nS, n))
+        net.set_state(P, "gi", rng.uniform(0, 400 * nS, n))
+        ls = -rng.integers(0, 60, n) * DT
+        net.set_state(P, "lastspike", ls)
+        net.spike_monitor(P, 2 * n)
+        net.finalize()
+        net.run(1)
+        res[name] = {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi")}
+        res[name]["spk"] = np.sort(net.spikes(P)[0])
+    scale = {"v": 0.1, "m": 1, "h": 1, "n": 1, "ge": 80 * nS, "gi": 400 * nS}
+    for v, sc in scale.items():
+        _close(res["gpu"][v], res["orc"][v], 1e-5, 1e-5 * sc, v)
+    v = res["gpu"]["v"]
+    not_ref = ((0 - ls + 1e-3 * DT) / DT).astype(np.int64) >= 30
+    expect = np.nonzero((v > np.float32(-20 * mV)) & not_ref)[0]
+    assert len(expect) > 1000
+    np.testing.assert_array_equal(res["gpu"]["spk"], expect)
+
+
+def _cobahh_rollout(gpu_factory, oracle_factory, dtype, f32_oracle, steps):
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT, f32=f32_oracle) if name == "orc" else make(DT)
+        ids = models.build_cobahh(net, n=100_000, p=0.02, dtype=dtype, generated=True,
+                                  monitor_capacity=2_000_000)
+        net.finalize()
+        net.run(steps)
+        P = ids["P"]
+        out[name] = {"spk": net.spikes(P), "q": (net.queue(ids["Ce"]), net.queue(ids["Ci"])),
+                     "n_syn": net.syn_count(ids["Ce"]) + net.syn_count(ids["Ci"]),
+                     "state": {v: net.get_state(P, v) for v in ("v", "m", "h", "n", "ge", "gi")}}
+        net.close()
+    return out["gpu"], out["orc"]
+
+
+def test_cobahh_config_rollout_float64_exact(gpu_factory, oracle_factory):
+    """The configured network (1e5 neurons, 200,007,783 generated synapses, delays 1..50) in
+    float64 for 200 steps, through the initial burst (~12,700 spikes, each delivered to ~2000
+    targets through the delay ring): every spike at the same step, the delay-queue contents
+    after the last step equal (bundle for bundle), state within 1e-10."""
+    g, o = _cobahh_rollout(gpu_factory, oracle_factory, "float64", False, 200)
+    assert g["n_syn"] == o["n_syn"] == 200_007_783
+    (gi, gs), (oi, os_) = g["spk"], o["spk"]
+    assert len(gi) > 10_000
+    np.testing.assert_array_equal(gs, os_)
+    np.testing.assert_array_equal(gi, oi)
+    for k in range(2):
+        assert len(g["q"][k]) > 0
+        np.testing.assert_array_equal(g["q"][k], o["q"][k])
+    scale = {"v": 0.1, "m": 1, "h": 1, "n": 1, "ge": 80 * nS, "gi": 400 * nS}
+    for v, sc in scale.items():
+        _close(g["state"][v], o["state"][v], 1e-10, 1e-10 * sc, v)
+
+
+def test_cobahh_config_rollout_float32_within_one_step(gpu_factory, oracle_factory):
+    """The configured network in its configured float32 for 200 steps against the oracle's
+    float32 mode (the GPU's exp and division are the hardware forms, the oracle's the
+    correctly rounded ones): every spike within one dt of the other side's, both ways."""
+    g, o = _cobahh_rollout(gpu_factory, oracle_factory, "float32", True, 200)
+    assert g["n_syn"] == o["n_syn"] == 200_007_783
+    (gi, gs), (oi, os_) = g["spk"], o["spk"]
+    assert len(gi) > 10_000
+    assert _within_one_step(gi, gs, oi, os_) == 1.0
+    assert _within_one_step(oi, os_, gi, gs) == 1.0
+    assert abs(len(gi) - len(oi)) <= 0.001 * len(oi)
+
+
+# ---- STDP: 1e4 Poisson at 15 Hz -> 1e3 LIF, all-to-all (1e7 synapses) -----------------------
+@pytest.mark.parametrize("post_grouped", [False, True])
+def test_stdp_config_float64(gpu_factory, oracle_factory, post_grouped):
+    """The configured 1e4 -> 1e3 all-to-all STDP network (1e7 synapses, both pathways), in
+    float64, for 300 steps with the GPU's cuRAND uniforms fed to the oracle: input and output
+    spikes exact, every synapse's w, Apre, Apost and lastupdate within 1e-10 relative.  Both
+    record orders of the synapse variables (autotuner site kind 8)."""
+    K = 50
+    gpu = gpu_factory(DT, steps_per_graph=K, seed=models.SEED_BASE + 2)
+    orc = oracle_factory(DT)
+    ids = {}
+    for name, net in (("gpu", gpu), ("orc", orc)):
+        ids[name] = models.build_stdp(net, n_in=10_000, n_out=1_000, rate=15.0,
+                                      dtype="float64", monitor_capacity=4_000_000)
+        net.finalize()
+    if post_grouped:
+        gpu.tune_apply([{"site_kind": 8, "site_index": 0, "choice_a": 1, "choice_b": 0}])
+    for _ in range(6):
+        gpu.run(K)
+        orc.set_uniforms(ids["orc"]["inp"], gpu.rng_uniforms(ids["gpu"]["inp"], K))
+        orc.run(K)
+    for g in ("inp", "out"):
+        a, b = gpu.spikes(ids["gpu"][g]), orc.spikes(ids["orc"][g])
+        np.testing.assert_array_equal(a[1], b[1])
+        np.testing.assert_array_equal(a[0], b[0])
+    assert len(gpu.spikes(ids["gpu"]["inp"])[0]) > 3000
+    assert len(gpu.spikes(ids["gpu"]["out"])[0]) > 1000
+    S = ids["gpu"]["S"]
+    for v, atol in (("w", 1e-18), ("Apre", 1e-20), ("Apost", 1e-20), ("lastupdate", 1e-15)):
+        _close(gpu.syn_get(S, v), orc.syn_get(ids["orc"]["S"], v), 1e-10, atol, v)
+
+
+def test_stdp_config_float32(gpu_factory, oracle_factory):
+    """The same network in the configured float32 against the oracle's float32 mode, with
+    the GPU's uniforms: input spikes exact; output spikes within one dt both ways (the GPU
+    adds the per-synapse weights into ge with atomics in no fixed order, so v can differ in
+    its last bits); weights within 1e-5 relative of gmax."""
+    K = 50
+    gpu = gpu_factory(DT, steps_per_graph=K, seed=models.SEED_BASE + 2)
+    orc = oracle_factory(DT, f32=True)
+    ids = {}
+    for name, net in (("gpu", gpu), ("orc", orc)):
+        ids[name] = models.build_stdp(net, n_in=10_000, n_out=1_000, rate=15.0,
+                                      dtype="float32", monitor_capacity=4_000_000)
+        net.finalize()
+    for _ in range(6):
+        gpu.run(K)
+        orc.set_uniforms(ids["orc"]["inp"], gpu.rng_uniforms(ids["gpu"]["inp"], K))
+        orc.run(K)
+    a, b = gpu.spikes(ids["gpu"]["inp"]), orc.spikes(ids["orc"]["inp"])
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[0], b[0])
+    (gi, gs), (oi, os_) = gpu.spikes(ids["gpu"]["out"]), orc.spikes(ids["orc"]["out"])
+    assert len(gi) > 1000
+    assert _within_one_step(gi, gs, oi, os_) == 1.0
+    assert _within_one_step(oi, os_, gi, gs) == 1.0
+    _close(gpu.syn_get(ids["gpu"]["S"], "w"), orc.syn_get(ids["orc"]["S"], "w"), 1e-5,
+           1e-5 * 0.01, "w")
+
+
+# ---- multicompartment Hines batch: the configured 1024 morphologies -------------------------
+def _hines_config(gpu_factory, channel_dtype, steps):
+    from oracle.oracle import OracleHines
+    net = gpu_factory(25e-6)
+    hb, morph, params, current = models.build_hines(net, n_neurons=1024,
+                                                    channel_dtype=channel_dtype)
+    n_comp = int(morph["comp_off"][-1])
+    assert 1024 * 200 <= n_comp <= 1024 * 1000
+    orc = OracleHines(25e-6, morph["comp_off"], morph["sec_off"], morph["sec_start"],
+                      morph["sec_end"], morph["sec_parent"], morph["diameter"], morph["length"],
+                      params, f32=(channel_dtype == "float32"))
+    for k, v in models.hines_rest_state().items():
+        orc.set_state(k, v)
+    orc.set_current(current)
+    hb.run(steps)
+    orc.run(steps)
+    return hb, orc
+
+
+def test_hines_config_float64_channels(gpu_factory):
+    """All 1024 configured morphologies (200-1000 compartments each) for 200 steps (5 ms, past
+    the first soma spikes) with float64 channels: every compartment's v, m, h, n within 1e-10
+    relative, Ic within 1e-10 relative, soma spike counts equal."""
+    hb, orc = _hines_config(gpu_factory, "float64", 200)
+    for v, atol in (("v", 1e-15), ("m", 1e-15), ("h", 1e-15), ("n", 1e-15), ("Ic", 1e-12)):
+        _close(hb.get_state(v), orc.get_state(v), 1e-10, atol, v)
+    np.testing.assert_array_equal(hb.spike_counts(), orc.spike_counts())
+
+
+def test_hines_config_float32_channels(gpu_factory):
+    """The configured batch as configured (float32 channels, float64 cable solve) against
+    the oracle in the same precisions: v within 1e-4 relative (1e-6 V), gates within 1e-4."""
+    hb, orc = _hines_config(gpu_factory, "float32", 200)
+    _close(hb.get_state("v"), orc.get_state("v"), 1e-4, 1e-6, "v")
+    for v in ("m", "h", "n"):
+        _close(hb.get_state(v), orc.get_state(v), 1e-4, 1e-5, v)
+
+
+# ---- batched: instances of the 256-instance population ----------------------------------------
+SAMPLED = list(range(0, 256, 16))   # 16 of the 256 configured instances, their own sizes
+
+
+def _batched(gpu_factory, oracle_factory, dtype, f32_oracle, steps):
+    sizes, we = models.batch_sizes()
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT, f32=f32_oracle) if name == "orc" else make(DT)
+        ids = models.build_cobahh_batch(net, sizes, we, dtype=dtype, instances=SAMPLED,
+                                        monitor_capacity=1_000_000)
+        net.finalize()
+        net.run(steps)
+        out[name] = [(net.spikes(G), net.get_state(G, "v")) for G in ids["groups"]]
+        net.close()
+    return out["gpu"], out["orc"], sizes
+
+
+def test_batched_config_instances_float64_exact(gpu_factory, oracle_factory):
+    """16 instances of the configured batch (every 16th of the 256, with the sizes, weights,
+    seeds and initial states they have there) merged into one population and one projection,
+    in float64 for 100 steps: every instance's spikes exact, v within 1e-10."""
+    g, o, sizes = _batched(gpu_factory, oracle_factory, "float64", False, 100)
+    assert sum(int(sizes[k]) for k in SAMPLED) > 50_000
+    total = 0
+    for k, ((gsp, gv), (osp, ov)) in enumerate(zip(g, o)):
+        np.testing.assert_array_equal(gsp[1], osp[1], err_msg=f"instance {SAMPLED[k]}")
+        np.testing.assert_array_equal(gsp[0], osp[0], err_msg=f"instance {SAMPLED[k]}")
+        _close(gv, ov, 1e-10, 1e-12, f"v of instance {SAMPLED[k]}")
+        total += len(gsp[0])
+    assert total > 1000
+
+
+def test_batched_config_instances_float32_within_one_step(gpu_factory, oracle_factory):
+    """The same 16 instances in the configured float32 against the oracle's float32 mode for
+    100 steps: every spike of every instance within one dt of the other side's, both ways."""
+    g, o, _ = _batched(gpu_factory, oracle_factory, "float32", True, 100)
+    total = 0
+    for k, ((gsp, _gv), (osp, _ov)) in enumerate(zip(g, o)):
+        (gi, gs), (oi, os_) = gsp, osp
+        assert _within_one_step(gi, gs, oi, os_) == 1.0, f"instance {SAMPLED[k]}"
+        assert _within_one_step(oi, os_, gi, gs) == 1.0, f"instance {SAMPLED[k]}"
+        total += len(gi)
+    assert total > 1000

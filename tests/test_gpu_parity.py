@@ -439,6 +439,39 @@ def test_profile_advances_like_run(gpu_factory):
         _close(out["profile"][3], out["run"][3], 1e-12, 1e-15)
 
 
+def test_profile_graph_advances_like_run(gpu_factory):
+    """Timing every launch site inside the replayed step graphs (event-record nodes) leaves
+    the net where b2b_run would, and the per-site times fit inside the step: in the per-step
+    form the sites run one after another, so their sum is at most the step time; in the
+    two-launch form each of the two overlapping sites is."""
+    for fused in (True, False):
+        out = {}
+        for how in ("run", "profile"):
+            net = gpu_factory(DT, fused=fused, steps_per_graph=25)
+            G, Ce, Ci, _ = _delay_net(net, n=1000)
+            net.finalize()
+            net.run(40)
+            if how == "run":
+                net.run(150)
+            else:
+                prof, step_ms = net.profile_graph(150)
+                kinds = [k for k, _ in prof]
+                assert kinds == ([5, 1] if fused else [1, 6, 6]), kinds
+                assert all(ms > 0 for _, ms in prof) and step_ms > 0
+                if fused:
+                    assert max(ms for _, ms in prof) <= step_ms
+                else:
+                    assert sum(ms for _, ms in prof) <= step_ms
+            assert net.timestep == 190
+            net.run(30)
+            idx, st = net.spikes(G)
+            out[how] = (idx, st, net.get_state(G, "v"), net.queue(Ce))
+        assert len(out["run"][0]) > 50
+        for k in (0, 1, 3):
+            np.testing.assert_array_equal(out["profile"][k], out["run"][k])
+        _close(out["profile"][2], out["run"][2], 1e-12, 1e-15)
+
+
 def _spikes_within_one_step(a_idx, a_stp, b_idx, b_stp):
     """Fraction of spikes of a that b has at the same neuron within one step."""
     keys = set(zip(b_idx.tolist(), b_stp.tolist()))
