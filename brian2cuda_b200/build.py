@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                  "-Xcompiler", "-Wall", "-Xcompiler", "-Wno-unused-function",
                  f"-I{os.path.join(ROOT, 'include')}"]
-LDFLAGS = ARCH + ["-shared", f"-L{CUDA_HOME}/lib64", "-lcurand",
+LDFLAGS = ARCH + ["-shared", f"-L{CUDA_HOME}/lib64", "-lcurand", "-ldl",
                   "-Xlinker", f"-rpath={CUDA_HOME}/lib64"]
 
 

@@ -5,6 +5,8 @@
 // but as a library: the network is described once, laid out on the GPU by b2b_finalize,
 // and advanced by replaying a CUDA graph of `steps_per_graph` steps per launch with no host
 // synchronisation inside a run.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <cstdarg>
 #include <cstdlib>
@@ -54,13 +56,17 @@ size_t var_size(int dtype, int var) {
 }
 size_t real_size(int dtype) { return dtype == B2B_F32 ? 4 : 8; }
 
-bool kind_has_var(int kind, int var) {
+// model_vars: state variables of a generated model (KIND_MODEL), slots 0 .. model_vars-1.
+bool kind_has_var(int kind, int var, int model_vars = 0) {
   switch (kind) {
     case KIND_LIF:
       return var == B2B_VAR_V || var == B2B_VAR_GE || var == B2B_VAR_GI ||
              var == B2B_VAR_LASTSPIKE || var == B2B_VAR_NOT_REFRACTORY;
     case KIND_HH:
       return var >= 0 && var < kMaxVars;
+    case KIND_MODEL:
+      return (var >= 0 && var < model_vars) || var == B2B_VAR_LASTSPIKE ||
+             var == B2B_VAR_NOT_REFRACTORY;
     default:
       return false;
   }
@@ -135,6 +141,7 @@ HhDev hh_dev(const Group& g, double dt) {
 bool has_refractory(const Group& g) {
   if (g.kind == KIND_LIF) return g.lif.refractory > 0;
   if (g.kind == KIND_HH) return g.hh.refractory > 0;
+  if (g.kind == KIND_MODEL) return g.model_refractory > 0;
   return false;
 }
 
@@ -183,12 +190,16 @@ b2b_status finalize_pops(b2b_net* net) {
   for (size_t gi = 0; gi < net->groups.size(); ++gi) {
     Group& g = net->groups[gi];
     int pi = -1;
-    for (size_t p = 0; p < net->pops.size(); ++p)
-      if (net->pops[p].kind == g.kind && net->pops[p].dtype == g.dtype) pi = (int)p;
+    // a generated model's group is a population of its own (its kernel is the model's)
+    if (g.kind != KIND_MODEL)
+      for (size_t p = 0; p < net->pops.size(); ++p)
+        if (net->pops[p].kind == g.kind && net->pops[p].dtype == g.dtype) pi = (int)p;
     if (pi < 0) {
       net->pops.emplace_back();
       net->pops.back().kind = g.kind;
       net->pops.back().dtype = g.dtype;
+      net->pops.back().model_launch = g.model_launch;
+      net->pops.back().minfo = g.minfo;
       pi = (int)net->pops.size() - 1;
     }
     Pop& pop = net->pops[pi];
@@ -205,6 +216,9 @@ b2b_status finalize_pops(b2b_net* net) {
     if (post.kind == KIND_LIF && post.lif.has_reset && s.target_var == B2B_VAR_V &&
         !(net->cfg.flags & B2B_NET_RESET_BEFORE_SYNAPSES))
       net->pops[post.pop].late_reset = true;
+    if (post.kind == KIND_MODEL && (post.minfo.reset_mask & (1 << s.target_var)) &&
+        !(net->cfg.flags & B2B_NET_RESET_BEFORE_SYNAPSES))
+      net->pops[post.pop].late_reset = true;
   }
   for (size_t pi = 0; pi < net->pops.size(); ++pi) {
     Pop& pop = net->pops[pi];
@@ -215,9 +229,9 @@ b2b_status finalize_pops(b2b_net* net) {
     D.late_reset = pop.late_reset ? 1 : 0;
     const size_t rs = real_size(pop.dtype);
     // state
-    if (pop.kind == KIND_LIF || pop.kind == KIND_HH) {
+    if (pop.kind == KIND_LIF || pop.kind == KIND_HH || pop.kind == KIND_MODEL) {
       for (int v = 0; v < kMaxVars; ++v) {
-        if (!kind_has_var(pop.kind, v)) continue;
+        if (!kind_has_var(pop.kind, v, pop.minfo.n_vars)) continue;
         const size_t es = var_size(pop.dtype, v);
         std::vector<uint8_t> host(es * pop.n, 0);
         for (int gi : pop.groups) {
@@ -265,6 +279,10 @@ b2b_status finalize_pops(b2b_net* net) {
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       } else if (pop.kind == KIND_POISSON) {
         PoissonDev d{g.rate * dt, g.offset, g.n};
+        prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
+      } else if (pop.kind == KIND_MODEL) {
+        ModelGroupDev d{g.offset, g.n,
+                        has_refractory(g) ? timestep_host(g.model_refractory, dt) : -1};
         prm.insert(prm.end(), (uint8_t*)&d, (uint8_t*)&d + sizeof(d));
       }
     }
@@ -332,11 +350,20 @@ b2b_status finalize_pops(b2b_net* net) {
       CU(cudaMemset(D.mon_cnt, 0, sizeof(unsigned long long)));
       D.mon_cap = cap;
     }
-    // Poisson uniform buffer
-    if (pop.kind == KIND_POISSON) {
+    // Poisson uniform buffer; a generated model's uniform and normal buffers
+    const int64_t n_uni = pop.kind == KIND_POISSON ? 1
+                          : (pop.kind == KIND_MODEL ? pop.minfo.n_uniform : 0);
+    const int64_t n_nrm = pop.kind == KIND_MODEL ? pop.minfo.n_normal : 0;
+    if (n_uni > 0 || n_nrm > 0) {
       pop.rng_steps = net->cfg.steps_per_graph;
-      CU(dalloc(pop, (uint8_t**)&pop.rng_buf, rs * pop.rng_steps * pop.n));
-      D.rng = pop.rng_buf;
+      if (n_uni > 0) {
+        CU(dalloc(pop, (uint8_t**)&pop.rng_buf, rs * pop.rng_steps * n_uni * pop.n));
+        D.rng = pop.rng_buf;
+      }
+      if (n_nrm > 0) {
+        CU(dalloc(pop, (uint8_t**)&pop.rng_normal_buf, rs * pop.rng_steps * n_nrm * pop.n));
+        D.rng_normal = pop.rng_normal_buf;
+      }
       if (!net->gen) {
         if (curandCreateGenerator(&net->gen, CURAND_RNG_PSEUDO_PHILOX4_32_10) !=
                 CURAND_STATUS_SUCCESS ||
@@ -918,14 +945,31 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
 
 b2b_status refill_rng(b2b_net* net, int kk) {
   for (Pop& pop : net->pops) {
-    if (pop.kind != KIND_POISSON) continue;
-    const size_t n = (size_t)kk * pop.n;
-    curandStatus_t st = pop.dtype == B2B_F32
-                            ? curandGenerateUniform(net->gen, (float*)pop.rng_buf, n)
-                            : curandGenerateUniformDouble(net->gen, (double*)pop.rng_buf, n);
-    if (st != CURAND_STATUS_SUCCESS)
-      return fail(net, B2B_ERR_CUDA, "curandGenerateUniform failed (%d)", (int)st);
-    net->rng_offset += n;
+    const int64_t n_uni = pop.kind == KIND_POISSON ? 1
+                          : (pop.kind == KIND_MODEL ? pop.minfo.n_uniform : 0);
+    const int64_t n_nrm = pop.kind == KIND_MODEL ? pop.minfo.n_normal : 0;
+    if (n_uni > 0) {
+      const size_t n = (size_t)kk * n_uni * pop.n;
+      curandStatus_t st = pop.dtype == B2B_F32
+                              ? curandGenerateUniform(net->gen, (float*)pop.rng_buf, n)
+                              : curandGenerateUniformDouble(net->gen, (double*)pop.rng_buf, n);
+      if (st != CURAND_STATUS_SUCCESS)
+        return fail(net, B2B_ERR_CUDA, "curandGenerateUniform failed (%d)", (int)st);
+      net->rng_offset += n;
+    }
+    if (n_nrm > 0) {
+      // standard normal numbers for the model's noise terms (xi) and randn(): the buffer
+      // brian2cuda refills with curandGenerateNormal (brian2cuda/device.py:751-775); the
+      // count is even (populations are padded to 128 neurons), as the generator requires
+      const size_t n = (size_t)kk * n_nrm * pop.n;
+      curandStatus_t st =
+          pop.dtype == B2B_F32
+              ? curandGenerateNormal(net->gen, (float*)pop.rng_normal_buf, n, 0.0f, 1.0f)
+              : curandGenerateNormalDouble(net->gen, (double*)pop.rng_normal_buf, n, 0.0, 1.0);
+      if (st != CURAND_STATUS_SUCCESS)
+        return fail(net, B2B_ERR_CUDA, "curandGenerateNormal failed (%d)", (int)st);
+      net->rng_offset += n;
+    }
   }
   return B2B_OK;
 }
@@ -962,6 +1006,34 @@ b2b_status capture_graph(b2b_net* net) {
   if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   net->graph_nodes = (int64_t)nodes;
   net->graph_steps = net->cfg.steps_per_graph;
+  return B2B_OK;
+}
+
+// Copies the random numbers the last chunk drew for group gid to the host: a Poisson group's
+// uniforms (n = group size per step), or a generated model's uniforms / normals (n = draws
+// per step x group size, draw-major).
+b2b_status rng_buffer_get(b2b_net* net, int32_t gid, bool normal, void* host, int64_t steps,
+                          int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
+  const Group& g = net->groups[gid];
+  int64_t draws = 0;
+  if (g.kind == KIND_POISSON && !normal) draws = 1;
+  if (g.kind == KIND_MODEL) draws = normal ? g.minfo.n_normal : g.minfo.n_uniform;
+  CHECK(draws > 0, B2B_ERR_INVALID_ARG, "group %d draws no %s numbers", gid,
+        normal ? "normal" : "uniform");
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(host && n == draws * g.n && steps > 0 && steps <= net->last_chunk_steps,
+        B2B_ERR_INVALID_ARG, "bad shape");
+  const Pop& pop = net->pops[g.pop];
+  const uint8_t* buf = static_cast<const uint8_t*>(normal ? pop.rng_normal_buf : pop.rng_buf);
+  const size_t rs = real_size(pop.dtype);
+  CU(cudaStreamSynchronize(net->stream));
+  for (int64_t k = 0; k < steps; ++k)
+    for (int64_t d = 0; d < draws; ++d)
+      CU(cudaMemcpy((uint8_t*)host + rs * (k * n + d * g.n),
+                    buf + rs * ((k * draws + d) * pop.n + g.offset), rs * g.n,
+                    cudaMemcpyDeviceToHost));
   return B2B_OK;
 }
 
@@ -1275,7 +1347,8 @@ b2b_status b2b_state_set(b2b_net* net, int32_t gid, int32_t var, const void* hos
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   Group& g = net->groups[gid];
-  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(kind_has_var(g.kind, var, g.minfo.n_vars), B2B_ERR_INVALID_ARG,
+        "group %d has no variable %d", gid, var);
   CHECK(host && n == g.n, B2B_ERR_INVALID_ARG, "expected %lld values", (long long)g.n);
   const size_t es = var_size(g.dtype, var);
   GUARD_BEGIN
@@ -1294,7 +1367,8 @@ b2b_status b2b_state_get(b2b_net* net, int32_t gid, int32_t var, void* host, int
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   Group& g = net->groups[gid];
-  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(kind_has_var(g.kind, var, g.minfo.n_vars), B2B_ERR_INVALID_ARG,
+        "group %d has no variable %d", gid, var);
   CHECK(host && n == g.n, B2B_ERR_INVALID_ARG, "expected %lld values", (long long)g.n);
   CHECK(net->finalized, B2B_ERR_STATE, "state is on the device only after b2b_finalize");
   const size_t es = var_size(g.dtype, var);
@@ -1308,7 +1382,8 @@ b2b_status b2b_state_ptr(b2b_net* net, int32_t gid, int32_t var, void** dev, int
   if (b2b_status st = check_net(net)) return st;
   CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
   Group& g = net->groups[gid];
-  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(kind_has_var(g.kind, var, g.minfo.n_vars), B2B_ERR_INVALID_ARG,
+        "group %d has no variable %d", gid, var);
   CHECK(dev && n, B2B_ERR_INVALID_ARG, "NULL output");
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   *dev = (uint8_t*)net->pops[g.pop].dev.var[var] + var_size(g.dtype, var) * g.offset;
@@ -1406,7 +1481,8 @@ b2b_status b2b_statemon(b2b_net* net, int32_t gid, int32_t var, const int64_t* i
   CHECK(gid >= 0 && gid < (int)net->groups.size() && mid, B2B_ERR_INVALID_ARG,
         "bad group %d", gid);
   const Group& g = net->groups[gid];
-  CHECK(kind_has_var(g.kind, var), B2B_ERR_INVALID_ARG, "group %d has no variable %d", gid, var);
+  CHECK(kind_has_var(g.kind, var, g.minfo.n_vars), B2B_ERR_INVALID_ARG,
+        "group %d has no variable %d", gid, var);
   CHECK(n >= 0 && (idx || n == 0) && every >= 1 && capacity > 0, B2B_ERR_INVALID_ARG,
         "bad indices, interval or capacity");
   StateMon m;
@@ -2299,21 +2375,39 @@ b2b_status b2b_queue_get(b2b_net* net, int32_t sid, int64_t* n, int32_t* offset,
 
 b2b_status b2b_rng_uniforms_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
                                 int64_t n) {
+  return rng_buffer_get(net, gid, false, host, steps, n);
+}
+
+b2b_status b2b_rng_normals_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
+                               int64_t n) {
+  return rng_buffer_get(net, gid, true, host, steps, n);
+}
+
+b2b_status b2b_group_model(b2b_net* net, int64_t n, int32_t dtype, const char* module_path,
+                           double refractory, int32_t* gid) {
   if (b2b_status st = check_net(net)) return st;
-  CHECK(gid >= 0 && gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG, "bad group %d", gid);
-  const Group& g = net->groups[gid];
-  CHECK(g.kind == KIND_POISSON, B2B_ERR_INVALID_ARG, "group %d is not a Poisson group", gid);
-  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
-  CHECK(host && n == g.n && steps > 0 && steps <= net->last_chunk_steps, B2B_ERR_INVALID_ARG,
-        "bad shape");
-  const Pop& pop = net->pops[g.pop];
-  const size_t rs = real_size(pop.dtype);
-  CU(cudaStreamSynchronize(net->stream));
-  for (int64_t k = 0; k < steps; ++k)
-    CU(cudaMemcpy((uint8_t*)host + rs * n * k,
-                  (const uint8_t*)pop.rng_buf + rs * (k * pop.n + g.offset), rs * n,
-                  cudaMemcpyDeviceToHost));
-  return B2B_OK;
+  CHECK(module_path != nullptr, B2B_ERR_INVALID_ARG, "module_path is NULL");
+  CHECK(refractory >= 0 && std::isfinite(refractory), B2B_ERR_INVALID_ARG, "bad refractory");
+  GUARD_BEGIN
+  // The object stays loaded until the process exits: its kernels may be referenced by
+  // captured graphs and other nets.
+  void* dl = dlopen(module_path, RTLD_NOW | RTLD_LOCAL);
+  CHECK(dl != nullptr, B2B_ERR_INVALID_ARG, "cannot load model %s: %s", module_path, dlerror());
+  auto info = reinterpret_cast<ModelInfoFn>(dlsym(dl, "b2b_model_info_v1"));
+  auto launch = reinterpret_cast<ModelLaunchFn>(dlsym(dl, "b2b_model_launch_v1"));
+  CHECK(info && launch, B2B_ERR_INVALID_ARG, "%s exports no b2b model entry points",
+        module_path);
+  Group g;
+  g.kind = KIND_MODEL; g.n = n; g.dtype = dtype;
+  CHECK(info(&g.minfo) == 0 && g.minfo.abi == B2B_MODEL_ABI, B2B_ERR_UNSUPPORTED,
+        "model %s: ABI %d, this library expects %d", module_path, g.minfo.abi, B2B_MODEL_ABI);
+  CHECK(g.minfo.n_vars >= 1 && g.minfo.n_vars <= B2B_MODEL_MAX_VARS && g.minfo.n_normal >= 0 &&
+            g.minfo.n_uniform >= 0, B2B_ERR_UNSUPPORTED, "model %s: bad shape", module_path);
+  g.model_dl = dl;
+  g.model_launch = launch;
+  g.model_refractory = refractory;
+  return add_group(net, std::move(g), gid);
+  GUARD_END
 }
 
 b2b_status b2b_out_degree(b2b_net* net, int32_t gid, int32_t* host, int64_t n) {

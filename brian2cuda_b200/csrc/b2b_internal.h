@@ -20,7 +20,19 @@ constexpr int kChunk = 128;          // synapses one warp takes from a bundle pe
 constexpr int kMaxProjBatch = 8;     // additive projections delivered by one launch
 constexpr int kNumSMs = 148;         // B200
 
-enum Kind { KIND_LIF = 1, KIND_HH = 2, KIND_POISSON = 3, KIND_SPIKEGEN = 4 };
+enum Kind { KIND_LIF = 1, KIND_HH = 2, KIND_POISSON = 3, KIND_SPIKEGEN = 4, KIND_MODEL = 5 };
+
+// Launcher exported by a generated model's shared object (b2b_group_model): phase 0 steps
+// every neuron of the population `pop` (a PopDev), phase 1 applies the deferred reset.
+typedef int32_t (*ModelLaunchFn)(const void* pop, const int64_t* clock, int32_t k, double dt,
+                                 int32_t* status, void* stream, int32_t dtype, int32_t phase);
+typedef int32_t (*ModelInfoFn)(b2b_model_info* info);
+
+// Parameters of a generated-model group as its kernel reads them.
+struct ModelGroupDev {
+  int64_t offset, n;
+  int64_t ref_steps;                      // timestep(refractory, dt); -1 = no refractoriness
+};
 
 // Per-group parameters as the kernels read them (doubles; cast to the state type in-kernel).
 // TimedArray input of a group (b2b_timedarray): values[rows][cols] in the population's
@@ -90,7 +102,9 @@ struct PopDev {
   int64_t* mon_step;
   unsigned long long* mon_cnt;
   int64_t mon_cap;
-  const void* rng;                // uniform buffer [steps][n] (Poisson)
+  const void* rng;                // uniform buffer [steps][n] (Poisson); generated models:
+                                  // [steps][n_uniform][n]
+  const void* rng_normal;         // generated models: normal buffer [steps][n_normal][n]
   const int32_t* sg_idx;          // spike generator entries sorted by step
   const int64_t* sg_step;
   int64_t sg_n;
@@ -212,6 +226,11 @@ struct Group {
   std::vector<double> ta;
   int64_t ta_rows = 0, ta_cols = 0, ta_mul = 1, ta_div = 1;
   std::vector<PoissonIn> pins;                // PoissonInputs (b2b_poisson_input)
+  // generated model (b2b_group_model): its shared object, launcher and requirements
+  void* model_dl = nullptr;
+  ModelLaunchFn model_launch = nullptr;
+  b2b_model_info minfo{};
+  double model_refractory = 0;
 };
 
 struct Pop {
@@ -224,6 +243,9 @@ struct Pop {
   std::vector<void*> allocs;
   int64_t rng_steps = 0;          // rows held by the uniform buffer
   void* rng_buf = nullptr;
+  void* rng_normal_buf = nullptr; // generated models: normal numbers [steps][n_normal][n]
+  ModelLaunchFn model_launch = nullptr;   // generated model (one group per population)
+  b2b_model_info minfo{};
   bool late_reset = false;
   bool inputs = false;            // some group has a TimedArray or PoissonInput input
   int max_delay = 0;

@@ -410,6 +410,8 @@ cudaError_t launch_pop_step(const Pop& pop, const int64_t* clock, int k, double 
 cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t* clock, int k,
                                 double dt, int32_t* status, cudaStream_t s) {
   if (pop.kind == KIND_HH && pop.surr_img) return launch_hh_surrogate(pop, clock, k, dt, status, s);
+  if (pop.kind == KIND_MODEL)   // the generated model's own kernel, from its shared object
+    return (cudaError_t)pop.model_launch(&dev, clock, k, dt, status, s, pop.dtype, 0);
   if (pop.kind == KIND_SPIKEGEN) {
     spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
     return cudaGetLastError();
@@ -423,6 +425,8 @@ cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {
+  if (pop.kind == KIND_MODEL)
+    return (cudaError_t)pop.model_launch(&pop.dev, clock, k, 0.0, nullptr, s, pop.dtype, 1);
   if (pop.kind != KIND_LIF) return cudaSuccess;
   const unsigned grid = 2 * kNumSMs;
   if (pop.dtype == B2B_F32) lif_late_reset_kernel<float><<<grid, kBlock, 0, s>>>(pop.dev, clock, k);

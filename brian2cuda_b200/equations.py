@@ -204,6 +204,16 @@ def to_sympy(expr: str, symbols: dict[str, sp.Symbol]) -> sp.Expr:
         raise EquationError(f"cannot parse expression {expr!r}: {exc}") from None
 
 
+def condition_to_sympy(cond: str, symbols: dict[str, sp.Symbol]) -> sp.Basic:
+    """A Brian2 condition (comparisons joined by and / or, negated by not) as a sympy
+    boolean; each operand of and / or is parenthesised, since & and | bind tighter than the
+    comparisons in the expression grammar."""
+    c = re.sub(r"\bor\b", ") | (", cond)
+    c = re.sub(r"\band\b", ") & (", c)
+    c = re.sub(r"\bnot\b", "~", c)
+    return to_sympy("(" + c + ")", symbols)
+
+
 def numeric_namespace(namespace: dict) -> dict[str, float]:
     """Unit names and the user's numeric constants (floats in SI)."""
     ns = dict(UNITS)
@@ -287,17 +297,21 @@ def linear_system(res: Resolved) -> tuple[np.ndarray, np.ndarray]:
     zero = {y: sp.Integer(0) for y in xs}
     for r, x in enumerate(res.state):
         ex = sp.expand(res.f[x])
-        if XI in ex.free_symbols or T in ex.free_symbols:
-            raise EquationError(f"d{x}/dt is not autonomous and noise-free")
-        for c, y in enumerate(xs):
-            coef = sp.diff(ex, y)
-            if coef.free_symbols:
-                raise EquationError(f"d{x}/dt is not linear with constant coefficients")
-            A[r, c] = float(coef)
-        rest = ex.xreplace(zero)          # affine: the right-hand side at x = 0
-        if rest.free_symbols:
-            raise EquationError(f"d{x}/dt is not linear with constant coefficients")
-        b[r] = float(rest)
+        if ex.free_symbols & {XI, T} or any(s.name.startswith("xi_") for s in ex.free_symbols) \
+                or ex.has(RAND) or ex.has(RANDN):
+            raise EquationError(f"d{x}/dt is not autonomous and deterministic")
+        try:
+            for c, y in enumerate(xs):
+                coef = sp.diff(ex, y)
+                if coef.free_symbols:
+                    raise TypeError
+                A[r, c] = float(coef)
+            rest = ex.xreplace(zero)          # affine: the right-hand side at x = 0
+            if rest.free_symbols:
+                raise TypeError
+            b[r] = float(rest)
+        except TypeError:
+            raise EquationError(f"d{x}/dt is not linear with constant coefficients") from None
     return A, b
 
 

@@ -137,11 +137,14 @@ class Script:
     that builds and runs it on a backend."""
 
     def __init__(self, dt: float = 1e-4, seed: int = 0, dtype: str = "float64",
-                 namespace: dict | None = None):
+                 namespace: dict | None = None, generated_only: bool = False):
+        """generated_only: integrate every NeuronGroup with generated code, also models the
+        hand-written kernels would take (to compare the two)."""
         self.dt = float(dt)
         self.seed = int(seed)
         self.dtype = dtype
         self.namespace = dict(namespace or {})
+        self.generated_only = bool(generated_only)
         self.objects: list = []
         self.runs: list[int] = []
         self._n = 0
@@ -238,22 +241,33 @@ def _ns(script, *extra):
     return ns
 
 
-def _threshold(expr: str | None, ns) -> tuple[str, float] | None:
+_OTHER = "*"    # a threshold or reset the hand-written kernels do not take (generated code)
+
+
+def _threshold(expr: str | None, ns) -> tuple[str, float | None] | None:
+    """(var, value) for `var > value`; (_OTHER, None) for any other condition."""
     if expr is None:
         return None
     m = re.match(r"^\s*([A-Za-z_]\w*)\s*>\s*(.+?)\s*$", expr)
-    if not m:
-        raise ModelUnsupported(f"threshold {expr!r}: only `var > value` is lowered")
-    return m.group(1), E.value_of(m.group(2), ns)
+    if m:
+        try:
+            return m.group(1), E.value_of(m.group(2), ns)
+        except E.EquationError:
+            pass
+    return _OTHER, None
 
 
-def _reset(expr: str | None, ns) -> tuple[str, float] | None:
+def _reset(expr: str | None, ns) -> tuple[str, float | None] | None:
+    """(var, value) for `var = value`; (_OTHER, None) for other statements."""
     if not expr:
         return None
     st = statements(expr)
-    if len(st) != 1 or st[0][1] != "=":
-        raise ModelUnsupported(f"reset {expr!r}: only `var = value` is lowered")
-    return st[0][0], E.value_of(st[0][2], ns)
+    if len(st) == 1 and st[0][1] == "=":
+        try:
+            return st[0][0], E.value_of(st[0][2], ns)
+        except E.EquationError:
+            pass
+    return _OTHER, None
 
 
 def _seconds(v, ns) -> float:
@@ -445,6 +459,8 @@ def _lower_group(script, g: GroupDesc, ops, groups, rng, notes):
     method = sp_["method"]
     dtype = sp_["dtype"]
     vname = thr[0] if thr else (rst[0] if rst else (res.state[0] if res.state else None))
+    if thr and thr[0] == _OTHER or rst and rst[0] == _OTHER or script.generated_only:
+        vname = None         # neither hand-written kernel takes this threshold / reset
     lowered = None
     if method in (None, "exact", "linear"):
         m = R.match_lif(res, vname, ns) if vname else None

@@ -581,6 +581,28 @@ class Network:
         self._check(self._lib.b2b_rng_uniforms_get(self._h, gid, _ptr(a), steps, n), "rng")
         return a
 
+    def rng_normals(self, gid: int, steps: int, n_normal: int) -> np.ndarray:
+        """Normal numbers the last run chunk drew for a generated-model group: (steps,
+        n_normal * size), draw d of neuron i at [:, d * size + i]."""
+        n = n_normal * self.group_size(gid)
+        a = np.empty((steps, n), dtype=_np_dtype(self._groups[gid][2]))
+        self._check(self._lib.b2b_rng_normals_get(self._h, gid, _ptr(a), steps, n),
+                    "rng_normals")
+        return a
+
+    def model_group(self, n: int, model, dtype="float64") -> int:
+        """A group integrated by a generated model (codegen.GeneratedModel): its source is
+        compiled for sm_100a once (cached by content) and the shared object is loaded into
+        the net (b2b_group_model)."""
+        from .codegen import compile_model
+        if model.path is None:
+            model.path = compile_model(model.source)
+        gid = C.c_int32()
+        code = _dt_code(dtype)
+        self._check(self._lib.b2b_group_model(self._h, int(n), code, model.path.encode(),
+                                              float(model.refractory), C.byref(gid)), "model")
+        return self._add("model", n, code, gid)
+
     # -- multicompartment batch -----------------------------------------------------------------
     def hines_batch(self, comp_off, sec_off, sec_start, sec_end, sec_parent, diameter, length,
                     params: HinesParams) -> "HinesBatch":

@@ -165,6 +165,45 @@ b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64
 b2b_status b2b_poisson_input(b2b_net* net, int32_t gid, int32_t var, int64_t n_inputs,
                              double rate_hz, double weight, int32_t* pid);
 
+/* ---- generated neuron models -------------------------------------------------------------
+ * A neuron model that no hand-written kernel integrates: the device plugin generates its
+ * state update, threshold and reset from the Brian2 equations as CUDA device code around this
+ * library's kernel template (brian2cuda_b200/csrc/model_kernel.cuh), compiles it with nvcc
+ * into a shared object (the role of the code objects brian2cuda generates and compiles,
+ * brian2cuda/cuda_generator.py:281-461, templates/common_group.cu:108-160), and the net loads
+ * it and launches it every step like its own kernels.  The object exports
+ *   int32_t b2b_model_info_v1(b2b_model_info* info);
+ *   int32_t b2b_model_launch_v1(const void* pop, const int64_t* clock, int32_t k, double dt,
+ *                               int32_t* status, void* stream, int32_t dtype, int32_t phase);
+ * (phase 0: update, threshold and, unless deferred, reset of every neuron; phase 1: the
+ * deferred reset of the step's spiking neurons).  State variable k of the model is variable
+ * index k of this API (B2B_VAR_V = 0 ... B2B_VAR_N = 5); LASTSPIKE and NOT_REFRACTORY as for the
+ * other groups.  Synapses may add into variables 0, 1 and 2. */
+#define B2B_MODEL_ABI 1
+#define B2B_MODEL_MAX_VARS 6
+typedef struct {
+  int32_t abi;           /* B2B_MODEL_ABI                                                    */
+  int32_t n_vars;        /* state variables, 1 .. B2B_MODEL_MAX_VARS                         */
+  int32_t n_normal;      /* standard normal numbers per neuron and step (noise xi, randn())  */
+  int32_t n_uniform;     /* uniform numbers per neuron and step (rand())                     */
+  int32_t reset_mask;    /* bit k set: the reset writes variable k                           */
+  int32_t has_threshold;
+} b2b_model_info;
+
+/* Adds a group of n neurons integrated by the generated model in the shared object at
+ * module_path (its variables in dtype; refractory in seconds, 0 = none: while refractory the
+ * threshold is off and the model's `(unless refractory)` variables are held).  The numbers the
+ * model draws come from the net's cuRAND generator, one bulk buffer per chunk of steps
+ * (templates/rand.cu:340-463 fills the same kind of buffer), readable with
+ * b2b_rng_normals_get / b2b_rng_uniforms_get.  Before b2b_finalize. */
+b2b_status b2b_group_model(b2b_net* net, int64_t n, int32_t dtype, const char* module_path,
+                           double refractory, int32_t* gid);
+/* Normal numbers the last b2b_run chunk drew for generated-model group gid: `steps` rows of
+ * n_normal x (group size) values, row k = step k of the chunk, draw d of neuron i at
+ * [k][d * size + i]. */
+b2b_status b2b_rng_normals_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
+                               int64_t n);
+
 /* State variables of a group.  Values are in the group's dtype; NOT_REFRACTORY is uint8. */
 enum {
   B2B_VAR_V = 0, B2B_VAR_GE = 1, B2B_VAR_GI = 2, B2B_VAR_M = 3, B2B_VAR_H = 4, B2B_VAR_N = 5,
@@ -406,7 +445,8 @@ b2b_status b2b_spikes_last(b2b_net* net, int32_t gid, int64_t* n, int32_t* idx, 
 b2b_status b2b_queue_get(b2b_net* net, int32_t sid, int64_t* n, int32_t* offset,
                          int32_t* pre, int32_t* delay, int64_t cap);
 /* Uniform numbers the last b2b_run chunk consumed for Poisson group gid: `steps` rows of
- * n values each (row k = step k of the chunk). */
+ * n values each (row k = step k of the chunk); for a generated-model group, rows of
+ * n_uniform x (group size) values laid out as for b2b_rng_normals_get. */
 b2b_status b2b_rng_uniforms_get(b2b_net* net, int32_t gid, void* host, int64_t steps,
                                 int64_t n);
 

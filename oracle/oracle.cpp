@@ -56,7 +56,15 @@
 
 namespace {
 
-enum { LIF = 1, HH = 2, POISSON = 3, SPIKEGEN = 4 };
+enum { LIF = 1, HH = 2, POISSON = 3, SPIKEGEN = 4, MODEL = 5 };
+
+// A group whose arithmetic a caller supplies (generated models): phase 0 advances the state
+// vars[nv][n] by one step (mask = not_refractory in, normals = the step's normal numbers
+// [nn][n]), phase 1 writes the threshold condition into mask, phase 2 resets the n_idx
+// neurons idx.  Returns 0 on success.
+typedef int (*ModelFn)(void* user, int phase, int64_t ts, double t, double dt, int64_t n,
+                       double* vars, uint8_t* mask, const int32_t* idx, int64_t n_idx,
+                       const double* normals);
 enum { V = 0, GE = 1, GI = 2, M = 3, H = 4, N = 5, LASTSPIKE = 6, NOT_REF = 7 };
 enum { ADD = 1, STDP = 2 };
 enum { SYN_I = 0, SYN_J = 1, SYN_DELAY = 2, SYN_W = 3, SYN_APRE = 4, SYN_APOST = 5, SYN_LU = 6 };
@@ -132,6 +140,14 @@ struct Group {
     uint32_t id;
   };
   std::vector<PIn> pins;
+  // MODEL: the caller's arithmetic, its variable count, normal draws per step, refractory
+  // period, reset flag and the queued normal numbers (one row of nn*n per step)
+  ModelFn model_fn = nullptr;
+  void* model_user = nullptr;
+  int model_nv = 0, model_nn = 0, model_reset = 0, model_thr = 0;
+  double model_ref = 0;
+  std::vector<std::vector<double>> normals;
+  size_t nrm_next = 0;
   R input(int64_t ts, int64_t i) const {
     if (ta.empty()) return (R)0;
     const int64_t row = std::min(ts * ta_mul / ta_div, ta_rows - 1);
@@ -140,6 +156,7 @@ struct Group {
   double refractory() const {
     if (kind == LIF) return p[8];
     if (kind == HH) return p[13];
+    if (kind == MODEL) return model_ref;
     return 0;
   }
 };
@@ -319,10 +336,65 @@ void update_hh(Group<R>& g, int64_t ts, double t, double dt) {
   }
 }
 
+// Runs a phase of a MODEL group's callback on a double copy of its variables.
+template <typename R>
+bool model_phase(Net<R>& net, Group<R>& g, int phase, double t, uint8_t* mask,
+                 const std::vector<int32_t>* idx) {
+  const int64_t n = g.n;
+  std::vector<double> x((size_t)g.model_nv * n);
+  for (int v = 0; v < g.model_nv; ++v)
+    for (int64_t i = 0; i < n; ++i) x[(size_t)v * n + i] = (double)g.var[v][i];
+  const double* nrm = nullptr;
+  if (phase == 0 && g.model_nn > 0) {
+    if (g.nrm_next >= g.normals.size()) {
+      net.err = "model group ran out of normal numbers";
+      return false;
+    }
+    nrm = g.normals[g.nrm_next++].data();
+  }
+  const int rc = g.model_fn(g.model_user, phase, net.ts, t, net.dt, n, x.data(), mask,
+                            idx ? idx->data() : nullptr, idx ? (int64_t)idx->size() : 0, nrm);
+  if (rc != 0) {
+    net.err = "model callback failed";
+    return false;
+  }
+  if (phase != 1)
+    for (int v = 0; v < g.model_nv; ++v)
+      for (int64_t i = 0; i < n; ++i) g.var[v][i] = (R)x[(size_t)v * n + i];
+  return true;
+}
+
+template <typename R>
+bool update_model(Net<R>& net, Group<R>& g, double t) {
+  const double refr = g.refractory();
+  const int64_t ref_steps = refr > 0 ? timestep(refr, net.dt) : -1;
+  for (int64_t i = 0; i < g.n; ++i) {
+    bool nr = true;
+    if (ref_steps >= 0) nr = timestep(t - (double)g.var[LASTSPIKE][i], net.dt) >= ref_steps;
+    g.not_ref[i] = nr ? 1 : 0;
+  }
+  return model_phase(net, g, 0, t, g.not_ref.data(), nullptr);
+}
+
 template <typename R>
 bool threshold(Net<R>& net, Group<R>& g, double t) {
   g.spikes.clear();
-  if (g.kind == LIF || g.kind == HH) {
+  if (g.kind == MODEL) {
+    if (g.model_thr) {
+      std::vector<uint8_t> cond(g.n, 0);
+      if (!model_phase(net, g, 1, t, cond.data(), nullptr)) return false;
+      const bool refr = g.refractory() > 0;
+      for (int64_t i = 0; i < g.n; ++i) {
+        if (cond[i] && (!refr || g.not_ref[i])) {
+          g.spikes.push_back((int32_t)i);
+          if (refr) {
+            g.not_ref[i] = 0;
+            g.var[LASTSPIKE][i] = (R)t;
+          }
+        }
+      }
+    }
+  } else if (g.kind == LIF || g.kind == HH) {
     const bool has_thr = g.kind == HH || g.p[9] != 0;
     if (!has_thr) return true;
     const R thr = (R)(g.kind == LIF ? g.p[6] : g.p[12]);
@@ -473,13 +545,18 @@ bool step(Net<R>& net) {
   for (Group<R>& g : net.groups) {
     if (g.kind == LIF) update_lif(g, net.ts, t, net.dt);
     else if (g.kind == HH) update_hh(g, net.ts, t, net.dt);
+    else if (g.kind == MODEL && !update_model(net, g, t)) return false;
   }
   for (Group<R>& g : net.groups)
     if (!threshold(net, g, t)) return false;
+  bool reset_ok = true;
   auto resets = [&]() {
-    for (Group<R>& g : net.groups)
+    for (Group<R>& g : net.groups) {
       if (g.kind == LIF && g.p[10] != 0)
         for (int32_t i : g.spikes) g.var[V][i] = (R)g.p[7];
+      if (g.kind == MODEL && g.model_reset && !g.spikes.empty())
+        reset_ok = model_phase(net, g, 2, t, nullptr, &g.spikes) && reset_ok;
+    }
   };
   if (net.reset_first) resets();
   for (Group<R>& g : net.groups) poisson_inputs(net, g);
@@ -487,6 +564,7 @@ bool step(Net<R>& net) {
   for (Syn<R>& s : net.syns)
     if (s.effect == STDP) pathway_post(net, s, t);
   if (!net.reset_first) resets();
+  if (!reset_ok) return false;
   for (RateMon& m : net.rmons) {
     m.steps.push_back(net.ts);
     m.counts.push_back((int64_t)net.groups[m.gid].spikes.size());
@@ -894,6 +972,32 @@ int api_syn_get(Net<R>& net, int sid, int var, double* out, int64_t n) {
 }
 
 template <typename R>
+int api_group_model(Net<R>& net, int64_t n, int nv, int nn, int has_thr, int has_reset,
+                    double refractory, ModelFn fn, void* user) {
+  if (nv < 1 || nv > 6 || nn < 0 || !fn) return -1;
+  Group<R> g;
+  g.kind = MODEL;
+  g.n = n;
+  g.model_fn = fn;
+  g.model_user = user;
+  g.model_nv = nv;
+  g.model_nn = nn;
+  g.model_thr = has_thr;
+  g.model_reset = has_reset;
+  g.model_ref = refractory;
+  return add_group(net, std::move(g));
+}
+
+template <typename R>
+int api_normals(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n) {
+  if (gid < 0 || gid >= (int)net.groups.size()) return -1;
+  Group<R>& g = net.groups[gid];
+  if (g.kind != MODEL || n != (int64_t)g.model_nn * g.n) return -1;
+  for (int64_t k = 0; k < steps; ++k) g.normals.emplace_back(u + k * n, u + (k + 1) * n);
+  return 0;
+}
+
+template <typename R>
 int api_uniforms(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n) {
   if (gid < 0 || gid >= (int)net.groups.size()) return -1;
   Group<R>& g = net.groups[gid];
@@ -1105,6 +1209,16 @@ int orc_group_lif(void* hp, int64_t n, const double* p) {
 int orc_group_hh(void* hp, int64_t n, const double* p) {
   Handle* h = static_cast<Handle*>(hp);
   return DISPATCH(h, api_group, HH, n, p, 14, 0.0);
+}
+int orc_group_model(void* hp, int64_t n, int nv, int nn, int has_thr, int has_reset,
+                    double refractory, ModelFn fn, void* user) {
+  Handle* h = static_cast<Handle*>(hp);
+  return h->f32 ? api_group_model(h->nf, n, nv, nn, has_thr, has_reset, refractory, fn, user)
+                : api_group_model(h->nd, n, nv, nn, has_thr, has_reset, refractory, fn, user);
+}
+int orc_set_normals(void* hp, int gid, const double* u, int64_t steps, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_normals, gid, u, steps, n);
 }
 int orc_group_poisson(void* hp, int64_t n, double rate) {
   Handle* h = static_cast<Handle*>(hp);

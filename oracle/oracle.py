@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
             "orc_group_lif": (C.c_int, [P, I64, P]),
             "orc_group_hh": (C.c_int, [P, I64, P]),
             "orc_group_poisson": (C.c_int, [P, I64, D]),
+            "orc_group_model": (C.c_int, [P, I64, C.c_int, C.c_int, C.c_int, C.c_int, D, P, P]),
+            "orc_set_normals": (C.c_int, [P, C.c_int, P, I64, I64]),
             "orc_group_spikegen": (C.c_int, [P, I64, I64, P, P]),
             "orc_timedarray": (C.c_int, [P, C.c_int, P, I64, I64, I64, I64]),
             "orc_poisson_input": (C.c_int, [P, C.c_int, C.c_int, I64, D, D]),
@@ -137,6 +139,27 @@ class OracleNet:
     def hh_group(self, n, params, dtype=None):
         p = np.ascontiguousarray(params.as_array(), dtype=np.float64)
         return self._add("hh", n, self._lib.orc_group_hh(self._h, n, _p(p)))
+
+    def model_group(self, n, model, dtype=None):
+        """A group integrated by the oracle's own numpy evaluation of a generated model
+        (model_oracle.ModelCallback) inside the oracle's schedule."""
+        from oracle.model_oracle import ModelCallback
+        cb = ModelCallback(model, self.dt)
+        self._callbacks = getattr(self, "_callbacks", []) + [cb]
+        gid = self._lib.orc_group_model(self._h, int(n), cb.n_vars, len(cb.noise),
+                                        1 if model.threshold else 0, 1 if model.reset else 0,
+                                        float(model.refractory),
+                                        C.cast(cb.cfunc, C.c_void_p), None)
+        self._model_nn = getattr(self, "_model_nn", {})
+        out = self._add("model", n, gid)
+        self._model_nn[out] = len(cb.noise)
+        return out
+
+    def set_normals(self, gid, u):
+        """Queues normal numbers of a model group: rows (steps) of n_normal x size values."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        steps, n = u.shape
+        self._ok(self._lib.orc_set_normals(self._h, gid, _p(u), steps, n), "set_normals")
 
     def poisson_group(self, n, rate, dtype=None):
         return self._add("poisson", n, self._lib.orc_group_poisson(self._h, n, float(rate)))
