@@ -617,3 +617,36 @@ b2b_status b2b_hines_destroy(b2b_hines* h) {
 }
 
 }  // extern "C"
+
+// ---- the solver's reciprocal against the IEEE quotient ---------------------------------------
+namespace b2b {
+namespace {
+__global__ void recip_selftest_kernel(const double* __restrict__ x, double* __restrict__ y,
+                                      int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = recip(x[i]);
+}
+}  // namespace
+}  // namespace b2b
+
+extern "C" b2b_status b2b_recip_selftest(int32_t device, const double* x, double* y,
+                                         int64_t n) {
+  if (!x || !y || n <= 0) return B2B_ERR_INVALID_ARG;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess)
+    return B2B_ERR_CUDA;
+  double *dx = nullptr, *dy = nullptr;
+  cudaError_t e = cudaMalloc(&dx, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&dy, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    b2b::recip_selftest_kernel<<<256, 256>>>(dx, dy, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  if (dx) cudaFree(dx);
+  if (dy) cudaFree(dy);
+  cudaSetDevice(prev);
+  return e == cudaSuccess ? B2B_OK : B2B_ERR_CUDA;
+}

@@ -1105,3 +1105,52 @@ b2b_status b2b_hh_gating_exact(const b2b_hh_params* p, double dt, const float* d
 }
 
 }  // extern "C"
+
+// ---- the bounded wait, made to run out ------------------------------------------------------
+namespace b2b {
+namespace {
+// One CTA waits on an mbarrier with the kernels' own bounded wait (wait_mma, here with `polls`
+// polls).  arrive = 0: nothing arrives and no MMA is in flight, so the wait gives up and the
+// CTA records B2B_ERR_TIMEOUT and returns; arrive = 1: thread 0 arrives first, so the wait
+// completes and the status stays B2B_OK.
+__global__ void wait_selftest_kernel(uint32_t polls, int32_t arrive, int32_t* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar)) : "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0u, polls);
+  const bool all_ok = !__syncthreads_or(!ok);
+  if (!all_ok && threadIdx.x == 0) set_status(status, B2B_ERR_TIMEOUT);
+}
+}  // namespace
+}  // namespace b2b
+
+extern "C" b2b_status b2b_wait_selftest(int32_t device, void* stream, uint32_t polls,
+                                        int32_t arrive, int32_t* device_status) {
+  if (!device_status || polls == 0 || polls > (1u << 20)) return B2B_ERR_INVALID_ARG;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess)
+    return B2B_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int32_t* d = nullptr;
+  int32_t h = -1;
+  cudaError_t e = cudaMalloc(&d, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(int32_t), s);
+  if (e == cudaSuccess) {
+    b2b::wait_selftest_kernel<<<1, 128, 0, s>>>(polls, arrive, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (d) cudaFree(d);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return B2B_ERR_CUDA;
+  *device_status = h;
+  return B2B_OK;
+}

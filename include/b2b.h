@@ -55,7 +55,10 @@ enum { B2B_F32 = 1, B2B_F64 = 2 };
 /* Network flags (b2b_config.flags). */
 enum {
   B2B_NET_NO_GRAPH = 1,   /* launch every step eagerly instead of replaying CUDA graphs */
-  B2B_NET_CHECKED = 2,    /* kernels check indices and record B2B_ERR_INDEX            */
+  B2B_NET_CHECKED = 2,    /* every launch site a kernel of its own (no one-CTA small form,
+                             no two-launch form unless B2B_NET_FUSED is also set), so a
+                             fault or a device status names one launch; input indices are
+                             checked on the host in every mode (B2B_ERR_INDEX)           */
   B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
@@ -288,6 +291,17 @@ b2b_status b2b_connect_random_static(int32_t device, void* stream, int32_t pre_l
  * launches after one warm-up each.  Allocates and frees its own buffers; runs on `stream`. */
 b2b_status b2b_atomic_rate(int32_t device, void* stream, int64_t n_targets, int64_t n_events,
                            int32_t reps, double* loaded_per_s, double* hashed_per_s);
+
+/* Self-tests of two device-side building blocks (no counterpart in the reference):
+ * b2b_wait_selftest runs one CTA that waits with the kernels' bounded mbarrier wait (`polls`
+ * polls, at most 2^20) on a barrier that nothing arrives on (arrive = 0: the wait gives up,
+ * the CTA records B2B_ERR_TIMEOUT in the status word and returns) or that thread 0 arrives on
+ * first (arrive = 1: B2B_OK); *device_status receives the status word.
+ * b2b_recip_selftest evaluates the multicompartment solver's reciprocal (the reciprocal
+ * unit's approximation refined by two Newton-Raphson steps) at x[0..n) into y. */
+b2b_status b2b_wait_selftest(int32_t device, void* stream, uint32_t polls, int32_t arrive,
+                             int32_t* device_status);
+b2b_status b2b_recip_selftest(int32_t device, const double* x, double* y, int64_t n);
 
 /* Synapse variables. I, J, DELAY are int32; the others use the target group's dtype. */
 enum {
