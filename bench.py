@@ -477,8 +477,8 @@ def bench_cobahh(args, world, rank, local):
     d_ms = prof[dsite][1]
     # the delivery's own ceiling: scattered f32 atomics into the population's ge and gi
     # (2e5 floats), one index load per event from HBM
-    loaded, hashed = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
-                                 stream=stream.cuda_stream)
+    loaded, hashed, dsmem = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
+                                        stream=stream.cuda_stream)
     d_rate = p_ev / (d_ms * 1e-3 * SIM_STEPS)
     names = [lab for lab, _ in kernels]
 
@@ -513,7 +513,8 @@ def bench_cobahh(args, world, rank, local):
                      "frac_hbm": deliver_bytes / (d_ms * 1e-3) / 1e9 / hbm,
                      "events_per_s_in_kernel": d_rate,
                      "atomic_ceiling_events_per_s": {"index_loaded": loaded,
-                                                     "index_in_registers": hashed},
+                                                     "index_in_registers": hashed,
+                                                     "cluster_shared_memory": dsmem},
                      "frac_of_atomic_ceiling": d_rate / loaded,
                      "note": "at the network's ~3 Hz a step delivers ~6e4 events: the "
                              "kernel is latency-bound; see configs.propagation for load"},
@@ -961,12 +962,13 @@ def bench_small(args, world, rank, local):
         roof["note"] = ("12 B per event (target index 4 B + target read/write 8 B) + 8 B per "
                         "(spike, delay) bundle; bound: one L2 atomic per event")
         from brian2cuda_b200.network import atomic_rate
-        loaded, hashed = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
-                                     stream=stream.cuda_stream)
+        loaded, hashed, dsmem = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
+                                            stream=stream.cuda_stream)
         d_rate = per_step_events / (dmsk[0] * 1e-3)
         roof["events_per_s_in_kernel"] = d_rate
         roof["atomic_ceiling_events_per_s"] = {"index_loaded": loaded,
-                                               "index_in_registers": hashed}
+                                               "index_in_registers": hashed,
+                                               "cluster_shared_memory": dsmem}
         roof["frac_of_atomic_ceiling"] = d_rate / loaded
         line = _line_base(args, world, "synaptic events/s", value, "events/s",
                           ms / args.steps, WORKLOADS[wl],

@@ -112,7 +112,8 @@ PROTOTYPES = {
     "b2b_recip_selftest": (I32, [I32, P, P, I64]),
     "b2b_group_model": (I32, [P, I64, I32, C.c_char_p, DBL, PI32]),
     "b2b_rng_normals_get": (I32, [P, I32, P, I64, I64]),
-    "b2b_atomic_rate": (I32, [I32, P, I64, I64, I32, C.POINTER(DBL), C.POINTER(DBL)]),
+    "b2b_atomic_rate": (I32, [I32, P, I64, I64, I32, C.POINTER(DBL), C.POINTER(DBL),
+                              C.POINTER(DBL)]),
     "b2b_profile_graph": (I32, [P, I64, C.POINTER(DBL), PI32, I32, PI32, C.POINTER(DBL)]),
     "b2b_spikemon": (I32, [P, I32, I64]),
     "b2b_spikemon_get": (I32, [P, I32, PI64, P, P, I64]),

@@ -143,17 +143,18 @@ def spike_steps(times, dt: float) -> np.ndarray:
 
 
 def atomic_rate(n_targets: int, n_events: int, device: int = 0, stream: int | None = None,
-                reps: int = 5) -> tuple[float, float]:
+                reps: int = 5) -> tuple[float, float, float]:
     """Scattered float32 atomic additions per second that the GPU sustains into an array of
     n_targets floats at uniform indices: (index loaded from device memory per event, index
-    computed in registers).  The ceiling of the additive spike delivery."""
+    computed in registers, into the distributed shared memory of 8-CTA clusters).  The
+    ceiling of the additive spike delivery, and of a delivery accumulating in clusters."""
     lib = N.lib()
-    a, b = C.c_double(), C.c_double()
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
     st = lib.b2b_atomic_rate(int(device), stream, int(n_targets), int(n_events), int(reps),
-                             C.byref(a), C.byref(b))
+                             C.byref(a), C.byref(b), C.byref(c))
     if st != N.B2B_OK:
         raise B2BError(st, "b2b_atomic_rate")
-    return a.value, b.value
+    return a.value, b.value, c.value
 
 
 class Network:

@@ -287,10 +287,13 @@ b2b_status b2b_connect_random_static(int32_t device, void* stream, int32_t pre_l
  * brian2cuda/templates/synapses.cu:117-162; no counterpart as a measurement) into an array of
  * n_targets floats, at indices uniform over the array.  *loaded_per_s: every event's index
  * loaded from an n_events-entry int32 array in device memory first (the delivery's form);
- * *hashed_per_s: the index computed in registers (the atomics alone).  Best of `reps` timed
+ * *hashed_per_s: the index computed in registers (the atomics alone); *dsmem_per_s: the
+ * same additions into the distributed shared memory of 8-CTA thread-block clusters (the
+ * array split into one slice per CTA; 0 when a slice exceeds 200 KB).  Best of `reps` timed
  * launches after one warm-up each.  Allocates and frees its own buffers; runs on `stream`. */
 b2b_status b2b_atomic_rate(int32_t device, void* stream, int64_t n_targets, int64_t n_events,
-                           int32_t reps, double* loaded_per_s, double* hashed_per_s);
+                           int32_t reps, double* loaded_per_s, double* hashed_per_s,
+                           double* dsmem_per_s);
 
 /* Self-tests of two device-side building blocks (no counterpart in the reference):
  * b2b_wait_selftest runs one CTA that waits with the kernels' bounded mbarrier wait (`polls`

@@ -27,6 +27,16 @@ def test_bounded_wait_runs_out_and_reports_timeout():
     assert float(x.sum().item()) == 28.0
 
 
+def test_atomic_rate_probe_measures_three_forms():
+    """The delivery's ceiling probe returns positive rates for the L2 forms and the cluster
+    form (2e5 targets: 100 KB slices of an 8-CTA cluster), and every form's additions land
+    (a form that skipped its work would read far above the others)."""
+    from brian2cuda_b200.network import atomic_rate
+    loaded, hashed, dsmem = atomic_rate(200_000, 20_000_000, reps=2)
+    assert loaded > 1e9 and hashed > 1e9 and dsmem > 1e9
+    assert hashed < 1e13 and dsmem < 1e13
+
+
 def test_solver_reciprocal_within_two_ulps():
     from brian2cuda_b200 import _native
     lib = _native.lib()
