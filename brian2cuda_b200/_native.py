@@ -108,6 +108,7 @@ PROTOTYPES = {
     "b2b_kernel_launches": (I32, [P, PI64]),
     "b2b_run_mode": (I32, [P, PI32]),
     "b2b_profile": (I32, [P, I64, C.POINTER(DBL), PI32, I32, PI32]),
+    "b2b_syn_set_delays": (I32, [P, I32, P, I64]),
     "b2b_wait_selftest": (I32, [I32, P, C.c_uint32, I32, PI32]),
     "b2b_recip_selftest": (I32, [I32, P, P, I64]),
     "b2b_group_model": (I32, [P, I64, I32, C.c_char_p, DBL, PI32]),

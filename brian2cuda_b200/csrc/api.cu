@@ -589,6 +589,27 @@ b2b_status build_proj(b2b_net* net, int pj) {
   return B2B_OK;
 }
 
+// Additive projections with the same kernel variant share one delivery launch (retired
+// projections of a delay change included); the launch shapes go back to the built-in rule.
+void build_add_batches(b2b_net* net) {
+  net->add_batches.clear();
+  for (const Proj& pr : net->projs) {
+    if (pr.effect != B2B_EFFECT_ADD) continue;
+    bool placed = false;
+    for (auto& b : net->add_batches) {
+      const Proj& q = *b[0];
+      if ((int)b.size() < kMaxProjBatch && q.dtype == pr.dtype &&
+          (q.dev.w != nullptr) == (pr.dev.w != nullptr) && q.dev.aggregate == pr.dev.aggregate) {
+        b.push_back(&pr);
+        placed = true;
+        break;
+      }
+    }
+    if (!placed) net->add_batches.push_back({&pr});
+  }
+  net->add_tune.assign(net->add_batches.size(), AddTune{});  // built-in shapes until tuned
+}
+
 b2b_status finalize_projs(b2b_net* net) {
   // merge Synapses objects into projections
   for (size_t si = 0; si < net->syns.size(); ++si) {
@@ -640,22 +661,7 @@ b2b_status finalize_projs(b2b_net* net) {
     b2b_status st = build_proj(net, (int)p);
     if (st != B2B_OK) return st;
   }
-  // additive projections with the same kernel variant share one delivery launch
-  for (const Proj& pr : net->projs) {
-    if (pr.effect != B2B_EFFECT_ADD) continue;
-    bool placed = false;
-    for (auto& b : net->add_batches) {
-      const Proj& q = *b[0];
-      if ((int)b.size() < kMaxProjBatch && q.dtype == pr.dtype &&
-          (q.dev.w != nullptr) == (pr.dev.w != nullptr) && q.dev.aggregate == pr.dev.aggregate) {
-        b.push_back(&pr);
-        placed = true;
-        break;
-      }
-    }
-    if (!placed) net->add_batches.push_back({&pr});
-  }
-  net->add_tune.assign(net->add_batches.size(), AddTune{});  // built-in shapes until tuned
+  build_add_batches(net);
   return B2B_OK;
 }
 
@@ -1006,6 +1012,124 @@ b2b_status capture_graph(b2b_net* net) {
   if (e != cudaSuccess) return fail(net, B2B_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   net->graph_nodes = (int64_t)nodes;
   net->graph_steps = net->cfg.steps_per_graph;
+  return B2B_OK;
+}
+
+// ---- delays changed between runs -----------------------------------------------------------
+// Re-derives the two-launch step's device view from the projections (after a delay change
+// added or dropped one); turns the form off when the projections no longer allow it (a delay
+// of 0, more projections than one launch takes).  Between runs the pending input is folded
+// in, so the per-step form can take over at any run boundary.
+void refresh_two_launch(b2b_net* net) {
+  if (!net->two_launch_ok) return;
+  PendingDev& F = net->pdev;
+  bool ok = net->projs.size() <= (size_t)kMaxProjBatch;
+  int32_t nd_max = 1;
+  for (const Proj& pr : net->projs) {
+    ok = ok && pr.effect == B2B_EFFECT_ADD && pr.dmin >= 1;
+    for (int m : pr.members) ok = ok && F.acc[net->syns[m].target_var] != nullptr;
+    nd_max = std::max(nd_max, pr.dev.nd);
+  }
+  if (!ok) {
+    net->two_launch = false;
+    net->two_launch_ok = false;
+    return;
+  }
+  const Pop& pop = net->pops[0];
+  F.pop = pop.dev;
+  F.n_proj = (int32_t)net->projs.size();
+  F.nd_max = nd_max;
+  for (size_t p = 0; p < net->projs.size(); ++p) {
+    const Proj& pr = net->projs[p];
+    F.proj[p] = pr.dev;
+    for (int m : pr.members) {
+      const int v = net->syns[m].target_var;
+      F.proj[p].targets[v] = F.acc[v];
+    }
+    F.proj[p].target = F.acc[pr.target_var];
+  }
+  net->fold_dev = pop.dev;
+  for (int v = 0; v < 3; ++v) net->fold_dev.fold[v] = F.acc[v];
+}
+
+// Grows population pi's spike-history ring to new_len slots, keeping the spikes of the last
+// old_len - 1 steps (those a delivery can still reach) at their slots in the new ring, and
+// points every view of the ring at the new one.  Snapshots hold rings of the old length and
+// become unusable.
+b2b_status grow_ring(b2b_net* net, int pi, int32_t new_len) {
+  Pop& pop = net->pops[pi];
+  PopDev& D = pop.dev;
+  const int32_t old_len = D.ring_len;
+  int32_t* idx = nullptr;
+  int32_t* cnt = nullptr;
+  CU(dalloc(pop, &idx, (size_t)new_len * pop.n));
+  CU(dalloc(pop, &cnt, (size_t)new_len));
+  CU(cudaMemset(cnt, 0, sizeof(int32_t) * new_len));
+  const int64_t T = net->ts;
+  for (int64_t s = T - 1; s >= 0 && s > T - old_len; --s) {
+    const int64_t so = s % old_len, sn = s % new_len;
+    CU(cudaMemcpy(idx + sn * pop.n, D.ring_idx + so * pop.n, sizeof(int32_t) * pop.n,
+                  cudaMemcpyDeviceToDevice));
+    CU(cudaMemcpy(cnt + sn, D.ring_cnt + so, sizeof(int32_t), cudaMemcpyDeviceToDevice));
+  }
+  for (void* old : {(void*)D.ring_idx, (void*)D.ring_cnt}) {
+    pop.allocs.erase(std::remove(pop.allocs.begin(), pop.allocs.end(), old), pop.allocs.end());
+    cudaFree(old);
+  }
+  D.ring_idx = idx;
+  D.ring_cnt = cnt;
+  D.ring_len = new_len;
+  pop.max_delay = new_len - 2;
+  for (Proj& pr : net->projs) {
+    if (pr.src_pop == pi) {
+      pr.dev.src_ring_idx = idx;
+      pr.dev.src_ring_cnt = cnt;
+      pr.dev.src_ring_len = new_len;
+    }
+    if (pr.effect == B2B_EFFECT_STDP && pr.dst_pop == pi) {
+      pr.dev.post_ring_idx = idx;
+      pr.dev.post_ring_cnt = cnt;
+      pr.dev.post_ring_len = new_len;
+    }
+  }
+  if (!net->rmons.empty()) {
+    std::vector<RateMonDev> devs;
+    for (RateMon& m : net->rmons) {
+      if (net->groups[m.gid].pop == pi) {
+        m.dev.ring_idx = idx;
+        m.dev.ring_cnt = cnt;
+        m.dev.ring_len = new_len;
+      }
+      devs.push_back(m.dev);
+    }
+    CU(cudaMemcpy(net->d_rmons, devs.data(), sizeof(RateMonDev) * devs.size(),
+                  cudaMemcpyHostToDevice));
+  }
+  for (Snapshot& sn : net->snapshots) sn.valid = false;
+  return B2B_OK;
+}
+
+// Drops the retired projections whose last spikes have arrived.
+b2b_status drop_retired(b2b_net* net) {
+  bool any = false;
+  for (size_t p = 0; p < net->projs.size();) {
+    Proj& pr = net->projs[p];
+    if (pr.retire_after >= 0 && net->ts > pr.retire_after) {
+      for (void* a : pr.allocs) cudaFree(a);
+      net->projs.erase(net->projs.begin() + p);
+      any = true;
+    } else {
+      ++p;
+    }
+  }
+  if (any) {
+    build_add_batches(net);
+    refresh_two_launch(net);
+    if (net->graph) {
+      cudaGraphExecDestroy(net->graph);
+      net->graph = nullptr;
+    }
+  }
   return B2B_OK;
 }
 
@@ -1573,6 +1697,7 @@ b2b_status b2b_run(b2b_net* net, int64_t n_steps) {
   CHECK(n_steps >= 0, B2B_ERR_INVALID_ARG, "negative step count");
   const int K = net->cfg.steps_per_graph;
   const bool use_graph = !(net->cfg.flags & B2B_NET_NO_GRAPH);
+  if (b2b_status st = drop_retired(net)) return st;
   while (n_steps > 0) {
     const int kk = (int)std::min<int64_t>(n_steps, K);
     if (b2b_status st = refill_rng(net, kk)) return st;
@@ -2422,13 +2547,79 @@ b2b_status b2b_out_degree(b2b_net* net, int32_t gid, int32_t* host, int64_t n) {
   CU(cudaMalloc(&d, sizeof(int32_t) * std::max<int64_t>(n, 1)));
   cudaError_t e = cudaMemsetAsync(d, 0, sizeof(int32_t) * n, net->stream);
   for (const Proj& pr : net->projs)
-    if (e == cudaSuccess && pr.src_pop == g.pop && n > 0)
+    if (e == cudaSuccess && pr.src_pop == g.pop && n > 0 && pr.retire_after < 0)
       e = add_out_degree(pr.off, pr.dev.nd, g.offset, n, d, net->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(host, d, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, net->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
   cudaFree(d);
   CU(e);
+  return B2B_OK;
+  GUARD_END
+}
+
+b2b_status b2b_syn_set_delays(b2b_net* net, int32_t sid, const int32_t* delay_steps,
+                              int64_t n) {
+  if (b2b_status st = check_net(net)) return st;
+  CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
+  CHECK(sid >= 0 && sid < (int)net->syns.size(), B2B_ERR_INVALID_ARG, "bad synapses id %d", sid);
+  Syn& sy = net->syns[sid];
+  CHECK(!sy.generated, B2B_ERR_UNSUPPORTED,
+        "delays of connectivity generated on the GPU are fixed");
+  CHECK(sy.effect == B2B_EFFECT_ADD, B2B_ERR_UNSUPPORTED, "delays of STDP synapses are fixed");
+  CHECK(!net->small, B2B_ERR_UNSUPPORTED, "the one-CTA small form keeps its delays");
+  CHECK(delay_steps && n == sy.n, B2B_ERR_INVALID_ARG, "n must be the synapse count");
+  for (int64_t k = 0; k < n; ++k)
+    CHECK(delay_steps[k] >= 0, B2B_ERR_INVALID_ARG, "negative delay at synapse %lld",
+          (long long)k);
+  GUARD_BEGIN
+  CU(cudaStreamSynchronize(net->stream));
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  const int64_t T = net->ts;                  // spikes from this step on use the new delays
+  const int pj = sy.proj;
+  // the projection as built keeps delivering the spikes sent before step T
+  Proj old = net->projs[pj];
+  old.dev.src_hi = std::min(old.dev.src_hi, T);
+  old.retire_after = T - 1 + old.dmax;
+  // the new delays, and the projection rebuilt from its members
+  sy.delay.assign(delay_steps, delay_steps + n);
+  sy.dmin = n ? *std::min_element(sy.delay.begin(), sy.delay.end()) : sy.delay_scalar;
+  sy.dmax = n ? *std::max_element(sy.delay.begin(), sy.delay.end()) : sy.delay_scalar;
+  {
+    Proj& pr = net->projs[pj];
+    pr.allocs.clear();
+    pr.dev = ProjDev{};
+    pr.off = nullptr;
+    pr.post = nullptr;
+    pr.w = nullptr;
+    pr.n_syn = 0;
+    pr.max_bundle = 0;
+    pr.dmin = INT32_MAX;
+    pr.dmax = 0;
+    for (int m : pr.members) {
+      pr.dmin = std::min(pr.dmin, net->syns[m].dmin);
+      pr.dmax = std::max(pr.dmax, net->syns[m].dmax);
+    }
+    Pop& src = net->pops[pr.src_pop];
+    if (pr.dmax + 2 > src.dev.ring_len) {
+      if (b2b_status st = grow_ring(net, pr.src_pop, pr.dmax + 2)) return st;
+      old.dev.src_ring_idx = src.dev.ring_idx;
+      old.dev.src_ring_cnt = src.dev.ring_cnt;
+      old.dev.src_ring_len = src.dev.ring_len;
+    }
+    if (b2b_status st = build_proj(net, pj)) return st;
+    net->projs[pj].dev.src_lo = T;
+  }
+  if (old.dev.src_lo < old.dev.src_hi && old.retire_after >= T) {
+    net->projs.push_back(std::move(old));
+  } else {
+    for (void* a : old.allocs) cudaFree(a);
+  }
+  build_add_batches(net);
+  refresh_two_launch(net);
   return B2B_OK;
   GUARD_END
 }

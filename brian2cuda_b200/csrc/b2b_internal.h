@@ -124,6 +124,11 @@ struct ProjDev {
   int64_t src_n;                  // ring row stride (padded source population size)
   int32_t src_ring_len;
   int32_t dmin, nd;               // delays dmin .. dmin+nd-1
+  // source steps whose spikes this projection delivers: [src_lo, src_hi).  After a change
+  // of delays between runs, the projection as built before delivers the spikes sent before
+  // the change (src_hi = the first step after it) and the rebuilt one the later spikes.
+  int64_t src_lo = 0;
+  int64_t src_hi = INT64_MAX;
   int32_t chunks;                 // work items per bundle = ceil(max bundle / kChunk)
   const int64_t* off;             // [n_src*nd + 1] bundle offsets, key = pre*nd + (d-dmin)
   const int32_t* post;            // [n_syn] target index in the target population
@@ -309,6 +314,10 @@ struct Proj {
   void* w = nullptr;
   std::vector<void*> allocs;
   int32_t* rec_buf = nullptr;                // STDP: record of each synapse, post-grouped order
+  // A projection retired by b2b_syn_set_delays: it only delivers the spikes sent before the
+  // change (dev.src_hi) and is dropped once the last of them has arrived (after this step).
+  // Retired projections follow the live ones in b2b_net::projs and belong to no Synapses.
+  int64_t retire_after = -1;
 };
 
 }  // namespace b2b

@@ -36,13 +36,24 @@ struct DuePrefix {
   int incl0, incl1, total;
 };
 
+// Whether the spikes of source step ts - d are delivered: the step exists (>= 0) and lies
+// in the projection's source window [lo, hi) (a projection whose delays changed between runs
+// delivers the spikes sent before the change through its old bundles, and the later ones
+// through its new bundles).
+__device__ __forceinline__ bool in_window(int64_t ts, int d, int64_t lo, int64_t hi) {
+  const int64_t s = ts - d;
+  return s >= 0 && s >= lo && s < hi;
+}
+
 __device__ __forceinline__ DuePrefix due_prefix_warp(const int32_t* __restrict__ ring_cnt,
-                                                     int ring_len, int64_t ts, int dmin, int nd) {
+                                                     int ring_len, int64_t ts, int dmin, int nd,
+                                                     int64_t lo, int64_t hi) {
   const int lane = threadIdx.x & 31;
   const int base = ring_slot(ts, ring_len);
   int c0 = 0, c1 = 0;
-  if (lane < nd && ts - (dmin + lane) >= 0) c0 = ring_cnt[ring_back(base, dmin + lane, ring_len)];
-  if (32 + lane < nd && ts - (dmin + 32 + lane) >= 0)
+  if (lane < nd && in_window(ts, dmin + lane, lo, hi))
+    c0 = ring_cnt[ring_back(base, dmin + lane, ring_len)];
+  if (32 + lane < nd && in_window(ts, dmin + 32 + lane, lo, hi))
     c1 = ring_cnt[ring_back(base, dmin + 32 + lane, ring_len)];
   DuePrefix p;
   p.incl0 = warp_incl_scan(c0);
@@ -68,10 +79,11 @@ __device__ __forceinline__ int find_delay_warp(const DuePrefix& p, int sp, int* 
 // indices < i.  Every thread of the CTA must call this.
 __device__ __forceinline__ int due_prefix_block(const int32_t* __restrict__ ring_cnt,
                                                 int ring_len, int64_t ts, int dmin, int nd,
-                                                int* s_pref) {
+                                                int64_t lo, int64_t hi, int* s_pref) {
   const int base = ring_slot(ts, ring_len);
   for (int di = threadIdx.x; di < nd; di += blockDim.x)
-    s_pref[di + 1] = ts - (dmin + di) >= 0 ? ring_cnt[ring_back(base, dmin + di, ring_len)] : 0;
+    s_pref[di + 1] = in_window(ts, dmin + di, lo, hi)
+                         ? ring_cnt[ring_back(base, dmin + di, ring_len)] : 0;
   if (threadIdx.x == 0) s_pref[0] = 0;
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -116,10 +128,12 @@ __device__ __forceinline__ void for_each_due_item(const ProjDev& J, int64_t ts, 
   DuePrefix wp{};
   int nspk;
   if constexpr (WARP_PREFIX) {
-    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd);
+    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, J.src_lo,
+                         J.src_hi);
     nspk = wp.total;
   } else {
-    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, s_pref);
+    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, J.src_lo,
+                            J.src_hi, s_pref);
   }
   const int64_t items = (int64_t)nspk * J.chunks;
   const int base = ring_slot(ts, J.src_ring_len);

@@ -61,10 +61,12 @@ __device__ __forceinline__ void small_deliver(const ProjDev& J, int64_t ts, int*
   DuePrefix wp{};
   int nspk;
   if constexpr (WP) {
-    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd);
+    wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, J.src_lo,
+                         J.src_hi);
     nspk = wp.total;
   } else {
-    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, s_pref);
+    nspk = due_prefix_block(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd, J.src_lo,
+                            J.src_hi, s_pref);
   }
   const int sub = J.chunks * (kChunk / 32);
   const int64_t items = (int64_t)nspk * sub;

@@ -349,6 +349,13 @@ class Network:
         self._check(self._lib.b2b_out_degree(self._h, gid, _ptr(a), n), "out_degree")
         return a
 
+    def syn_set_delays(self, sid: int, delay_steps) -> None:
+        """Brian2's `S.delay = ...` between runs: new per-synapse delays (steps, in the order
+        the synapses were given); spikes already sent keep the delay they were sent with."""
+        d = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        self._check(self._lib.b2b_syn_set_delays(self._h, sid, _ptr(d), len(d)),
+                    "syn_set_delays")
+
     def syn_count(self, sid: int) -> int:
         n = C.c_int64()
         self._check(self._lib.b2b_syn_count(self._h, sid, C.byref(n)), "syn_count")

@@ -312,6 +312,16 @@ enum {
   B2B_SYN_APOST = 5, B2B_SYN_LASTUPDATE = 6
 };
 b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n);
+/* New per-synapse delays (steps, in the order the synapses were given) of additive Synapses
+ * object sid between runs (Brian2's `S.delay = ...` before another run()).  As in Brian2,
+ * spikes already sent keep the delay they were sent with and spikes from the next step on
+ * use the new ones (brian2cuda/tests/test_network_multiple_runs.py:110-156): the projection
+ * as built stays, delivering only spikes of earlier steps, until its last one has arrived;
+ * the rebuilt one delivers the later spikes.  A population's spike-history ring grows when
+ * the new delays need it (snapshots taken before become unusable).  Not for connectivity
+ * generated on the GPU, STDP synapses or the one-CTA small form (B2B_ERR_UNSUPPORTED). */
+b2b_status b2b_syn_set_delays(b2b_net* net, int32_t sid, const int32_t* delay_steps,
+                              int64_t n);
 /* Reads a synapse variable in the order the synapses were given (after b2b_finalize). */
 b2b_status b2b_syn_get(b2b_net* net, int32_t sid, int32_t var, void* host, int64_t n);
 

@@ -181,6 +181,8 @@ struct Syn {
   std::vector<std::vector<int64_t>> queue;  // slot -> bundle ids (key = pre*(D+1)+delay)
   // on_post (delay 0): synapses by post
   std::vector<int64_t> post_off, post_syn;
+  // deliveries still due from before a change of delays: (step, synapse)
+  std::vector<std::pair<int64_t, int64_t>> legacy;
 };
 
 // StateMonitor (brian2cuda/templates/statemonitor.cu: one value per recorded index per tick
@@ -451,6 +453,14 @@ void pathway_pre(Net<R>& net, Syn<R>& s, double t) {
   const R taupre = (R)s.stdp[0], taupost = (R)s.stdp[1], dApre = (R)s.stdp[2];
   const R wmin = (R)s.stdp[4], wmax = (R)s.stdp[5];
   const bool adds = s.stdp[6] != 0;
+  if (!s.legacy.empty()) {
+    // spikes sent before a change of delays arrive with the delay they were sent with
+    for (const auto& e : s.legacy)
+      if (e.first == net.ts) T[s.j[e.second]] += s.has_w ? s.w[e.second] : s.w_scalar;
+    s.legacy.erase(std::remove_if(s.legacy.begin(), s.legacy.end(),
+                                  [&](const auto& e) { return e.first <= net.ts; }),
+                   s.legacy.end());
+  }
   for (int64_t key : s.queue[s.current_offset]) {
     for (int64_t q = s.bundle_off[key]; q < s.bundle_off[key + 1]; ++q) {
       const int64_t k = s.bundle_syn[q];
@@ -997,6 +1007,33 @@ int api_normals(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n)
   return 0;
 }
 
+// New delays of an additive Synapses object between runs: the bundles still in its queue
+// become explicit (step, synapse) deliveries with their old delays, and the bundle tables
+// and the queue are rebuilt for the new delays (the reference's queue keeps what it holds
+// and pushes later spikes with the new delays, brian2cuda/brianlib/spikequeue.h:98-201).
+template <typename R>
+int api_syn_set_delays(Net<R>& net, int sid, const int32_t* d, int64_t n) {
+  if (sid < 0 || sid >= (int)net.syns.size()) return -1;
+  ensure_built(net);
+  Syn<R>& s = net.syns[sid];
+  if (n != s.n || s.effect != ADD) return -1;
+  const int nq = s.num_queues;
+  for (int o = 1; o < nq; ++o) {
+    // slot current_offset + o holds the bundles due o steps after the last simulated step
+    for (int64_t key : s.queue[(s.current_offset + o) % nq])
+      for (int64_t q = s.bundle_off[key]; q < s.bundle_off[key + 1]; ++q)
+        s.legacy.emplace_back(net.ts - 1 + o, s.bundle_syn[q]);
+  }
+  s.delay.assign(d, d + n);
+  s.max_delay = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    if (d[k] < 0) return -1;
+    s.max_delay = std::max(s.max_delay, d[k]);
+  }
+  build_syn(net, s);
+  return 0;
+}
+
 template <typename R>
 int api_uniforms(Net<R>& net, int gid, const double* u, int64_t steps, int64_t n) {
   if (gid < 0 || gid >= (int)net.groups.size()) return -1;
@@ -1285,6 +1322,10 @@ void orc_clear_spikes(void* hp) {
   Handle* h = static_cast<Handle*>(hp);
   if (h->f32) { for (auto& g : h->nf.groups) g.recorded.clear(); }
   else { for (auto& g : h->nd.groups) g.recorded.clear(); }
+}
+int orc_syn_set_delays(void* hp, int sid, const int32_t* d, int64_t n) {
+  Handle* h = static_cast<Handle*>(hp);
+  return DISPATCH(h, api_syn_set_delays, sid, d, n);
 }
 int orc_store(void* hp) {
   Handle* h = static_cast<Handle*>(hp);

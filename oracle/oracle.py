@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
             "orc_set_uniforms": (C.c_int, [P, C.c_int, P, I64, I64]),
             "orc_run": (C.c_int, [P, I64]),
             "orc_store": (C.c_int, [P]),
+            "orc_syn_set_delays": (C.c_int, [P, C.c_int, P, I64]),
             "orc_clear_spikes": (None, [P]),
             "orc_restore": (C.c_int, [P]),
             "orc_timestep": (I64, [P]),
@@ -225,6 +226,12 @@ class OracleNet:
                                                       VARS[target], float(p), int(dmin),
                                                       int(dmax), float(w), int(seed)),
                         "synapses_random")
+
+    def syn_set_delays(self, sid, delay_steps):
+        """New delays (steps) of an additive Synapses object between runs; spikes already
+        sent keep theirs."""
+        d = np.ascontiguousarray(delay_steps, dtype=np.int32)
+        self._ok(self._lib.orc_syn_set_delays(self._h, sid, _p(d), len(d)), "syn_set_delays")
 
     def syn_count(self, sid):
         return self._ok(self._lib.orc_syn_count(self._h, sid), "syn_count")

@@ -367,6 +367,47 @@ def multiple_runs_heterogeneous_delay(make):
     np.testing.assert_array_equal(vals[:, 1], [0, 0, 1, 2])
 
 
+def _delay_change(make, n_post, before, after):
+    """An always-spiking input, `v += 1` onto n_post neurons with delays `before` (steps);
+    one step run, delays changed to `after`, five more steps; v at the start of each step."""
+    net = make(DT)
+    inG = net.lif_group(1, LIF(taum=math.inf, Vt=-math.inf, has_reset=False), "float64")
+    G = net.lif_group(n_post, LIF(taum=math.inf, has_threshold=False, has_reset=False),
+                      "float64")
+    S = net.synapses(inG, G, "v", [0] * n_post, list(range(n_post)), w_scalar=1.0,
+                     delay=np.array(before, np.int32))
+    mon = net.state_monitor(G, "v", capacity=6)
+    net.finalize()
+    net.run(1)
+    net.syn_set_delays(S, np.array(after, np.int32))
+    net.run(5)
+    steps, vals = net.state_values(mon)
+    np.testing.assert_array_equal(steps, [0, 1, 2, 3, 4, 5])
+    return vals
+
+
+def increasing_delay_scalar(make):
+    """test_network_multiple_runs.py:36-57 (expected to fail on the reference's CUDA device,
+    issue #302): delay dt, then 2 dt; the spike in flight keeps dt: [0, 0, 1, 1, 2, 3]."""
+    np.testing.assert_array_equal(_delay_change(make, 1, [1], [2])[:, 0], [0, 0, 1, 1, 2, 3])
+
+
+def increasing_delay_heterogeneous(make):
+    """test_network_multiple_runs.py:110-131: delays j*dt, then 2*j*dt, onto two neurons:
+    [0, 1, 2, 3, 4, 5] and [0, 0, 1, 1, 2, 3]."""
+    vals = _delay_change(make, 2, [0, 1], [0, 2])
+    np.testing.assert_array_equal(vals[:, 0], [0, 1, 2, 3, 4, 5])
+    np.testing.assert_array_equal(vals[:, 1], [0, 0, 1, 1, 2, 3])
+
+
+def reducing_delay_heterogeneous(make):
+    """test_network_multiple_runs.py:134-156: delays 2*j*dt, then j*dt: [0, 1, 2, 3, 4, 5]
+    and [0, 0, 0, 2, 3, 4] (the spike in flight and the first new one arrive together)."""
+    vals = _delay_change(make, 2, [0, 2], [0, 1])
+    np.testing.assert_array_equal(vals[:, 0], [0, 1, 2, 3, 4, 5])
+    np.testing.assert_array_equal(vals[:, 1], [0, 0, 0, 2, 3, 4])
+
+
 def time_after_run(make):
     """test_cuda_standalone.py:139-167: t is 0 before a run, 10 ms after run(10 ms) and
     20 ms after a second one (dt = 0.1 ms)."""
@@ -388,4 +429,5 @@ ALL = [example_run, push_outer_loop, push_outer_loop2, circular_eventspaces,
        state_monitor_more_threads_than_single_block, spike_monitor_all_attr,
        binomial_values_seeds, threads_per_synapse_bundle, synaptic_effects_onto_one_target,
        poisson_input_schedule, refractory_without_spikes, multiple_runs_heterogeneous_delay,
-       time_after_run]
+       increasing_delay_scalar, increasing_delay_heterogeneous,
+       reducing_delay_heterogeneous, time_after_run]

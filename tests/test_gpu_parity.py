@@ -164,6 +164,38 @@ def test_merged_synapses_onto_two_variables_of_few_targets(gpu_factory, oracle_f
         _close(out["gpu"][v], out["orc"][v], 1e-10, 1e-15)
 
 
+def test_delays_changed_between_runs_match_oracle(gpu_factory, oracle_factory):
+    """Delays changed between runs while spikes are in flight (Brian2's `S.delay = ...`):
+    first longer than the spike-history ring holds (the ring grows), then with delays of 0
+    (the net leaves the two-launch form for the per-step kernels); spikes exact, v within
+    1e-10, synapse delays read back in input order."""
+    rng = np.random.default_rng(21)
+    out = {}
+    for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
+        net = make(DT)
+        G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=800)
+        net.finalize()
+        if name == "gpu":
+            assert net.run_mode == "fused"
+        net.run(100)
+        d1 = np.random.default_rng(5).integers(1, 41, size=int(exc.sum())).astype(np.int32)
+        net.syn_set_delays(Ce, d1)
+        net.run(150)
+        d2 = np.random.default_rng(6).integers(0, 6, size=int((~exc).sum())).astype(np.int32)
+        net.syn_set_delays(Ci, d2)
+        net.run(120)
+        if name == "gpu":
+            assert net.run_mode == "per-step"
+            np.testing.assert_array_equal(net.syn_get(Ce, "delay"), d1)
+            np.testing.assert_array_equal(net.syn_get(Ci, "delay"), d2)
+        idx, st = net.spikes(G)
+        out[name] = (idx, st, net.get_state(G, "v"))
+    assert len(out["gpu"][0]) > 300 and rng is not None
+    np.testing.assert_array_equal(out["gpu"][1], out["orc"][1])
+    np.testing.assert_array_equal(out["gpu"][0], out["orc"][0])
+    _close(out["gpu"][2], out["orc"][2], 1e-10, 1e-15)
+
+
 def test_synapse_readback_in_input_order(gpu_factory):
     net = gpu_factory(DT)
     G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=300)
