@@ -267,7 +267,7 @@ def main():
     ap.add_argument("--ncu-case", type=int, default=0, metavar="STEPS",
                     help="profiling case: build the workload, simulate STEPS steps, print "
                          "nothing (for ncu captures of the step kernels)")
-    ap.add_argument("--fused", action="store_true",
+    ap.add_argument("--two-launch", action="store_true",
                     help="run every step as two concurrent launches (neuron update, delivery "
                          "of earlier spikes) where the net allows it")
     ap.add_argument("--per-step", action="store_true",
@@ -348,7 +348,7 @@ def bench_cobahh(args, world, rank, local):
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
                   stream=stream.cuda_stream,
-                  fused=True if args.fused else (False if args.per_step else None))
+                  two_launch=True if args.two_launch else (False if args.per_step else None))
     t_setup = time.perf_counter()
     ids = models.build_cobahh(net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
                               monitor_capacity=mon_cap)
@@ -450,7 +450,7 @@ def bench_cobahh(args, world, rank, local):
     nd = DMAX - DMIN + 1
     deliver_bytes = (BYTES_EVENT * p_ev + BYTES_BUNDLE * nd * float(len(pidx))) / SIM_STEPS
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
-    two_launch = net.run_mode == "fused"
+    two_launch = net.run_mode == "two-launch"
     if two_launch:
         # the update also adds in and clears the pending input of ge and gi
         neuron_bytes += BYTES_NEURON_FOLD * N_NEURONS

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     8: "B2B_ERR_INDEX",
 }
 F32, F64 = 1, 2
-NET_NO_GRAPH, NET_CHECKED, NET_RESET_BEFORE_SYNAPSES, NET_FUSED, NET_SMALL = 1, 2, 4, 8, 16
+NET_NO_GRAPH, NET_CHECKED, NET_RESET_BEFORE_SYNAPSES, NET_TWO_LAUNCH, NET_SMALL = 1, 2, 4, 8, 16
 NET_PER_STEP = 32
 EFFECT_ADD, EFFECT_STDP = 1, 2
 VARS = {"v": 0, "ge": 1, "gi": 2, "m": 3, "h": 4, "n": 5, "lastspike": 6,

@@ -741,7 +741,7 @@ b2b_status setup_monitors(b2b_net* net) {
 // CTA: one LIF/HH population of at most 4096 neurons (no gating surrogate) whose Synapses
 // objects are all additive and target it, with the state fitting the CTA's shared memory.
 b2b_status setup_small(b2b_net* net) {
-  if (!(net->cfg.flags & B2B_NET_SMALL) || (net->cfg.flags & (B2B_NET_CHECKED | B2B_NET_FUSED)))
+  if (!(net->cfg.flags & B2B_NET_SMALL) || (net->cfg.flags & (B2B_NET_CHECKED | B2B_NET_TWO_LAUNCH)))
     return B2B_OK;
   if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.size() > kMaxProjBatch) return B2B_OK;
@@ -787,7 +787,7 @@ constexpr int64_t kAutoTwoLaunchMaxNeurons = 1 << 18;
 b2b_status setup_two_launch(b2b_net* net) {
   const int32_t flags = net->cfg.flags;
   if (flags & (B2B_NET_PER_STEP | B2B_NET_SMALL)) return B2B_OK;
-  if ((flags & B2B_NET_CHECKED) && !(flags & B2B_NET_FUSED)) return B2B_OK;
+  if ((flags & B2B_NET_CHECKED) && !(flags & B2B_NET_TWO_LAUNCH)) return B2B_OK;
   if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
     return B2B_OK;
@@ -836,7 +836,7 @@ b2b_status setup_two_launch(b2b_net* net) {
   CU(cudaEventCreateWithFlags(&net->ev_d[0], cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&net->ev_d[1], cudaEventDisableTiming));
   net->two_launch_ok = true;
-  net->two_launch = (flags & B2B_NET_FUSED) || pop.n <= kAutoTwoLaunchMaxNeurons;
+  net->two_launch = (flags & B2B_NET_TWO_LAUNCH) || pop.n <= kAutoTwoLaunchMaxNeurons;
   return B2B_OK;
 }
 

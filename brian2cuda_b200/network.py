@@ -163,9 +163,10 @@ class Network:
 
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
-                 stream: int | None = None, fused: bool | None = None, small: bool = False):
+                 stream: int | None = None, two_launch: bool | None = None,
+                 small: bool = False):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
-        default the network creates its own non-blocking stream.  `fused`: True runs every
+        default the network creates its own non-blocking stream.  `two_launch`: True runs every
         step as two concurrent launches (the neuron update, and the delivery of earlier
         steps' spikes into a double-buffered input) where the net allows it, False always
         the per-step kernels, None (default) the two launches for nets that allow them with at
@@ -178,9 +179,9 @@ class Network:
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
         if reset_before_synapses:
             flags |= N.NET_RESET_BEFORE_SYNAPSES
-        if fused is True:
-            flags |= N.NET_FUSED
-        elif fused is False:
+        if two_launch is True:
+            flags |= N.NET_TWO_LAUNCH
+        elif two_launch is False:
             flags |= N.NET_PER_STEP
         if small:
             flags |= N.NET_SMALL
@@ -454,11 +455,11 @@ class Network:
 
     @property
     def run_mode(self) -> str:
-        """'fused' (two concurrent launches per step), 'small' (one CTA runs every step of a
-        chunk) or 'per-step' (graph-replayed kernels)."""
+        """'two-launch' (two concurrent launches per step), 'small' (one CTA runs every step
+        of a chunk) or 'per-step' (graph-replayed kernels)."""
         m = C.c_int32()
         self._check(self._lib.b2b_run_mode(self._h, C.byref(m)), "run_mode")
-        return {1: "fused", 2: "small"}.get(m.value, "per-step")
+        return {1: "two-launch", 2: "small"}.get(m.value, "per-step")
 
     @property
     def kernel_launches(self) -> int:

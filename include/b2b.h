@@ -56,13 +56,13 @@ enum { B2B_F32 = 1, B2B_F64 = 2 };
 enum {
   B2B_NET_NO_GRAPH = 1,   /* launch every step eagerly instead of replaying CUDA graphs */
   B2B_NET_CHECKED = 2,    /* every launch site a kernel of its own (no one-CTA small form,
-                             no two-launch form unless B2B_NET_FUSED is also set), so a
+                             no two-launch form unless B2B_NET_TWO_LAUNCH is also set), so a
                              fault or a device status names one launch; input indices are
                              checked on the host in every mode (B2B_ERR_INDEX)           */
   B2B_NET_RESET_BEFORE_SYNAPSES = 4, /* schedule start, groups, thresholds, resets, synapses,
                                         end (Brian2 prefs core.network.default_schedule);
                                         default: resets after synapses                   */
-  B2B_NET_FUSED = 8,      /* run every step as two concurrent launches (neuron update, and
+  B2B_NET_TWO_LAUNCH = 8,      /* run every step as two concurrent launches (neuron update, and
                              the delivery of spikes of earlier steps into a double-buffered
                              input) whenever the net allows it: one LIF/HH population, additive
                              synapses onto ge/gi only, all delays >= 1 step, no state or rate
@@ -352,7 +352,7 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
 b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
 /* How b2b_run advances the net (after b2b_finalize): *mode = 1 for every step as two
- * concurrent launches (B2B_NET_FUSED, or chosen automatically), 2 for a small network run by
+ * concurrent launches (B2B_NET_TWO_LAUNCH, or chosen automatically), 2 for a small network run by
  * one CTA per chunk of steps, 0 for per-step kernels replayed from CUDA graphs. */
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,

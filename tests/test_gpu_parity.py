@@ -176,7 +176,7 @@ def test_delays_changed_between_runs_match_oracle(gpu_factory, oracle_factory):
         G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=800)
         net.finalize()
         if name == "gpu":
-            assert net.run_mode == "fused"
+            assert net.run_mode == "two-launch"
         net.run(100)
         d1 = np.random.default_rng(5).integers(1, 41, size=int(exc.sum())).astype(np.int32)
         net.syn_set_delays(Ce, d1)
@@ -424,17 +424,17 @@ def test_store_restore_replays_identically(gpu_factory):
     assert len(idx1) > 50
 
 
-def test_fused_and_per_step_paths_agree(gpu_factory):
+def test_two_launch_and_per_step_paths_agree(gpu_factory):
     res = {}
-    for fused in (True, False):
-        net = gpu_factory(DT, fused=fused)
+    for two_launch in (True, False):
+        net = gpu_factory(DT, two_launch=two_launch)
         G, Ce, Ci, _ = _delay_net(net, n=1000)
         net.finalize()
-        assert net.run_mode == ("fused" if fused else "per-step")
+        assert net.run_mode == ("two-launch" if two_launch else "per-step")
         net.run(150)
         net.run(89)
         idx, st = net.spikes(G)
-        res[fused] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
+        res[two_launch] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
     for k in (0, 1, 4):
         np.testing.assert_array_equal(res[True][k], res[False][k])
     _close(res[True][2], res[False][2], 1e-10, 1e-15)
@@ -444,10 +444,10 @@ def test_fused_and_per_step_paths_agree(gpu_factory):
 def test_profile_advances_like_run(gpu_factory):
     """The profiling run launches every kernel eagerly and times it; in either form of the
     step it reports the form's launch sites and leaves the net where b2b_run would."""
-    for fused in (True, False):
+    for two_launch in (True, False):
         out = {}
         for how in ("run", "profile"):
-            net = gpu_factory(DT, fused=fused)
+            net = gpu_factory(DT, two_launch=two_launch)
             G, Ce, Ci, _ = _delay_net(net, n=1000)
             net.finalize()
             net.run(40)
@@ -458,7 +458,7 @@ def test_profile_advances_like_run(gpu_factory):
                 kinds = [k for k, _ in prof]
                 # per-step: Ce (a weight per synapse) and Ci (one scalar weight) are two
                 # kernel variants, so two delivery launches
-                assert kinds == ([5, 1] if fused else [1, 6, 6]), kinds
+                assert kinds == ([5, 1] if two_launch else [1, 6, 6]), kinds
                 assert all(ms > 0 for _, ms in prof)
             assert net.timestep == 170
             net.run(30)
@@ -476,10 +476,10 @@ def test_profile_graph_advances_like_run(gpu_factory):
     the net where b2b_run would, and the per-site times fit inside the step: in the per-step
     form the sites run one after another, so their sum is at most the step time; in the
     two-launch form each of the two overlapping sites is."""
-    for fused in (True, False):
+    for two_launch in (True, False):
         out = {}
         for how in ("run", "profile"):
-            net = gpu_factory(DT, fused=fused, steps_per_graph=25)
+            net = gpu_factory(DT, two_launch=two_launch, steps_per_graph=25)
             G, Ce, Ci, _ = _delay_net(net, n=1000)
             net.finalize()
             net.run(40)
@@ -488,9 +488,9 @@ def test_profile_graph_advances_like_run(gpu_factory):
             else:
                 prof, step_ms = net.profile_graph(150)
                 kinds = [k for k, _ in prof]
-                assert kinds == ([5, 1] if fused else [1, 6, 6]), kinds
+                assert kinds == ([5, 1] if two_launch else [1, 6, 6]), kinds
                 assert all(ms > 0 for _, ms in prof) and step_ms > 0
-                if fused:
+                if two_launch:
                     assert max(ms for _, ms in prof) <= step_ms
                 else:
                     assert sum(ms for _, ms in prof) <= step_ms
@@ -512,14 +512,14 @@ def _spikes_within_one_step(a_idx, a_stp, b_idx, b_stp):
     return hit / max(1, len(a_idx))
 
 
-def test_fused_cobahh_float32_matches_oracle(gpu_factory, oracle_factory):
+def test_two_launch_cobahh_float32_matches_oracle(gpu_factory, oracle_factory):
     out = {}
     for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
-        net = make(DT, f32=True) if name == "orc" else make(DT, fused=True)
+        net = make(DT, f32=True) if name == "orc" else make(DT, two_launch=True)
         ids = models.build_cobahh(net, n=3000, p=0.02, generated=False, monitor_capacity=10**6)
         net.finalize()
         if name == "gpu":
-            assert net.run_mode == "fused"
+            assert net.run_mode == "two-launch"
         net.run(60)
         out[name] = (net.spikes(ids["P"]), {v: net.get_state(ids["P"], v)
                                             for v in ("v", "m", "h", "n", "ge", "gi")})
@@ -585,7 +585,7 @@ def test_autotune_chooses_step_form(gpu_factory):
         net = gpu_factory(DT)
         G, Ce, Ci, _ = _delay_net(net, n=800)
         net.finalize()
-        assert net.run_mode == "fused"   # <= 2^18 neurons: the two launches until tuned
+        assert net.run_mode == "two-launch"   # <= 2^18 neurons: the two launches until tuned
         net.run(60)
         v0 = net.get_state(G, "v").copy()
         if mode == "tuned":
@@ -593,13 +593,13 @@ def test_autotune_chooses_step_form(gpu_factory):
             kinds = [r["site_kind"] for r in res]
             assert {1, 6, 5, 11} <= set(kinds), kinds
             form = [r for r in res if r["site_kind"] == 11][0]
-            assert net.run_mode == ("fused" if form["choice_a"] == 1 else "per-step")
+            assert net.run_mode == ("two-launch" if form["choice_a"] == 1 else "per-step")
             np.testing.assert_array_equal(net.get_state(G, "v"), v0)
             assert net.timestep == 60
         elif mode != "untuned":
             net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_b": 0,
                              "choice_a": 1 if mode == "two launches" else 0}])
-            assert net.run_mode == ("fused" if mode == "two launches" else "per-step")
+            assert net.run_mode == ("two-launch" if mode == "two launches" else "per-step")
         net.run(240)
         idx, st = net.spikes(G)
         out[mode] = (idx, st, net.get_state(G, "v"))
@@ -627,7 +627,7 @@ def test_small_network_path_matches_per_step(gpu_factory, case):
     target variable is equal, so the order of the additions cannot change a sum)."""
     out = {}
     for small in (True, False):
-        net = gpu_factory(DT, small=small, fused=None if small else False)
+        net = gpu_factory(DT, small=small, two_launch=None if small else False)
         if case == "cobahh_delays":
             ids = models.build_cobahh(net, n=3000, p=0.05, monitor_capacity=10**6)
             G, steps = ids["P"], 300

@@ -100,11 +100,11 @@ def test_lif_poisson_input_matches_oracle(gpu_factory, oracle_factory, form):
             net = oracle_factory(DT, seed=9, reset_before_synapses=rf)
         else:
             net = gpu_factory(DT, seed=9, reset_before_synapses=rf,
-                              fused=True if form == "two launches" else False)
+                              two_launch=True if form == "two launches" else False)
         G = _lif_net_with_inputs(net)
         net.finalize()
         if name == "gpu":
-            assert net.run_mode == ("fused" if form == "two launches" else "per-step")
+            assert net.run_mode == ("two-launch" if form == "two launches" else "per-step")
         net.run(150)
         net.run(100)
         idx, st = net.spikes(G)

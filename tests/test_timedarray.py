@@ -116,12 +116,12 @@ def test_lif_timedarray_matches_oracle(gpu_factory, oracle_factory, form):
         if name == "orc":
             net = oracle_factory(DT)
         else:
-            net = gpu_factory(DT, fused={"per-step": False, "two launches": True}.get(form),
+            net = gpu_factory(DT, two_launch={"per-step": False, "two launches": True}.get(form),
                               small=form == "small")
         G = _lif_net_with_drive(net)
         net.finalize()
         if name == "gpu":
-            assert net.run_mode == {"per-step": "per-step", "two launches": "fused",
+            assert net.run_mode == {"per-step": "per-step", "two launches": "two-launch",
                                     "small": "small"}[form]
         net.run(120)
         net.run(80)
