@@ -282,7 +282,7 @@ def main():
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
                     choices=["hh4m", "surrogate1m", "mlp_train", "propagation",
-                             "propagation3000", "stdp", "stdp_synorder", "hines"],
+                             "propagation3000", "stdp", "stdp_synorder", "hines", "model"],
                     help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
     if args.kernel_case:
@@ -1064,7 +1064,8 @@ def kernel_case(name: str):
     then 20 profiled ones (deliver_add_batch_kernel, 6e6 / 6e7 events per step), stdp /
     stdp_synorder = the STDP workload with its records grouped by postsynaptic neuron / in
     synapse order, 200 steps then 20 profiled ones (deliver_stdp_post_kernel), hines = the
-    1024-neuron multicompartment batch for one 1000-step launch (hines_kernel)."""
+    1024-neuron multicompartment batch for one 1000-step launch (hines_kernel), model = a
+    generated model (noisy adaptive LIF, 8e6 neurons, 20 steps: model_step_kernel)."""
     import torch
 
     from brian2cuda_b200 import Network, models
@@ -1104,6 +1105,24 @@ def kernel_case(name: str):
         net.finalize()
         net.run(2 * DMAX)       # 100 delivery launches before the profiled ones
         net.profile(20)
+        net.sync()
+        net.close()
+    elif name == "model":
+        # a generated model (noisy adaptive LIF, Euler-Maruyama with one cuRAND normal per
+        # neuron and step), 8e6 neurons, float32 (17 B per neuron and step: above the L2):
+        # 20 launches of model_step_kernel
+        from brian2cuda_b200.lowering import Script
+        s = Script(dt=DT, seed=4, dtype="float32",
+                   namespace=dict(tau=10e-3, tauw=100e-3, a=0.5, sigma=2e-3, El=-70e-3,
+                                  Vt=-50e-3, Vr=-65e-3, b=1e-3, I0=22e-3))
+        G = s.NeuronGroup(8_000_000, """dv/dt = (El - v - w + I0) / tau + sigma * xi * tau**-0.5
+                                        : volt
+                                        dw/dt = (a * (v - El) - w) / tauw : volt""",
+                          threshold="v > Vt", reset="v = Vr; w += b", refractory=2e-3)
+        G.v = "El + rand()*20*mV"
+        net = Network(DT, seed=4, graphs=False)
+        s.lower().build(net)
+        net.run(20)
         net.sync()
         net.close()
     elif name == "mlp_train":
