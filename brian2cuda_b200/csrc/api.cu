@@ -558,6 +558,9 @@ b2b_status build_proj(b2b_net* net, int pj) {
   int64_t n_dst_valid = 0;
   for (int gi : dst.groups) n_dst_valid += net->groups[gi].n;
   D.aggregate = n_dst_valid < 64 ? 1 : 0;
+  pr.var_mask = 0;
+  for (int m : pr.members) pr.var_mask |= (uint8_t)(1u << net->syns[m].target_var);
+  pr.dst_n = dst.n;
   if (pr.effect == B2B_EFFECT_STDP) {
     const b2b_stdp_params& sp = net->syns[pr.members[0]].stdp;
     CHECK(pr.n_syn < (1ll << 31), B2B_ERR_UNSUPPORTED, "STDP projection above 2^31 synapses");
@@ -2102,6 +2105,26 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
+  // additive delivery launches that can accumulate in thread-block clusters (float32, one
+  // target population): with the chosen lanes per item, cluster accumulation on or off
+  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
+    const auto& bat = net->add_batches[b];
+    if (!add_batch_cluster_capable(bat.data(), (int)bat.size())) continue;
+    AddTune& t = net->add_tune[b];
+    b2b_tune_result r{12, (int32_t)b, 0, 0, 0.0, 0.0};
+    double off_ms = 0, on_ms = 0;
+    t.cluster = 0;
+    st = trial(&off_ms);
+    if (st != B2B_OK) break;
+    t.cluster = 1;
+    st = trial(&on_ms);
+    const bool use = st == B2B_OK && on_ms < kTuneMargin * off_ms;
+    t.cluster = use ? 1 : 0;
+    r.choice_a = t.cluster;
+    r.default_ms = off_ms;
+    r.best_ms = use ? on_ms : off_ms;
+    res.push_back(r);
+  }
   if (net->two_launch_ok && st == B2B_OK) {
     const double per_step_ms = res.empty() ? 1e30 : res.back().best_ms;
     net->two_launch = true;
@@ -2203,6 +2226,15 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       net->add_tune[t.site_index].group = t.choice_a;
       net->add_tune[t.site_index].grid = t.choice_b;
+    } else if (t.site_kind == 12) {
+      CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->add_batches.size() &&
+                (t.choice_a == 0 || t.choice_a == 1),
+            B2B_ERR_INVALID_ARG, "bad cluster choice for delivery launch %d", t.site_index);
+      const auto& bat = net->add_batches[t.site_index];
+      CHECK(t.choice_a == 0 || add_batch_cluster_capable(bat.data(), (int)bat.size()),
+            B2B_ERR_UNSUPPORTED, "delivery launch %d cannot accumulate in clusters",
+            t.site_index);
+      net->add_tune[t.site_index].cluster = t.choice_a;
     } else if (t.site_kind == 11) {
       CHECK(net->two_launch_ok && t.site_index == 0 && (t.choice_a == 0 || t.choice_a == 1),
             B2B_ERR_INVALID_ARG, "site kind 11 exists only for nets that allow both step forms");

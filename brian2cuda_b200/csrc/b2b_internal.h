@@ -269,6 +269,8 @@ struct Pop {
 struct AddTune {
   int32_t grid = 0;               // CTAs per projection
   int32_t group = 0;              // lanes per work item: 8, 16 or 32
+  int32_t cluster = 0;            // 1: accumulate in the distributed shared memory of
+                                  // thread-block clusters, then flush (propagate.cu)
 };
 
 struct StateMon {  // one StateMonitor (b2b_statemon)
@@ -318,6 +320,8 @@ struct Proj {
   // change (dev.src_hi) and is dropped once the last of them has arrived (after this step).
   // Retired projections follow the live ones in b2b_net::projs and belong to no Synapses.
   int64_t retire_after = -1;
+  uint8_t var_mask = 0;                      // bit v: some member adds into variable v
+  int64_t dst_n = 0;                         // padded size of the target population
 };
 
 }  // namespace b2b
@@ -396,6 +400,8 @@ cudaError_t launch_proj_post(const Proj& pr, const int64_t* clock, int k, double
 // One launch for n (<= kMaxProjBatch) additive projections of equal dtype / weight mode.
 cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* clock, int k,
                                   cudaStream_t s, const AddTune* tune = nullptr);
+// Whether such a launch can accumulate in thread-block clusters (AddTune::cluster).
+bool add_batch_cluster_capable(const Proj* const* prs, int n);
 cudaError_t launch_tick(int64_t* clock, int steps, cudaStream_t s);
 // All state monitors (start of step k of the chunk) / all rate monitors (end of the step).
 cudaError_t launch_statemon(const StateMonDev* d_mons, int n_mons, int64_t max_idx,

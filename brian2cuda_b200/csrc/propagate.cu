@@ -15,9 +15,15 @@
 // (pre, d) in the (pre, delay)-sorted synapse arrays (delivery.cuh).  This is the same set of
 // bundles the reference's queue holds in slot `current_offset` after its push, without the
 // push kernel, the host sync on the spike count, the locks or the device heap.
+#include <cooperative_groups.h>
+
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 #include "delivery.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace b2b {
 
@@ -249,6 +255,166 @@ void launch_add_r(const ProjBatch& B, dim3 g, bool hw, bool ag, bool wp, size_t 
   }
 }
 
+// ---- on_pre accumulated in the distributed shared memory of thread-block clusters -------
+// One L2 atomic per event bounds the scattered delivery at high event rates.  Here every
+// cluster of kClusterCtas CTAs holds a private copy of the target variables the batch adds
+// into (slots of the padded target population laid end to end, one slice per CTA's shared
+// memory), adds its share of the events there (remote shared-memory atomics within the
+// cluster), and after a cluster barrier adds its non-zero partial sums to the targets with
+// one vector atomic per four elements.  The sums are regrouped (partial sums per cluster),
+// so results equal the scattered form's up to rounding.  float32 only.
+constexpr int kClusterCtas = 8;
+
+struct ClusterAcc {
+  float* slot_ptr[3];            // target array of each slot
+  int32_t slot_of_var[3];        // slot of variable v (v, ge, gi), -1 if none
+  int32_t n_slots;
+  int32_t slice;                 // floats per CTA (a multiple of 4)
+  int64_t n;                     // padded target population size (a multiple of 128)
+};
+
+template <bool HAS_W, bool WARP_PREFIX, int GROUP>
+__global__ void __launch_bounds__(kDeliverBlock)
+deliver_cluster_kernel(const __grid_constant__ ProjBatch B,
+                       const __grid_constant__ ClusterAcc A, const int64_t* __restrict__ clock,
+                       int k, int pref_ints) {
+  extern __shared__ __align__(16) float s_dyn[];
+  int* s_pref = reinterpret_cast<int*>(s_dyn);
+  float* s_acc = s_dyn + pref_ints;          // pref_ints is a multiple of 4
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  for (int i = 4 * threadIdx.x; i < A.slice; i += 4 * blockDim.x)
+    *reinterpret_cast<float4*>(s_acc + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+  cl.sync();
+  const ProjDev& P = B.p[blockIdx.y];
+  const int64_t ts = clock[0] + k;
+  const float* __restrict__ W = static_cast<const float*>(P.w);
+  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int glane = (threadIdx.x & 31) % GROUP;
+  MemberCache<float> mc;
+  for_each_due_item<WARP_PREFIX, GROUP>(P, ts, warp0, nwarps, s_pref,
+                                        [&](int64_t b0, int64_t b1, int64_t len, int32_t pre) {
+    member_lookup<float>(P, pre, mc);
+    const int v = mc.target == P.targets[0] ? 0 : (mc.target == P.targets[1] ? 1 : 2);
+    const int64_t base = (int64_t)A.slot_of_var[v] * A.n;
+    for (int64_t off = 0; off < len; off += kAddUnroll * GROUP) {
+      int32_t post[kAddUnroll];
+      float w[kAddUnroll];
+      bool ok[kAddUnroll];
+#pragma unroll
+      for (int u = 0; u < kAddUnroll; ++u) {
+        const int64_t s = b0 + off + u * GROUP + glane;
+        ok[u] = s < b1;
+        post[u] = ok[u] ? __ldg(P.post + s) : 0;
+        w[u] = mc.w;
+        if constexpr (HAS_W) w[u] = ok[u] ? __ldg(W + s) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < kAddUnroll; ++u) {
+        if (!ok[u]) continue;
+        const int64_t flat = base + post[u];
+        const unsigned r = (unsigned)(flat / A.slice);
+        float* dst = cl.map_shared_rank(s_acc, r);
+        atomicAdd(dst + (flat - (int64_t)r * A.slice), w[u]);
+      }
+    }
+  });
+  cl.sync();
+  // this CTA's slice of the cluster's partial sums into the targets
+  const int64_t lo = (int64_t)rank * A.slice;
+  const int64_t total = (int64_t)A.n_slots * A.n;
+  for (int i = 4 * threadIdx.x; i < A.slice; i += 4 * blockDim.x) {
+    const int64_t flat = lo + i;
+    if (flat >= total) break;
+    const float4 x = *reinterpret_cast<const float4*>(s_acc + i);
+    if (x.x == 0.f && x.y == 0.f && x.z == 0.f && x.w == 0.f) continue;
+    const int slot = (int)(flat / A.n);
+    atomicAdd(reinterpret_cast<float4*>(A.slot_ptr[slot] + (flat - (int64_t)slot * A.n)), x);
+  }
+}
+
+// Whether a batch can accumulate in clusters, and its accumulator layout (slice <= 200 KB).
+bool cluster_layout(const Proj* const* prs, int n, ClusterAcc* A) {
+  if (prs[0]->dtype != B2B_F32) return false;
+  uint8_t mask = 0;
+  for (int i = 0; i < n; ++i) {
+    if (prs[i]->dst_pop != prs[0]->dst_pop || prs[i]->dev.aggregate) return false;
+    mask |= prs[i]->var_mask;
+  }
+  *A = ClusterAcc{};
+  A->n = 0;
+  int ns = 0;
+  for (int v = 0; v < 3; ++v) {
+    A->slot_of_var[v] = -1;
+    if (mask & (1u << v)) {
+      A->slot_of_var[v] = ns;
+      A->slot_ptr[ns] = static_cast<float*>(prs[0]->dev.targets[v]);
+      ++ns;
+    }
+  }
+  if (mask & ~7u || ns == 0) return false;
+  A->n_slots = ns;
+  A->n = prs[0]->dst_n;                     // every projection targets the same population
+  const int64_t total = (int64_t)ns * A->n;
+  A->slice = (int32_t)(((total + 4 * kClusterCtas - 1) / (4 * kClusterCtas)) * 4);
+  return (int64_t)A->slice * 4 <= 200 * 1024;
+}
+
+// Clusters of the cluster kernel that are resident together for `smem` bytes per CTA
+// (queried once per shared-memory size).
+unsigned resident_clusters(const void* kern, size_t smem) {
+  static std::mutex mu;
+  static std::vector<std::pair<size_t, int>> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& c : cache)
+    if (c.first == smem) return (unsigned)c.second;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kClusterCtas * 64);
+  cfg.blockDim = dim3(kDeliverBlock);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = kClusterCtas;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess)
+    clusters = 0;
+  cache.emplace_back(smem, clusters);
+  return (unsigned)clusters;
+}
+
+template <bool HAS_W, int GROUP>
+cudaError_t launch_cluster_g(const ProjBatch& B, const ClusterAcc& A, unsigned clusters,
+                             bool wp, int pref_ints, size_t smem, const int64_t* clock, int k,
+                             cudaStream_t s, int n) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kClusterCtas * clusters, (unsigned)n);
+  cfg.blockDim = dim3(kDeliverBlock);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = kClusterCtas;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  if (wp) {
+    auto kern = deliver_cluster_kernel<HAS_W, true, GROUP>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaLaunchKernelEx(&cfg, kern, B, A, clock, k, pref_ints);
+  }
+  auto kern = deliver_cluster_kernel<HAS_W, false, GROUP>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaLaunchKernelEx(&cfg, kern, B, A, clock, k, pref_ints);
+}
+
 template <typename R>
 void launch_stdp_pre(const ProjDev& P, unsigned grid, bool ag, bool wp, size_t smem,
                      const int64_t* clock, int k, double dt, cudaStream_t s) {
@@ -277,14 +443,43 @@ cudaError_t launch_proj_add_batch(const Proj* const* prs, int n, const int64_t* 
   }
   const bool wp = nd <= kWarpPrefixMaxDelays;
   const size_t smem = sizeof(int) * (size_t)(nd + 1);
-  if (tune && tune->grid > 0) grid = (unsigned)tune->grid;
   const int group = tune && tune->group > 0 ? tune->group : 8;
+  ClusterAcc A;
+  if (tune && tune->cluster && cluster_layout(prs, n, &A)) {
+    const int pref_ints = ((nd + 1 + 3) / 4) * 4;
+    const size_t csmem = sizeof(float) * ((size_t)pref_ints + A.slice);
+    const unsigned clusters =
+        resident_clusters((const void*)deliver_cluster_kernel<false, true, 8>, csmem);
+    if (clusters > 0) {
+      const bool hw = prs[0]->dev.w != nullptr;
+      switch (group) {
+        case 4:
+          return hw ? launch_cluster_g<true, 4>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n)
+                    : launch_cluster_g<false, 4>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n);
+        case 16:
+          return hw ? launch_cluster_g<true, 16>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n)
+                    : launch_cluster_g<false, 16>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n);
+        case 32:
+          return hw ? launch_cluster_g<true, 32>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n)
+                    : launch_cluster_g<false, 32>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n);
+        default:
+          return hw ? launch_cluster_g<true, 8>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n)
+                    : launch_cluster_g<false, 8>(B, A, clusters, wp, pref_ints, csmem, clock, k, s, n);
+      }
+    }
+  }
+  if (tune && tune->grid > 0) grid = (unsigned)tune->grid;
   const dim3 g(grid, (unsigned)n);
   const bool hw = prs[0]->dev.w != nullptr;
   const bool ag = prs[0]->dev.aggregate != 0;
   if (prs[0]->dtype == B2B_F32) launch_add_r<float>(B, g, hw, ag, wp, smem, clock, k, s, group);
   else launch_add_r<double>(B, g, hw, ag, wp, smem, clock, k, s, group);
   return cudaGetLastError();
+}
+
+bool add_batch_cluster_capable(const Proj* const* prs, int n) {
+  ClusterAcc A;
+  return n > 0 && n <= kMaxProjBatch && cluster_layout(prs, n, &A);
 }
 
 cudaError_t launch_proj_pre(const Proj& pr, const int64_t* clock, int k, double dt,

@@ -401,7 +401,11 @@ b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int
  * representative stretch of the run (bursts included). */
 typedef struct {
   int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records,
-                            5 pending delivery of the two-launch step, 11 step form     */
+                            5 pending delivery of the two-launch step, 11 step form,
+                            12 additive delivery launch accumulated in the distributed
+                            shared memory of 8-CTA thread-block clusters (choice_a 1) or
+                            with one global atomic per event (0); float32 launches onto
+                            one population of at most ~400k padded elements             */
   int32_t site_index;    /* population / delivery launch / projection index              */
   int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item /
                             record order / step form                                      */

@@ -196,6 +196,38 @@ def test_delays_changed_between_runs_match_oracle(gpu_factory, oracle_factory):
     _close(out["gpu"][2], out["orc"][2], 1e-10, 1e-15)
 
 
+def test_cluster_accumulation_delivers_the_same_input(gpu_factory):
+    """Additive delivery accumulated in the distributed shared memory of thread-block
+    clusters (autotuner site kind 12) adds the same input as one atomic per event: a
+    20,000-neuron Poisson source at 400 Hz onto ge and gi of 50,000 float32 LIF targets that
+    do not spike, delays 1-20 steps, per-synapse weights onto ge; ge and gi within 1e-5
+    relative after 60 steps (the partial sums are grouped differently)."""
+    out = {}
+    for cluster in (0, 1):
+        net = gpu_factory(DT, seed=3)
+        S = net.poisson_group(20_000, 400.0, "float32")
+        G = net.lif_group(50_000, LIF(El=0.0, taum=20e-3, taue=5e-3, taui=10e-3, ke=1.0,
+                                      ki=1.0, has_threshold=False, has_reset=False), "float32")
+        rng = np.random.default_rng(8)
+        i, j = models.bernoulli_pairs(rng, 20_000, 50_000, 0.01)
+        d = rng.integers(1, 21, size=len(i)).astype(np.int32)
+        e = i < 16_000
+        net.synapses(S, G, "ge", i[e], j[e], w=rng.uniform(0.5e-3, 1e-3, int(e.sum())),
+                     delay=d[e])
+        net.synapses(S, G, "gi", i[~e], j[~e], w_scalar=-1e-3, delay=d[~e])
+        net.finalize()
+        assert net.run_mode == "per-step"
+        if cluster:
+            net.tune_apply([{"site_kind": 12, "site_index": b, "choice_a": 1, "choice_b": 0}
+                            for b in range(2)])
+        net.run(60)
+        out[cluster] = (net.get_state(G, "ge"), net.get_state(G, "gi"))
+    for k in range(2):
+        a, b = out[1][k].astype(np.float64), out[0][k].astype(np.float64)
+        assert np.abs(b).max() > 0
+        _close(a, b, 1e-5, 1e-5 * np.abs(b).max())
+
+
 def test_synapse_readback_in_input_order(gpu_factory):
     net = gpu_factory(DT)
     G, Ce, Ci, (i, j, d, exc) = _delay_net(net, n=300)
