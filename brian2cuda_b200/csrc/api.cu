@@ -2043,12 +2043,12 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   if (net->two_launch_ok) net->two_launch = false;
   for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->two_launch; ++p) {
     Pop& pop = net->pops[p];
-    if (pop.kind == KIND_SPIKEGEN) continue;
+    if (pop.kind == KIND_SPIKEGEN || pop.kind == KIND_MODEL) continue;
     std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
     if (pop.surr_img) {
       cands = {{0, 0}, {2, 0}, {3, 0}, {4, 0}, {6, 0}};
     } else {
-      cands = {{0, 0}, {1, 128}, {1, 256}, {4, 128}, {4, 256}};
+      cands = {{0, 0}, {1, 128}, {1, 256}, {2, 128}, {2, 256}, {4, 128}, {4, 256}};
     }
     b2b_tune_result r{1, (int32_t)p, 0, 0, 0.0, 0.0};
     double best = 1e30;
@@ -2211,7 +2211,7 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
         CHECK(t.choice_a >= 0 && t.choice_a <= 8, B2B_ERR_INVALID_ARG, "bad CTAs per SM");
         pop.tune_ctas = t.choice_a;
       } else {
-        CHECK((t.choice_a == 0 || t.choice_a == 1 || t.choice_a == 4) &&
+        CHECK((t.choice_a == 0 || t.choice_a == 1 || t.choice_a == 2 || t.choice_a == 4) &&
                   (t.choice_b == 0 || t.choice_b == 128 || t.choice_b == 256),
               B2B_ERR_INVALID_ARG, "bad neuron launch shape");
         pop.tune_e = t.choice_a;

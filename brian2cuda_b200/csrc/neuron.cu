@@ -416,12 +416,16 @@ cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t
     spikegen_step_kernel<<<1, kBlock, 0, s>>>(pop.dev, clock, k, status);
     return cudaGetLastError();
   }
-  const bool four = pop.tune_e > 0 ? pop.tune_e == 4 : wide(pop.dev.n);
-  if (pop.inputs)
-    return four ? launch_e<4, true>(pop, dev, clock, k, dt, status, s)
-                : launch_e<1, true>(pop, dev, clock, k, dt, status, s);
-  return four ? launch_e<4, false>(pop, dev, clock, k, dt, status, s)
-              : launch_e<1, false>(pop, dev, clock, k, dt, status, s);
+  // neurons per thread: the autotuner's choice (1, 2 or 4), else 4 for wide populations
+  const int e = pop.tune_e > 0 ? pop.tune_e : (wide(pop.dev.n) ? 4 : 1);
+  if (pop.inputs) {
+    if (e == 4) return launch_e<4, true>(pop, dev, clock, k, dt, status, s);
+    if (e == 2) return launch_e<2, true>(pop, dev, clock, k, dt, status, s);
+    return launch_e<1, true>(pop, dev, clock, k, dt, status, s);
+  }
+  if (e == 4) return launch_e<4, false>(pop, dev, clock, k, dt, status, s);
+  if (e == 2) return launch_e<2, false>(pop, dev, clock, k, dt, status, s);
+  return launch_e<1, false>(pop, dev, clock, k, dt, status, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -12,12 +12,19 @@ struct Pack {
   R x[E];
 };
 
-// Loads/stores the E values of thread q from one state array (vectorised for E = 4).
+// Loads/stores the E values of thread q from one state array (vectorised for E = 2, 4).
 template <typename R, int E>
 __device__ __forceinline__ Pack<R, E> load_pack(const void* base, int64_t q) {
+  static_assert(E == 1 || E == 2 || E == 4, "neurons per thread");
   Pack<R, E> r;
   if constexpr (E == 1) {
     r.x[0] = static_cast<const R*>(base)[q];
+  } else if constexpr (E == 2 && sizeof(R) == 4) {
+    float2 a = reinterpret_cast<const float2*>(base)[q];
+    r.x[0] = a.x; r.x[1] = a.y;
+  } else if constexpr (E == 2) {
+    double2 a = reinterpret_cast<const double2*>(base)[q];
+    r.x[0] = a.x; r.x[1] = a.y;
   } else if constexpr (sizeof(R) == 4) {
     float4 a = reinterpret_cast<const float4*>(base)[q];
     r.x[0] = a.x; r.x[1] = a.y; r.x[2] = a.z; r.x[3] = a.w;
@@ -33,6 +40,10 @@ template <typename R, int E>
 __device__ __forceinline__ void store_pack(void* base, int64_t q, const Pack<R, E>& r) {
   if constexpr (E == 1) {
     static_cast<R*>(base)[q] = r.x[0];
+  } else if constexpr (E == 2 && sizeof(R) == 4) {
+    reinterpret_cast<float2*>(base)[q] = make_float2(r.x[0], r.x[1]);
+  } else if constexpr (E == 2) {
+    reinterpret_cast<double2*>(base)[q] = make_double2(r.x[0], r.x[1]);
   } else if constexpr (sizeof(R) == 4) {
     reinterpret_cast<float4*>(base)[q] = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
   } else {
@@ -45,6 +56,7 @@ __device__ __forceinline__ void store_pack(void* base, int64_t q, const Pack<R, 
 template <int E>
 __device__ __forceinline__ void store_flags(void* base, int64_t q, uint32_t packed) {
   if constexpr (E == 1) static_cast<uint8_t*>(base)[q] = (uint8_t)packed;
+  else if constexpr (E == 2) reinterpret_cast<uint16_t*>(base)[q] = (uint16_t)packed;
   else reinterpret_cast<uint32_t*>(base)[q] = packed;
 }
 
@@ -52,7 +64,7 @@ __device__ __forceinline__ void store_flags(void* base, int64_t q, uint32_t pack
 template <int E>
 __device__ __forceinline__ int group_of(const PopDev& P, int64_t q) {
   if (!P.vec_group) return 0;
-  return P.vec_group[E == 4 ? q : (q >> 2)];
+  return P.vec_group[E == 4 ? q : (E == 2 ? (q >> 1) : (q >> 2))];
 }
 
 // Writes the spikes flagged in `fl` (bit e = neuron E*q+e) into the ring slot and the spike

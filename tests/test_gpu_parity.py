@@ -694,7 +694,7 @@ def test_hh_stream_kernel_matches_per_step_kernel(gpu_factory, inputs):
     arithmetic is shared.  With inputs, a PoissonInput onto ge exercises that variant."""
     n = 640_000
     out = {}
-    for e in (4, 1):
+    for e in (4, 2, 1):
         net = gpu_factory(DT, seed=2)
         P = net.hh_group(n, models.cobahh_hh(), "float32")
         rng = np.random.default_rng(4)
@@ -710,3 +710,4 @@ def test_hh_stream_kernel_matches_per_step_kernel(gpu_factory, inputs):
     assert len(out[1][0]) > 1000
     for k in range(5):
         np.testing.assert_array_equal(out[4][k], out[1][k], err_msg=str(k))
+        np.testing.assert_array_equal(out[2][k], out[1][k], err_msg=f"two per thread, {k}")
