@@ -84,6 +84,16 @@ class _Emitter:
                     vals = ", ".join(_lit(x) for x in prm.as_array())
                     L.append(f"  {{ b2b_hh_params p = {{{vals}}};")
                     L.append(f"    CHECK(b2b_group_hh(net, {n}, {_DT[dtype]}, &p, &{out})); }}")
+            elif m == "model_group":
+                n, gm, dtype = a
+                from .codegen import compile_model
+                if gm.path is None:
+                    gm.path = compile_model(gm.source)
+                self.gdtype[op.key] = np.float32 if dtype == "float32" else np.float64
+                self.gsize[op.key] = n
+                path = gm.path.replace("\\", "\\\\").replace('"', '\\"')
+                L.append(f"  CHECK(b2b_group_model(net, {n}, {_DT[dtype]}, \"{path}\", "
+                         f"{_lit(gm.refractory)}, &{out}));")
             elif m == "poisson_group":
                 n, rate, dtype = a
                 self.gdtype[op.key] = np.float32 if dtype == "float32" else np.float64
@@ -242,7 +252,7 @@ static const char* results_dir = "results";
     }}                                                                                \
   }} while (0)
 
-static void* load_array(const char* name, size_t bytes) {{
+static inline void* load_array(const char* name, size_t bytes) {{
   char path[1024];
   snprintf(path, sizeof path, "static_arrays/%s.bin", name);
   FILE* f = fopen(path, "rb");
@@ -254,7 +264,7 @@ static void* load_array(const char* name, size_t bytes) {{
   return p;
 }}
 
-static void write_result(const char* name, const void* data, size_t bytes) {{
+static inline void write_result(const char* name, const void* data, size_t bytes) {{
   char path[1024];
   snprintf(path, sizeof path, "%s/%s.bin", results_dir, name);
   FILE* f = fopen(path, "wb");

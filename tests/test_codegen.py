@@ -1,6 +1,7 @@
 """Generated neuron models (CPU only): models outside the hand-written kernels' systems are
 generated with the expected integrator, their CUDA source compiles for sm_100a, and the
 oracle's independent derivation of the exact propagator agrees with the generator's."""
+import os
 import numpy as np
 import pytest
 
@@ -146,3 +147,20 @@ def test_unsupported_model_forms_fail_clearly():
         s.lower()
     with pytest.raises(E.EquationError):
         E.parse_equations("dv/dt = -v")
+
+
+def test_generated_model_reaches_the_c_program(tmp_path):
+    """A script with a generated model emits a C program that loads the compiled model
+    object through b2b_group_model and compiles against the header."""
+    from brian2cuda_b200 import cemit
+    s = Script(dt=DT, seed=3, namespace=ALPHA_NS)
+    G = s.NeuronGroup(100, ALPHA_EQS, threshold="v > Vt", reset="v = Vr", refractory=2e-3)
+    S = s.Synapses(G, G, on_pre="y += 0.9*mV")
+    S.connect(p=0.05)
+    s.SpikeMonitor(G, name="spk")
+    s.run(0.002)
+    prog = s.lower()
+    text = open(cemit.emit_c(prog, str(tmp_path))).read()
+    assert "b2b_group_model(" in text and ".so\"" in text
+    exe = cemit.compile_c(str(tmp_path))
+    assert os.access(exe, os.X_OK)

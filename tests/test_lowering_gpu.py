@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from brian2cuda_b200 import examples
+from brian2cuda_b200.lowering import Script
 
 pytestmark = pytest.mark.gpu
 DT = 1e-4
@@ -85,3 +86,29 @@ def test_generated_c_program_matches_python_binding(gpu_factory, tmp_path):
         np.testing.assert_array_equal(got["vmon"][v][1], ref["vmon"][v][1])
     np.testing.assert_array_equal(got["rate"][0], ref["rate"][0])
     np.testing.assert_array_equal(got["rate"][1], ref["rate"][1])
+
+
+def test_generated_c_program_with_a_generated_model(gpu_factory, tmp_path):
+    """A C program whose group uses a generated model object (b2b_group_model) gives the
+    spikes the Python binding gives."""
+    from brian2cuda_b200 import cemit
+    from test_codegen import ALPHA_EQS, ALPHA_NS
+    s = Script(dt=DT, seed=21, namespace=ALPHA_NS)
+    G = s.NeuronGroup(1500, ALPHA_EQS, threshold="v > Vt", reset="v = Vr", refractory=2e-3)
+    G.v = "Vr + rand() * 22*mV"
+    S = s.Synapses(G, G, on_pre="y += 0.9*mV", delay=3e-4)
+    S.connect(p=0.02)
+    s.SpikeMonitor(G, name="spk")
+    s.run(0.03)
+    prog = s.lower()
+    ref = prog.execute(gpu_factory(DT, seed=s.seed))
+    cemit.emit_c(prog, str(tmp_path))
+    exe = cemit.compile_c(str(tmp_path))
+    os.makedirs(tmp_path / "results", exist_ok=True)
+    r = subprocess.run([exe, "results"], cwd=str(tmp_path), capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = cemit.read_results(prog, str(tmp_path / "results"))
+    assert len(ref["spk"][0]) > 100
+    np.testing.assert_array_equal(got["spk"][0], ref["spk"][0])
+    np.testing.assert_array_equal(got["spk"][1], ref["spk"][1])
