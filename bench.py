@@ -440,47 +440,40 @@ def bench_cobahh(args, world, rank, local):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = e2e_events * world / e2e_s
 
-    # ---- per-kernel device times inside the replayed step graphs: one configured 1 s run
-    # from the checkpoint with an event-record node before and after every launch
-    net.restore(0)
-    prof, prof_step_ms = net.profile_graph(SIM_STEPS)
-    pidx, pst, cursor = net.spikes_fetch(P, cursor, cap=1 << 24)
+    # ---- roofline.  The update and the delivery of a step run as two concurrent launches
+    # (or back to back in the per-step form), so neither takes longer than the step's device
+    # time over the timed region; bytes / that time is a lower bound on each launch's
+    # bandwidth.
     hbm, peak_kind = peaks()
-    p_ev = delivered_events(cum, pidx, pst, SIM_STEPS)
+    step_ms = ms_total / (args.steps * SIM_STEPS)
     nd = DMAX - DMIN + 1
-    deliver_bytes = (BYTES_EVENT * p_ev + BYTES_BUNDLE * nd * float(len(pidx))) / SIM_STEPS
-    neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     two_launch = net.run_mode == "two-launch"
+    neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     if two_launch:
         # the update also adds in and clears the pending input of ge and gi
         neuron_bytes += BYTES_NEURON_FOLD * N_NEURONS
-    site_info = {1: ("neuron (HH update+threshold+compaction"
-                     + (", folding in the pending input)" if two_launch else ")"),
-                     "hh_step_kernel@fold" if two_launch else "hh_step_kernel"),
-                 6: ("delivery on_pre (Ce and Ci, one launch)", "deliver_add_batch_kernel"),
-                 5: ("delivery on_pre into the pending input (Ce and Ci, one launch)",
-                     "deliver_pending_kernel")}
-    kernel_ms, per_launch_bytes, kernels = {}, [], []
-    for k, (kd, ms) in enumerate(prof):
-        label, kname = site_info.get(kd, (f"site kind {kd}", None))
-        b = neuron_bytes if kd == 1 else (deliver_bytes if kd in (5, 6) else 0.0)
-        kernel_ms[label] = round(ms, 6)
-        per_launch_bytes.append(b)
-        kernels.append((label, kname))
-    # the dominant launch site: the largest device time per step inside the graphs
-    dom = max(range(len(prof)), key=lambda k: prof[k][1])
-    dom_ms = prof[dom][1]
-    alg = per_launch_bytes[dom]
-    achieved = alg / (dom_ms * 1e-3) / 1e9
-    traffic = _traffic_lookup(kernels[dom][1]) if kernels[dom][1] else None
-    dsite = [k for k, (kd, _) in enumerate(prof) if kd in (5, 6)][0]
-    d_ms = prof[dsite][1]
+    run_events = (ev_exc + ev_inh) / args.steps
+    deliver_bytes = (BYTES_EVENT * run_events + BYTES_BUNDLE * nd * nspk / args.steps) / SIM_STEPS
+    upd_name = ("neuron (HH update+threshold+compaction"
+                + (", folding in the pending input)" if two_launch else ")"))
+    upd_kernel = "hh_step_kernel@fold" if two_launch else "hh_step_kernel"
+    del_name = ("delivery on_pre into the pending input (Ce and Ci, one launch)" if two_launch
+                else "delivery on_pre (Ce and Ci, one launch)")
+    achieved = neuron_bytes / (step_ms * 1e-3) / 1e9
+    d_achieved = deliver_bytes / (step_ms * 1e-3) / 1e9
+    d_rate = run_events / (step_ms * 1e-3 * SIM_STEPS)
     # the delivery's own ceiling: scattered f32 atomics into the population's ge and gi
     # (2e5 floats), one index load per event from HBM
     loaded, hashed, dsmem = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
                                         stream=stream.cuda_stream)
-    d_rate = p_ev / (d_ms * 1e-3 * SIM_STEPS)
-    names = [lab for lab, _ in kernels]
+    # diagnostic only: one configured run from the checkpoint with an event-record node
+    # before and after every launch; the nodes lengthen each launch by microseconds, so at
+    # this step size the figures give the order of the launches' shares, not their times
+    net.restore(0)
+    prof, prof_step_ms = net.profile_graph(SIM_STEPS)
+    net.spikes_fetch(P, cursor, cap=1 << 24)
+    site_label = {1: "neuron", 5: "delivery (pending)", 6: "delivery"}
+    in_graph = {site_label.get(kd, f"site kind {kd}"): round(ms, 6) for kd, ms in prof}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -498,26 +491,36 @@ def bench_cobahh(args, world, rank, local):
         "setup_s": setup_s,
         "run_mode": net.run_mode,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "kernel": names[dom],
-                     "kernel_ms": dom_ms, "peak_source": peak_kind,
-                     "bytes_per_launch": alg,
-                     "timing": "mean device time per step inside the replayed step graphs "
-                               "(event-record nodes around the launch, one configured run)",
-                     "note": "the neuron state (5.4 MB) is L2-resident, so the update is "
-                             "latency-bound, not HBM-bound"},
-        "kernel_ms_per_step_in_graph": kernel_ms,
-        "profiled_step_ms": prof_step_ms,
-        "delivery": {"kernel": names[dsite], "kernel_ms": d_ms,
+                     "frac": achieved / hbm, "traffic": _traffic_lookup(upd_kernel),
+                     "kernel": upd_name, "kernel_ms": step_ms, "peak_source": peak_kind,
+                     "bytes_per_launch": neuron_bytes,
+                     "bytes_per_unit": (f"{BYTES_NEURON_UPDATE} B per neuron-update"
+                                        + (f" + {BYTES_NEURON_FOLD} B pending input read and "
+                                           "cleared" if two_launch else "")),
+                     "timing": "kernel_ms = device time per simulation step over the timed "
+                               "region (CUDA events); the step's launches run inside it, so "
+                               "it bounds the kernel's duration from above and achieved/frac "
+                               "are lower bounds",
+                     "note": "the neuron state (5.4 MB) is L2-resident between steps, so the "
+                             "update is latency-bound, not HBM-bound"},
+        "delivery": {"kernel": del_name, "kernel_ms": step_ms,
                      "bytes_per_launch": deliver_bytes,
-                     "achieved_gbs": deliver_bytes / (d_ms * 1e-3) / 1e9,
-                     "frac_hbm": deliver_bytes / (d_ms * 1e-3) / 1e9 / hbm,
+                     "bytes_per_unit": f"{BYTES_EVENT} B per event + {BYTES_BUNDLE} B per "
+                                       "(spike, delay) bundle",
+                     "achieved_gbs": d_achieved, "frac_hbm": d_achieved / hbm,
+                     "traffic": _traffic_lookup("deliver_pending_kernel" if two_launch
+                                                else "deliver_add_batch_kernel"),
                      "events_per_s_in_kernel": d_rate,
                      "atomic_ceiling_events_per_s": {"index_loaded": loaded,
                                                      "index_in_registers": hashed,
                                                      "cluster_shared_memory": dsmem},
                      "frac_of_atomic_ceiling": d_rate / loaded,
-                     "note": "at the network's ~3 Hz a step delivers ~6e4 events: the "
-                             "kernel is latency-bound; see configs.propagation for load"},
+                     "note": "lower bounds from the step time, as for the roofline; at the "
+                             "network's ~3 Hz a step delivers ~6e4 events and the kernel is "
+                             "latency-bound; configs.propagation measures it under load"},
+        "in_graph_event_nodes": {"ms_per_step": in_graph, "step_ms": prof_step_ms,
+                                 "note": "event-record nodes around every launch (diagnostic; "
+                                         f"they lengthen the {step_ms * 1e3:.2f} us step)"},
         "autotune": tune,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h // max(1, args.steps),
@@ -639,7 +642,7 @@ def bench_batched(args, world, rank, local):
     net.restore(0)
     prof, _ = net.profile_graph(200)
     hbm, peak_kind = peaks()
-    neuron_ms = [ms for k, ms in prof if k == 1][0]
+    neuron_ms = min([ms for k, ms in prof if k == 1][0], ms_total / (args.steps * BATCH_STEPS))
     neuron_bytes = float(BYTES_NEURON_UPDATE * n_total)
     achieved = neuron_bytes / (neuron_ms * 1e-3) / 1e9
     # raster of the exact form, first 300 steps, for the surrogate comparison
@@ -786,12 +789,22 @@ def _line_base(args, world, metric, value, unit, ms_per_step, workload, config, 
             "data": "synthetic", "config": dict({"workload": workload}, **config)}
 
 
-def _roofline(bytes_per_launch, ms, kernel):
+def _roofline(bytes_per_launch, ms, kernel, step_ms=None):
+    """ms: the launch's mean device time per step inside the step graphs, measured with
+    event-record nodes around it; those nodes lengthen a launch by microseconds, so where
+    that exceeds the step's own device time over the timed region (step_ms), the step time
+    (an upper bound on the launch's duration) is used instead."""
     hbm, kind = peaks()
+    timing = "in-graph device time (event-record nodes around the launch)"
+    if step_ms is not None and ms > step_ms:
+        ms = step_ms
+        timing = ("device time per simulation step over the timed region (CUDA events), an "
+                  "upper bound on the launch's duration: achieved and frac are lower bounds")
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": _traffic_lookup(kernel), "kernel": kernel,
-            "kernel_ms": ms, "peak_source": kind, "bytes_per_launch": bytes_per_launch}
+            "kernel_ms": ms, "peak_source": kind, "bytes_per_launch": bytes_per_launch,
+            "timing": timing}
 
 
 def _timed_net_runs(net, stream, args, world, local, steps_per_run):
@@ -849,8 +862,9 @@ def bench_small(args, world, rank, local):
         nb = BYTES["cuba_neuron"] * 4000.0
         db = BYTES["cuba_event"] * events / (args.steps * steps_run)
         dom = max(prof, key=lambda kv: kv[1])
-        roof = (_roofline(nb, dom[1], "lif_step_kernel") if dom[0] == 1 else
-                _roofline(db, dom[1], "deliver_add_batch_kernel"))
+        step_ms = ms / (args.steps * steps_run)
+        roof = (_roofline(nb, dom[1], "lif_step_kernel", step_ms) if dom[0] == 1 else
+                _roofline(db, dom[1], "deliver_add_batch_kernel", step_ms))
         line = _line_base(args, world, "synaptic events/s", value, "events/s",
                           ms / args.steps, WORKLOADS[wl],
                           {"sim_steps_per_step": steps_run, "neurons": 4000,
@@ -904,7 +918,7 @@ def bench_small(args, world, rank, local):
                            "synapses": 10_000_000, "parallelism": f"replicas x{world}",
                            "l2": "working set > L2 (1e7 synapses x 4 f32 variables = 160 MB)"},
                           "f32")
-        roof = _roofline(b, dom[1], kname)
+        roof = _roofline(b, dom[1], kname, ms / (args.steps * steps_run))
         if kname == "deliver_stdp_post_kernel":
             post_grouped = any(t["site_kind"] == 8 and t["choice_a"] == 1 for t in tune)
             roof["traffic"] = _traffic_lookup(kname + ("" if post_grouped else "@synorder"))
@@ -957,14 +971,14 @@ def bench_small(args, world, rank, local):
         per_step_bundles = nspk / (args.steps * steps_run) * (DMAX - DMIN + 1)
         db = BYTES_EVENT * per_step_events + BYTES_BUNDLE * per_step_bundles
         dmsk = [m for k, m in prof if k == 6]
-        roof = _roofline(db, dmsk[0], "deliver_add_batch_kernel")
+        roof = _roofline(db, dmsk[0], "deliver_add_batch_kernel", ms / (args.steps * steps_run))
         roof["traffic"] = _traffic_lookup("deliver_add_batch_kernel@propagation")
         roof["note"] = ("12 B per event (target index 4 B + target read/write 8 B) + 8 B per "
                         "(spike, delay) bundle; bound: one L2 atomic per event")
         from brian2cuda_b200.network import atomic_rate
         loaded, hashed, dsmem = atomic_rate(2 * N_NEURONS, 60_000_000, device=local,
                                             stream=stream.cuda_stream)
-        d_rate = per_step_events / (dmsk[0] * 1e-3)
+        d_rate = per_step_events / (roof["kernel_ms"] * 1e-3)
         roof["events_per_s_in_kernel"] = d_rate
         roof["atomic_ceiling_events_per_s"] = {"index_loaded": loaded,
                                                "index_in_registers": hashed,

@@ -172,10 +172,13 @@ b2b_status add_syn(b2b_net* net, Syn&& s, int32_t* sid) {
   CHECK(s.post_gid >= 0 && s.post_gid < (int)net->groups.size(), B2B_ERR_INVALID_ARG,
         "bad post group %d", s.post_gid);
   const Group& post = net->groups[s.post_gid];
-  CHECK(post.kind == KIND_LIF || post.kind == KIND_HH, B2B_ERR_INVALID_ARG,
-        "synapse targets must be LIF or HH groups");
+  CHECK(post.kind == KIND_LIF || post.kind == KIND_HH || post.kind == KIND_MODEL,
+        B2B_ERR_INVALID_ARG, "synapse targets must be LIF, HH or generated-model groups");
   CHECK(s.target_var == B2B_VAR_V || s.target_var == B2B_VAR_GE || s.target_var == B2B_VAR_GI,
-        B2B_ERR_INVALID_ARG, "target variable must be v, ge or gi");
+        B2B_ERR_INVALID_ARG, "target variable must be v, ge or gi (slots 0-2)");
+  // a generated model's synaptic targets are its first state variables (slots 0-2)
+  CHECK(post.kind != KIND_MODEL || s.target_var < post.minfo.n_vars, B2B_ERR_INVALID_ARG,
+        "target slot %d is not a state variable of the generated model", s.target_var);
   CHECK(s.effect == B2B_EFFECT_ADD || s.effect == B2B_EFFECT_STDP, B2B_ERR_INVALID_ARG,
         "bad effect %d", s.effect);
   net->syns.push_back(std::move(s));

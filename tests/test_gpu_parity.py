@@ -169,7 +169,6 @@ def test_delays_changed_between_runs_match_oracle(gpu_factory, oracle_factory):
     first longer than the spike-history ring holds (the ring grows), then with delays of 0
     (the net leaves the two-launch form for the per-step kernels); spikes exact, v within
     1e-10, synapse delays read back in input order."""
-    rng = np.random.default_rng(21)
     out = {}
     for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
         net = make(DT)
@@ -190,7 +189,7 @@ def test_delays_changed_between_runs_match_oracle(gpu_factory, oracle_factory):
             np.testing.assert_array_equal(net.syn_get(Ci, "delay"), d2)
         idx, st = net.spikes(G)
         out[name] = (idx, st, net.get_state(G, "v"))
-    assert len(out["gpu"][0]) > 300 and rng is not None
+    assert len(out["gpu"][0]) > 150
     np.testing.assert_array_equal(out["gpu"][1], out["orc"][1])
     np.testing.assert_array_equal(out["gpu"][0], out["orc"][0])
     _close(out["gpu"][2], out["orc"][2], 1e-10, 1e-15)
