@@ -270,6 +270,9 @@ def main():
     ap.add_argument("--two-launch", action="store_true",
                     help="run every step as two concurrent launches (neuron update, delivery "
                          "of earlier spikes) where the net allows it")
+    ap.add_argument("--one-launch", action="store_true",
+                    help="run both halves of every step (update, delivery of earlier spikes) "
+                         "as one launch where the net allows it")
     ap.add_argument("--per-step", action="store_true",
                     help="always the per-step kernels (default: the library's choice, which "
                          "the autotuner settles)")
@@ -348,7 +351,8 @@ def bench_cobahh(args, world, rank, local):
     mon_cap = int(N_NEURONS * SIM_STEPS * DT * 30 * runs)  # mean rate up to 30 Hz
     net = Network(DT, seed=models.SEED_BASE + 1, device=local, steps_per_graph=50,
                   stream=stream.cuda_stream,
-                  two_launch=True if args.two_launch else (False if args.per_step else None))
+                  two_launch=True if args.two_launch else (False if args.per_step else None),
+                  one_launch=args.one_launch)
     t_setup = time.perf_counter()
     ids = models.build_cobahh(net, n=N_NEURONS, p=P_CONNECT, dmin=DMIN, dmax=DMAX,
                               monitor_capacity=mon_cap)
@@ -447,7 +451,8 @@ def bench_cobahh(args, world, rank, local):
     hbm, peak_kind = peaks()
     step_ms = ms_total / (args.steps * SIM_STEPS)
     nd = DMAX - DMIN + 1
-    two_launch = net.run_mode == "two-launch"
+    one_launch = net.run_mode == "one-launch"
+    two_launch = net.run_mode == "two-launch" or one_launch
     neuron_bytes = float(BYTES_NEURON_UPDATE * N_NEURONS)
     if two_launch:
         # the update also adds in and clears the pending input of ge and gi
@@ -459,7 +464,15 @@ def bench_cobahh(args, world, rank, local):
     upd_kernel = "hh_step_kernel@fold" if two_launch else "hh_step_kernel"
     del_name = ("delivery on_pre into the pending input (Ce and Ci, one launch)" if two_launch
                 else "delivery on_pre (Ce and Ci, one launch)")
-    achieved = neuron_bytes / (step_ms * 1e-3) / 1e9
+    roof_bytes = neuron_bytes
+    if one_launch:
+        # one kernel holds both halves of the step: its bytes are the update's and the
+        # delivery's
+        upd_name = ("one_launch_step_kernel: " + upd_name + " and " + del_name.split(" (")[0]
+                    + " in one grid")
+        upd_kernel = "one_launch_step_kernel"
+        roof_bytes = neuron_bytes + deliver_bytes
+    achieved = roof_bytes / (step_ms * 1e-3) / 1e9
     d_achieved = deliver_bytes / (step_ms * 1e-3) / 1e9
     d_rate = run_events / (step_ms * 1e-3 * SIM_STEPS)
     # the delivery's own ceiling: scattered f32 atomics into the population's ge and gi
@@ -472,7 +485,7 @@ def bench_cobahh(args, world, rank, local):
     net.restore(0)
     prof, prof_step_ms = net.profile_graph(SIM_STEPS)
     net.spikes_fetch(P, cursor, cap=1 << 24)
-    site_label = {1: "neuron", 5: "delivery (pending)", 6: "delivery"}
+    site_label = {1: "neuron", 5: "delivery (pending)", 6: "delivery", 13: "one launch"}
     in_graph = {site_label.get(kd, f"site kind {kd}"): round(ms, 6) for kd, ms in prof}
 
     line = {
@@ -493,10 +506,13 @@ def bench_cobahh(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": _traffic_lookup(upd_kernel),
                      "kernel": upd_name, "kernel_ms": step_ms, "peak_source": peak_kind,
-                     "bytes_per_launch": neuron_bytes,
+                     "bytes_per_launch": roof_bytes,
                      "bytes_per_unit": (f"{BYTES_NEURON_UPDATE} B per neuron-update"
                                         + (f" + {BYTES_NEURON_FOLD} B pending input read and "
-                                           "cleared" if two_launch else "")),
+                                           "cleared" if two_launch else "")
+                                        + (f"; + {BYTES_EVENT} B per event and {BYTES_BUNDLE} "
+                                           "B per (spike, delay) bundle" if one_launch
+                                           else "")),
                      "timing": "kernel_ms = device time per simulation step over the timed "
                                "region (CUDA events); the step's launches run inside it, so "
                                "it bounds the kernel's duration from above and achieved/frac "
@@ -1027,11 +1043,14 @@ def bench_small(args, world, rank, local):
         net.sync()
         torch.cuda.synchronize()
         clocks = Clocks(local)
-        t0 = time.perf_counter()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
         for _ in range(args.steps):
             hb.run(steps_run)
+        ev1.record(stream)
+        ev1.synchronize()
         net.sync()
-        el = max_over_ranks(time.perf_counter() - t0, world)
+        el = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, world)
         clk = clocks.stop()
         n_comp = hb.n_comp
         value = float(n_comp) * steps_run * args.steps * world / el
@@ -1045,7 +1064,7 @@ def bench_small(args, world, rank, local):
         line.update({"neuron_updates_per_s": 1024.0 * steps_run * args.steps * world / el,
                      "roofline": _roofline(BYTES["hines_comp"] * n_comp * steps_run,
                                            1e3 * el / args.steps, "hines_kernel"),
-                     "timing": "wall clock around b2b_hines_run with a device sync (one "
+                     "timing": "CUDA events on the net's stream around the runs (one "
                                "kernel per 1000-step chunk)",
                      "gpu_launches": args.steps * (steps_run // 1000), "clocks": clk})
         line["roofline"]["note"] = ("achieved = algorithmic 136 B per compartment-step / time; "

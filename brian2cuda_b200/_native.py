@@ -20,6 +20,7 @@ STATUS_NAMES = {
 F32, F64 = 1, 2
 NET_NO_GRAPH, NET_CHECKED, NET_RESET_BEFORE_SYNAPSES, NET_TWO_LAUNCH, NET_SMALL = 1, 2, 4, 8, 16
 NET_PER_STEP = 32
+NET_ONE_LAUNCH = 64
 EFFECT_ADD, EFFECT_STDP = 1, 2
 VARS = {"v": 0, "ge": 1, "gi": 2, "m": 3, "h": 4, "n": 5, "lastspike": 6,
         "not_refractory": 7}

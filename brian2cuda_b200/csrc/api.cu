@@ -793,7 +793,8 @@ constexpr int64_t kAutoTwoLaunchMaxNeurons = 1 << 18;
 b2b_status setup_two_launch(b2b_net* net) {
   const int32_t flags = net->cfg.flags;
   if (flags & (B2B_NET_PER_STEP | B2B_NET_SMALL)) return B2B_OK;
-  if ((flags & B2B_NET_CHECKED) && !(flags & B2B_NET_TWO_LAUNCH)) return B2B_OK;
+  if ((flags & B2B_NET_CHECKED) && !(flags & (B2B_NET_TWO_LAUNCH | B2B_NET_ONE_LAUNCH)))
+    return B2B_OK;
   if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.empty() || net->projs.size() > kMaxProjBatch)
     return B2B_OK;
@@ -842,7 +843,11 @@ b2b_status setup_two_launch(b2b_net* net) {
   CU(cudaEventCreateWithFlags(&net->ev_d[0], cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&net->ev_d[1], cudaEventDisableTiming));
   net->two_launch_ok = true;
-  net->two_launch = (flags & B2B_NET_TWO_LAUNCH) || pop.n <= kAutoTwoLaunchMaxNeurons;
+  net->two_launch = (flags & (B2B_NET_TWO_LAUNCH | B2B_NET_ONE_LAUNCH)) ||
+                    pop.n <= kAutoTwoLaunchMaxNeurons;
+  net->one_launch_ok = one_launch_supported(pop, F);
+  net->one_launch_grid = net->pending_grid;
+  net->one_launch = net->one_launch_ok && (flags & B2B_NET_ONE_LAUNCH);
   return B2B_OK;
 }
 
@@ -865,6 +870,23 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
                     net->d_status, net->stream));
     CU(prof_mark(net, 0, 0, 1, net->stream));
     CU(launch_tick(net->d_clock, kk, net->stream));
+    net->launches += 2;
+    return B2B_OK;
+  }
+  if (net->two_launch && net->one_launch) {
+    // The same two halves as one grid per step (neuron.cu): consecutive launches on the
+    // net's stream order step k+1 after both halves of step k.  Profiling site 0.
+    const Pop& pop = net->pops[0];
+    cudaStream_t s = net->stream;
+    for (int k = 0; k < kk; ++k) {
+      CU(prof_mark(net, k, 0, 0, s));
+      CU(launch_one_launch_step(pop, net->fold_dev, net->pdev, net->one_launch_grid,
+                                net->d_clock, k, net->cfg.dt, net->d_status, s));
+      CU(prof_mark(net, k, 0, 1, s));
+      ++net->launches;
+    }
+    CU(launch_fold_pending(net->pdev, pop.dtype, net->d_clock, kk - 1, s));
+    CU(launch_tick(net->d_clock, kk, s));
     net->launches += 2;
     return B2B_OK;
   }
@@ -1039,6 +1061,8 @@ void refresh_two_launch(b2b_net* net) {
   if (!ok) {
     net->two_launch = false;
     net->two_launch_ok = false;
+    net->one_launch = false;
+    net->one_launch_ok = false;
     return;
   }
   const Pop& pop = net->pops[0];
@@ -1056,6 +1080,8 @@ void refresh_two_launch(b2b_net* net) {
   }
   net->fold_dev = pop.dev;
   for (int v = 0; v < 3; ++v) net->fold_dev.fold[v] = F.acc[v];
+  net->one_launch_ok = one_launch_supported(pop, F);
+  if (!net->one_launch_ok) net->one_launch = false;
 }
 
 // Grows population pi's spike-history ring to new_len slots, keeping the spikes of the last
@@ -1170,12 +1196,15 @@ b2b_status rng_buffer_get(b2b_net* net, int32_t gid, bool normal, void* host, in
 // Launch sites of one step, in the order enqueue_steps marks them for profiling: the state
 // monitors (kind 9), each population (1), each additive delivery launch (6), each STDP
 // projection's on_pre (2) and on_post (3), each deferred reset (4), the rate monitors (10);
-// the two-launch step: its delivery (5) and update (1); the one-CTA small path: its kernel (7).
+// the two-launch step: its delivery (5) and update (1); the one-launch step: its kernel (13);
+// the one-CTA small path: its kernel (7).
 struct ProfSite { int kind; int idx; };
 std::vector<ProfSite> profile_sites(const b2b_net* net) {
   std::vector<ProfSite> sites;
   if (net->small) {
     sites.push_back({7, 0});
+  } else if (net->two_launch && net->one_launch) {
+    sites.push_back({13, 0});
   } else if (net->two_launch) {
     sites.push_back({5, 0});
     sites.push_back({1, 0});
@@ -1766,6 +1795,9 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
       if (s.kind == 5)
         e = launch_pending_delivery(net->pdev, net->pops[0].dtype, net->pending_grid, clk, 0,
                                     net->stream);
+      if (s.kind == 13)
+        e = launch_one_launch_step(net->pops[0], net->fold_dev, net->pdev, net->one_launch_grid,
+                                   clk, 0, net->cfg.dt, net->d_status, net->stream);
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
       ++net->launches;
@@ -1942,6 +1974,14 @@ constexpr double kTuneMargin = 0.98;
 
 // Launch shape of the delivery launch of a net run with two launches per step (pending.cu):
 // lanes per work item (0: 8) and CTAs (0: two per SM).
+void set_one_launch_grid(b2b_net* net, int grid) {
+  net->one_launch_grid = grid > 0 ? grid : net->pending_grid;
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+}
+
 void set_pending_shape(b2b_net* net, int group, int grid) {
   int sms = kNumSMs;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
@@ -2043,7 +2083,9 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   // a net that allows both forms of the step tunes the per-step kernels first, then the two
   // concurrent launches, and keeps the faster form
   const bool builtin_two_launch = net->two_launch;
+  const bool builtin_one_launch = net->two_launch && net->one_launch;
   if (net->two_launch_ok) net->two_launch = false;
+  net->one_launch = false;
   for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->two_launch; ++p) {
     Pop& pop = net->pops[p];
     if (pop.kind == KIND_SPIKEGEN || pop.kind == KIND_MODEL) continue;
@@ -2153,12 +2195,36 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
     const double two_launch_ms = res.back().best_ms;
-    // the built-in form stays unless the other is 2 % faster
-    const bool use_two_launch = builtin_two_launch ? !(per_step_ms < kTuneMargin * two_launch_ms)
-                                         : two_launch_ms < kTuneMargin * per_step_ms;
-    net->two_launch = use_two_launch;
-    res.push_back(b2b_tune_result{11, 0, use_two_launch ? 1 : 0, 0, std::min(per_step_ms, two_launch_ms),
-                                  builtin_two_launch ? two_launch_ms : per_step_ms});
+    // the same halves as one grid per step: CTAs of the delivery after the update's
+    double one_launch_ms = 1e30;
+    int one_grid = net->pending_grid;
+    if (net->one_launch_ok && st == B2B_OK) {
+      net->one_launch = true;
+      const int grids[] = {net->pending_grid, sms / 2, sms, 2 * sms, 4 * sms};
+      for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
+        set_one_launch_grid(net, grids[c]);
+        double ms = 0;
+        st = trial(&ms);
+        if (st == B2B_OK && (c == 0 || ms < kTuneMargin * one_launch_ms)) {
+          one_launch_ms = ms;
+          one_grid = grids[c];
+        }
+      }
+      set_one_launch_grid(net, one_grid);
+      net->one_launch = false;
+    }
+    // the form of the step: 0 per-step kernels, 1 two concurrent launches, 2 one launch; the
+    // built-in form stays unless another is 2 % faster
+    const double form_ms[3] = {per_step_ms, two_launch_ms, one_launch_ms};
+    const int builtin = builtin_two_launch ? (builtin_one_launch ? 2 : 1) : 0;
+    int other = -1;
+    for (int f = 0; f < 3; ++f)
+      if (f != builtin && (other < 0 || form_ms[f] < form_ms[other])) other = f;
+    const int form = form_ms[other] < kTuneMargin * form_ms[builtin] ? other : builtin;
+    net->two_launch = form >= 1;
+    net->one_launch = form == 2;
+    res.push_back(b2b_tune_result{11, 0, form, form == 2 ? one_grid : 0, form_ms[form],
+                                  form_ms[builtin]});
   }
   // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
   for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
@@ -2180,7 +2246,10 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     r.best_ms = best;
     res.push_back(r);
   }
-  if (st != B2B_OK && net->two_launch_ok) net->two_launch = builtin_two_launch;
+  if (st != B2B_OK && net->two_launch_ok) {
+    net->two_launch = builtin_two_launch;
+    net->one_launch = builtin_one_launch;
+  }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
   if (st2 == B2B_OK) st2 = put_back_monitors();
@@ -2239,9 +2308,13 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             t.site_index);
       net->add_tune[t.site_index].cluster = t.choice_a;
     } else if (t.site_kind == 11) {
-      CHECK(net->two_launch_ok && t.site_index == 0 && (t.choice_a == 0 || t.choice_a == 1),
+      CHECK(net->two_launch_ok && t.site_index == 0 && t.choice_a >= 0 && t.choice_a <= 2,
             B2B_ERR_INVALID_ARG, "site kind 11 exists only for nets that allow both step forms");
-      net->two_launch = t.choice_a == 1;
+      CHECK(t.choice_a != 2 || (net->one_launch_ok && t.choice_b >= 0 && t.choice_b <= 65535),
+            B2B_ERR_INVALID_ARG, "the net does not allow the one-launch step");
+      net->two_launch = t.choice_a >= 1;
+      net->one_launch = t.choice_a == 2;
+      if (t.choice_a == 2) set_one_launch_grid(net, t.choice_b);
     } else if (t.site_kind == 5) {
       CHECK(net->two_launch_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
             "site kind 5 exists only for nets that allow two launches per step");
@@ -2331,7 +2404,7 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t) {
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode) {
   if (!net || !mode) return B2B_ERR_INVALID_ARG;
   if (!net->finalized) return fail(net, B2B_ERR_STATE, "call b2b_finalize first");
-  *mode = net->small ? 2 : (net->two_launch ? 1 : 0);
+  *mode = net->small ? 2 : (net->two_launch ? (net->one_launch ? 3 : 1) : 0);
   return B2B_OK;
 }
 

@@ -368,6 +368,11 @@ struct b2b_net {
   b2b::PendingDev pdev{};
   b2b::PopDev fold_dev{};                  // the population's view whose update folds acc in
   int pending_grid = 0;
+  // the same two halves as one grid per step on the net's stream (neuron.cu), the delivery
+  // with one_launch_grid CTAs after the update's; only where two_launch_ok
+  bool one_launch = false;
+  bool one_launch_ok = false;
+  int one_launch_grid = 0;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
   std::vector<void*> pending_allocs;
@@ -425,6 +430,11 @@ cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* 
 // fold of the pending input at the end of a chunk.
 cudaError_t launch_pending_delivery(const PendingDev& F, int dtype, int grid,
                                     const int64_t* clock, int k, cudaStream_t s);
+// The step as one launch (neuron.cu): the update's CTAs, then deliver_ctas delivering CTAs.
+bool one_launch_supported(const Pop& pop, const PendingDev& F);
+cudaError_t launch_one_launch_step(const Pop& pop, const PopDev& U, const PendingDev& F,
+                                   int deliver_ctas, const int64_t* clock, int k, double dt,
+                                   int32_t* status, cudaStream_t s);
 cudaError_t launch_fold_pending(const PendingDev& F, int dtype, const int64_t* clock, int k_last,
                                 cudaStream_t s);
 }  // namespace b2b

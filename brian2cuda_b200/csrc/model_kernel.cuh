@@ -4,7 +4,7 @@
 // device functions — the integration step of its equations, its threshold condition and its
 // reset statements, written out by brian2cuda_b200/codegen.py — and compiles it with this
 // header into a shared object.  The kernel around them is the same fused pass as the
-// hand-written neuron kernels (neuron.cu): one thread per neuron, refractoriness from
+// hand-written neuron kernels (neuron.cu): one or four neurons per thread, refractoriness from
 // lastspike, update, threshold, reset (unless a synapse writes a variable the reset writes:
 // then a second launch resets the step's spiking neurons after the synaptic delivery, as
 // Brian2's schedule orders them), and the CTA's spikes compacted into the population's slot of
@@ -39,7 +39,11 @@ __device__ __forceinline__ R clip(R v, R lo, R hi) {
   return v < lo ? lo : (v > hi ? hi : v);
 }
 
-template <class M, typename R>
+// A thread owns E consecutive neurons (E = 4 for populations large enough to fill the GPU
+// that way: every state array and draw row read with one 128-bit access per thread, 8 B
+// of index arithmetic and one compaction per four neurons); the arithmetic of each neuron is
+// the same for every E.
+template <class M, typename R, int E>
 __global__ void __launch_bounds__(kBlock)
 model_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
                   int32_t* status) {
@@ -49,38 +53,58 @@ model_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned fl = 0;
-  if (q < P.n) {
+  if (q < P.n / E) {
     const ModelGroupDev g = static_cast<const ModelGroupDev*>(P.params)[0];
     const bool refr = g.ref_steps >= 0;
-    R x[M::NV];
+    Pack<R, E> X[M::NV];
 #pragma unroll
-    for (int v = 0; v < M::NV; ++v) x[v] = static_cast<const R*>(P.var[v])[q];
-    R ls = (R)0;
-    bool nr = true;
-    if (refr) {
-      ls = static_cast<const R*>(P.var[B2B_VAR_LASTSPIKE])[q];
-      nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
-    }
-    const R* nrm = M::NN ? static_cast<const R*>(P.rng_normal) + (int64_t)k * M::NN * P.n + q
-                         : nullptr;
-    const R* uni = M::NU ? static_cast<const R*>(P.rng) + (int64_t)k * M::NU * P.n + q
-                         : nullptr;
-    M::template update<R>(x, t, dt, nr, nrm, uni, P.n);
-    const bool valid = q - g.offset < g.n;
-    if (M::HAS_THRESHOLD && valid && nr && M::template threshold<R>(x)) {
-      fl = 1;
-      nr = false;
-      if (refr) ls = (R)t;
-      if (!P.late_reset) M::template reset<R>(x);
+    for (int v = 0; v < M::NV; ++v) X[v] = load_pack<R, E>(P.var[v], q);
+    Pack<R, E> LS;
+    if (refr) LS = load_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q);
+    // this step's draws of the E neurons: draw d of neuron E q + e at D[d].x[e]
+    constexpr int ND = M::NN + M::NU > 0 ? M::NN + M::NU : 1;
+    Pack<R, E> D[ND];
+#pragma unroll
+    for (int d = 0; d < M::NN; ++d)
+      D[d] = load_pack<R, E>(static_cast<const R*>(P.rng_normal) +
+                                 ((int64_t)k * M::NN + d) * P.n, q);
+#pragma unroll
+    for (int d = 0; d < M::NU; ++d)
+      D[M::NN + d] = load_pack<R, E>(static_cast<const R*>(P.rng) +
+                                         ((int64_t)k * M::NU + d) * P.n, q);
+    uint32_t NRout = 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      R x[M::NV];
+#pragma unroll
+      for (int v = 0; v < M::NV; ++v) x[v] = X[v].x[e];
+      bool nr = true;
+      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+      R dn[ND], du[ND];
+#pragma unroll
+      for (int d = 0; d < M::NN; ++d) dn[d] = D[d].x[e];
+#pragma unroll
+      for (int d = 0; d < M::NU; ++d) du[d] = D[M::NN + d].x[e];
+      M::template update<R>(x, t, dt, nr, dn, du, 1);
+      const bool valid = E * q + e - g.offset < g.n;
+      if (M::HAS_THRESHOLD && valid && nr && M::template threshold<R>(x)) {
+        fl |= 1u << e;
+        nr = false;
+        if (refr) LS.x[e] = (R)t;
+        if (!P.late_reset) M::template reset<R>(x);
+      }
+#pragma unroll
+      for (int v = 0; v < M::NV; ++v) X[v].x[e] = x[v];
+      NRout |= (nr ? 1u : 0u) << (8 * e);
     }
 #pragma unroll
-    for (int v = 0; v < M::NV; ++v) static_cast<R*>(P.var[v])[q] = x[v];
+    for (int v = 0; v < M::NV; ++v) store_pack<R, E>(P.var[v], q, X[v]);
     if (refr) {
-      if (fl) static_cast<R*>(P.var[B2B_VAR_LASTSPIKE])[q] = ls;
-      static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY])[q] = nr ? 1 : 0;
+      if (fl) store_pack<R, E>(P.var[B2B_VAR_LASTSPIKE], q, LS);   // changes only on a spike
+      store_flags<E>(P.var[B2B_VAR_NOT_REFRACTORY], q, NRout);
     }
   }
-  emit_spikes<1>(P, q, fl, ts, slot, status);
+  emit_spikes<E>(P, q, fl, ts, slot, status);
   clear_next_slot(P, ts);
 }
 
@@ -109,11 +133,16 @@ int32_t launch(const void* pop, const int64_t* clock, int32_t k, double dt, int3
   const PopDev& P = *static_cast<const PopDev*>(pop);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (phase == 0) {
-    const unsigned grid = (unsigned)((P.n + kBlock - 1) / kBlock);
-    if (dtype == B2B_F32)
-      model_step_kernel<M, float><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
-    else
-      model_step_kernel<M, double><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+    // four neurons per thread once that still gives every SM several CTAs' worth of warps
+    const bool wide = P.n / 4 >= (int64_t)kNumSMs * 4 * kBlock;
+    const unsigned grid = (unsigned)((P.n / (wide ? 4 : 1) + kBlock - 1) / kBlock);
+    if (dtype == B2B_F32) {
+      if (wide) model_step_kernel<M, float, 4><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      else model_step_kernel<M, float, 1><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+    } else {
+      if (wide) model_step_kernel<M, double, 4><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+      else model_step_kernel<M, double, 1><<<grid, kBlock, 0, s>>>(P, clock, k, dt, status);
+    }
   } else {
     const unsigned grid = 2 * kNumSMs;
     if (dtype == B2B_F32)

@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include "neuron_common.cuh"
+#include "pending_body.cuh"
 
 namespace b2b {
 
@@ -48,16 +49,16 @@ __device__ __forceinline__ void fold_clear(R* a, int64_t q) {
 
 // ---- LIF, exact integration ------------------------------------------------------------
 // INPUTS: the population has TimedArray or PoissonInput inputs (compiled out otherwise).
+// The work of CTA `blk` of the update (blockDim.x threads, E neurons each).
 template <typename R, int E, bool INPUTS>
-__global__ void __launch_bounds__(kBlock)
-lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
-                int32_t* status) {
+__device__ __forceinline__ void lif_step_body(const PopDev& P, const int64_t* __restrict__ clock,
+                                              int k, double dt, int32_t* status, int64_t blk) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
   const double inv_dt = 1.0 / dt;
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t nthr = P.n / E;
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t q = blk * blockDim.x + threadIdx.x;
   unsigned fl = 0;
   if (q < nthr) {
     const LifDev* prm = static_cast<const LifDev*>(P.params);
@@ -113,20 +114,26 @@ lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     fold_clear<R, E>(fgi, q);
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
-  clear_next_slot(P, ts);
+  clear_next_slot(P, ts, blk);
+}
+
+template <typename R, int E, bool INPUTS>
+__global__ void __launch_bounds__(kBlock)
+lif_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
+                int32_t* status) {
+  lif_step_body<R, E, INPUTS>(P, clock, k, dt, status, blockIdx.x);
 }
 
 // ---- Hodgkin-Huxley (COBAHH), exponential Euler (hh_advance) ------------------------
 template <typename R, int E, bool INPUTS>
-__global__ void __launch_bounds__(kBlock)
-hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
-               int32_t* status) {
+__device__ __forceinline__ void hh_step_body(const PopDev& P, const int64_t* __restrict__ clock,
+                                             int k, double dt, int32_t* status, int64_t blk) {
   const int64_t ts = clock[0] + k;
   const double t = (double)ts * dt;
   const double inv_dt = 1.0 / dt;
   const int slot = ring_slot(ts, P.ring_len);
   const int64_t nthr = P.n / E;
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t q = blk * blockDim.x + threadIdx.x;
   unsigned fl = 0;
   if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
@@ -178,7 +185,51 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
     fold_clear<R, E>(fgi, q);
   }
   emit_spikes<E>(P, q, fl, ts, slot, status);
-  clear_next_slot(P, ts);
+  clear_next_slot(P, ts, blk);
+}
+
+template <typename R, int E, bool INPUTS>
+__global__ void __launch_bounds__(kBlock)
+hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
+               int32_t* status) {
+  hh_step_body<R, E, INPUTS>(P, clock, k, dt, status, blockIdx.x);
+}
+
+// ---- one launch per step (nets of the two-launch form, pending.cu) --------------------
+// The update of step t and the delivery of step t into the pending input are independent
+// (pending.cu); here they are one grid: CTAs [0, n_upd) do the per-step update (one neuron
+// per thread, folding in the input pending from step t-1), the CTAs after them deliver the
+// bundles due at step t into acc[t & 1].  Consecutive steps are consecutive launches on one
+// stream, so one launch boundary orders step t+1 after both halves of step t, where the two
+// concurrent launches need a boundary each and dependencies across two streams.
+template <typename R, int KIND, int GROUP>
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 4)
+one_launch_step_kernel(const __grid_constant__ PopDev U, const __grid_constant__ PendingDev F,
+                       const int64_t* __restrict__ clock, int k, double dt, int32_t* status,
+                       int n_upd) {
+  static_assert(kBlock == kPendingBlock, "one block size for both halves");
+  if ((int)blockIdx.x < n_upd) {
+    if constexpr (KIND == KIND_HH)
+      hh_step_body<R, 1, false>(U, clock, k, dt, status, blockIdx.x);
+    else
+      lif_step_body<R, 1, false>(U, clock, k, dt, status, blockIdx.x);
+  } else {
+    deliver_pending_body<R, true, GROUP>(F, clock, k, (int64_t)blockIdx.x - n_upd,
+                                         (int64_t)gridDim.x - n_upd, nullptr);
+  }
+}
+
+template <typename R, int KIND>
+cudaError_t launch_one_r(const PopDev& U, const PendingDev& F, unsigned grid,
+                         const int64_t* clock, int k, double dt, int32_t* status, int n_upd,
+                         cudaStream_t s) {
+  if (F.group == 16)
+    one_launch_step_kernel<R, KIND, 16><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
+  else if (F.group == 4)
+    one_launch_step_kernel<R, KIND, 4><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
+  else
+    one_launch_step_kernel<R, KIND, 8><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
+  return cudaGetLastError();
 }
 
 // Large HH populations: a persistent grid (resident CTAs only) walks the population in
@@ -426,6 +477,25 @@ cudaError_t launch_pop_step_dev(const Pop& pop, const PopDev& dev, const int64_t
   if (e == 4) return launch_e<4, false>(pop, dev, clock, k, dt, status, s);
   if (e == 2) return launch_e<2, false>(pop, dev, clock, k, dt, status, s);
   return launch_e<1, false>(pop, dev, clock, k, dt, status, s);
+}
+
+bool one_launch_supported(const Pop& pop, const PendingDev& F) {
+  return (pop.kind == KIND_LIF || pop.kind == KIND_HH) && !pop.inputs && !pop.surr_img &&
+         F.nd_max <= kWarpPrefixMaxDelays;
+}
+
+cudaError_t launch_one_launch_step(const Pop& pop, const PopDev& U, const PendingDev& F,
+                                   int deliver_ctas, const int64_t* clock, int k, double dt,
+                                   int32_t* status, cudaStream_t s) {
+  if (!one_launch_supported(pop, F) || deliver_ctas < 1) return cudaErrorInvalidValue;
+  const int n_upd = (int)((U.n + kBlock - 1) / kBlock);
+  const unsigned grid = (unsigned)(n_upd + deliver_ctas);
+  const bool f32 = pop.dtype == B2B_F32;
+  if (pop.kind == KIND_HH)
+    return f32 ? launch_one_r<float, KIND_HH>(U, F, grid, clock, k, dt, status, n_upd, s)
+               : launch_one_r<double, KIND_HH>(U, F, grid, clock, k, dt, status, n_upd, s);
+  return f32 ? launch_one_r<float, KIND_LIF>(U, F, grid, clock, k, dt, status, n_upd, s)
+             : launch_one_r<double, KIND_LIF>(U, F, grid, clock, k, dt, status, n_upd, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -162,6 +162,10 @@ __device__ __forceinline__ void emit_spikes_warp(const PopDev& P, int64_t q, uns
 __device__ __forceinline__ void clear_next_slot(const PopDev& P, int64_t ts) {
   if (blockIdx.x == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
 }
+// The same from CTA `blk` of the update when the update's CTAs are not the whole grid.
+__device__ __forceinline__ void clear_next_slot(const PopDev& P, int64_t ts, int64_t blk) {
+  if (blk == 0 && threadIdx.x == 0) P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
+}
 
 }  // namespace
 }  // namespace b2b

@@ -17,14 +17,11 @@
 // value Brian2's schedule produces (state after step t's update plus every effect of step t's
 // synapses slot).  A fold kernel at the end of every chunk of steps adds the pending input
 // into the target variables, so between chunks the state is the ordinary one.
-#include "delivery.cuh"
+#include "pending_body.cuh"
 
 namespace b2b {
 
 namespace {
-
-constexpr int kPendingBlock = 256;
-constexpr int kPendingUnroll = 4;   // rounds of a bundle whose loads a lane issues together
 
 // Bundles due at step clock+k (spikes of steps ts - d, d >= 1) added into acc[ts & 1].
 template <typename R, bool WARP_PREFIX, int GROUP>
@@ -32,36 +29,7 @@ __global__ void __launch_bounds__(kPendingBlock)
 deliver_pending_kernel(const __grid_constant__ PendingDev F, const int64_t* __restrict__ clock,
                        int k) {
   extern __shared__ int s_pref[];  // F.nd_max + 1 ints when !WARP_PREFIX
-  const int64_t ts = clock[0] + k;
-  const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t row = (int64_t)(ts & 1) * F.pop.n;
-  const int glane = (threadIdx.x & 31) % GROUP;
-  for (int p = 0; p < F.n_proj; ++p) {
-    const ProjDev& J = F.proj[p];
-    const R* W = static_cast<const R*>(J.w);
-    MemberCache<R> mc;
-    for_each_due_item<WARP_PREFIX, GROUP>(J, ts, warp0, nwarps, s_pref,
-                                          [&](int64_t b0, int64_t b1, int64_t len, int32_t pre) {
-      member_lookup<R>(J, pre, mc);
-      // the loads of kPendingUnroll rounds first, then their atomics
-      for (int64_t off = 0; off < len; off += kPendingUnroll * GROUP) {
-        int32_t post[kPendingUnroll];
-        R w[kPendingUnroll];
-        bool v[kPendingUnroll];
-#pragma unroll
-        for (int u = 0; u < kPendingUnroll; ++u) {
-          const int64_t s = b0 + off + u * GROUP + glane;
-          v[u] = s < b1;
-          post[u] = v[u] ? __ldg(J.post + s) : 0;
-          w[u] = v[u] && W ? __ldg(W + s) : mc.w;
-        }
-#pragma unroll
-        for (int u = 0; u < kPendingUnroll; ++u)
-          if (v[u]) atomicAdd(mc.target + row + post[u], w[u]);
-      }
-    });
-  }
+  deliver_pending_body<R, WARP_PREFIX, GROUP>(F, clock, k, blockIdx.x, gridDim.x, s_pref);
 }
 
 // Adds the input delivered in step clock+k_last into the target variables and zeroes it.

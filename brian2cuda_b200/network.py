@@ -164,7 +164,7 @@ class Network:
     def __init__(self, dt: float, seed: int = 0, device: int = 0, steps_per_graph: int = 50,
                  graphs: bool = True, checked: bool = False, reset_before_synapses: bool = False,
                  stream: int | None = None, two_launch: bool | None = None,
-                 small: bool = False):
+                 small: bool = False, one_launch: bool = False):
         """`stream`: raw cudaStream_t (e.g. torch.cuda.Stream().cuda_stream) to run on; by
         default the network creates its own non-blocking stream.  `two_launch`: True runs every
         step as two concurrent launches (the neuron update, and the delivery of earlier
@@ -173,7 +173,9 @@ class Network:
         most 2^18 neurons, until autotune() picks the faster form.  `small`: run
         a small network (one LIF/HH population of <= 4096 neurons, additive synapses onto
         itself) in one CTA per chunk of steps with the state in shared memory; it pays off for
-        nets of a few hundred to ~2000 neurons with few delays."""
+        nets of a few hundred to ~2000 neurons with few delays.  `one_launch`: where the net
+        allows the two launches (and every projection has at most 64 delays, no TimedArray or
+        PoissonInput drives the population), run both halves of every step as one launch."""
         self._lib = N.lib()
         self.dt = float(dt)
         flags = (0 if graphs else N.NET_NO_GRAPH) | (N.NET_CHECKED if checked else 0)
@@ -185,6 +187,8 @@ class Network:
             flags |= N.NET_PER_STEP
         if small:
             flags |= N.NET_SMALL
+        if one_launch:
+            flags |= N.NET_ONE_LAUNCH
         cfg = N.Config(self.dt, device, steps_per_graph, seed, stream, flags, 0)
         h = C.c_void_p()
         st = self._lib.b2b_create(C.byref(cfg), C.byref(h))
@@ -455,11 +459,12 @@ class Network:
 
     @property
     def run_mode(self) -> str:
-        """'two-launch' (two concurrent launches per step), 'small' (one CTA runs every step
-        of a chunk) or 'per-step' (graph-replayed kernels)."""
+        """'two-launch' (two concurrent launches per step), 'one-launch' (both halves of a
+        step in one launch), 'small' (one CTA runs every step of a chunk) or 'per-step'
+        (graph-replayed kernels)."""
         m = C.c_int32()
         self._check(self._lib.b2b_run_mode(self._h, C.byref(m)), "run_mode")
-        return {1: "two-launch", 2: "small"}.get(m.value, "per-step")
+        return {1: "two-launch", 2: "small", 3: "one-launch"}.get(m.value, "per-step")
 
     @property
     def kernel_launches(self) -> int:

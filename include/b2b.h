@@ -75,8 +75,15 @@ enum {
                              per-step kernels only for nets of a few hundred to ~2000
                              neurons with few delays (measured: 500-neuron CUBA 3.8 vs
                              4.9 us per step); otherwise per-step kernels                */
-  B2B_NET_PER_STEP = 32   /* always the per-step kernels (one launch per population, then
+  B2B_NET_PER_STEP = 32,  /* always the per-step kernels (one launch per population, then
                              the delivery), never the two concurrent launches             */
+  B2B_NET_ONE_LAUNCH = 64 /* where the net allows the two concurrent launches (see
+                             B2B_NET_TWO_LAUNCH) and every projection has at most 64
+                             delays, no TimedArray or PoissonInput drives the population and
+                             no gating surrogate is attached: run both halves of a step as
+                             one launch (the update's CTAs, then the delivery's), one launch
+                             boundary per step on the net's stream; b2b_autotune otherwise
+                             picks among the three forms                                  */
 };
 
 typedef struct {
@@ -352,7 +359,8 @@ b2b_status b2b_time(b2b_net* net, int64_t* timestep, double* t);
 /* Number of kernels launched so far by b2b_run (eager launches plus graph kernel nodes). */
 b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
 /* How b2b_run advances the net (after b2b_finalize): *mode = 1 for every step as two
- * concurrent launches (B2B_NET_TWO_LAUNCH, or chosen automatically), 2 for a small network run by
+ * concurrent launches (B2B_NET_TWO_LAUNCH, or chosen automatically), 3 for both halves of
+ * every step as one launch (B2B_NET_ONE_LAUNCH or the autotuner), 2 for a small network run by
  * one CTA per chunk of steps, 0 for per-step kernels replayed from CUDA graphs. */
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,
@@ -366,7 +374,8 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * on_post delivery (kind 3), one per population with a deferred reset (kind 4), the rate
  * monitors (kind 10, one launch for all); or, when the net runs every step as two
  * concurrent launches (b2b_run_mode 1), the delivery into the pending input (kind 5) and the
- * neuron update folding it in (kind 1), launched one after the other; or, for a small network
+ * neuron update folding it in (kind 1), launched one after the other; or, in the one-launch
+ * form (b2b_run_mode 3), the one kernel of the step (kind 13); or, for a small network
  * run by one CTA (b2b_run_mode 2), that kernel advancing one step (kind 7).  *n_sites receives the number
  * of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
@@ -394,14 +403,16 @@ b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int
  * records (0 synapse order, 1 grouped by postsynaptic neuron, where on_post reads contiguous
  * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
  * through the order); a net that can run every step as two concurrent launches: the pending
- * delivery's lanes per item x CTAs (kind 5), then the form itself (kind 11: 1 two launches,
- * 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
+ * delivery's lanes per item x CTAs (kind 5), then the form itself (kind 11: choice_a 2 one
+ * launch per step holding both halves, with choice_b delivering CTAs after the update's; 1 two
+ * launches; 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
  * and the next b2b_run captures its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
  * rule) to be chosen.  A choice of 0 means the built-in rule won.  The trials should cover a
  * representative stretch of the run (bursts included). */
 typedef struct {
   int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records,
-                            5 pending delivery of the two-launch step, 11 step form,
+                            5 pending delivery of the two-launch step, 11 step form
+                            (0 per-step kernels, 1 two launches, 2 one launch),
                             12 additive delivery launch accumulated in the distributed
                             shared memory of 8-CTA thread-block clusters (choice_a 1) or
                             with one global atomic per event (0); float32 launches onto

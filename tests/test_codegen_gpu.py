@@ -25,8 +25,9 @@ def _close(a, b, rtol, atol, what=""):
 
 def test_alpha_synapse_network_matches_oracle(gpu_factory, oracle_factory):
     """A second-order (alpha) synapse LIF network, integrated exactly by generated code, with
-    recurrent synapses onto the synaptic variable y and delays of 1-8 steps."""
-    s = Script(dt=DT, seed=11, namespace=ALPHA_NS)
+    recurrent synapses onto the synaptic variable y and delays of 1-8 steps (resting
+    potential 1 mV above threshold: every neuron fires repeatedly)."""
+    s = Script(dt=DT, seed=11, namespace=dict(ALPHA_NS, El=-49e-3))
     G = s.NeuronGroup(2000, ALPHA_EQS, threshold="v > Vt", reset="v = Vr", refractory=2e-3)
     G.v = "Vr + rand() * 22*mV"
     S = s.Synapses(G, G, on_pre="y += 0.9*mV")
@@ -47,23 +48,28 @@ def test_alpha_synapse_network_matches_oracle(gpu_factory, oracle_factory):
         _close(g["st"][v][1], o["st"][v][1], 1e-9, 1e-15, v)
 
 
-def test_noisy_adaptive_network_matches_oracle(gpu_factory, oracle_factory):
+@pytest.mark.parametrize("n,synapses,chunks", [(1500, True, 6), (700_000, False, 2)])
+def test_noisy_adaptive_network_matches_oracle(gpu_factory, oracle_factory, n, synapses,
+                                               chunks):
     """Euler-Maruyama with the GPU's cuRAND normal numbers fed to the oracle, a two-statement
     reset, refractoriness, and synapses onto v (a variable the reset writes: the reset is
-    deferred until after the delivery, as in Brian2's schedule)."""
+    deferred until after the delivery, as in Brian2's schedule).  7e5 neurons without
+    synapses (the oracle's connect visits every pair): the generated kernel's
+    four-neurons-per-thread form."""
     K = 50
     s = Script(dt=DT, seed=5, namespace=ADAPT_NS)
-    G = s.NeuronGroup(1500, ADAPT_EQS, threshold="v > Vt", reset="v = Vr; w += b",
+    G = s.NeuronGroup(n, ADAPT_EQS, threshold="v > Vt", reset="v = Vr; w += b",
                       refractory=2e-3)
     G.v = "El + rand()*20*mV"
-    S = s.Synapses(G, G, on_pre="v += 0.3*mV", delay=2e-4)
-    S.connect(p=0.02)
+    if synapses:
+        S = s.Synapses(G, G, on_pre="v += 0.3*mV", delay=2e-4)
+        S.connect(p=0.02)
     s.SpikeMonitor(G, name="spk")
     prog = s.lower()
     gnet = gpu_factory(DT, seed=s.seed, steps_per_graph=K)
     onet = oracle_factory(DT)
     gids, oids = prog.build(gnet), prog.build(onet)
-    for _ in range(6):
+    for _ in range(chunks):
         gnet.run(K)
         onet.set_normals(oids[G.name], gnet.rng_normals(gids[G.name], K, 1))
         onet.run(K)
@@ -115,7 +121,9 @@ def test_generated_cobahh_matches_the_handwritten_kernel(gpu_factory):
         assert ("model_group" in kinds) == gen and ("hh_group" in kinds) != gen
         net = gpu_factory(DT, seed=s.seed)
         res = prog.execute(net)
-        out[gen] = (res["spikes"], net.get_state(0, "v"))
+        # the generated model's state slots follow its own order (synaptic targets first)
+        v_slot = prog.groups[h["P"].name]["slots"]["v"]
+        out[gen] = (res["spikes"], net.get_state(0, v_slot))
     (gi, gs), gv = out[True]
     (hi, hs), hv = out[False]
     assert len(hi) > 1000

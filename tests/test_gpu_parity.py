@@ -455,30 +455,41 @@ def test_store_restore_replays_identically(gpu_factory):
     assert len(idx1) > 50
 
 
-def test_two_launch_and_per_step_paths_agree(gpu_factory):
+# the three forms of a step for nets whose every delay is >= 1 step: Network kwargs
+FORMS = {"per-step": dict(two_launch=False), "two-launch": dict(two_launch=True),
+         "one-launch": dict(one_launch=True)}
+
+
+def test_step_forms_agree(gpu_factory):
+    """The per-step kernels, the two concurrent launches and the one launch holding both
+    halves of a step compute the same network (float64 LIF, delays 1-16 steps; a chunk
+    boundary mid-run)."""
     res = {}
-    for two_launch in (True, False):
-        net = gpu_factory(DT, two_launch=two_launch)
+    for form, kw in FORMS.items():
+        net = gpu_factory(DT, **kw)
         G, Ce, Ci, _ = _delay_net(net, n=1000)
         net.finalize()
-        assert net.run_mode == ("two-launch" if two_launch else "per-step")
+        assert net.run_mode == form
         net.run(150)
         net.run(89)
         idx, st = net.spikes(G)
-        res[two_launch] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
-    for k in (0, 1, 4):
-        np.testing.assert_array_equal(res[True][k], res[False][k])
-    _close(res[True][2], res[False][2], 1e-10, 1e-15)
-    _close(res[True][3], res[False][3], 1e-10, 1e-15)
+        res[form] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
+    assert len(res["per-step"][0]) > 100
+    for form in ("two-launch", "one-launch"):
+        for k in (0, 1, 4):
+            np.testing.assert_array_equal(res[form][k], res["per-step"][k])
+        _close(res[form][2], res["per-step"][2], 1e-10, 1e-15)
+        _close(res[form][3], res["per-step"][3], 1e-10, 1e-15)
 
 
 def test_profile_advances_like_run(gpu_factory):
     """The profiling run launches every kernel eagerly and times it; in either form of the
     step it reports the form's launch sites and leaves the net where b2b_run would."""
-    for two_launch in (True, False):
+    sites = {"per-step": [1, 6, 6], "two-launch": [5, 1], "one-launch": [13]}
+    for form, kw in FORMS.items():
         out = {}
         for how in ("run", "profile"):
-            net = gpu_factory(DT, two_launch=two_launch)
+            net = gpu_factory(DT, **kw)
             G, Ce, Ci, _ = _delay_net(net, n=1000)
             net.finalize()
             net.run(40)
@@ -489,7 +500,7 @@ def test_profile_advances_like_run(gpu_factory):
                 kinds = [k for k, _ in prof]
                 # per-step: Ce (a weight per synapse) and Ci (one scalar weight) are two
                 # kernel variants, so two delivery launches
-                assert kinds == ([5, 1] if two_launch else [1, 6, 6]), kinds
+                assert kinds == sites[form], kinds
                 assert all(ms > 0 for _, ms in prof)
             assert net.timestep == 170
             net.run(30)
@@ -507,10 +518,11 @@ def test_profile_graph_advances_like_run(gpu_factory):
     the net where b2b_run would, and the per-site times fit inside the step: in the per-step
     form the sites run one after another, so their sum is at most the step time; in the
     two-launch form each of the two overlapping sites is."""
-    for two_launch in (True, False):
+    sites = {"per-step": [1, 6, 6], "two-launch": [5, 1], "one-launch": [13]}
+    for form, kw in FORMS.items():
         out = {}
         for how in ("run", "profile"):
-            net = gpu_factory(DT, two_launch=two_launch, steps_per_graph=25)
+            net = gpu_factory(DT, steps_per_graph=25, **kw)
             G, Ce, Ci, _ = _delay_net(net, n=1000)
             net.finalize()
             net.run(40)
@@ -519,9 +531,9 @@ def test_profile_graph_advances_like_run(gpu_factory):
             else:
                 prof, step_ms = net.profile_graph(150)
                 kinds = [k for k, _ in prof]
-                assert kinds == ([5, 1] if two_launch else [1, 6, 6]), kinds
+                assert kinds == sites[form], kinds
                 assert all(ms > 0 for _, ms in prof) and step_ms > 0
-                if two_launch:
+                if form == "two-launch":
                     assert max(ms for _, ms in prof) <= step_ms
                 else:
                     assert sum(ms for _, ms in prof) <= step_ms
@@ -543,14 +555,15 @@ def _spikes_within_one_step(a_idx, a_stp, b_idx, b_stp):
     return hit / max(1, len(a_idx))
 
 
-def test_two_launch_cobahh_float32_matches_oracle(gpu_factory, oracle_factory):
+@pytest.mark.parametrize("form", ["two-launch", "one-launch"])
+def test_two_launch_cobahh_float32_matches_oracle(gpu_factory, oracle_factory, form):
     out = {}
     for name, make in (("gpu", gpu_factory), ("orc", oracle_factory)):
-        net = make(DT, f32=True) if name == "orc" else make(DT, two_launch=True)
+        net = make(DT, f32=True) if name == "orc" else make(DT, **FORMS[form])
         ids = models.build_cobahh(net, n=3000, p=0.02, generated=False, monitor_capacity=10**6)
         net.finalize()
         if name == "gpu":
-            assert net.run_mode == "two-launch"
+            assert net.run_mode == form
         net.run(60)
         out[name] = (net.spikes(ids["P"]), {v: net.get_state(ids["P"], v)
                                             for v in ("v", "m", "h", "n", "ge", "gi")})
@@ -607,12 +620,13 @@ def test_autotune_keeps_state_and_results(gpu_factory):
 
 
 def test_autotune_chooses_step_form(gpu_factory):
-    """A net that allows both forms of the step (one population, additive synapses onto ge
-    and gi, delays >= 1): the tuner tunes the per-step kernels and the two concurrent
-    launches, keeps the faster form (site kind 11), leaves the state as it was, and either
-    form computes the same network; tune_apply reproduces each form."""
+    """A net that allows every form of the step (one population, additive synapses onto ge
+    and gi, delays >= 1): the tuner tunes the per-step kernels, the two concurrent launches
+    and the one launch, keeps the fastest form (site kind 11), leaves the state as it was, and
+    every form computes the same network; tune_apply reproduces each form."""
     out = {}
-    for mode in ("untuned", "tuned", "per-step", "two launches"):
+    mode_of = {0: "per-step", 1: "two-launch", 2: "one-launch"}
+    for mode in ("untuned", "tuned", "per-step", "two launches", "one launch"):
         net = gpu_factory(DT)
         G, Ce, Ci, _ = _delay_net(net, n=800)
         net.finalize()
@@ -624,18 +638,19 @@ def test_autotune_chooses_step_form(gpu_factory):
             kinds = [r["site_kind"] for r in res]
             assert {1, 6, 5, 11} <= set(kinds), kinds
             form = [r for r in res if r["site_kind"] == 11][0]
-            assert net.run_mode == ("two-launch" if form["choice_a"] == 1 else "per-step")
+            assert net.run_mode == mode_of[form["choice_a"]]
             np.testing.assert_array_equal(net.get_state(G, "v"), v0)
             assert net.timestep == 60
         elif mode != "untuned":
-            net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_b": 0,
-                             "choice_a": 1 if mode == "two launches" else 0}])
-            assert net.run_mode == ("two-launch" if mode == "two launches" else "per-step")
+            a = {"per-step": 0, "two launches": 1, "one launch": 2}[mode]
+            net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_a": a,
+                             "choice_b": 148 if a == 2 else 0}])
+            assert net.run_mode == mode_of[a]
         net.run(240)
         idx, st = net.spikes(G)
         out[mode] = (idx, st, net.get_state(G, "v"))
     assert len(out["untuned"][0]) > 100
-    for mode in ("tuned", "per-step", "two launches"):
+    for mode in ("tuned", "per-step", "two launches", "one launch"):
         np.testing.assert_array_equal(out[mode][1], out["untuned"][1])
         np.testing.assert_array_equal(out[mode][0], out["untuned"][0])
         _close(out[mode][2], out["untuned"][2], 1e-10, 1e-15)
