@@ -64,7 +64,7 @@ def test_noisy_adaptive_network_matches_oracle(gpu_factory, oracle_factory, n, s
     if synapses:
         S = s.Synapses(G, G, on_pre="v += 0.3*mV", delay=2e-4)
         S.connect(p=0.02)
-    s.SpikeMonitor(G, name="spk")
+    s.SpikeMonitor(G, capacity=max(10**6, n), name="spk")   # the runs are made by hand
     prog = s.lower()
     gnet = gpu_factory(DT, seed=s.seed, steps_per_graph=K)
     onet = oracle_factory(DT)
