@@ -880,8 +880,11 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
     cudaStream_t s = net->stream;
     for (int k = 0; k < kk; ++k) {
       CU(prof_mark(net, k, 0, 0, s));
+      // the first step of a chunk follows other kernels (the previous chunk's fold and
+      // clock tick): an ordinary launch
       CU(launch_one_launch_step(pop, net->fold_dev, net->pdev, net->one_launch_grid,
-                                net->d_clock, k, net->cfg.dt, net->d_status, s));
+                                net->one_launch_chained && k > 0, net->d_clock, k, net->cfg.dt,
+                                net->d_status, s));
       CU(prof_mark(net, k, 0, 1, s));
       ++net->launches;
     }
@@ -1797,7 +1800,7 @@ b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* 
                                     net->stream);
       if (s.kind == 13)
         e = launch_one_launch_step(net->pops[0], net->fold_dev, net->pdev, net->one_launch_grid,
-                                   clk, 0, net->cfg.dt, net->d_status, net->stream);
+                                   false, clk, 0, net->cfg.dt, net->d_status, net->stream);
       cudaEventRecord(ev[2 * k + 1], net->stream);
       if (e != cudaSuccess) result = fail(net, B2B_ERR_CUDA, "profile launch: %s", cudaGetErrorString(e));
       ++net->launches;
@@ -2211,19 +2214,29 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         }
       }
       set_one_launch_grid(net, one_grid);
-      net->one_launch = false;
     }
-    // the form of the step: 0 per-step kernels, 1 two concurrent launches, 2 one launch; the
-    // built-in form stays unless another is 2 % faster
-    const double form_ms[3] = {per_step_ms, two_launch_ms, one_launch_ms};
+    // the same, each step's launch chained to the previous one (programmatic dependent launch)
+    double chained_ms = 1e30;
+    if (net->one_launch_ok && st == B2B_OK) {
+      net->one_launch_chained = true;
+      set_one_launch_grid(net, one_grid);
+      st = trial(&chained_ms);
+      net->one_launch_chained = false;
+      set_one_launch_grid(net, one_grid);
+    }
+    net->one_launch = false;
+    // the form of the step: 0 per-step kernels, 1 two concurrent launches, 2 one launch, 3 one
+    // launch chained; the built-in form stays unless another is 2 % faster
+    const double form_ms[4] = {per_step_ms, two_launch_ms, one_launch_ms, chained_ms};
     const int builtin = builtin_two_launch ? (builtin_one_launch ? 2 : 1) : 0;
     int other = -1;
-    for (int f = 0; f < 3; ++f)
+    for (int f = 0; f < 4; ++f)
       if (f != builtin && (other < 0 || form_ms[f] < form_ms[other])) other = f;
     const int form = form_ms[other] < kTuneMargin * form_ms[builtin] ? other : builtin;
     net->two_launch = form >= 1;
-    net->one_launch = form == 2;
-    res.push_back(b2b_tune_result{11, 0, form, form == 2 ? one_grid : 0, form_ms[form],
+    net->one_launch = form >= 2;
+    net->one_launch_chained = form == 3;
+    res.push_back(b2b_tune_result{11, 0, form, form >= 2 ? one_grid : 0, form_ms[form],
                                   form_ms[builtin]});
   }
   // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
@@ -2249,6 +2262,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   if (st != B2B_OK && net->two_launch_ok) {
     net->two_launch = builtin_two_launch;
     net->one_launch = builtin_one_launch;
+    net->one_launch_chained = false;
   }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
@@ -2308,13 +2322,14 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             t.site_index);
       net->add_tune[t.site_index].cluster = t.choice_a;
     } else if (t.site_kind == 11) {
-      CHECK(net->two_launch_ok && t.site_index == 0 && t.choice_a >= 0 && t.choice_a <= 2,
+      CHECK(net->two_launch_ok && t.site_index == 0 && t.choice_a >= 0 && t.choice_a <= 3,
             B2B_ERR_INVALID_ARG, "site kind 11 exists only for nets that allow both step forms");
-      CHECK(t.choice_a != 2 || (net->one_launch_ok && t.choice_b >= 0 && t.choice_b <= 65535),
+      CHECK(t.choice_a < 2 || (net->one_launch_ok && t.choice_b >= 0 && t.choice_b <= 65535),
             B2B_ERR_INVALID_ARG, "the net does not allow the one-launch step");
       net->two_launch = t.choice_a >= 1;
-      net->one_launch = t.choice_a == 2;
-      if (t.choice_a == 2) set_one_launch_grid(net, t.choice_b);
+      net->one_launch = t.choice_a >= 2;
+      net->one_launch_chained = t.choice_a == 3;
+      if (t.choice_a >= 2) set_one_launch_grid(net, t.choice_b);
     } else if (t.site_kind == 5) {
       CHECK(net->two_launch_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
             "site kind 5 exists only for nets that allow two launches per step");

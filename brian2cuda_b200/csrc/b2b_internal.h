@@ -373,6 +373,7 @@ struct b2b_net {
   bool one_launch = false;
   bool one_launch_ok = false;
   int one_launch_grid = 0;
+  bool one_launch_chained = false;         // programmatic dependent launch between steps
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
   std::vector<void*> pending_allocs;
@@ -430,11 +431,13 @@ cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* 
 // fold of the pending input at the end of a chunk.
 cudaError_t launch_pending_delivery(const PendingDev& F, int dtype, int grid,
                                     const int64_t* clock, int k, cudaStream_t s);
-// The step as one launch (neuron.cu): the update's CTAs, then deliver_ctas delivering CTAs.
+// The step as one launch (neuron.cu): the update's CTAs, then deliver_ctas delivering CTAs
+// (counted in CTAs of kBlock threads); chained: with programmatic dependent launch on the
+// previous launch of the stream.
 bool one_launch_supported(const Pop& pop, const PendingDev& F);
 cudaError_t launch_one_launch_step(const Pop& pop, const PopDev& U, const PendingDev& F,
-                                   int deliver_ctas, const int64_t* clock, int k, double dt,
-                                   int32_t* status, cudaStream_t s);
+                                   int deliver_ctas, bool chained, const int64_t* clock, int k,
+                                   double dt, int32_t* status, cudaStream_t s);
 cudaError_t launch_fold_pending(const PendingDev& F, int dtype, const int64_t* clock, int k_last,
                                 cudaStream_t s);
 }  // namespace b2b

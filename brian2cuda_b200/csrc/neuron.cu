@@ -202,34 +202,63 @@ hh_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 // bundles due at step t into acc[t & 1].  Consecutive steps are consecutive launches on one
 // stream, so one launch boundary orders step t+1 after both halves of step t, where the two
 // concurrent launches need a boundary each and dependencies across two streams.
-template <typename R, int KIND, int GROUP>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 4)
+template <typename R, int KIND, int E, int GROUP>
+__global__ void __launch_bounds__(kBlock, E == 1 ? (sizeof(R) == 4 ? 5 : 4) : 3)
 one_launch_step_kernel(const __grid_constant__ PopDev U, const __grid_constant__ PendingDev F,
                        const int64_t* __restrict__ clock, int k, double dt, int32_t* status,
                        int n_upd) {
-  static_assert(kBlock == kPendingBlock, "one block size for both halves");
+  // chained launches (programmatic dependent launch): wait for the previous step's grid to
+  // complete and its memory to be visible, then let the next step's grid be scheduled, so its
+  // CTAs are resident by the time this one ends; without that launch attribute both are no-ops
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;");
   if ((int)blockIdx.x < n_upd) {
     if constexpr (KIND == KIND_HH)
-      hh_step_body<R, 1, false>(U, clock, k, dt, status, blockIdx.x);
+      hh_step_body<R, E, false>(U, clock, k, dt, status, blockIdx.x);
     else
-      lif_step_body<R, 1, false>(U, clock, k, dt, status, blockIdx.x);
+      lif_step_body<R, E, false>(U, clock, k, dt, status, blockIdx.x);
   } else {
     deliver_pending_body<R, true, GROUP>(F, clock, k, (int64_t)blockIdx.x - n_upd,
                                          (int64_t)gridDim.x - n_upd, nullptr);
   }
 }
 
-template <typename R, int KIND>
-cudaError_t launch_one_r(const PopDev& U, const PendingDev& F, unsigned grid,
-                         const int64_t* clock, int k, double dt, int32_t* status, int n_upd,
-                         cudaStream_t s) {
+template <typename R, int KIND, int E, int GROUP>
+cudaError_t launch_one_g(const PopDev& U, const PendingDev& F, unsigned grid, int block,
+                         bool chained, const int64_t* clock, int k, double dt, int32_t* status,
+                         int n_upd, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = chained ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, one_launch_step_kernel<R, KIND, E, GROUP>, U, F, clock, k,
+                            dt, status, n_upd);
+}
+
+template <typename R, int KIND, int E>
+cudaError_t launch_one_r(const PopDev& U, const PendingDev& F, unsigned grid, int block,
+                         bool chained, const int64_t* clock, int k, double dt, int32_t* status,
+                         int n_upd, cudaStream_t s) {
   if (F.group == 16)
-    one_launch_step_kernel<R, KIND, 16><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
-  else if (F.group == 4)
-    one_launch_step_kernel<R, KIND, 4><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
-  else
-    one_launch_step_kernel<R, KIND, 8><<<grid, kBlock, 0, s>>>(U, F, clock, k, dt, status, n_upd);
-  return cudaGetLastError();
+    return launch_one_g<R, KIND, E, 16>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
+  if (F.group == 4)
+    return launch_one_g<R, KIND, E, 4>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
+  return launch_one_g<R, KIND, E, 8>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
+}
+
+template <int KIND, int E>
+cudaError_t launch_one_k(const PopDev& U, const PendingDev& F, bool f32, unsigned grid,
+                         int block, bool chained, const int64_t* clock, int k, double dt,
+                         int32_t* status, int n_upd, cudaStream_t s) {
+  return f32 ? launch_one_r<float, KIND, E>(U, F, grid, block, chained, clock, k, dt, status,
+                                            n_upd, s)
+             : launch_one_r<double, KIND, E>(U, F, grid, block, chained, clock, k, dt, status,
+                                             n_upd, s);
 }
 
 // Large HH populations: a persistent grid (resident CTAs only) walks the population in
@@ -485,17 +514,26 @@ bool one_launch_supported(const Pop& pop, const PendingDev& F) {
 }
 
 cudaError_t launch_one_launch_step(const Pop& pop, const PopDev& U, const PendingDev& F,
-                                   int deliver_ctas, const int64_t* clock, int k, double dt,
-                                   int32_t* status, cudaStream_t s) {
+                                   int deliver_ctas, bool chained, const int64_t* clock, int k,
+                                   double dt, int32_t* status, cudaStream_t s) {
   if (!one_launch_supported(pop, F) || deliver_ctas < 1) return cudaErrorInvalidValue;
-  const int n_upd = (int)((U.n + kBlock - 1) / kBlock);
-  const unsigned grid = (unsigned)(n_upd + deliver_ctas);
+  // the update half takes the population's tuned shape (neurons per thread 1 or 2, 128 or
+  // 256 threads per CTA); the delivery half the same threads per CTA, deliver_ctas counted
+  // in CTAs of kBlock threads
+  const int e = pop.tune_e == 2 || pop.tune_e == 4 ? 2 : 1;
+  const int block = pop.tune_block > 0 ? pop.tune_block : kBlock;
+  const int n_upd = (int)((U.n / e + block - 1) / block);
+  const unsigned grid = (unsigned)(n_upd + (int64_t)deliver_ctas * kBlock / block);
   const bool f32 = pop.dtype == B2B_F32;
   if (pop.kind == KIND_HH)
-    return f32 ? launch_one_r<float, KIND_HH>(U, F, grid, clock, k, dt, status, n_upd, s)
-               : launch_one_r<double, KIND_HH>(U, F, grid, clock, k, dt, status, n_upd, s);
-  return f32 ? launch_one_r<float, KIND_LIF>(U, F, grid, clock, k, dt, status, n_upd, s)
-             : launch_one_r<double, KIND_LIF>(U, F, grid, clock, k, dt, status, n_upd, s);
+    return e == 2 ? launch_one_k<KIND_HH, 2>(U, F, f32, grid, block, chained, clock, k, dt,
+                                             status, n_upd, s)
+                  : launch_one_k<KIND_HH, 1>(U, F, f32, grid, block, chained, clock, k, dt,
+                                             status, n_upd, s);
+  return e == 2 ? launch_one_k<KIND_LIF, 2>(U, F, f32, grid, block, chained, clock, k, dt,
+                                            status, n_upd, s)
+                : launch_one_k<KIND_LIF, 1>(U, F, f32, grid, block, chained, clock, k, dt,
+                                            status, n_upd, s);
 }
 
 cudaError_t launch_pop_late_reset(const Pop& pop, const int64_t* clock, int k, cudaStream_t s) {

@@ -404,15 +404,17 @@ b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int
  * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
  * through the order); a net that can run every step as two concurrent launches: the pending
  * delivery's lanes per item x CTAs (kind 5), then the form itself (kind 11: choice_a 2 one
- * launch per step holding both halves, with choice_b delivering CTAs after the update's; 1 two
- * launches; 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
+ * launch per step holding both halves, with choice_b delivering CTAs after the update's, 3 the
+ * same with each step's launch chained to the previous one by programmatic dependent launch;
+ * 1 two launches; 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
  * and the next b2b_run captures its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
  * rule) to be chosen.  A choice of 0 means the built-in rule won.  The trials should cover a
  * representative stretch of the run (bursts included). */
 typedef struct {
   int32_t site_kind;     /* 1 population, 6 additive delivery launch, 8 STDP records,
                             5 pending delivery of the two-launch step, 11 step form
-                            (0 per-step kernels, 1 two launches, 2 one launch),
+                            (0 per-step kernels, 1 two launches, 2 one launch,
+                            3 one launch chained),
                             12 additive delivery launch accumulated in the distributed
                             shared memory of 8-CTA thread-block clusters (choice_a 1) or
                             with one global atomic per event (0); float32 launches onto

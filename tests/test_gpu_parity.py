@@ -465,17 +465,22 @@ def test_step_forms_agree(gpu_factory):
     halves of a step compute the same network (float64 LIF, delays 1-16 steps; a chunk
     boundary mid-run)."""
     res = {}
-    for form, kw in FORMS.items():
+    for form, kw in list(FORMS.items()) + [("chained", FORMS["one-launch"])]:
         net = gpu_factory(DT, **kw)
         G, Ce, Ci, _ = _delay_net(net, n=1000)
         net.finalize()
-        assert net.run_mode == form
+        if form == "chained":
+            # each step's launch chained to the previous one (programmatic dependent launch)
+            net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_a": 3, "choice_b": 148}])
+            assert net.run_mode == "one-launch"
+        else:
+            assert net.run_mode == form
         net.run(150)
         net.run(89)
         idx, st = net.spikes(G)
         res[form] = (idx, st, net.get_state(G, "v"), net.get_state(G, "ge"), net.queue(Ce))
     assert len(res["per-step"][0]) > 100
-    for form in ("two-launch", "one-launch"):
+    for form in ("two-launch", "one-launch", "chained"):
         for k in (0, 1, 4):
             np.testing.assert_array_equal(res[form][k], res["per-step"][k])
         _close(res[form][2], res["per-step"][2], 1e-10, 1e-15)
@@ -625,8 +630,8 @@ def test_autotune_chooses_step_form(gpu_factory):
     and the one launch, keeps the fastest form (site kind 11), leaves the state as it was, and
     every form computes the same network; tune_apply reproduces each form."""
     out = {}
-    mode_of = {0: "per-step", 1: "two-launch", 2: "one-launch"}
-    for mode in ("untuned", "tuned", "per-step", "two launches", "one launch"):
+    mode_of = {0: "per-step", 1: "two-launch", 2: "one-launch", 3: "one-launch"}
+    for mode in ("untuned", "tuned", "per-step", "two launches", "one launch", "chained"):
         net = gpu_factory(DT)
         G, Ce, Ci, _ = _delay_net(net, n=800)
         net.finalize()
@@ -642,15 +647,15 @@ def test_autotune_chooses_step_form(gpu_factory):
             np.testing.assert_array_equal(net.get_state(G, "v"), v0)
             assert net.timestep == 60
         elif mode != "untuned":
-            a = {"per-step": 0, "two launches": 1, "one launch": 2}[mode]
+            a = {"per-step": 0, "two launches": 1, "one launch": 2, "chained": 3}[mode]
             net.tune_apply([{"site_kind": 11, "site_index": 0, "choice_a": a,
-                             "choice_b": 148 if a == 2 else 0}])
+                             "choice_b": 148 if a >= 2 else 0}])
             assert net.run_mode == mode_of[a]
         net.run(240)
         idx, st = net.spikes(G)
         out[mode] = (idx, st, net.get_state(G, "v"))
     assert len(out["untuned"][0]) > 100
-    for mode in ("tuned", "per-step", "two launches", "one launch"):
+    for mode in ("tuned", "per-step", "two launches", "one launch", "chained"):
         np.testing.assert_array_equal(out[mode][1], out["untuned"][1])
         np.testing.assert_array_equal(out[mode][0], out["untuned"][0])
         _close(out[mode][2], out["untuned"][2], 1e-10, 1e-15)
