@@ -1069,6 +1069,8 @@ def bench_small(args, world, rank, local):
                      "timing": "CUDA events on the net's stream around the runs (one "
                                "kernel per 1000-step chunk)",
                      "gpu_launches": args.steps * (steps_run // 1000), "clocks": clk})
+        line["roofline"]["timing"] = ("CUDA events on the net's stream around the runs, per "
+                                      "8000-step run (eight launches of 1000 steps)")
         line["roofline"]["note"] = ("achieved = algorithmic 136 B per compartment-step / time; "
                                     "the kernel keeps the state in shared memory, so HBM is "
                                     "not what bounds it")
