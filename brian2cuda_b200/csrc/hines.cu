@@ -64,6 +64,10 @@ struct HinesDev {
   int32_t* spikes;
   int32_t* above;
   double Cm, dt, El, EK, ENa, gl, gNa, gK, Vthr;
+  // neuron of CTA k: neurons by decreasing estimated cost, so that the CTAs the block
+  // scheduler starts last (when fewer than all neurons fit on the GPU at once) are the
+  // shortest
+  const int32_t* order;
 };
 
 template <typename RC>
@@ -106,7 +110,7 @@ template <typename RC>
 __global__ void __launch_bounds__(kHinesBlock)
 hines_kernel(HinesDev H, int n_steps, int write_currents) {
   extern __shared__ __align__(16) uint8_t sm[];
-  const int b = blockIdx.x;
+  const int b = H.order[blockIdx.x];
   const int tid = threadIdx.x, bs = blockDim.x;
   const int64_t c0 = H.comp_off[b];
   const int nc = (int)(H.comp_off[b + 1] - c0);
@@ -506,6 +510,18 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     up(&D.g0, g0); up(&D.gn, gn); up(&D.rhs_first, rfirst); up(&D.rhs_last, rlast);
     up(&D.child_off, child_off); up(&D.child_sec, child_sec);
     up(&D.level_rec, level_rec); up(&D.level_off, level_off);
+    // cost of a neuron's step: the node system walks its levels on one warp (~1000 cycles
+    // per level, the largest phase), the compartment-parallel phases grow with its size
+    std::vector<int32_t> order(n_neurons);
+    std::vector<double> cost(n_neurons);
+    for (int b = 0; b < n_neurons; ++b) {
+      order[b] = b;
+      cost[b] = 1000.0 * (lvl_base[b + 1] - lvl_base[b] - 1) +
+                15.0 * (double)(comp_off[b + 1] - comp_off[b]);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t c) { return cost[a] > cost[c]; });
+    up(&D.order, order);
     std::vector<double> zeros_d(n_comp, 0.0), zero_I(n_neurons, 0.0);
     std::vector<int32_t> zeros_i(n_neurons, 0);
     const double* cv = nullptr;
