@@ -294,10 +294,6 @@ b2b_status finalize_pops(b2b_net* net) {
       CU(cudaMemcpy(pop.params_dev, prm.data(), prm.size(), cudaMemcpyHostToDevice));
       D.params = pop.params_dev;
     }
-    if (pop.kind == KIND_LIF && prm.size() >= sizeof(LifDev))
-      std::memcpy(&D.g0.lif, prm.data(), sizeof(LifDev));
-    if (pop.kind == KIND_HH && prm.size() >= sizeof(HhDev))
-      std::memcpy(&D.g0.hh, prm.data(), sizeof(HhDev));
     if (pop.inputs) {
       GroupInputs* d = nullptr;
       CU(dalloc(pop, &d, gins.size()));

@@ -114,12 +114,6 @@ struct PopDev {
   // The step as two concurrent launches (pending.cu): per variable (v, ge, gi), [2][n] input
   // delivered during the previous step, which the update adds in and clears (NULL: none).
   void* fold[3];
-  // LIF / HH: the first group's parameters by value, which the per-step kernels of a
-  // one-group population (vec_group == NULL) read from their parameter space
-  union {
-    LifDev lif;
-    HhDev hh;
-  } g0;
 };
 
 // Device view of a projection (merged Synapses objects with one source population, one

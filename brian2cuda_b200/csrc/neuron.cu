@@ -63,10 +63,7 @@ __device__ __forceinline__ void lif_step_body(const PopDev& P, const int64_t* __
   if (q < nthr) {
     const LifDev* prm = static_cast<const LifDev*>(P.params);
     const int grp = group_of<E>(P, q);
-    // one group: its parameters from the kernel's parameter space (no dependent load)
-    LifDev g;
-    if (P.vec_group) g = prm[grp];
-    else g = P.g0.lif;
+    const LifDev g = prm[grp];
     const GroupInputs* gin = INPUTS ? P.inputs + grp : nullptr;
     const bool after_reset = INPUTS && gin->pin.after_reset;
     const R Vt = (R)g.Vt, Vr = (R)g.Vr;
@@ -141,10 +138,7 @@ __device__ __forceinline__ void hh_step_body(const PopDev& P, const int64_t* __r
   if (q < nthr) {
     const HhDev* prm = static_cast<const HhDev*>(P.params);
     const int grp = group_of<E>(P, q);
-    // one group: its parameters from the kernel's parameter space (no dependent load)
-    HhRun<R> g;
-    if (P.vec_group) g = hh_run(prm[grp], R());
-    else g = hh_run(P.g0.hh, R());
+    const HhRun<R> g = hh_run(prm[grp], R());
     const GroupInputs* gin = INPUTS ? P.inputs + grp : nullptr;
     const R Vthr = (R)g.Vthr, dtR = (R)dt;
     const bool refr = g.ref_steps >= 0;
