@@ -346,6 +346,14 @@ struct b2b_hines {
   int64_t n_comp = 0;
   int32_t n_neurons = 0;
   size_t smem = 0;
+  // Neurons whose shared-memory image fits five CTAs per SM run as a second launch of their
+  // own size beside the others (on stream2, forked from and joined to the net's stream), so
+  // that small neurons do not reserve the largest neuron's shared memory.
+  int32_t n_large = 0;                   // CTAs of the first launch (all neurons when 1 class)
+  b2b::HinesDev dev_small{};
+  size_t smem_small = 0;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<double> soma_area;
   std::vector<void*> allocs;
   std::string err;
@@ -394,6 +402,7 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     // r: cross section over half the length; g: axial conductance into c from c - 1
     std::vector<double> area(n_comp), rl(n_comp), g(n_comp + 1, 0.0);
     std::vector<double> soma_area(n_neurons);
+    std::vector<int> nlev_of(n_neurons, 0);
     int nc_max = 0, ns_max = 0, nlev_max = 0;
     const double Ri = p->Ri, Cm = p->Cm;
     for (int b = 0; b < n_neurons; ++b) {
@@ -451,6 +460,7 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       for (int s = 0; s < ns; ++s) depth[s + 1] = depth[spn[s0 + s]] + 1;
       const int nlev = *std::max_element(depth.begin(), depth.end()) + 1;
       nlev_max = std::max(nlev_max, nlev);
+      nlev_of[b] = nlev;
       const int edge_base = (int)child_sec.size();
       std::vector<int> first_edge(nB + 1);
       for (int i = 0; i < nB; ++i) {
@@ -519,9 +529,46 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       cost[b] = 1000.0 * (lvl_base[b + 1] - lvl_base[b] - 1) +
                 15.0 * (double)(comp_off[b + 1] - comp_off[b]);
     }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t a, int32_t c) { return cost[a] > cost[c]; });
+    // two classes by shared-memory image: those that fit five CTAs per SM, and the rest; each
+    // class in decreasing order of cost, the large class first
+    int sm_bytes = 0, reserved = 0;
+    cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, net->cfg.device);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, net->cfg.device);
+    const size_t small_cap = sm_bytes > 0 ? (size_t)(sm_bytes / 5 - reserved) : 0;
+    std::vector<char> small(n_neurons, 0);
+    int n_small = 0;
+    for (int b = 0; b < n_neurons; ++b) {
+      const int nc = (int)(comp_off[b + 1] - comp_off[b]), ns = sec_off[b + 1] - sec_off[b];
+      small[b] = hines_smem(nc, ns, nlev_of[b], rc) <= small_cap ? 1 : 0;
+      n_small += small[b];
+    }
+    if (n_small == 0 || n_small == n_neurons || smem <= small_cap)
+      std::fill(small.begin(), small.end(), 0);   // one class, one launch
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
+      if (small[a] != small[c]) return small[a] < small[c];
+      return cost[a] > cost[c];
+    });
+    int n_large = 0, ncs = 0, nss = 0, nls = 0, ncl = 0, nsl = 0, nll = 0;
+    for (int b = 0; b < n_neurons; ++b) {
+      const int nc = (int)(comp_off[b + 1] - comp_off[b]), ns = sec_off[b + 1] - sec_off[b];
+      if (small[b]) {
+        ncs = std::max(ncs, nc); nss = std::max(nss, ns); nls = std::max(nls, nlev_of[b]);
+      } else {
+        ++n_large;
+        ncl = std::max(ncl, nc); nsl = std::max(nsl, ns); nll = std::max(nll, nlev_of[b]);
+      }
+    }
     up(&D.order, order);
+    h->n_large = n_large;
+    if (n_large < n_neurons) {
+      // the large class's image bounds its own arrays; the small class has its own bounds
+      D.nc_max = ncl; D.ns_max = nsl; D.nlev_max = nll;
+      h->smem = hines_smem(ncl, nsl, nll, rc);
+      h->smem_small = hines_smem(ncs, nss, nls, rc);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+    }
     std::vector<double> zeros_d(n_comp, 0.0), zero_I(n_neurons, 0.0);
     std::vector<int32_t> zeros_i(n_neurons, 0);
     const double* cv = nullptr;
@@ -535,6 +582,12 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       if (e != cudaSuccess) break;
       e = cudaMalloc(g, rc * std::max<int64_t>(n_comp, 1));
       if (e == cudaSuccess) { h->allocs.push_back(*g); e = cudaMemset(*g, 0, rc * n_comp); }
+    }
+    if (n_large < n_neurons) {
+      // the small class: the same arrays, its own bounds and its part of the order
+      h->dev_small = D;
+      h->dev_small.nc_max = ncs; h->dev_small.ns_max = nss; h->dev_small.nlev_max = nls;
+      h->dev_small.order = D.order + n_large;
     }
     if (e == cudaSuccess)
       e = rc == 4 ? cudaFuncSetAttribute(hines_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
@@ -600,12 +653,31 @@ b2b_status b2b_hines_run(b2b_hines* h, int64_t n_steps) {
   while (n_steps > 0) {
     const int k = (int)std::min<int64_t>(n_steps, kHinesMaxStepsPerLaunch);
     const int wc = n_steps == k ? 1 : 0;
-    if (h->channel_dtype == B2B_F32)
-      hines_kernel<float><<<h->n_neurons, kHinesBlock, h->smem, h->net->stream>>>(h->dev, k, wc);
-    else
-      hines_kernel<double><<<h->n_neurons, kHinesBlock, h->smem, h->net->stream>>>(h->dev, k, wc);
+    cudaStream_t s = h->net->stream;
+    const bool two = h->n_large < h->n_neurons;
+    if (two) {
+      if (cudaEventRecord(h->ev_fork, s) != cudaSuccess) return B2B_ERR_CUDA;
+      if (cudaStreamWaitEvent(h->stream2, h->ev_fork, 0) != cudaSuccess) return B2B_ERR_CUDA;
+    }
+    if (h->channel_dtype == B2B_F32) {
+      if (h->n_large > 0)
+        hines_kernel<float><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (two)
+        hines_kernel<float><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+                              h->stream2>>>(h->dev_small, k, wc);
+    } else {
+      if (h->n_large > 0)
+        hines_kernel<double><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (two)
+        hines_kernel<double><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+                               h->stream2>>>(h->dev_small, k, wc);
+    }
     if (cudaGetLastError() != cudaSuccess) return B2B_ERR_CUDA;
-    h->net->launches += 1;
+    if (two) {
+      if (cudaEventRecord(h->ev_join, h->stream2) != cudaSuccess) return B2B_ERR_CUDA;
+      if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return B2B_ERR_CUDA;
+    }
+    h->net->launches += two ? 2 : 1;
     n_steps -= k;
   }
   return B2B_OK;
@@ -627,6 +699,12 @@ b2b_status b2b_hines_destroy(b2b_hines* h) {
     auto& v = h->net->hines;
     v.erase(std::remove(v.begin(), v.end(), h), v.end());
   }
+  if (h->stream2) {
+    cudaStreamSynchronize(h->stream2);
+    cudaStreamDestroy(h->stream2);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   for (void* a : h->allocs) cudaFree(a);
   delete h;
   return B2B_OK;
