@@ -285,7 +285,8 @@ def main():
                          "COBAHH instances, plain vs batched vs batched + gating surrogate")
     ap.add_argument("--kernel-case", default=None,
                     choices=["hh4m", "surrogate1m", "mlp_train", "propagation",
-                             "propagation3000", "stdp", "stdp_synorder", "hines", "model"],
+                             "propagation3000", "stdp", "stdp_synorder", "hines", "model",
+                             "batched"],
                     help="profiling case of one kernel (see kernel_case); prints nothing")
     args = ap.parse_args()
     if args.kernel_case:
@@ -640,7 +641,7 @@ def bench_batched(args, world, rank, local):
     for g, o, n in zip(ids["groups"], offs, sizes):
         outdeg[o:o + int(n)] = net.out_degree(g)
     net.run(300)
-    tune = net.autotune(trial_steps=20)
+    tune = net.autotune(trial_steps=100)
     start = net.spikes_recorded(ids["groups"][0])
     clocks = Clocks(local)
     ms_total, launches = timed(net, args.steps)
@@ -1102,7 +1103,8 @@ def kernel_case(name: str):
     stdp_synorder = the STDP workload with its records grouped by postsynaptic neuron / in
     synapse order, 200 steps then 20 profiled ones (deliver_stdp_post_kernel), hines = the
     1024-neuron multicompartment batch for one 1000-step launch (hines_kernel), model = a
-    generated model (noisy adaptive LIF, 8e6 neurons, 20 steps: model_step_kernel)."""
+    generated model (noisy adaptive LIF, 8e6 neurons, 20 steps: model_step_kernel), batched =
+    the 256-instance batched workload for 500 steps (20 GB on the device: a launch list only)."""
     import torch
 
     from brian2cuda_b200 import Network, models
@@ -1160,6 +1162,16 @@ def kernel_case(name: str):
         net = Network(DT, seed=4, graphs=False)
         s.lower().build(net)
         net.run(20)
+        net.sync()
+        net.close()
+    elif name == "batched":
+        # the 256-instance batched workload with the built-in launch shapes: 300 steps (the
+        # initial burst), then 200 more (for a launch list of the quiet phase)
+        sizes, we = models.batch_sizes()
+        net = Network(DT, seed=models.SEED_BASE + 5, steps_per_graph=50)
+        models.build_cobahh_batch(net, sizes, we)
+        net.finalize()
+        net.run(500)
         net.sync()
         net.close()
     elif name == "mlp_train":
