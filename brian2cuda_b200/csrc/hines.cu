@@ -346,19 +346,14 @@ struct b2b_hines {
   int64_t n_comp = 0;
   int32_t n_neurons = 0;
   size_t smem = 0;
-  // Neurons in classes by shared-memory image (fitting 6, 5 or 4 CTAs per SM, and the
-  // rest): one launch per class, each sized for its own largest neuron, run side by side on
-  // streams forked from and joined to the net's stream, so that small neurons do not reserve
-  // the largest neuron's shared memory.  Class 0 (the largest) runs on the net's stream.
-  struct Class {
-    b2b::HinesDev dev{};
-    int32_t n = 0;                      // its CTAs
-    size_t smem = 0;
-    cudaStream_t stream = nullptr;      // NULL for class 0
-  };
-  std::vector<Class> classes;
-  cudaEvent_t ev_fork = nullptr;
-  std::vector<cudaEvent_t> ev_join;
+  // Neurons whose shared-memory image fits five CTAs per SM run as a second launch of their
+  // own size beside the others (on stream2, forked from and joined to the net's stream), so
+  // that small neurons do not reserve the largest neuron's shared memory.
+  int32_t n_large = 0;                   // CTAs of the first launch (all neurons when 1 class)
+  b2b::HinesDev dev_small{};
+  size_t smem_small = 0;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<double> soma_area;
   std::vector<void*> allocs;
   std::string err;
@@ -534,57 +529,46 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       cost[b] = 1000.0 * (lvl_base[b + 1] - lvl_base[b] - 1) +
                 15.0 * (double)(comp_off[b + 1] - comp_off[b]);
     }
-    // classes by shared-memory image: fitting 6, 5 or 4 CTAs per SM, and the rest; each
-    // class in decreasing order of cost, the largest class first
+    // two classes by shared-memory image: those that fit five CTAs per SM, and the rest; each
+    // class in decreasing order of cost, the large class first
     int sm_bytes = 0, reserved = 0;
     cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, net->cfg.device);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, net->cfg.device);
-    constexpr int kClasses = 4;
-    const int per_sm[kClasses - 1] = {4, 5, 6};   // classes 1..3; class 0 takes the rest
-    std::vector<int> cls(n_neurons, 0);
+    const size_t small_cap = sm_bytes > 0 ? (size_t)(sm_bytes / 5 - reserved) : 0;
+    std::vector<char> small(n_neurons, 0);
+    int n_small = 0;
     for (int b = 0; b < n_neurons; ++b) {
       const int nc = (int)(comp_off[b + 1] - comp_off[b]), ns = sec_off[b + 1] - sec_off[b];
-      const size_t need = hines_smem(nc, ns, nlev_of[b], rc);
-      for (int c = kClasses - 1; c >= 1; --c)
-        if (sm_bytes > 0 && need <= (size_t)(sm_bytes / per_sm[c - 1] - reserved)) {
-          cls[b] = c;
-          break;
-        }
+      small[b] = hines_smem(nc, ns, nlev_of[b], rc) <= small_cap ? 1 : 0;
+      n_small += small[b];
     }
+    if (n_small == 0 || n_small == n_neurons || smem <= small_cap)
+      std::fill(small.begin(), small.end(), 0);   // one class, one launch
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
-      if (cls[a] != cls[c]) return cls[a] < cls[c];
+      if (small[a] != small[c]) return small[a] < small[c];
       return cost[a] > cost[c];
     });
-    int cnt[kClasses] = {0}, cnc[kClasses] = {0}, cns[kClasses] = {0}, clv[kClasses] = {0};
+    int n_large = 0, ncs = 0, nss = 0, nls = 0, ncl = 0, nsl = 0, nll = 0;
     for (int b = 0; b < n_neurons; ++b) {
-      const int c = cls[b];
-      ++cnt[c];
-      cnc[c] = std::max(cnc[c], (int)(comp_off[b + 1] - comp_off[b]));
-      cns[c] = std::max(cns[c], sec_off[b + 1] - sec_off[b]);
-      clv[c] = std::max(clv[c], nlev_of[b]);
+      const int nc = (int)(comp_off[b + 1] - comp_off[b]), ns = sec_off[b + 1] - sec_off[b];
+      if (small[b]) {
+        ncs = std::max(ncs, nc); nss = std::max(nss, ns); nls = std::max(nls, nlev_of[b]);
+      } else {
+        ++n_large;
+        ncl = std::max(ncl, nc); nsl = std::max(nsl, ns); nll = std::max(nll, nlev_of[b]);
+      }
     }
     up(&D.order, order);
-    int base = 0;
-    for (int c = 0; c < kClasses; ++c) {
-      if (!cnt[c]) continue;
-      b2b_hines::Class k;
-      k.n = cnt[c];
-      k.smem = hines_smem(cnc[c], cns[c], clv[c], rc);
-      k.dev.nc_max = cnc[c];     // the rest of dev is filled in below, once D is complete
-      k.dev.ns_max = cns[c];
-      k.dev.nlev_max = clv[c];
-      k.dev.n_neurons = base;    // offset of the class in the order, until then
-      base += cnt[c];
-      if (!h->classes.empty() && e == cudaSuccess) {
-        e = cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking);
-        cudaEvent_t ev = nullptr;
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-        h->ev_join.push_back(ev);
-      }
-      h->classes.push_back(k);
+    h->n_large = n_large;
+    if (n_large < n_neurons) {
+      // the large class's image bounds its own arrays; the small class has its own bounds
+      D.nc_max = ncl; D.ns_max = nsl; D.nlev_max = nll;
+      h->smem = hines_smem(ncl, nsl, nll, rc);
+      h->smem_small = hines_smem(ncs, nss, nls, rc);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
     }
-    if (h->classes.size() > 1 && e == cudaSuccess)
-      e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
     std::vector<double> zeros_d(n_comp, 0.0), zero_I(n_neurons, 0.0);
     std::vector<int32_t> zeros_i(n_neurons, 0);
     const double* cv = nullptr;
@@ -599,13 +583,11 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       e = cudaMalloc(g, rc * std::max<int64_t>(n_comp, 1));
       if (e == cudaSuccess) { h->allocs.push_back(*g); e = cudaMemset(*g, 0, rc * n_comp); }
     }
-    for (b2b_hines::Class& k : h->classes) {
-      // the same arrays; the class's own bounds and its part of the order
-      const int32_t off = k.dev.n_neurons;
-      const int32_t ncm = k.dev.nc_max, nsm = k.dev.ns_max, nlm = k.dev.nlev_max;
-      k.dev = D;
-      k.dev.nc_max = ncm; k.dev.ns_max = nsm; k.dev.nlev_max = nlm;
-      k.dev.order = D.order + off;
+    if (n_large < n_neurons) {
+      // the small class: the same arrays, its own bounds and its part of the order
+      h->dev_small = D;
+      h->dev_small.nc_max = ncs; h->dev_small.ns_max = nss; h->dev_small.nlev_max = nls;
+      h->dev_small.order = D.order + n_large;
     }
     if (e == cudaSuccess)
       e = rc == 4 ? cudaFuncSetAttribute(hines_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
@@ -672,28 +654,30 @@ b2b_status b2b_hines_run(b2b_hines* h, int64_t n_steps) {
     const int k = (int)std::min<int64_t>(n_steps, kHinesMaxStepsPerLaunch);
     const int wc = n_steps == k ? 1 : 0;
     cudaStream_t s = h->net->stream;
-    const size_t nk = h->classes.size();
-    if (nk > 1) {
+    const bool two = h->n_large < h->n_neurons;
+    if (two) {
       if (cudaEventRecord(h->ev_fork, s) != cudaSuccess) return B2B_ERR_CUDA;
-      for (size_t c = 1; c < nk; ++c)
-        if (cudaStreamWaitEvent(h->classes[c].stream, h->ev_fork, 0) != cudaSuccess)
-          return B2B_ERR_CUDA;
+      if (cudaStreamWaitEvent(h->stream2, h->ev_fork, 0) != cudaSuccess) return B2B_ERR_CUDA;
     }
-    for (size_t c = 0; c < nk; ++c) {
-      const b2b_hines::Class& K = h->classes[c];
-      cudaStream_t ks = c == 0 ? s : K.stream;
-      if (h->channel_dtype == B2B_F32)
-        hines_kernel<float><<<K.n, kHinesBlock, K.smem, ks>>>(K.dev, k, wc);
-      else
-        hines_kernel<double><<<K.n, kHinesBlock, K.smem, ks>>>(K.dev, k, wc);
+    if (h->channel_dtype == B2B_F32) {
+      if (h->n_large > 0)
+        hines_kernel<float><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (two)
+        hines_kernel<float><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+                              h->stream2>>>(h->dev_small, k, wc);
+    } else {
+      if (h->n_large > 0)
+        hines_kernel<double><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (two)
+        hines_kernel<double><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+                               h->stream2>>>(h->dev_small, k, wc);
     }
     if (cudaGetLastError() != cudaSuccess) return B2B_ERR_CUDA;
-    for (size_t c = 1; c < nk; ++c) {
-      if (cudaEventRecord(h->ev_join[c - 1], h->classes[c].stream) != cudaSuccess)
-        return B2B_ERR_CUDA;
-      if (cudaStreamWaitEvent(s, h->ev_join[c - 1], 0) != cudaSuccess) return B2B_ERR_CUDA;
+    if (two) {
+      if (cudaEventRecord(h->ev_join, h->stream2) != cudaSuccess) return B2B_ERR_CUDA;
+      if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return B2B_ERR_CUDA;
     }
-    h->net->launches += (int64_t)nk;
+    h->net->launches += two ? 2 : 1;
     n_steps -= k;
   }
   return B2B_OK;
@@ -715,14 +699,12 @@ b2b_status b2b_hines_destroy(b2b_hines* h) {
     auto& v = h->net->hines;
     v.erase(std::remove(v.begin(), v.end(), h), v.end());
   }
-  for (b2b_hines::Class& k : h->classes)
-    if (k.stream) {
-      cudaStreamSynchronize(k.stream);
-      cudaStreamDestroy(k.stream);
-    }
+  if (h->stream2) {
+    cudaStreamSynchronize(h->stream2);
+    cudaStreamDestroy(h->stream2);
+  }
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-  for (cudaEvent_t ev : h->ev_join)
-    if (ev) cudaEventDestroy(ev);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   for (void* a : h->allocs) cudaFree(a);
   delete h;
   return B2B_OK;
