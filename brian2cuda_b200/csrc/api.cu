@@ -2130,7 +2130,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
     AddTune& t = net->add_tune[b];
     std::vector<std::pair<int, int>> cands = {{0, 0}};
-    for (int g : {4, 8, 16, 32})
+    for (int g : {2, 4, 8, 16, 32})
       for (int mult : {1, 2, 4, 8, 16}) cands.push_back({g, mult * sms / 2});
     b2b_tune_result r{6, (int32_t)b, 0, 0, 0.0, 0.0};
     double best = 1e30;
@@ -2179,7 +2179,7 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     // the step's delivery launch: lanes per work item x CTAs (the neuron launch has one
     // thread per neuron)
     std::vector<std::pair<int, int>> cands = {{0, 0}};
-    for (int g : {4, 8, 16})
+    for (int g : {2, 4, 8, 16})
       for (int mult : {1, 2, 4}) cands.push_back({g, mult * sms / 2});
     b2b_tune_result r{5, 0, 0, 0, 0.0, 0.0};
     double best = 1e30;
@@ -2342,8 +2342,8 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
     } else if (t.site_kind == 6) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->add_batches.size(),
             B2B_ERR_INVALID_ARG, "bad delivery launch index %d", t.site_index);
-      CHECK((t.choice_a == 0 || t.choice_a == 4 || t.choice_a == 8 || t.choice_a == 16 ||
-             t.choice_a == 32) &&
+      CHECK((t.choice_a == 0 || t.choice_a == 2 || t.choice_a == 4 || t.choice_a == 8 ||
+             t.choice_a == 16 || t.choice_a == 32) &&
                 t.choice_b >= 0 && t.choice_b <= 65535,
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       net->add_tune[t.site_index].group = t.choice_a;
@@ -2369,7 +2369,8 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
     } else if (t.site_kind == 5) {
       CHECK(net->two_launch_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
             "site kind 5 exists only for nets that allow two launches per step");
-      CHECK((t.choice_a == 0 || t.choice_a == 4 || t.choice_a == 8 || t.choice_a == 16) &&
+      CHECK((t.choice_a == 0 || t.choice_a == 2 || t.choice_a == 4 || t.choice_a == 8 ||
+             t.choice_a == 16) &&
                 t.choice_b >= 0 && t.choice_b <= 65535,
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       set_pending_shape(net, t.choice_a, t.choice_b);

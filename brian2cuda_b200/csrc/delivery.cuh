@@ -75,6 +75,27 @@ __device__ __forceinline__ int find_delay_warp(const DuePrefix& p, int sp, int* 
   return di;
 }
 
+// The same for every lane's own sp at once (lanes may ask for different spikes): the count
+// of delay indices whose inclusive prefix is <= sp, found by binary lifting over the 64
+// prefix values spread over the warp (lane l holds indices l and 32 + l), 14 shuffles.  Every
+// lane of the warp must call this.
+__device__ __forceinline__ int find_delay_lane(const DuePrefix& p, int sp, int* rank) {
+  int di = 0;
+#pragma unroll
+  for (int b = 32; b >= 1; b >>= 1) {
+    const int probe = di + b - 1;              // is the prefix through index probe <= sp?
+    const int a0 = __shfl_sync(kFull, p.incl0, probe & 31);
+    const int a1 = __shfl_sync(kFull, p.incl1, probe & 31);
+    if ((probe < 32 ? a0 : a1) <= sp) di += b;
+  }
+  const int src = (di - 1) & 31;
+  const int v0 = __shfl_sync(kFull, p.incl0, src);
+  const int v1 = __shfl_sync(kFull, p.incl1, src);
+  const int excl = di == 0 ? 0 : (di - 1 < 32 ? v0 : v1);
+  *rank = sp - excl;
+  return di;
+}
+
 // Per-CTA prefix in shared memory (any nd): s_pref[0] = 0, s_pref[i] = counts of delay
 // indices < i.  Every thread of the CTA must call this.
 __device__ __forceinline__ int due_prefix_block(const int32_t* __restrict__ ring_cnt,
@@ -121,7 +142,8 @@ __device__ __forceinline__ int find_delay_block(const int* s_pref, int nd, int s
 template <bool WARP_PREFIX, int GROUP = 32, class Item>
 __device__ __forceinline__ void for_each_due_item(const ProjDev& J, int64_t ts, int64_t warp0,
                                                   int64_t nwarps, int* s_pref, Item item) {
-  static_assert(GROUP == 32 || GROUP == 16 || GROUP == 8 || GROUP == 4, "group size");
+  static_assert(GROUP == 32 || GROUP == 16 || GROUP == 8 || GROUP == 4 || GROUP == 2,
+                "group size");
   constexpr int G = 32 / GROUP;  // items per warp per round
   const int lane = threadIdx.x & 31;
   const int grp = lane / GROUP;
@@ -143,7 +165,9 @@ __device__ __forceinline__ void for_each_due_item(const ProjDev& J, int64_t ts, 
     const int sp = have ? (int)(it / J.chunks) : 0;
     const int ch = have ? (int)(it - (int64_t)sp * J.chunks) : 0;
     int kk = 0, di = 0;
-    if constexpr (WARP_PREFIX) {
+    if constexpr (WARP_PREFIX && G >= 4) {
+      di = find_delay_lane(wp, sp, &kk);     // one search for all groups of the warp
+    } else if constexpr (WARP_PREFIX) {
 #pragma unroll
       for (int g = 0; g < G; ++g) {
         int r;

@@ -248,6 +248,8 @@ cudaError_t launch_one_r(const PopDev& U, const PendingDev& F, unsigned grid, in
     return launch_one_g<R, KIND, E, 16>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
   if (F.group == 4)
     return launch_one_g<R, KIND, E, 4>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
+  if (F.group == 2)
+    return launch_one_g<R, KIND, E, 2>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
   return launch_one_g<R, KIND, E, 8>(U, F, grid, block, chained, clock, k, dt, status, n_upd, s);
 }
 

@@ -57,6 +57,8 @@ cudaError_t launch_pending_r(const PendingDev& F, dim3 g, size_t smem, const int
     deliver_pending_kernel<R, WP, 16><<<g, kPendingBlock, smem, s>>>(F, clock, k);
   else if (F.group == 4)
     deliver_pending_kernel<R, WP, 4><<<g, kPendingBlock, smem, s>>>(F, clock, k);
+  else if (F.group == 2)
+    deliver_pending_kernel<R, WP, 2><<<g, kPendingBlock, smem, s>>>(F, clock, k);
   else
     deliver_pending_kernel<R, WP, 8><<<g, kPendingBlock, smem, s>>>(F, clock, k);
   return cudaGetLastError();

@@ -233,13 +233,14 @@ void launch_add_g(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem,
                                                                                          k);
 }
 
-// Lanes per work item: 8 (four items in flight per warp, the default), 4, 16 or 32.
+// Lanes per work item: 8 (four items in flight per warp, the default), 2, 4, 16 or 32.
 template <typename R, bool HAS_W, bool AGG>
 void launch_add(const ProjBatch& B, dim3 g, bool warp_prefix, size_t smem, const int64_t* clock,
                 int k, cudaStream_t s, int group) {
   if (group == 32) launch_add_g<R, HAS_W, AGG, 32>(B, g, warp_prefix, smem, clock, k, s);
   else if (group == 16) launch_add_g<R, HAS_W, AGG, 16>(B, g, warp_prefix, smem, clock, k, s);
   else if (group == 4) launch_add_g<R, HAS_W, AGG, 4>(B, g, warp_prefix, smem, clock, k, s);
+  else if (group == 2) launch_add_g<R, HAS_W, AGG, 2>(B, g, warp_prefix, smem, clock, k, s);
   else launch_add_g<R, HAS_W, AGG, 8>(B, g, warp_prefix, smem, clock, k, s);
 }
 

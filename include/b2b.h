@@ -399,7 +399,7 @@ b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int
  * steps run as b2b_run runs them (graph replays), so a shape is judged by the step time it
  * gives.  Populations: neurons per thread (1, 2 or 4) x threads per CTA (128 or 256), or, with a
  * gating surrogate, CTAs per SM (2..6); additive delivery launches: lanes per work item
- * (4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM); STDP projections: the order of the synapse
+ * (2, 4, 8, 16, 32) x CTAs (1/2, 1, 2, 4, 8 per SM); STDP projections: the order of the synapse
  * records (0 synapse order, 1 grouped by postsynaptic neuron, where on_post reads contiguous
  * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
  * through the order); a net that can run every step as two concurrent launches: the pending

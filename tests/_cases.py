@@ -273,8 +273,8 @@ def threads_per_synapse_bundle(make):
     """test_synaptic_propagations.py:343-374: whatever the threads per synapse bundle, a
     spike at t = 0 with delays j*dt onto neurons 3 and 4 (v += 1.1, threshold v > 1) makes
     them spike at steps 4 and 5.  The launch-shape counterpart here is the delivery's lanes
-    per work item (4, 8, 16, 32; the oracle has one form)."""
-    shapes = [4, 8, 16, 32]
+    per work item (2, 4, 8, 16, 32; the oracle has one form)."""
+    shapes = [2, 4, 8, 16, 32]
     for lanes in shapes:
         net = make(DT)
         inp = net.spikegen_group(1, [0], [0])

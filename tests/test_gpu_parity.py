@@ -487,6 +487,31 @@ def test_step_forms_agree(gpu_factory):
         _close(res[form][3], res["per-step"][3], 1e-10, 1e-15)
 
 
+def test_delivery_lanes_per_item_agree(gpu_factory):
+    """Every delivery launch shape computes the same network: lanes per work item 2-32 for the
+    per-step delivery (site kind 6) and 2-16 for the pending delivery of the two launches
+    (site kind 5), against the built-in shapes (float64 LIF, delays 1-16 steps, bundles of a
+    few synapses)."""
+    def run(form, tune):
+        net = gpu_factory(DT, **FORMS[form])
+        G, Ce, Ci, _ = _delay_net(net, n=1000)
+        net.finalize()
+        if tune:
+            net.tune_apply(tune)
+        net.run(200)
+        idx, st = net.spikes(G)
+        return idx, st, net.get_state(G, "v")
+    for form, kind, groups in (("per-step", 6, (2, 4, 16, 32)), ("two-launch", 5, (2, 4, 16))):
+        ref = run(form, None)
+        assert len(ref[0]) > 100
+        for g in groups:
+            got = run(form, [{"site_kind": kind, "site_index": 0, "choice_a": g,
+                              "choice_b": 148}])
+            np.testing.assert_array_equal(got[1], ref[1], err_msg=f"{form} {g}")
+            np.testing.assert_array_equal(got[0], ref[0], err_msg=f"{form} {g}")
+            _close(got[2], ref[2], 1e-10, 1e-15)
+
+
 def test_profile_advances_like_run(gpu_factory):
     """The profiling run launches every kernel eagerly and times it; in either form of the
     step it reports the form's launch sites and leaves the net where b2b_run would."""
