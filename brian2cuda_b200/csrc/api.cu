@@ -777,6 +777,8 @@ b2b_status setup_small(b2b_net* net) {
   if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) return B2B_OK;
   D.ring_in_smem = 1;
   if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) D.ring_in_smem = 0;
+  D.cluster = 1;                 // one CTA until tuned (b2b_autotune, site kind 14)
+  D.slice = pop.n;
   net->small = true;
   return B2B_OK;
 }
@@ -1977,6 +1979,33 @@ constexpr double kTuneMargin = 0.98;
 
 // Launch shape of the delivery launch of a net run with two launches per step (pending.cu):
 // lanes per work item (0: 8) and CTAs (0: two per SM).
+// The small-network path as one CTA (c == 1) or one cluster of c CTAs, each holding a slice
+// of the population; false (nothing changed) when the cluster form cannot run the net.
+bool set_small_cluster(b2b_net* net, int c) {
+  SmallDev& D = net->sdev;
+  const Pop& pop = net->pops[0];
+  const int32_t c0 = D.cluster;
+  const int64_t s0 = D.slice;
+  if (c == 1) {
+    D.cluster = 1;
+    D.slice = pop.n;
+  } else {
+    if (c != 8 && c != 16) return false;
+    D.cluster = c;
+    D.slice = ((pop.n + c - 1) / c + 3) / 4 * 4;
+    if (!small_cluster_possible(D, pop.kind, pop.dtype)) {
+      D.cluster = c0;
+      D.slice = s0;
+      return false;
+    }
+  }
+  if (net->graph) {
+    cudaGraphExecDestroy(net->graph);
+    net->graph = nullptr;
+  }
+  return true;
+}
+
 void set_one_launch_grid(b2b_net* net, int grid) {
   net->one_launch_grid = grid > 0 ? grid : net->pending_grid;
   if (net->graph) {
@@ -2032,10 +2061,6 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
   if (b2b_status st = check_net(net)) return st;
   CHECK(net->finalized, B2B_ERR_STATE, "call b2b_finalize first");
   CHECK(trial_steps > 0 && trial_steps <= 100000 && n_out, B2B_ERR_INVALID_ARG, "bad arguments");
-  if (net->small) {  // one CTA with a fixed shape: nothing to tune
-    *n_out = 0;
-    return B2B_OK;
-  }
   GUARD_BEGIN
   CU(cudaStreamSynchronize(net->stream));
   // the state to start every trial from, in a slot of its own; monitor counts to put back
@@ -2081,224 +2106,251 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     double ms = 0;
     st = trial(&ms);
   }
-  int sms = kNumSMs;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
-  // a net that allows both forms of the step tunes the per-step kernels first, then the two
-  // concurrent launches, and keeps the faster form
-  const bool builtin_two_launch = net->two_launch;
-  const bool builtin_one_launch = net->two_launch && net->one_launch;
-  if (net->two_launch_ok) net->two_launch = false;
-  net->one_launch = false;
-  for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->two_launch; ++p) {
-    Pop& pop = net->pops[p];
-    if (pop.kind == KIND_SPIKEGEN || pop.kind == KIND_MODEL) continue;
-    std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
-    if (pop.surr_img) {
-      cands = {{0, 0}, {2, 0}, {3, 0}, {4, 0}, {6, 0}};
-    } else {
-      cands = {{0, 0}, {1, 128}, {1, 256}, {2, 128}, {2, 256}, {4, 128}, {4, 256}};
-    }
-    b2b_tune_result r{1, (int32_t)p, 0, 0, 0.0, 0.0};
+  if (net->small) {
+    // the small-network path: one CTA, or one thread-block cluster of 8 or 16 CTAs
+    SmallDev& D = net->sdev;
+    const int32_t c0 = D.cluster;
+    const int64_t s0 = D.slice;
+    b2b_tune_result r{14, 0, c0, 0, 0.0, 0.0};
     double best = 1e30;
-    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
-      if (pop.surr_img) {
-        pop.tune_ctas = cands[c].first;
-      } else {
-        pop.tune_e = cands[c].first;
-        pop.tune_block = cands[c].second;
-      }
+    const int sizes[] = {c0, 1, 8, 16};
+    for (int c = 0; c < 4 && st == B2B_OK; ++c) {
+      if (c > 0 && sizes[c] == c0) continue;
+      if (!set_small_cluster(net, sizes[c])) continue;
       double ms = 0;
       st = trial(&ms);
-      if (c == 0) r.default_ms = ms;
-      // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
-      // near-equal shapes differ by noise, and noise should not pick the shape
-      if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
-        best = ms;
-        r.choice_a = cands[c].first;
-        r.choice_b = cands[c].second;
-      }
-    }
-    if (pop.surr_img) {
-      pop.tune_ctas = r.choice_a;
-    } else {
-      pop.tune_e = r.choice_a;
-      pop.tune_block = r.choice_b;
-    }
-    r.best_ms = best;
-    res.push_back(r);
-  }
-  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
-    AddTune& t = net->add_tune[b];
-    std::vector<std::pair<int, int>> cands = {{0, 0}};
-    for (int g : {2, 4, 8, 16, 32})
-      for (int mult : {1, 2, 4, 8, 16}) cands.push_back({g, mult * sms / 2});
-    b2b_tune_result r{6, (int32_t)b, 0, 0, 0.0, 0.0};
-    double best = 1e30;
-    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
-      t.group = cands[c].first;
-      t.grid = cands[c].second;
-      double ms = 0;
-      st = trial(&ms);
-      if (c == 0) r.default_ms = ms;
-      // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
-      // near-equal shapes differ by noise, and noise should not pick the shape
-      if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
-        best = ms;
-        r.choice_a = cands[c].first;
-        r.choice_b = cands[c].second;
-      }
-    }
-    t.group = r.choice_a;
-    t.grid = r.choice_b;
-    r.best_ms = best;
-    res.push_back(r);
-  }
-  // additive delivery launches that can accumulate in thread-block clusters (float32, one
-  // target population): with the chosen lanes per item, cluster accumulation on or off
-  for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
-    const auto& bat = net->add_batches[b];
-    if (!add_batch_cluster_capable(bat.data(), (int)bat.size())) continue;
-    AddTune& t = net->add_tune[b];
-    b2b_tune_result r{12, (int32_t)b, 0, 0, 0.0, 0.0};
-    double off_ms = 0, on_ms = 0;
-    t.cluster = 0;
-    st = trial(&off_ms);
-    if (st != B2B_OK) break;
-    t.cluster = 1;
-    st = trial(&on_ms);
-    const bool use = st == B2B_OK && on_ms < kTuneMargin * off_ms;
-    t.cluster = use ? 1 : 0;
-    r.choice_a = t.cluster;
-    r.default_ms = off_ms;
-    r.best_ms = use ? on_ms : off_ms;
-    res.push_back(r);
-  }
-  if (net->two_launch_ok && st == B2B_OK) {
-    const double per_step_ms = res.empty() ? 1e30 : res.back().best_ms;
-    net->two_launch = true;
-    // the step's delivery launch: lanes per work item x CTAs (the neuron launch has one
-    // thread per neuron)
-    std::vector<std::pair<int, int>> cands = {{0, 0}};
-    for (int g : {2, 4, 8, 16})
-      for (int mult : {1, 2, 4}) cands.push_back({g, mult * sms / 2});
-    b2b_tune_result r{5, 0, 0, 0, 0.0, 0.0};
-    double best = 1e30;
-    for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
-      set_pending_shape(net, cands[c].first, cands[c].second);
-      double ms = 0;
-      st = trial(&ms);
-      if (c == 0) r.default_ms = ms;
-      if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
-        best = ms;
-        r.choice_a = cands[c].first;
-        r.choice_b = cands[c].second;
-      }
-    }
-    set_pending_shape(net, r.choice_a, r.choice_b);
-    r.best_ms = best;
-    res.push_back(r);
-    // the update's shape again, inside this form: the per-step form tuned it for an update
-    // followed by its own delivery, and the forms rank the shapes differently (COBAHH 1e5:
-    // 1 x 256 against 2 x 128 neurons per thread x threads, 45.8 against 37.7 ms per
-    // simulated second with two launches)
-    Pop& pop0 = net->pops[0];
-    const int ps_e = pop0.tune_e, ps_block = pop0.tune_block;
-    b2b_tune_result r1{1, 0, ps_e, ps_block, best, best};
-    {
-      const std::pair<int, int> shapes[] = {{0, 0}, {1, 128}, {1, 256}, {2, 128}, {2, 256},
-                                            {4, 128}, {4, 256}};
-      for (const auto& sh : shapes) {
-        if (st != B2B_OK) break;
-        if (sh.first == ps_e && sh.second == ps_block) continue;   // timed above
-        pop0.tune_e = sh.first;
-        pop0.tune_block = sh.second;
-        set_pending_shape(net, r.choice_a, r.choice_b);   // a fresh graph
-        double ms = 0;
-        st = trial(&ms);
-        if (st == B2B_OK && ms < kTuneMargin * r1.best_ms) {
-          r1.best_ms = ms;
-          r1.choice_a = sh.first;
-          r1.choice_b = sh.second;
-        }
-      }
-      pop0.tune_e = r1.choice_a;
-      pop0.tune_block = r1.choice_b;
-      set_pending_shape(net, r.choice_a, r.choice_b);
-    }
-    const double two_launch_ms = r1.best_ms;
-    // the same halves as one grid per step: CTAs of the delivery after the update's
-    double one_launch_ms = 1e30;
-    int one_grid = net->pending_grid;
-    if (net->one_launch_ok && st == B2B_OK) {
-      net->one_launch = true;
-      const int grids[] = {net->pending_grid, sms / 2, sms, 2 * sms, 4 * sms};
-      for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
-        set_one_launch_grid(net, grids[c]);
-        double ms = 0;
-        st = trial(&ms);
-        if (st == B2B_OK && (c == 0 || ms < kTuneMargin * one_launch_ms)) {
-          one_launch_ms = ms;
-          one_grid = grids[c];
-        }
-      }
-      set_one_launch_grid(net, one_grid);
-    }
-    // the same, each step's launch chained to the previous one (programmatic dependent launch)
-    double chained_ms = 1e30;
-    if (net->one_launch_ok && st == B2B_OK) {
-      net->one_launch_chained = true;
-      set_one_launch_grid(net, one_grid);
-      st = trial(&chained_ms);
-      net->one_launch_chained = false;
-      set_one_launch_grid(net, one_grid);
-    }
-    net->one_launch = false;
-    // the form of the step: 0 per-step kernels, 1 two concurrent launches, 2 one launch, 3 one
-    // launch chained; the built-in form stays unless another is 2 % faster
-    const double form_ms[4] = {per_step_ms, two_launch_ms, one_launch_ms, chained_ms};
-    const int builtin = builtin_two_launch ? (builtin_one_launch ? 2 : 1) : 0;
-    int other = -1;
-    for (int f = 0; f < 4; ++f)
-      if (f != builtin && (other < 0 || form_ms[f] < form_ms[other])) other = f;
-    const int form = form_ms[other] < kTuneMargin * form_ms[builtin] ? other : builtin;
-    net->two_launch = form >= 1;
-    net->one_launch = form >= 2;
-    net->one_launch_chained = form == 3;
-    if (form == 0) {
-      // the per-step form keeps the shape tuned for it
-      pop0.tune_e = ps_e;
-      pop0.tune_block = ps_block;
-    } else if (r1.choice_a != ps_e || r1.choice_b != ps_block) {
-      res.push_back(r1);   // after the per-step form's entry, so that tune_apply ends on it
-    }
-    set_pending_shape(net, r.choice_a, r.choice_b);
-    res.push_back(b2b_tune_result{11, 0, form, form >= 2 ? one_grid : 0, form_ms[form],
-                                  form_ms[builtin]});
-  }
-  // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
-  for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
-    Proj& pr = net->projs[p];
-    if (pr.effect != B2B_EFFECT_STDP) continue;
-    b2b_tune_result r{8, (int32_t)p, 0, 0, 0.0, 0.0};
-    double best = 1e30;
-    for (int c = 0; c < 2 && st == B2B_OK; ++c) {
-      st = set_record_order(net, pr, c == 1);
-      double ms = 0;
-      if (st == B2B_OK) st = trial(&ms);
       if (c == 0) r.default_ms = ms;
       if (st == B2B_OK && (c == 0 || ms < kTuneMargin * best)) {
         best = ms;
-        r.choice_a = c;
+        r.choice_a = sizes[c];
       }
     }
-    if (st == B2B_OK) st = set_record_order(net, pr, r.choice_a == 1);
+    if (!set_small_cluster(net, r.choice_a)) {
+      D.cluster = c0;
+      D.slice = s0;
+    }
     r.best_ms = best;
     res.push_back(r);
-  }
-  if (st != B2B_OK && net->two_launch_ok) {
-    net->two_launch = builtin_two_launch;
-    net->one_launch = builtin_one_launch;
-    net->one_launch_chained = false;
+  } else {
+    int sms = kNumSMs;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+    // a net that allows both forms of the step tunes the per-step kernels first, then the two
+    // concurrent launches, and keeps the faster form
+    const bool builtin_two_launch = net->two_launch;
+    const bool builtin_one_launch = net->two_launch && net->one_launch;
+    if (net->two_launch_ok) net->two_launch = false;
+    net->one_launch = false;
+    for (size_t p = 0; p < net->pops.size() && st == B2B_OK && !net->two_launch; ++p) {
+      Pop& pop = net->pops[p];
+      if (pop.kind == KIND_SPIKEGEN || pop.kind == KIND_MODEL) continue;
+      std::vector<std::pair<int, int>> cands;   // (a, b); the first is the built-in choice
+      if (pop.surr_img) {
+        cands = {{0, 0}, {2, 0}, {3, 0}, {4, 0}, {6, 0}};
+      } else {
+        cands = {{0, 0}, {1, 128}, {1, 256}, {2, 128}, {2, 256}, {4, 128}, {4, 256}};
+      }
+      b2b_tune_result r{1, (int32_t)p, 0, 0, 0.0, 0.0};
+      double best = 1e30;
+      for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+        if (pop.surr_img) {
+          pop.tune_ctas = cands[c].first;
+        } else {
+          pop.tune_e = cands[c].first;
+          pop.tune_block = cands[c].second;
+        }
+        double ms = 0;
+        st = trial(&ms);
+        if (c == 0) r.default_ms = ms;
+        // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
+        // near-equal shapes differ by noise, and noise should not pick the shape
+        if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
+          best = ms;
+          r.choice_a = cands[c].first;
+          r.choice_b = cands[c].second;
+        }
+      }
+      if (pop.surr_img) {
+        pop.tune_ctas = r.choice_a;
+      } else {
+        pop.tune_e = r.choice_a;
+        pop.tune_block = r.choice_b;
+      }
+      r.best_ms = best;
+      res.push_back(r);
+    }
+    for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
+      AddTune& t = net->add_tune[b];
+      std::vector<std::pair<int, int>> cands = {{0, 0}};
+      for (int g : {2, 4, 8, 16, 32})
+        for (int mult : {1, 2, 4, 8, 16}) cands.push_back({g, mult * sms / 2});
+      b2b_tune_result r{6, (int32_t)b, 0, 0, 0.0, 0.0};
+      double best = 1e30;
+      for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+        t.group = cands[c].first;
+        t.grid = cands[c].second;
+        double ms = 0;
+        st = trial(&ms);
+        if (c == 0) r.default_ms = ms;
+        // a candidate replaces the built-in shape only when it is 2 % faster: trial times of
+        // near-equal shapes differ by noise, and noise should not pick the shape
+        if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
+          best = ms;
+          r.choice_a = cands[c].first;
+          r.choice_b = cands[c].second;
+        }
+      }
+      t.group = r.choice_a;
+      t.grid = r.choice_b;
+      r.best_ms = best;
+      res.push_back(r);
+    }
+    // additive delivery launches that can accumulate in thread-block clusters (float32, one
+    // target population): with the chosen lanes per item, cluster accumulation on or off
+    for (size_t b = 0; b < net->add_batches.size() && st == B2B_OK && !net->two_launch; ++b) {
+      const auto& bat = net->add_batches[b];
+      if (!add_batch_cluster_capable(bat.data(), (int)bat.size())) continue;
+      AddTune& t = net->add_tune[b];
+      b2b_tune_result r{12, (int32_t)b, 0, 0, 0.0, 0.0};
+      double off_ms = 0, on_ms = 0;
+      t.cluster = 0;
+      st = trial(&off_ms);
+      if (st != B2B_OK) break;
+      t.cluster = 1;
+      st = trial(&on_ms);
+      const bool use = st == B2B_OK && on_ms < kTuneMargin * off_ms;
+      t.cluster = use ? 1 : 0;
+      r.choice_a = t.cluster;
+      r.default_ms = off_ms;
+      r.best_ms = use ? on_ms : off_ms;
+      res.push_back(r);
+    }
+    if (net->two_launch_ok && st == B2B_OK) {
+      const double per_step_ms = res.empty() ? 1e30 : res.back().best_ms;
+      net->two_launch = true;
+      // the step's delivery launch: lanes per work item x CTAs (the neuron launch has one
+      // thread per neuron)
+      std::vector<std::pair<int, int>> cands = {{0, 0}};
+      for (int g : {2, 4, 8, 16})
+        for (int mult : {1, 2, 4}) cands.push_back({g, mult * sms / 2});
+      b2b_tune_result r{5, 0, 0, 0, 0.0, 0.0};
+      double best = 1e30;
+      for (size_t c = 0; c < cands.size() && st == B2B_OK; ++c) {
+        set_pending_shape(net, cands[c].first, cands[c].second);
+        double ms = 0;
+        st = trial(&ms);
+        if (c == 0) r.default_ms = ms;
+        if (st == B2B_OK && (c == 0 ? true : ms < kTuneMargin * best)) {
+          best = ms;
+          r.choice_a = cands[c].first;
+          r.choice_b = cands[c].second;
+        }
+      }
+      set_pending_shape(net, r.choice_a, r.choice_b);
+      r.best_ms = best;
+      res.push_back(r);
+      // the update's shape again, inside this form: the per-step form tuned it for an update
+      // followed by its own delivery, and the forms rank the shapes differently (COBAHH 1e5:
+      // 1 x 256 against 2 x 128 neurons per thread x threads, 45.8 against 37.7 ms per
+      // simulated second with two launches)
+      Pop& pop0 = net->pops[0];
+      const int ps_e = pop0.tune_e, ps_block = pop0.tune_block;
+      b2b_tune_result r1{1, 0, ps_e, ps_block, best, best};
+      {
+        const std::pair<int, int> shapes[] = {{0, 0}, {1, 128}, {1, 256}, {2, 128}, {2, 256},
+                                              {4, 128}, {4, 256}};
+        for (const auto& sh : shapes) {
+          if (st != B2B_OK) break;
+          if (sh.first == ps_e && sh.second == ps_block) continue;   // timed above
+          pop0.tune_e = sh.first;
+          pop0.tune_block = sh.second;
+          set_pending_shape(net, r.choice_a, r.choice_b);   // a fresh graph
+          double ms = 0;
+          st = trial(&ms);
+          if (st == B2B_OK && ms < kTuneMargin * r1.best_ms) {
+            r1.best_ms = ms;
+            r1.choice_a = sh.first;
+            r1.choice_b = sh.second;
+          }
+        }
+        pop0.tune_e = r1.choice_a;
+        pop0.tune_block = r1.choice_b;
+        set_pending_shape(net, r.choice_a, r.choice_b);
+      }
+      const double two_launch_ms = r1.best_ms;
+      // the same halves as one grid per step: CTAs of the delivery after the update's
+      double one_launch_ms = 1e30;
+      int one_grid = net->pending_grid;
+      if (net->one_launch_ok && st == B2B_OK) {
+        net->one_launch = true;
+        const int grids[] = {net->pending_grid, sms / 2, sms, 2 * sms, 4 * sms};
+        for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
+          set_one_launch_grid(net, grids[c]);
+          double ms = 0;
+          st = trial(&ms);
+          if (st == B2B_OK && (c == 0 || ms < kTuneMargin * one_launch_ms)) {
+            one_launch_ms = ms;
+            one_grid = grids[c];
+          }
+        }
+        set_one_launch_grid(net, one_grid);
+      }
+      // the same, each step's launch chained to the previous one (programmatic dependent launch)
+      double chained_ms = 1e30;
+      if (net->one_launch_ok && st == B2B_OK) {
+        net->one_launch_chained = true;
+        set_one_launch_grid(net, one_grid);
+        st = trial(&chained_ms);
+        net->one_launch_chained = false;
+        set_one_launch_grid(net, one_grid);
+      }
+      net->one_launch = false;
+      // the form of the step: 0 per-step kernels, 1 two concurrent launches, 2 one launch, 3 one
+      // launch chained; the built-in form stays unless another is 2 % faster
+      const double form_ms[4] = {per_step_ms, two_launch_ms, one_launch_ms, chained_ms};
+      const int builtin = builtin_two_launch ? (builtin_one_launch ? 2 : 1) : 0;
+      int other = -1;
+      for (int f = 0; f < 4; ++f)
+        if (f != builtin && (other < 0 || form_ms[f] < form_ms[other])) other = f;
+      const int form = form_ms[other] < kTuneMargin * form_ms[builtin] ? other : builtin;
+      net->two_launch = form >= 1;
+      net->one_launch = form >= 2;
+      net->one_launch_chained = form == 3;
+      if (form == 0) {
+        // the per-step form keeps the shape tuned for it
+        pop0.tune_e = ps_e;
+        pop0.tune_block = ps_block;
+      } else if (r1.choice_a != ps_e || r1.choice_b != ps_block) {
+        res.push_back(r1);   // after the per-step form's entry, so that tune_apply ends on it
+      }
+      set_pending_shape(net, r.choice_a, r.choice_b);
+      res.push_back(b2b_tune_result{11, 0, form, form >= 2 ? one_grid : 0, form_ms[form],
+                                    form_ms[builtin]});
+    }
+    // STDP projections: order of the synapse records (0 synapse order, 1 post-grouped)
+    for (size_t p = 0; p < net->projs.size() && st == B2B_OK; ++p) {
+      Proj& pr = net->projs[p];
+      if (pr.effect != B2B_EFFECT_STDP) continue;
+      b2b_tune_result r{8, (int32_t)p, 0, 0, 0.0, 0.0};
+      double best = 1e30;
+      for (int c = 0; c < 2 && st == B2B_OK; ++c) {
+        st = set_record_order(net, pr, c == 1);
+        double ms = 0;
+        if (st == B2B_OK) st = trial(&ms);
+        if (c == 0) r.default_ms = ms;
+        if (st == B2B_OK && (c == 0 || ms < kTuneMargin * best)) {
+          best = ms;
+          r.choice_a = c;
+        }
+      }
+      if (st == B2B_OK) st = set_record_order(net, pr, r.choice_a == 1);
+      r.best_ms = best;
+      res.push_back(r);
+    }
+    if (st != B2B_OK && net->two_launch_ok) {
+      net->two_launch = builtin_two_launch;
+      net->one_launch = builtin_one_launch;
+      net->one_launch_chained = false;
+    }
   }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
@@ -2374,6 +2426,11 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
                 t.choice_b >= 0 && t.choice_b <= 65535,
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       set_pending_shape(net, t.choice_a, t.choice_b);
+    } else if (t.site_kind == 14) {
+      CHECK(net->small && t.site_index == 0, B2B_ERR_INVALID_ARG,
+            "site kind 14 exists only for a net on the small-network path");
+      CHECK(set_small_cluster(net, t.choice_a), B2B_ERR_UNSUPPORTED,
+            "the small-network path cannot run as %d CTAs here", t.choice_a);
     } else if (t.site_kind == 8) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
                 net->projs[t.site_index].effect == B2B_EFFECT_STDP,

@@ -210,6 +210,9 @@ struct SmallDev {
   int32_t n_proj, nd_max;
   int32_t warp_prefix;                  // every projection has <= 64 delays
   int32_t ring_in_smem;                 // the spike-history ring is mirrored in shared memory
+  int32_t cluster;                      // CTAs of the one thread-block cluster (1: one CTA)
+  int32_t pad_small;
+  int64_t slice;                        // neurons per CTA of the cluster (multiple of 4)
 };
 
 struct Group {
@@ -425,6 +428,9 @@ const void* mlp_image(const b2b_mlp* m);
 int mlp_device(const b2b_mlp* m);
 // Small networks (small.cu): `steps` steps of the net in one one-CTA launch.
 size_t small_smem(const SmallDev& D, int kind, int dtype);
+// Whether the cluster form of the small-network path (D.cluster CTAs of D.slice neurons) can
+// be launched on the current device.
+bool small_cluster_possible(const SmallDev& D, int kind, int dtype);
 cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                          int steps, double dt, int32_t* status, cudaStream_t s);
 // The two-launch step (pending.cu): the delivery into the pending input of the step, and the

@@ -18,6 +18,8 @@
 // per-step kernels: CUBA-type LIF nets of 500 / 1000 / 2000 neurons 3.8 / 4.4 / 5.8 us per
 // step against 4.9 / 5.5 / 6.6 us; at 4000 neurons, or with many delays (COBAHH with delays
 // of 1-50 steps), one SM's issue rate loses to the whole GPU, so the path is opt-in.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 #include "delivery.cuh"
@@ -281,6 +283,247 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
   if (tid == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
 }
 
+// ---- the same, spread over one thread-block cluster ------------------------------------
+// The one-CTA form is bound by one SM's issue rate once a step has a few thousand neurons;
+// here the CTAs of one cluster (up to 16 SMs) share the chunk: CTA r keeps neurons
+// [r S, (r+1) S) in its shared memory, and cluster barriers (hardware, no spinning) take the
+// place of the block barriers between the phases of a step:
+//   update and threshold of the CTA's slice, compaction of its spikes in shared memory;
+//   barrier; each CTA reads every CTA's spike count from distributed shared memory, writes its
+//   spikes at its offset into the step's slot of the spike-history ring in global memory (in
+//   ascending neuron order, as the per-step kernels' compaction leaves them per CTA);
+//   barrier (the ring slot is complete and visible to the cluster);
+//   delivery of the due bundles by every warp of the cluster, each effect an atomic addition
+//   into the shared memory of the CTA that owns the target neuron;
+//   barrier (every effect has landed); a deferred reset by each CTA for its own neurons.
+// Requires every projection to have at most 64 delays (the per-warp prefix).
+namespace cg = cooperative_groups;
+
+template <typename R>
+__device__ __forceinline__ void cluster_deliver(const cg::cluster_group& cl, const ProjDev& J,
+                                                int64_t ts, int64_t S, int64_t wid,
+                                                int64_t nw) {
+  const int lane = threadIdx.x & 31;
+  const DuePrefix wp = due_prefix_warp(J.src_ring_cnt, J.src_ring_len, ts, J.dmin, J.nd,
+                                       J.src_lo, J.src_hi);
+  const int sub = J.chunks * (kChunk / 32);
+  const int64_t items = (int64_t)wp.total * sub;
+  const int base = ring_slot(ts, J.src_ring_len);
+  const R* W = static_cast<const R*>(J.w);
+  MemberCache<R> mc;
+  for (int64_t it = wid; it < items; it += nw) {   // warp-uniform
+    const int sp = (int)(it / sub);
+    const int ch = (int)(it - (int64_t)sp * sub);
+    int kk;
+    const int di = find_delay_warp(wp, sp, &kk);
+    const int slot = ring_back(base, J.dmin + di, J.src_ring_len);
+    const int32_t pre = J.src_ring_idx[(int64_t)slot * J.src_n + kk];
+    const int64_t key = (int64_t)pre * J.nd + di;
+    const int64_t s = J.off[key] + (int64_t)ch * 32 + lane;
+    if (s < J.off[key + 1]) {
+      const int32_t post = __ldg(J.post + s);
+      member_lookup<R>(J, pre, mc);
+      const R w = W ? __ldg(W + s) : mc.w;
+      const unsigned owner = (unsigned)(post / S);
+      R* dst = cl.map_shared_rank(mc.target, owner) + (post - (int64_t)owner * S);
+      atomicAdd(dst, w);
+    }
+  }
+}
+
+template <typename R, int KIND>
+__global__ void __launch_bounds__(kSmallThreads, 1)
+small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
+                     int steps, double dt, int32_t* status, int64_t S) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int C = (int)cl.num_blocks();
+  const PopDev& P = D.pop;
+  const SmallLayout L = small_layout(KIND);
+  const int64_t n = P.n;
+  const int64_t lo = (int64_t)rank * S;
+  const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;   // neurons of this CTA
+  R* const base = reinterpret_cast<R*>(smem);
+  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const sV = base;
+  R* const sGE = base + S;
+  R* const sGI = base + 2 * S;
+  R* const sLS = base + kLS * S;
+  R* const sM = base + 3 * S;   // HH only
+  R* const sH = base + 4 * S;
+  R* const sN = base + 5 * S;
+  uint8_t* snr = smem + sizeof(R) * L.nvars * S;
+  int32_t* s_ring_cnt = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
+  __shared__ int s_warp[33];
+  __shared__ int s_cnt, s_off, s_tot;
+  __shared__ unsigned long long s_mon;
+  const int tid = threadIdx.x;
+  const int64_t ts0 = clock[0];
+
+  for (int i = 0; i < L.nvars; ++i) {
+    const R* g = static_cast<const R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) base[i * S + q] = g[lo + q];
+  }
+  {
+    const uint8_t* g = static_cast<const uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) snr[q] = g[lo + q];
+  }
+  for (int r = tid; r < P.ring_len; r += blockDim.x) s_ring_cnt[r] = P.ring_cnt[r];
+  if (tid == 0) s_mon = P.mon_cnt ? *P.mon_cnt : 0ull;
+  // delivery targets: this CTA's shared-memory arrays (the same offsets in every CTA of the
+  // cluster, mapped to the owner's at each effect); source ring: the global ring, counts
+  // from the shared-memory mirror
+  __shared__ ProjDev J[kMaxProjBatch];
+  if (tid < D.n_proj) {
+    J[tid] = D.proj[tid];
+    for (int v = 0; v < 3; ++v) J[tid].targets[v] = base + v * S;   // v, ge, gi
+    J[tid].target = base + D.proj_target[tid] * S;
+    J[tid].src_ring_cnt = s_ring_cnt;
+  }
+  __syncthreads();
+  const int64_t nwarps = blockDim.x >> 5;
+  const int64_t wid = (int64_t)rank * nwarps + (tid >> 5);
+  const int64_t nw = (int64_t)C * nwarps;
+
+  const double inv_dt = 1.0 / dt;
+  for (int k = 0; k < steps; ++k) {
+    const int64_t ts = ts0 + k;
+    const double t = (double)ts * dt;
+    const int slot = ring_slot(ts, P.ring_len);
+    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
+    unsigned fl = 0;
+    const int64_t j4 = 4 * (int64_t)tid;
+    if (j4 < mine) {
+      const int gidx = P.vec_group ? P.vec_group[(lo + j4) >> 2] : 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t jl = j4 + e;      // local index
+        const int64_t i = lo + jl;      // population index
+        R v = sV[jl], ge = sGE[jl], gi = sGI[jl];
+        R ls = sLS[jl];
+        bool nr = true;
+        if constexpr (KIND == KIND_LIF) {
+          const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R vn = lif_advance<R>(
+              g, v, ge, gi, nr,
+              P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
+          if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
+            fl |= 1u << e;
+          }
+          v = vn;
+          if (refr) {
+            sLS[jl] = ls;
+            snr[jl] = nr ? 1 : 0;
+          }
+        } else {
+          const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R m = sM[jl], h = sH[jl], nn = sN[jl];
+          const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
+                                     P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
+                                                               i - g.offset)
+                                              : R(0));
+          if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            fl |= 1u << e;
+          }
+          v = vn;
+          sM[jl] = m;
+          sH[jl] = h;
+          sN[jl] = nn;
+          if (refr) {
+            sLS[jl] = ls;
+            snr[jl] = nr ? 1 : 0;
+          }
+        }
+        sV[jl] = v;
+        sGE[jl] = ge;
+        sGI[jl] = gi;
+      }
+    }
+    // ---- compaction: this CTA's count, then its offset among the cluster's CTAs
+    int total;
+    const int c = __popc(fl);
+    const int excl = block_exclusive_scan(c, s_warp, &total);
+    if (tid == 0) s_cnt = total;
+    cl.sync();
+    if (tid == 0) {
+      int off = 0, tot = 0;
+      for (int q = 0; q < C; ++q) {
+        const int cq = *cl.map_shared_rank(&s_cnt, (unsigned)q);
+        if (q < rank) off += cq;
+        tot += cq;
+      }
+      s_off = off;
+      s_tot = tot;
+      const int next = ring_slot(ts + 1, P.ring_len);
+      s_ring_cnt[slot] = tot;
+      s_ring_cnt[next] = 0;
+      if (rank == 0) {
+        P.ring_cnt[slot] = tot;
+        P.ring_cnt[next] = 0;
+      }
+    }
+    __syncthreads();
+    if (c) {
+      int pos = s_off + excl;
+      int32_t* out = P.ring_idx + (int64_t)slot * P.n;
+      unsigned long long mpos = s_mon + (unsigned long long)(s_off + excl);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!(fl & (1u << e))) continue;
+        const int32_t idx = (int32_t)(lo + j4 + e);
+        out[pos++] = idx;
+        if (P.mon_cnt) {
+          if (mpos < (unsigned long long)P.mon_cap) {
+            P.mon_idx[mpos] = idx;
+            P.mon_step[mpos] = ts;
+          } else {
+            set_status(status, B2B_ERR_QUEUE_OVERFLOW);
+          }
+          ++mpos;
+        }
+      }
+    }
+    cl.sync();   // the ring slot is complete, and every CTA has read the counts
+    if (tid == 0) s_mon += (unsigned long long)s_tot;
+    // ---- synapses: every warp of the cluster, effects into the owners' shared memory
+    for (int p = 0; p < D.n_proj; ++p) cluster_deliver<R>(cl, J[p], ts, S, wid, nw);
+    cl.sync();   // every effect has landed
+    // ---- resets deferred after the synapses, each CTA for its own neurons
+    if constexpr (KIND == KIND_LIF) {
+      if (P.late_reset) {
+        const int32_t* idx = P.ring_idx + (int64_t)slot * P.n;
+        const int tot = s_tot;
+        for (int r = tid; r < tot; r += blockDim.x) {
+          const int32_t i = idx[r];
+          if (i < lo || i >= lo + mine) continue;
+          const LifDev& g = static_cast<const LifDev*>(P.params)[P.vec_group ? P.vec_group[i >> 2] : 0];
+          if (g.has_reset) sV[i - lo] = (R)g.Vr;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = 0; i < L.nvars; ++i) {
+    R* g = static_cast<R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) g[lo + q] = base[i * S + q];
+  }
+  {
+    uint8_t* g = static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) g[lo + q] = snr[q];
+  }
+  if (tid == 0 && rank == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
+}
+
 }  // namespace
 
 size_t small_smem(const SmallDev& D, int kind, int dtype) {
@@ -293,8 +536,72 @@ size_t small_smem(const SmallDev& D, int kind, int dtype) {
   return bytes;
 }
 
+// Shared memory of one CTA of the cluster form: its slice of the state and flags, and the
+// ring counts.
+size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
+  const SmallLayout L = small_layout(kind);
+  const size_t rs = dtype == B2B_F32 ? 4 : 8;
+  const size_t S = (size_t)D.slice;
+  return ((rs * L.nvars * S + S + 15) & ~(size_t)15) +
+         sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
+}
+
+namespace {
+template <typename R, int K>
+cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps, double dt,
+                              int32_t* status, cudaStream_t s, size_t smem, bool probe) {
+  auto kern = small_cluster_kernel<R, K>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e == cudaSuccess && D.cluster > 8)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  const int threads = (int)std::min<int64_t>(
+      kSmallThreads, std::max<int64_t>(256, ((D.slice / 4 + 31) / 32) * 32));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)D.cluster);
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)D.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (probe) {
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, (const void*)kern, &cfg);
+    return e != cudaSuccess ? e : (clusters >= 1 ? cudaSuccess : cudaErrorInvalidConfiguration);
+  }
+  return cudaLaunchKernelEx(&cfg, kern, D, clock, steps, dt, status, (int64_t)D.slice);
+}
+
+cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t* clock,
+                           int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
+  if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
+      D.slice / 4 > kSmallThreads)
+    return cudaErrorInvalidValue;
+  const size_t smem = small_cluster_smem(D, kind, dtype);
+  if (kind == KIND_LIF && dtype == B2B_F32)
+    return launch_cluster_rk<float, KIND_LIF>(D, clock, steps, dt, status, s, smem, probe);
+  if (kind == KIND_LIF)
+    return launch_cluster_rk<double, KIND_LIF>(D, clock, steps, dt, status, s, smem, probe);
+  if (dtype == B2B_F32)
+    return launch_cluster_rk<float, KIND_HH>(D, clock, steps, dt, status, s, smem, probe);
+  return launch_cluster_rk<double, KIND_HH>(D, clock, steps, dt, status, s, smem, probe);
+}
+}  // namespace
+
+bool small_cluster_possible(const SmallDev& D, int kind, int dtype) {
+  return launch_cluster(D, kind, dtype, nullptr, 0, 0.0, nullptr, nullptr, true) == cudaSuccess;
+}
+
 cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                          int steps, double dt, int32_t* status, cudaStream_t s) {
+  if (D.cluster > 1)
+    return launch_cluster(D, kind, dtype, clock, steps, dt, status, s, false);
   const size_t smem = small_smem(D, kind, dtype);
   cudaError_t e = cudaSuccess;
 #define B2B_SMALL(R, K)                                                                       \

@@ -642,11 +642,14 @@ def test_autotune_keeps_state_and_results(gpu_factory):
     np.testing.assert_array_equal(out[True][0], out[False][0])
     np.testing.assert_array_equal(out[True][1], out[False][1])
     np.testing.assert_array_equal(out[True][2], out[False][2])
-    # a small network run by one CTA has a fixed shape: nothing to tune
+    # a small network: the tuner chooses one CTA or one cluster of 8 or 16 (site kind 14)
     net = gpu_factory(DT, small=True)
     models.build_cuba(net, n=1000, p=0.05, dtype="float64")
     net.finalize()
-    assert net.run_mode == "small" and net.autotune(trial_steps=5) == []
+    assert net.run_mode == "small"
+    res = net.autotune(trial_steps=5)
+    assert [r["site_kind"] for r in res] == [14] and res[0]["choice_a"] in (1, 8, 16)
+    assert net.run_mode == "small"
 
 
 def test_autotune_chooses_step_form(gpu_factory):
@@ -698,11 +701,14 @@ def test_out_degree_matches_synapses(gpu_factory):
 
 @pytest.mark.parametrize("case", ["cobahh_delays", "lif_onto_v_late_reset"])
 def test_small_network_path_matches_per_step(gpu_factory, case):
-    """The opt-in small-network path runs every step of a chunk in one CTA with the state in
-    shared memory; the result must be the per-step kernels' result exactly (every delivered weight of one
-    target variable is equal, so the order of the additions cannot change a sum)."""
+    """The opt-in small-network path runs every step of a chunk in one CTA, or in one
+    thread-block cluster of 8 or 16 CTAs (autotuner site kind 14), with the state in shared
+    memory; the result must be the per-step kernels' result exactly (every delivered weight
+    of one target variable is equal, so the order of the additions cannot change a sum)."""
+    from brian2cuda_b200._native import B2BError
     out = {}
-    for small in (True, False):
+    for form in (1, 8, 16, False):
+        small = form is not False
         net = gpu_factory(DT, small=small, two_launch=None if small else False)
         if case == "cobahh_delays":
             ids = models.build_cobahh(net, n=3000, p=0.05, monitor_capacity=10**6)
@@ -719,15 +725,26 @@ def test_small_network_path_matches_per_step(gpu_factory, case):
             steps = 200
         net.finalize()
         assert net.run_mode == ("small" if small else "per-step")
+        if small and form > 1:
+            try:
+                net.tune_apply([{"site_kind": 14, "site_index": 0, "choice_a": form,
+                                 "choice_b": 0}])
+            except B2BError:
+                assert form == 16, "an 8-CTA cluster must be possible"
+                continue          # 16-CTA clusters are not available on this device
         net.run(steps)
         assert net.sync() == 0
         idx, st = net.spikes(G)
-        out[small] = (idx, st, {v: net.get_state(G, v) for v in ("v", "ge", "gi", "lastspike")})
-    assert len(out[True][0]) > 50
-    np.testing.assert_array_equal(out[True][0], out[False][0])
-    np.testing.assert_array_equal(out[True][1], out[False][1])
-    for v in ("v", "ge", "gi", "lastspike"):
-        np.testing.assert_array_equal(out[True][2][v], out[False][2][v], err_msg=v)
+        out[form] = (idx, st, {v: net.get_state(G, v) for v in ("v", "ge", "gi", "lastspike")})
+    assert len(out[False][0]) > 50
+    for form in (1, 8, 16):
+        if form not in out:
+            continue
+        np.testing.assert_array_equal(out[form][0], out[False][0], err_msg=str(form))
+        np.testing.assert_array_equal(out[form][1], out[False][1], err_msg=str(form))
+        for v in ("v", "ge", "gi", "lastspike"):
+            np.testing.assert_array_equal(out[form][2][v], out[False][2][v],
+                                          err_msg=f"{form} {v}")
 
 
 @pytest.mark.parametrize("inputs", [False, True])
