@@ -779,6 +779,38 @@ b2b_status setup_small(b2b_net* net) {
   if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) D.ring_in_smem = 0;
   D.cluster = 1;                 // one CTA until tuned (b2b_autotune, site kind 14)
   D.slice = pop.n;
+  // the pull form's bit rows: every synapse without a delay of its own (delay 0) and without
+  // a weight of its own, at most one synapse per (pre, post) pair
+  bool pull = pop.n <= 8192;
+  for (const Proj& pr : net->projs)
+    pull = pull && pr.dmin == 0 && pr.dmax == 0 && pr.dev.w == nullptr;
+  if (pull && !net->projs.empty()) {
+    const int64_t n = pop.n, row = n / 32;
+    std::vector<uint32_t> bits((size_t)net->projs.size() * n * row, 0u);
+    for (size_t p = 0; p < net->projs.size() && pull; ++p) {
+      const Proj& pr = net->projs[p];
+      std::vector<int64_t> off(n + 1);
+      std::vector<int32_t> post(std::max<int64_t>(pr.n_syn, 1));
+      CU(cudaMemcpy(off.data(), pr.off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+      if (pr.n_syn)
+        CU(cudaMemcpy(post.data(), pr.post, sizeof(int32_t) * pr.n_syn, cudaMemcpyDeviceToHost));
+      uint32_t* B = bits.data() + p * n * row;
+      for (int64_t pre = 0; pre < n && pull; ++pre)
+        for (int64_t s = off[pre]; s < off[pre + 1]; ++s) {
+          uint32_t& w = B[pre * row + post[s] / 32];
+          const uint32_t b = 1u << (post[s] % 32);
+          if (w & b) { pull = false; break; }     // a second synapse of the pair
+          w |= b;
+        }
+    }
+    if (pull) {
+      uint32_t* d = nullptr;
+      CU(cudaMalloc(&d, sizeof(uint32_t) * bits.size()));
+      net->pending_allocs.push_back(d);
+      CU(cudaMemcpy(d, bits.data(), sizeof(uint32_t) * bits.size(), cudaMemcpyHostToDevice));
+      D.pull_bits = d;
+    }
+  }
   net->small = true;
   return B2B_OK;
 }
@@ -1980,21 +2012,26 @@ constexpr double kTuneMargin = 0.98;
 // Launch shape of the delivery launch of a net run with two launches per step (pending.cu):
 // lanes per work item (0: 8) and CTAs (0: two per SM).
 // The small-network path as one CTA (c == 1) or one cluster of c CTAs, each holding a slice
-// of the population; false (nothing changed) when the cluster form cannot run the net.
-bool set_small_cluster(b2b_net* net, int c) {
+// of the population, pushing the effects or (pull) gathering them at the targets; false
+// (nothing changed) when that form cannot run the net.
+bool set_small_cluster(b2b_net* net, int c, bool pull) {
   SmallDev& D = net->sdev;
   const Pop& pop = net->pops[0];
-  const int32_t c0 = D.cluster;
+  const int32_t c0 = D.cluster, p0 = D.pull;
   const int64_t s0 = D.slice;
-  if (c == 1) {
+  if (c == 1 && !pull) {
     D.cluster = 1;
+    D.pull = 0;
     D.slice = pop.n;
   } else {
-    if (c != 8 && c != 16) return false;
+    if ((c != 8 && c != 16) || (pull && !D.pull_bits)) return false;
+    const int64_t q = pull ? 32 : 4;
     D.cluster = c;
-    D.slice = ((pop.n + c - 1) / c + 3) / 4 * 4;
+    D.pull = pull ? 1 : 0;
+    D.slice = ((pop.n + c - 1) / c + q - 1) / q * q;
     if (!small_cluster_possible(D, pop.kind, pop.dtype)) {
       D.cluster = c0;
+      D.pull = p0;
       D.slice = s0;
       return false;
     }
@@ -2107,28 +2144,26 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
     st = trial(&ms);
   }
   if (net->small) {
-    // the small-network path: one CTA, or one thread-block cluster of 8 or 16 CTAs
+    // the small-network path: one CTA, or one thread-block cluster of 8 or 16 CTAs pushing
+    // the effects or pulling them at the targets
     SmallDev& D = net->sdev;
-    const int32_t c0 = D.cluster;
-    const int64_t s0 = D.slice;
-    b2b_tune_result r{14, 0, c0, 0, 0.0, 0.0};
+    const int32_t c0 = D.cluster, p0 = D.pull;
+    b2b_tune_result r{14, 0, c0, p0, 0.0, 0.0};
     double best = 1e30;
-    const int sizes[] = {c0, 1, 8, 16};
-    for (int c = 0; c < 4 && st == B2B_OK; ++c) {
-      if (c > 0 && sizes[c] == c0) continue;
-      if (!set_small_cluster(net, sizes[c])) continue;
+    const std::pair<int, int> forms[] = {{c0, p0}, {1, 0}, {8, 0}, {16, 0}, {8, 1}, {16, 1}};
+    for (int c = 0; c < 6 && st == B2B_OK; ++c) {
+      if (c > 0 && forms[c].first == c0 && forms[c].second == p0) continue;
+      if (!set_small_cluster(net, forms[c].first, forms[c].second != 0)) continue;
       double ms = 0;
       st = trial(&ms);
       if (c == 0) r.default_ms = ms;
       if (st == B2B_OK && (c == 0 || ms < kTuneMargin * best)) {
         best = ms;
-        r.choice_a = sizes[c];
+        r.choice_a = forms[c].first;
+        r.choice_b = forms[c].second;
       }
     }
-    if (!set_small_cluster(net, r.choice_a)) {
-      D.cluster = c0;
-      D.slice = s0;
-    }
+    set_small_cluster(net, r.choice_a, r.choice_b != 0);
     r.best_ms = best;
     res.push_back(r);
   } else {
@@ -2429,8 +2464,10 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
     } else if (t.site_kind == 14) {
       CHECK(net->small && t.site_index == 0, B2B_ERR_INVALID_ARG,
             "site kind 14 exists only for a net on the small-network path");
-      CHECK(set_small_cluster(net, t.choice_a), B2B_ERR_UNSUPPORTED,
-            "the small-network path cannot run as %d CTAs here", t.choice_a);
+      CHECK(t.choice_b == 0 || t.choice_b == 1, B2B_ERR_INVALID_ARG, "bad small-path form");
+      CHECK(set_small_cluster(net, t.choice_a, t.choice_b == 1), B2B_ERR_UNSUPPORTED,
+            "the small-network path cannot run as %d CTAs%s here", t.choice_a,
+            t.choice_b == 1 ? " pulling the effects" : "");
     } else if (t.site_kind == 8) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
                 net->projs[t.site_index].effect == B2B_EFFECT_STDP,

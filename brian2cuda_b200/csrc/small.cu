@@ -524,6 +524,239 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
   if (tid == 0 && rank == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
 }
 
+// ---- the cluster form with the delivery pulled by the targets --------------------------
+// For a net whose every synapse has a delay of 0 steps and one weight per Synapses object
+// (the CUBA example), the effects of a step can be gathered by the target neurons instead
+// of scattered by the spikes: CTA r keeps, beside its slice of the state, the connectivity
+// of its slice as bit rows (bit j of row `pre` set when pre connects to neuron r S + j) in
+// shared memory.  A step is then one cluster barrier:
+//   update and threshold of the slice; compaction of its spikes into a local list (double
+//   buffered by step parity);
+//   barrier;
+//   every CTA copies all CTAs' lists (distributed shared memory) into one list of the step's
+//   spikes, in rank order, and writes its own spikes at their offset into the global ring and
+//   monitor (the per-step kernels' record of the step);
+//   each target neuron adds, for every spike whose bit row has its bit, that Synapses
+//   object's weight to its target variable (the synapses slot), then the deferred reset.
+// Inside the step loop global memory is written (ring, monitor) and read only for the group
+// parameters and the projections' member tables, a few cached entries.  A final barrier keeps
+// every CTA's lists alive until all CTAs have read them.
+template <typename R, int KIND>
+__global__ void __launch_bounds__(kSmallThreads, 1)
+small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
+                  int steps, double dt, int32_t* status, int64_t S) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int C = (int)cl.num_blocks();
+  const PopDev& P = D.pop;
+  const SmallLayout L = small_layout(KIND);
+  const int64_t n = P.n;
+  const int64_t lo = (int64_t)rank * S;
+  const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;
+  const int64_t words = S / 32;                 // bit words per row of a slice
+  R* const base = reinterpret_cast<R*>(smem);
+  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const sV = base;
+  R* const sGE = base + S;
+  R* const sGI = base + 2 * S;
+  R* const sLS = base + kLS * S;
+  R* const sM = base + 3 * S;   // HH only
+  R* const sH = base + 4 * S;
+  R* const sN = base + 5 * S;
+  uint8_t* snr = smem + sizeof(R) * L.nvars * S;
+  uint32_t* bits = reinterpret_cast<uint32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
+  int32_t* lists = reinterpret_cast<int32_t*>(bits + (int64_t)D.n_proj * n * words);   // [2][S]
+  int32_t* all = lists + 2 * S;                 // the step's spikes, [n]
+  __shared__ int s_warp[33];
+  __shared__ int s_cnt[2];
+  __shared__ int s_pre[17];                     // counts of the ranks before each rank
+  __shared__ unsigned long long s_mon;
+  const int tid = threadIdx.x;
+  const int64_t ts0 = clock[0];
+
+  for (int i = 0; i < L.nvars; ++i) {
+    const R* g = static_cast<const R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) base[i * S + q] = g[lo + q];
+  }
+  {
+    const uint8_t* g = static_cast<const uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) snr[q] = g[lo + q];
+  }
+  // this slice's columns of every projection's bit rows
+  const int64_t row_words = n / 32;
+  for (int p = 0; p < D.n_proj; ++p)
+    for (int64_t x = tid; x < n * words; x += blockDim.x) {
+      const int64_t pre = x / words, w = x - pre * words;
+      const int64_t gw = lo / 32 + w;           // past the population for a partial slice
+      bits[((int64_t)p * n + pre) * words + w] =
+          gw < row_words ? D.pull_bits[((int64_t)p * n + pre) * row_words + gw] : 0u;
+    }
+  if (tid == 0) s_mon = P.mon_cnt ? *P.mon_cnt : 0ull;
+  __syncthreads();
+
+  const double inv_dt = 1.0 / dt;
+  for (int k = 0; k < steps; ++k) {
+    const int64_t ts = ts0 + k;
+    const double t = (double)ts * dt;
+    const int slot = ring_slot(ts, P.ring_len);
+    const int par = k & 1;
+    int32_t* mylist = lists + par * S;
+    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
+    unsigned fl = 0;
+    const int64_t j4 = 4 * (int64_t)tid;
+    if (j4 < mine) {
+      const int gidx = P.vec_group ? P.vec_group[(lo + j4) >> 2] : 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t jl = j4 + e;
+        const int64_t i = lo + jl;
+        R v = sV[jl], ge = sGE[jl], gi = sGI[jl];
+        R ls = sLS[jl];
+        bool nr = true;
+        if constexpr (KIND == KIND_LIF) {
+          const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R vn = lif_advance<R>(
+              g, v, ge, gi, nr,
+              P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
+          if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
+            fl |= 1u << e;
+          }
+          v = vn;
+          if (refr) {
+            sLS[jl] = ls;
+            snr[jl] = nr ? 1 : 0;
+          }
+        } else {
+          const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
+          const bool refr = g.ref_steps >= 0;
+          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          R m = sM[jl], h = sH[jl], nn = sN[jl];
+          const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
+                                     P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
+                                                               i - g.offset)
+                                              : R(0));
+          if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
+            nr = false;
+            if (refr) ls = (R)t;
+            fl |= 1u << e;
+          }
+          v = vn;
+          sM[jl] = m;
+          sH[jl] = h;
+          sN[jl] = nn;
+          if (refr) {
+            sLS[jl] = ls;
+            snr[jl] = nr ? 1 : 0;
+          }
+        }
+        sV[jl] = v;
+        sGE[jl] = ge;
+        sGI[jl] = gi;
+      }
+    }
+    // ---- this CTA's spikes into its local list (ascending neuron order)
+    int total;
+    const int c = __popc(fl);
+    const int excl = block_exclusive_scan(c, s_warp, &total);
+    if (c) {
+      int pos = excl;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (fl & (1u << e)) mylist[pos++] = (int32_t)(lo + j4 + e);
+    }
+    if (tid == 0) s_cnt[par] = total;
+    cl.sync();
+    // ---- every CTA's spikes of the step, in rank order
+    if (tid == 0) {
+      int acc = 0;
+      for (int q = 0; q < C; ++q) {
+        s_pre[q] = acc;
+        acc += *cl.map_shared_rank(&s_cnt[par], (unsigned)q);
+      }
+      s_pre[C] = acc;
+    }
+    __syncthreads();
+    const int tot = s_pre[C];
+    for (int x = tid; x < tot; x += blockDim.x) {
+      int q = 0;
+      while (q + 1 < C && s_pre[q + 1] <= x) ++q;
+      all[x] = *cl.map_shared_rank(lists + par * S + (x - s_pre[q]), (unsigned)q);
+    }
+    // the per-step kernels' record of the step: global ring slot and monitor
+    {
+      const int off = s_pre[rank];
+      int32_t* out = P.ring_idx + (int64_t)slot * P.n;
+      for (int x = tid; x < total; x += blockDim.x) {
+        const int32_t idx = mylist[x];
+        out[off + x] = idx;
+        if (P.mon_cnt) {
+          const unsigned long long mpos = s_mon + (unsigned long long)(off + x);
+          if (mpos < (unsigned long long)P.mon_cap) {
+            P.mon_idx[mpos] = idx;
+            P.mon_step[mpos] = ts;
+          } else {
+            set_status(status, B2B_ERR_QUEUE_OVERFLOW);
+          }
+        }
+      }
+      if (tid == 0 && rank == 0) {
+        P.ring_cnt[slot] = tot;
+        P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) s_mon += (unsigned long long)tot;
+    // ---- synapses slot: each target neuron gathers the effects of the step's spikes
+    if (j4 < mine && tot > 0) {
+      const int64_t w = j4 / 32;
+      const int sh = (int)(j4 & 31);
+      for (int p = 0; p < D.n_proj; ++p) {
+        const ProjDev& J = D.proj[p];
+        const uint32_t* B = bits + (int64_t)p * n * words;
+        for (int x = 0; x < tot; ++x) {
+          const int32_t pre = all[x];
+          const unsigned b4 = (B[(int64_t)pre * words + w] >> sh) & 0xFu;
+          if (!b4) continue;
+          const int m = J.n_mem == 1 ? 0 : member_of(J, pre);
+          const int var = J.n_mem == 1 ? D.proj_target[p] : (int)J.mem_var[m];
+          const R wgt = (R)(J.mem_w ? J.mem_w[m] : J.w_scalar);
+          R* T = base + var * S;                    // v, ge, gi: columns 0-2
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (b4 & (1u << e)) T[j4 + e] += wgt;
+        }
+      }
+    }
+    // ---- resets deferred after the synapses, for this CTA's spiking neurons
+    if constexpr (KIND == KIND_LIF) {
+      if (P.late_reset) {
+        for (int x = tid; x < total; x += blockDim.x) {
+          const int32_t i = mylist[x];
+          const LifDev& g = static_cast<const LifDev*>(P.params)[P.vec_group ? P.vec_group[i >> 2] : 0];
+          if (g.has_reset) sV[i - lo] = (R)g.Vr;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cl.sync();   // every CTA is done reading the others' lists
+  for (int i = 0; i < L.nvars; ++i) {
+    R* g = static_cast<R*>(P.var[L.var[i]]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) g[lo + q] = base[i * S + q];
+  }
+  {
+    uint8_t* g = static_cast<uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
+    for (int64_t q = tid; q < mine; q += blockDim.x) g[lo + q] = snr[q];
+  }
+  if (tid == 0 && rank == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
+}
+
 }  // namespace
 
 size_t small_smem(const SmallDev& D, int kind, int dtype) {
@@ -536,21 +769,25 @@ size_t small_smem(const SmallDev& D, int kind, int dtype) {
   return bytes;
 }
 
-// Shared memory of one CTA of the cluster form: its slice of the state and flags, and the
-// ring counts.
+// Shared memory of one CTA of the cluster form: its slice of the state and flags, then the
+// ring counts (push form) or the slice's bit rows, two local spike lists and the step's list
+// (pull form).
 size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const SmallLayout L = small_layout(kind);
   const size_t rs = dtype == B2B_F32 ? 4 : 8;
   const size_t S = (size_t)D.slice;
-  return ((rs * L.nvars * S + S + 15) & ~(size_t)15) +
-         sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
+  const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
+  if (D.pull)
+    return state + sizeof(uint32_t) * (size_t)D.n_proj * (size_t)D.pop.n * (S / 32) +
+           sizeof(int32_t) * (2 * S + (size_t)D.pop.n);
+  return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
 
 namespace {
 template <typename R, int K>
 cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps, double dt,
                               int32_t* status, cudaStream_t s, size_t smem, bool probe) {
-  auto kern = small_cluster_kernel<R, K>;
+  auto kern = D.pull ? small_pull_kernel<R, K> : small_cluster_kernel<R, K>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess && D.cluster > 8)
@@ -581,7 +818,7 @@ cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps
 cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
-      D.slice / 4 > kSmallThreads)
+      D.slice / 4 > kSmallThreads || (D.pull && (!D.pull_bits || D.slice % 32)))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)

@@ -699,20 +699,26 @@ def test_out_degree_matches_synapses(gpu_factory):
     np.testing.assert_array_equal(net.out_degree(ids["P"]), want)
 
 
-@pytest.mark.parametrize("case", ["cobahh_delays", "lif_onto_v_late_reset"])
+@pytest.mark.parametrize("case", ["cobahh_delays", "lif_onto_v_late_reset", "cuba"])
 def test_small_network_path_matches_per_step(gpu_factory, case):
     """The opt-in small-network path runs every step of a chunk in one CTA, or in one
     thread-block cluster of 8 or 16 CTAs (autotuner site kind 14), with the state in shared
-    memory; the result must be the per-step kernels' result exactly (every delivered weight
-    of one target variable is equal, so the order of the additions cannot change a sum)."""
+    memory, the cluster either pushing the effects or, for synapses without delays or
+    weights of their own (CUBA), pulling them at the targets; the result must be the
+    per-step kernels' result exactly (every delivered weight of one target variable is
+    equal, so the order of the additions cannot change a sum)."""
     from brian2cuda_b200._native import B2BError
     out = {}
-    for form in (1, 8, 16, False):
+    forms = [(1, 0), (8, 0), (16, 0), (8, 1), (16, 1), False]
+    for form in forms:
         small = form is not False
         net = gpu_factory(DT, small=small, two_launch=None if small else False)
         if case == "cobahh_delays":
             ids = models.build_cobahh(net, n=3000, p=0.05, monitor_capacity=10**6)
             G, steps = ids["P"], 300
+        elif case == "cuba":
+            ids = models.build_cuba(net, n=4000, dtype="float64")
+            G, steps = ids["P"], 400
         else:
             rng = np.random.default_rng(5)
             n = 700
@@ -725,19 +731,23 @@ def test_small_network_path_matches_per_step(gpu_factory, case):
             steps = 200
         net.finalize()
         assert net.run_mode == ("small" if small else "per-step")
-        if small and form > 1:
+        if small and form != (1, 0):
             try:
-                net.tune_apply([{"site_kind": 14, "site_index": 0, "choice_a": form,
-                                 "choice_b": 0}])
+                net.tune_apply([{"site_kind": 14, "site_index": 0, "choice_a": form[0],
+                                 "choice_b": form[1]}])
             except B2BError:
-                assert form == 16, "an 8-CTA cluster must be possible"
-                continue          # 16-CTA clusters are not available on this device
+                # the pull form needs synapses without delays; 16-CTA clusters a device
+                # that allows them; 8-CTA pushing clusters must always be possible
+                assert form != (8, 0)
+                continue
         net.run(steps)
         assert net.sync() == 0
         idx, st = net.spikes(G)
         out[form] = (idx, st, {v: net.get_state(G, v) for v in ("v", "ge", "gi", "lastspike")})
     assert len(out[False][0]) > 50
-    for form in (1, 8, 16):
+    if case == "cuba":
+        assert (8, 1) in out or (16, 1) in out, "the pull form must run CUBA"
+    for form in forms[:-1]:
         if form not in out:
             continue
         np.testing.assert_array_equal(out[form][0], out[False][0], err_msg=str(form))
