@@ -384,8 +384,10 @@ unsigned resident_clusters(const void* kern, size_t smem) {
   int clusters = 0;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess ||
-      cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess)
+      cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess) {
     clusters = 0;
+    cudaGetLastError();   // the refusal's error must not be reported by the next launch
+  }
   cache.emplace_back(smem, clusters);
   return (unsigned)clusters;
 }

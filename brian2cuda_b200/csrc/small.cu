@@ -832,7 +832,12 @@ cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t
 }  // namespace
 
 bool small_cluster_possible(const SmallDev& D, int kind, int dtype) {
-  return launch_cluster(D, kind, dtype, nullptr, 0, 0.0, nullptr, nullptr, true) == cudaSuccess;
+  const bool ok =
+      launch_cluster(D, kind, dtype, nullptr, 0, 0.0, nullptr, nullptr, true) == cudaSuccess;
+  // a refused attribute or occupancy query leaves its (non-sticky) error as the last error,
+  // which the next launch check would report as its own
+  if (!ok) cudaGetLastError();
+  return ok;
 }
 
 cudaError_t launch_small(const SmallDev& D, int kind, int dtype, const int64_t* clock,
