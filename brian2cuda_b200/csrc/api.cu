@@ -2025,10 +2025,9 @@ bool set_small_cluster(b2b_net* net, int c, bool pull) {
     D.slice = pop.n;
   } else {
     if ((c != 8 && c != 16) || (pull && !D.pull_bits)) return false;
-    const int64_t q = pull ? 32 : 4;
     D.cluster = c;
     D.pull = pull ? 1 : 0;
-    D.slice = ((pop.n + c - 1) / c + q - 1) / q * q;
+    D.slice = ((pop.n + c - 1) / c + 3) / 4 * 4;
     if (!small_cluster_possible(D, pop.kind, pop.dtype)) {
       D.cluster = c0;
       D.pull = p0;

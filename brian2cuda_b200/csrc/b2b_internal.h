@@ -212,8 +212,7 @@ struct SmallDev {
   int32_t ring_in_smem;                 // the spike-history ring is mirrored in shared memory
   int32_t cluster;                      // CTAs of the one thread-block cluster (1: one CTA)
   int32_t pull;                         // cluster form with the delivery pulled by targets
-  int64_t slice;                        // neurons per CTA of the cluster (multiple of 4; of
-                                        // 32 when pulling)
+  int64_t slice;                        // neurons per CTA of the cluster (multiple of 4)
   // pull form: per projection, bit rows [pre][n / 32 words] (bit of post set when pre
   // connects to it), or NULL when a synapse has a delay or a weight of its own
   const uint32_t* pull_bits;

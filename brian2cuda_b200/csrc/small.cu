@@ -528,8 +528,9 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
 // For a net whose every synapse has a delay of 0 steps and one weight per Synapses object
 // (the CUBA example), the effects of a step can be gathered by the target neurons instead
 // of scattered by the spikes: CTA r keeps, beside its slice of the state, the connectivity
-// of its slice as bit rows (bit j of row `pre` set when pre connects to neuron r S + j) in
-// shared memory.  A step is then one cluster barrier:
+// of the population as bit rows (bit i of row `pre` set when pre connects to neuron i; 2 MB
+// for 4096 neurons, resident in L2), and each target thread reads the words of its neurons.
+// A step is then one cluster barrier:
 //   update and threshold of the slice; compaction of its spikes into a local list (double
 //   buffered by step parity);
 //   barrier;
@@ -538,9 +539,9 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
 //   monitor (the per-step kernels' record of the step);
 //   each target neuron adds, for every spike whose bit row has its bit, that Synapses
 //   object's weight to its target variable (the synapses slot), then the deferred reset.
-// Inside the step loop global memory is written (ring, monitor) and read only for the group
-// parameters and the projections' member tables, a few cached entries.  A final barrier keeps
-// every CTA's lists alive until all CTAs have read them.
+// Inside the step loop global memory is written (ring, monitor) and read for the bit words
+// of the step's spikes, the group parameters and the projections' member tables.  A final
+// barrier keeps every CTA's lists alive until all CTAs have read them.
 template <typename R, int KIND>
 __global__ void __launch_bounds__(kSmallThreads, 1)
 small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
@@ -554,7 +555,6 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   const int64_t n = P.n;
   const int64_t lo = (int64_t)rank * S;
   const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;
-  const int64_t words = S / 32;                 // bit words per row of a slice
   R* const base = reinterpret_cast<R*>(smem);
   constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
   R* const sV = base;
@@ -565,9 +565,8 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   R* const sH = base + 4 * S;
   R* const sN = base + 5 * S;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
-  uint32_t* bits = reinterpret_cast<uint32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
-  int32_t* lists = reinterpret_cast<int32_t*>(bits + (int64_t)D.n_proj * n * words);   // [2][S]
-  int32_t* all = lists + 2 * S;                 // the step's spikes, [n]
+  int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
+  int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
   __shared__ int s_warp[33];
   __shared__ int s_cnt[2];
   __shared__ int s_pre[17];                     // counts of the ranks before each rank
@@ -583,15 +582,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const uint8_t* g = static_cast<const uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
     for (int64_t q = tid; q < mine; q += blockDim.x) snr[q] = g[lo + q];
   }
-  // this slice's columns of every projection's bit rows
   const int64_t row_words = n / 32;
-  for (int p = 0; p < D.n_proj; ++p)
-    for (int64_t x = tid; x < n * words; x += blockDim.x) {
-      const int64_t pre = x / words, w = x - pre * words;
-      const int64_t gw = lo / 32 + w;           // past the population for a partial slice
-      bits[((int64_t)p * n + pre) * words + w] =
-          gw < row_words ? D.pull_bits[((int64_t)p * n + pre) * row_words + gw] : 0u;
-    }
   if (tid == 0) s_mon = P.mon_cnt ? *P.mon_cnt : 0ull;
   __syncthreads();
 
@@ -714,22 +705,31 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     if (tid == 0) s_mon += (unsigned long long)tot;
     // ---- synapses slot: each target neuron gathers the effects of the step's spikes
     if (j4 < mine && tot > 0) {
-      const int64_t w = j4 / 32;
-      const int sh = (int)(j4 & 31);
+      const int64_t w = (lo + j4) / 32;         // the word holding this thread's 4 neurons
+      const int sh = (int)((lo + j4) & 31);
       for (int p = 0; p < D.n_proj; ++p) {
         const ProjDev& J = D.proj[p];
-        const uint32_t* B = bits + (int64_t)p * n * words;
-        for (int x = 0; x < tot; ++x) {
-          const int32_t pre = all[x];
-          const unsigned b4 = (B[(int64_t)pre * words + w] >> sh) & 0xFu;
-          if (!b4) continue;
-          const int m = J.n_mem == 1 ? 0 : member_of(J, pre);
-          const int var = J.n_mem == 1 ? D.proj_target[p] : (int)J.mem_var[m];
-          const R wgt = (R)(J.mem_w ? J.mem_w[m] : J.w_scalar);
-          R* T = base + var * S;                    // v, ge, gi: columns 0-2
+        const uint32_t* B = D.pull_bits + (int64_t)p * n * row_words;
+        // four spikes' words loaded before any is used, in spike order
+        for (int x0 = 0; x0 < tot; x0 += 4) {
+          int32_t pre[4];
+          unsigned b4[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (b4 & (1u << e)) T[j4 + e] += wgt;
+          for (int u = 0; u < 4; ++u) {
+            pre[u] = x0 + u < tot ? all[x0 + u] : -1;
+            b4[u] = pre[u] >= 0 ? (__ldg(B + (int64_t)pre[u] * row_words + w) >> sh) & 0xFu : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (!b4[u]) continue;
+            const int m = J.n_mem == 1 ? 0 : member_of(J, pre[u]);
+            const int var = J.n_mem == 1 ? D.proj_target[p] : (int)J.mem_var[m];
+            const R wgt = (R)(J.mem_w ? J.mem_w[m] : J.w_scalar);
+            R* T = base + var * S;                  // v, ge, gi: columns 0-2
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (b4[u] & (1u << e)) T[j4 + e] += wgt;
+          }
         }
       }
     }
@@ -777,9 +777,7 @@ size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const size_t rs = dtype == B2B_F32 ? 4 : 8;
   const size_t S = (size_t)D.slice;
   const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
-  if (D.pull)
-    return state + sizeof(uint32_t) * (size_t)D.n_proj * (size_t)D.pop.n * (S / 32) +
-           sizeof(int32_t) * (2 * S + (size_t)D.pop.n);
+  if (D.pull) return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n);
   return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
 
@@ -818,7 +816,7 @@ cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps
 cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
-      D.slice / 4 > kSmallThreads || (D.pull && (!D.pull_bits || D.slice % 32)))
+      D.slice / 4 > kSmallThreads || (D.pull && !D.pull_bits))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)
