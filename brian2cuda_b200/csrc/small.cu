@@ -30,6 +30,9 @@ namespace b2b {
 namespace {
 
 constexpr int kSmallThreads = 1024;
+// the pull form keeps these in shared memory (larger nets use the push form)
+constexpr int kPullMaxGroups = 16;
+constexpr int kPullMaxMembers = 16;
 
 // Shared-memory image of the population: one array per real-valued variable of the kind,
 // then the not_refractory flags, then the delivery prefix of the block path.
@@ -567,12 +570,39 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
   int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
   int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
+  int32_t* s_vg = all + n;                      // group of each 4 neurons of the slice
   __shared__ int s_warp[33];
   __shared__ int s_cnt[2];
   __shared__ int s_pre[17];                     // counts of the ranks before each rank
   __shared__ unsigned long long s_mon;
+  // The cluster barrier's acquire empties the L1 cache every step, so whatever the step loop
+  // reads repeatedly lives in shared memory: the groups' parameters, the slice's group ids and
+  // the projections' member tables (Synapses object of a presynaptic range: target variable
+  // and weight).
+  __shared__ __align__(16) unsigned char s_prm[kPullMaxGroups * sizeof(HhDev)];
+  __shared__ int64_t s_mhi[kMaxProjBatch][kPullMaxMembers];
+  __shared__ int32_t s_mvar[kMaxProjBatch][kPullMaxMembers];
+  __shared__ double s_mw[kMaxProjBatch][kPullMaxMembers];
+  __shared__ int32_t s_nmem[kMaxProjBatch];
   const int tid = threadIdx.x;
   const int64_t ts0 = clock[0];
+  {
+    const size_t psz = KIND == KIND_LIF ? sizeof(LifDev) : sizeof(HhDev);
+    const unsigned char* gp = static_cast<const unsigned char*>(P.params);
+    for (size_t b = tid; b < psz * (size_t)P.n_groups; b += blockDim.x) s_prm[b] = gp[b];
+    for (int64_t q = tid; q < (mine + 3) / 4; q += blockDim.x)
+      s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
+    for (int x = tid; x < D.n_proj * kPullMaxMembers; x += blockDim.x) {
+      const int p = x / kPullMaxMembers, m = x - p * kPullMaxMembers;
+      const ProjDev& J = D.proj[p];
+      if (m == 0) s_nmem[p] = J.n_mem;
+      if (m < J.n_mem) {
+        s_mhi[p][m] = J.n_mem == 1 ? INT64_MAX : J.mem_hi[m];
+        s_mvar[p][m] = J.n_mem == 1 ? D.proj_target[p] : (int32_t)J.mem_var[m];
+        s_mw[p][m] = J.mem_w ? J.mem_w[m] : J.w_scalar;
+      }
+    }
+  }
 
   for (int i = 0; i < L.nvars; ++i) {
     const R* g = static_cast<const R*>(P.var[L.var[i]]);
@@ -597,7 +627,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     unsigned fl = 0;
     const int64_t j4 = 4 * (int64_t)tid;
     if (j4 < mine) {
-      const int gidx = P.vec_group ? P.vec_group[(lo + j4) >> 2] : 0;
+      const int gidx = s_vg[j4 >> 2];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int64_t jl = j4 + e;
@@ -606,7 +636,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
         R ls = sLS[jl];
         bool nr = true;
         if constexpr (KIND == KIND_LIF) {
-          const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
+          const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
           const bool refr = g.ref_steps >= 0;
           if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
           R vn = lif_advance<R>(
@@ -624,7 +654,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
             snr[jl] = nr ? 1 : 0;
           }
         } else {
-          const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
+          const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
           const bool refr = g.ref_steps >= 0;
           if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
           R m = sM[jl], h = sH[jl], nn = sN[jl];
@@ -664,13 +694,11 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     if (tid == 0) s_cnt[par] = total;
     cl.sync();
     // ---- every CTA's spikes of the step, in rank order
-    if (tid == 0) {
-      int acc = 0;
-      for (int q = 0; q < C; ++q) {
-        s_pre[q] = acc;
-        acc += *cl.map_shared_rank(&s_cnt[par], (unsigned)q);
-      }
-      s_pre[C] = acc;
+    if (tid < 32) {   // warp 0: one rank's count per lane, then their prefix
+      const int cq = tid < C ? *cl.map_shared_rank(&s_cnt[par], (unsigned)tid) : 0;
+      const int incl = warp_incl_scan(cq);
+      if (tid < C) s_pre[tid] = incl - cq;
+      if (tid == 31) s_pre[C] = incl;
     }
     __syncthreads();
     const int tot = s_pre[C];
@@ -708,7 +736,6 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
       const int64_t w = (lo + j4) / 32;         // the word holding this thread's 4 neurons
       const int sh = (int)((lo + j4) & 31);
       for (int p = 0; p < D.n_proj; ++p) {
-        const ProjDev& J = D.proj[p];
         const uint32_t* B = D.pull_bits + (int64_t)p * n * row_words;
         // four spikes' words loaded before any is used, in spike order
         for (int x0 = 0; x0 < tot; x0 += 4) {
@@ -722,10 +749,13 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (!b4[u]) continue;
-            const int m = J.n_mem == 1 ? 0 : member_of(J, pre[u]);
-            const int var = J.n_mem == 1 ? D.proj_target[p] : (int)J.mem_var[m];
-            const R wgt = (R)(J.mem_w ? J.mem_w[m] : J.w_scalar);
-            R* T = base + var * S;                  // v, ge, gi: columns 0-2
+            int m = 0, mh = s_nmem[p] - 1;          // the member whose range holds pre
+            while (m < mh) {
+              const int mid = (m + mh) >> 1;
+              if (pre[u] < s_mhi[p][mid]) mh = mid; else m = mid + 1;
+            }
+            R* T = base + s_mvar[p][m] * S;         // v, ge, gi: columns 0-2
+            const R wgt = (R)s_mw[p][m];
 #pragma unroll
             for (int e = 0; e < 4; ++e)
               if (b4[u] & (1u << e)) T[j4 + e] += wgt;
@@ -738,7 +768,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
       if (P.late_reset) {
         for (int x = tid; x < total; x += blockDim.x) {
           const int32_t i = mylist[x];
-          const LifDev& g = static_cast<const LifDev*>(P.params)[P.vec_group ? P.vec_group[i >> 2] : 0];
+          const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[s_vg[(i - lo) >> 2]];
           if (g.has_reset) sV[i - lo] = (R)g.Vr;
         }
       }
@@ -777,11 +807,17 @@ size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const size_t rs = dtype == B2B_F32 ? 4 : 8;
   const size_t S = (size_t)D.slice;
   const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
-  if (D.pull) return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n);
+  if (D.pull) return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4);
   return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
 
 namespace {
+bool pull_members_fit(const SmallDev& D) {
+  for (int p = 0; p < D.n_proj; ++p)
+    if (D.proj[p].n_mem > kPullMaxMembers) return false;
+  return true;
+}
+
 template <typename R, int K>
 cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps, double dt,
                               int32_t* status, cudaStream_t s, size_t smem, bool probe) {
@@ -816,7 +852,8 @@ cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps
 cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
-      D.slice / 4 > kSmallThreads || (D.pull && !D.pull_bits))
+      D.slice / 4 > kSmallThreads ||
+      (D.pull && (!D.pull_bits || D.pop.n_groups > kPullMaxGroups || !pull_members_fit(D))))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)
