@@ -623,68 +623,79 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const int slot = ring_slot(ts, P.ring_len);
     const int par = k & 1;
     int32_t* mylist = lists + par * S;
-    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
+    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3, each variable of the
+    // four read and written as one vector, the four updates independent of each other
     unsigned fl = 0;
     const int64_t j4 = 4 * (int64_t)tid;
     if (j4 < mine) {
       const int gidx = s_vg[j4 >> 2];
+      Pack<R, 4> V = load_pack<R, 4>(sV, tid), GE = load_pack<R, 4>(sGE, tid);
+      Pack<R, 4> GI = load_pack<R, 4>(sGI, tid), LS = load_pack<R, 4>(sLS, tid);
+      uint32_t NR = 0;
+      if constexpr (KIND == KIND_LIF) {
+        const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
+        const bool refr = g.ref_steps >= 0;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int64_t jl = j4 + e;
-        const int64_t i = lo + jl;
-        R v = sV[jl], ge = sGE[jl], gi = sGI[jl];
-        R ls = sLS[jl];
-        bool nr = true;
-        if constexpr (KIND == KIND_LIF) {
-          const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
-          const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+        for (int e = 0; e < 4; ++e) {
+          const int64_t i = lo + j4 + e;
+          bool nr = true;
+          if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
           R vn = lif_advance<R>(
-              g, v, ge, gi, nr,
+              g, V.x[e], GE.x[e], GI.x[e], nr,
               P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
           if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
             nr = false;
-            if (refr) ls = (R)t;
+            if (refr) LS.x[e] = (R)t;
             if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
             fl |= 1u << e;
           }
-          v = vn;
-          if (refr) {
-            sLS[jl] = ls;
-            snr[jl] = nr ? 1 : 0;
-          }
-        } else {
-          const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
-          const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
-          R m = sM[jl], h = sH[jl], nn = sN[jl];
-          const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
+          V.x[e] = vn;
+          NR |= (nr ? 1u : 0u) << (8 * e);
+        }
+        if (refr) {
+          store_pack<R, 4>(sLS, tid, LS);
+          store_flags<4>(snr, tid, NR);
+        }
+      } else {
+        const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
+        const bool refr = g.ref_steps >= 0;
+        Pack<R, 4> M = load_pack<R, 4>(sM, tid), H = load_pack<R, 4>(sH, tid);
+        Pack<R, 4> NN = load_pack<R, 4>(sN, tid);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int64_t i = lo + j4 + e;
+          bool nr = true;
+          if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+          const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], NN.x[e], GE.x[e], GI.x[e],
+                                     (R)dt,
                                      P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
                                                                i - g.offset)
                                               : R(0));
           if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
             nr = false;
-            if (refr) ls = (R)t;
+            if (refr) LS.x[e] = (R)t;
             fl |= 1u << e;
           }
-          v = vn;
-          sM[jl] = m;
-          sH[jl] = h;
-          sN[jl] = nn;
-          if (refr) {
-            sLS[jl] = ls;
-            snr[jl] = nr ? 1 : 0;
-          }
+          V.x[e] = vn;
+          NR |= (nr ? 1u : 0u) << (8 * e);
         }
-        sV[jl] = v;
-        sGE[jl] = ge;
-        sGI[jl] = gi;
+        store_pack<R, 4>(sM, tid, M);
+        store_pack<R, 4>(sH, tid, H);
+        store_pack<R, 4>(sN, tid, NN);
+        if (refr) {
+          store_pack<R, 4>(sLS, tid, LS);
+          store_flags<4>(snr, tid, NR);
+        }
       }
+      store_pack<R, 4>(sV, tid, V);
+      store_pack<R, 4>(sGE, tid, GE);
+      store_pack<R, 4>(sGI, tid, GI);
     }
     // ---- this CTA's spikes into its local list (ascending neuron order)
-    int total;
+    // (most CTAs of most steps have no spike: one barrier decides that for the CTA)
+    int total = 0, excl = 0;
     const int c = __popc(fl);
-    const int excl = block_exclusive_scan(c, s_warp, &total);
+    if (__syncthreads_or(fl != 0)) excl = block_exclusive_scan(c, s_warp, &total);
     if (c) {
       int pos = excl;
 #pragma unroll
