@@ -534,18 +534,17 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
 // of the population as bit rows (bit i of row `pre` set when pre connects to neuron i; 2 MB
 // for 4096 neurons, resident in L2), and each target thread reads the words of its neurons.
 // A step is then one cluster barrier:
-//   update and threshold of the slice; compaction of its spikes, each written straight into
-//   this rank's segment of every CTA's shared memory (double buffered by step parity), and
-//   the count into every CTA's table;
-//   barrier: every CTA now holds the step's spikes of the whole population locally;
-//   each CTA writes its own spikes at their offset into the global ring and monitor (the
-//   per-step kernels' record of the step), and each target neuron adds, for every spike whose
-//   bit row has its bit, that Synapses object's weight to its target variable (the synapses
-//   slot), then the deferred reset.
-// Nothing is read from another CTA's shared memory, and inside the step loop global memory
-// is read only for the bit words of the step's spikes.  The group parameters, group ids and
-// member tables are copied to shared memory first: the cluster barrier's acquire empties the
-// L1 cache every step.
+//   update and threshold of the slice; compaction of its spikes into a local list (double
+//   buffered by step parity);
+//   barrier;
+//   every CTA copies all CTAs' lists (distributed shared memory) into one list of the step's
+//   spikes, in rank order, and writes its own spikes at their offset into the global ring and
+//   monitor (the per-step kernels' record of the step);
+//   each target neuron adds, for every spike whose bit row has its bit, that Synapses
+//   object's weight to its target variable (the synapses slot), then the deferred reset.
+// Inside the step loop global memory is written (ring, monitor) and read for the bit words
+// of the step's spikes, the group parameters and the projections' member tables.  A final
+// barrier keeps every CTA's lists alive until all CTAs have read them.
 template <typename R, int KIND>
 __global__ void __launch_bounds__(kSmallThreads, 1)
 small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
@@ -569,16 +568,17 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   R* const sH = base + 4 * S;
   R* const sN = base + 5 * S;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
-  // segs[par][q][0 .. S): the spikes of rank q's slice in the step of parity par, written
-  // into every CTA's shared memory by rank q itself
-  int32_t* segs = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
-  int32_t* s_vg = segs + 2 * (int64_t)C * S;    // group of each 4 neurons of the slice
+  int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
+  int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
+  int32_t* s_vg = all + n;                      // group of each 4 neurons of the slice
   __shared__ int s_warp[33];
-  __shared__ int s_cnts[2][16];                 // [par][q]: rank q's spike count
+  __shared__ int s_cnt[2];
+  __shared__ int s_pre[17];                     // counts of the ranks before each rank
   __shared__ unsigned long long s_mon;
-  // what the step loop reads repeatedly: the groups' parameters, the slice's group ids and
+  // The cluster barrier's acquire empties the L1 cache every step, so whatever the step loop
+  // reads repeatedly lives in shared memory: the groups' parameters, the slice's group ids and
   // the projections' member tables (Synapses object of a presynaptic range: target variable
-  // and weight)
+  // and weight).
   __shared__ __align__(16) unsigned char s_prm[kPullMaxGroups * sizeof(HhDev)];
   __shared__ int64_t s_mhi[kMaxProjBatch][kPullMaxMembers];
   __shared__ int32_t s_mvar[kMaxProjBatch][kPullMaxMembers];
@@ -622,6 +622,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const double t = (double)ts * dt;
     const int slot = ring_slot(ts, P.ring_len);
     const int par = k & 1;
+    int32_t* mylist = lists + par * S;
     // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3, each variable of the
     // four read and written as one vector, the four updates independent of each other
     unsigned fl = 0;
@@ -690,35 +691,39 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
       store_pack<R, 4>(sGE, tid, GE);
       store_pack<R, 4>(sGI, tid, GI);
     }
-    // ---- this CTA's spikes, in ascending neuron order, into its segment of every CTA's
-    // shared memory (most CTAs of most steps have none: one barrier decides that)
+    // ---- this CTA's spikes into its local list (ascending neuron order)
+    // (most CTAs of most steps have no spike: one barrier decides that for the CTA)
     int total = 0, excl = 0;
     const int c = __popc(fl);
     if (__syncthreads_or(fl != 0)) excl = block_exclusive_scan(c, s_warp, &total);
-    int32_t* myseg = segs + ((int64_t)par * C + rank) * S;
     if (c) {
       int pos = excl;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        if (!(fl & (1u << e))) continue;
-        const int32_t idx = (int32_t)(lo + j4 + e);
-        for (int q = 0; q < C; ++q) *cl.map_shared_rank(myseg + pos, (unsigned)q) = idx;
-        ++pos;
-      }
+      for (int e = 0; e < 4; ++e)
+        if (fl & (1u << e)) mylist[pos++] = (int32_t)(lo + j4 + e);
     }
-    if (tid < C) *cl.map_shared_rank(&s_cnts[par][rank], (unsigned)tid) = total;
-    cl.sync();   // every CTA's segments and counts of this step are here
-    int tot = 0, off = 0;
-    for (int q = 0; q < C; ++q) {
-      const int cq = s_cnts[par][q];
-      if (q < rank) off += cq;
-      tot += cq;
+    if (tid == 0) s_cnt[par] = total;
+    cl.sync();
+    // ---- every CTA's spikes of the step, in rank order
+    if (tid < 32) {   // warp 0: one rank's count per lane, then their prefix
+      const int cq = tid < C ? *cl.map_shared_rank(&s_cnt[par], (unsigned)tid) : 0;
+      const int incl = warp_incl_scan(cq);
+      if (tid < C) s_pre[tid] = incl - cq;
+      if (tid == 31) s_pre[C] = incl;
+    }
+    __syncthreads();
+    const int tot = s_pre[C];
+    for (int x = tid; x < tot; x += blockDim.x) {
+      int q = 0;
+      while (q + 1 < C && s_pre[q + 1] <= x) ++q;
+      all[x] = *cl.map_shared_rank(lists + par * S + (x - s_pre[q]), (unsigned)q);
     }
     // the per-step kernels' record of the step: global ring slot and monitor
     {
+      const int off = s_pre[rank];
       int32_t* out = P.ring_idx + (int64_t)slot * P.n;
       for (int x = tid; x < total; x += blockDim.x) {
-        const int32_t idx = myseg[x];
+        const int32_t idx = mylist[x];
         out[off + x] = idx;
         if (P.mon_cnt) {
           const unsigned long long mpos = s_mon + (unsigned long long)(off + x);
@@ -735,39 +740,36 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
         P.ring_cnt[ring_slot(ts + 1, P.ring_len)] = 0;
       }
     }
+    __syncthreads();
+    if (tid == 0) s_mon += (unsigned long long)tot;
     // ---- synapses slot: each target neuron gathers the effects of the step's spikes
     if (j4 < mine && tot > 0) {
       const int64_t w = (lo + j4) / 32;         // the word holding this thread's 4 neurons
       const int sh = (int)((lo + j4) & 31);
       for (int p = 0; p < D.n_proj; ++p) {
         const uint32_t* B = D.pull_bits + (int64_t)p * n * row_words;
-        for (int q = 0; q < C; ++q) {
-          const int cq = s_cnts[par][q];
-          const int32_t* seg = segs + ((int64_t)par * C + q) * S;
-          // four spikes' words loaded before any is used, in spike order
-          for (int x0 = 0; x0 < cq; x0 += 4) {
-            int32_t pre[4];
-            unsigned b4[4];
+        // four spikes' words loaded before any is used, in spike order
+        for (int x0 = 0; x0 < tot; x0 += 4) {
+          int32_t pre[4];
+          unsigned b4[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              pre[u] = x0 + u < cq ? seg[x0 + u] : -1;
-              b4[u] = pre[u] >= 0 ? (__ldg(B + (int64_t)pre[u] * row_words + w) >> sh) & 0xFu
-                                  : 0u;
+          for (int u = 0; u < 4; ++u) {
+            pre[u] = x0 + u < tot ? all[x0 + u] : -1;
+            b4[u] = pre[u] >= 0 ? (__ldg(B + (int64_t)pre[u] * row_words + w) >> sh) & 0xFu : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (!b4[u]) continue;
+            int m = 0, mh = s_nmem[p] - 1;          // the member whose range holds pre
+            while (m < mh) {
+              const int mid = (m + mh) >> 1;
+              if (pre[u] < s_mhi[p][mid]) mh = mid; else m = mid + 1;
             }
+            R* T = base + s_mvar[p][m] * S;         // v, ge, gi: columns 0-2
+            const R wgt = (R)s_mw[p][m];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (!b4[u]) continue;
-              int m = 0, mh = s_nmem[p] - 1;        // the member whose range holds pre
-              while (m < mh) {
-                const int mid = (m + mh) >> 1;
-                if (pre[u] < s_mhi[p][mid]) mh = mid; else m = mid + 1;
-              }
-              R* T = base + s_mvar[p][m] * S;       // v, ge, gi: columns 0-2
-              const R wgt = (R)s_mw[p][m];
-#pragma unroll
-              for (int e = 0; e < 4; ++e)
-                if (b4[u] & (1u << e)) T[j4 + e] += wgt;
-            }
+            for (int e = 0; e < 4; ++e)
+              if (b4[u] & (1u << e)) T[j4 + e] += wgt;
           }
         }
       }
@@ -776,16 +778,15 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     if constexpr (KIND == KIND_LIF) {
       if (P.late_reset) {
         for (int x = tid; x < total; x += blockDim.x) {
-          const int32_t i = myseg[x];
+          const int32_t i = mylist[x];
           const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[s_vg[(i - lo) >> 2]];
           if (g.has_reset) sV[i - lo] = (R)g.Vr;
         }
       }
     }
-    if (tid == 0) s_mon += (unsigned long long)tot;
     __syncthreads();
   }
-  cl.sync();   // no CTA writes into another's segments any more
+  cl.sync();   // every CTA is done reading the others' lists
   for (int i = 0; i < L.nvars; ++i) {
     R* g = static_cast<R*>(P.var[L.var[i]]);
     for (int64_t q = tid; q < mine; q += blockDim.x) g[lo + q] = base[i * S + q];
@@ -810,14 +811,14 @@ size_t small_smem(const SmallDev& D, int kind, int dtype) {
 }
 
 // Shared memory of one CTA of the cluster form: its slice of the state and flags, then the
-// ring counts (push form) or every rank's spike segment for two step parities and the
-// slice's group ids (pull form).
+// ring counts (push form) or the slice's bit rows, two local spike lists and the step's list
+// (pull form).
 size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const SmallLayout L = small_layout(kind);
   const size_t rs = dtype == B2B_F32 ? 4 : 8;
   const size_t S = (size_t)D.slice;
   const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
-  if (D.pull) return state + sizeof(int32_t) * (2 * (size_t)D.cluster * S + (S + 3) / 4);
+  if (D.pull) return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4);
   return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
 
