@@ -743,12 +743,14 @@ b2b_status setup_monitors(b2b_net* net) {
   return B2B_OK;
 }
 
-// A small network (small.cu, opt-in with B2B_NET_SMALL) runs every step of a chunk in one
-// CTA: one LIF/HH population of at most 4096 neurons (no gating surrogate) whose Synapses
-// objects are all additive and target it, with the state fitting the CTA's shared memory.
+// A small network (small.cu) runs every step of a chunk in one CTA or one thread-block
+// cluster: one LIF/HH population of at most 4096 neurons (no gating surrogate) whose
+// Synapses objects are all additive and target it, with the state fitting the CTA's shared
+// memory.  B2B_NET_SMALL selects the path; otherwise b2b_autotune may (site kind 14).
 b2b_status setup_small(b2b_net* net) {
-  if (!(net->cfg.flags & B2B_NET_SMALL) || (net->cfg.flags & (B2B_NET_CHECKED | B2B_NET_TWO_LAUNCH)))
-    return B2B_OK;
+  const int32_t flags = net->cfg.flags;
+  if (flags & (B2B_NET_CHECKED | B2B_NET_TWO_LAUNCH | B2B_NET_ONE_LAUNCH)) return B2B_OK;
+  if ((flags & B2B_NET_PER_STEP) && !(flags & B2B_NET_SMALL)) return B2B_OK;
   if (!net->smons.empty() || !net->rmons.empty()) return B2B_OK;  // per-step path records
   if (net->pops.size() != 1 || net->projs.size() > kMaxProjBatch) return B2B_OK;
   const Pop& pop = net->pops[0];
@@ -811,7 +813,8 @@ b2b_status setup_small(b2b_net* net) {
       D.pull_bits = d;
     }
   }
-  net->small = true;
+  net->small_ok = true;
+  net->small = (flags & B2B_NET_SMALL) != 0;
   return B2B_OK;
 }
 
@@ -2385,6 +2388,32 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
       net->one_launch = builtin_one_launch;
       net->one_launch_chained = false;
     }
+    // a net that allows the small-network path: its forms against the step as tuned above
+    if (net->small_ok && st == B2B_OK) {
+      double base_ms = 0;
+      st = trial(&base_ms);
+      b2b_tune_result r{14, 0, 0, 0, base_ms, base_ms};
+      const std::pair<int, int> forms[] = {{1, 0}, {8, 0}, {16, 0}, {8, 1}, {16, 1}};
+      for (const auto& f : forms) {
+        if (st != B2B_OK) break;
+        net->small = true;
+        if (!set_small_cluster(net, f.first, f.second != 0)) continue;
+        double ms = 0;
+        st = trial(&ms);
+        if (st == B2B_OK && ms < kTuneMargin * r.best_ms) {
+          r.best_ms = ms;
+          r.choice_a = f.first;
+          r.choice_b = f.second;
+        }
+      }
+      net->small = r.choice_a > 0;
+      if (net->small) set_small_cluster(net, r.choice_a, r.choice_b != 0);
+      if (net->graph) {
+        cudaGraphExecDestroy(net->graph);
+        net->graph = nullptr;
+      }
+      res.push_back(r);
+    }
   }
   // back to the starting state; the next b2b_run captures a graph with the chosen shapes
   b2b_status st2 = b2b_restore(net, slot);
@@ -2461,12 +2490,26 @@ b2b_status b2b_tune_apply(b2b_net* net, const b2b_tune_result* r, int32_t n) {
             B2B_ERR_INVALID_ARG, "bad delivery launch shape");
       set_pending_shape(net, t.choice_a, t.choice_b);
     } else if (t.site_kind == 14) {
-      CHECK(net->small && t.site_index == 0, B2B_ERR_INVALID_ARG,
-            "site kind 14 exists only for a net on the small-network path");
+      CHECK(net->small_ok && t.site_index == 0, B2B_ERR_INVALID_ARG,
+            "site kind 14 exists only for a net that allows the small-network path");
       CHECK(t.choice_b == 0 || t.choice_b == 1, B2B_ERR_INVALID_ARG, "bad small-path form");
-      CHECK(set_small_cluster(net, t.choice_a, t.choice_b == 1), B2B_ERR_UNSUPPORTED,
-            "the small-network path cannot run as %d CTAs%s here", t.choice_a,
-            t.choice_b == 1 ? " pulling the effects" : "");
+      CHECK(t.choice_a != 0 || !(net->cfg.flags & B2B_NET_SMALL), B2B_ERR_INVALID_ARG,
+            "B2B_NET_SMALL keeps the small-network path");
+      if (t.choice_a == 0) {
+        net->small = false;
+        if (net->graph) {
+          cudaGraphExecDestroy(net->graph);
+          net->graph = nullptr;
+        }
+      } else {
+        const bool was = net->small;
+        net->small = true;
+        if (!set_small_cluster(net, t.choice_a, t.choice_b == 1)) {
+          net->small = was;
+          CHECK(false, B2B_ERR_UNSUPPORTED, "the small-network path cannot run as %d CTAs%s here",
+                t.choice_a, t.choice_b == 1 ? " pulling the effects" : "");
+        }
+      }
     } else if (t.site_kind == 8) {
       CHECK(t.site_index >= 0 && t.site_index < (int32_t)net->projs.size() &&
                 net->projs[t.site_index].effect == B2B_EFFECT_STDP,
@@ -2820,11 +2863,22 @@ b2b_status b2b_syn_set_delays(b2b_net* net, int32_t sid, const int32_t* delay_st
   CHECK(!sy.generated, B2B_ERR_UNSUPPORTED,
         "delays of connectivity generated on the GPU are fixed");
   CHECK(sy.effect == B2B_EFFECT_ADD, B2B_ERR_UNSUPPORTED, "delays of STDP synapses are fixed");
-  CHECK(!net->small, B2B_ERR_UNSUPPORTED, "the one-CTA small form keeps its delays");
+  CHECK(!(net->cfg.flags & B2B_NET_SMALL), B2B_ERR_UNSUPPORTED,
+        "B2B_NET_SMALL keeps the small-network path, whose delays are fixed");
   CHECK(delay_steps && n == sy.n, B2B_ERR_INVALID_ARG, "n must be the synapse count");
   for (int64_t k = 0; k < n; ++k)
     CHECK(delay_steps[k] >= 0, B2B_ERR_INVALID_ARG, "negative delay at synapse %lld",
           (long long)k);
+  // the small-network path, if the autotuner chose it, hands over to the per-step kernels
+  // (its connectivity views are built once)
+  if (net->small_ok) {
+    net->small = false;
+    net->small_ok = false;
+    if (net->graph) {
+      cudaGraphExecDestroy(net->graph);
+      net->graph = nullptr;
+    }
+  }
   GUARD_BEGIN
   CU(cudaStreamSynchronize(net->stream));
   if (net->graph) {

@@ -365,7 +365,8 @@ struct b2b_net {
   b2b::RateMonDev* d_rmons = nullptr;
   int64_t smon_max_idx = 0;                // largest recorded index count
   std::vector<void*> mon_allocs;
-  bool small = false;                      // one CTA runs every step (small.cu)
+  bool small = false;                      // the small-network path runs every step (small.cu)
+  bool small_ok = false;                   // the net allows that path (sdev is built)
   b2b::SmallDev sdev{};
   bool two_launch = false;                 // the step as two concurrent launches (pending.cu)
   bool two_launch_ok = false;              // the net allows them (their buffers exist)

@@ -70,11 +70,14 @@ enum {
                              the two launches when its population has at most 2^18 neurons,
                              and b2b_autotune picks the faster of the two forms             */
   B2B_NET_SMALL = 16,     /* run a small network (one LIF/HH population of <= 4096 neurons
-                             with additive synapses onto itself) in one CTA per chunk of
-                             steps, with the state in shared memory; faster than the
-                             per-step kernels only for nets of a few hundred to ~2000
-                             neurons with few delays (measured: 500-neuron CUBA 3.8 vs
-                             4.9 us per step); otherwise per-step kernels                */
+                             with additive synapses onto itself) on the small-network path:
+                             every step of a chunk in one launch, the state in shared
+                             memory, as one CTA or as one thread-block cluster of 8 or 16
+                             CTAs (b2b_autotune site kind 14), the cluster either pushing
+                             the effects or, for synapses without delays or weights of their
+                             own, gathering them at the targets.  Without this flag such a
+                             net runs the per-step kernels until b2b_autotune measures the
+                             path faster (CUBA 4000: 4.3 against 5.4 us per step)         */
   B2B_NET_PER_STEP = 32,  /* always the per-step kernels (one launch per population, then
                              the delivery), never the two concurrent launches             */
   B2B_NET_ONE_LAUNCH = 64 /* where the net allows the two concurrent launches (see
@@ -418,7 +421,10 @@ typedef struct {
                             12 additive delivery launch accumulated in the distributed
                             shared memory of 8-CTA thread-block clusters (choice_a 1) or
                             with one global atomic per event (0); float32 launches onto
-                            one population of at most ~400k padded elements             */
+                            one population of at most ~400k padded elements;
+                            14 the small-network path: choice_a 0 not used, 1 one CTA,
+                            8 or 16 a cluster of that many CTAs, choice_b 1 gathering the
+                            effects at the targets                                        */
   int32_t site_index;    /* population / delivery launch / projection index              */
   int32_t choice_a;      /* neurons per thread (surrogate: CTAs per SM) / lanes per item /
                             record order / step form                                      */

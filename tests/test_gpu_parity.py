@@ -631,8 +631,11 @@ def test_autotune_keeps_state_and_results(gpu_factory):
         if tuned:
             res = net.autotune(trial_steps=10)
             kinds = {r["site_kind"] for r in res}
-            assert kinds == {1, 6}
+            # one population of <= 4096 neurons: the small-network path is tried too (14)
+            assert kinds == {1, 6, 14}
             assert all(r["best_ms"] <= r["default_ms"] for r in res)
+            small = [r for r in res if r["site_kind"] == 14][0]
+            assert net.run_mode == ("small" if small["choice_a"] > 0 else "per-step")
             after = (net.timestep, net.get_state(ids["P"], "v"), len(net.spikes(ids["P"])[0]))
             assert after[0] == before[0] and after[2] == before[2]
             np.testing.assert_array_equal(after[1], before[1])
@@ -671,7 +674,11 @@ def test_autotune_chooses_step_form(gpu_factory):
             kinds = [r["site_kind"] for r in res]
             assert {1, 6, 5, 11} <= set(kinds), kinds
             form = [r for r in res if r["site_kind"] == 11][0]
-            assert net.run_mode == mode_of[form["choice_a"]]
+            small = [r for r in res if r["site_kind"] == 14]
+            if small and small[0]["choice_a"] > 0:   # the small-network path won
+                assert net.run_mode == "small"
+            else:
+                assert net.run_mode == mode_of[form["choice_a"]]
             np.testing.assert_array_equal(net.get_state(G, "v"), v0)
             assert net.timestep == 60
         elif mode != "untuned":
