@@ -55,7 +55,7 @@ enum { B2B_F32 = 1, B2B_F64 = 2 };
 /* Network flags (b2b_config.flags). */
 enum {
   B2B_NET_NO_GRAPH = 1,   /* launch every step eagerly instead of replaying CUDA graphs */
-  B2B_NET_CHECKED = 2,    /* every launch site a kernel of its own (no one-CTA small form,
+  B2B_NET_CHECKED = 2,    /* every launch site a kernel of its own (no small-network path,
                              no two-launch form unless B2B_NET_TWO_LAUNCH is also set), so a
                              fault or a device status names one launch; input indices are
                              checked on the host in every mode (B2B_ERR_INDEX)           */
@@ -174,7 +174,7 @@ b2b_status b2b_timedarray(b2b_net* net, int32_t gid, const double* values, int64
  * seed.  The draw is exact inversion for every n * p (the reference switches to a normal
  * approximation above n p = 5).  At most two per group; before b2b_finalize.  *pid receives
  * the input's index (its random stream).  Not combinable with the gating surrogate; a net
- * with one runs the per-step or two-launch form, not the one-CTA small form. */
+ * with one runs the per-step or two-launch form, not the small-network path. */
 b2b_status b2b_poisson_input(b2b_net* net, int32_t gid, int32_t var, int64_t n_inputs,
                              double rate_hz, double weight, int32_t* pid);
 
@@ -329,7 +329,9 @@ b2b_status b2b_syn_count(b2b_net* net, int32_t sid, int64_t* n);
  * as built stays, delivering only spikes of earlier steps, until its last one has arrived;
  * the rebuilt one delivers the later spikes.  A population's spike-history ring grows when
  * the new delays need it (snapshots taken before become unusable).  Not for connectivity
- * generated on the GPU, STDP synapses or the one-CTA small form (B2B_ERR_UNSUPPORTED). */
+ * generated on the GPU, STDP synapses or a net made to run the small-network path with
+ * B2B_NET_SMALL (B2B_ERR_UNSUPPORTED); a net on that path by the autotuner's choice goes
+ * back to the per-step kernels. */
 b2b_status b2b_syn_set_delays(b2b_net* net, int32_t sid, const int32_t* delay_steps,
                               int64_t n);
 /* Reads a synapse variable in the order the synapses were given (after b2b_finalize). */
@@ -364,7 +366,8 @@ b2b_status b2b_kernel_launches(b2b_net* net, int64_t* n);
 /* How b2b_run advances the net (after b2b_finalize): *mode = 1 for every step as two
  * concurrent launches (B2B_NET_TWO_LAUNCH, or chosen automatically), 3 for both halves of
  * every step as one launch (B2B_NET_ONE_LAUNCH or the autotuner), 2 for a small network run by
- * one CTA per chunk of steps, 0 for per-step kernels replayed from CUDA graphs. */
+ * one CTA or one thread-block cluster per chunk of steps, 0 for per-step kernels replayed from
+ * CUDA graphs. */
 b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
 /* Profiling run (the role of run(..., profile=True): per-code-object device timing,
  * brian2cuda/templates/common_group.cu:170-174, 328-337, objects.cu:603-629).  Advances the
@@ -379,7 +382,7 @@ b2b_status b2b_run_mode(b2b_net* net, int32_t* mode);
  * concurrent launches (b2b_run_mode 1), the delivery into the pending input (kind 5) and the
  * neuron update folding it in (kind 1), launched one after the other; or, in the one-launch
  * form (b2b_run_mode 3), the one kernel of the step (kind 13); or, for a small network
- * run by one CTA (b2b_run_mode 2), that kernel advancing one step (kind 7).  *n_sites receives the number
+ * run by one CTA or cluster (b2b_run_mode 2), that kernel advancing one step (kind 7).  *n_sites receives the number
  * of sites (<= cap filled). */
 b2b_status b2b_profile(b2b_net* net, int64_t n_steps, double* mean_ms, int32_t* site_kind,
                        int32_t cap, int32_t* n_sites);
