@@ -874,6 +874,7 @@ def bench_small(args, world, rank, local):
         runs = args.warmup + args.steps
         events = float(outdeg[idx].sum()) / runs * args.steps
         nspk = len(idx) / runs
+        net_mode = net.run_mode
         net.restore(0)
         prof, _ = net.profile_graph(2000)
         sec = ms / 1e3
@@ -882,8 +883,15 @@ def bench_small(args, world, rank, local):
         db = BYTES["cuba_event"] * events / (args.steps * steps_run)
         dom = max(prof, key=lambda kv: kv[1])
         step_ms = ms / (args.steps * steps_run)
-        roof = (_roofline(nb, dom[1], "lif_step_kernel", step_ms) if dom[0] == 1 else
-                _roofline(db, dom[1], "deliver_add_batch_kernel", step_ms))
+        if net_mode == "small":
+            # one launch runs a chunk of steps (update and delivery): its time per step is
+            # the step's
+            roof = _roofline(nb + db, step_ms, "small_pull_kernel / small_cluster_kernel "
+                             "(small-network path: update and delivery)", step_ms)
+        elif dom[0] == 1:
+            roof = _roofline(nb, dom[1], "lif_step_kernel", step_ms)
+        else:
+            roof = _roofline(db, dom[1], "deliver_add_batch_kernel", step_ms)
         line = _line_base(args, world, "synaptic events/s", value, "events/s",
                           ms / args.steps, WORKLOADS[wl],
                           {"sim_steps_per_step": steps_run, "neurons": 4000,
@@ -891,6 +899,7 @@ def bench_small(args, world, rank, local):
                            "l2": "working set < L2 (the net is 2.6 MB): no flush"},
                           "f64")
         line.update({"neuron_updates_per_s": 4000.0 * steps_run * args.steps * world / sec,
+                     "run_mode": net_mode,
                      "firing_rate_hz": nspk / (4000 * steps_run * DT), "roofline": roof,
                      "kernel_ms_mean_per_launch": {f"site {k}": v for k, v in prof},
                      "autotune": tune, "gpu_launches": launches, "clocks": clk})
