@@ -79,7 +79,7 @@ model_step_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 #pragma unroll
       for (int v = 0; v < M::NV; ++v) x[v] = X[v].x[e];
       bool nr = true;
-      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+      if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
       R dn[ND], du[ND];
 #pragma unroll
       for (int d = 0; d < M::NN; ++d) dn[d] = D[d].x[e];

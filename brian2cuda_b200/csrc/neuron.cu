@@ -80,7 +80,7 @@ __device__ __forceinline__ void lif_step_body(const PopDev& P, const int64_t* __
     for (int e = 0; e < E; ++e) {
       R ge = GE.x[e], gi = GI.x[e];
       bool nr = true;
-      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+      if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
       R vn = lif_advance<R>(g, V.x[e], ge, gi, nr,
                             INPUTS ? timed_input<R>(gin->ta, ts, E * q + e - g.offset) : R(0));
       GE.x[e] = ge;
@@ -156,7 +156,7 @@ __device__ __forceinline__ void hh_step_body(const PopDev& P, const int64_t* __r
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       bool nr = true;
-      if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+      if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
       const int64_t local = E * q + e - g.offset;
       R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], N.x[e], GE.x[e], GI.x[e], dtR,
                            INPUTS ? timed_input<R>(gin->ta, ts, local) : R(0));
@@ -318,7 +318,7 @@ hh_stream_kernel(PopDev P, const int64_t* __restrict__ clock, int k, double dt,
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         bool nr = true;
-        if (refr) nr = timestep_of(t - (double)cur.LS.x[e], dt, inv_dt) >= g.ref_steps;
+        if (refr) nr = past_refractory(t - (double)cur.LS.x[e], dt, inv_dt, g.ref_steps);
         const int64_t local = 4 * q + e - g.offset;
         R vn = hh_advance<R>(g, cur.V.x[e], cur.M.x[e], cur.H.x[e], cur.N.x[e],
                              cur.GE.x[e], cur.GI.x[e], dtR,

@@ -6,12 +6,18 @@
 
 namespace b2b {
 
-// Brian2's `timestep(t, dt)` = (int64)((t + 1e-3 dt) / dt) (brian2cuda/cuda_generator.py:
-// 997-1006), with the division replaced by a product with inv_dt = 1/dt: the quotient is an
-// integer plus 1e-3 (plus the rounding of a float32 lastspike, below 1e-3 of a step for
-// t < 100 s), so the one-ulp difference between the two forms never changes the truncation.
-__device__ __forceinline__ int64_t timestep_of(double t, double dt, double inv_dt) {
-  return (int64_t)((t + 1e-3 * dt) * inv_dt);
+// Brian2's not_refractory test, timestep(t - lastspike) >= timestep(refractory) = k, with
+// timestep(t, dt) = (int64)((t + 1e-3 dt) / dt) (brian2cuda/cuda_generator.py:997-1006).  The
+// division is a product with inv_dt = 1/dt: the quotient is an integer plus 1e-3 (plus the
+// rounding of a float32 lastspike, below 1e-3 of a step for t < 100 s), so the one-ulp
+// difference between the two forms never changes the truncation.  The elapsed time
+// e = t - lastspike is never negative (lastspike starts at -1e4 s and is set to t on a
+// spike), so the quotient is positive, its truncation is its floor, and floor(y) >= k exactly
+// when y >= k for an integer k: the comparison is made on the quotient, without converting a
+// double to a 64-bit integer.
+__device__ __forceinline__ bool past_refractory(double e, double dt, double inv_dt,
+                                                int64_t k) {
+  return (e + 1e-3 * dt) * inv_dt >= (double)k;
 }
 
 // Exact propagator of dv/dt = (El + u - v + ke ge + ki gi)/taum, dge/dt = -ge/taue,

@@ -172,7 +172,7 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
         if constexpr (KIND == KIND_LIF) {
           const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
           const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
           R vn = lif_advance<R>(
               g, v, ge, gi, nr,
               P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
@@ -190,7 +190,7 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
         } else {
           const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
           const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
           R m = sM[i], h = sH[i], nn = sN[i];
           const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
                                      P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
@@ -409,7 +409,7 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
         if constexpr (KIND == KIND_LIF) {
           const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
           const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
           R vn = lif_advance<R>(
               g, v, ge, gi, nr,
               P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
@@ -427,7 +427,7 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
         } else {
           const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
           const bool refr = g.ref_steps >= 0;
-          if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
           R m = sM[jl], h = sH[jl], nn = sN[jl];
           const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
                                      P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
@@ -639,7 +639,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
         for (int e = 0; e < 4; ++e) {
           const int64_t i = lo + j4 + e;
           bool nr = true;
-          if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
           R vn = lif_advance<R>(
               g, V.x[e], GE.x[e], GI.x[e], nr,
               P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
@@ -665,7 +665,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
         for (int e = 0; e < 4; ++e) {
           const int64_t i = lo + j4 + e;
           bool nr = true;
-          if (refr) nr = timestep_of(t - (double)LS.x[e], dt, inv_dt) >= g.ref_steps;
+          if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
           const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], NN.x[e], GE.x[e], GI.x[e],
                                      (R)dt,
                                      P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,

@@ -383,7 +383,7 @@ hh_surrogate_step_kernel(PopDev P, SurrDev D, const int64_t* __restrict__ clock,
       n_fb += __popc(fb);
     }
     bool nr = true;
-    if (refr) nr = timestep_of(t - (double)ls, dt, inv_dt) >= g.ref_steps;
+    if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
     const float vn = hh_membrane<float>(g, v, m, h, n, ge, gi, dtR);
     unsigned fl = 0;
     if (valid && vn > (float)g.Vthr && nr) {
