@@ -781,36 +781,19 @@ b2b_status setup_small(b2b_net* net) {
   if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) D.ring_in_smem = 0;
   D.cluster = 1;                 // one CTA until tuned (b2b_autotune, site kind 14)
   D.slice = pop.n;
-  // the pull form's bit rows: every synapse without a delay of its own (delay 0) and without
-  // a weight of its own, at most one synapse per (pre, post) pair
-  bool pull = pop.n <= 8192;
-  for (const Proj& pr : net->projs)
-    pull = pull && pr.dmin == 0 && pr.dmax == 0 && pr.dev.w == nullptr;
-  if (pull && !net->projs.empty()) {
-    const int64_t n = pop.n, row = n / 32;
-    std::vector<uint32_t> bits((size_t)net->projs.size() * n * row, 0u);
-    for (size_t p = 0; p < net->projs.size() && pull; ++p) {
-      const Proj& pr = net->projs[p];
-      std::vector<int64_t> off(n + 1);
-      std::vector<int32_t> post(std::max<int64_t>(pr.n_syn, 1));
-      CU(cudaMemcpy(off.data(), pr.off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+  // the pull form: one projection whose synapses have no delay (0 steps) and no weight of
+  // their own; its connectivity is kept on the host to be split by slice for a cluster size
+  if (net->projs.size() == 1 && pop.n <= 8192) {
+    const Proj& pr = net->projs[0];
+    if (pr.dmin == 0 && pr.dmax == 0 && pr.dev.w == nullptr && pr.n_syn < (1ll << 26)) {
+      net->pull_host_off.assign(pop.n + 1, 0);
+      net->pull_host_post.assign(std::max<int64_t>(pr.n_syn, 1), 0);
+      CU(cudaMemcpy(net->pull_host_off.data(), pr.off, sizeof(int64_t) * (pop.n + 1),
+                    cudaMemcpyDeviceToHost));
       if (pr.n_syn)
-        CU(cudaMemcpy(post.data(), pr.post, sizeof(int32_t) * pr.n_syn, cudaMemcpyDeviceToHost));
-      uint32_t* B = bits.data() + p * n * row;
-      for (int64_t pre = 0; pre < n && pull; ++pre)
-        for (int64_t s = off[pre]; s < off[pre + 1]; ++s) {
-          uint32_t& w = B[pre * row + post[s] / 32];
-          const uint32_t b = 1u << (post[s] % 32);
-          if (w & b) { pull = false; break; }     // a second synapse of the pair
-          w |= b;
-        }
-    }
-    if (pull) {
-      uint32_t* d = nullptr;
-      CU(cudaMalloc(&d, sizeof(uint32_t) * bits.size()));
-      net->pending_allocs.push_back(d);
-      CU(cudaMemcpy(d, bits.data(), sizeof(uint32_t) * bits.size(), cudaMemcpyHostToDevice));
-      D.pull_bits = d;
+        CU(cudaMemcpy(net->pull_host_post.data(), pr.post, sizeof(int32_t) * pr.n_syn,
+                      cudaMemcpyDeviceToHost));
+      net->pull_ok = true;
     }
   }
   net->small_ok = true;
@@ -1335,6 +1318,7 @@ b2b_status b2b_destroy(b2b_net* net) {
   for (Snapshot& sn : net->snapshots)
     for (void* a : sn.buffers) cudaFree(a);
   for (void* a : net->pending_allocs) cudaFree(a);
+  if (net->pull_buf) cudaFree(net->pull_buf);
   if (net->stream2) cudaStreamDestroy(net->stream2);
   for (cudaEvent_t ev : {net->ev_n, net->ev_d[0], net->ev_d[1]})
     if (ev) cudaEventDestroy(ev);
@@ -2014,6 +1998,65 @@ constexpr double kTuneMargin = 0.98;
 
 // Launch shape of the delivery launch of a net run with two launches per step (pending.cu):
 // lanes per work item (0: 8) and CTAs (0: two per SM).
+// The pull form's connectivity split by the slices of sdev (cluster and slice set): for each
+// rank, offsets by presynaptic neuron and slice-local targets, uploaded to the device; false
+// when a slice's targets do not fit a CTA's shared memory.
+bool build_pull_slices(b2b_net* net) {
+  SmallDev& D = net->sdev;
+  const int64_t n = net->pops[0].n, S = D.slice;
+  const int C = D.cluster;
+  const std::vector<int64_t>& off = net->pull_host_off;
+  const std::vector<int32_t>& post = net->pull_host_post;
+  std::vector<int64_t> cnt((size_t)C * (n + 1), 0);      // per rank, per pre
+  for (int64_t pre = 0; pre < n; ++pre)
+    for (int64_t s = off[pre]; s < off[pre + 1]; ++s)
+      ++cnt[(size_t)(post[s] / S) * (n + 1) + pre];
+  std::vector<int32_t> hoff((size_t)C * (n + 1));
+  int64_t base[17] = {0};
+  int64_t most = 0;
+  for (int r = 0; r < C; ++r) {
+    int64_t acc = 0;
+    for (int64_t pre = 0; pre < n; ++pre) {
+      hoff[(size_t)r * (n + 1) + pre] = (int32_t)acc;
+      acc += cnt[(size_t)r * (n + 1) + pre];
+    }
+    hoff[(size_t)r * (n + 1) + n] = (int32_t)acc;
+    base[r + 1] = base[r] + acc;
+    most = std::max(most, acc);
+  }
+  std::vector<uint16_t> htgt((size_t)std::max<int64_t>(base[C], 1));
+  std::vector<int64_t> fill((size_t)C * (n + 1), 0);
+  for (int64_t pre = 0; pre < n; ++pre)
+    for (int64_t s = off[pre]; s < off[pre + 1]; ++s) {
+      const int r = (int)(post[s] / S);
+      const size_t at = (size_t)(base[r] + hoff[(size_t)r * (n + 1) + pre] +
+                                 fill[(size_t)r * (n + 1) + pre]++);
+      htgt[at] = (uint16_t)(post[s] - (int64_t)r * S);
+    }
+  D.pull_max_tgt = (int32_t)most;
+  const size_t need = small_cluster_smem(D, net->pops[0].kind, net->pops[0].dtype);
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net->cfg.device);
+  if (optin > 0 && need > (size_t)optin - 4096) return false;
+  const size_t ob = sizeof(int32_t) * hoff.size(), tb = sizeof(uint16_t) * htgt.size();
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, ob + tb) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaMemcpy(buf, hoff.data(), ob, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy((uint8_t*)buf + ob, htgt.data(), tb, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(buf);
+    return false;
+  }
+  if (net->pull_buf) cudaFree(net->pull_buf);
+  net->pull_buf = buf;
+  D.pull_off = static_cast<const int32_t*>(buf);
+  D.pull_tgt = reinterpret_cast<const uint16_t*>((uint8_t*)buf + ob);
+  for (int r = 0; r <= C; ++r) D.pull_tgt_base[r] = base[r];
+  return true;
+}
+
 // The small-network path as one CTA (c == 1) or one cluster of c CTAs, each holding a slice
 // of the population, pushing the effects or (pull) gathering them at the targets; false
 // (nothing changed) when that form cannot run the net.
@@ -2027,10 +2070,16 @@ bool set_small_cluster(b2b_net* net, int c, bool pull) {
     D.pull = 0;
     D.slice = pop.n;
   } else {
-    if ((c != 8 && c != 16) || (pull && !D.pull_bits)) return false;
+    if ((c != 8 && c != 16) || (pull && !net->pull_ok)) return false;
     D.cluster = c;
     D.pull = pull ? 1 : 0;
     D.slice = ((pop.n + c - 1) / c + 3) / 4 * 4;
+    if (pull && !build_pull_slices(net)) {
+      D.cluster = c0;
+      D.pull = p0;
+      D.slice = s0;
+      return false;
+    }
     if (!small_cluster_possible(D, pop.kind, pop.dtype)) {
       D.cluster = c0;
       D.pull = p0;

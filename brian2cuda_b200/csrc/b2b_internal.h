@@ -211,11 +211,16 @@ struct SmallDev {
   int32_t warp_prefix;                  // every projection has <= 64 delays
   int32_t ring_in_smem;                 // the spike-history ring is mirrored in shared memory
   int32_t cluster;                      // CTAs of the one thread-block cluster (1: one CTA)
-  int32_t pull;                         // cluster form with the delivery pulled by targets
+  int32_t pull;                         // cluster form with the effects gathered per slice
   int64_t slice;                        // neurons per CTA of the cluster (multiple of 4)
-  // pull form: per projection, bit rows [pre][n / 32 words] (bit of post set when pre
-  // connects to it), or NULL when a synapse has a delay or a weight of its own
-  const uint32_t* pull_bits;
+  // pull form (one projection, no delays or weights of their own): for rank r of the
+  // cluster, the synapses into its slice grouped by presynaptic neuron, n + 1 offsets at
+  // pull_off + r (n + 1) and slice-local targets at pull_tgt + pull_tgt_base[r]
+  const int32_t* pull_off;
+  const uint16_t* pull_tgt;
+  int64_t pull_tgt_base[17];
+  int32_t pull_max_tgt;                 // most synapses into one slice
+  int32_t pull_pad;
 };
 
 struct Group {
@@ -367,6 +372,12 @@ struct b2b_net {
   std::vector<void*> mon_allocs;
   bool small = false;                      // the small-network path runs every step (small.cu)
   bool small_ok = false;                   // the net allows that path (sdev is built)
+  // the pull form's connectivity on the host (offsets by presynaptic neuron, targets), and
+  // its per-slice device copy for the current cluster size
+  bool pull_ok = false;
+  std::vector<int64_t> pull_host_off;
+  std::vector<int32_t> pull_host_post;
+  void* pull_buf = nullptr;
   b2b::SmallDev sdev{};
   bool two_launch = false;                 // the step as two concurrent launches (pending.cu)
   bool two_launch_ok = false;              // the net allows them (their buffers exist)
@@ -432,6 +443,8 @@ const void* mlp_image(const b2b_mlp* m);
 int mlp_device(const b2b_mlp* m);
 // Small networks (small.cu): `steps` steps of the net in one one-CTA launch.
 size_t small_smem(const SmallDev& D, int kind, int dtype);
+// Shared memory of one CTA of the small path's cluster forms.
+size_t small_cluster_smem(const SmallDev& D, int kind, int dtype);
 // Whether the cluster form of the small-network path (D.cluster CTAs of D.slice neurons) can
 // be launched on the current device.
 bool small_cluster_possible(const SmallDev& D, int kind, int dtype);

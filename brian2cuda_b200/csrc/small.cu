@@ -527,24 +527,23 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
   if (tid == 0 && rank == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
 }
 
-// ---- the cluster form with the delivery pulled by the targets --------------------------
-// For a net whose every synapse has a delay of 0 steps and one weight per Synapses object
-// (the CUBA example), the effects of a step can be gathered by the target neurons instead
-// of scattered by the spikes: CTA r keeps, beside its slice of the state, the connectivity
-// of the population as bit rows (bit i of row `pre` set when pre connects to neuron i; 2 MB
-// for 4096 neurons, resident in L2), and each target thread reads the words of its neurons.
-// A step is then one cluster barrier:
+// ---- the cluster form with the effects gathered per slice -----------------------------
+// For a net whose synapses have no delays and no weights of their own (the CUBA example), a
+// step needs one cluster barrier: CTA r keeps, beside its slice of the state, the synapses
+// into its slice grouped by presynaptic neuron (offsets and slice-local targets, loaded into
+// shared memory at launch):
 //   update and threshold of the slice; compaction of its spikes into a local list (double
 //   buffered by step parity);
 //   barrier;
 //   every CTA copies all CTAs' lists (distributed shared memory) into one list of the step's
 //   spikes, in rank order, and writes its own spikes at their offset into the global ring and
 //   monitor (the per-step kernels' record of the step);
-//   each target neuron adds, for every spike whose bit row has its bit, that Synapses
-//   object's weight to its target variable (the synapses slot), then the deferred reset.
-// Inside the step loop global memory is written (ring, monitor) and read for the bit words
-// of the step's spikes, the group parameters and the projections' member tables.  A final
-// barrier keeps every CTA's lists alive until all CTAs have read them.
+//   each spike's synapses into the slice add that Synapses object's weight to their target
+//   variable in shared memory (a warp per spike; the synapses slot), then the deferred reset.
+// No global memory is read inside the step loop.  The group parameters, group ids and member
+// tables are copied to shared memory first as well: the cluster barrier's acquire empties
+// the L1 cache every step.  A final barrier keeps every CTA's lists alive until all CTAs
+// have read them.
 template <typename R, int KIND>
 __global__ void __launch_bounds__(kSmallThreads, 1)
 small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__ clock,
@@ -571,6 +570,8 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
   int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
   int32_t* s_vg = all + n;                      // group of each 4 neurons of the slice
+  int32_t* s_off = s_vg + (S + 3) / 4;          // [n + 1] synapses into the slice by pre
+  uint16_t* s_tgt = reinterpret_cast<uint16_t*>(s_off + n + 1);   // their targets
   __shared__ int s_warp[33];
   __shared__ int s_cnt[2];
   __shared__ int s_pre[17];                     // counts of the ranks before each rank
@@ -592,6 +593,11 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     for (size_t b = tid; b < psz * (size_t)P.n_groups; b += blockDim.x) s_prm[b] = gp[b];
     for (int64_t q = tid; q < (mine + 3) / 4; q += blockDim.x)
       s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
+    const int32_t* goff = D.pull_off + (int64_t)rank * (n + 1);
+    for (int64_t x = tid; x <= n; x += blockDim.x) s_off[x] = goff[x];
+    const uint16_t* gtgt = D.pull_tgt + D.pull_tgt_base[rank];
+    const int64_t ntgt = D.pull_tgt_base[rank + 1] - D.pull_tgt_base[rank];
+    for (int64_t x = tid; x < ntgt; x += blockDim.x) s_tgt[x] = gtgt[x];
     for (int x = tid; x < D.n_proj * kPullMaxMembers; x += blockDim.x) {
       const int p = x / kPullMaxMembers, m = x - p * kPullMaxMembers;
       const ProjDev& J = D.proj[p];
@@ -612,7 +618,6 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const uint8_t* g = static_cast<const uint8_t*>(P.var[B2B_VAR_NOT_REFRACTORY]);
     for (int64_t q = tid; q < mine; q += blockDim.x) snr[q] = g[lo + q];
   }
-  const int64_t row_words = n / 32;
   if (tid == 0) s_mon = P.mon_cnt ? *P.mon_cnt : 0ull;
   __syncthreads();
 
@@ -742,38 +747,24 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     }
     __syncthreads();
     if (tid == 0) s_mon += (unsigned long long)tot;
-    // ---- synapses slot: each target neuron gathers the effects of the step's spikes
-    if (j4 < mine && tot > 0) {
-      const int64_t w = (lo + j4) / 32;         // the word holding this thread's 4 neurons
-      const int sh = (int)((lo + j4) & 31);
-      for (int p = 0; p < D.n_proj; ++p) {
-        const uint32_t* B = D.pull_bits + (int64_t)p * n * row_words;
-        // four spikes' words loaded before any is used, in spike order
-        for (int x0 = 0; x0 < tot; x0 += 4) {
-          int32_t pre[4];
-          unsigned b4[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            pre[u] = x0 + u < tot ? all[x0 + u] : -1;
-            b4[u] = pre[u] >= 0 ? (__ldg(B + (int64_t)pre[u] * row_words + w) >> sh) & 0xFu : 0u;
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (!b4[u]) continue;
-            int m = 0, mh = s_nmem[p] - 1;          // the member whose range holds pre
-            while (m < mh) {
-              const int mid = (m + mh) >> 1;
-              if (pre[u] < s_mhi[p][mid]) mh = mid; else m = mid + 1;
-            }
-            R* T = base + s_mvar[p][m] * S;         // v, ge, gi: columns 0-2
-            const R wgt = (R)s_mw[p][m];
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-              if (b4[u] & (1u << e)) T[j4 + e] += wgt;
-          }
+    // ---- synapses slot: a warp per spike, its synapses into this slice
+    {
+      const int lane = tid & 31;
+      const int nw = (int)(blockDim.x >> 5);
+      for (int x = tid >> 5; x < tot; x += nw) {
+        const int32_t pre = all[x];
+        int m = 0, mh = s_nmem[0] - 1;              // the member whose range holds pre
+        while (m < mh) {
+          const int mid = (m + mh) >> 1;
+          if (pre < s_mhi[0][mid]) mh = mid; else m = mid + 1;
         }
+        R* T = base + s_mvar[0][m] * S;             // v, ge, gi: columns 0-2
+        const R wgt = (R)s_mw[0][m];
+        for (int32_t s = s_off[pre] + lane; s < s_off[pre + 1]; s += 32)
+          atomicAdd(T + s_tgt[s], wgt);
       }
     }
+    __syncthreads();
     // ---- resets deferred after the synapses, for this CTA's spiking neurons
     if constexpr (KIND == KIND_LIF) {
       if (P.late_reset) {
@@ -818,7 +809,9 @@ size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const size_t rs = dtype == B2B_F32 ? 4 : 8;
   const size_t S = (size_t)D.slice;
   const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
-  if (D.pull) return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4);
+  if (D.pull)
+    return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4 + D.pop.n + 1) +
+           sizeof(uint16_t) * (size_t)D.pull_max_tgt;
   return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
 
@@ -864,7 +857,8 @@ cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
       D.slice / 4 > kSmallThreads ||
-      (D.pull && (!D.pull_bits || D.pop.n_groups > kPullMaxGroups || !pull_members_fit(D))))
+      (D.pull && (!D.pull_off || D.n_proj != 1 || D.pop.n_groups > kPullMaxGroups ||
+                  !pull_members_fit(D))))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)
