@@ -781,20 +781,25 @@ b2b_status setup_small(b2b_net* net) {
   if (small_smem(D, pop.kind, pop.dtype) > 200 * 1024) D.ring_in_smem = 0;
   D.cluster = 1;                 // one CTA until tuned (b2b_autotune, site kind 14)
   D.slice = pop.n;
-  // the pull form: one projection whose synapses have no delay (0 steps) and no weight of
-  // their own; its connectivity is kept on the host to be split by slice for a cluster size
-  if (net->projs.size() == 1 && pop.n <= 8192) {
-    const Proj& pr = net->projs[0];
-    if (pr.dmin == 0 && pr.dmax == 0 && pr.dev.w == nullptr && pr.n_syn < (1ll << 26)) {
-      net->pull_host_off.assign(pop.n + 1, 0);
-      net->pull_host_post.assign(std::max<int64_t>(pr.n_syn, 1), 0);
-      CU(cudaMemcpy(net->pull_host_off.data(), pr.off, sizeof(int64_t) * (pop.n + 1),
+  // the pull form: projections whose synapses have no delay (0 steps) and no weight of
+  // their own; their connectivity is kept on the host to be split by slice for a cluster size
+  bool pull = pop.n <= 8192;
+  for (const Proj& pr : net->projs)
+    pull = pull && pr.dmin == 0 && pr.dmax == 0 && pr.dev.w == nullptr && pr.n_syn < (1ll << 26);
+  if (pull) {
+    net->pull_host_off.assign(net->projs.size(), {});
+    net->pull_host_post.assign(net->projs.size(), {});
+    for (size_t p = 0; p < net->projs.size(); ++p) {
+      const Proj& pr = net->projs[p];
+      net->pull_host_off[p].assign(pop.n + 1, 0);
+      net->pull_host_post[p].assign(std::max<int64_t>(pr.n_syn, 1), 0);
+      CU(cudaMemcpy(net->pull_host_off[p].data(), pr.off, sizeof(int64_t) * (pop.n + 1),
                     cudaMemcpyDeviceToHost));
       if (pr.n_syn)
-        CU(cudaMemcpy(net->pull_host_post.data(), pr.post, sizeof(int32_t) * pr.n_syn,
+        CU(cudaMemcpy(net->pull_host_post[p].data(), pr.post, sizeof(int32_t) * pr.n_syn,
                       cudaMemcpyDeviceToHost));
-      net->pull_ok = true;
     }
+    net->pull_ok = true;
   }
   net->small_ok = true;
   net->small = (flags & B2B_NET_SMALL) != 0;
@@ -2005,55 +2010,71 @@ bool build_pull_slices(b2b_net* net) {
   SmallDev& D = net->sdev;
   const int64_t n = net->pops[0].n, S = D.slice;
   const int C = D.cluster;
-  const std::vector<int64_t>& off = net->pull_host_off;
-  const std::vector<int32_t>& post = net->pull_host_post;
-  std::vector<int64_t> cnt((size_t)C * (n + 1), 0);      // per rank, per pre
-  for (int64_t pre = 0; pre < n; ++pre)
-    for (int64_t s = off[pre]; s < off[pre + 1]; ++s)
-      ++cnt[(size_t)(post[s] / S) * (n + 1) + pre];
-  std::vector<int32_t> hoff((size_t)C * (n + 1));
-  int64_t base[17] = {0};
-  int64_t most = 0;
-  for (int r = 0; r < C; ++r) {
-    int64_t acc = 0;
-    for (int64_t pre = 0; pre < n; ++pre) {
-      hoff[(size_t)r * (n + 1) + pre] = (int32_t)acc;
-      acc += cnt[(size_t)r * (n + 1) + pre];
+  const int P = (int)net->projs.size();
+  std::vector<int32_t> hoff((size_t)P * C * (n + 1));
+  std::vector<int64_t> base((size_t)P * (C + 1), 0);
+  std::vector<int64_t> per_rank(C, 0);
+  for (int p = 0; p < P; ++p) {
+    const std::vector<int64_t>& off = net->pull_host_off[p];
+    const std::vector<int32_t>& post = net->pull_host_post[p];
+    std::vector<int64_t> cnt((size_t)C * (n + 1), 0);
+    for (int64_t pre = 0; pre < n; ++pre)
+      for (int64_t s = off[pre]; s < off[pre + 1]; ++s)
+        ++cnt[(size_t)(post[s] / S) * (n + 1) + pre];
+    for (int r = 0; r < C; ++r) {
+      int64_t acc = 0;
+      int32_t* o = hoff.data() + ((size_t)p * C + r) * (n + 1);
+      for (int64_t pre = 0; pre < n; ++pre) {
+        o[pre] = (int32_t)acc;
+        acc += cnt[(size_t)r * (n + 1) + pre];
+      }
+      o[n] = (int32_t)acc;
+      base[(size_t)p * (C + 1) + r + 1] = base[(size_t)p * (C + 1) + r] + acc;
+      per_rank[r] += acc;
     }
-    hoff[(size_t)r * (n + 1) + n] = (int32_t)acc;
-    base[r + 1] = base[r] + acc;
-    most = std::max(most, acc);
   }
-  std::vector<uint16_t> htgt((size_t)std::max<int64_t>(base[C], 1));
-  std::vector<int64_t> fill((size_t)C * (n + 1), 0);
-  for (int64_t pre = 0; pre < n; ++pre)
-    for (int64_t s = off[pre]; s < off[pre + 1]; ++s) {
-      const int r = (int)(post[s] / S);
-      const size_t at = (size_t)(base[r] + hoff[(size_t)r * (n + 1) + pre] +
-                                 fill[(size_t)r * (n + 1) + pre]++);
-      htgt[at] = (uint16_t)(post[s] - (int64_t)r * S);
-    }
-  D.pull_max_tgt = (int32_t)most;
+  // targets: projection-major, then rank, then presynaptic neuron
+  std::vector<int64_t> pstart(P + 1, 0);
+  for (int p = 0; p < P; ++p) pstart[p + 1] = pstart[p] + base[(size_t)p * (C + 1) + C];
+  std::vector<uint16_t> htgt((size_t)std::max<int64_t>(pstart[P], 1));
+  for (int p = 0; p < P; ++p) {
+    const std::vector<int64_t>& off = net->pull_host_off[p];
+    const std::vector<int32_t>& post = net->pull_host_post[p];
+    std::vector<int32_t> fill((size_t)C * (n + 1), 0);
+    for (int64_t pre = 0; pre < n; ++pre)
+      for (int64_t s = off[pre]; s < off[pre + 1]; ++s) {
+        const int r = (int)(post[s] / S);
+        const size_t at = (size_t)(pstart[p] + base[(size_t)p * (C + 1) + r] +
+                                   hoff[((size_t)p * C + r) * (n + 1) + pre] +
+                                   fill[(size_t)r * (n + 1) + pre]++);
+        htgt[at] = (uint16_t)(post[s] - (int64_t)r * S);
+      }
+    for (int r = 0; r <= C; ++r) base[(size_t)p * (C + 1) + r] += pstart[p];   // absolute
+  }
+  D.pull_max_tgt = (int32_t)*std::max_element(per_rank.begin(), per_rank.end());
   const size_t need = small_cluster_smem(D, net->pops[0].kind, net->pops[0].dtype);
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, net->cfg.device);
   if (optin > 0 && need > (size_t)optin - 4096) return false;
-  const size_t ob = sizeof(int32_t) * hoff.size(), tb = sizeof(uint16_t) * htgt.size();
+  const size_t bb = sizeof(int64_t) * base.size(), ob = sizeof(int32_t) * hoff.size();
+  const size_t tb = sizeof(uint16_t) * htgt.size();
   void* buf = nullptr;
-  if (cudaMalloc(&buf, ob + tb) != cudaSuccess) {
+  if (cudaMalloc(&buf, bb + ob + tb) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  if (cudaMemcpy(buf, hoff.data(), ob, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy((uint8_t*)buf + ob, htgt.data(), tb, cudaMemcpyHostToDevice) != cudaSuccess) {
+  uint8_t* b8 = static_cast<uint8_t*>(buf);
+  if (cudaMemcpy(b8, base.data(), bb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b8 + bb, hoff.data(), ob, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b8 + bb + ob, htgt.data(), tb, cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(buf);
     return false;
   }
   if (net->pull_buf) cudaFree(net->pull_buf);
   net->pull_buf = buf;
-  D.pull_off = static_cast<const int32_t*>(buf);
-  D.pull_tgt = reinterpret_cast<const uint16_t*>((uint8_t*)buf + ob);
-  for (int r = 0; r <= C; ++r) D.pull_tgt_base[r] = base[r];
+  D.pull_base = reinterpret_cast<const int64_t*>(b8);
+  D.pull_off = reinterpret_cast<const int32_t*>(b8 + bb);
+  D.pull_tgt = reinterpret_cast<const uint16_t*>(b8 + bb + ob);
   return true;
 }
 

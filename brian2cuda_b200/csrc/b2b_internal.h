@@ -213,13 +213,14 @@ struct SmallDev {
   int32_t cluster;                      // CTAs of the one thread-block cluster (1: one CTA)
   int32_t pull;                         // cluster form with the effects gathered per slice
   int64_t slice;                        // neurons per CTA of the cluster (multiple of 4)
-  // pull form (one projection, no delays or weights of their own): for rank r of the
-  // cluster, the synapses into its slice grouped by presynaptic neuron, n + 1 offsets at
-  // pull_off + r (n + 1) and slice-local targets at pull_tgt + pull_tgt_base[r]
+  // pull form (synapses without delays or weights of their own): for projection p and rank
+  // r of the cluster, the synapses into r's slice grouped by presynaptic neuron: n + 1
+  // offsets at pull_off + (p C + r)(n + 1) and slice-local targets at
+  // pull_tgt + pull_base[p (C + 1) + r]
   const int32_t* pull_off;
   const uint16_t* pull_tgt;
-  int64_t pull_tgt_base[17];
-  int32_t pull_max_tgt;                 // most synapses into one slice
+  const int64_t* pull_base;
+  int32_t pull_max_tgt;                 // most synapses (of all projections) into one slice
   int32_t pull_pad;
 };
 
@@ -375,8 +376,8 @@ struct b2b_net {
   // the pull form's connectivity on the host (offsets by presynaptic neuron, targets), and
   // its per-slice device copy for the current cluster size
   bool pull_ok = false;
-  std::vector<int64_t> pull_host_off;
-  std::vector<int32_t> pull_host_post;
+  std::vector<std::vector<int64_t>> pull_host_off;   // per projection
+  std::vector<std::vector<int32_t>> pull_host_post;
   void* pull_buf = nullptr;
   b2b::SmallDev sdev{};
   bool two_launch = false;                 // the step as two concurrent launches (pending.cu)

@@ -570,8 +570,9 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
   int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
   int32_t* s_vg = all + n;                      // group of each 4 neurons of the slice
-  int32_t* s_off = s_vg + (S + 3) / 4;          // [n + 1] synapses into the slice by pre
-  uint16_t* s_tgt = reinterpret_cast<uint16_t*>(s_off + n + 1);   // their targets
+  int32_t* s_off = s_vg + (S + 3) / 4;          // [n_proj][n + 1] synapses into the slice by pre
+  uint16_t* s_tgt = reinterpret_cast<uint16_t*>(s_off + (int64_t)D.n_proj * (n + 1));
+  __shared__ int32_t s_tstart[kMaxProjBatch + 1];   // each projection's targets in s_tgt
   __shared__ int s_warp[33];
   __shared__ int s_cnt[2];
   __shared__ int s_pre[17];                     // counts of the ranks before each rank
@@ -593,11 +594,22 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     for (size_t b = tid; b < psz * (size_t)P.n_groups; b += blockDim.x) s_prm[b] = gp[b];
     for (int64_t q = tid; q < (mine + 3) / 4; q += blockDim.x)
       s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
-    const int32_t* goff = D.pull_off + (int64_t)rank * (n + 1);
-    for (int64_t x = tid; x <= n; x += blockDim.x) s_off[x] = goff[x];
-    const uint16_t* gtgt = D.pull_tgt + D.pull_tgt_base[rank];
-    const int64_t ntgt = D.pull_tgt_base[rank + 1] - D.pull_tgt_base[rank];
-    for (int64_t x = tid; x < ntgt; x += blockDim.x) s_tgt[x] = gtgt[x];
+    if (tid == 0) {
+      int32_t acc = 0;
+      for (int p = 0; p < D.n_proj; ++p) {
+        s_tstart[p] = acc;
+        acc += (int32_t)(D.pull_base[p * (C + 1) + rank + 1] - D.pull_base[p * (C + 1) + rank]);
+      }
+      s_tstart[D.n_proj] = acc;
+    }
+    __syncthreads();
+    for (int p = 0; p < D.n_proj; ++p) {
+      const int32_t* goff = D.pull_off + ((int64_t)p * C + rank) * (n + 1);
+      for (int64_t x = tid; x <= n; x += blockDim.x) s_off[p * (n + 1) + x] = goff[x];
+      const uint16_t* gtgt = D.pull_tgt + D.pull_base[p * (C + 1) + rank];
+      for (int64_t x = tid; x < s_tstart[p + 1] - s_tstart[p]; x += blockDim.x)
+        s_tgt[s_tstart[p] + x] = gtgt[x];
+    }
     for (int x = tid; x < D.n_proj * kPullMaxMembers; x += blockDim.x) {
       const int p = x / kPullMaxMembers, m = x - p * kPullMaxMembers;
       const ProjDev& J = D.proj[p];
@@ -747,21 +759,25 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     }
     __syncthreads();
     if (tid == 0) s_mon += (unsigned long long)tot;
-    // ---- synapses slot: a warp per spike, its synapses into this slice
+    // ---- synapses slot: a warp per spike and projection, its synapses into this slice
     {
       const int lane = tid & 31;
       const int nw = (int)(blockDim.x >> 5);
-      for (int x = tid >> 5; x < tot; x += nw) {
-        const int32_t pre = all[x];
-        int m = 0, mh = s_nmem[0] - 1;              // the member whose range holds pre
-        while (m < mh) {
-          const int mid = (m + mh) >> 1;
-          if (pre < s_mhi[0][mid]) mh = mid; else m = mid + 1;
+      for (int p = 0; p < D.n_proj; ++p) {
+        const int32_t* o = s_off + p * (n + 1);
+        const uint16_t* tg = s_tgt + s_tstart[p];
+        for (int x = tid >> 5; x < tot; x += nw) {
+          const int32_t pre = all[x];
+          if (o[pre] == o[pre + 1]) continue;
+          int m = 0, mh = s_nmem[p] - 1;            // the member whose range holds pre
+          while (m < mh) {
+            const int mid = (m + mh) >> 1;
+            if (pre < s_mhi[p][mid]) mh = mid; else m = mid + 1;
+          }
+          R* T = base + s_mvar[p][m] * S;           // v, ge, gi: columns 0-2
+          const R wgt = (R)s_mw[p][m];
+          for (int32_t s = o[pre] + lane; s < o[pre + 1]; s += 32) atomicAdd(T + tg[s], wgt);
         }
-        R* T = base + s_mvar[0][m] * S;             // v, ge, gi: columns 0-2
-        const R wgt = (R)s_mw[0][m];
-        for (int32_t s = s_off[pre] + lane; s < s_off[pre + 1]; s += 32)
-          atomicAdd(T + s_tgt[s], wgt);
       }
     }
     __syncthreads();
@@ -810,7 +826,9 @@ size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
   const size_t S = (size_t)D.slice;
   const size_t state = (rs * L.nvars * S + S + 15) & ~(size_t)15;
   if (D.pull)
-    return state + sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4 + D.pop.n + 1) +
+    return state +
+           sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4 +
+                              (size_t)D.n_proj * (D.pop.n + 1)) +
            sizeof(uint16_t) * (size_t)D.pull_max_tgt;
   return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
 }
@@ -857,8 +875,7 @@ cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
       D.slice / 4 > kSmallThreads ||
-      (D.pull && (!D.pull_off || D.n_proj != 1 || D.pop.n_groups > kPullMaxGroups ||
-                  !pull_members_fit(D))))
+      (D.pull && (!D.pull_off || D.pop.n_groups > kPullMaxGroups || !pull_members_fit(D))))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)
