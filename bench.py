@@ -867,7 +867,9 @@ def bench_small(args, world, rank, local):
         P = ids["P"]
         outdeg = net.out_degree(P).astype(np.int64)
         net.run(500)
-        tune = net.autotune(trial_steps=50)
+        # trials of 500 steps: ten chunks each, so the comparison of the step's forms (the
+        # per-step kernels, the small-network path's one launch per chunk) is not one replay's
+        tune = net.autotune(trial_steps=500)
         start = net.spikes_recorded(P)
         ms, launches, clk = _timed_net_runs(net, stream, args, world, local, steps_run)
         idx, _, _ = net.spikes_fetch(P, start, cap=1 << 26)
