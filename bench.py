@@ -890,6 +890,8 @@ def bench_small(args, world, rank, local):
             # the step's
             roof = _roofline(nb + db, step_ms, "small_pull_kernel / small_cluster_kernel "
                              "(small-network path: update and delivery)", step_ms)
+            roof["timing"] = ("device time per simulation step over the timed region (CUDA "
+                              "events): one launch runs 50 steps")
         elif dom[0] == 1:
             roof = _roofline(nb, dom[1], "lif_step_kernel", step_ms)
         else:
