@@ -957,12 +957,26 @@ b2b_status enqueue_steps(b2b_net* net, int kk) {
       CU(prof_mark(net, k, si++, 1, s));
       ++net->launches;
     }
-    for (const Pop& pop : net->pops) {
-      CU(prof_mark(net, k, si, 0, s));
-      CU(launch_pop_step(pop, net->d_clock, k, net->cfg.dt, net->d_status, s));
-      CU(prof_mark(net, k, si++, 1, s));
+    // the populations' updates of a step are independent: the first on the net's stream,
+    // the others side by side on their own streams, joined before the deliveries
+    const size_t np = net->pops.size();
+    const bool fork = np > 1 && net->pop_streams.size() + 1 == np;
+    if (fork) {
+      CU(cudaEventRecord(net->ev_pop_fork, s));
+      for (cudaStream_t ps : net->pop_streams) CU(cudaStreamWaitEvent(ps, net->ev_pop_fork, 0));
+    }
+    for (size_t p = 0; p < np; ++p) {
+      cudaStream_t ps = fork && p > 0 ? net->pop_streams[p - 1] : s;
+      CU(prof_mark(net, k, si, 0, ps));
+      CU(launch_pop_step(net->pops[p], net->d_clock, k, net->cfg.dt, net->d_status, ps));
+      CU(prof_mark(net, k, si++, 1, ps));
       ++net->launches;
     }
+    if (fork)
+      for (size_t p = 1; p < np; ++p) {
+        CU(cudaEventRecord(net->ev_pop_join[p - 1], net->pop_streams[p - 1]));
+        CU(cudaStreamWaitEvent(s, net->ev_pop_join[p - 1], 0));
+      }
     for (size_t b = 0; b < net->add_batches.size(); ++b) {
       const auto& B = net->add_batches[b];
       CU(prof_mark(net, k, si, 0, s));
@@ -1325,6 +1339,13 @@ b2b_status b2b_destroy(b2b_net* net) {
   for (void* a : net->pending_allocs) cudaFree(a);
   if (net->pull_buf) cudaFree(net->pull_buf);
   if (net->stream2) cudaStreamDestroy(net->stream2);
+  for (cudaStream_t ps : net->pop_streams) {
+    cudaStreamSynchronize(ps);
+    cudaStreamDestroy(ps);
+  }
+  if (net->ev_pop_fork) cudaEventDestroy(net->ev_pop_fork);
+  for (cudaEvent_t ev : net->ev_pop_join)
+    if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : {net->ev_n, net->ev_d[0], net->ev_d[1]})
     if (ev) cudaEventDestroy(ev);
   for (void* a : net->mon_allocs) cudaFree(a);
@@ -1748,6 +1769,17 @@ b2b_status b2b_finalize(b2b_net* net) {
   if (st == B2B_OK) st = setup_two_launch(net);
   if (st == B2B_OK) st = setup_small(net);
   if (st != B2B_OK) return st;
+  if (net->pops.size() > 1) {
+    CU(cudaEventCreateWithFlags(&net->ev_pop_fork, cudaEventDisableTiming));
+    for (size_t p = 1; p < net->pops.size(); ++p) {
+      cudaStream_t ps = nullptr;
+      cudaEvent_t ev = nullptr;
+      CU(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+      net->pop_streams.push_back(ps);
+      CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      net->ev_pop_join.push_back(ev);
+    }
+  }
   CU(cudaMemcpy(net->d_clock, &net->ts, sizeof(int64_t), cudaMemcpyHostToDevice));
   CU(cudaDeviceSynchronize());
   net->finalized = true;

@@ -394,6 +394,11 @@ struct b2b_net {
   int one_launch_grid = 0;
   bool one_launch_chained = false;         // programmatic dependent launch between steps
   cudaStream_t stream2 = nullptr;
+  // per-step form with several populations: populations 1.. update on streams of their own,
+  // forked from and joined to the net's stream every step (the updates are independent)
+  std::vector<cudaStream_t> pop_streams;
+  cudaEvent_t ev_pop_fork = nullptr;
+  std::vector<cudaEvent_t> ev_pop_join;
   cudaEvent_t ev_n = nullptr, ev_d[2] = {nullptr, nullptr};
   std::vector<void*> pending_allocs;
   cudaGraphExec_t graph = nullptr;
