@@ -286,6 +286,105 @@ small_net_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict__
   if (tid == 0 && P.mon_cnt) *P.mon_cnt = s_mon;
 }
 
+// Shared-memory copies of what the cluster kernels' step loops read repeatedly (the cluster
+// barrier's acquire empties the L1 cache every step): the groups' parameters (at most
+// kPullMaxGroups) and the group id of every four neurons of the slice [lo, lo + mine).
+template <int KIND>
+__device__ __forceinline__ void load_slice_constants(const PopDev& P, int64_t lo, int64_t mine,
+                                                     unsigned char* s_prm, int32_t* s_vg) {
+  const size_t psz = KIND == KIND_LIF ? sizeof(LifDev) : sizeof(HhDev);
+  const unsigned char* gp = static_cast<const unsigned char*>(P.params);
+  for (size_t b = threadIdx.x; b < psz * (size_t)P.n_groups; b += blockDim.x) s_prm[b] = gp[b];
+  for (int64_t q = threadIdx.x; q < (mine + 3) / 4; q += blockDim.x)
+    s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
+}
+
+// Update and threshold of this thread's four neurons of the slice (local 4 tid .. 4 tid + 3,
+// population index lo + local) held in shared memory at base (variable c of the layout at
+// base + c S, flags at snr): each variable of the four read and written as one vector, the
+// four updates independent of each other.  Returns the spike bits (bit e: neuron 4 tid + e).
+template <typename R, int KIND>
+__device__ __forceinline__ unsigned slice_update(R* base, uint8_t* snr, int64_t S,
+                                                 const unsigned char* s_prm,
+                                                 const int32_t* s_vg, const PopDev& P,
+                                                 int64_t lo, int64_t ts, double t, double dt,
+                                                 double inv_dt) {
+  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const sV = base;
+  R* const sGE = base + S;
+  R* const sGI = base + 2 * S;
+  R* const sLS = base + kLS * S;
+  R* const sM = base + 3 * S;   // HH only
+  R* const sH = base + 4 * S;
+  R* const sN = base + 5 * S;
+  const int tid = threadIdx.x;
+  const int64_t j4 = 4 * (int64_t)tid;
+  unsigned fl = 0;
+  const int gidx = s_vg[j4 >> 2];
+  Pack<R, 4> V = load_pack<R, 4>(sV, tid), GE = load_pack<R, 4>(sGE, tid);
+  Pack<R, 4> GI = load_pack<R, 4>(sGI, tid), LS = load_pack<R, 4>(sLS, tid);
+  uint32_t NR = 0;
+  if constexpr (KIND == KIND_LIF) {
+    const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
+    const bool refr = g.ref_steps >= 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int64_t i = lo + j4 + e;
+      bool nr = true;
+      if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
+      R vn = lif_advance<R>(
+          g, V.x[e], GE.x[e], GI.x[e], nr,
+          P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
+      if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
+        nr = false;
+        if (refr) LS.x[e] = (R)t;
+        if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
+        fl |= 1u << e;
+      }
+      V.x[e] = vn;
+      NR |= (nr ? 1u : 0u) << (8 * e);
+    }
+    if (refr) {
+      store_pack<R, 4>(sLS, tid, LS);
+      store_flags<4>(snr, tid, NR);
+    }
+  } else {
+    const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
+    const bool refr = g.ref_steps >= 0;
+    Pack<R, 4> M = load_pack<R, 4>(sM, tid), H = load_pack<R, 4>(sH, tid);
+    Pack<R, 4> NN = load_pack<R, 4>(sN, tid);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int64_t i = lo + j4 + e;
+      bool nr = true;
+      if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
+      const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], NN.x[e], GE.x[e], GI.x[e],
+                                 (R)dt,
+                                 P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
+                                                           i - g.offset)
+                                          : R(0));
+      if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
+        nr = false;
+        if (refr) LS.x[e] = (R)t;
+        fl |= 1u << e;
+      }
+      V.x[e] = vn;
+      NR |= (nr ? 1u : 0u) << (8 * e);
+    }
+    store_pack<R, 4>(sM, tid, M);
+    store_pack<R, 4>(sH, tid, H);
+    store_pack<R, 4>(sN, tid, NN);
+    if (refr) {
+      store_pack<R, 4>(sLS, tid, LS);
+      store_flags<4>(snr, tid, NR);
+    }
+  }
+  store_pack<R, 4>(sV, tid, V);
+  store_pack<R, 4>(sGE, tid, GE);
+  store_pack<R, 4>(sGI, tid, GI);
+  return fl;
+}
+
 // ---- the same, spread over one thread-block cluster ------------------------------------
 // The one-CTA form is bound by one SM's issue rate once a step has a few thousand neurons;
 // here the CTAs of one cluster (up to 16 SMs) share the chunk: CTA r keeps neurons
@@ -347,22 +446,18 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
   const int64_t n = P.n;
   const int64_t lo = (int64_t)rank * S;
   const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;   // neurons of this CTA
-  R* const base = reinterpret_cast<R*>(smem);
-  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const base = reinterpret_cast<R*>(smem);   // the slice's variables, as in slice_update
   R* const sV = base;
-  R* const sGE = base + S;
-  R* const sGI = base + 2 * S;
-  R* const sLS = base + kLS * S;
-  R* const sM = base + 3 * S;   // HH only
-  R* const sH = base + 4 * S;
-  R* const sN = base + 5 * S;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
   int32_t* s_ring_cnt = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
+  int32_t* s_vg = s_ring_cnt + ((P.ring_len + 3) & ~3);   // group of each 4 neurons of the slice
   __shared__ int s_warp[33];
   __shared__ int s_cnt, s_off, s_tot;
   __shared__ unsigned long long s_mon;
+  __shared__ __align__(16) unsigned char s_prm[kPullMaxGroups * sizeof(HhDev)];
   const int tid = threadIdx.x;
   const int64_t ts0 = clock[0];
+  load_slice_constants<KIND>(P, lo, mine, s_prm, s_vg);
 
   for (int i = 0; i < L.nvars; ++i) {
     const R* g = static_cast<const R*>(P.var[L.var[i]]);
@@ -395,63 +490,10 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
     const double t = (double)ts * dt;
     const int slot = ring_slot(ts, P.ring_len);
     // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
-    unsigned fl = 0;
     const int64_t j4 = 4 * (int64_t)tid;
-    if (j4 < mine) {
-      const int gidx = P.vec_group ? P.vec_group[(lo + j4) >> 2] : 0;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int64_t jl = j4 + e;      // local index
-        const int64_t i = lo + jl;      // population index
-        R v = sV[jl], ge = sGE[jl], gi = sGI[jl];
-        R ls = sLS[jl];
-        bool nr = true;
-        if constexpr (KIND == KIND_LIF) {
-          const LifDev& g = static_cast<const LifDev*>(P.params)[gidx];
-          const bool refr = g.ref_steps >= 0;
-          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
-          R vn = lif_advance<R>(
-              g, v, ge, gi, nr,
-              P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
-          if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
-            nr = false;
-            if (refr) ls = (R)t;
-            if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
-            fl |= 1u << e;
-          }
-          v = vn;
-          if (refr) {
-            sLS[jl] = ls;
-            snr[jl] = nr ? 1 : 0;
-          }
-        } else {
-          const HhRun<R> g = hh_run(static_cast<const HhDev*>(P.params)[gidx], R());
-          const bool refr = g.ref_steps >= 0;
-          if (refr) nr = past_refractory(t - (double)ls, dt, inv_dt, g.ref_steps);
-          R m = sM[jl], h = sH[jl], nn = sN[jl];
-          const R vn = hh_advance<R>(g, v, m, h, nn, ge, gi, (R)dt,
-                                     P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
-                                                               i - g.offset)
-                                              : R(0));
-          if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
-            nr = false;
-            if (refr) ls = (R)t;
-            fl |= 1u << e;
-          }
-          v = vn;
-          sM[jl] = m;
-          sH[jl] = h;
-          sN[jl] = nn;
-          if (refr) {
-            sLS[jl] = ls;
-            snr[jl] = nr ? 1 : 0;
-          }
-        }
-        sV[jl] = v;
-        sGE[jl] = ge;
-        sGI[jl] = gi;
-      }
-    }
+    const unsigned fl = j4 < mine ? slice_update<R, KIND>(base, snr, S, s_prm, s_vg, P, lo, ts,
+                                                             t, dt, inv_dt)
+                                  : 0u;
     // ---- compaction: this CTA's count, then its offset among the cluster's CTAs
     int total;
     const int c = __popc(fl);
@@ -509,7 +551,7 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
         for (int r = tid; r < tot; r += blockDim.x) {
           const int32_t i = idx[r];
           if (i < lo || i >= lo + mine) continue;
-          const LifDev& g = static_cast<const LifDev*>(P.params)[P.vec_group ? P.vec_group[i >> 2] : 0];
+          const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[s_vg[(i - lo) >> 2]];
           if (g.has_reset) sV[i - lo] = (R)g.Vr;
         }
       }
@@ -557,15 +599,8 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   const int64_t n = P.n;
   const int64_t lo = (int64_t)rank * S;
   const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;
-  R* const base = reinterpret_cast<R*>(smem);
-  constexpr int kLS = KIND == KIND_LIF ? 3 : 6;
+  R* const base = reinterpret_cast<R*>(smem);   // the slice's variables, as in slice_update
   R* const sV = base;
-  R* const sGE = base + S;
-  R* const sGI = base + 2 * S;
-  R* const sLS = base + kLS * S;
-  R* const sM = base + 3 * S;   // HH only
-  R* const sH = base + 4 * S;
-  R* const sN = base + 5 * S;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
   int32_t* lists = reinterpret_cast<int32_t*>(smem + ((sizeof(R) * L.nvars * S + S + 15) & ~15));
   int32_t* all = lists + 2 * S;                 // lists: [2][S]; the step's spikes, [n]
@@ -589,11 +624,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   const int tid = threadIdx.x;
   const int64_t ts0 = clock[0];
   {
-    const size_t psz = KIND == KIND_LIF ? sizeof(LifDev) : sizeof(HhDev);
-    const unsigned char* gp = static_cast<const unsigned char*>(P.params);
-    for (size_t b = tid; b < psz * (size_t)P.n_groups; b += blockDim.x) s_prm[b] = gp[b];
-    for (int64_t q = tid; q < (mine + 3) / 4; q += blockDim.x)
-      s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
+    load_slice_constants<KIND>(P, lo, mine, s_prm, s_vg);
     if (tid == 0) {
       int32_t acc = 0;
       for (int p = 0; p < D.n_proj; ++p) {
@@ -640,74 +671,11 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const int slot = ring_slot(ts, P.ring_len);
     const int par = k & 1;
     int32_t* mylist = lists + par * S;
-    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3, each variable of the
-    // four read and written as one vector, the four updates independent of each other
-    unsigned fl = 0;
+    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
     const int64_t j4 = 4 * (int64_t)tid;
-    if (j4 < mine) {
-      const int gidx = s_vg[j4 >> 2];
-      Pack<R, 4> V = load_pack<R, 4>(sV, tid), GE = load_pack<R, 4>(sGE, tid);
-      Pack<R, 4> GI = load_pack<R, 4>(sGI, tid), LS = load_pack<R, 4>(sLS, tid);
-      uint32_t NR = 0;
-      if constexpr (KIND == KIND_LIF) {
-        const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
-        const bool refr = g.ref_steps >= 0;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int64_t i = lo + j4 + e;
-          bool nr = true;
-          if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
-          R vn = lif_advance<R>(
-              g, V.x[e], GE.x[e], GI.x[e], nr,
-              P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts, i - g.offset) : R(0));
-          if (g.has_threshold && (i - g.offset) < g.n && vn > (R)g.Vt && nr) {
-            nr = false;
-            if (refr) LS.x[e] = (R)t;
-            if (g.has_reset && !P.late_reset) vn = (R)g.Vr;
-            fl |= 1u << e;
-          }
-          V.x[e] = vn;
-          NR |= (nr ? 1u : 0u) << (8 * e);
-        }
-        if (refr) {
-          store_pack<R, 4>(sLS, tid, LS);
-          store_flags<4>(snr, tid, NR);
-        }
-      } else {
-        const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
-        const bool refr = g.ref_steps >= 0;
-        Pack<R, 4> M = load_pack<R, 4>(sM, tid), H = load_pack<R, 4>(sH, tid);
-        Pack<R, 4> NN = load_pack<R, 4>(sN, tid);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int64_t i = lo + j4 + e;
-          bool nr = true;
-          if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
-          const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], NN.x[e], GE.x[e], GI.x[e],
-                                     (R)dt,
-                                     P.inputs ? timed_input<R>(P.inputs[gidx].ta, ts,
-                                                               i - g.offset)
-                                              : R(0));
-          if ((i - g.offset) < g.n && vn > (R)g.Vthr && nr) {
-            nr = false;
-            if (refr) LS.x[e] = (R)t;
-            fl |= 1u << e;
-          }
-          V.x[e] = vn;
-          NR |= (nr ? 1u : 0u) << (8 * e);
-        }
-        store_pack<R, 4>(sM, tid, M);
-        store_pack<R, 4>(sH, tid, H);
-        store_pack<R, 4>(sN, tid, NN);
-        if (refr) {
-          store_pack<R, 4>(sLS, tid, LS);
-          store_flags<4>(snr, tid, NR);
-        }
-      }
-      store_pack<R, 4>(sV, tid, V);
-      store_pack<R, 4>(sGE, tid, GE);
-      store_pack<R, 4>(sGI, tid, GI);
-    }
+    const unsigned fl = j4 < mine ? slice_update<R, KIND>(base, snr, S, s_prm, s_vg, P, lo, ts,
+                                                             t, dt, inv_dt)
+                                  : 0u;
     // ---- this CTA's spikes into its local list (ascending neuron order)
     // (most CTAs of most steps have no spike: one barrier decides that for the CTA)
     int total = 0, excl = 0;
@@ -830,7 +798,7 @@ size_t small_cluster_smem(const SmallDev& D, int kind, int dtype) {
            sizeof(int32_t) * (2 * S + (size_t)D.pop.n + (S + 3) / 4 +
                               (size_t)D.n_proj * (D.pop.n + 1)) +
            sizeof(uint16_t) * (size_t)D.pull_max_tgt;
-  return state + sizeof(int32_t) * (size_t)((D.pop.ring_len + 3) & ~3);
+  return state + sizeof(int32_t) * ((size_t)((D.pop.ring_len + 3) & ~3) + (S + 3) / 4);
 }
 
 namespace {
@@ -874,8 +842,8 @@ cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps
 cudaError_t launch_cluster(const SmallDev& D, int kind, int dtype, const int64_t* clock,
                            int steps, double dt, int32_t* status, cudaStream_t s, bool probe) {
   if (D.cluster < 2 || D.cluster > 16 || D.slice < 4 || D.slice % 4 || !D.warp_prefix ||
-      D.slice / 4 > kSmallThreads ||
-      (D.pull && (!D.pull_off || D.pop.n_groups > kPullMaxGroups || !pull_members_fit(D))))
+      D.slice / 4 > kSmallThreads || D.pop.n_groups > kPullMaxGroups ||
+      (D.pull && (!D.pull_off || !pull_members_fit(D))))
     return cudaErrorInvalidValue;
   const size_t smem = small_cluster_smem(D, kind, dtype);
   if (kind == KIND_LIF && dtype == B2B_F32)
