@@ -611,9 +611,6 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   __shared__ int s_warp[33];
   __shared__ int s_cnt[2];
   __shared__ int s_pre[17];                     // counts of the ranks before each rank
-  constexpr int kHead = 4;
-  __shared__ int s_cq[16];                      // each rank's count of the step
-  __shared__ int s_head[16][kHead];             // each rank's first list entries
   __shared__ unsigned long long s_mon;
   // The cluster barrier's acquire empties the L1 cache every step, so whatever the step loop
   // reads repeatedly lives in shared memory: the groups' parameters, the slice's group ids and
@@ -692,17 +689,9 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     }
     if (tid == 0) s_cnt[par] = total;
     cl.sync();
-    // ---- every CTA's spikes of the step, in rank order: each rank's count and its first
-    // kHead list entries in one round of remote reads (most ranks have none or few spikes;
-    // entries past a count are read and ignored), the rest in a second round
-    if (tid < C * (kHead + 1)) {
-      const int q = tid / (kHead + 1), j = tid - q * (kHead + 1);
-      if (j == 0) s_cq[q] = *cl.map_shared_rank(&s_cnt[par], (unsigned)q);
-      else s_head[q][j - 1] = *cl.map_shared_rank(lists + par * S + (j - 1), (unsigned)q);
-    }
-    __syncthreads();
-    if (tid < 32) {   // warp 0: the counts' prefix
-      const int cq = tid < C ? s_cq[tid] : 0;
+    // ---- every CTA's spikes of the step, in rank order
+    if (tid < 32) {   // warp 0: one rank's count per lane, then their prefix
+      const int cq = tid < C ? *cl.map_shared_rank(&s_cnt[par], (unsigned)tid) : 0;
       const int incl = warp_incl_scan(cq);
       if (tid < C) s_pre[tid] = incl - cq;
       if (tid == 31) s_pre[C] = incl;
@@ -712,9 +701,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     for (int x = tid; x < tot; x += blockDim.x) {
       int q = 0;
       while (q + 1 < C && s_pre[q + 1] <= x) ++q;
-      const int kq = x - s_pre[q];
-      all[x] = kq < kHead ? s_head[q][kq]
-                          : *cl.map_shared_rank(lists + par * S + kq, (unsigned)q);
+      all[x] = *cl.map_shared_rank(lists + par * S + (x - s_pre[q]), (unsigned)q);
     }
     // the per-step kernels' record of the step: global ring slot and monitor
     {
