@@ -2419,19 +2419,43 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
       // the same halves as one grid per step: CTAs of the delivery after the update's
       double one_launch_ms = 1e30;
       int one_grid = net->pending_grid;
+      const int two_group = net->pdev.group;
+      int one_group = two_group;
       if (net->one_launch_ok && st == B2B_OK) {
         net->one_launch = true;
         const int grids[] = {net->pending_grid, sms / 2, sms, 2 * sms, 4 * sms};
-        for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
-          set_one_launch_grid(net, grids[c]);
+        auto tune_grid = [&](bool first) {
+          for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
+            if (!first && grids[c] == one_grid) continue;   // timed already
+            set_one_launch_grid(net, grids[c]);
+            double ms = 0;
+            st = trial(&ms);
+            if (st == B2B_OK && ((first && c == 0) || ms < kTuneMargin * one_launch_ms)) {
+              one_launch_ms = ms;
+              one_grid = grids[c];
+            }
+          }
+          set_one_launch_grid(net, one_grid);
+        };
+        tune_grid(true);
+        // lanes per work item inside this form: its delivering CTAs share the SMs with the
+        // update's, and a population burst's delivery is many short bundles, so the form
+        // ranks them differently from the two launches (COBAHH 1e5: 4 lanes 37.0-37.4
+        // against 16 lanes 39.7 ms per simulated second, on one box)
+        const int groups[] = {2, 4, 8, 16};
+        for (int g : groups) {
+          if (g == two_group || st != B2B_OK) continue;
+          net->pdev.group = g;
+          set_one_launch_grid(net, one_grid);
           double ms = 0;
           st = trial(&ms);
-          if (st == B2B_OK && (c == 0 || ms < kTuneMargin * one_launch_ms)) {
+          if (st == B2B_OK && ms < kTuneMargin * one_launch_ms) {
             one_launch_ms = ms;
-            one_grid = grids[c];
+            one_group = g;
           }
         }
-        set_one_launch_grid(net, one_grid);
+        net->pdev.group = one_group;
+        if (one_group != two_group) tune_grid(false);   // the CTAs again, for these lanes
       }
       // the same, each step's launch chained to the previous one (programmatic dependent launch)
       double chained_ms = 1e30;
@@ -2462,6 +2486,11 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         res.push_back(r1);   // after the per-step form's entry, so that tune_apply ends on it
       }
       set_pending_shape(net, r.choice_a, r.choice_b);
+      if (form >= 2 && one_group != two_group) {
+        // the one-launch form's lanes per item (the pending delivery's CTAs stay as tuned)
+        set_pending_shape(net, one_group, r.choice_b);
+        res.push_back(b2b_tune_result{5, 0, one_group, r.choice_b, form_ms[form], r.best_ms});
+      }
       res.push_back(b2b_tune_result{11, 0, form, form >= 2 ? one_grid : 0, form_ms[form],
                                     form_ms[builtin]});
     }
