@@ -2456,7 +2456,32 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         }
         net->pdev.group = one_group;
         if (one_group != two_group) tune_grid(false);   // the CTAs again, for these lanes
+        // the update's CTAs inside this form (one or two neurons per thread x 128 or 256
+        // threads): they share the grid with the delivery's, and fewer, larger CTAs shorten
+        // the launch
+        const std::pair<int, int> one_shapes[] = {{1, 128}, {1, 256}, {2, 128}, {2, 256}};
+        auto eff = [](int e, int b) {
+          return std::make_pair(e == 2 || e == 4 ? 2 : 1, b > 0 ? b : kBlock);
+        };
+        const auto cur = eff(pop0.tune_e, pop0.tune_block);
+        for (const auto& sh : one_shapes) {
+          if (sh == cur || st != B2B_OK) continue;
+          const int pe = pop0.tune_e, pb = pop0.tune_block;
+          pop0.tune_e = sh.first;
+          pop0.tune_block = sh.second;
+          set_one_launch_grid(net, one_grid);
+          double ms = 0;
+          st = trial(&ms);
+          if (st == B2B_OK && ms < kTuneMargin * one_launch_ms) {
+            one_launch_ms = ms;
+          } else {
+            pop0.tune_e = pe;
+            pop0.tune_block = pb;
+          }
+        }
+        set_one_launch_grid(net, one_grid);
       }
+      const int one_e = pop0.tune_e, one_block = pop0.tune_block;
       // the same, each step's launch chained to the previous one (programmatic dependent launch)
       double chained_ms = 1e30;
       if (net->one_launch_ok && st == B2B_OK) {
@@ -2482,8 +2507,16 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
         // the per-step form keeps the shape tuned for it
         pop0.tune_e = ps_e;
         pop0.tune_block = ps_block;
-      } else if (r1.choice_a != ps_e || r1.choice_b != ps_block) {
-        res.push_back(r1);   // after the per-step form's entry, so that tune_apply ends on it
+      } else {
+        if (r1.choice_a != ps_e || r1.choice_b != ps_block)
+          res.push_back(r1);   // after the per-step form's entry, so that tune_apply ends on it
+        pop0.tune_e = r1.choice_a;
+        pop0.tune_block = r1.choice_b;
+        if (form >= 2 && (one_e != r1.choice_a || one_block != r1.choice_b)) {
+          pop0.tune_e = one_e;
+          pop0.tune_block = one_block;
+          res.push_back(b2b_tune_result{1, 0, one_e, one_block, form_ms[form], r1.best_ms});
+        }
       }
       set_pending_shape(net, r.choice_a, r.choice_b);
       if (form >= 2 && one_group != two_group) {
