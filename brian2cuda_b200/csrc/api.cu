@@ -1338,6 +1338,7 @@ b2b_status b2b_destroy(b2b_net* net) {
     for (void* a : sn.buffers) cudaFree(a);
   for (void* a : net->pending_allocs) cudaFree(a);
   if (net->pull_buf) cudaFree(net->pull_buf);
+  if (net->fetch_pinned) cudaFreeHost(net->fetch_pinned);
   if (net->stream2) cudaStreamDestroy(net->stream2);
   for (cudaStream_t ps : net->pop_streams) {
     cudaStreamSynchronize(ps);
@@ -2856,16 +2857,32 @@ b2b_status spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* tot
   const int64_t hi = std::min<int64_t>(stored, start + cap);
   if (hi <= start) return B2B_OK;
   const int64_t m = hi - start;
-  CU(cudaMemcpyAsync(idx, D.mon_idx + start, 4 * m, cudaMemcpyDeviceToHost, net->stream));
-  CU(cudaMemcpyAsync(step, D.mon_step + start, 8 * m, cudaMemcpyDeviceToHost, net->stream));
+  // through pinned host memory kept by the net: a copy into pageable memory is staged by the
+  // driver at a fraction of the link's rate (3e5 spikes: 1.6 ms against ~0.3 ms)
+  const size_t need = 12 * (size_t)m;
+  if (need > net->fetch_pinned_bytes) {
+    if (net->fetch_pinned) cudaFreeHost(net->fetch_pinned);
+    net->fetch_pinned = nullptr;
+    net->fetch_pinned_bytes = 0;
+    const size_t bytes = std::max(need, (size_t)1 << 20);
+    CU(cudaMallocHost(&net->fetch_pinned, bytes));
+    net->fetch_pinned_bytes = bytes;
+  }
+  int64_t* sstep = static_cast<int64_t*>(net->fetch_pinned);
+  int32_t* sidx = reinterpret_cast<int32_t*>(sstep + m);
+  CU(cudaMemcpyAsync(sidx, D.mon_idx + start, 4 * m, cudaMemcpyDeviceToHost, net->stream));
+  CU(cudaMemcpyAsync(sstep, D.mon_step + start, 8 * m, cudaMemcpyDeviceToHost, net->stream));
   CU(cudaStreamSynchronize(net->stream));
   int64_t k = m;
-  if (!whole_population) {
+  if (whole_population) {
+    std::memcpy(idx, sidx, 4 * (size_t)m);
+    std::memcpy(step, sstep, 8 * (size_t)m);
+  } else {
     k = 0;
     for (int64_t r = 0; r < m; ++r) {
-      if (idx[r] < g.offset || idx[r] >= g.offset + g.n) continue;
-      idx[k] = (int32_t)(idx[r] - g.offset);
-      step[k] = step[r];
+      if (sidx[r] < g.offset || sidx[r] >= g.offset + g.n) continue;
+      idx[k] = (int32_t)(sidx[r] - g.offset);
+      step[k] = sstep[r];
       ++k;
     }
   }

@@ -379,6 +379,9 @@ struct b2b_net {
   std::vector<std::vector<int64_t>> pull_host_off;   // per projection
   std::vector<std::vector<int32_t>> pull_host_post;
   void* pull_buf = nullptr;
+  // pinned host staging of spike-monitor reads (b2b_spikemon_fetch)
+  void* fetch_pinned = nullptr;
+  size_t fetch_pinned_bytes = 0;
   b2b::SmallDev sdev{};
   bool two_launch = false;                 // the step as two concurrent launches (pending.cu)
   bool two_launch_ok = false;              // the net allows them (their buffers exist)

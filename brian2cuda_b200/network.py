@@ -538,10 +538,11 @@ class Network:
         """Recorded spikes from monitor entry `start` on, in recording order; returns
         (indices, steps, next_start)."""
         total, n = C.c_int64(), C.c_int64()
-        idx = np.empty(cap, dtype=np.int32)
-        stp = np.empty(cap, dtype=np.int64)
+        m = max(1, min(int(cap), self.spikes_recorded(gid) - int(start)))
+        idx = np.empty(m, dtype=np.int32)
+        stp = np.empty(m, dtype=np.int64)
         self._check(self._lib.b2b_spikemon_fetch(self._h, gid, int(start), C.byref(total),
-                                                 C.byref(n), _ptr(idx), _ptr(stp), cap),
+                                                 C.byref(n), _ptr(idx), _ptr(stp), m),
                     "spikemon_fetch")
         nxt = min(total.value, int(start) + cap)
         return idx[: n.value], stp[: n.value], nxt
@@ -550,10 +551,11 @@ class Network:
         """Like spikes_fetch, for every monitored group of gid's population at once, with
         population indices (see group_offset)."""
         total, n = C.c_int64(), C.c_int64()
-        idx = np.empty(cap, dtype=np.int32)
-        stp = np.empty(cap, dtype=np.int64)
+        m = max(1, min(int(cap), self.spikes_recorded(gid) - int(start)))
+        idx = np.empty(m, dtype=np.int32)
+        stp = np.empty(m, dtype=np.int64)
         self._check(self._lib.b2b_spikemon_fetch_population(
-            self._h, gid, int(start), C.byref(total), C.byref(n), _ptr(idx), _ptr(stp), cap),
+            self._h, gid, int(start), C.byref(total), C.byref(n), _ptr(idx), _ptr(stp), m),
             "spikemon_fetch_population")
         nxt = min(total.value, int(start) + cap)
         return idx[: n.value], stp[: n.value], nxt
