@@ -54,9 +54,61 @@ def peaks():
 
 
 class Clocks:
-    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons during the timed region: NVML from
+    a thread every 10 ms, live before the constructor returns (an nvidia-smi child takes
+    longer to start than a short timed region lasts); nvidia-smi where NVML is missing."""
 
-    def __init__(self, gpu: int):
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, gpu: int, period_s: float = 0.01):
+        import threading
+        self.samples = []
+        self.p = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = self._nvml_handle(pynvml, gpu)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+        except Exception:
+            self._start_smi(gpu)
+            return
+        self.stop_ev = threading.Event()
+        first = threading.Event()
+
+        def loop():
+            while True:
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(smax),
+                                         {nm for nm, b in bits.items() if r & b}))
+                except Exception:
+                    pass
+                first.set()
+                if self.stop_ev.wait(period_s):
+                    return
+
+        self.th = threading.Thread(target=loop, daemon=True)
+        self.th.start()
+        first.wait(2.0)
+
+    @staticmethod
+    def _nvml_handle(pynvml, gpu: int):
+        # the CUDA device's PCI address: NVML numbers every GPU of the machine, CUDA only the
+        # visible ones
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(gpu)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(gpu)
+
+    def _start_smi(self, gpu):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -66,33 +118,40 @@ class Clocks:
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
-            self.p = None
+            self.p = False
 
     def stop(self):
-        if self.p is None:
+        if self.p is False:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        self.p.terminate()
-        self.p.wait()
-        self.f.flush()
-        self.f.seek(0)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f.read().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[3:7]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        os.unlink(self.f.name)
+        if self.p is None:
+            self.stop_ev.set()
+            self.th.join()
+            samples = list(self.samples)
+            source = "nvml"
+        else:
+            self.p.terminate()
+            self.p.wait()
+            self.f.flush()
+            self.f.seek(0)
+            samples = []
+            for line in self.f.read().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm, smax = float(parts[0]), float(parts[1])
+                except ValueError:
+                    continue
+                samples.append((sm, smax, {nm for nm, val in zip(self.NAMES, parts[3:7])
+                                           if val.lower() == "active"}))
+            os.unlink(self.f.name)
+            source = "nvidia-smi"
+        sm = [a for a, _, _ in samples]
+        smax = [b for _, b, _ in samples]
+        reasons = set().union(*[r for _, _, r in samples]) if samples else set()
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": source}
 
 
 def dist_setup(n_gpus, backend: str = "nccl"):
