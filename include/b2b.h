@@ -457,7 +457,8 @@ b2b_status b2b_spikemon_get_range(b2b_net* net, int32_t gid, int64_t lo, int64_t
  * population has recorded; entries [start, min(total, start + cap)) are copied in recording
  * order, keeping those of group gid (group-local index), and *n receives how many were kept.
  * Lets a caller drain new spikes after every run chunk (the role of the per-run result
- * files, brian2cuda/templates/objects.cu:522-641). */
+ * files, brian2cuda/templates/objects.cu:522-641).  The copy goes through a page-locked host
+ * buffer kept by the net (grown to the largest read, freed by b2b_destroy). */
 b2b_status b2b_spikemon_fetch(b2b_net* net, int32_t gid, int64_t start, int64_t* total,
                               int64_t* n, int32_t* idx, int64_t* step, int64_t cap);
 /* b2b_spikemon_fetch without the group filter: entries of every monitored group of gid's
