@@ -871,7 +871,9 @@ b2b_status setup_two_launch(b2b_net* net) {
   net->two_launch = (flags & (B2B_NET_TWO_LAUNCH | B2B_NET_ONE_LAUNCH)) ||
                     pop.n <= kAutoTwoLaunchMaxNeurons;
   net->one_launch_ok = one_launch_supported(pop, F);
-  net->one_launch_grid = net->pending_grid;
+  // delivering CTAs of the one-launch step: 1.5 per SM (in CTAs of kBlock threads) still fit
+  // beside the update's in one wave for the populations this form is built for
+  net->one_launch_grid = 3 * sms / 2;
   net->one_launch = net->one_launch_ok && (flags & B2B_NET_ONE_LAUNCH);
   return B2B_OK;
 }
@@ -2419,12 +2421,18 @@ b2b_status b2b_autotune(b2b_net* net, int32_t trial_steps, b2b_tune_result* out,
       const double two_launch_ms = r1.best_ms;
       // the same halves as one grid per step: CTAs of the delivery after the update's
       double one_launch_ms = 1e30;
-      int one_grid = net->pending_grid;
+      int one_grid = 3 * sms / 2;
       const int two_group = net->pdev.group;
       int one_group = two_group;
       if (net->one_launch_ok && st == B2B_OK) {
         net->one_launch = true;
-        const int grids[] = {net->pending_grid, sms / 2, sms, 2 * sms, 4 * sms};
+        // the built-in 1.5 per SM first: between 1 and 2 per SM the delivering CTAs still fit
+        // beside the update's in one wave (COBAHH 1e5, update 2 x 128: 148, 185, 222, 259 gave
+        // 38.1, 37.4, 36.9, 37.8 ms per simulated second on one box, 148 against 222 38.1
+        // against 37.2 on another; 296 needs a second wave), and the 2000-step window does not
+        // tell 1 and 1.5 per SM apart by the 2 % margin
+        const int grids[] = {3 * sms / 2, net->pending_grid, sms / 2, sms, 5 * sms / 4,
+                             7 * sms / 4, 2 * sms, 4 * sms};
         auto tune_grid = [&](bool first) {
           for (size_t c = 0; c < sizeof(grids) / sizeof(grids[0]) && st == B2B_OK; ++c) {
             if (!first && grids[c] == one_grid) continue;   // timed already
