@@ -2151,7 +2151,9 @@ bool set_small_cluster(b2b_net* net, int c, bool pull) {
 }
 
 void set_one_launch_grid(b2b_net* net, int grid) {
-  net->one_launch_grid = grid > 0 ? grid : net->pending_grid;
+  int sms = kNumSMs;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->cfg.device);
+  net->one_launch_grid = grid > 0 ? grid : 3 * sms / 2;   // 0: the built-in 1.5 per SM
   if (net->graph) {
     cudaGraphExecDestroy(net->graph);
     net->graph = nullptr;

@@ -410,7 +410,8 @@ b2b_status b2b_profile_graph(b2b_net* net, int64_t n_steps, double* mean_ms, int
  * records; the live records and every snapshot are permuted together, and b2b_syn_get reads
  * through the order); a net that can run every step as two concurrent launches: the pending
  * delivery's lanes per item x CTAs (kind 5), then the form itself (kind 11: choice_a 2 one
- * launch per step holding both halves, with choice_b delivering CTAs after the update's, 3 the
+ * launch per step holding both halves, with choice_b delivering CTAs (of 256 threads; 0: the
+ * built-in 1.5 per SM) after the update's, 3 the
  * same with each step's launch chained to the previous one by programmatic dependent launch;
  * 1 two launches; 0 the per-step kernels).  Afterwards the state, clock and monitor counts are as before the call,
  * and the next b2b_run captures its graph with the chosen shapes.  A candidate must be 2 % faster than the best so far (starting from the built-in
