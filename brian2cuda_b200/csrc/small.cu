@@ -299,11 +299,13 @@ __device__ __forceinline__ void load_slice_constants(const PopDev& P, int64_t lo
     s_vg[q] = P.vec_group ? P.vec_group[(lo >> 2) + q] : 0;
 }
 
-// Update and threshold of this thread's four neurons of the slice (local 4 tid .. 4 tid + 3,
+// Update and threshold of this thread's E neurons of the slice (local E tid .. E tid + E - 1,
 // population index lo + local) held in shared memory at base (variable c of the layout at
-// base + c S, flags at snr): each variable of the four read and written as one vector, the
-// four updates independent of each other.  Returns the spike bits (bit e: neuron 4 tid + e).
-template <typename R, int KIND>
+// base + c S, flags at snr): with E = 4 each variable of the four read and written as one
+// vector, the four updates independent of each other; E = 1 where the CTA has a thread for
+// every neuron of its slice, so that a step's update is one neuron's chain long.  Returns the
+// spike bits (bit e: neuron E tid + e).
+template <typename R, int KIND, int E>
 __device__ __forceinline__ unsigned slice_update(R* base, uint8_t* snr, int64_t S,
                                                  const unsigned char* s_prm,
                                                  const int32_t* s_vg, const PopDev& P,
@@ -318,18 +320,18 @@ __device__ __forceinline__ unsigned slice_update(R* base, uint8_t* snr, int64_t 
   R* const sH = base + 4 * S;
   R* const sN = base + 5 * S;
   const int tid = threadIdx.x;
-  const int64_t j4 = 4 * (int64_t)tid;
+  const int64_t j0 = E * (int64_t)tid;
   unsigned fl = 0;
-  const int gidx = s_vg[j4 >> 2];
-  Pack<R, 4> V = load_pack<R, 4>(sV, tid), GE = load_pack<R, 4>(sGE, tid);
-  Pack<R, 4> GI = load_pack<R, 4>(sGI, tid), LS = load_pack<R, 4>(sLS, tid);
+  const int gidx = s_vg[j0 >> 2];
+  Pack<R, E> V = load_pack<R, E>(sV, tid), GE = load_pack<R, E>(sGE, tid);
+  Pack<R, E> GI = load_pack<R, E>(sGI, tid), LS = load_pack<R, E>(sLS, tid);
   uint32_t NR = 0;
   if constexpr (KIND == KIND_LIF) {
     const LifDev& g = reinterpret_cast<const LifDev*>(s_prm)[gidx];
     const bool refr = g.ref_steps >= 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int64_t i = lo + j4 + e;
+    for (int e = 0; e < E; ++e) {
+      const int64_t i = lo + j0 + e;
       bool nr = true;
       if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
       R vn = lif_advance<R>(
@@ -345,17 +347,17 @@ __device__ __forceinline__ unsigned slice_update(R* base, uint8_t* snr, int64_t 
       NR |= (nr ? 1u : 0u) << (8 * e);
     }
     if (refr) {
-      store_pack<R, 4>(sLS, tid, LS);
-      store_flags<4>(snr, tid, NR);
+      store_pack<R, E>(sLS, tid, LS);
+      store_flags<E>(snr, tid, NR);
     }
   } else {
     const HhRun<R> g = hh_run(reinterpret_cast<const HhDev*>(s_prm)[gidx], R());
     const bool refr = g.ref_steps >= 0;
-    Pack<R, 4> M = load_pack<R, 4>(sM, tid), H = load_pack<R, 4>(sH, tid);
-    Pack<R, 4> NN = load_pack<R, 4>(sN, tid);
+    Pack<R, E> M = load_pack<R, E>(sM, tid), H = load_pack<R, E>(sH, tid);
+    Pack<R, E> NN = load_pack<R, E>(sN, tid);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int64_t i = lo + j4 + e;
+    for (int e = 0; e < E; ++e) {
+      const int64_t i = lo + j0 + e;
       bool nr = true;
       if (refr) nr = past_refractory(t - (double)LS.x[e], dt, inv_dt, g.ref_steps);
       const R vn = hh_advance<R>(g, V.x[e], M.x[e], H.x[e], NN.x[e], GE.x[e], GI.x[e],
@@ -371,17 +373,17 @@ __device__ __forceinline__ unsigned slice_update(R* base, uint8_t* snr, int64_t 
       V.x[e] = vn;
       NR |= (nr ? 1u : 0u) << (8 * e);
     }
-    store_pack<R, 4>(sM, tid, M);
-    store_pack<R, 4>(sH, tid, H);
-    store_pack<R, 4>(sN, tid, NN);
+    store_pack<R, E>(sM, tid, M);
+    store_pack<R, E>(sH, tid, H);
+    store_pack<R, E>(sN, tid, NN);
     if (refr) {
-      store_pack<R, 4>(sLS, tid, LS);
-      store_flags<4>(snr, tid, NR);
+      store_pack<R, E>(sLS, tid, LS);
+      store_flags<E>(snr, tid, NR);
     }
   }
-  store_pack<R, 4>(sV, tid, V);
-  store_pack<R, 4>(sGE, tid, GE);
-  store_pack<R, 4>(sGI, tid, GI);
+  store_pack<R, E>(sV, tid, V);
+  store_pack<R, E>(sGE, tid, GE);
+  store_pack<R, E>(sGI, tid, GI);
   return fl;
 }
 
@@ -446,6 +448,7 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
   const int64_t n = P.n;
   const int64_t lo = (int64_t)rank * S;
   const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;   // neurons of this CTA
+  const bool one_each = mine <= (int64_t)blockDim.x;   // one neuron per thread
   R* const base = reinterpret_cast<R*>(smem);   // the slice's variables, as in slice_update
   R* const sV = base;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
@@ -489,11 +492,13 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
     const int64_t ts = ts0 + k;
     const double t = (double)ts * dt;
     const int slot = ring_slot(ts, P.ring_len);
-    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
-    const int64_t j4 = 4 * (int64_t)tid;
-    const unsigned fl = j4 < mine ? slice_update<R, KIND>(base, snr, S, s_prm, s_vg, P, lo, ts,
-                                                             t, dt, inv_dt)
-                                  : 0u;
+    // ---- groups and thresholds: local neurons E tid .. E tid + E - 1 (E = 1 when the CTA
+    // has a thread for every neuron of its slice, else 4)
+    const int64_t j0 = (one_each ? 1 : 4) * (int64_t)tid;
+    const unsigned fl =
+        j0 >= mine ? 0u
+        : one_each ? slice_update<R, KIND, 1>(base, snr, S, s_prm, s_vg, P, lo, ts, t, dt, inv_dt)
+                   : slice_update<R, KIND, 4>(base, snr, S, s_prm, s_vg, P, lo, ts, t, dt, inv_dt);
     // ---- compaction: this CTA's count, then its offset among the cluster's CTAs
     int total;
     const int c = __popc(fl);
@@ -525,7 +530,7 @@ small_cluster_kernel(const __grid_constant__ SmallDev D, const int64_t* __restri
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         if (!(fl & (1u << e))) continue;
-        const int32_t idx = (int32_t)(lo + j4 + e);
+        const int32_t idx = (int32_t)(lo + j0 + e);
         out[pos++] = idx;
         if (P.mon_cnt) {
           if (mpos < (unsigned long long)P.mon_cap) {
@@ -599,6 +604,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
   const int64_t n = P.n;
   const int64_t lo = (int64_t)rank * S;
   const int64_t mine = lo < n ? (n - lo < S ? n - lo : S) : 0;
+  const bool one_each = mine <= (int64_t)blockDim.x;   // one neuron per thread
   R* const base = reinterpret_cast<R*>(smem);   // the slice's variables, as in slice_update
   R* const sV = base;
   uint8_t* snr = smem + sizeof(R) * L.nvars * S;
@@ -671,11 +677,13 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
     const int slot = ring_slot(ts, P.ring_len);
     const int par = k & 1;
     int32_t* mylist = lists + par * S;
-    // ---- groups and thresholds: local neurons 4 tid .. 4 tid + 3
-    const int64_t j4 = 4 * (int64_t)tid;
-    const unsigned fl = j4 < mine ? slice_update<R, KIND>(base, snr, S, s_prm, s_vg, P, lo, ts,
-                                                             t, dt, inv_dt)
-                                  : 0u;
+    // ---- groups and thresholds: local neurons E tid .. E tid + E - 1 (E = 1 when the CTA
+    // has a thread for every neuron of its slice, else 4)
+    const int64_t j0 = (one_each ? 1 : 4) * (int64_t)tid;
+    const unsigned fl =
+        j0 >= mine ? 0u
+        : one_each ? slice_update<R, KIND, 1>(base, snr, S, s_prm, s_vg, P, lo, ts, t, dt, inv_dt)
+                   : slice_update<R, KIND, 4>(base, snr, S, s_prm, s_vg, P, lo, ts, t, dt, inv_dt);
     // ---- this CTA's spikes into its local list (ascending neuron order)
     // (most CTAs of most steps have no spike: one barrier decides that for the CTA)
     int total = 0, excl = 0;
@@ -685,7 +693,7 @@ small_pull_kernel(const __grid_constant__ SmallDev D, const int64_t* __restrict_
       int pos = excl;
 #pragma unroll
       for (int e = 0; e < 4; ++e)
-        if (fl & (1u << e)) mylist[pos++] = (int32_t)(lo + j4 + e);
+        if (fl & (1u << e)) mylist[pos++] = (int32_t)(lo + j0 + e);
     }
     if (tid == 0) s_cnt[par] = total;
     cl.sync();
@@ -817,8 +825,11 @@ cudaError_t launch_cluster_rk(const SmallDev& D, const int64_t* clock, int steps
   if (e == cudaSuccess && D.cluster > 8)
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
-  const int threads = (int)std::min<int64_t>(
-      kSmallThreads, std::max<int64_t>(256, ((D.slice / 4 + 31) / 32) * 32));
+  // a thread per neuron of the slice where that fits the CTA (the update is then one
+  // neuron's chain long), else a thread per four
+  const int64_t per = D.slice <= kSmallThreads ? D.slice : D.slice / 4;
+  const int threads =
+      (int)std::min<int64_t>(kSmallThreads, std::max<int64_t>(256, ((per + 31) / 32) * 32));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)D.cluster);
   cfg.blockDim = dim3((unsigned)threads);
