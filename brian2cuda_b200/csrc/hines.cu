@@ -36,6 +36,8 @@ namespace {
 
 constexpr int kHinesBlock = 256;
 constexpr int kHinesMaxStepsPerLaunch = 1000;
+constexpr int kHinesLargeCtas = 3;   // CTAs per SM of the large class (shared-memory bound)
+constexpr int kHinesSmallCtas = 5;   // and of the small class
 
 struct HinesDev {
   int32_t n_neurons;
@@ -106,8 +108,11 @@ __device__ __forceinline__ double recip(double x) {
   return fma(y, e, y);
 }
 
-template <typename RC>
-__global__ void __launch_bounds__(kHinesBlock)
+// MINB: CTAs per SM the register budget is sized for.  The large class runs 3 per SM (its
+// shared memory allows no more), so its kernel may keep its values in 80 registers instead of
+// spilling; the small class runs 5 per SM.
+template <typename RC, int MINB>
+__global__ void __launch_bounds__(kHinesBlock, MINB)
 hines_kernel(HinesDev H, int n_steps, int write_currents) {
   extern __shared__ __align__(16) uint8_t sm[];
   const int b = H.order[blockIdx.x];
@@ -350,6 +355,7 @@ struct b2b_hines {
   // own size beside the others (on stream2, forked from and joined to the net's stream), so
   // that small neurons do not reserve the largest neuron's shared memory.
   int32_t n_large = 0;                   // CTAs of the first launch (all neurons when 1 class)
+  bool large_fits5 = false;              // the first launch's image fits 5 CTAs per SM too
   b2b::HinesDev dev_small{};
   size_t smem_small = 0;
   cudaStream_t stream2 = nullptr;
@@ -544,6 +550,7 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
     }
     if (n_small == 0 || n_small == n_neurons || smem <= small_cap)
       std::fill(small.begin(), small.end(), 0);   // one class, one launch
+    h->large_fits5 = smem <= small_cap;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
       if (small[a] != small[c]) return small[a] < small[c];
       return cost[a] > cost[c];
@@ -589,9 +596,19 @@ b2b_status b2b_hines_create(b2b_net* net, int32_t n_neurons, const int64_t* comp
       h->dev_small.nc_max = ncs; h->dev_small.ns_max = nss; h->dev_small.nlev_max = nls;
       h->dev_small.order = D.order + n_large;
     }
-    if (e == cudaSuccess)
-      e = rc == 4 ? cudaFuncSetAttribute(hines_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                  : cudaFuncSetAttribute(hines_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // shared memory of each kernel variant: the first launch's image for the variant it runs
+    // (5 CTAs per SM when its image fits them), the small class's for the other
+    const int s5 = (int)std::max(h->large_fits5 ? smem : 0, n_large < n_neurons ? h->smem_small : 0);
+    if (e == cudaSuccess && !h->large_fits5)
+      e = rc == 4 ? cudaFuncSetAttribute(hines_kernel<float, kHinesLargeCtas>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                  : cudaFuncSetAttribute(hines_kernel<double, kHinesLargeCtas>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && s5 > 0)
+      e = rc == 4 ? cudaFuncSetAttribute(hines_kernel<float, kHinesSmallCtas>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, s5)
+                  : cudaFuncSetAttribute(hines_kernel<double, kHinesSmallCtas>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, s5);
     if (e != cudaSuccess) {
       b2b_hines_destroy(h);
       return e == cudaErrorMemoryAllocation ? B2B_ERR_OOM : B2B_ERR_CUDA;
@@ -660,16 +677,20 @@ b2b_status b2b_hines_run(b2b_hines* h, int64_t n_steps) {
       if (cudaStreamWaitEvent(h->stream2, h->ev_fork, 0) != cudaSuccess) return B2B_ERR_CUDA;
     }
     if (h->channel_dtype == B2B_F32) {
-      if (h->n_large > 0)
-        hines_kernel<float><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (h->n_large > 0 && h->large_fits5)
+        hines_kernel<float, kHinesSmallCtas><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      else if (h->n_large > 0)
+        hines_kernel<float, kHinesLargeCtas><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
       if (two)
-        hines_kernel<float><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+        hines_kernel<float, kHinesSmallCtas><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
                               h->stream2>>>(h->dev_small, k, wc);
     } else {
-      if (h->n_large > 0)
-        hines_kernel<double><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      if (h->n_large > 0 && h->large_fits5)
+        hines_kernel<double, kHinesSmallCtas><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
+      else if (h->n_large > 0)
+        hines_kernel<double, kHinesLargeCtas><<<h->n_large, kHinesBlock, h->smem, s>>>(h->dev, k, wc);
       if (two)
-        hines_kernel<double><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
+        hines_kernel<double, kHinesSmallCtas><<<h->n_neurons - h->n_large, kHinesBlock, h->smem_small,
                                h->stream2>>>(h->dev_small, k, wc);
     }
     if (cudaGetLastError() != cudaSuccess) return B2B_ERR_CUDA;
